@@ -1,0 +1,105 @@
+/*
+ * s2b.h -- C ABI of the B200 spin spherical-harmonic / Wigner transform library.
+ *
+ * Plain pointers and sizes only. Every entry point returns an int status
+ * (S2B_OK == 0) and never exits the process; s2b_last_error() gives the
+ * message of the last failure on the calling thread.
+ *
+ * Device buffers are caller-owned. Inputs are never modified. Execution is
+ * stream-ordered on the given cudaStream_t (passed as void*), performs no
+ * device allocation and no host synchronisation, so it can be captured in a
+ * CUDA graph once the plan exists.
+ *
+ * Array layouts (row-major, innermost last), for B = desc.batch maps:
+ *   flm   [B][L][2L-1]           complex, index [l][L-1+m]
+ *   f     [B][ntheta][nphi]      equiangular (mw, mwss, dh, gl)
+ *         [B][12*nside^2]        healpix, ring-ordered
+ *   f is complex, or real when desc.reality != 0.
+ *   complex = interleaved (re, im); double for S2B_F64, float for S2B_F32.
+ *   flmn  [B][2N-1][L][2L-1]     Wigner coefficients, index [N-1+n][l][L-1+m]
+ *   f_so3 [B][2N-1][ntheta][nphi] (or [B][2N-1][12 nside^2])
+ *
+ * Reference interfaces these replace (upstream astro-informatics/s2fft):
+ *   s2b_inverse  <- s2fft/transforms/spherical.py:21-109 (inverse, method dispatch)
+ *                   + transforms/otf_recursions.py:15-171 (inverse_latitudinal_step)
+ *   s2b_forward  <- s2fft/transforms/spherical.py:352-464 (forward, incl. iter refinement)
+ *                   + transforms/otf_recursions.py:432-588 (forward_latitudinal_step)
+ *   s2b_healpix_fft / s2b_healpix_ifft
+ *                <- lib/src/extensions.cc:26-100 (XLA custom call healpix_fft_cuda:
+ *                   healpix_forward / healpix_backward) and
+ *                   s2fft/utils/healpix_ffts.py:187-423 (healpix_fft / healpix_ifft)
+ *   s2b_plan_create <- lib/src/extensions.cc:115-149 (build_healpix_fft_descriptor,
+ *                   plan cache init) and recursions/price_mcewen.py:118-255
+ *                   (generate_precomputes_jax: per-plan recursion tables)
+ *   s2b_wigner_inverse / s2b_wigner_forward
+ *                <- s2fft/transforms/wigner.py:13-107, 346-439
+ *   s2b_kernel_build <- s2fft/precompute_transforms/construct.py:16-161
+ *                   (spin_spherical_kernel)
+ *   s2b_precompute_inverse / s2b_precompute_forward
+ *                <- s2fft/precompute_transforms/spherical.py:87-149, 314-380
+ */
+#ifndef S2B_H
+#define S2B_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum s2b_status {
+  S2B_OK = 0,
+  S2B_ERR_INVALID = 1,   /* bad descriptor or argument                   */
+  S2B_ERR_CUDA = 2,      /* a CUDA runtime call failed                    */
+  S2B_ERR_WORKSPACE = 3, /* workspace missing or too small                */
+  S2B_ERR_ALIGN = 4,     /* a pointer is NULL or not 16-byte aligned      */
+  S2B_ERR_TIMEOUT = 5,   /* a bounded device wait gave up (status word)   */
+  S2B_ERR_INTERNAL = 6
+};
+
+enum s2b_sampling { S2B_MW = 0, S2B_MWSS = 1, S2B_DH = 2, S2B_GL = 3, S2B_HEALPIX = 4 };
+
+/* S2B_F64: everything in double.
+ * S2B_F32: recursion and projection in float; recursion seeds, exponent
+ *          bookkeeping, lambda(theta, m) and quadrature weights in double. */
+enum s2b_precision { S2B_F64 = 0, S2B_F32 = 1 };
+
+typedef struct s2b_desc {
+  int L;          /* harmonic band-limit                                  */
+  int spin;       /* spin s (Wigner: ignored, set by N)                   */
+  int nside;      /* HEALPix resolution (healpix only)                    */
+  int sampling;   /* enum s2b_sampling                                    */
+  int reality;    /* signal is real (spin 0 only)                         */
+  int L_lower;    /* harmonic lower bound                                 */
+  int precision;  /* enum s2b_precision                                   */
+  int batch;      /* maps per execute call                                */
+  int iter;       /* forward: Jacobi refinement iterations                */
+  int N;          /* Wigner directional band-limit (0 = spin transform)   */
+} s2b_desc;
+
+typedef struct s2b_plan s2b_plan;
+
+/* Library version, e.g. 100 for 0.1.0. */
+int s2b_version(void);
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* s2b_last_error(void);
+
+/* Build a plan (host + device tables) on the current device. Synchronous. */
+int s2b_plan_create(const s2b_desc* desc, s2b_plan** plan);
+int s2b_plan_destroy(s2b_plan* plan);
+
+/* Bytes of device workspace an execute call needs (0 allowed). */
+int s2b_workspace_size(const s2b_plan* plan, int forward, size_t* bytes);
+
+/* Spin spherical-harmonic transforms. */
+int s2b_inverse(s2b_plan* plan, const void* flm, void* f, void* workspace,
+                size_t workspace_bytes, void* stream);
+int s2b_forward(s2b_plan* plan, const void* f, void* flm, void* workspace,
+                size_t workspace_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* S2B_H */

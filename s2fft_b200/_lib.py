@@ -1,0 +1,125 @@
+"""ctypes binding of ``libs2b.so`` and the plan cache.
+
+The library is the product: there is no CPU fallback. If the shared library
+is missing, or no CUDA device is present, every transform raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+import torch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libs2b.so")
+
+SAMPLING = {"mw": 0, "mwss": 1, "dh": 2, "gl": 3, "healpix": 4}
+PRECISION = {"f64": 0, "f32": 1}
+
+S2B_OK = 0
+STATUS = {1: "invalid argument", 2: "CUDA error", 3: "workspace too small",
+          4: "NULL or misaligned pointer", 5: "device wait timed out", 6: "internal error"}
+
+
+class S2BError(RuntimeError):
+    """A C-ABI call returned a non-zero status."""
+
+
+class Desc(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in
+                ("L", "spin", "nside", "sampling", "reality", "L_lower", "precision",
+                 "batch", "iter", "N")]
+
+
+_lib = None
+_lib_lock = threading.Lock()
+
+# name -> (argtypes); every entry point returns int
+_SIGS = {
+    "s2b_version": [],
+    "s2b_plan_create": [ctypes.POINTER(Desc), ctypes.POINTER(ctypes.c_void_p)],
+    "s2b_plan_destroy": [ctypes.c_void_p],
+    "s2b_workspace_size": [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)],
+    "s2b_inverse": [ctypes.c_void_p] * 4 + [ctypes.c_size_t, ctypes.c_void_p],
+    "s2b_forward": [ctypes.c_void_p] * 4 + [ctypes.c_size_t, ctypes.c_void_p],
+}
+
+
+def lib():
+    """Load the shared library (raises if it is absent)."""
+    global _lib
+    with _lib_lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(
+                    f"{LIB_PATH} not found: build it with `python -m s2fft_b200._build`")
+            handle = ctypes.CDLL(LIB_PATH)
+            for name, argt in _SIGS.items():
+                fn = getattr(handle, name)
+                fn.argtypes = argt
+                fn.restype = ctypes.c_int
+            handle.s2b_last_error.argtypes = []
+            handle.s2b_last_error.restype = ctypes.c_char_p
+            _lib = handle
+    return _lib
+
+
+def check(rc):
+    if rc != S2B_OK:
+        msg = lib().s2b_last_error().decode()
+        raise S2BError(f"s2b status {rc} ({STATUS.get(rc, '?')}): {msg}")
+
+
+class Plan:
+    """A device plan plus its cached workspaces (one per direction)."""
+
+    def __init__(self, device, **desc):
+        self.device = device
+        self.desc = dict(desc)
+        d = Desc(**desc)
+        ptr = ctypes.c_void_p()
+        with torch.cuda.device(device):
+            check(lib().s2b_plan_create(ctypes.byref(d), ctypes.byref(ptr)))
+        self.ptr = ptr
+        self._ws = {}
+
+    def workspace(self, forward):
+        key = int(bool(forward))
+        if key not in self._ws:
+            n = ctypes.c_size_t()
+            check(lib().s2b_workspace_size(self.ptr, key, ctypes.byref(n)))
+            self._ws[key] = torch.empty(max(int(n.value), 256), dtype=torch.uint8,
+                                        device=self.device)
+        return self._ws[key]
+
+    def __del__(self):
+        try:
+            if getattr(self, "ptr", None) and self.ptr.value:
+                lib().s2b_plan_destroy(self.ptr)
+        except Exception:
+            pass
+
+
+_plans: dict = {}
+_plans_lock = threading.Lock()
+
+
+def get_plan(device, **desc) -> Plan:
+    key = (str(device),) + tuple(sorted(desc.items()))
+    with _plans_lock:
+        plan = _plans.get(key)
+        if plan is None:
+            plan = Plan(device, **desc)
+            _plans[key] = plan
+    return plan
+
+
+def clear_plans():
+    with _plans_lock:
+        _plans.clear()
+
+
+def stream_handle(device):
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)

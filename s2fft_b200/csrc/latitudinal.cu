@@ -1,0 +1,465 @@
+// Fused Wigner-d recursion + projection (the latitudinal step of the spin SHT).
+//
+// Follows the Price-McEwen recursion of upstream s2fft
+// (s2fft/transforms/otf_recursions.py:15-171 inverse, 432-588 forward;
+// coefficients s2fft/recursions/price_mcewen.py:118-255): for fixed (theta, l)
+// the values d^l_{m,n}(theta), n = -spin, are generated from the edge m = l
+// towards m = 0 with a three-term recursion in m, so every (theta, l) pair is
+// an independent state. The projection onto ftm (inverse) or flm (forward)
+// happens in the same step, so the O(L^3) d-table never exists in memory.
+//
+// B200 formulation (own design, not the upstream loop):
+//  * monic form: d_m = g_{l,m} dt_m with dt_{m-1} = (lambda_m h_{l,m}) dt_m - dt_{m+1},
+//    lambda_m = 2 (n - m cos theta) / sin theta; g is folded into the inputs
+//    (inverse) or outputs (forward), so a step costs one MUL and one FMA;
+//  * lambda_m is evaluated once per (theta, m) as a single double FMA and then
+//    rounded (a float cot(theta) would shift theta systematically);
+//  * instead of renormalising every step in log space, each state carries a
+//    mantissa and an integer exponent (units of 2^kScale) that is updated every
+//    R steps, and only states above the significance floor are projected;
+//  * negative m comes from the symmetry d^l_{-m,n} = (-1)^(m-n) d^l_{m,-n}: a
+//    second recursion with n -> -n ("half" 1); for spin 0 both halves share one
+//    recursion and every state feeds two projections ("dual");
+//  * CTA tile = (QT*T rings) x (QA*K l's of one residue class l = j mod C), the
+//    l's of a thread strided by QA*C so that the triangular l >= m work stays
+//    balanced across lanes; states live in registers; per-step partial sums go
+//    to shared memory and are reduced every R steps, then accumulated into the
+//    output with vector atomics (reduction over l classes / ring tiles).
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <type_traits>
+
+#include "s2b_internal.h"
+
+namespace s2b {
+
+template <typename Real>
+struct Vec;
+template <>
+struct Vec<float> {
+  using t2 = float2;
+  using t4 = float4;
+};
+template <>
+struct Vec<double> {
+  using t2 = double2;
+  using t4 = double4;
+};
+
+template <typename Real>
+struct SeedT {
+  Real v;
+  int e;
+};
+
+// ---------------------------------------------------------------------------
+// Seeds d^l_{l,n}(theta) = (-1)^(l-n) sqrt(binom(2l, l+n)) cos^(l+n)(t/2) sin^(l-n)(t/2)
+// stored as mantissa * 2^(kScale * e) (price_mcewen.py:212-243 keeps the same
+// quantity as a float64 logarithm). Layout [half][class j][q][ring], l = j + C q.
+// ---------------------------------------------------------------------------
+template <typename Real>
+__global__ void seed_kernel(int L, int L0, int spin, int nhalf, int C, int Q,
+                            const RingInfo* __restrict__ rings, int nrings,
+                            const double* __restrict__ lbin, SeedT<Real>* __restrict__ out) {
+  const long total = (long)nhalf * C * Q * nrings;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long)gridDim.x * blockDim.x) {
+    const int r = (int)(idx % nrings);
+    long rest = idx / nrings;
+    const int q = (int)(rest % Q);
+    rest /= Q;
+    const int j = (int)(rest % C);
+    const int half = (int)(rest / C);
+    const int l = j + C * q;
+    const int n = half == 0 ? -spin : spin;
+    SeedT<Real> s{Real(0), 0};
+    if (l < L && l >= L0 && l >= (n < 0 ? -n : n)) {
+      const RingInfo ri = rings[r];
+      const double lg = lbin[l] + (double)(l + n) * ri.lc + (double)(l - n) * ri.ls;
+      int e = 0;
+      if (lg < Scaling<Real>::kSignif)
+        e = -(int)ceil((Scaling<Real>::kSignif - lg) / Scaling<Real>::kScale);
+      const double mant = exp2(lg - Scaling<Real>::kScale * (double)e);
+      s.v = (Real)((((l - n) & 1) ? -1.0 : 1.0) * mant);
+      s.e = e;
+    }
+    out[idx] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// main kernel
+// ---------------------------------------------------------------------------
+template <typename Real, bool FWD, bool DUAL, int T, int K, int QA, int QT, int R>
+struct LatCfg {
+  using R2 = typename Vec<Real>::t2;
+  using R4 = typename Vec<Real>::t4;
+  using Acc = std::conditional_t<DUAL, R4, R2>;
+  static constexpr int NT = QA * QT;
+  // shared buffer: inverse [R][T][QT][QA+1] Acc ; forward [R][K][QT][QA] Acc
+  static constexpr int kSmemInv = R * T * QT * (QA + 1);
+  static constexpr int kSmemFwd = R * K * QT * QA;
+  static constexpr int kSmemElems = FWD ? kSmemFwd : kSmemInv;
+  static constexpr size_t kSmemBytes = sizeof(Acc) * kSmemElems;
+};
+
+template <typename T2>
+__device__ __forceinline__ void red_add(T2* addr, T2 v);
+template <>
+__device__ __forceinline__ void red_add<float2>(float2* addr, float2 v) {
+  atomicAdd(addr, v);  // red.global.add.v2.f32 (sm_90+)
+}
+template <>
+__device__ __forceinline__ void red_add<double2>(double2* addr, double2 v) {
+  atomicAdd(&addr->x, v.x);
+  atomicAdd(&addr->y, v.y);
+}
+template <>
+__device__ __forceinline__ void red_add<float4>(float4* addr, float4 v) {
+  atomicAdd(addr, v);  // red.global.add.v4.f32 (sm_90+)
+}
+template <>
+__device__ __forceinline__ void red_add<double4>(double4* addr, double4 v) {
+  atomicAdd(&addr->x, v.x);
+  atomicAdd(&addr->y, v.y);
+  atomicAdd(&addr->z, v.z);
+  atomicAdd(&addr->w, v.w);
+}
+
+template <typename A>
+__device__ __forceinline__ A zero_acc() {
+  A a;
+  a.x = 0;
+  a.y = 0;
+  if constexpr (sizeof(A) == 4 * sizeof(a.x)) {
+    a.z = 0;
+    a.w = 0;
+  }
+  return a;
+}
+
+template <typename A>
+__device__ __forceinline__ void acc_add(A& a, const A& b) {
+  a.x += b.x;
+  a.y += b.y;
+  if constexpr (sizeof(A) == 4 * sizeof(a.x)) {
+    a.z += b.z;
+    a.w += b.w;
+  }
+}
+
+// d_m * (vector) accumulate: a += x * f
+template <typename A, typename Real>
+__device__ __forceinline__ void acc_fma(A& a, Real x, const A& f) {
+  a.x = fma(x, f.x, a.x);
+  a.y = fma(x, f.y, a.y);
+  if constexpr (sizeof(A) == 4 * sizeof(Real)) {
+    a.z = fma(x, f.z, a.z);
+    a.w = fma(x, f.w, a.w);
+  }
+}
+
+template <typename Real, bool FWD, bool DUAL, int T, int K, int QA, int QT, int R>
+__global__ void __launch_bounds__(QA* QT)
+    lat_kernel(const LatParams p) {
+  using Cfg = LatCfg<Real, FWD, DUAL, T, K, QA, QT, R>;
+  using Acc = typename Cfg::Acc;
+  static_assert(R % 2 == 0, "R must be even");
+  static_assert(QA % 2 == 0, "QA must be even");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Acc* buf = reinterpret_cast<Acc*>(smem_raw);
+
+  const int tid = threadIdx.x;
+  const int ql = tid % QA;
+  const int qt = tid / QA;
+  const int L = p.L;
+  const int C = p.nclass;
+  const int j = blockIdx.y;
+  const int half = (int)(blockIdx.z % p.nhalf);
+  const int b = (int)(blockIdx.z / p.nhalf);
+  const int n = half == 0 ? -p.spin : p.spin;
+  const int Q = (L + C - 1) / C;  // l's per class (padded)
+  const int rbase = blockIdx.x * (QT * T) + qt * T;
+  if (j >= L) return;
+  const int lmax = j + C * ((L - 1 - j) / C);
+
+  // ring constants: lambda = n*A - m*B (double FMA per (ring, m))
+  double nA[T], Bc[T];
+  int rrow[T];
+#pragma unroll
+  for (int i = 0; i < T; ++i) {
+    const int r = rbase + i;
+    if (r < p.nrings) {
+      nA[i] = (double)n * p.rings[r].A;
+      Bc[i] = p.rings[r].B;
+      rrow[i] = p.ring_row[r];
+    } else {
+      nA[i] = 0.0;
+      Bc[i] = 0.0;
+      rrow[i] = -1;
+    }
+  }
+
+  Real v[K][T], w[K][T], sc[K][T];
+  int ex[K][T];
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+#pragma unroll
+    for (int i = 0; i < T; ++i) {
+      v[k][i] = Real(0);
+      w[k][i] = Real(0);
+      sc[k][i] = Real(0);
+      ex[k][i] = 0;
+    }
+
+  const Real* __restrict__ Hc = reinterpret_cast<const Real*>(p.H) + (size_t)j * L * Q;
+  const SeedT<Real>* __restrict__ seeds =
+      reinterpret_cast<const SeedT<Real>*>(p.seeds) + ((size_t)half * C + j) * Q * p.nrings;
+  // inverse input F [b][half][j][m][q]; forward input G [b][half][m][ring]
+  const Acc* __restrict__ Fin;
+  if constexpr (!FWD)
+    Fin = reinterpret_cast<const Acc*>(p.in) + (((size_t)b * p.nhalf + half) * C + j) * L * Q;
+  else
+    Fin = reinterpret_cast<const Acc*>(p.in) + ((size_t)b * p.nhalf + half) * L * p.nrows;
+
+  // even-aligned chunk boundaries: chunk k covers m in [clo(k), clo(k+1)-1]
+  auto clo = [&](int k) -> int {
+    const int x = j + C * QA * k;
+    return k == 0 ? 0 : (x & ~1);
+  };
+  int mtop = lmax | 1;  // odd, >= lmax
+  // highest chunk that contains any valid l of this class
+  int ktop = (lmax - j) / (C * QA);
+  if (ktop > K - 1) ktop = K - 1;
+
+  int gstep = 0;  // steps since the last reduction
+  int mgrp = mtop;  // m of the first step of the current reduction group
+
+  // reduction + renormalisation, every R steps (and at the end)
+  auto flush = [&](int nsteps) {
+    __syncthreads();
+    if constexpr (!FWD) {
+      // buf [s][i][qt][ql] (row stride QA+1) -> sum over ql
+      const int items = R * T * QT;
+      for (int o = tid; o < items; o += Cfg::NT) {
+        const int s = o / (T * QT);
+        const int rem = o % (T * QT);
+        const int i = rem / QT;
+        const int qq = rem % QT;
+        if (s >= nsteps) continue;
+        const int m = mgrp - s;
+        const int r = blockIdx.x * (QT * T) + qq * T + i;
+        if (m < 0 || m >= L || r >= p.nrings) continue;
+        const Acc* row = buf + ((s * T + i) * QT + qq) * (QA + 1);
+        Acc a = zero_acc<Acc>();
+#pragma unroll
+        for (int x = 0; x < QA; ++x) acc_add(a, row[x]);
+        using R2 = typename Cfg::R2;
+        R2* ftm = reinterpret_cast<R2*>(p.out) +
+                  ((size_t)b * p.nrows + p.ring_row[r]) * p.ncol;
+        const int mo = p.mo;
+        if constexpr (DUAL) {
+          R2 ap, an;
+          ap.x = a.x;
+          ap.y = a.y;
+          an.x = a.z;
+          an.y = a.w;
+          red_add(ftm + (L - 1 + m + mo), ap);
+          if (m > 0) red_add(ftm + (L - 1 - m + mo), an);
+        } else {
+          R2 ap;
+          ap.x = a.x;
+          ap.y = a.y;
+          if (half == 0)
+            red_add(ftm + (L - 1 + m + mo), ap);
+          else if (m > 0)
+            red_add(ftm + (L - 1 - m + mo), ap);
+        }
+      }
+    } else {
+      // buf [s][k][qt][ql] -> sum over qt; out acc [b][half][j][m][q]
+      const int items = R * K * QA;
+      for (int o = tid; o < items; o += Cfg::NT) {
+        const int s = o / (K * QA);
+        const int rem = o % (K * QA);
+        const int k = rem / QA;
+        const int x = rem % QA;
+        if (s >= nsteps) continue;
+        const int m = mgrp - s;
+        const int q = x + QA * k;
+        const int l = j + C * q;
+        if (m < 0 || m >= L || l >= L || l < m) continue;
+        Acc a = zero_acc<Acc>();
+#pragma unroll
+        for (int y = 0; y < QT; ++y) acc_add(a, buf[((s * K + k) * QT + y) * QA + x]);
+        Acc* out = reinterpret_cast<Acc*>(p.out) +
+                   ((((size_t)b * p.nhalf + half) * C + j) * L + m) * Q + q;
+        red_add(out, a);
+      }
+    }
+    __syncthreads();
+    // renormalise states whose mantissa grew past the trigger
+    Real mx = Real(0);
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+#pragma unroll
+      for (int i = 0; i < T; ++i) mx = fmax(mx, fabs(v[k][i]));
+    const Real trig = Scaling<Real>::kTrig;
+    if (mx > trig) {
+      const Real down = Scaling<Real>::kDown;
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+#pragma unroll
+        for (int i = 0; i < T; ++i)
+          if (fabs(v[k][i]) > trig) {
+            v[k][i] *= down;
+            w[k][i] *= down;
+            ex[k][i] += 1;
+            sc[k][i] = ex[k][i] >= 0 ? Real(1) : Real(0);
+          }
+    }
+  };
+
+  // one recursion step at m; CUR selects which register array holds dt_m
+#define S2B_STEP(CUR, PRV, KC)                                                         \
+  {                                                                                    \
+    const bool mvalid = (m < L);                                                       \
+    Real lam[T];                                                                       \
+    _Pragma("unroll") for (int i = 0; i < T; ++i) lam[i] = (Real)fma(-md, Bc[i], nA[i]); \
+    Acc accT[T];                                                                       \
+    _Pragma("unroll") for (int i = 0; i < T; ++i) accT[i] = zero_acc<Acc>();           \
+    Acc gin[T];                                                                        \
+    if constexpr (FWD) {                                                               \
+      _Pragma("unroll") for (int i = 0; i < T; ++i) {                                  \
+        gin[i] = (mvalid && rrow[i] >= 0) ? Fin[(size_t)m * p.nrows + rrow[i]]         \
+                                          : zero_acc<Acc>();                           \
+      }                                                                                \
+    }                                                                                  \
+    _Pragma("unroll") for (int k = KC; k < K; ++k) {                                   \
+      const int q = ql + QA * k;                                                       \
+      const int l = j + C * q;                                                         \
+      if (k == KC) {                                                                   \
+        if (l == m && l < L) {                                                         \
+          const SeedT<Real>* sp = seeds + (size_t)q * p.nrings;                        \
+          _Pragma("unroll") for (int i = 0; i < T; ++i) {                              \
+            const int r = rbase + i;                                                   \
+            SeedT<Real> sd = (r < p.nrings) ? sp[r] : SeedT<Real>{Real(0), 0};         \
+            CUR[k][i] = sd.v;                                                          \
+            PRV[k][i] = Real(0);                                                       \
+            ex[k][i] = sd.e;                                                           \
+            sc[k][i] = sd.e >= 0 ? Real(1) : Real(0);                                  \
+          }                                                                            \
+        }                                                                              \
+      }                                                                                \
+      Real h = Real(0);                                                                \
+      Acc fk = zero_acc<Acc>();                                                        \
+      if (mvalid && l < L) {                                                           \
+        h = Hc[(size_t)m * Q + q];                                                     \
+        if constexpr (!FWD) fk = Fin[(size_t)m * Q + q];                               \
+      }                                                                                \
+      Acc accK = zero_acc<Acc>();                                                      \
+      _Pragma("unroll") for (int i = 0; i < T; ++i) {                                  \
+        const Real x = CUR[k][i] * sc[k][i];                                           \
+        if constexpr (!FWD)                                                            \
+          acc_fma(accT[i], x, fk);                                                     \
+        else                                                                           \
+          acc_fma(accK, x, gin[i]);                                                    \
+        PRV[k][i] = fma(lam[i] * h, CUR[k][i], -PRV[k][i]);                            \
+      }                                                                                \
+      if constexpr (FWD) buf[(((gstep)*K + k) * QT + qt) * QA + ql] = accK;            \
+    }                                                                                  \
+    if constexpr (FWD) {                                                               \
+      _Pragma("unroll") for (int k = 0; k < KC; ++k)                                   \
+          buf[(((gstep)*K + k) * QT + qt) * QA + ql] = zero_acc<Acc>();                \
+    } else {                                                                           \
+      _Pragma("unroll") for (int i = 0; i < T; ++i)                                    \
+          buf[(((gstep)*T + i) * QT + qt) * (QA + 1) + ql] = accT[i];                  \
+    }                                                                                  \
+    ++gstep;                                                                           \
+    --m;                                                                               \
+    md -= 1.0;                                                                         \
+  }
+
+  int m = mtop;
+  double md = (double)mtop;
+#pragma unroll
+  for (int kc = K - 1; kc >= 0; --kc) {
+    if (kc > ktop) continue;
+    const int lo = clo(kc);
+    // m runs from the current value down to lo, two steps at a time (even length)
+    while (m >= lo) {
+      S2B_STEP(v, w, kc)
+      S2B_STEP(w, v, kc)
+      if (gstep == R) {
+        flush(R);
+        gstep = 0;
+        mgrp = m;
+      }
+    }
+  }
+  if (gstep > 0) flush(gstep);
+#undef S2B_STEP
+}
+
+// ---------------------------------------------------------------------------
+// launch configuration
+// ---------------------------------------------------------------------------
+template <typename Real, bool FWD, bool DUAL, int T, int K, int QA, int QT, int R>
+static cudaError_t launch_cfg(const LatParams& p0, cudaStream_t s) {
+  using Cfg = LatCfg<Real, FWD, DUAL, T, K, QA, QT, R>;
+  LatParams p = p0;
+  p.nclass = (p.L + QA * K - 1) / (QA * K);
+  auto kern = lat_kernel<Real, FWD, DUAL, T, K, QA, QT, R>;
+  cudaError_t err =
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::kSmemBytes);
+  if (err != cudaSuccess) return err;
+  dim3 grid((p.nrings + QT * T - 1) / (QT * T), p.nclass, p.nhalf * p.batch);
+  kern<<<grid, Cfg::NT, Cfg::kSmemBytes, s>>>(p);
+  return cudaGetLastError();
+}
+
+int lat_nclass(bool fp64, int L) {
+  const int per = fp64 ? 16 * 4 : 16 * 4;
+  return (L + per - 1) / per;
+}
+
+cudaError_t launch_latitudinal(bool fp64, bool forward, bool dual, const LatParams& p,
+                               cudaStream_t s) {
+  if (!fp64) {
+    if (!forward)
+      return dual ? launch_cfg<float, false, true, 4, 4, 16, 8, 4>(p, s)
+                  : launch_cfg<float, false, false, 4, 4, 16, 8, 4>(p, s);
+    return dual ? launch_cfg<float, true, true, 4, 4, 16, 8, 4>(p, s)
+                : launch_cfg<float, true, false, 4, 4, 16, 8, 4>(p, s);
+  }
+  if (!forward)
+    return dual ? launch_cfg<double, false, true, 2, 4, 16, 8, 4>(p, s)
+                : launch_cfg<double, false, false, 2, 4, 16, 8, 4>(p, s);
+  return dual ? launch_cfg<double, true, true, 2, 4, 16, 8, 4>(p, s)
+              : launch_cfg<double, true, false, 2, 4, 16, 8, 4>(p, s);
+}
+
+cudaError_t launch_seeds(bool fp64, int L, int L0, int spin, int nhalf, const RingInfo* rings,
+                         int nrings, const double* lbin, void* seeds, cudaStream_t s) {
+  const int C = lat_nclass(fp64, L);
+  const int Q = (L + C - 1) / C;
+  const long total = (long)nhalf * C * Q * nrings;
+  const int threads = 256;
+  const int blocks = (int)((total + threads - 1) / threads > 4096 ? 4096 : (total + threads - 1) / threads);
+  if (fp64)
+    seed_kernel<double><<<blocks, threads, 0, s>>>(L, L0, spin, nhalf, C, Q, rings, nrings, lbin,
+                                                   reinterpret_cast<SeedT<double>*>(seeds));
+  else
+    seed_kernel<float><<<blocks, threads, 0, s>>>(L, L0, spin, nhalf, C, Q, rings, nrings, lbin,
+                                                  reinterpret_cast<SeedT<float>*>(seeds));
+  return cudaGetLastError();
+}
+
+size_t seed_bytes(bool fp64, int L, int nhalf, int nrings) {
+  const int C = lat_nclass(fp64, L);
+  const int Q = (L + C - 1) / C;
+  return (size_t)nhalf * C * Q * nrings * (fp64 ? sizeof(SeedT<double>) : sizeof(SeedT<float>));
+}
+
+}  // namespace s2b

@@ -1,0 +1,882 @@
+// Host side of the C ABI: plan construction and execution order.
+//
+// A plan holds every table a transform needs, computed once in double on the
+// host and uploaded (the role of upstream's precomps / generate_precomputes_jax,
+// s2fft/recursions/price_mcewen.py:118-255, and of the cuFFT plan cache,
+// lib/src/plan_cache.cc:12-50): ring colatitudes and quadrature weights
+// (s2fft/sampling/s2_samples.py:203-308, s2fft/utils/quadrature.py:7-320),
+// monic recursion coefficients, log-binomial seed prefactors, HEALPix ring
+// geometry and phase offsets (healpix_ffts.py:429-452), FFT twiddles, chirps
+// and pre-transformed Bluestein filters. Plans are owned by the caller
+// (create / destroy); execution is stream-ordered and allocation-free.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/s2b.h"
+#include "s2b_fft.h"
+#include "s2b_internal.h"
+#include "s2b_stages.h"
+
+namespace s2b {
+size_t seed_bytes(bool fp64, int L, int nhalf, int nrings);
+int lat_nclass(bool fp64, int L);
+}  // namespace s2b
+
+using namespace s2b;
+using cd = std::complex<double>;
+
+static thread_local std::string g_last_error;
+
+static int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define S2B_CK(call)                                                                    \
+  do {                                                                                  \
+    cudaError_t _e = (call);                                                            \
+    if (_e != cudaSuccess)                                                              \
+      return fail(S2B_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(_e));    \
+  } while (0)
+
+static const double kPi = 3.14159265358979323846;
+
+// ----------------------------------------------------------------------------
+// sampling geometry and quadrature (double)
+// ----------------------------------------------------------------------------
+static int ntheta(int L, int sampling, int nside) {
+  switch (sampling) {
+    case S2B_MW:
+    case S2B_GL:
+      return L;
+    case S2B_MWSS:
+      return L + 1;
+    case S2B_DH:
+      return 2 * L;
+    default:
+      return 4 * nside - 1;
+  }
+}
+
+static int nphi_equiang(int L, int sampling) { return sampling == S2B_MWSS ? 2 * L : 2 * L - 1; }
+
+static void gauss_legendre(int L, std::vector<double>& nodes, std::vector<double>& weights) {
+  // Newton iteration on P_L (quadrature.py:125-161); nodes ascending in x.
+  nodes.assign(L, 0.0);
+  weights.assign(L, 0.0);
+  const int m = (L + 1) / 2;
+  for (int i = 1; i <= m; ++i) {
+    double z = std::cos(kPi * (i - 0.25) / (L + 0.5)), z1 = 2.0, pp = 0.0;
+    for (int it = 0; it < 100 && std::fabs(z - z1) > 1e-15; ++it) {
+      double p1 = 1.0, p2 = 0.0;
+      for (int j = 1; j <= L; ++j) {
+        const double p3 = p2;
+        p2 = p1;
+        p1 = ((2.0 * j - 1.0) * z * p2 - (j - 1.0) * p3) / j;
+      }
+      pp = L * (z * p1 - p2) / (z * z - 1.0);
+      z1 = z;
+      z = z1 - p1 / pp;
+    }
+    {
+      double p1 = 1.0, p2 = 0.0;
+      for (int j = 1; j <= L; ++j) {
+        const double p3 = p2;
+        p2 = p1;
+        p1 = ((2.0 * j - 1.0) * z * p2 - (j - 1.0) * p3) / j;
+      }
+      pp = L * (z * p1 - p2) / (z * z - 1.0);
+    }
+    const double w = 2.0 / ((1.0 - z * z) * pp * pp);
+    nodes[L - i] = z;  // descending cos -> ascending theta after arccos
+    nodes[i - 1] = -z;
+    weights[i - 1] = w;
+    weights[L - i] = w;
+  }
+}
+
+static std::vector<double> thetas(int L, int sampling, int nside) {
+  const int nt = ntheta(L, sampling, nside);
+  std::vector<double> th(nt);
+  if (sampling == S2B_GL) {
+    std::vector<double> x, w;
+    gauss_legendre(L, x, w);
+    // thetas = flip(arccos(nodes ascending)) -> ascending theta
+    for (int t = 0; t < L; ++t) th[t] = std::acos(x[L - 1 - t]);
+    return th;
+  }
+  for (int t = 0; t < nt; ++t) {
+    switch (sampling) {
+      case S2B_MW:
+        th[t] = (2.0 * t + 1.0) * kPi / (2.0 * L - 1.0);
+        break;
+      case S2B_MWSS:
+        th[t] = 2.0 * t * kPi / (2.0 * L);
+        break;
+      case S2B_DH:
+        th[t] = (2.0 * t + 1.0) * kPi / (4.0 * L);
+        break;
+      default: {
+        double z;
+        if (t < nside - 1)
+          z = 1.0 - (t + 1.0) * (t + 1.0) / (3.0 * nside * nside);
+        else if (t <= 3 * nside - 1)
+          z = 4.0 / 3.0 - 2.0 * (t + 1.0) / (3.0 * nside);
+        else
+          z = (4.0 * nside - 1.0 - t) * (4.0 * nside - 1.0 - t) / (3.0 * nside * nside) - 1.0;
+        th[t] = std::acos(z);
+      }
+    }
+  }
+  return th;
+}
+
+// exact DFT helper on the host (used only at plan time for small tables)
+static std::vector<cd> dft_exact(const std::vector<cd>& x) {
+  const int n = (int)x.size();
+  std::vector<cd> tw(n);
+  for (int k = 0; k < n; ++k) tw[k] = cd(std::cos(-2.0 * kPi * k / n), std::sin(-2.0 * kPi * k / n));
+  std::vector<cd> X(n);
+  for (int j = 0; j < n; ++j) {
+    cd s = 0;
+    long idx = 0;
+    for (int k = 0; k < n; ++k) {
+      s += x[k] * tw[idx];
+      idx += j;
+      if (idx >= n) idx -= n;
+    }
+    X[j] = s;
+  }
+  return X;
+}
+
+static cd mw_weight(int m) {
+  if (m == 1) return cd(0, kPi / 2);
+  if (m == -1) return cd(0, -kPi / 2);
+  if (m % 2 == 0) return cd(2.0 / (1.0 - (double)m * m), 0);
+  return 0;
+}
+
+// transform weights (quadrature.py:7-50); MW/MWSS use the MWSS grid at 2L
+static std::vector<double> transform_weights(int L, int sampling, int nside) {
+  std::vector<double> q;
+  if (sampling == S2B_MW || sampling == S2B_MWSS) {
+    const int Lp = 2 * L;  // quad_weights_mwss_theta_only(2L)
+    std::vector<cd> w(2 * Lp, 0.0);
+    for (int i = -(Lp - 1) + 1; i < Lp + 1; ++i) w[i + Lp - 1] = mw_weight(i - 1);
+    // ifftshift: index k of shifted = (k + n/2) mod n of the original
+    const int n = 2 * Lp;
+    std::vector<cd> ws(n);
+    for (int k = 0; k < n; ++k) ws[k] = w[(k + n / 2) % n];
+    std::vector<cd> W = dft_exact(ws);
+    std::vector<double> wr(n);
+    for (int k = 0; k < n; ++k) wr[k] = W[k].real() / n;
+    q.assign(wr.begin(), wr.begin() + Lp + 1);
+    for (int i = 1; i < Lp; ++i) q[i] += wr[n - i];  // (-1)^0 * wr[-1:L:-1]
+    for (auto& v : q) v *= 2.0 * kPi / (2.0 * L);
+  } else if (sampling == S2B_DH) {
+    std::vector<double> th = thetas(L, S2B_DH, 0);
+    q.resize(th.size());
+    for (size_t t = 0; t < th.size(); ++t) {
+      double s = 0.0;
+      for (int k = 0; k < L; ++k) s += std::sin((2.0 * k + 1.0) * th[t]) / (2.0 * k + 1.0);
+      q[t] = s * 2.0 / L * std::sin(th[t]) * 2.0 * kPi / (2.0 * L - 1.0);
+    }
+  } else if (sampling == S2B_GL) {
+    std::vector<double> x, w;
+    gauss_legendre(L, x, w);
+    q.resize(L);
+    for (int t = 0; t < L; ++t) q[t] = w[t] * 2.0 * kPi / (2.0 * L - 1.0);
+  } else {
+    q.assign(4 * nside - 1, 4.0 * kPi / (12.0 * nside * nside));
+  }
+  return q;
+}
+
+static int hp_nphi(int t, int nside) {
+  if (t < nside - 1) return 4 * (t + 1);
+  if (t <= 3 * nside - 1) return 4 * nside;
+  return 4 * (4 * nside - t - 1);
+}
+
+static double hp_phi0(int t, int nside) {
+  if (t + 1 >= nside && t + 1 <= 3 * nside) return 0.5 * ((t - nside + 2) % 2) * kPi / (2.0 * nside);
+  if (t + 1 > 3 * nside) return 0.5 * kPi / (2.0 * (4 * nside - t - 1));
+  return 0.5 * kPi / (2.0 * (t + 1));
+}
+
+// ----------------------------------------------------------------------------
+// FFT tables
+// ----------------------------------------------------------------------------
+static void fft_pow2_host(std::vector<cd>& a) {
+  const int n = (int)a.size();
+  for (int i = 1, j = 0; i < n; ++i) {
+    int bit = n >> 1;
+    for (; j & bit; bit >>= 1) j ^= bit;
+    j ^= bit;
+    if (i < j) std::swap(a[i], a[j]);
+  }
+  for (int len = 2; len <= n; len <<= 1) {
+    for (int i = 0; i < n; i += len)
+      for (int k = 0; k < len / 2; ++k) {
+        const double ang = -2.0 * kPi * k / len;
+        const cd w(std::cos(ang), std::sin(ang));
+        const cd u = a[i + k], v = a[i + k + len / 2] * w;
+        a[i + k] = u + v;
+        a[i + k + len / 2] = u - v;
+      }
+  }
+}
+
+static int ilog2(int x) {
+  int r = 0;
+  while ((1 << r) < x) ++r;
+  return r;
+}
+
+struct FFTBuild {
+  std::vector<FFTDesc> descs;
+  std::vector<cd> tw, chirp, bf;
+  std::map<int, int> by_n;       // n -> desc index
+  std::map<int, long> tw_by_M;   // M -> tw offset
+  int maxM = 1;
+
+  int add(int n) {
+    auto it = by_n.find(n);
+    if (it != by_n.end()) return it->second;
+    FFTDesc d{};
+    d.n = n;
+    const bool pow2 = (n & (n - 1)) == 0;
+    d.bluestein = pow2 ? 0 : 1;
+    d.M = pow2 ? n : (1 << ilog2(2 * n - 1));
+    if (d.M < 2) d.M = 2;
+    d.logM = ilog2(d.M);
+    auto tt = tw_by_M.find(d.M);
+    if (tt == tw_by_M.end()) {
+      const long off = (long)tw.size();
+      for (int k = 0; k < d.M / 2; ++k) {
+        const double ang = -2.0 * kPi * k / d.M;
+        tw.emplace_back(std::cos(ang), std::sin(ang));
+      }
+      tw_by_M[d.M] = off;
+      d.tw_off = off;
+    } else {
+      d.tw_off = tt->second;
+    }
+    if (d.bluestein) {
+      d.chirp_off = (long)chirp.size();
+      std::vector<cd> w(n);
+      for (int k = 0; k < n; ++k) {
+        const long r = ((long)k * k) % (2L * n);  // exact k^2 mod 2n
+        const double ang = -kPi * (double)r / n;
+        w[k] = cd(std::cos(ang), std::sin(ang));
+        chirp.push_back(w[k]);
+      }
+      std::vector<cd> b(d.M, 0.0);
+      b[0] = std::conj(w[0]);
+      for (int k = 1; k < n; ++k) {
+        b[k] = std::conj(w[k]);
+        b[d.M - k] = std::conj(w[k]);
+      }
+      fft_pow2_host(b);
+      d.bf_off = (long)bf.size();
+      std::vector<cd> br(d.M);
+      for (int k = 0; k < d.M; ++k) {
+        int rv = 0;
+        for (int bit = 0; bit < d.logM; ++bit)
+          if (k & (1 << bit)) rv |= 1 << (d.logM - 1 - bit);
+        br[rv] = b[k] / (double)d.M;
+      }
+      bf.insert(bf.end(), br.begin(), br.end());
+    }
+    maxM = std::max(maxM, d.M);
+    const int idx = (int)descs.size();
+    descs.push_back(d);
+    by_n[n] = idx;
+    return idx;
+  }
+};
+
+// ----------------------------------------------------------------------------
+// plan
+// ----------------------------------------------------------------------------
+struct DevBuf {
+  void* p = nullptr;
+  size_t n = 0;
+};
+
+struct s2b_plan {
+  s2b_desc d;
+  bool fp64;
+  size_t rsz;   // sizeof(Real)
+  int nth;      // rings of the sampling
+  int nphi;     // equiangular ring length
+  long npix;    // pixels per map
+  int nclass, Q;
+  int dual;     // spin 0 complex: both m signs from one recursion
+  int nhalf;
+  // inverse geometry
+  int inv_nrings, inv_ncol, inv_mo, inv_pole_s, inv_pole_n;
+  // forward geometry
+  int fwd_nrows, fwd_nrings, fwd_pole_s, fwd_pole_n;
+  int fwd_mode;  // 0 direct rows, 1 mw chain, 2 mwss chain
+  // device tables
+  std::vector<void*> allocs;
+  RingInfo* inv_rings = nullptr;
+  int* inv_ring_row = nullptr;
+  RingInfo* fwd_rings = nullptr;
+  int* fwd_ring_row = nullptr;
+  void* inv_seeds = nullptr;
+  void* fwd_seeds = nullptr;
+  double* lbin = nullptr;
+  double* gtab = nullptr;
+  void* htab = nullptr;
+  double* fwd_weights = nullptr;   // per forward row
+  double* hp_phi0 = nullptr;
+  long* ring_off = nullptr;        // pixel offsets of the sampling rings
+  int* ring_desc = nullptr;        // per ring FFT desc (healpix)
+  FFTDesc* descs = nullptr;
+  void* tw = nullptr;
+  void* chirp = nullptr;
+  void* bf = nullptr;
+  int row_desc = 0, col_d1 = 0, col_d2 = 0, maxM = 2, M1 = 2, M2 = 2;
+  // workspace layout (bytes)
+  size_t ws_inv_F, ws_inv_ftm, ws_fwd_cols, ws_fwd_G, ws_fwd_acc, ws_iter_f, ws_iter_flm;
+};
+
+template <typename T>
+static int upload(s2b_plan* p, T** dst, const std::vector<T>& src) {
+  if (src.empty()) {
+    *dst = nullptr;
+    return S2B_OK;
+  }
+  void* ptr = nullptr;
+  S2B_CK(cudaMalloc(&ptr, src.size() * sizeof(T)));
+  p->allocs.push_back(ptr);
+  S2B_CK(cudaMemcpy(ptr, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+  *dst = reinterpret_cast<T*>(ptr);
+  return S2B_OK;
+}
+
+static int upload_complex(s2b_plan* p, void** dst, const std::vector<cd>& src) {
+  if (src.empty()) {
+    *dst = nullptr;
+    return S2B_OK;
+  }
+  if (p->fp64) {
+    std::vector<double2> v(src.size());
+    for (size_t i = 0; i < src.size(); ++i) v[i] = make_double2(src[i].real(), src[i].imag());
+    double2* d = nullptr;
+    int rc = upload(p, &d, v);
+    *dst = d;
+    return rc;
+  }
+  std::vector<float2> v(src.size());
+  for (size_t i = 0; i < src.size(); ++i)
+    v[i] = make_float2((float)src[i].real(), (float)src[i].imag());
+  float2* d = nullptr;
+  int rc = upload(p, &d, v);
+  *dst = d;
+  return rc;
+}
+
+static RingInfo ring_info(double th) {
+  RingInfo r;
+  r.B = 2.0 * std::cos(th) / std::sin(th);
+  r.A = 2.0 / std::sin(th);
+  r.lc = std::log2(std::cos(th / 2.0));
+  r.ls = std::log2(std::sin(th / 2.0));
+  return r;
+}
+
+static int build_plan(s2b_plan* p) {
+  const s2b_desc& d = p->d;
+  const int L = d.L;
+  p->fp64 = d.precision == S2B_F64;
+  p->rsz = p->fp64 ? 8 : 4;
+  p->nth = ntheta(L, d.sampling, d.nside);
+  p->nphi = d.sampling == S2B_HEALPIX ? 0 : nphi_equiang(L, d.sampling);
+  p->npix = d.sampling == S2B_HEALPIX ? 12L * d.nside * d.nside : (long)p->nth * p->nphi;
+  p->dual = (d.spin == 0 && !d.reality) ? 1 : 0;
+  p->nhalf = (d.spin == 0) ? 1 : 2;
+  p->nclass = lat_nclass(p->fp64, L);
+  p->Q = (L + p->nclass - 1) / p->nclass;
+
+  // ---- recursion tables: g[m][l], h[j][m][q], lbin[l]
+  std::vector<double> g((size_t)L * L, 0.0), h((size_t)L * L, 0.0);
+  for (int l = 0; l < L; ++l) {
+    auto f = [&](int m) { return std::sqrt((double)(l + m) * (double)(l - m + 1)); };
+    std::vector<double> gl(l + 2, 0.0);
+    gl[l] = 1.0;
+    if (l >= 1) gl[l - 1] = 1.0 / f(l);
+    for (int m = l - 1; m >= 1; --m) gl[m - 1] = f(m + 1) * gl[m + 1] / f(m);
+    for (int m = 0; m <= l; ++m) g[(size_t)m * L + l] = gl[m];
+    h[(size_t)l * L + l] = 1.0;
+    for (int m = l - 1; m >= 0; --m) h[(size_t)m * L + l] = gl[m] / (f(m + 1) * gl[m + 1]);
+  }
+  int rc = upload(p, &p->gtab, g);
+  if (rc) return rc;
+  {
+    const int C = p->nclass, Q = p->Q;
+    if (p->fp64) {
+      std::vector<double> hc((size_t)C * L * Q, 0.0);
+      for (int j = 0; j < C; ++j)
+        for (int m = 0; m < L; ++m)
+          for (int q = 0; q < Q; ++q) {
+            const int l = j + C * q;
+            if (l < L) hc[((size_t)j * L + m) * Q + q] = h[(size_t)m * L + l];
+          }
+      double* dp = nullptr;
+      rc = upload(p, &dp, hc);
+      p->htab = dp;
+    } else {
+      std::vector<float> hc((size_t)C * L * Q, 0.0f);
+      for (int j = 0; j < C; ++j)
+        for (int m = 0; m < L; ++m)
+          for (int q = 0; q < Q; ++q) {
+            const int l = j + C * q;
+            if (l < L) hc[((size_t)j * L + m) * Q + q] = (float)h[(size_t)m * L + l];
+          }
+      float* fp = nullptr;
+      rc = upload(p, &fp, hc);
+      p->htab = fp;
+    }
+    if (rc) return rc;
+  }
+  {
+    const int as = std::abs(d.spin);
+    std::vector<double> lb(L, 0.0);
+    for (int l = 0; l < L; ++l) {
+      if (l < as) continue;
+      lb[l] = 0.5 * (std::lgamma(2.0 * l + 1.0) - std::lgamma(l + as + 1.0) -
+                     std::lgamma(l - as + 1.0)) / std::log(2.0);
+    }
+    rc = upload(p, &p->lbin, lb);
+    if (rc) return rc;
+  }
+
+  // ---- inverse geometry: rings of the sampling, poles in closed form
+  std::vector<double> th = thetas(L, d.sampling, d.nside);
+  {
+    std::vector<RingInfo> ri;
+    std::vector<int> rr;
+    p->inv_pole_s = -1;
+    p->inv_pole_n = -1;
+    for (int t = 0; t < p->nth; ++t) {
+      if (d.sampling == S2B_MW && t == p->nth - 1) {
+        p->inv_pole_s = t;
+        continue;
+      }
+      if (d.sampling == S2B_MWSS && (t == 0 || t == p->nth - 1)) {
+        if (t == 0)
+          p->inv_pole_n = t;
+        else
+          p->inv_pole_s = t;
+        continue;
+      }
+      ri.push_back(ring_info(th[t]));
+      rr.push_back(t);
+    }
+    p->inv_nrings = (int)ri.size();
+    p->inv_ncol = (d.sampling == S2B_MWSS || d.sampling == S2B_HEALPIX) ? 2 * L : 2 * L - 1;
+    p->inv_mo = (d.sampling == S2B_MWSS || d.sampling == S2B_HEALPIX) ? 1 : 0;
+    if ((rc = upload(p, &p->inv_rings, ri))) return rc;
+    if ((rc = upload(p, &p->inv_ring_row, rr))) return rc;
+  }
+  // ---- forward geometry
+  {
+    std::vector<RingInfo> ri;
+    std::vector<int> rr;
+    std::vector<double> w = transform_weights(L, d.sampling, d.nside);
+    if (d.sampling == S2B_MW || d.sampling == S2B_MWSS) {
+      p->fwd_mode = d.sampling == S2B_MW ? 1 : 2;
+      std::vector<double> th2 = thetas(2 * L, S2B_MWSS, 0);
+      p->fwd_nrows = 2 * L + 1;
+      p->fwd_pole_n = 0;
+      p->fwd_pole_s = 2 * L;
+      for (int t = 1; t < 2 * L; ++t) {
+        ri.push_back(ring_info(th2[t]));
+        rr.push_back(t);
+      }
+    } else {
+      p->fwd_mode = 0;
+      p->fwd_nrows = p->nth;
+      p->fwd_pole_n = -1;
+      p->fwd_pole_s = -1;
+      for (int t = 0; t < p->nth; ++t) {
+        ri.push_back(ring_info(th[t]));
+        rr.push_back(t);
+      }
+    }
+    p->fwd_nrings = (int)ri.size();
+    if ((rc = upload(p, &p->fwd_rings, ri))) return rc;
+    if ((rc = upload(p, &p->fwd_ring_row, rr))) return rc;
+    if ((rc = upload(p, &p->fwd_weights, w))) return rc;
+  }
+
+  // ---- seeds (device kernel, double arithmetic)
+  {
+    const size_t bi = seed_bytes(p->fp64, L, p->nhalf, p->inv_nrings);
+    const size_t bf = seed_bytes(p->fp64, L, p->nhalf, p->fwd_nrings);
+    S2B_CK(cudaMalloc(&p->inv_seeds, std::max<size_t>(bi, 16)));
+    p->allocs.push_back(p->inv_seeds);
+    S2B_CK(cudaMalloc(&p->fwd_seeds, std::max<size_t>(bf, 16)));
+    p->allocs.push_back(p->fwd_seeds);
+    if (p->inv_nrings > 0)
+      S2B_CK(launch_seeds(p->fp64, L, d.L_lower, d.spin, p->nhalf, p->inv_rings, p->inv_nrings,
+                          p->lbin, p->inv_seeds, 0));
+    S2B_CK(launch_seeds(p->fp64, L, d.L_lower, d.spin, p->nhalf, p->fwd_rings, p->fwd_nrings,
+                        p->lbin, p->fwd_seeds, 0));
+  }
+
+  // ---- FFT tables and ring layout
+  FFTBuild fb;
+  std::vector<long> roff(p->nth);
+  std::vector<int> rdesc;
+  if (d.sampling == S2B_HEALPIX) {
+    std::vector<double> phi0(p->nth);
+    rdesc.resize(p->nth);
+    long off = 0;
+    for (int t = 0; t < p->nth; ++t) {
+      const int n = hp_nphi(t, d.nside);
+      roff[t] = off;
+      off += n;
+      rdesc[t] = fb.add(n);
+      phi0[t] = hp_phi0(t, d.nside);
+    }
+    if ((rc = upload(p, &p->hp_phi0, phi0))) return rc;
+    if ((rc = upload(p, &p->ring_desc, rdesc))) return rc;
+  } else {
+    for (int t = 0; t < p->nth; ++t) roff[t] = (long)t * p->nphi;
+    p->row_desc = fb.add(p->nphi);
+  }
+  if ((rc = upload(p, &p->ring_off, roff))) return rc;
+  if (p->fwd_mode != 0) {
+    p->col_d1 = fb.add(p->fwd_mode == 1 ? 2 * L - 1 : 2 * L);
+    p->col_d2 = fb.add(4 * L);
+    p->M1 = fb.descs[p->col_d1].M;
+    p->M2 = fb.descs[p->col_d2].M;
+  }
+  p->maxM = 2;
+  if (d.sampling == S2B_HEALPIX) {
+    for (int t = 0; t < p->nth; ++t) p->maxM = std::max(p->maxM, fb.descs[rdesc[t]].M);
+  } else {
+    p->maxM = fb.descs[p->row_desc].M;
+  }
+  if ((rc = upload(p, &p->descs, fb.descs))) return rc;
+  if ((rc = upload_complex(p, &p->tw, fb.tw))) return rc;
+  if ((rc = upload_complex(p, &p->chirp, fb.chirp))) return rc;
+  if ((rc = upload_complex(p, &p->bf, fb.bf))) return rc;
+  const size_t maxsmem = (size_t)227 * 1024;
+  if ((size_t)p->maxM * 2 * p->rsz > maxsmem || (size_t)(p->M1 + p->M2) * 2 * p->rsz > maxsmem)
+    return fail(S2B_ERR_INVALID, "band-limit too large for the shared-memory ring FFT");
+
+  // ---- workspace layout
+  const size_t c2 = 2 * p->rsz;
+  const size_t acc = p->dual ? 2 * c2 : c2;
+  const size_t B = (size_t)d.batch;
+  p->ws_inv_F = B * p->nhalf * p->nclass * (size_t)L * p->Q * acc;
+  p->ws_inv_ftm = B * (size_t)p->nth * p->inv_ncol * c2;
+  const int ncm = p->fwd_mode == 1 ? 2 * L - 1 : 2 * L;
+  p->ws_fwd_cols = p->fwd_mode ? B * (size_t)ncm * p->nth * c2 : 0;
+  p->ws_fwd_G = B * p->nhalf * (size_t)L * p->fwd_nrows * acc;
+  p->ws_fwd_acc = B * p->nhalf * p->nclass * (size_t)L * p->Q * acc;
+  const size_t fel = d.reality ? p->rsz : c2;
+  p->ws_iter_f = d.iter > 0 ? B * (size_t)p->npix * fel : 0;
+  p->ws_iter_flm = d.iter > 0 ? B * (size_t)L * (2 * L - 1) * c2 : 0;
+  S2B_CK(cudaDeviceSynchronize());
+  return S2B_OK;
+}
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static size_t inv_ws(const s2b_plan* p) { return align256(p->ws_inv_F) + align256(p->ws_inv_ftm); }
+static size_t fwd_ws(const s2b_plan* p) {
+  size_t once = align256(p->ws_fwd_cols) + align256(p->ws_fwd_G) + align256(p->ws_fwd_acc);
+  if (p->d.iter > 0)
+    once = std::max(once, inv_ws(p)) + align256(p->ws_iter_f) + align256(p->ws_iter_flm);
+  return once;
+}
+
+// ----------------------------------------------------------------------------
+// execution
+// ----------------------------------------------------------------------------
+template <typename Real>
+static FFTTables<Real> tables(const s2b_plan* p) {
+  FFTTables<Real> t;
+  t.tw = reinterpret_cast<const typename FFTTables<Real>::R2*>(p->tw);
+  t.chirp = reinterpret_cast<const typename FFTTables<Real>::R2*>(p->chirp);
+  t.bfilt = reinterpret_cast<const typename FFTTables<Real>::R2*>(p->bf);
+  return t;
+}
+
+static int check_ptr(const void* ptr, const char* what) {
+  if (!ptr) return fail(S2B_ERR_ALIGN, std::string(what) + " is NULL");
+  if (reinterpret_cast<uintptr_t>(ptr) % 16 != 0)
+    return fail(S2B_ERR_ALIGN, std::string(what) + " is not 16-byte aligned");
+  return S2B_OK;
+}
+
+template <typename Real>
+static int run_inverse(s2b_plan* p, const void* flm, void* f, char* ws, cudaStream_t s) {
+  const s2b_desc& d = p->d;
+  const int L = d.L;
+  void* F = ws;
+  void* ftm = ws + align256(p->ws_inv_F);
+  S2B_CK(cudaMemsetAsync(ftm, 0, p->ws_inv_ftm, s));
+  StageParams sp{};
+  sp.L = L;
+  sp.L0 = d.L_lower;
+  sp.spin = d.spin;
+  sp.batch = d.batch;
+  sp.nclass = p->nclass;
+  sp.Q = p->Q;
+  sp.nhalf = p->nhalf;
+  sp.dual = p->dual;
+  sp.nrows = p->nth;
+  sp.ncol = p->inv_ncol;
+  sp.mo = p->inv_mo;
+  sp.pole_south = p->inv_pole_s;
+  sp.pole_north = p->inv_pole_n;
+  sp.g = p->gtab;
+  sp.flm = flm;
+  sp.F = F;
+  sp.ftm = ftm;
+  S2B_CK(launch_prologue(p->fp64, sp, s));
+  S2B_CK(launch_poles(p->fp64, sp, s));
+  if (p->inv_nrings > 0) {
+    LatParams lp{};
+    lp.L = L;
+    lp.L0 = d.L_lower;
+    lp.spin = d.spin;
+    lp.nrings = p->inv_nrings;
+    lp.nhalf = p->nhalf;
+    lp.batch = d.batch;
+    lp.rings = p->inv_rings;
+    lp.ring_row = p->inv_ring_row;
+    lp.seeds = p->inv_seeds;
+    lp.H = p->htab;
+    lp.in = F;
+    lp.out = ftm;
+    lp.nrows = p->nth;
+    lp.ncol = p->inv_ncol;
+    lp.mo = p->inv_mo;
+    lp.reality = d.reality;
+    S2B_CK(launch_latitudinal(p->fp64, false, p->dual, lp, s));
+  }
+  RowsParams<Real> rp{};
+  rp.L = L;
+  rp.nrows = p->nth;
+  rp.ncol = p->inv_ncol;
+  rp.mo = p->inv_mo;
+  rp.reality = d.reality;
+  rp.real_out = d.reality;
+  rp.scale = 1.0;
+  rp.desc = p->descs + p->row_desc;
+  rp.ring_desc = d.sampling == S2B_HEALPIX ? p->ring_desc : nullptr;
+  if (d.sampling == S2B_HEALPIX) rp.desc = p->descs;
+  rp.ring_off = p->ring_off;
+  rp.out_batch_stride = p->npix;
+  rp.phi0 = d.sampling == S2B_HEALPIX ? p->hp_phi0 : nullptr;
+  rp.tb = tables<Real>(p);
+  rp.in = ftm;
+  rp.out = f;
+  S2B_CK(launch_inv_rows<Real>(rp, p->nth, d.batch, p->maxM, s));
+  return S2B_OK;
+}
+
+template <typename Real>
+static int run_forward_once(s2b_plan* p, const void* f, void* flm, char* ws, cudaStream_t s) {
+  const s2b_desc& d = p->d;
+  const int L = d.L;
+  char* cols = ws;
+  char* G = cols + align256(p->ws_fwd_cols);
+  char* acc = G + align256(p->ws_fwd_G);
+  S2B_CK(cudaMemsetAsync(acc, 0, p->ws_fwd_acc, s));
+  RowsParams<Real> rp{};
+  rp.L = L;
+  rp.nrows = p->fwd_mode ? p->nth : p->fwd_nrows;
+  rp.mo = p->fwd_mode == 2 ? 1 : 0;
+  rp.real_in = d.reality;
+  rp.dual = p->dual;
+  rp.nhalf = p->nhalf;
+  rp.scale = 1.0;
+  rp.desc = p->descs + p->row_desc;
+  rp.ring_desc = nullptr;
+  if (d.sampling == S2B_HEALPIX) {
+    rp.desc = p->descs;
+    rp.ring_desc = p->ring_desc;
+    rp.phi0 = p->hp_phi0;
+  }
+  rp.ring_off = p->ring_off;
+  rp.out_batch_stride = p->npix;
+  rp.tb = tables<Real>(p);
+  rp.in = f;
+  if (p->fwd_mode == 0) {
+    rp.mode = FWD_TO_SPECTRA;
+    rp.weights = p->fwd_weights;
+    rp.out = G;
+    S2B_CK(launch_fwd_rows<Real>(rp, p->nth, d.batch, p->maxM, s));
+  } else {
+    rp.mode = FWD_TO_COLS;
+    rp.out = cols;
+    S2B_CK(launch_fwd_rows<Real>(rp, p->nth, d.batch, p->maxM, s));
+    ColsParams<Real> cp{};
+    cp.L = L;
+    cp.spin = d.spin;
+    cp.mw = p->fwd_mode == 1;
+    cp.nin = p->nth;
+    cp.dual = p->dual;
+    cp.nhalf = p->nhalf;
+    cp.scale = p->fwd_mode == 1 ? (2.0 * L) / (2.0 * L - 1.0) : 1.0;
+    cp.d1 = p->descs + p->col_d1;
+    cp.d2 = p->descs + p->col_d2;
+    cp.weights = p->fwd_weights;
+    cp.tb = tables<Real>(p);
+    cp.in = cols;
+    cp.out = G;
+    const int ncm = p->fwd_mode == 1 ? 2 * L - 1 : 2 * L;
+    S2B_CK(launch_mw_cols<Real>(cp, ncm, d.batch, p->M1, p->M2, s));
+  }
+  LatParams lp{};
+  lp.L = L;
+  lp.L0 = d.L_lower;
+  lp.spin = d.spin;
+  lp.nrings = p->fwd_nrings;
+  lp.nhalf = p->nhalf;
+  lp.batch = d.batch;
+  lp.rings = p->fwd_rings;
+  lp.ring_row = p->fwd_ring_row;
+  lp.seeds = p->fwd_seeds;
+  lp.H = p->htab;
+  lp.in = G;
+  lp.out = acc;
+  lp.nrows = p->fwd_nrows;
+  S2B_CK(launch_latitudinal(p->fp64, true, p->dual, lp, s));
+  StageParams sp{};
+  sp.L = L;
+  sp.L0 = d.L_lower;
+  sp.spin = d.spin;
+  sp.batch = d.batch;
+  sp.nclass = p->nclass;
+  sp.Q = p->Q;
+  sp.nhalf = p->nhalf;
+  sp.dual = p->dual;
+  sp.nrows = p->fwd_nrows;
+  sp.pole_south = p->fwd_pole_s;
+  sp.pole_north = p->fwd_pole_n;
+  sp.g = p->gtab;
+  sp.G = G;
+  sp.acc = acc;
+  sp.flm_out = flm;
+  S2B_CK(launch_epilogue(p->fp64, sp, s));
+  return S2B_OK;
+}
+
+template <typename Real>
+static int run_forward(s2b_plan* p, const void* f, void* flm, char* ws, cudaStream_t s) {
+  const s2b_desc& d = p->d;
+  int rc = run_forward_once<Real>(p, f, flm, ws, s);
+  if (rc || d.iter <= 0) return rc;
+  // Jacobi refinement: flm += F(f - I(flm))   (iterative_refinement.py:9-46)
+  const size_t scratch = std::max(align256(p->ws_fwd_cols) + align256(p->ws_fwd_G) +
+                                      align256(p->ws_fwd_acc),
+                                  inv_ws(p));
+  char* fr = ws + scratch;
+  char* dflm = fr + align256(p->ws_iter_f);
+  const long nf = (long)d.batch * p->npix * (d.reality ? 1 : 2);
+  const long nflm = (long)d.batch * d.L * (2 * d.L - 1);
+  for (int it = 0; it < d.iter; ++it) {
+    if ((rc = run_inverse<Real>(p, flm, fr, ws, s))) return rc;
+    S2B_CK(launch_sub(p->fp64, nf, f, fr, fr, s));
+    if ((rc = run_forward_once<Real>(p, fr, dflm, ws, s))) return rc;
+    S2B_CK(launch_axpy(p->fp64, nflm, 1.0, dflm, flm, s));
+  }
+  return S2B_OK;
+}
+
+// ----------------------------------------------------------------------------
+// C ABI
+// ----------------------------------------------------------------------------
+extern "C" {
+
+int s2b_version(void) { return 100; }
+
+const char* s2b_last_error(void) { return g_last_error.c_str(); }
+
+int s2b_plan_create(const s2b_desc* desc, s2b_plan** out) {
+  g_last_error.clear();
+  if (!desc || !out) return fail(S2B_ERR_INVALID, "desc and plan must be non-NULL");
+  const s2b_desc& d = *desc;
+  if (d.L < 2) return fail(S2B_ERR_INVALID, "L must be >= 2");
+  if (d.sampling < S2B_MW || d.sampling > S2B_HEALPIX)
+    return fail(S2B_ERR_INVALID, "unknown sampling");
+  if (d.sampling == S2B_HEALPIX) {
+    if (d.nside < 1) return fail(S2B_ERR_INVALID, "healpix sampling needs nside >= 1");
+    if (d.L < 2 * d.nside) return fail(S2B_ERR_INVALID, "healpix requires L >= 2*nside");
+  }
+  if (d.precision != S2B_F64 && d.precision != S2B_F32)
+    return fail(S2B_ERR_INVALID, "unknown precision");
+  if (d.reality && d.spin != 0) return fail(S2B_ERR_INVALID, "reality requires spin 0");
+  if (std::abs(d.spin) >= d.L) return fail(S2B_ERR_INVALID, "|spin| must be < L");
+  if (d.L_lower < 0 || d.L_lower >= d.L) return fail(S2B_ERR_INVALID, "0 <= L_lower < L");
+  if (d.batch < 1) return fail(S2B_ERR_INVALID, "batch must be >= 1");
+  if (d.iter < 0) return fail(S2B_ERR_INVALID, "iter must be >= 0");
+  if (d.L > 8192) return fail(S2B_ERR_INVALID, "L > 8192 not supported");
+  s2b_plan* p = new s2b_plan();
+  p->d = d;
+  const int rc = build_plan(p);
+  if (rc) {
+    for (void* a : p->allocs) cudaFree(a);
+    delete p;
+    return rc;
+  }
+  *out = p;
+  return S2B_OK;
+}
+
+int s2b_plan_destroy(s2b_plan* p) {
+  if (!p) return S2B_OK;
+  for (void* a : p->allocs) cudaFree(a);
+  delete p;
+  return S2B_OK;
+}
+
+int s2b_workspace_size(const s2b_plan* p, int forward, size_t* bytes) {
+  if (!p || !bytes) return fail(S2B_ERR_INVALID, "plan and bytes must be non-NULL");
+  *bytes = forward ? fwd_ws(p) : inv_ws(p);
+  return S2B_OK;
+}
+
+int s2b_inverse(s2b_plan* p, const void* flm, void* f, void* ws, size_t ws_bytes, void* stream) {
+  if (!p) return fail(S2B_ERR_INVALID, "plan is NULL");
+  int rc;
+  if ((rc = check_ptr(flm, "flm")) || (rc = check_ptr(f, "f")) || (rc = check_ptr(ws, "workspace")))
+    return rc;
+  if (ws_bytes < inv_ws(p)) return fail(S2B_ERR_WORKSPACE, "workspace too small");
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  return p->fp64 ? run_inverse<double>(p, flm, f, (char*)ws, s)
+                 : run_inverse<float>(p, flm, f, (char*)ws, s);
+}
+
+int s2b_forward(s2b_plan* p, const void* f, void* flm, void* ws, size_t ws_bytes, void* stream) {
+  if (!p) return fail(S2B_ERR_INVALID, "plan is NULL");
+  int rc;
+  if ((rc = check_ptr(flm, "flm")) || (rc = check_ptr(f, "f")) || (rc = check_ptr(ws, "workspace")))
+    return rc;
+  if (ws_bytes < fwd_ws(p)) return fail(S2B_ERR_WORKSPACE, "workspace too small");
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  return p->fp64 ? run_forward<double>(p, f, flm, (char*)ws, s)
+                 : run_forward<float>(p, f, flm, (char*)ws, s);
+}
+
+}  // extern "C"

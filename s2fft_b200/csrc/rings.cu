@@ -1,0 +1,464 @@
+// Ring FFTs and the element-wise stages around the latitudinal kernel.
+//
+// Replaces the longitudinal steps of upstream s2fft:
+//   equiangular rows: np.fft.fft / ifft / rfft / irfft in
+//     s2fft/transforms/spherical.py:191-208 (inverse) and 527-541 (forward);
+//   MW -> MWSS resampling and x2 upsampling (s2fft/utils/resampling.py:104-355),
+//     folded into one per-column chain in the phi-Fourier domain;
+//   HEALPix ring FFTs with spectral extension / folding and phi0 phase shifts
+//     (s2fft/utils/healpix_ffts.py:19-117, 187-226, 335-371, 482-509) and the
+//     native cuFFT path (lib/src/s2fft.cu:119-154, lib/src/s2fft_kernels.cu:46-235).
+//
+// One CTA per transform (ring, row or column). Lengths that are powers of two
+// use a radix-2 decimation-in-frequency pass; other lengths use Bluestein's
+// chirp-z algorithm with a power-of-two convolution (forward DIF, pointwise
+// product with the pre-transformed chirp filter in bit-reversed order, inverse
+// DIT), so no permutation pass is ever needed. Shifts, scalings, weights,
+// phase factors, spectral extension and folding are fused into the load/store
+// of each transform.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <type_traits>
+
+#include "s2b_fft.h"
+
+namespace s2b {
+
+template <typename Real>
+struct C2;
+template <>
+struct C2<float> {
+  using t = float2;
+};
+template <>
+struct C2<double> {
+  using t = double2;
+};
+
+template <typename R2>
+__device__ __forceinline__ R2 cmul(R2 a, R2 b) {
+  R2 r;
+  r.x = a.x * b.x - a.y * b.y;
+  r.y = a.x * b.y + a.y * b.x;
+  return r;
+}
+template <typename R2>
+__device__ __forceinline__ R2 cadd(R2 a, R2 b) {
+  R2 r;
+  r.x = a.x + b.x;
+  r.y = a.y + b.y;
+  return r;
+}
+template <typename R2>
+__device__ __forceinline__ R2 csub(R2 a, R2 b) {
+  R2 r;
+  r.x = a.x - b.x;
+  r.y = a.y - b.y;
+  return r;
+}
+template <typename R2>
+__device__ __forceinline__ R2 cconj(R2 a) {
+  a.y = -a.y;
+  return a;
+}
+template <typename R2, typename Real>
+__device__ __forceinline__ R2 cscale(R2 a, Real s) {
+  a.x *= s;
+  a.y *= s;
+  return a;
+}
+template <typename R2>
+__device__ __forceinline__ R2 czero() {
+  R2 r;
+  r.x = 0;
+  r.y = 0;
+  return r;
+}
+
+// tw[k] = exp(-2 pi i k / M), k < M/2. DIF: natural order in, bit-reversed out.
+template <typename R2>
+__device__ void fft_dif(R2* s, int M, const R2* __restrict__ tw, bool inv) {
+  for (int half = M >> 1, stride = 1; half >= 1; half >>= 1, stride <<= 1) {
+    __syncthreads();
+    for (int t = threadIdx.x; t < (M >> 1); t += blockDim.x) {
+      const int pos = t & (half - 1);
+      const int i0 = ((t - pos) << 1) + pos;
+      const int i1 = i0 + half;
+      const R2 a = s[i0], b = s[i1];
+      R2 w = tw[pos * stride];
+      if (inv) w.y = -w.y;
+      s[i0] = cadd(a, b);
+      s[i1] = cmul(csub(a, b), w);
+    }
+  }
+  __syncthreads();
+}
+
+// DIT: bit-reversed order in, natural out.
+template <typename R2>
+__device__ void fft_dit(R2* s, int M, const R2* __restrict__ tw, bool inv) {
+  for (int half = 1, stride = M >> 1; half < M; half <<= 1, stride >>= 1) {
+    __syncthreads();
+    for (int t = threadIdx.x; t < (M >> 1); t += blockDim.x) {
+      const int pos = t & (half - 1);
+      const int i0 = ((t - pos) << 1) + pos;
+      const int i1 = i0 + half;
+      R2 w = tw[pos * stride];
+      if (inv) w.y = -w.y;
+      const R2 a = s[i0];
+      const R2 b = cmul(s[i1], w);
+      s[i0] = cadd(a, b);
+      s[i1] = csub(a, b);
+    }
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ int bitrev(int x, int logM) { return __brev(x) >> (32 - logM); }
+
+// DFT of length d.n of the sequence produced by load(k) (k < n); after the call
+// get(j) returns X_j (j < n). inv selects exp(+2 pi i jk / n).
+// The buffer s must hold d.M complex values.
+template <typename Real, typename Load>
+__device__ void dft_run(typename C2<Real>::t* s, const FFTDesc& d, const FFTTables<Real>& tb,
+                        bool inv, Load load) {
+  using R2 = typename C2<Real>::t;
+  const R2* tw = tb.tw + d.tw_off;
+  if (d.bluestein) {
+    const R2* ch = tb.chirp + d.chirp_off;
+    const R2* bf = tb.bfilt + d.bf_off;
+    for (int k = threadIdx.x; k < d.M; k += blockDim.x) {
+      R2 x = czero<R2>();
+      if (k < d.n) {
+        x = load(k);
+        if (inv) x = cconj(x);
+        x = cmul(x, ch[k]);
+      }
+      s[k] = x;
+    }
+    fft_dif(s, d.M, tw, false);
+    for (int k = threadIdx.x; k < d.M; k += blockDim.x) s[k] = cmul(s[k], bf[k]);
+    fft_dit(s, d.M, tw, true);
+  } else {
+    for (int k = threadIdx.x; k < d.M; k += blockDim.x) {
+      R2 x = load(k);
+      if (inv) x = cconj(x);
+      s[k] = x;
+    }
+    fft_dif(s, d.M, tw, false);
+  }
+}
+
+template <typename Real>
+__device__ __forceinline__ typename C2<Real>::t dft_get(const typename C2<Real>::t* s,
+                                                        const FFTDesc& d,
+                                                        const FFTTables<Real>& tb, bool inv,
+                                                        int j) {
+  using R2 = typename C2<Real>::t;
+  R2 x;
+  if (d.bluestein)
+    x = cmul(s[j], tb.chirp[d.chirp_off + j]);
+  else
+    x = s[bitrev(j, d.logM)];
+  return inv ? cconj(x) : x;
+}
+
+__device__ __forceinline__ int pmod(int a, int n) {
+  int r = a % n;
+  return r < 0 ? r + n : r;
+}
+
+// ---------------------------------------------------------------------------
+// Inverse rows: ftm [B][nrows][ncol] -> f (equiangular rows or HEALPix rings).
+// One CTA per (ring, map). Column c of ftm holds m = c - (L-1) - mo.
+// ---------------------------------------------------------------------------
+template <typename Real>
+__global__ void inv_rows_kernel(RowsParams<Real> p) {
+  using R2 = typename C2<Real>::t;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R2* s = reinterpret_cast<R2*>(smem_raw);
+  const int t = blockIdx.x;
+  const int b = blockIdx.y;
+  const FFTDesc d = p.desc[p.ring_desc ? p.ring_desc[t] : 0];
+  const int n = d.n;
+  const R2* row = reinterpret_cast<const R2*>(p.in) + ((size_t)b * p.nrows + t) * p.ncol;
+  const int L = p.L;
+  const double phi0 = p.phi0 ? p.phi0[t] : 0.0;
+  // coefficient C_m with the HEALPix phase exp(+i m phi0) and reality mirror
+  auto coef = [&](int m) -> R2 {
+    R2 c;
+    if (p.reality && m < 0) {
+      c = cconj(row[L - 1 - m + p.mo]);
+      if (p.phi0) {
+        double sn, cs;
+        sincos((double)(-m) * phi0, &sn, &cs);
+        R2 e;
+        e.x = (Real)cs;
+        e.y = (Real)sn;
+        c = cconj(cmul(cconj(c), e));
+      }
+      return c;
+    }
+    c = row[L - 1 + m + p.mo];
+    if (p.phi0) {
+      double sn, cs;
+      sincos((double)m * phi0, &sn, &cs);
+      R2 e;
+      e.x = (Real)cs;
+      e.y = (Real)sn;
+      c = cmul(c, e);
+    }
+    return c;
+  };
+  const int mlo = p.reality ? -(L - 1) : -(L - 1) - p.mo;  // lowest m present
+  const int mhi = L - 1;
+  auto load = [&](int k) -> R2 {
+    // X_k = sum of C_m over m == k (mod n), m in [mlo, mhi]
+    R2 acc = czero<R2>();
+    if (n >= p.ncol) {
+      // no aliasing: unique m with m mod n == k, |m| small
+      int m = k;
+      if (m > mhi) m -= n;
+      if (m >= mlo && m <= mhi) acc = coef(m);
+      return acc;
+    }
+    int m = k;
+    while (m - n >= mlo) m -= n;
+    for (; m <= mhi; m += n) acc = cadd(acc, coef(m));
+    return acc;
+  };
+  dft_run<Real>(s, d, p.tb, true, load);
+  const Real scale = (Real)p.scale;
+  if (p.real_out) {
+    Real* out = reinterpret_cast<Real*>(p.out) + (size_t)b * p.out_batch_stride + p.ring_off[t];
+    for (int j = threadIdx.x; j < n; j += blockDim.x)
+      out[j] = dft_get<Real>(s, d, p.tb, true, j).x * scale;
+  } else {
+    R2* out = reinterpret_cast<R2*>(p.out) + (size_t)b * p.out_batch_stride + p.ring_off[t];
+    for (int j = threadIdx.x; j < n; j += blockDim.x)
+      out[j] = cscale(dft_get<Real>(s, d, p.tb, true, j), scale);
+  }
+}
+
+template <typename Real, typename Val>
+__device__ __forceinline__ void store_spectra(const RowsParams<Real>& p, int b, int t, Val val) {
+  using R2 = typename C2<Real>::t;
+  const int L = p.L;
+  if (p.dual) {
+    using R4 = std::conditional_t<sizeof(Real) == 4, float4, double4>;
+    R4* out = reinterpret_cast<R4*>(p.out);
+    for (int m = threadIdx.x; m < L; m += blockDim.x) {
+      const R2 a = val(m);
+      const R2 c = m > 0 ? val(-m) : czero<R2>();
+      R4 o;
+      o.x = a.x;
+      o.y = a.y;
+      o.z = c.x;
+      o.w = c.y;
+      out[((size_t)b * L + m) * p.nrows + t] = o;
+    }
+  } else {
+    R2* out = reinterpret_cast<R2*>(p.out);
+    for (int m = threadIdx.x; m < L; m += blockDim.x) {
+      out[(((size_t)b * p.nhalf + 0) * L + m) * p.nrows + t] = val(m);
+      if (p.nhalf > 1)
+        out[(((size_t)b * p.nhalf + 1) * L + m) * p.nrows + t] = m > 0 ? val(-m) : czero<R2>();
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Forward rows: f rows/rings -> weighted spectra G [B][half][m][nrows]
+// (dual: Real4 {+m, -m}; single: half 0 holds +m, half 1 holds -m), or, for
+// the MW/MWSS resampling chain, the transposed raw spectra Fc [B][ncolm][nrows].
+// ---------------------------------------------------------------------------
+template <typename Real>
+__global__ void fwd_rows_kernel(RowsParams<Real> p) {
+  using R2 = typename C2<Real>::t;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R2* s = reinterpret_cast<R2*>(smem_raw);
+  const int t = blockIdx.x;
+  const int b = blockIdx.y;
+  const FFTDesc d = p.desc[p.ring_desc ? p.ring_desc[t] : 0];
+  const int n = d.n;
+  const int L = p.L;
+  const size_t off = (size_t)b * p.out_batch_stride + p.ring_off[t];
+  auto load = [&](int k) -> R2 {
+    R2 x;
+    if (p.real_in) {
+      x.x = reinterpret_cast<const Real*>(p.in)[off + k];
+      x.y = 0;
+    } else {
+      x = reinterpret_cast<const R2*>(p.in)[off + k];
+    }
+    return x;
+  };
+  dft_run<Real>(s, d, p.tb, false, load);
+  const double w = p.weights ? p.weights[t] : 1.0;
+  const double phi0 = p.phi0 ? p.phi0[t] : 0.0;
+  if (p.mode == FWD_TO_COLS) {
+    // Fc[b][m + mshift][t] = scale * X_m for m in [mlo, L-1]
+    R2* out = reinterpret_cast<R2*>(p.out);
+    const int mlo = -(L - 1) - p.mo;
+    const int ncm = L - mlo;
+    for (int mi = threadIdx.x; mi < ncm; mi += blockDim.x) {
+      const int m = mlo + mi;
+      R2 x = dft_get<Real>(s, d, p.tb, false, pmod(m, n));
+      out[((size_t)b * ncm + mi) * p.nrows + t] = cscale(x, (Real)p.scale);
+    }
+    return;
+  }
+  // weighted, phase-shifted spectrum for m in [-(L-1), L-1] (periodic in n)
+  auto val = [&](int m) -> R2 {
+    R2 x = dft_get<Real>(s, d, p.tb, false, pmod(m, n));
+    double re = (double)x.x * w, im = (double)x.y * w;
+    if (p.phi0) {
+      double sn, cs;
+      sincos(-(double)m * phi0, &sn, &cs);
+      const double r2 = re * cs - im * sn;
+      im = re * sn + im * cs;
+      re = r2;
+    }
+    R2 o;
+    o.x = (Real)re;
+    o.y = (Real)im;
+    return o;
+  };
+  store_spectra<Real>(p, b, t, val);
+}
+
+
+// ---------------------------------------------------------------------------
+// MW / MWSS forward resampling, per phi-frequency column m (one CTA per column):
+//   theta periodic extension with parity (-1)^(m+s) (resampling.py:6-61, 64-101),
+//   DFT over the extended circle, MW half-sample shift exp(-i p pi/(2L-1))
+//   (resampling.py:284-326), zero-padding to 4L and inverse DFT
+//   (resampling.py:104-160), evaluation on the 2L+1 MWSS(2L) rings, times the
+//   quadrature weights. The phi resampling 2L-1 -> 2L (resampling.py:248-281)
+//   reduces to the overall factor 2L/(2L-1) in the phi-Fourier domain.
+// ---------------------------------------------------------------------------
+template <typename Real>
+__global__ void mw_cols_kernel(ColsParams<Real> p) {
+  using R2 = typename C2<Real>::t;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const FFTDesc d1 = *p.d1;
+  const FFTDesc d2 = *p.d2;
+  R2* s1 = reinterpret_cast<R2*>(smem_raw);
+  R2* s2 = s1 + d1.M;
+  const int L = p.L;
+  const int mlo = p.mw ? -(L - 1) : -L;
+  const int ncm = L - mlo;
+  const int mi = blockIdx.x;
+  const int b = blockIdx.y;
+  const int m = mlo + mi;
+  if (m < -(L - 1)) return;  // MWSS m = -L never reaches the recursion
+  const R2* c = reinterpret_cast<const R2*>(p.in) + ((size_t)b * ncm + mi) * p.nin;
+  const int par = ((m + p.spin) % 2 + 2) % 2;
+  const Real sgn = par ? Real(-1) : Real(1);
+  const int n1 = d1.n;
+  auto load1 = [&](int t) -> R2 {
+    if (p.mw) {
+      if (t < L) return c[t];
+      return cscale(c[2 * L - 2 - t], sgn);  // t = L + jj -> c[L-2-jj]
+    }
+    if (t <= L) return c[t];
+    return cscale(c[2 * L - t], sgn);  // t = L+1+jj -> c[L-1-jj]
+  };
+  dft_run<Real>(s1, d1, p.tb, false, load1);
+  const int plo = p.mw ? -(L - 1) : -L;
+  const int phi = L - 1;
+  const int n2 = d2.n;  // 4L
+  const double inv_n1 = 1.0 / (double)n1;
+  auto load2 = [&](int k) -> R2 {
+    // k = p mod 4L for p in [plo, phi]
+    int pp = k <= phi ? k : k - n2;
+    if (pp < plo || pp > phi) return czero<R2>();
+    R2 g = dft_get<Real>(s1, d1, p.tb, false, pmod(pp, n1));
+    double re = (double)g.x * inv_n1, im = (double)g.y * inv_n1;
+    if (p.mw) {
+      double sn, cs;
+      sincospi(-(double)pp / (double)(2 * L - 1), &sn, &cs);
+      const double r2 = re * cs - im * sn;
+      im = re * sn + im * cs;
+      re = r2;
+    }
+    R2 o;
+    o.x = (Real)re;
+    o.y = (Real)im;
+    return o;
+  };
+  dft_run<Real>(s2, d2, p.tb, true, load2);
+  const int nout = 2 * L + 1;
+  const int am = m < 0 ? -m : m;
+  for (int t = threadIdx.x; t < nout; t += blockDim.x) {
+    R2 u = dft_get<Real>(s2, d2, p.tb, true, t);
+    const double f = p.scale * p.weights[t];
+    u.x = (Real)((double)u.x * f);
+    u.y = (Real)((double)u.y * f);
+    R2* out = reinterpret_cast<R2*>(p.out);
+    if (p.dual) {
+      // Real4 {+m, -m} viewed as pairs of Real2
+      out[(((size_t)b * L + am) * nout + t) * 2 + (m < 0 ? 1 : 0)] = u;
+    } else if (m >= 0) {
+      out[(((size_t)b * p.nhalf + 0) * L + am) * nout + t] = u;
+    } else if (p.nhalf > 1) {
+      out[(((size_t)b * p.nhalf + 1) * L + am) * nout + t] = u;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+static int fft_threads(int M) {
+  int t = M / 2;
+  if (t > 512) t = 512;
+  if (t < 32) t = 32;
+  return t;
+}
+
+template <typename Real>
+cudaError_t launch_inv_rows(const RowsParams<Real>& p, int nrings, int batch, int maxM,
+                            cudaStream_t s) {
+  using R2 = typename C2<Real>::t;
+  const size_t smem = (size_t)maxM * sizeof(R2);
+  cudaError_t e = cudaFuncSetAttribute(inv_rows_kernel<Real>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  inv_rows_kernel<Real><<<dim3(nrings, batch), fft_threads(maxM), smem, s>>>(p);
+  return cudaGetLastError();
+}
+
+template <typename Real>
+cudaError_t launch_fwd_rows(const RowsParams<Real>& p, int nrings, int batch, int maxM,
+                            cudaStream_t s) {
+  using R2 = typename C2<Real>::t;
+  const size_t smem = (size_t)maxM * sizeof(R2);
+  cudaError_t e = cudaFuncSetAttribute(fwd_rows_kernel<Real>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  fwd_rows_kernel<Real><<<dim3(nrings, batch), fft_threads(maxM), smem, s>>>(p);
+  return cudaGetLastError();
+}
+
+template <typename Real>
+cudaError_t launch_mw_cols(const ColsParams<Real>& p, int ncm, int batch, int M1, int M2,
+                           cudaStream_t s) {
+  using R2 = typename C2<Real>::t;
+  const size_t smem = (size_t)(M1 + M2) * sizeof(R2);
+  cudaError_t e = cudaFuncSetAttribute(mw_cols_kernel<Real>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  mw_cols_kernel<Real><<<dim3(ncm, batch), fft_threads(M1 > M2 ? M1 : M2), smem, s>>>(p);
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_inv_rows<float>(const RowsParams<float>&, int, int, int, cudaStream_t);
+template cudaError_t launch_inv_rows<double>(const RowsParams<double>&, int, int, int, cudaStream_t);
+template cudaError_t launch_fwd_rows<float>(const RowsParams<float>&, int, int, int, cudaStream_t);
+template cudaError_t launch_fwd_rows<double>(const RowsParams<double>&, int, int, int, cudaStream_t);
+template cudaError_t launch_mw_cols<float>(const ColsParams<float>&, int, int, int, int, cudaStream_t);
+template cudaError_t launch_mw_cols<double>(const ColsParams<double>&, int, int, int, int, cudaStream_t);
+
+}  // namespace s2b

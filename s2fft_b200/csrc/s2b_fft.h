@@ -1,0 +1,82 @@
+// Ring-FFT descriptors and the parameter blocks of the element-wise kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <type_traits>
+
+namespace s2b {
+
+// One transform length. Tables live in pooled device arrays (FFTTables).
+struct FFTDesc {
+  int n;          // transform length
+  int M;          // power-of-two working length (n itself, or >= 2n-1 for Bluestein)
+  int logM;
+  int bluestein;  // 0: n == M (radix-2 only)
+  long tw_off;    // offset of exp(-2 pi i k / M), k < M/2
+  long chirp_off; // Bluestein: exp(-i pi k^2 / n), k < n
+  long bf_off;    // Bluestein: FFT_M(conj chirp, wrapped) / M, bit-reversed order
+};
+
+template <typename Real>
+struct FFTTables {
+  using R2 = std::conditional_t<sizeof(Real) == 4, float2, double2>;
+  const R2* tw;
+  const R2* chirp;
+  const R2* bfilt;
+};
+
+enum RowsMode { FWD_TO_SPECTRA = 0, FWD_TO_COLS = 1 };
+
+template <typename Real>
+struct RowsParams {
+  int L;
+  int nrows;            // rows (rings) of the spectrum arrays
+  int ncol;             // inverse: columns of ftm
+  int mo;               // column offset (1 for mwss / healpix)
+  int reality;          // inverse: fill m < 0 by conjugate symmetry
+  int real_out;         // inverse: write the real part only
+  int real_in;          // forward: real input map
+  int dual, nhalf;      // forward spectra layout
+  int mode;             // RowsMode
+  double scale;
+  const FFTDesc* desc;  // transform descriptors
+  const int* ring_desc; // per ring index into desc (nullptr: desc[0] for all)
+  const long* ring_off; // element offset of ring t inside one map
+  long out_batch_stride;// elements per map of the pixel-space array (f)
+  const double* weights;// forward: quadrature weight per ring (nullptr: 1)
+  const double* phi0;   // HEALPix ring phase (nullptr: none)
+  FFTTables<Real> tb;
+  const void* in;
+  void* out;
+};
+
+// MW / MWSS forward resampling chain, one CTA per (m column, map).
+template <typename Real>
+struct ColsParams {
+  int L, spin, mw;      // mw = 1: input has L MW rings, else L+1 MWSS rings
+  int nin;              // rings of the input columns
+  int dual, nhalf;
+  double scale;         // overall factor of the chain
+  const FFTDesc* d1;    // theta DFT over the periodic extension (2L-1 or 2L)
+  const FFTDesc* d2;    // inverse DFT of length 4L
+  const double* weights;// 2L+1 MWSS(2L) transform weights
+  FFTTables<Real> tb;
+  const void* in;       // Fc [B][ncm][nin]
+  void* out;            // G  [B][half][m][2L+1]
+};
+
+}  // namespace s2b
+
+namespace s2b {
+template <typename Real>
+cudaError_t launch_inv_rows(const RowsParams<Real>& p, int nrings, int batch, int maxM,
+                            cudaStream_t s);
+template <typename Real>
+cudaError_t launch_fwd_rows(const RowsParams<Real>& p, int nrings, int batch, int maxM,
+                            cudaStream_t s);
+template <typename Real>
+cudaError_t launch_mw_cols(const ColsParams<Real>& p, int ncm, int batch, int M1, int M2,
+                           cudaStream_t s);
+}  // namespace s2b

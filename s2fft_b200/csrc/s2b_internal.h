@@ -1,0 +1,72 @@
+// Internal declarations shared by the host plan code and the CUDA kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace s2b {
+
+// Renormalisation constants of the scaled recursion state.
+// A state stores a mantissa v and an integer exponent e; its true value is
+// v * 2^(kScale * e). e < 0 means "below significance": the state is advanced
+// but contributes nothing to the projection. Every kRenorm steps a state with
+// |v| > 2^kThresh is rescaled by 2^-kScale (e += 1).
+template <typename Real>
+struct Scaling;
+template <>
+struct Scaling<float> {
+  static constexpr double kThresh = 48.0;  // log2 of the rescale trigger
+  static constexpr double kScale = 112.0;  // log2 of one exponent unit
+  static constexpr double kSignif = -60.0; // log2 of the significance floor
+  static constexpr float kTrig = 281474976710656.0f;          // 2^48
+  static constexpr float kDown = 1.9259299443872359e-34f;    // 2^-112
+};
+template <>
+struct Scaling<double> {
+  static constexpr double kThresh = 400.0;
+  static constexpr double kScale = 800.0;
+  static constexpr double kSignif = -200.0;
+  static constexpr double kTrig = 0x1p400;
+  static constexpr double kDown = 0x1p-800;
+};
+
+// One recursed ring (pole rings are handled separately, in closed form).
+struct RingInfo {
+  double B;    // 2 cot(theta)
+  double A;    // 2 / sin(theta)
+  double lc;   // log2 cos(theta/2)
+  double ls;   // log2 sin(theta/2)
+};
+
+// Latitudinal (Wigner-d recursion + projection) launch parameters.
+struct LatParams {
+  int L, L0, spin;
+  int nrings;       // recursed rings
+  int nclass;       // C: l classes (CTAs along l); l = j + C*(ql + QA*k)
+  int nhalf;        // recursion halves handled by this launch (1 or 2)
+  int batch;
+  const RingInfo* rings;
+  const int* ring_row;   // row of ring r in the ftm array (inverse out / forward in)
+  const void* seeds;     // [nhalf][L][nrings] {mantissa, exponent}
+  const void* H;         // [L (m)][L (l)] monic recursion coefficient
+  // inverse: in = F  [batch][nhalf][L (m)][L (l)] Real2 (Real4 when dual)
+  //          out = ftm [batch][nrows][ncol] Real2 (accumulated with atomics)
+  // forward: in = G  [batch][nhalf][L (m)][nrows] Real2 (Real4 when dual)
+  //          out = acc [batch][nhalf][L (m)][L (l)] Real2 (accumulated with atomics)
+  const void* in;
+  void* out;
+  int nrows;        // rows of the ftm array
+  int ncol;         // inverse: columns of ftm
+  int mo;           // inverse: column offset (1 for mwss / healpix)
+  int reality;      // inverse: only m >= 0 is produced
+};
+
+// launchers (latitudinal.cu)
+cudaError_t launch_latitudinal(bool fp64, bool forward, bool dual, const LatParams& p,
+                               cudaStream_t s);
+cudaError_t launch_seeds(bool fp64, int L, int L0, int spin, int nhalf, const RingInfo* rings,
+                         int nrings, const double* lbin, void* seeds, cudaStream_t s);
+
+}  // namespace s2b

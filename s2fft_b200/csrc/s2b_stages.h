@@ -1,0 +1,29 @@
+// Parameters and launchers of the element-wise stages (stages.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace s2b {
+
+struct StageParams {
+  int L, L0, spin, batch;
+  int nclass, Q;        // l classes of the latitudinal tiling, l = j + C q
+  int nhalf, dual;
+  int nrows, ncol, mo;  // ftm / G row count, ftm columns, column offset
+  int pole_south, pole_north;  // rows of the closed-form pole rings (-1: none)
+  const double* g;      // [m][l] monic scale g_{l,m}
+  const void* flm;      // inverse input  [b][L][2L-1]
+  void* F;              // inverse recursion table
+  void* ftm;            // inverse ring spectra
+  const void* G;        // forward weighted spectra
+  const void* acc;      // forward projected sums
+  void* flm_out;        // forward output
+};
+
+cudaError_t launch_prologue(bool fp64, const StageParams& p, cudaStream_t s);
+cudaError_t launch_poles(bool fp64, const StageParams& p, cudaStream_t s);
+cudaError_t launch_epilogue(bool fp64, const StageParams& p, cudaStream_t s);
+cudaError_t launch_axpy(bool fp64, long n, double a, const void* x, void* y, cudaStream_t s);
+cudaError_t launch_sub(bool fp64, long n, const void* x, const void* y, void* z, cudaStream_t s);
+
+}  // namespace s2b

@@ -1,0 +1,287 @@
+// Element-wise stages around the latitudinal kernel:
+//  * inverse prologue: flm -> recursion-ready coefficient table F
+//    (harmonic normalisation sqrt((2l+1)/4pi), (-1)^s, the monic scale g_{l,m}
+//    and the m < 0 symmetry sign; s2fft/transforms/spherical.py:165-168, 192);
+//  * inverse pole rows in closed form (spherical.py:175-184);
+//  * forward epilogue: projected sums -> flm (g_{l,m}, pole terms, normalisation,
+//    reality mirror, spin/L_lower mask, (-1)^s; spherical.py:566-588).
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <type_traits>
+
+#include "s2b_stages.h"
+
+namespace s2b {
+
+template <typename Real>
+using R2_t = std::conditional_t<sizeof(Real) == 4, float2, double2>;
+template <typename Real>
+using R4_t = std::conditional_t<sizeof(Real) == 4, float4, double4>;
+
+__device__ __forceinline__ double lnorm(int l) { return sqrt((2.0 * l + 1.0) / (4.0 * 3.141592653589793)); }
+
+// F [b][half][j][m][q] (Real2, or Real4 when dual) from flm [b][l][L-1+m].
+template <typename Real>
+__global__ void prologue_kernel(StageParams p) {
+  using R2 = R2_t<Real>;
+  using R4 = R4_t<Real>;
+  const int L = p.L, C = p.nclass, Q = p.Q;
+  const long per_b = (long)p.nhalf * C * L * Q;
+  const long total = per_b * p.batch;
+  const R2* flm = reinterpret_cast<const R2*>(p.flm);
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long)gridDim.x * blockDim.x) {
+    long r = idx;
+    const int q = (int)(r % Q);
+    r /= Q;
+    const int m = (int)(r % L);
+    r /= L;
+    const int j = (int)(r % C);
+    r /= C;
+    const int half = (int)(r % p.nhalf);
+    const int b = (int)(r / p.nhalf);
+    const int l = j + C * q;
+    const int as = p.spin < 0 ? -p.spin : p.spin;
+    const bool ok = l < L && l >= m && l >= p.L0 && l >= as;
+    double g = 0.0;
+    if (ok) g = p.g[(size_t)m * L + l] * lnorm(l);
+    const R2* row = flm + ((size_t)b * L + (ok ? l : 0)) * (2 * L - 1);
+    const double sgn_s = (p.spin & 1) ? -1.0 : 1.0;
+    const double sgn_m = (m & 1) ? -1.0 : 1.0;
+    if (p.dual) {
+      R4 o;
+      R2 a = row[L - 1 + m], c = row[L - 1 - m];
+      const double gp = ok ? g : 0.0;
+      const double gn = (ok && m > 0) ? g * sgn_m : 0.0;
+      o.x = (Real)(gp * a.x);
+      o.y = (Real)(gp * a.y);
+      o.z = (Real)(gn * c.x);
+      o.w = (Real)(gn * c.y);
+      reinterpret_cast<R4*>(p.F)[idx] = o;
+    } else {
+      R2 o;
+      if (half == 0) {
+        const R2 a = row[L - 1 + m];
+        const double f = ok ? g * sgn_s : 0.0;
+        o.x = (Real)(f * a.x);
+        o.y = (Real)(f * a.y);
+      } else {
+        const R2 a = row[L - 1 - m];
+        const double f = (ok && m > 0) ? g * sgn_m : 0.0;
+        o.x = (Real)(f * a.x);
+        o.y = (Real)(f * a.y);
+      }
+      reinterpret_cast<R2*>(p.F)[idx] = o;
+    }
+  }
+}
+
+// Pole rows of the inverse: ftm[pole][L-1+ms+mo] = (-1)^s sum_l sign_l N_l flm[l][L-1+ms],
+// south (theta = pi): ms = s, sign_l = (-1)^(l-s); north (theta = 0): ms = -s, sign 1.
+template <typename Real>
+__global__ void poles_kernel(StageParams p) {
+  using R2 = R2_t<Real>;
+  const int L = p.L;
+  const int b = blockIdx.y;
+  const int which = blockIdx.x;  // 0 south, 1 north
+  const int row = which == 0 ? p.pole_south : p.pole_north;
+  if (row < 0) return;
+  const int ms = which == 0 ? p.spin : -p.spin;
+  const R2* flm = reinterpret_cast<const R2*>(p.flm) + (size_t)b * L * (2 * L - 1);
+  double sx = 0.0, sy = 0.0;
+  for (int l = p.L0 + threadIdx.x; l < L; l += blockDim.x) {
+    double f = lnorm(l);
+    if (which == 0 && (((l - p.spin) % 2 + 2) % 2)) f = -f;
+    const R2 a = flm[(size_t)l * (2 * L - 1) + L - 1 + ms];
+    sx += f * a.x;
+    sy += f * a.y;
+  }
+  __shared__ double red[2][256];
+  red[0][threadIdx.x] = sx;
+  red[1][threadIdx.x] = sy;
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st) {
+      red[0][threadIdx.x] += red[0][threadIdx.x + st];
+      red[1][threadIdx.x] += red[1][threadIdx.x + st];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double sg = (p.spin & 1) ? -1.0 : 1.0;
+    R2 o;
+    o.x = (Real)(sg * red[0][0]);
+    o.y = (Real)(sg * red[1][0]);
+    R2* ftm = reinterpret_cast<R2*>(p.ftm) + ((size_t)b * p.nrows + row) * p.ncol;
+    ftm[L - 1 + ms + p.mo] = o;
+  }
+}
+
+// Weighted ring spectrum at (row, m) from the forward spectra array G.
+template <typename Real>
+__device__ __forceinline__ R2_t<Real> spectrum_at(const StageParams& p, int b, int row, int m) {
+  using R2 = R2_t<Real>;
+  const int L = p.L;
+  const int am = m < 0 ? -m : m;
+  const R2* G = reinterpret_cast<const R2*>(p.G);
+  if (p.dual) return G[(((size_t)b * L + am) * p.nrows + row) * 2 + (m < 0 ? 1 : 0)];
+  if (m >= 0) return G[(((size_t)b * p.nhalf + 0) * L + am) * p.nrows + row];
+  if (p.nhalf > 1) return G[(((size_t)b * p.nhalf + 1) * L + am) * p.nrows + row];
+  R2 z;
+  z.x = 0;
+  z.y = 0;
+  return z;
+}
+
+// flm [b][l][L-1+m] from the projected sums acc [b][half][j][m][q].
+template <typename Real>
+__global__ void epilogue_kernel(StageParams p) {
+  using R2 = R2_t<Real>;
+  const int L = p.L, C = p.nclass, Q = p.Q;
+  const int W = 2 * L - 1;
+  const long total = (long)p.batch * L * W;
+  const int as = p.spin < 0 ? -p.spin : p.spin;
+  const int lmin = as > p.L0 ? as : p.L0;
+  const double sgn_s = (p.spin & 1) ? -1.0 : 1.0;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long)gridDim.x * blockDim.x) {
+    const int c = (int)(idx % W);
+    const int l = (int)((idx / W) % L);
+    const int b = (int)(idx / ((long)W * L));
+    const int m = c - (L - 1);
+    const int am = m < 0 ? -m : m;
+    double re = 0.0, im = 0.0;
+    if (l >= lmin && am <= l) {
+      const int j = l % C, q = l / C;
+      const double g = p.g[(size_t)am * L + l];
+      double ar = 0.0, ai = 0.0;
+      bool conj_mirror = false;
+      if (p.dual) {
+        const R2* A = reinterpret_cast<const R2*>(p.acc);
+        const R2 a = A[((((size_t)b * C + j) * L + am) * Q + q) * 2 + (m < 0 ? 1 : 0)];
+        ar = a.x;
+        ai = a.y;
+      } else if (m >= 0 || p.nhalf > 1) {
+        const int half = m >= 0 ? 0 : 1;
+        const R2* A = reinterpret_cast<const R2*>(p.acc);
+        const R2 a = A[((((size_t)b * p.nhalf + half) * C + j) * L + am) * Q + q];
+        ar = a.x;
+        ai = a.y;
+      } else {
+        // reality: flm[l, -m] = (-1)^m conj(flm[l, m])
+        const R2* A = reinterpret_cast<const R2*>(p.acc);
+        const R2 a = A[(((size_t)b * C + j) * L + am) * Q + q];
+        ar = a.x;
+        ai = a.y;
+        conj_mirror = true;
+      }
+      // d-projection with the m < 0 symmetry sign (-1)^(m+s) (spin folded below)
+      double f = g;
+      if (m < 0 && !conj_mirror) f *= ((am + p.spin) % 2 + 2) % 2 ? -1.0 : 1.0;
+      re = f * ar;
+      im = f * ai;
+      // closed-form pole rings (MWSS(2L) grid of the mw / mwss forward)
+      if (p.pole_south >= 0 && !conj_mirror) {
+        if (m == p.spin) {
+          const R2 s = spectrum_at<Real>(p, b, p.pole_south, m);
+          const double sg = ((l - p.spin) % 2 + 2) % 2 ? -1.0 : 1.0;
+          re += sg * s.x;
+          im += sg * s.y;
+        }
+        if (m == -p.spin) {
+          const R2 s = spectrum_at<Real>(p, b, p.pole_north, m);
+          re += s.x;
+          im += s.y;
+        }
+      }
+      const double nl = lnorm(l) * sgn_s;
+      re *= nl;
+      im *= nl;
+      if (conj_mirror) {
+        // value above is flm[l, |m|]; mirror (-1)^m conj(.)
+        const double sm = (am & 1) ? -1.0 : 1.0;
+        im = -im;
+        re *= sm;
+        im *= sm;
+      }
+    }
+    R2 o;
+    o.x = (Real)re;
+    o.y = (Real)im;
+    reinterpret_cast<R2*>(p.flm_out)[idx] = o;
+  }
+}
+
+// y += a * x over n complex elements (iterative refinement update)
+template <typename Real>
+__global__ void axpy_kernel(long n, Real a, const R2_t<Real>* x, R2_t<Real>* y) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x) {
+    R2_t<Real> v = y[i];
+    v.x += a * x[i].x;
+    v.y += a * x[i].y;
+    y[i] = v;
+  }
+}
+
+// z = x - y over n real elements
+template <typename Real>
+__global__ void sub_kernel(long n, const Real* x, const Real* y, Real* z) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x)
+    z[i] = x[i] - y[i];
+}
+
+static int grid_for(long n) {
+  long b = (n + 255) / 256;
+  if (b > 65535) b = 65535;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+cudaError_t launch_prologue(bool fp64, const StageParams& p, cudaStream_t s) {
+  const long total = (long)p.batch * p.nhalf * p.nclass * p.L * p.Q;
+  if (fp64)
+    prologue_kernel<double><<<grid_for(total), 256, 0, s>>>(p);
+  else
+    prologue_kernel<float><<<grid_for(total), 256, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_poles(bool fp64, const StageParams& p, cudaStream_t s) {
+  if (p.pole_south < 0 && p.pole_north < 0) return cudaSuccess;
+  if (fp64)
+    poles_kernel<double><<<dim3(2, p.batch), 256, 0, s>>>(p);
+  else
+    poles_kernel<float><<<dim3(2, p.batch), 256, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_epilogue(bool fp64, const StageParams& p, cudaStream_t s) {
+  const long total = (long)p.batch * p.L * (2 * p.L - 1);
+  if (fp64)
+    epilogue_kernel<double><<<grid_for(total), 256, 0, s>>>(p);
+  else
+    epilogue_kernel<float><<<grid_for(total), 256, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_axpy(bool fp64, long n, double a, const void* x, void* y, cudaStream_t s) {
+  if (fp64)
+    axpy_kernel<double><<<grid_for(n), 256, 0, s>>>(n, a, (const double2*)x, (double2*)y);
+  else
+    axpy_kernel<float><<<grid_for(n), 256, 0, s>>>(n, (float)a, (const float2*)x, (float2*)y);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sub(bool fp64, long n, const void* x, const void* y, void* z, cudaStream_t s) {
+  if (fp64)
+    sub_kernel<double><<<grid_for(n), 256, 0, s>>>(n, (const double*)x, (const double*)y,
+                                                    (double*)z);
+  else
+    sub_kernel<float><<<grid_for(n), 256, 0, s>>>(n, (const float*)x, (const float*)y, (float*)z);
+  return cudaGetLastError();
+}
+
+}  // namespace s2b
