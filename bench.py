@@ -1,0 +1,446 @@
+#!/usr/bin/env python
+"""Benchmark of the spin spherical-harmonic transform on B200.
+
+Workload (the headline configuration): MW sampling, L = 1024, spin 0, complex
+signal; one step = one inverse transform followed by one forward transform of
+a seeded band-limited map (flm with Re, Im ~ N(0,1) for every |m| <= l), in the
+mixed precision path (float32 recursion/projection, double seeds, exponent
+bookkeeping and weights). The same step on the float64 path is timed too.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs as N independent replicas (one process per GPU, torchrun), the
+transform does not shard across GPUs; value = total transforms of all ranks
+divided by the slowest rank's time. Rank 0 prints one JSON line.
+"""
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "L=1024 SHT fwd+inv/s & batched maps/s, mixed vs FP64 GPU path at <=1e-5 err"
+UNIT = "fwd+inv/s"
+FLOPS_PER_TRIPLE = 9  # recursion (5) + complex-by-real projection (4) per (theta, l, m)
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--L", type=int, default=1024)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=25.0,
+                    help="seconds of host work for the CPU baseline sample")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="small case for ncu: 2 steps, no baseline, no clocks")
+    return ap.parse_args()
+
+
+def triples(L, nrings, spin=0, reality=False):
+    """(theta, l, m) terms with max(|m|, |s|) <= l < L, summed over rings."""
+    ms = np.arange(0 if reality else -(L - 1), L)
+    return nrings * int(np.sum(L - np.maximum(np.abs(ms), abs(spin))))
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled with nvidia-smi during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            return json.load(fh), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def simt_peak_tflops(torch, fp64):
+    """FP32 / FP64 FMA rate measured with the library's FMA-chain probe."""
+    from s2fft_b200 import _lib
+
+    lib = _lib.lib()
+    lib.s2b_fma_probe.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                  ctypes.c_void_p]
+    lib.s2b_fma_probe.restype = ctypes.c_int
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    blocks, iters = sms * 8, 4000 if not fp64 else 2000
+    out = torch.empty(blocks * 256, dtype=torch.float64 if fp64 else torch.float32,
+                      device="cuda")
+    st = _lib.stream_handle(out.device)
+    best = 0.0
+    for rep in range(4):
+        e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
+        e0.record()
+        _lib.check(lib.s2b_fma_probe(int(fp64), blocks, iters, out.data_ptr(), st))
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        flops = blocks * 256.0 * iters * 16 * 8 * 2
+        if rep > 0:
+            best = max(best, flops / (ms * 1e-3) / 1e12)
+    return best
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def run_ours(args, rank, world, torch, dist):
+    import s2fft_b200
+    from s2fft_b200 import _lib
+
+    import oracle  # only to draw the seeded coefficients (same generator as upstream)
+
+    L = args.L
+    dev = torch.device("cuda", torch.cuda.current_device())
+    rng = np.random.default_rng(8966433580120847635 + rank)
+    flm_np = oracle.signal.generate_flm_full_complex(rng, L)
+    nrings_inv, nrings_fwd = L, 2 * L - 1
+    T_inv, T_fwd = triples(L, nrings_inv), triples(L, nrings_fwd)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)  # > 126 MB L2
+
+    def plans(precision):
+        kw = dict(L=L, spin=0, nside=0, sampling=0, reality=0, L_lower=0,
+                  precision=_lib.PRECISION[precision], batch=1, N=0)
+        return _lib.get_plan(dev, iter=0, **kw), _lib.get_plan(dev, iter=0, **kw)
+
+    def timed(precision, steps, warmup, lat_events):
+        cdt = torch.complex64 if precision == "f32" else torch.complex128
+        x = torch.from_numpy(flm_np).to(dev, cdt)
+        f = s2fft_b200.inverse(x, L, precision=precision)
+        y = s2fft_b200.forward(f, L, precision=precision)
+        torch.cuda.synchronize()
+        plan = plans(precision)[0]
+        lib = _lib.lib()
+        lib.s2b_plan_set_events.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                            ctypes.c_void_p]
+        lib.s2b_plan_set_events.restype = ctypes.c_int
+        for _ in range(warmup):
+            flush.zero_()
+            f = s2fft_b200.inverse(x, L, precision=precision)
+            y = s2fft_b200.forward(f, L, precision=precision)
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        step_ev, lat_ev = [], []
+        for _ in range(steps):
+            flush.zero_()  # L2 flush between timed steps, outside the events
+            e = [torch.cuda.Event(True) for _ in range(2)]
+            le = [torch.cuda.Event(True) for _ in range(4)] if lat_events else None
+            if le:
+                for ev in le:
+                    ev.record()  # materialise the handles before passing them to the library
+                _lib.check(lib.s2b_plan_set_events(plan.ptr, 0, le[0].cuda_event,
+                                                   le[1].cuda_event))
+                _lib.check(lib.s2b_plan_set_events(plan.ptr, 1, le[2].cuda_event,
+                                                   le[3].cuda_event))
+            e[0].record()
+            f = s2fft_b200.inverse(x, L, precision=precision)
+            y = s2fft_b200.forward(f, L, precision=precision)
+            e[1].record()
+            step_ev.append(e)
+            lat_ev.append(le)
+        torch.cuda.synchronize()
+        _lib.check(lib.s2b_plan_set_events(plan.ptr, 0, None, None))
+        _lib.check(lib.s2b_plan_set_events(plan.ptr, 1, None, None))
+        total_ms = sum(a.elapsed_time(b) for a, b in step_ev)
+        lat = None
+        if lat_events:
+            li = [le[0].elapsed_time(le[1]) for le in lat_ev]
+            lf = [le[2].elapsed_time(le[3]) for le in lat_ev]
+            lat = (float(np.mean(li)), float(np.mean(lf)))
+        err = float((y - x).abs().max().item() / x.abs().max().item())
+        return total_ms, lat, err, y
+
+    steps, warmup = args.steps, args.warmup
+    clocks = ClockSampler(dev.index if dev.index is not None else 0)
+    clocks.start()
+    ms32, lat32, err32, y32 = timed("f32", steps, warmup, True)
+    clk = clocks.stop()
+    ms64, lat64, err64, y64 = timed("f64", max(3, steps // 4), 2, True)
+    # mixed-path coefficient error against the float64 path (itself <= 1e-10 of the oracle)
+    err_mixed = float((y32.to(torch.complex128) - y64).abs().max().item()
+                      / y64.abs().max().item())
+
+    # end to end through the public API with pinned host buffers
+    host_in = torch.from_numpy(flm_np.astype(np.complex64)).pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+    for _ in range(2):
+        xd = host_in.to(dev, non_blocking=True)
+        yd = s2fft_b200.forward(s2fft_b200.inverse(xd, L, precision="f32"), L, precision="f32")
+        host_out.copy_(yd, non_blocking=True)
+    torch.cuda.synchronize()
+    e_steps = max(3, steps // 2)
+    evs = []
+    for _ in range(e_steps):
+        flush.zero_()
+        e = [torch.cuda.Event(True) for _ in range(2)]
+        e[0].record()
+        xd = host_in.to(dev, non_blocking=True)
+        yd = s2fft_b200.forward(s2fft_b200.inverse(xd, L, precision="f32"), L, precision="f32")
+        host_out.copy_(yd, non_blocking=True)
+        e[1].record()
+        evs.append(e)
+    torch.cuda.synchronize()
+    e2e_ms = sum(a.elapsed_time(b) for a, b in evs)
+
+    t = torch.tensor([ms32, ms64, e2e_ms], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms32, ms64, e2e_ms = t.tolist()
+    value = world * steps / (ms32 * 1e-3)
+    value64 = world * max(3, steps // 4) / (ms64 * 1e-3)
+    e2e = world * e_steps / (e2e_ms * 1e-3)
+    return dict(value=value, value64=value64, e2e=e2e, ms32=ms32 / steps, lat32=lat32,
+                lat64=lat64, err32=err32, err64=err64, err_mixed=err_mixed, clocks=clk,
+                T_inv=T_inv, T_fwd=T_fwd, h2d=host_in.numel() * 8, d2h=host_out.numel() * 8)
+
+
+# ---------------------------------------------------------------------------
+# CPU reference: the float64 numpy restatement of the upstream algorithm
+# (oracle/), on a bounded sample: the first k m-steps of every latitudinal
+# recursion on all rings (rings split over host processes), plus the full
+# resampling / FFT stages. The reference's dense formulation does the same
+# work at every m-step, so the full transform time is extrapolated linearly.
+# ---------------------------------------------------------------------------
+def _cpu_lat_worker(job):
+    import numpy as _np
+
+    import oracle as _o
+
+    kind, L, beta, ksteps, seed = job
+    rng = _np.random.default_rng(seed)
+    t0 = time.perf_counter()
+    pre = _o.recursion.precompute(L, 0, beta, 0)
+    t1 = time.perf_counter()
+    if kind == "inv":
+        flm = _o.signal.generate_flm_full_complex(rng, L)
+        _o.recursion.inverse_latitudinal_step(flm, beta, L, 0, "mw", False, pre, 0, ksteps)
+    else:
+        ftm = rng.standard_normal((len(beta), 2 * L)) + 1j * rng.standard_normal((len(beta), 2 * L))
+        _o.recursion.forward_latitudinal_step(ftm, beta, L, 0, "mwss", False, pre, 0, ksteps)
+    t2 = time.perf_counter()
+    return t1 - t0, t2 - t1
+
+
+def cpu_sample(L, budget_s, procs=None):
+    """fwd+inv/s of the CPU reference path, from a bounded sample."""
+    import multiprocessing as mp
+
+    import oracle
+
+    procs = procs or max(1, min(os.cpu_count() or 1, 64))
+    th_inv = oracle.samples.thetas(L, "mw")[:-1]  # south pole handled in closed form
+    th_fwd = oracle.samples.thetas(2 * L, "mwss")[1:-1]
+    # cost of one m-step (both halves, all rings) ~ c * nrings * L
+    rng = np.random.default_rng(0)
+    t0 = time.perf_counter()
+    ftm_fake = np.zeros((len(th_fwd), 2 * L), complex)
+    f_mw = rng.standard_normal((L, 2 * L - 1)) + 0j
+    up = oracle.resampling.upsample_by_two_mwss(oracle.resampling.mw_to_mwss(f_mw, L, 0), L, 0)
+    np.fft.fftshift(np.fft.fft(up, axis=1), axes=1)
+    np.fft.ifft(np.fft.ifftshift(ftm_fake[:L], axes=1), axis=1)
+    t_fft = time.perf_counter() - t0
+    steps_full = L - 1  # m-steps per half in the upstream loop (2 .. L-2+i)
+    # size the sample: measured rate of one m-step on one process for a small chunk
+    probe = _cpu_lat_worker(("inv", L, th_inv[:8], 2, 1))
+    per_step_per_ring = probe[1] / (2 * 2 * 8)
+    est_full_steps = per_step_per_ring * 2 * (len(th_inv) + len(th_fwd)) / procs
+    k = int(max(2, min(steps_full, budget_s / max(est_full_steps, 1e-9) * 0.5)))
+    ctx = mp.get_context("spawn")
+    jobs = []
+    for kind, th in (("inv", th_inv), ("fwd", th_fwd)):
+        for chunk in np.array_split(th, procs):
+            if len(chunk):
+                jobs.append((kind, L, chunk, k, 7))
+    t0 = time.perf_counter()
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_cpu_lat_worker, jobs)
+    wall = time.perf_counter() - t0
+    pre_total = sum(r[0] for r in res)
+    lat_total = sum(r[1] for r in res)
+    # wall-clock of the sampled latitudinal work, scaled to the full m range
+    lat_wall = wall * lat_total / max(pre_total + lat_total, 1e-12)
+    t_full = t_fft + lat_wall * (steps_full + 1) / (k + 1)
+    return dict(value=1.0 / t_full, cores=procs, k=k, t_full=t_full,
+                precompute_s=wall * pre_total / max(pre_total + lat_total, 1e-12),
+                sample=(f"oracle (numpy restatement of the upstream Price-McEwen path), "
+                        f"{k} of {steps_full} m-steps per half on all {len(th_inv)}+"
+                        f"{len(th_fwd)} rings split over {procs} processes + full "
+                        f"resampling/FFT stages, extrapolated linearly in m-steps; "
+                        f"precompute excluded"))
+
+
+# ---------------------------------------------------------------------------
+# main
+# ---------------------------------------------------------------------------
+def main():
+    args = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    config = {"workload": "spin SHT inverse+forward, MW sampling, L=1024, spin 0, complex, "
+                          "float32 recursion/projection with float64 seeds/exponents/weights",
+              "L": args.L, "sampling": "mw", "spin": 0, "maps_per_step": 1,
+              "l2": "flushed between timed steps (256 MB write)",
+              "parallelism": f"replicas x{world}"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        samples = []
+        budget = max(5.0, 150.0 / max(1, args.steps + args.warmup))
+        for i in range(args.warmup + args.steps):
+            r = cpu_sample(args.L, budget)
+            if i >= args.warmup:
+                samples.append(r)
+        v = float(np.mean([r["value"] for r in samples]))
+        r0 = samples[-1]
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT,
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded N(0,1) flm)",
+                "config": config,
+                "cpu_baseline": {"value": v, "unit": UNIT, "cores": r0["cores"], "kind": "port",
+                                 "sample": r0["sample"]},
+                "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as tdist
+
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    else:
+        torch.cuda.set_device(0)
+    if args.profile_case:
+        args.steps, args.warmup = 2, 1
+    r = run_ours(args, rank, world, torch, dist)
+    if dist is not None:
+        dist.barrier()
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    peaks, kind = measured_peaks()
+    fp32_peak = simt_peak_tflops(torch, False)
+    fp64_peak = simt_peak_tflops(torch, True)
+    lat_inv_ms, lat_fwd_ms = r["lat32"]
+    ach_fwd = FLOPS_PER_TRIPLE * r["T_fwd"] / (lat_fwd_ms * 1e-3) / 1e12
+    ach_inv = FLOPS_PER_TRIPLE * r["T_inv"] / (lat_inv_ms * 1e-3) / 1e12
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "latitudinal_traffic.txt")
+    if os.path.exists(tpath):
+        for ln in open(tpath):
+            if ln.startswith(f"L={args.L} forward_f32 bytes_per_launch="):
+                traffic = float(ln.split("=")[-1])
+    line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms32"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded N(0,1) flm, all |m| <= l)", "config": config,
+            "max_rel_err_vs_fp64": r["err_mixed"], "roundtrip_rel_err_f32": r["err32"],
+            "roundtrip_rel_err_f64": r["err64"],
+            "fp64_path": {"value": r["value64"], "unit": UNIT,
+                          "speedup_mixed_over_fp64": r["value"] / r["value64"]},
+            "roofline": {"bound": "fp32", "kernel": "latitudinal forward (recursion+projection)",
+                         "achieved": ach_fwd, "peak": fp32_peak, "unit": "TFLOP/s",
+                         "frac": ach_fwd / fp32_peak, "traffic": traffic,
+                         "peak_source": "measured FMA-chain probe (MEASURED_PEAKS.json has no "
+                                        "FP32-SIMT figure)",
+                         "flops_per_launch": FLOPS_PER_TRIPLE * r["T_fwd"],
+                         "launch_ms": lat_fwd_ms,
+                         "inverse": {"achieved": ach_inv, "frac": ach_inv / fp32_peak,
+                                     "launch_ms": lat_inv_ms}},
+            "fp64_roofline": {"achieved": FLOPS_PER_TRIPLE * r["T_fwd"] / (r["lat64"][1] * 1e-3)
+                              / 1e12, "peak": fp64_peak, "unit": "TFLOP/s"},
+            "hbm_peak_gbs": peaks.get("hbm_gbs"), "peaks_source": kind,
+            "clocks": r["clocks"],
+            "e2e": {"value": r["e2e"], "unit": UNIT, "h2d_bytes_per_step": r["h2d"],
+                    "d2h_bytes_per_step": r["d2h"]},
+            "gpu_launches": 8 * args.steps}
+    if not args.no_cpu_baseline and not args.profile_case:
+        c = cpu_sample(args.L, args.cpu_budget)
+        line["cpu_baseline"] = {"value": c["value"], "unit": UNIT, "cores": c["cores"],
+                                "kind": "port", "sample": c["sample"],
+                                "precompute_s": c["precompute_s"]}
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -99,6 +99,34 @@ int s2b_inverse(s2b_plan* plan, const void* flm, void* f, void* workspace,
 int s2b_forward(s2b_plan* plan, const void* f, void* flm, void* workspace,
                 size_t workspace_bytes, void* stream);
 
+/* Wigner transforms on SO(3) (plan with desc.N > 0; desc.spin is ignored):
+ *   flmn [B][2N-1][L][2L-1] <-> f [B][2N-1][ntheta][nphi] (or [B][2N-1][12 nside^2]);
+ *   f real when desc.reality (then flmn obeys the SO(3) conjugate symmetry).
+ * Replace s2fft/transforms/wigner.py:13-107 (inverse) and 346-439 (forward). */
+int s2b_wigner_inverse(s2b_plan* plan, const void* flmn, void* f, void* workspace,
+                       size_t workspace_bytes, void* stream);
+int s2b_wigner_forward(s2b_plan* plan, const void* f, void* flmn, void* workspace,
+                       size_t workspace_bytes, void* stream);
+
+/* Device status of the plan (synchronous): *status != 0 after a bounded
+ * wait inside a kernel ran out (the kernel then skipped its work); returns
+ * S2B_ERR_TIMEOUT in that case. No upstream counterpart (upstream exits the
+ * process on CUDA errors, lib/include/hresult.h:26-33). */
+int s2b_plan_status(s2b_plan* plan, int* status);
+
+/* Instrumentation: record the caller's cudaEvent_t objects (passed as void*)
+ * immediately before and after the latitudinal (recursion + projection) kernel
+ * of every later inverse (forward = 0) or forward (forward = 1) call on this
+ * plan. NULL events switch recording off. No upstream counterpart; used by the
+ * benchmark to time the dominant kernel on the launching stream. */
+int s2b_plan_set_events(s2b_plan* plan, int forward, void* ev_begin, void* ev_end);
+
+/* Peak-rate probe: a fused multiply-add chain kernel (float when fp64 == 0,
+ * double otherwise) over `blocks` CTAs of 256 threads, `iters` iterations of 8
+ * independent FMA chains per thread, writing one value per thread to `out`
+ * (blocks*256 elements). No upstream counterpart. */
+int s2b_fma_probe(int fp64, int blocks, int iters, void* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -44,6 +44,11 @@ _SIGS = {
     "s2b_workspace_size": [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)],
     "s2b_inverse": [ctypes.c_void_p] * 4 + [ctypes.c_size_t, ctypes.c_void_p],
     "s2b_forward": [ctypes.c_void_p] * 4 + [ctypes.c_size_t, ctypes.c_void_p],
+    "s2b_wigner_inverse": [ctypes.c_void_p] * 4 + [ctypes.c_size_t, ctypes.c_void_p],
+    "s2b_wigner_forward": [ctypes.c_void_p] * 4 + [ctypes.c_size_t, ctypes.c_void_p],
+    "s2b_plan_status": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)],
+    "s2b_plan_set_events": [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
+    "s2b_fma_probe": [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
 }
 
 
@@ -93,6 +98,12 @@ class Plan:
             self._ws[key] = torch.empty(max(int(n.value), 256), dtype=torch.uint8,
                                         device=self.device)
         return self._ws[key]
+
+    def status(self):
+        """Device status word (synchronous); raises if a bounded device wait gave up."""
+        st = ctypes.c_int()
+        check(lib().s2b_plan_status(self.ptr, ctypes.byref(st)))
+        return st.value
 
     def __del__(self):
         try:

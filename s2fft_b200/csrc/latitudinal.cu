@@ -159,16 +159,74 @@ __device__ __forceinline__ void acc_fma(A& a, Real x, const A& f) {
     a.w = fma(x, f.w, a.w);
   }
 }
+// ---------------------------------------------------------------------------
+// 1-D bulk asynchronous copies global -> shared (no multicast), completed on
+// an mbarrier. Waits are bounded; a wait that runs out sets the status word.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* ptr) {
+  return (uint32_t)__cvta_generic_to_shared(ptr);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* mb, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mb)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* mb, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mb)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes,
+                                         uint64_t* mb) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(mb))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t* mb, unsigned parity) {
+  const uint32_t a = smem_u32(mb);
+  for (int it = 0; it < (1 << 22); ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+// Shared-memory carve-up of the latitudinal kernel (bytes, all 16-aligned):
+//   [reduction buffer][stage 0: H rows | data rows][stage 1: ...][2 mbarriers]
+template <typename Real, typename Acc, bool FWD, int T, int K, int QA, int QT, int R>
+struct LatSmem {
+  static constexpr int NRT = QT * T;
+  static constexpr size_t red_elems = FWD ? (size_t)R * K * QT * QA : (size_t)R * T * QT * (QA + 1);
+  __host__ __device__ static size_t red_bytes() { return (red_elems * sizeof(Acc) + 15) & ~(size_t)15; }
+  __host__ __device__ static size_t h_bytes(int Qp) { return (size_t)R * Qp * sizeof(Real); }
+  __host__ __device__ static size_t d_bytes(int Qp) {
+    return (size_t)R * (FWD ? NRT : Qp) * sizeof(Acc);
+  }
+  __host__ __device__ static size_t stage_bytes(int Qp) { return h_bytes(Qp) + d_bytes(Qp); }
+  __host__ __device__ static size_t total(int Qp) { return red_bytes() + 2 * stage_bytes(Qp) + 16; }
+};
 
 template <typename Real, bool FWD, bool DUAL, int T, int K, int QA, int QT, int R>
 __global__ void __launch_bounds__(QA* QT)
     lat_kernel(const LatParams p) {
   using Cfg = LatCfg<Real, FWD, DUAL, T, K, QA, QT, R>;
   using Acc = typename Cfg::Acc;
+  using SM = LatSmem<Real, Acc, FWD, T, K, QA, QT, R>;
+  constexpr int NRT = SM::NRT;
   static_assert(R % 2 == 0, "R must be even");
   static_assert(QA % 2 == 0, "QA must be even");
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int Qp = p.Qp;
   Acc* buf = reinterpret_cast<Acc*>(smem_raw);
+  unsigned char* stage_base = smem_raw + SM::red_bytes();
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(stage_base + 2 * SM::stage_bytes(Qp));
 
   const int tid = threadIdx.x;
   const int ql = tid % QA;
@@ -179,26 +237,21 @@ __global__ void __launch_bounds__(QA* QT)
   const int half = (int)(blockIdx.z % p.nhalf);
   const int b = (int)(blockIdx.z / p.nhalf);
   const int n = half == 0 ? -p.spin : p.spin;
-  const int Q = (L + C - 1) / C;  // l's per class (padded)
-  const int rbase = blockIdx.x * (QT * T) + qt * T;
+  const int r0 = blockIdx.x * NRT;
+  const int rbase = r0 + qt * T;
   if (j >= L) return;
   const int lmax = j + C * ((L - 1 - j) / C);
+  const int TR = tab_rows(L);
 
   // ring constants: lambda = n*A - m*B (double FMA per (ring, m))
   double nA[T], Bc[T];
-  int rrow[T];
+  bool rvalid[T];
 #pragma unroll
   for (int i = 0; i < T; ++i) {
     const int r = rbase + i;
-    if (r < p.nrings) {
-      nA[i] = (double)n * p.rings[r].A;
-      Bc[i] = p.rings[r].B;
-      rrow[i] = p.ring_row[r];
-    } else {
-      nA[i] = 0.0;
-      Bc[i] = 0.0;
-      rrow[i] = -1;
-    }
+    rvalid[i] = r < p.nrings;
+    nA[i] = rvalid[i] ? (double)n * p.rings[r].A : 0.0;
+    Bc[i] = rvalid[i] ? p.rings[r].B : 0.0;
   }
 
   Real v[K][T], w[K][T], sc[K][T];
@@ -213,28 +266,69 @@ __global__ void __launch_bounds__(QA* QT)
       ex[k][i] = 0;
     }
 
-  const Real* __restrict__ Hc = reinterpret_cast<const Real*>(p.H) + (size_t)j * L * Q;
+  const Real* __restrict__ Hc = reinterpret_cast<const Real*>(p.H) + (size_t)j * TR * Qp;
   const SeedT<Real>* __restrict__ seeds =
-      reinterpret_cast<const SeedT<Real>*>(p.seeds) + ((size_t)half * C + j) * Q * p.nrings;
-  // inverse input F [b][half][j][m][q]; forward input G [b][half][m][ring]
-  const Acc* __restrict__ Fin;
+      reinterpret_cast<const SeedT<Real>*>(p.seeds) + ((size_t)half * C + j) * Qp * p.nrings;
+  // inverse input F [b][half][j][row][Qp]; forward input G [b][half][row][Gs]
+  const Acc* __restrict__ Din;
   if constexpr (!FWD)
-    Fin = reinterpret_cast<const Acc*>(p.in) + (((size_t)b * p.nhalf + half) * C + j) * L * Q;
+    Din = reinterpret_cast<const Acc*>(p.in) + (((size_t)b * p.nhalf + half) * C + j) * TR * Qp;
   else
-    Fin = reinterpret_cast<const Acc*>(p.in) + ((size_t)b * p.nhalf + half) * L * p.nrows;
+    Din = reinterpret_cast<const Acc*>(p.in) + ((size_t)b * p.nhalf + half) * TR * p.Gs;
+  int ncopy = NRT;
+  if constexpr (FWD) {
+    ncopy = p.Gs - r0;
+    if (ncopy > NRT) ncopy = NRT;
+  }
 
   // even-aligned chunk boundaries: chunk k covers m in [clo(k), clo(k+1)-1]
   auto clo = [&](int k) -> int {
     const int x = j + C * QA * k;
     return k == 0 ? 0 : (x & ~1);
   };
-  int mtop = lmax | 1;  // odd, >= lmax
-  // highest chunk that contains any valid l of this class
+  const int mtop = lmax | 1;  // odd, >= lmax
   int ktop = (lmax - j) / (C * QA);
   if (ktop > K - 1) ktop = K - 1;
+  const int ngroups = (mtop + R) / R;
 
-  int gstep = 0;  // steps since the last reduction
-  int mgrp = mtop;  // m of the first step of the current reduction group
+  // group g covers steps m = mtop - g R ... mtop - g R - R + 1 (table rows ascending)
+  auto issue = [&](int g) {
+    unsigned char* st = stage_base + (size_t)(g & 1) * SM::stage_bytes(Qp);
+    const int row0 = mtop - g * R - R + 1 + kPadLo;
+    unsigned bytes = (unsigned)SM::h_bytes(Qp);
+    if constexpr (!FWD)
+      bytes += (unsigned)SM::d_bytes(Qp);
+    else
+      bytes += (unsigned)(R * ncopy * sizeof(Acc));
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(&mbar[g & 1], bytes);
+    bulk_g2s(st, Hc + (size_t)row0 * Qp, (unsigned)SM::h_bytes(Qp), &mbar[g & 1]);
+    unsigned char* dst = st + SM::h_bytes(Qp);
+    if constexpr (!FWD) {
+      bulk_g2s(dst, Din + (size_t)row0 * Qp, (unsigned)SM::d_bytes(Qp), &mbar[g & 1]);
+    } else {
+#pragma unroll
+      for (int s = 0; s < R; ++s)
+        bulk_g2s(dst + (size_t)s * NRT * sizeof(Acc), Din + (size_t)(row0 + s) * p.Gs + r0,
+                 (unsigned)(ncopy * sizeof(Acc)), &mbar[g & 1]);
+    }
+  };
+  if (tid == 0) {
+    mbar_init(&mbar[0], 1);
+    mbar_init(&mbar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0) {
+    issue(0);
+    if (ngroups > 1) issue(1);
+  }
+
+  int gstep = 0;    // steps done in the current group
+  int grp = 0;      // current group
+  int mgrp = mtop;  // m of the first step of the current group
+  const Real* Hs = nullptr;
+  const Acc* Ds = nullptr;
 
   // reduction + renormalisation, every R steps (and at the end)
   auto flush = [&](int nsteps) {
@@ -249,15 +343,14 @@ __global__ void __launch_bounds__(QA* QT)
         const int qq = rem % QT;
         if (s >= nsteps) continue;
         const int m = mgrp - s;
-        const int r = blockIdx.x * (QT * T) + qq * T + i;
+        const int r = r0 + qq * T + i;
         if (m < 0 || m >= L || r >= p.nrings) continue;
         const Acc* row = buf + ((s * T + i) * QT + qq) * (QA + 1);
         Acc a = zero_acc<Acc>();
 #pragma unroll
         for (int x = 0; x < QA; ++x) acc_add(a, row[x]);
         using R2 = typename Cfg::R2;
-        R2* ftm = reinterpret_cast<R2*>(p.out) +
-                  ((size_t)b * p.nrows + p.ring_row[r]) * p.ncol;
+        R2* ftm = reinterpret_cast<R2*>(p.out) + ((size_t)b * p.nrows + p.ring_row[r]) * p.ncol;
         const int mo = p.mo;
         if constexpr (DUAL) {
           R2 ap, an;
@@ -278,7 +371,7 @@ __global__ void __launch_bounds__(QA* QT)
         }
       }
     } else {
-      // buf [s][k][qt][ql] -> sum over qt; out acc [b][half][j][m][q]
+      // buf [s][k][qt][ql] -> sum over qt; out acc [b][half][j][m][Qp]
       const int items = R * K * QA;
       for (int o = tid; o < items; o += Cfg::NT) {
         const int s = o / (K * QA);
@@ -294,7 +387,7 @@ __global__ void __launch_bounds__(QA* QT)
 #pragma unroll
         for (int y = 0; y < QT; ++y) acc_add(a, buf[((s * K + k) * QT + y) * QA + x]);
         Acc* out = reinterpret_cast<Acc*>(p.out) +
-                   ((((size_t)b * p.nhalf + half) * C + j) * L + m) * Q + q;
+                   ((((size_t)b * p.nhalf + half) * C + j) * L + m) * Qp + q;
         red_add(out, a);
       }
     }
@@ -321,42 +414,38 @@ __global__ void __launch_bounds__(QA* QT)
     }
   };
 
-  // one recursion step at m; CUR selects which register array holds dt_m
+  // one recursion step at m; CUR holds dt_m, PRV holds dt_{m+1} and receives dt_{m-1}
 #define S2B_STEP(CUR, PRV, KC)                                                         \
   {                                                                                    \
-    const bool mvalid = (m < L);                                                       \
+    const int srow = R - 1 - gstep;                                                    \
+    const Real* Hrow = Hs + srow * Qp;                                                 \
     Real lam[T];                                                                       \
     _Pragma("unroll") for (int i = 0; i < T; ++i) lam[i] = (Real)fma(-md, Bc[i], nA[i]); \
     Acc accT[T];                                                                       \
-    _Pragma("unroll") for (int i = 0; i < T; ++i) accT[i] = zero_acc<Acc>();           \
     Acc gin[T];                                                                        \
     if constexpr (FWD) {                                                               \
-      _Pragma("unroll") for (int i = 0; i < T; ++i) {                                  \
-        gin[i] = (mvalid && rrow[i] >= 0) ? Fin[(size_t)m * p.nrows + rrow[i]]         \
-                                          : zero_acc<Acc>();                           \
-      }                                                                                \
+      const Acc* Grow = Ds + srow * NRT + qt * T;                                      \
+      _Pragma("unroll") for (int i = 0; i < T; ++i) gin[i] =                           \
+          rvalid[i] ? Grow[i] : zero_acc<Acc>();                                       \
+    } else {                                                                           \
+      _Pragma("unroll") for (int i = 0; i < T; ++i) accT[i] = zero_acc<Acc>();         \
     }                                                                                  \
     _Pragma("unroll") for (int k = KC; k < K; ++k) {                                   \
       const int q = ql + QA * k;                                                       \
       const int l = j + C * q;                                                         \
-      if (k == KC) {                                                                   \
-        if (l == m && l < L) {                                                         \
-          const SeedT<Real>* sp = seeds + (size_t)q * p.nrings;                        \
-          _Pragma("unroll") for (int i = 0; i < T; ++i) {                              \
-            const int r = rbase + i;                                                   \
-            SeedT<Real> sd = (r < p.nrings) ? sp[r] : SeedT<Real>{Real(0), 0};         \
-            CUR[k][i] = sd.v;                                                          \
-            PRV[k][i] = Real(0);                                                       \
-            ex[k][i] = sd.e;                                                           \
-            sc[k][i] = sd.e >= 0 ? Real(1) : Real(0);                                  \
-          }                                                                            \
+      if (k == KC && l == m) {                                                         \
+        _Pragma("unroll") for (int i = 0; i < T; ++i) {                                \
+          CUR[k][i] = sdv[i];                                                          \
+          PRV[k][i] = Real(0);                                                         \
+          ex[k][i] = sde[i];                                                           \
+          sc[k][i] = sde[i] >= 0 ? Real(1) : Real(0);                                  \
         }                                                                              \
       }                                                                                \
       Real h = Real(0);                                                                \
       Acc fk = zero_acc<Acc>();                                                        \
-      if (mvalid && l < L) {                                                           \
-        h = Hc[(size_t)m * Q + q];                                                     \
-        if constexpr (!FWD) fk = Fin[(size_t)m * Q + q];                               \
+      if (l < L) {                                                                     \
+        h = Hrow[q];                                                                   \
+        if constexpr (!FWD) fk = Ds[srow * Qp + q];                                    \
       }                                                                                \
       Acc accK = zero_acc<Acc>();                                                      \
       _Pragma("unroll") for (int i = 0; i < T; ++i) {                                  \
@@ -383,18 +472,43 @@ __global__ void __launch_bounds__(QA* QT)
 
   int m = mtop;
   double md = (double)mtop;
+  Real sdv[T];
+  int sde[T];
 #pragma unroll
   for (int kc = K - 1; kc >= 0; --kc) {
     if (kc > ktop) continue;
+    // seeds of slot kc for this thread (activated when m reaches l)
+    {
+      const int q = ql + QA * kc;
+      const int l = j + C * q;
+#pragma unroll
+      for (int i = 0; i < T; ++i) {
+        SeedT<Real> sd{Real(0), 0};
+        if (l < L && rvalid[i]) sd = seeds[(size_t)q * p.nrings + rbase + i];
+        sdv[i] = sd.v;
+        sde[i] = sd.e;
+      }
+    }
     const int lo = clo(kc);
-    // m runs from the current value down to lo, two steps at a time (even length)
     while (m >= lo) {
+      if (gstep == 0) {
+        const bool ok = mbar_wait(&mbar[grp & 1], (grp >> 1) & 1);
+        if (!__syncthreads_and(ok)) {
+          if (tid == 0) atomicExch(p.status, 1);
+          return;
+        }
+        unsigned char* st = stage_base + (size_t)(grp & 1) * SM::stage_bytes(Qp);
+        Hs = reinterpret_cast<const Real*>(st);
+        Ds = reinterpret_cast<const Acc*>(st + SM::h_bytes(Qp));
+      }
       S2B_STEP(v, w, kc)
       S2B_STEP(w, v, kc)
       if (gstep == R) {
         flush(R);
         gstep = 0;
         mgrp = m;
+        ++grp;
+        if (tid == 0 && grp + 1 < ngroups) issue(grp + 1);
       }
     }
   }
@@ -405,61 +519,73 @@ __global__ void __launch_bounds__(QA* QT)
 // ---------------------------------------------------------------------------
 // launch configuration
 // ---------------------------------------------------------------------------
+constexpr int kQA = 16, kQT = 8, kK = 4, kR = 4;
+
+int lat_nclass(bool fp64, int L) {
+  (void)fp64;
+  const int per = kQA * kK;
+  return (L + per - 1) / per;
+}
+
+int lat_qp(bool fp64, int L) {
+  const int C = lat_nclass(fp64, L);
+  return round4((L + C - 1) / C);
+}
+
 template <typename Real, bool FWD, bool DUAL, int T, int K, int QA, int QT, int R>
 static cudaError_t launch_cfg(const LatParams& p0, cudaStream_t s) {
   using Cfg = LatCfg<Real, FWD, DUAL, T, K, QA, QT, R>;
+  using SM = LatSmem<Real, typename Cfg::Acc, FWD, T, K, QA, QT, R>;
   LatParams p = p0;
-  p.nclass = (p.L + QA * K - 1) / (QA * K);
+  p.nclass = lat_nclass(sizeof(Real) == 8, p.L);
+  p.Qp = lat_qp(sizeof(Real) == 8, p.L);
+  const size_t smem = SM::total(p.Qp);
   auto kern = lat_kernel<Real, FWD, DUAL, T, K, QA, QT, R>;
-  cudaError_t err =
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::kSmemBytes);
+  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (err != cudaSuccess) return err;
   dim3 grid((p.nrings + QT * T - 1) / (QT * T), p.nclass, p.nhalf * p.batch);
-  kern<<<grid, Cfg::NT, Cfg::kSmemBytes, s>>>(p);
+  kern<<<grid, Cfg::NT, smem, s>>>(p);
   return cudaGetLastError();
-}
-
-int lat_nclass(bool fp64, int L) {
-  const int per = fp64 ? 16 * 4 : 16 * 4;
-  return (L + per - 1) / per;
 }
 
 cudaError_t launch_latitudinal(bool fp64, bool forward, bool dual, const LatParams& p,
                                cudaStream_t s) {
   if (!fp64) {
     if (!forward)
-      return dual ? launch_cfg<float, false, true, 4, 4, 16, 8, 4>(p, s)
-                  : launch_cfg<float, false, false, 4, 4, 16, 8, 4>(p, s);
-    return dual ? launch_cfg<float, true, true, 4, 4, 16, 8, 4>(p, s)
-                : launch_cfg<float, true, false, 4, 4, 16, 8, 4>(p, s);
+      return dual ? launch_cfg<float, false, true, 4, kK, kQA, kQT, kR>(p, s)
+                  : launch_cfg<float, false, false, 4, kK, kQA, kQT, kR>(p, s);
+    return dual ? launch_cfg<float, true, true, 4, kK, kQA, kQT, kR>(p, s)
+                : launch_cfg<float, true, false, 4, kK, kQA, kQT, kR>(p, s);
   }
   if (!forward)
-    return dual ? launch_cfg<double, false, true, 2, 4, 16, 8, 4>(p, s)
-                : launch_cfg<double, false, false, 2, 4, 16, 8, 4>(p, s);
-  return dual ? launch_cfg<double, true, true, 2, 4, 16, 8, 4>(p, s)
-              : launch_cfg<double, true, false, 2, 4, 16, 8, 4>(p, s);
+    return dual ? launch_cfg<double, false, true, 2, kK, kQA, kQT, kR>(p, s)
+                : launch_cfg<double, false, false, 2, kK, kQA, kQT, kR>(p, s);
+  return dual ? launch_cfg<double, true, true, 2, kK, kQA, kQT, kR>(p, s)
+              : launch_cfg<double, true, false, 2, kK, kQA, kQT, kR>(p, s);
 }
 
 cudaError_t launch_seeds(bool fp64, int L, int L0, int spin, int nhalf, const RingInfo* rings,
                          int nrings, const double* lbin, void* seeds, cudaStream_t s) {
   const int C = lat_nclass(fp64, L);
-  const int Q = (L + C - 1) / C;
-  const long total = (long)nhalf * C * Q * nrings;
+  const int Qp = lat_qp(fp64, L);
+  const long total = (long)nhalf * C * Qp * nrings;
   const int threads = 256;
-  const int blocks = (int)((total + threads - 1) / threads > 4096 ? 4096 : (total + threads - 1) / threads);
+  long blocks = (total + threads - 1) / threads;
+  if (blocks > 4096) blocks = 4096;
+  if (blocks < 1) blocks = 1;
   if (fp64)
-    seed_kernel<double><<<blocks, threads, 0, s>>>(L, L0, spin, nhalf, C, Q, rings, nrings, lbin,
-                                                   reinterpret_cast<SeedT<double>*>(seeds));
+    seed_kernel<double><<<(int)blocks, threads, 0, s>>>(L, L0, spin, nhalf, C, Qp, rings, nrings,
+                                                        lbin, reinterpret_cast<SeedT<double>*>(seeds));
   else
-    seed_kernel<float><<<blocks, threads, 0, s>>>(L, L0, spin, nhalf, C, Q, rings, nrings, lbin,
-                                                  reinterpret_cast<SeedT<float>*>(seeds));
+    seed_kernel<float><<<(int)blocks, threads, 0, s>>>(L, L0, spin, nhalf, C, Qp, rings, nrings,
+                                                       lbin, reinterpret_cast<SeedT<float>*>(seeds));
   return cudaGetLastError();
 }
 
 size_t seed_bytes(bool fp64, int L, int nhalf, int nrings) {
   const int C = lat_nclass(fp64, L);
-  const int Q = (L + C - 1) / C;
-  return (size_t)nhalf * C * Q * nrings * (fp64 ? sizeof(SeedT<double>) : sizeof(SeedT<float>));
+  const int Qp = lat_qp(fp64, L);
+  return (size_t)nhalf * C * Qp * nrings * (fp64 ? sizeof(SeedT<double>) : sizeof(SeedT<float>));
 }
 
 }  // namespace s2b

@@ -25,11 +25,7 @@
 #include "s2b_fft.h"
 #include "s2b_internal.h"
 #include "s2b_stages.h"
-
-namespace s2b {
-size_t seed_bytes(bool fp64, int L, int nhalf, int nrings);
-int lat_nclass(bool fp64, int L);
-}  // namespace s2b
+#include "s2b_wigner.h"
 
 using namespace s2b;
 using cd = std::complex<double>;
@@ -321,7 +317,7 @@ struct s2b_plan {
   int nth;      // rings of the sampling
   int nphi;     // equiangular ring length
   long npix;    // pixels per map
-  int nclass, Q;
+  int nclass, Q, TR, Gs;
   int dual;     // spin 0 complex: both m signs from one recursion
   int nhalf;
   // inverse geometry
@@ -340,7 +336,8 @@ struct s2b_plan {
   double* lbin = nullptr;
   double* gtab = nullptr;
   void* htab = nullptr;
-  double* fwd_weights = nullptr;   // per forward row
+  double* fwd_weights = nullptr;   // per MWSS(2L) ring (mw/mwss) or per ring
+  int* status = nullptr;           // device status word (timed-out waits)
   double* hp_phi0 = nullptr;
   long* ring_off = nullptr;        // pixel offsets of the sampling rings
   int* ring_desc = nullptr;        // per ring FFT desc (healpix)
@@ -349,6 +346,12 @@ struct s2b_plan {
   void* chirp = nullptr;
   void* bf = nullptr;
   int row_desc = 0, col_d1 = 0, col_d2 = 0, maxM = 2, M1 = 2, M2 = 2;
+  // Wigner: one spin transform plan per n, gamma-DFT buffers
+  std::vector<s2b_plan*> subs;
+  size_t ws_w_fban = 0, ws_w_tmp = 0, ws_w_sub = 0;
+  // optional events recorded around the latitudinal launch ([0] inverse, [1] forward)
+  cudaEvent_t ev_begin[2] = {nullptr, nullptr};
+  cudaEvent_t ev_end[2] = {nullptr, nullptr};
   // workspace layout (bytes)
   size_t ws_inv_F, ws_inv_ftm, ws_fwd_cols, ws_fwd_G, ws_fwd_acc, ws_iter_f, ws_iter_flm;
 };
@@ -409,7 +412,8 @@ static int build_plan(s2b_plan* p) {
   p->dual = (d.spin == 0 && !d.reality) ? 1 : 0;
   p->nhalf = (d.spin == 0) ? 1 : 2;
   p->nclass = lat_nclass(p->fp64, L);
-  p->Q = (L + p->nclass - 1) / p->nclass;
+  p->Q = lat_qp(p->fp64, L);
+  p->TR = tab_rows(L);
 
   // ---- recursion tables: g[m][l], h[j][m][q], lbin[l]
   std::vector<double> g((size_t)L * L, 0.0), h((size_t)L * L, 0.0);
@@ -426,25 +430,25 @@ static int build_plan(s2b_plan* p) {
   int rc = upload(p, &p->gtab, g);
   if (rc) return rc;
   {
-    const int C = p->nclass, Q = p->Q;
+    const int C = p->nclass, Q = p->Q, TR = p->TR;
     if (p->fp64) {
-      std::vector<double> hc((size_t)C * L * Q, 0.0);
+      std::vector<double> hc((size_t)C * TR * Q, 0.0);
       for (int j = 0; j < C; ++j)
         for (int m = 0; m < L; ++m)
           for (int q = 0; q < Q; ++q) {
             const int l = j + C * q;
-            if (l < L) hc[((size_t)j * L + m) * Q + q] = h[(size_t)m * L + l];
+            if (l < L) hc[((size_t)j * TR + m + kPadLo) * Q + q] = h[(size_t)m * L + l];
           }
       double* dp = nullptr;
       rc = upload(p, &dp, hc);
       p->htab = dp;
     } else {
-      std::vector<float> hc((size_t)C * L * Q, 0.0f);
+      std::vector<float> hc((size_t)C * TR * Q, 0.0f);
       for (int j = 0; j < C; ++j)
         for (int m = 0; m < L; ++m)
           for (int q = 0; q < Q; ++q) {
             const int l = j + C * q;
-            if (l < L) hc[((size_t)j * L + m) * Q + q] = (float)h[(size_t)m * L + l];
+            if (l < L) hc[((size_t)j * TR + m + kPadLo) * Q + q] = (float)h[(size_t)m * L + l];
           }
       float* fp = nullptr;
       rc = upload(p, &fp, hc);
@@ -501,11 +505,11 @@ static int build_plan(s2b_plan* p) {
       p->fwd_mode = d.sampling == S2B_MW ? 1 : 2;
       std::vector<double> th2 = thetas(2 * L, S2B_MWSS, 0);
       p->fwd_nrows = 2 * L + 1;
-      p->fwd_pole_n = 0;
+      p->fwd_pole_n = 2 * L - 1;  // rows 0..2L-2: rings t = 1..2L-1; then the two poles
       p->fwd_pole_s = 2 * L;
       for (int t = 1; t < 2 * L; ++t) {
         ri.push_back(ring_info(th2[t]));
-        rr.push_back(t);
+        rr.push_back(t - 1);
       }
     } else {
       p->fwd_mode = 0;
@@ -518,10 +522,15 @@ static int build_plan(s2b_plan* p) {
       }
     }
     p->fwd_nrings = (int)ri.size();
+    p->Gs = round4(p->fwd_nrows);
     if ((rc = upload(p, &p->fwd_rings, ri))) return rc;
     if ((rc = upload(p, &p->fwd_ring_row, rr))) return rc;
     if ((rc = upload(p, &p->fwd_weights, w))) return rc;
   }
+
+  S2B_CK(cudaMalloc(&p->status, sizeof(int)));
+  p->allocs.push_back(p->status);
+  S2B_CK(cudaMemset(p->status, 0, sizeof(int)));
 
   // ---- seeds (device kernel, double arithmetic)
   {
@@ -584,11 +593,11 @@ static int build_plan(s2b_plan* p) {
   const size_t c2 = 2 * p->rsz;
   const size_t acc = p->dual ? 2 * c2 : c2;
   const size_t B = (size_t)d.batch;
-  p->ws_inv_F = B * p->nhalf * p->nclass * (size_t)L * p->Q * acc;
+  p->ws_inv_F = B * p->nhalf * p->nclass * (size_t)p->TR * p->Q * acc;
   p->ws_inv_ftm = B * (size_t)p->nth * p->inv_ncol * c2;
   const int ncm = p->fwd_mode == 1 ? 2 * L - 1 : 2 * L;
   p->ws_fwd_cols = p->fwd_mode ? B * (size_t)ncm * p->nth * c2 : 0;
-  p->ws_fwd_G = B * p->nhalf * (size_t)L * p->fwd_nrows * acc;
+  p->ws_fwd_G = B * p->nhalf * (size_t)p->TR * p->Gs * acc;
   p->ws_fwd_acc = B * p->nhalf * p->nclass * (size_t)L * p->Q * acc;
   const size_t fel = d.reality ? p->rsz : c2;
   p->ws_iter_f = d.iter > 0 ? B * (size_t)p->npix * fel : 0;
@@ -640,6 +649,8 @@ static int run_inverse(s2b_plan* p, const void* flm, void* f, char* ws, cudaStre
   sp.batch = d.batch;
   sp.nclass = p->nclass;
   sp.Q = p->Q;
+  sp.TR = p->TR;
+  sp.Gs = p->Gs;
   sp.nhalf = p->nhalf;
   sp.dual = p->dual;
   sp.nrows = p->nth;
@@ -671,7 +682,10 @@ static int run_inverse(s2b_plan* p, const void* flm, void* f, char* ws, cudaStre
     lp.ncol = p->inv_ncol;
     lp.mo = p->inv_mo;
     lp.reality = d.reality;
+    lp.status = p->status;
+    if (p->ev_begin[0]) S2B_CK(cudaEventRecord(p->ev_begin[0], s));
     S2B_CK(launch_latitudinal(p->fp64, false, p->dual, lp, s));
+    if (p->ev_end[0]) S2B_CK(cudaEventRecord(p->ev_end[0], s));
   }
   RowsParams<Real> rp{};
   rp.L = L;
@@ -709,6 +723,8 @@ static int run_forward_once(s2b_plan* p, const void* f, void* flm, char* ws, cud
   rp.real_in = d.reality;
   rp.dual = p->dual;
   rp.nhalf = p->nhalf;
+  rp.TR = p->TR;
+  rp.Gs = p->Gs;
   rp.scale = 1.0;
   rp.desc = p->descs + p->row_desc;
   rp.ring_desc = nullptr;
@@ -737,6 +753,8 @@ static int run_forward_once(s2b_plan* p, const void* f, void* flm, char* ws, cud
     cp.nin = p->nth;
     cp.dual = p->dual;
     cp.nhalf = p->nhalf;
+    cp.TR = p->TR;
+    cp.Gs = p->Gs;
     cp.scale = p->fwd_mode == 1 ? (2.0 * L) / (2.0 * L - 1.0) : 1.0;
     cp.d1 = p->descs + p->col_d1;
     cp.d2 = p->descs + p->col_d2;
@@ -761,7 +779,11 @@ static int run_forward_once(s2b_plan* p, const void* f, void* flm, char* ws, cud
   lp.in = G;
   lp.out = acc;
   lp.nrows = p->fwd_nrows;
+  lp.Gs = p->Gs;
+  lp.status = p->status;
+  if (p->ev_begin[1]) S2B_CK(cudaEventRecord(p->ev_begin[1], s));
   S2B_CK(launch_latitudinal(p->fp64, true, p->dual, lp, s));
+  if (p->ev_end[1]) S2B_CK(cudaEventRecord(p->ev_end[1], s));
   StageParams sp{};
   sp.L = L;
   sp.L0 = d.L_lower;
@@ -769,6 +791,8 @@ static int run_forward_once(s2b_plan* p, const void* f, void* flm, char* ws, cud
   sp.batch = d.batch;
   sp.nclass = p->nclass;
   sp.Q = p->Q;
+  sp.TR = p->TR;
+  sp.Gs = p->Gs;
   sp.nhalf = p->nhalf;
   sp.dual = p->dual;
   sp.nrows = p->fwd_nrows;
@@ -805,6 +829,74 @@ static int run_forward(s2b_plan* p, const void* f, void* flm, char* ws, cudaStre
 }
 
 // ----------------------------------------------------------------------------
+// Wigner (SO(3)) transforms: 2N-1 spin transforms + gamma DFT
+// (s2fft/transforms/wigner.py:110-196, 442-533)
+// ----------------------------------------------------------------------------
+static int build_wigner(s2b_plan* p) {
+  const s2b_desc& d = p->d;
+  p->fp64 = d.precision == S2B_F64;
+  p->rsz = p->fp64 ? 8 : 4;
+  p->nth = ntheta(d.L, d.sampling, d.nside);
+  p->nphi = d.sampling == S2B_HEALPIX ? 0 : nphi_equiang(d.L, d.sampling);
+  p->npix = d.sampling == S2B_HEALPIX ? 12L * d.nside * d.nside : (long)p->nth * p->nphi;
+  const int n0 = d.reality ? 0 : -(d.N - 1);
+  for (int n = n0; n < d.N; ++n) {
+    s2b_desc sd = d;
+    sd.spin = -n;
+    sd.reality = 0;
+    sd.N = 0;
+    sd.iter = 0;
+    s2b_plan* sub = nullptr;
+    const int rc = s2b_plan_create(&sd, &sub);
+    if (rc) return rc;
+    p->subs.push_back(sub);
+    p->ws_w_sub = std::max(p->ws_w_sub, std::max(inv_ws(sub), fwd_ws(sub)));
+  }
+  const size_t c2 = 2 * p->rsz;
+  p->ws_w_fban = (size_t)(2 * d.N - 1) * d.batch * p->npix * c2;
+  p->ws_w_tmp = (size_t)d.batch * d.L * (2 * d.L - 1) * c2;
+  return S2B_OK;
+}
+
+static size_t wigner_ws(const s2b_plan* p) {
+  return align256(p->ws_w_fban) + align256(p->ws_w_tmp) + align256(p->ws_w_sub);
+}
+
+static int run_wigner(s2b_plan* p, bool forward, const void* in, void* out, char* ws,
+                      cudaStream_t s) {
+  const s2b_desc& d = p->d;
+  const int n0 = d.reality ? 0 : -(d.N - 1);
+  char* fban = ws;
+  char* tmp = fban + align256(p->ws_w_fban);
+  char* subws = tmp + align256(p->ws_w_tmp);
+  const size_t slice = (size_t)d.batch * p->npix * 2 * p->rsz;
+  int rc;
+  if (!forward) {
+    for (int n = n0; n < d.N; ++n) {
+      s2b_plan* sub = p->subs[n - n0];
+      S2B_CK(launch_gather_n(p->fp64, in, tmp, d.batch, d.N, d.L, n, s));
+      char* dst = fban + (size_t)(d.N - 1 + n) * slice;
+      rc = p->fp64 ? run_inverse<double>(sub, tmp, dst, subws, s)
+                   : run_inverse<float>(sub, tmp, dst, subws, s);
+      if (rc) return rc;
+    }
+    S2B_CK(launch_gamma_inverse(p->fp64, fban, out, d.batch, d.N, p->npix, d.reality, s));
+    return S2B_OK;
+  }
+  S2B_CK(launch_gamma_forward(p->fp64, in, fban, d.batch, d.N, p->npix, d.reality, s));
+  for (int n = n0; n < d.N; ++n) {
+    s2b_plan* sub = p->subs[n - n0];
+    const char* src = fban + (size_t)(d.N - 1 + n) * slice;
+    rc = p->fp64 ? run_forward<double>(sub, src, tmp, subws, s)
+                 : run_forward<float>(sub, src, tmp, subws, s);
+    if (rc) return rc;
+    S2B_CK(launch_scatter_n(p->fp64, tmp, out, d.batch, d.N, d.L, n, d.L_lower, s));
+  }
+  if (d.reality) S2B_CK(launch_wigner_mirror(p->fp64, out, d.batch, d.N, d.L, s));
+  return S2B_OK;
+}
+
+// ----------------------------------------------------------------------------
 // C ABI
 // ----------------------------------------------------------------------------
 extern "C" {
@@ -832,10 +924,13 @@ int s2b_plan_create(const s2b_desc* desc, s2b_plan** out) {
   if (d.batch < 1) return fail(S2B_ERR_INVALID, "batch must be >= 1");
   if (d.iter < 0) return fail(S2B_ERR_INVALID, "iter must be >= 0");
   if (d.L > 8192) return fail(S2B_ERR_INVALID, "L > 8192 not supported");
+  if (d.N < 0 || d.N > d.L) return fail(S2B_ERR_INVALID, "0 <= N <= L required");
+  if (d.N > 0 && d.iter != 0) return fail(S2B_ERR_INVALID, "iter is not used by Wigner plans");
   s2b_plan* p = new s2b_plan();
   p->d = d;
-  const int rc = build_plan(p);
+  const int rc = d.N > 0 ? build_wigner(p) : build_plan(p);
   if (rc) {
+    for (s2b_plan* sp : p->subs) s2b_plan_destroy(sp);
     for (void* a : p->allocs) cudaFree(a);
     delete p;
     return rc;
@@ -846,6 +941,7 @@ int s2b_plan_create(const s2b_desc* desc, s2b_plan** out) {
 
 int s2b_plan_destroy(s2b_plan* p) {
   if (!p) return S2B_OK;
+  for (s2b_plan* sp : p->subs) s2b_plan_destroy(sp);
   for (void* a : p->allocs) cudaFree(a);
   delete p;
   return S2B_OK;
@@ -853,12 +949,12 @@ int s2b_plan_destroy(s2b_plan* p) {
 
 int s2b_workspace_size(const s2b_plan* p, int forward, size_t* bytes) {
   if (!p || !bytes) return fail(S2B_ERR_INVALID, "plan and bytes must be non-NULL");
-  *bytes = forward ? fwd_ws(p) : inv_ws(p);
+  *bytes = p->d.N > 0 ? wigner_ws(p) : (forward ? fwd_ws(p) : inv_ws(p));
   return S2B_OK;
 }
 
 int s2b_inverse(s2b_plan* p, const void* flm, void* f, void* ws, size_t ws_bytes, void* stream) {
-  if (!p) return fail(S2B_ERR_INVALID, "plan is NULL");
+  if (!p || p->d.N > 0) return fail(S2B_ERR_INVALID, "plan is NULL or a Wigner plan");
   int rc;
   if ((rc = check_ptr(flm, "flm")) || (rc = check_ptr(f, "f")) || (rc = check_ptr(ws, "workspace")))
     return rc;
@@ -869,7 +965,7 @@ int s2b_inverse(s2b_plan* p, const void* flm, void* f, void* ws, size_t ws_bytes
 }
 
 int s2b_forward(s2b_plan* p, const void* f, void* flm, void* ws, size_t ws_bytes, void* stream) {
-  if (!p) return fail(S2B_ERR_INVALID, "plan is NULL");
+  if (!p || p->d.N > 0) return fail(S2B_ERR_INVALID, "plan is NULL or a Wigner plan");
   int rc;
   if ((rc = check_ptr(flm, "flm")) || (rc = check_ptr(f, "f")) || (rc = check_ptr(ws, "workspace")))
     return rc;
@@ -877,6 +973,40 @@ int s2b_forward(s2b_plan* p, const void* f, void* flm, void* ws, size_t ws_bytes
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   return p->fp64 ? run_forward<double>(p, f, flm, (char*)ws, s)
                  : run_forward<float>(p, f, flm, (char*)ws, s);
+}
+
+int s2b_wigner_inverse(s2b_plan* p, const void* flmn, void* f, void* ws, size_t ws_bytes,
+                       void* stream) {
+  if (!p || p->d.N < 1) return fail(S2B_ERR_INVALID, "plan is not a Wigner plan (desc.N > 0)");
+  int rc;
+  if ((rc = check_ptr(flmn, "flmn")) || (rc = check_ptr(f, "f")) || (rc = check_ptr(ws, "workspace")))
+    return rc;
+  if (ws_bytes < wigner_ws(p)) return fail(S2B_ERR_WORKSPACE, "workspace too small");
+  return run_wigner(p, false, flmn, f, (char*)ws, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int s2b_wigner_forward(s2b_plan* p, const void* f, void* flmn, void* ws, size_t ws_bytes,
+                       void* stream) {
+  if (!p || p->d.N < 1) return fail(S2B_ERR_INVALID, "plan is not a Wigner plan (desc.N > 0)");
+  int rc;
+  if ((rc = check_ptr(flmn, "flmn")) || (rc = check_ptr(f, "f")) || (rc = check_ptr(ws, "workspace")))
+    return rc;
+  if (ws_bytes < wigner_ws(p)) return fail(S2B_ERR_WORKSPACE, "workspace too small");
+  return run_wigner(p, true, f, flmn, (char*)ws, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int s2b_plan_status(s2b_plan* p, int* status) {
+  if (!p || !status) return fail(S2B_ERR_INVALID, "plan and status must be non-NULL");
+  S2B_CK(cudaMemcpy(status, p->status, sizeof(int), cudaMemcpyDeviceToHost));
+  if (*status) return fail(S2B_ERR_TIMEOUT, "a bounded device wait gave up");
+  return S2B_OK;
+}
+
+int s2b_plan_set_events(s2b_plan* p, int forward, void* ev_begin, void* ev_end) {
+  if (!p || (forward != 0 && forward != 1)) return fail(S2B_ERR_INVALID, "bad plan or direction");
+  p->ev_begin[forward] = reinterpret_cast<cudaEvent_t>(ev_begin);
+  p->ev_end[forward] = reinterpret_cast<cudaEvent_t>(ev_end);
+  return S2B_OK;
 }
 
 }  // extern "C"

@@ -22,6 +22,7 @@
 #include <type_traits>
 
 #include "s2b_fft.h"
+#include "s2b_internal.h"
 
 namespace s2b {
 
@@ -243,27 +244,35 @@ __global__ void inv_rows_kernel(RowsParams<Real> p) {
 
 template <typename Real, typename Val>
 __device__ __forceinline__ void store_spectra(const RowsParams<Real>& p, int b, int t, Val val) {
+  // G [b][half][m + kPadLo][Gs]: rows m < 0 and m = L are zero pads
   using R2 = typename C2<Real>::t;
   const int L = p.L;
   if (p.dual) {
     using R4 = std::conditional_t<sizeof(Real) == 4, float4, double4>;
     R4* out = reinterpret_cast<R4*>(p.out);
-    for (int m = threadIdx.x; m < L; m += blockDim.x) {
-      const R2 a = val(m);
-      const R2 c = m > 0 ? val(-m) : czero<R2>();
+    for (int mr = threadIdx.x; mr < p.TR; mr += blockDim.x) {
+      const int m = mr - kPadLo;
+      R2 a = czero<R2>(), c = czero<R2>();
+      if (m >= 0 && m < L) {
+        a = val(m);
+        if (m > 0) c = val(-m);
+      }
       R4 o;
       o.x = a.x;
       o.y = a.y;
       o.z = c.x;
       o.w = c.y;
-      out[((size_t)b * L + m) * p.nrows + t] = o;
+      out[((size_t)b * p.TR + mr) * p.Gs + t] = o;
     }
   } else {
     R2* out = reinterpret_cast<R2*>(p.out);
-    for (int m = threadIdx.x; m < L; m += blockDim.x) {
-      out[(((size_t)b * p.nhalf + 0) * L + m) * p.nrows + t] = val(m);
+    for (int mr = threadIdx.x; mr < p.TR; mr += blockDim.x) {
+      const int m = mr - kPadLo;
+      const bool ok = m >= 0 && m < L;
+      out[(((size_t)b * p.nhalf + 0) * p.TR + mr) * p.Gs + t] = ok ? val(m) : czero<R2>();
       if (p.nhalf > 1)
-        out[(((size_t)b * p.nhalf + 1) * L + m) * p.nrows + t] = m > 0 ? val(-m) : czero<R2>();
+        out[(((size_t)b * p.nhalf + 1) * p.TR + mr) * p.Gs + t] =
+            (ok && m > 0) ? val(-m) : czero<R2>();
     }
   }
 }
@@ -391,19 +400,45 @@ __global__ void mw_cols_kernel(ColsParams<Real> p) {
   dft_run<Real>(s2, d2, p.tb, true, load2);
   const int nout = 2 * L + 1;
   const int am = m < 0 ? -m : m;
+  R2* out = reinterpret_cast<R2*>(p.out);
   for (int t = threadIdx.x; t < nout; t += blockDim.x) {
     R2 u = dft_get<Real>(s2, d2, p.tb, true, t);
     const double f = p.scale * p.weights[t];
     u.x = (Real)((double)u.x * f);
     u.y = (Real)((double)u.y * f);
-    R2* out = reinterpret_cast<R2*>(p.out);
+    const int row = t == 0 ? 2 * L - 1 : t - 1;  // poles after the recursed rings
+    const size_t mr = (size_t)(am + kPadLo);
     if (p.dual) {
       // Real4 {+m, -m} viewed as pairs of Real2
-      out[(((size_t)b * L + am) * nout + t) * 2 + (m < 0 ? 1 : 0)] = u;
+      out[(((size_t)b * p.TR + mr) * p.Gs + row) * 2 + (m < 0 ? 1 : 0)] = u;
     } else if (m >= 0) {
-      out[(((size_t)b * p.nhalf + 0) * L + am) * nout + t] = u;
+      out[(((size_t)b * p.nhalf + 0) * p.TR + mr) * p.Gs + row] = u;
     } else if (p.nhalf > 1) {
-      out[(((size_t)b * p.nhalf + 1) * L + am) * nout + t] = u;
+      out[(((size_t)b * p.nhalf + 1) * p.TR + mr) * p.Gs + row] = u;
+    }
+  }
+  // zero pad rows (m < 0 and m = L), written once per map by the m = 0 column
+  if (m == 0) {
+    const int per = p.dual ? 2 : 1;
+    const int halves = p.dual ? 1 : p.nhalf;
+    for (int h = 0; h < halves; ++h)
+      for (int pr = 0; pr < kPadLo + 1; ++pr) {
+        const int mr = pr < kPadLo ? pr : p.TR - 1;
+        R2* base = out + (((size_t)b * halves + h) * p.TR + mr) * p.Gs * per;
+        for (int x = threadIdx.x; x < p.Gs * per; x += blockDim.x) base[x] = czero<R2>();
+      }
+    if (p.dual || p.nhalf > 1) {
+      // the unused half of m = 0 in the dual layout is zero as well
+      if (p.dual)
+        for (int t = threadIdx.x; t < nout; t += blockDim.x) {
+          const int row = t == 0 ? 2 * L - 1 : t - 1;
+          out[(((size_t)b * p.TR + kPadLo) * p.Gs + row) * 2 + 1] = czero<R2>();
+        }
+      else
+        for (int t = threadIdx.x; t < nout; t += blockDim.x) {
+          const int row = t == 0 ? 2 * L - 1 : t - 1;
+          out[(((size_t)b * p.nhalf + 1) * p.TR + kPadLo) * p.Gs + row] = czero<R2>();
+        }
     }
   }
 }

@@ -39,6 +39,7 @@ struct RowsParams {
   int real_out;         // inverse: write the real part only
   int real_in;          // forward: real input map
   int dual, nhalf;      // forward spectra layout
+  int TR, Gs;           // forward spectra: table rows (m + kPadLo) and row stride
   int mode;             // RowsMode
   double scale;
   const FFTDesc* desc;  // transform descriptors
@@ -58,13 +59,15 @@ struct ColsParams {
   int L, spin, mw;      // mw = 1: input has L MW rings, else L+1 MWSS rings
   int nin;              // rings of the input columns
   int dual, nhalf;
+  int TR, Gs;           // spectra table rows and row stride
   double scale;         // overall factor of the chain
   const FFTDesc* d1;    // theta DFT over the periodic extension (2L-1 or 2L)
   const FFTDesc* d2;    // inverse DFT of length 4L
   const double* weights;// 2L+1 MWSS(2L) transform weights
   FFTTables<Real> tb;
   const void* in;       // Fc [B][ncm][nin]
-  void* out;            // G  [B][half][m][2L+1]
+  void* out;            // G  [B][half][m + kPadLo][Gs]; MWSS(2L) ring t -> row t-1,
+                        // north pole -> row 2L-1, south pole -> row 2L
 };
 
 }  // namespace s2b

@@ -32,6 +32,13 @@ struct Scaling<double> {
   static constexpr double kDown = 0x1p-800;
 };
 
+// Coefficient tables indexed by m are stored with kPadLo zero rows below m = 0
+// and one zero row above m = L - 1 (rows m in [-kPadLo, L]), so that every
+// R-step group of the latitudinal kernel is one fixed-size contiguous copy.
+constexpr int kPadLo = 8;
+__host__ __device__ inline int tab_rows(int L) { return L + kPadLo + 1; }
+__host__ __device__ inline int round4(int x) { return (x + 3) & ~3; }
+
 // One recursed ring (pole rings are handled separately, in closed form).
 struct RingInfo {
   double B;    // 2 cot(theta)
@@ -45,16 +52,20 @@ struct LatParams {
   int L, L0, spin;
   int nrings;       // recursed rings
   int nclass;       // C: l classes (CTAs along l); l = j + C*(ql + QA*k)
+  int Qp;           // l slots per class (padded to a multiple of 4)
   int nhalf;        // recursion halves handled by this launch (1 or 2)
   int batch;
   const RingInfo* rings;
   const int* ring_row;   // row of ring r in the ftm array (inverse out / forward in)
-  const void* seeds;     // [nhalf][L][nrings] {mantissa, exponent}
-  const void* H;         // [L (m)][L (l)] monic recursion coefficient
-  // inverse: in = F  [batch][nhalf][L (m)][L (l)] Real2 (Real4 when dual)
+  const void* seeds;     // [nhalf][C][Qp][nrings] {mantissa, exponent}
+  const void* H;         // [C][tab_rows][Qp] monic recursion coefficient h_{l,m}
+  // inverse: in = F  [batch][nhalf][C][tab_rows][Qp] Real2 (Real4 when dual)
   //          out = ftm [batch][nrows][ncol] Real2 (accumulated with atomics)
-  // forward: in = G  [batch][nhalf][L (m)][nrows] Real2 (Real4 when dual)
-  //          out = acc [batch][nhalf][L (m)][L (l)] Real2 (accumulated with atomics)
+  // forward: in = G  [batch][nhalf][tab_rows][Gs] Real2 (Real4 when dual);
+  //          ring r of the launch is row r of G (pole rows, if any, come after)
+  //          out = acc [batch][nhalf][C][L (m)][Qp] Real2 (accumulated with atomics)
+  int Gs;           // forward: row stride of G (multiple of 4)
+  int* status;      // device status word: nonzero after a timed-out wait
   const void* in;
   void* out;
   int nrows;        // rows of the ftm array
@@ -68,5 +79,8 @@ cudaError_t launch_latitudinal(bool fp64, bool forward, bool dual, const LatPara
                                cudaStream_t s);
 cudaError_t launch_seeds(bool fp64, int L, int L0, int spin, int nhalf, const RingInfo* rings,
                          int nrings, const double* lbin, void* seeds, cudaStream_t s);
+int lat_nclass(bool fp64, int L);
+int lat_qp(bool fp64, int L);
+size_t seed_bytes(bool fp64, int L, int nhalf, int nrings);
 
 }  // namespace s2b

@@ -7,7 +7,8 @@ namespace s2b {
 
 struct StageParams {
   int L, L0, spin, batch;
-  int nclass, Q;        // l classes of the latitudinal tiling, l = j + C q
+  int nclass, Q;        // l classes of the latitudinal tiling, l = j + C q (Q padded)
+  int TR, Gs;           // table rows (m + kPadLo) and forward spectra row stride
   int nhalf, dual;
   int nrows, ncol, mo;  // ftm / G row count, ftm columns, column offset
   int pole_south, pole_north;  // rows of the closed-form pole rings (-1: none)

@@ -10,6 +10,7 @@
 #include <cstdint>
 #include <type_traits>
 
+#include "s2b_internal.h"
 #include "s2b_stages.h"
 
 namespace s2b {
@@ -21,13 +22,14 @@ using R4_t = std::conditional_t<sizeof(Real) == 4, float4, double4>;
 
 __device__ __forceinline__ double lnorm(int l) { return sqrt((2.0 * l + 1.0) / (4.0 * 3.141592653589793)); }
 
-// F [b][half][j][m][q] (Real2, or Real4 when dual) from flm [b][l][L-1+m].
+// F [b][half][j][m + kPadLo][q] (Real2, or Real4 when dual) from flm [b][l][L-1+m];
+// the pad rows (m < 0, m = L) are written as zeros.
 template <typename Real>
 __global__ void prologue_kernel(StageParams p) {
   using R2 = R2_t<Real>;
   using R4 = R4_t<Real>;
-  const int L = p.L, C = p.nclass, Q = p.Q;
-  const long per_b = (long)p.nhalf * C * L * Q;
+  const int L = p.L, C = p.nclass, Q = p.Q, TR = p.TR;
+  const long per_b = (long)p.nhalf * C * TR * Q;
   const long total = per_b * p.batch;
   const R2* flm = reinterpret_cast<const R2*>(p.flm);
   for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
@@ -35,23 +37,24 @@ __global__ void prologue_kernel(StageParams p) {
     long r = idx;
     const int q = (int)(r % Q);
     r /= Q;
-    const int m = (int)(r % L);
-    r /= L;
+    const int m = (int)(r % TR) - kPadLo;
+    r /= TR;
     const int j = (int)(r % C);
     r /= C;
     const int half = (int)(r % p.nhalf);
     const int b = (int)(r / p.nhalf);
     const int l = j + C * q;
     const int as = p.spin < 0 ? -p.spin : p.spin;
-    const bool ok = l < L && l >= m && l >= p.L0 && l >= as;
+    const bool ok = m >= 0 && m < L && l < L && l >= m && l >= p.L0 && l >= as;
     double g = 0.0;
     if (ok) g = p.g[(size_t)m * L + l] * lnorm(l);
-    const R2* row = flm + ((size_t)b * L + (ok ? l : 0)) * (2 * L - 1);
+    const R2* row = flm + ((size_t)b * L + (ok ? l : 0)) * (2 * L - 1) + (ok ? 0 : (L - 1));
+    const int mm = ok ? m : 0;
     const double sgn_s = (p.spin & 1) ? -1.0 : 1.0;
     const double sgn_m = (m & 1) ? -1.0 : 1.0;
     if (p.dual) {
       R4 o;
-      R2 a = row[L - 1 + m], c = row[L - 1 - m];
+      R2 a = row[L - 1 + mm], c = row[L - 1 - mm];
       const double gp = ok ? g : 0.0;
       const double gn = (ok && m > 0) ? g * sgn_m : 0.0;
       o.x = (Real)(gp * a.x);
@@ -62,12 +65,12 @@ __global__ void prologue_kernel(StageParams p) {
     } else {
       R2 o;
       if (half == 0) {
-        const R2 a = row[L - 1 + m];
+        const R2 a = row[L - 1 + mm];
         const double f = ok ? g * sgn_s : 0.0;
         o.x = (Real)(f * a.x);
         o.y = (Real)(f * a.y);
       } else {
-        const R2 a = row[L - 1 - m];
+        const R2 a = row[L - 1 - mm];
         const double f = (ok && m > 0) ? g * sgn_m : 0.0;
         o.x = (Real)(f * a.x);
         o.y = (Real)(f * a.y);
@@ -125,9 +128,10 @@ __device__ __forceinline__ R2_t<Real> spectrum_at(const StageParams& p, int b, i
   const int L = p.L;
   const int am = m < 0 ? -m : m;
   const R2* G = reinterpret_cast<const R2*>(p.G);
-  if (p.dual) return G[(((size_t)b * L + am) * p.nrows + row) * 2 + (m < 0 ? 1 : 0)];
-  if (m >= 0) return G[(((size_t)b * p.nhalf + 0) * L + am) * p.nrows + row];
-  if (p.nhalf > 1) return G[(((size_t)b * p.nhalf + 1) * L + am) * p.nrows + row];
+  const size_t mr = (size_t)(am + kPadLo);
+  if (p.dual) return G[(((size_t)b * p.TR + mr) * p.Gs + row) * 2 + (m < 0 ? 1 : 0)];
+  if (m >= 0) return G[(((size_t)b * p.nhalf + 0) * p.TR + mr) * p.Gs + row];
+  if (p.nhalf > 1) return G[(((size_t)b * p.nhalf + 1) * p.TR + mr) * p.Gs + row];
   R2 z;
   z.x = 0;
   z.y = 0;
@@ -241,7 +245,7 @@ static int grid_for(long n) {
 }
 
 cudaError_t launch_prologue(bool fp64, const StageParams& p, cudaStream_t s) {
-  const long total = (long)p.batch * p.nhalf * p.nclass * p.L * p.Q;
+  const long total = (long)p.batch * p.nhalf * p.nclass * p.TR * p.Q;
   if (fp64)
     prologue_kernel<double><<<grid_for(total), 256, 0, s>>>(p);
   else

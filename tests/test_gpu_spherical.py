@@ -114,3 +114,35 @@ def test_torch_device_io(s2b, rng):
     assert isinstance(f, torch.Tensor) and f.is_cuda
     g = s2b.forward(f, L)
     assert relerr(g.cpu().numpy(), flm) < TOL64
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_golden_wigner(s2b, golden, precision):
+    data, index = golden
+    tol = TOL64 if precision == "f64" else TOL32
+    for c in [c for c in index["cases"] if c["kind"] == "wigner"]:
+        n = c["name"]
+        f = s2b.wigner.inverse(data[f"{n}/flmn"], c["L"], c["N"], None, c["sampling"],
+                               reality=c["reality"], precision=precision)
+        ref = np.real(data[f"{n}/f"]) if c["reality"] else data[f"{n}/f"]
+        assert relerr(f, ref) < tol, (n, relerr(f, ref))
+        g = s2b.wigner.forward(ref, c["L"], c["N"], None, c["sampling"],
+                               reality=c["reality"], precision=precision)
+        assert relerr(g, data[f"{n}/flmn_fwd"]) < tol, (n, relerr(g, data[f"{n}/flmn_fwd"]))
+
+
+def test_wigner_so3_L32_N4(s2b, rng):
+    L, N = 32, 4
+    flmn = oracle.signal.generate_flmn(rng, L, N)
+    ref = oracle.wigner.inverse(flmn, L, N)
+    f = s2b.wigner.inverse(flmn, L, N)
+    assert relerr(f, ref) < TOL64
+    g = s2b.wigner.forward(ref, L, N)
+    assert relerr(g, flmn) < TOL64
+
+
+def test_device_status_clean(s2b):
+    from s2fft_b200 import _lib
+
+    for key, plan in list(_lib._plans.items()):
+        assert plan.status() == 0
