@@ -88,6 +88,26 @@ __global__ void seed_kernel(int L, int L0, int spin, int nhalf, int C, int Q,
   }
 }
 
+// lambda(theta_r, m) = 2 (n - m cos theta) / sin theta = n A_r - m B_r, evaluated in
+// double and rounded once; layout [half][m + kPadLo][Ls], zero outside 0 <= m < L.
+template <typename Real>
+__global__ void lambda_kernel(int L, int spin, int nhalf, const RingInfo* __restrict__ rings,
+                              int nrings, int Ls, Real* __restrict__ out) {
+  const int TR = tab_rows(L);
+  const long total = (long)nhalf * TR * Ls;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long)gridDim.x * blockDim.x) {
+    const int r = (int)(idx % Ls);
+    const int mr = (int)((idx / Ls) % TR);
+    const int half = (int)(idx / ((long)Ls * TR));
+    const int m = mr - kPadLo;
+    const int n = half == 0 ? -spin : spin;
+    double v = 0.0;
+    if (r < nrings && m >= 0 && m < L) v = fma(-(double)m, rings[r].B, (double)n * rings[r].A);
+    out[idx] = (Real)v;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // main kernel
 // ---------------------------------------------------------------------------
@@ -209,7 +229,8 @@ struct LatSmem {
   __host__ __device__ static size_t d_bytes(int Qp) {
     return (size_t)R * (FWD ? NRT : Qp) * sizeof(Acc);
   }
-  __host__ __device__ static size_t stage_bytes(int Qp) { return h_bytes(Qp) + d_bytes(Qp); }
+  __host__ __device__ static size_t l_bytes() { return (size_t)R * NRT * sizeof(Real); }
+  __host__ __device__ static size_t stage_bytes(int Qp) { return h_bytes(Qp) + d_bytes(Qp) + l_bytes(); }
   __host__ __device__ static size_t total(int Qp) { return red_bytes() + 2 * stage_bytes(Qp) + 16; }
 };
 
@@ -243,16 +264,7 @@ __global__ void __launch_bounds__(QA* QT)
   const int lmax = j + C * ((L - 1 - j) / C);
   const int TR = tab_rows(L);
 
-  // ring constants: lambda = n*A - m*B (double FMA per (ring, m))
-  double nA[T], Bc[T];
-  bool rvalid[T];
-#pragma unroll
-  for (int i = 0; i < T; ++i) {
-    const int r = rbase + i;
-    rvalid[i] = r < p.nrings;
-    nA[i] = rvalid[i] ? (double)n * p.rings[r].A : 0.0;
-    Bc[i] = rvalid[i] ? p.rings[r].B : 0.0;
-  }
+  (void)n;
 
   Real v[K][T], w[K][T], sc[K][T];
   int ex[K][T];
@@ -280,6 +292,9 @@ __global__ void __launch_bounds__(QA* QT)
     ncopy = p.Gs - r0;
     if (ncopy > NRT) ncopy = NRT;
   }
+  const Real* __restrict__ lamh = reinterpret_cast<const Real*>(p.lam) + (size_t)half * TR * p.Ls;
+  int nlam = p.Ls - r0;
+  if (nlam > NRT) nlam = NRT;
 
   // even-aligned chunk boundaries: chunk k covers m in [clo(k), clo(k+1)-1]
   auto clo = [&](int k) -> int {
@@ -295,7 +310,7 @@ __global__ void __launch_bounds__(QA* QT)
   auto issue = [&](int g) {
     unsigned char* st = stage_base + (size_t)(g & 1) * SM::stage_bytes(Qp);
     const int row0 = mtop - g * R - R + 1 + kPadLo;
-    unsigned bytes = (unsigned)SM::h_bytes(Qp);
+    unsigned bytes = (unsigned)SM::h_bytes(Qp) + (unsigned)(R * nlam * sizeof(Real));
     if constexpr (!FWD)
       bytes += (unsigned)SM::d_bytes(Qp);
     else
@@ -312,7 +327,16 @@ __global__ void __launch_bounds__(QA* QT)
         bulk_g2s(dst + (size_t)s * NRT * sizeof(Acc), Din + (size_t)(row0 + s) * p.Gs + r0,
                  (unsigned)(ncopy * sizeof(Acc)), &mbar[g & 1]);
     }
+    unsigned char* ldst = st + SM::h_bytes(Qp) + SM::d_bytes(Qp);
+#pragma unroll
+    for (int s = 0; s < R; ++s)
+      bulk_g2s(ldst + (size_t)s * NRT * sizeof(Real), lamh + (size_t)(row0 + s) * p.Ls + r0,
+               (unsigned)(nlam * sizeof(Real)), &mbar[g & 1]);
   };
+  // zero both stages once: columns beyond a copy's extent then read as zeros
+  for (size_t x = tid * 16; x < 2 * SM::stage_bytes(Qp); x += (size_t)Cfg::NT * 16)
+    *reinterpret_cast<uint4*>(stage_base + x) = make_uint4(0, 0, 0, 0);
+  __syncthreads();
   if (tid == 0) {
     mbar_init(&mbar[0], 1);
     mbar_init(&mbar[1], 1);
@@ -329,6 +353,7 @@ __global__ void __launch_bounds__(QA* QT)
   int mgrp = mtop;  // m of the first step of the current group
   const Real* Hs = nullptr;
   const Acc* Ds = nullptr;
+  const Real* Ls_ = nullptr;
 
   // reduction + renormalisation, every R steps (and at the end)
   auto flush = [&](int nsteps) {
@@ -420,13 +445,12 @@ __global__ void __launch_bounds__(QA* QT)
     const int srow = R - 1 - gstep;                                                    \
     const Real* Hrow = Hs + srow * Qp;                                                 \
     Real lam[T];                                                                       \
-    _Pragma("unroll") for (int i = 0; i < T; ++i) lam[i] = (Real)fma(-md, Bc[i], nA[i]); \
+    _Pragma("unroll") for (int i = 0; i < T; ++i) lam[i] = Ls_[srow * NRT + qt * T + i]; \
     Acc accT[T];                                                                       \
     Acc gin[T];                                                                        \
     if constexpr (FWD) {                                                               \
       const Acc* Grow = Ds + srow * NRT + qt * T;                                      \
-      _Pragma("unroll") for (int i = 0; i < T; ++i) gin[i] =                           \
-          rvalid[i] ? Grow[i] : zero_acc<Acc>();                                       \
+      _Pragma("unroll") for (int i = 0; i < T; ++i) gin[i] = Grow[i];                  \
     } else {                                                                           \
       _Pragma("unroll") for (int i = 0; i < T; ++i) accT[i] = zero_acc<Acc>();         \
     }                                                                                  \
@@ -441,12 +465,9 @@ __global__ void __launch_bounds__(QA* QT)
           sc[k][i] = sde[i] >= 0 ? Real(1) : Real(0);                                  \
         }                                                                              \
       }                                                                                \
-      Real h = Real(0);                                                                \
-      Acc fk = zero_acc<Acc>();                                                        \
-      if (l < L) {                                                                     \
-        h = Hrow[q];                                                                   \
-        if constexpr (!FWD) fk = Ds[srow * Qp + q];                                    \
-      }                                                                                \
+      const Real h = Hrow[q];                                                          \
+      Acc fk;                                                                          \
+      if constexpr (!FWD) fk = Ds[srow * Qp + q];                                      \
       Acc accK = zero_acc<Acc>();                                                      \
       _Pragma("unroll") for (int i = 0; i < T; ++i) {                                  \
         const Real x = CUR[k][i] * sc[k][i];                                           \
@@ -467,11 +488,9 @@ __global__ void __launch_bounds__(QA* QT)
     }                                                                                  \
     ++gstep;                                                                           \
     --m;                                                                               \
-    md -= 1.0;                                                                         \
   }
 
   int m = mtop;
-  double md = (double)mtop;
   Real sdv[T];
   int sde[T];
 #pragma unroll
@@ -484,7 +503,7 @@ __global__ void __launch_bounds__(QA* QT)
 #pragma unroll
       for (int i = 0; i < T; ++i) {
         SeedT<Real> sd{Real(0), 0};
-        if (l < L && rvalid[i]) sd = seeds[(size_t)q * p.nrings + rbase + i];
+        if (l < L && rbase + i < p.nrings) sd = seeds[(size_t)q * p.nrings + rbase + i];
         sdv[i] = sd.v;
         sde[i] = sd.e;
       }
@@ -500,6 +519,7 @@ __global__ void __launch_bounds__(QA* QT)
         unsigned char* st = stage_base + (size_t)(grp & 1) * SM::stage_bytes(Qp);
         Hs = reinterpret_cast<const Real*>(st);
         Ds = reinterpret_cast<const Acc*>(st + SM::h_bytes(Qp));
+        Ls_ = reinterpret_cast<const Real*>(st + SM::h_bytes(Qp) + SM::d_bytes(Qp));
       }
       S2B_STEP(v, w, kc)
       S2B_STEP(w, v, kc)
@@ -528,8 +548,9 @@ int lat_nclass(bool fp64, int L) {
 }
 
 int lat_qp(bool fp64, int L) {
-  const int C = lat_nclass(fp64, L);
-  return round4((L + C - 1) / C);
+  (void)fp64;
+  (void)L;
+  return kQA * kK;  // fixed row width: every slot load of the kernel stays inside the row
 }
 
 template <typename Real, bool FWD, bool DUAL, int T, int K, int QA, int QT, int R>
@@ -579,6 +600,18 @@ cudaError_t launch_seeds(bool fp64, int L, int L0, int spin, int nhalf, const Ri
   else
     seed_kernel<float><<<(int)blocks, threads, 0, s>>>(L, L0, spin, nhalf, C, Qp, rings, nrings,
                                                        lbin, reinterpret_cast<SeedT<float>*>(seeds));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lambda(bool fp64, int L, int spin, int nhalf, const RingInfo* rings, int nrings,
+                          int Ls, void* lam, cudaStream_t s) {
+  const long total = (long)nhalf * tab_rows(L) * Ls;
+  long blocks = (total + 255) / 256;
+  if (blocks > 8192) blocks = 8192;
+  if (fp64)
+    lambda_kernel<double><<<(int)blocks, 256, 0, s>>>(L, spin, nhalf, rings, nrings, Ls, (double*)lam);
+  else
+    lambda_kernel<float><<<(int)blocks, 256, 0, s>>>(L, spin, nhalf, rings, nrings, Ls, (float*)lam);
   return cudaGetLastError();
 }
 

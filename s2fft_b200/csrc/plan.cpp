@@ -333,6 +333,9 @@ struct s2b_plan {
   int* fwd_ring_row = nullptr;
   void* inv_seeds = nullptr;
   void* fwd_seeds = nullptr;
+  void* inv_lam = nullptr;
+  void* fwd_lam = nullptr;
+  int inv_Ls = 4, fwd_Ls = 4;
   double* lbin = nullptr;
   double* gtab = nullptr;
   void* htab = nullptr;
@@ -547,6 +550,25 @@ static int build_plan(s2b_plan* p) {
                         p->lbin, p->fwd_seeds, 0));
   }
 
+  // ---- lambda(theta, m) tables (double, rounded once to the plan precision)
+  {
+    p->inv_Ls = round4(std::max(p->inv_nrings, 1));
+    p->fwd_Ls = round4(p->fwd_nrings);
+    const size_t bi = (size_t)p->nhalf * p->TR * p->inv_Ls * p->rsz;
+    const size_t bf = (size_t)p->nhalf * p->TR * p->fwd_Ls * p->rsz;
+    S2B_CK(cudaMalloc(&p->inv_lam, bi));
+    p->allocs.push_back(p->inv_lam);
+    S2B_CK(cudaMalloc(&p->fwd_lam, bf));
+    p->allocs.push_back(p->fwd_lam);
+    if (p->inv_nrings > 0)
+      S2B_CK(launch_lambda(p->fp64, L, d.spin, p->nhalf, p->inv_rings, p->inv_nrings, p->inv_Ls,
+                           p->inv_lam, 0));
+    else
+      S2B_CK(cudaMemset(p->inv_lam, 0, bi));
+    S2B_CK(launch_lambda(p->fp64, L, d.spin, p->nhalf, p->fwd_rings, p->fwd_nrings, p->fwd_Ls,
+                         p->fwd_lam, 0));
+  }
+
   // ---- FFT tables and ring layout
   FFTBuild fb;
   std::vector<long> roff(p->nth);
@@ -683,6 +705,8 @@ static int run_inverse(s2b_plan* p, const void* flm, void* f, char* ws, cudaStre
     lp.mo = p->inv_mo;
     lp.reality = d.reality;
     lp.status = p->status;
+    lp.lam = p->inv_lam;
+    lp.Ls = p->inv_Ls;
     if (p->ev_begin[0]) S2B_CK(cudaEventRecord(p->ev_begin[0], s));
     S2B_CK(launch_latitudinal(p->fp64, false, p->dual, lp, s));
     if (p->ev_end[0]) S2B_CK(cudaEventRecord(p->ev_end[0], s));
@@ -781,6 +805,8 @@ static int run_forward_once(s2b_plan* p, const void* f, void* flm, char* ws, cud
   lp.nrows = p->fwd_nrows;
   lp.Gs = p->Gs;
   lp.status = p->status;
+  lp.lam = p->fwd_lam;
+  lp.Ls = p->fwd_Ls;
   if (p->ev_begin[1]) S2B_CK(cudaEventRecord(p->ev_begin[1], s));
   S2B_CK(launch_latitudinal(p->fp64, true, p->dual, lp, s));
   if (p->ev_end[1]) S2B_CK(cudaEventRecord(p->ev_end[1], s));
@@ -997,7 +1023,17 @@ int s2b_wigner_forward(s2b_plan* p, const void* f, void* flmn, void* ws, size_t 
 
 int s2b_plan_status(s2b_plan* p, int* status) {
   if (!p || !status) return fail(S2B_ERR_INVALID, "plan and status must be non-NULL");
-  S2B_CK(cudaMemcpy(status, p->status, sizeof(int), cudaMemcpyDeviceToHost));
+  *status = 0;
+  for (s2b_plan* sp : p->subs) {
+    int st = 0;
+    S2B_CK(cudaMemcpy(&st, sp->status, sizeof(int), cudaMemcpyDeviceToHost));
+    *status |= st;
+  }
+  if (p->status) {
+    int st = 0;
+    S2B_CK(cudaMemcpy(&st, p->status, sizeof(int), cudaMemcpyDeviceToHost));
+    *status |= st;
+  }
   if (*status) return fail(S2B_ERR_TIMEOUT, "a bounded device wait gave up");
   return S2B_OK;
 }

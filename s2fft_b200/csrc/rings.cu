@@ -406,7 +406,7 @@ __global__ void mw_cols_kernel(ColsParams<Real> p) {
     const double f = p.scale * p.weights[t];
     u.x = (Real)((double)u.x * f);
     u.y = (Real)((double)u.y * f);
-    const int row = t == 0 ? 2 * L - 1 : t - 1;  // poles after the recursed rings
+    const int row = t == 0 ? 2 * L - 1 : (t == 2 * L ? 2 * L : t - 1);  // poles after the recursed rings
     const size_t mr = (size_t)(am + kPadLo);
     if (p.dual) {
       // Real4 {+m, -m} viewed as pairs of Real2
@@ -431,12 +431,12 @@ __global__ void mw_cols_kernel(ColsParams<Real> p) {
       // the unused half of m = 0 in the dual layout is zero as well
       if (p.dual)
         for (int t = threadIdx.x; t < nout; t += blockDim.x) {
-          const int row = t == 0 ? 2 * L - 1 : t - 1;
+          const int row = t == 0 ? 2 * L - 1 : (t == 2 * L ? 2 * L : t - 1);
           out[(((size_t)b * p.TR + kPadLo) * p.Gs + row) * 2 + 1] = czero<R2>();
         }
       else
         for (int t = threadIdx.x; t < nout; t += blockDim.x) {
-          const int row = t == 0 ? 2 * L - 1 : t - 1;
+          const int row = t == 0 ? 2 * L - 1 : (t == 2 * L ? 2 * L : t - 1);
           out[(((size_t)b * p.nhalf + 1) * p.TR + kPadLo) * p.Gs + row] = czero<R2>();
         }
     }

@@ -65,6 +65,8 @@ struct LatParams {
   //          ring r of the launch is row r of G (pole rows, if any, come after)
   //          out = acc [batch][nhalf][C][L (m)][Qp] Real2 (accumulated with atomics)
   int Gs;           // forward: row stride of G (multiple of 4)
+  const void* lam;  // [nhalf][tab_rows][Ls] lambda(theta_r, m) = 2 (n - m cos) / sin, rounded once
+  int Ls;           // row stride of lam (multiple of 4, >= nrings)
   int* status;      // device status word: nonzero after a timed-out wait
   const void* in;
   void* out;
@@ -80,6 +82,8 @@ cudaError_t launch_latitudinal(bool fp64, bool forward, bool dual, const LatPara
 cudaError_t launch_seeds(bool fp64, int L, int L0, int spin, int nhalf, const RingInfo* rings,
                          int nrings, const double* lbin, void* seeds, cudaStream_t s);
 int lat_nclass(bool fp64, int L);
+cudaError_t launch_lambda(bool fp64, int L, int spin, int nhalf, const RingInfo* rings, int nrings,
+                          int Ls, void* lam, cudaStream_t s);
 int lat_qp(bool fp64, int L);
 size_t seed_bytes(bool fp64, int L, int nhalf, int nrings);
 

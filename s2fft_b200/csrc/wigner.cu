@@ -21,16 +21,18 @@ static int wgrid(long n) {
   return b < 1 ? 1 : (int)b;
 }
 
-// tmp[b][l][c] = flmn[b][N-1+n][l][c] * (-1)^n / (2 pi): the spin transform then
-// supplies sqrt((2l+1)/4pi), so the product is sqrt((2l+1)/(16 pi^3)).
+// tmp[b][l][c] = flmn[b][N-1+n][l][c] * (-1)^n sqrt((2l+1)/(16 pi^3)); the spin
+// transform that follows applies its own sqrt((2l+1)/4pi) on top, as upstream does.
 template <typename Real>
 __global__ void gather_n_kernel(const W2<Real>* flmn, W2<Real>* tmp, int B, int N, int L, int n) {
   const long per = (long)L * (2 * L - 1);
   const long total = per * B;
-  const double f = ((n & 1) ? -1.0 : 1.0) / (2.0 * 3.141592653589793);
+  const double pi = 3.141592653589793;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
        i += (long)gridDim.x * blockDim.x) {
     const long b = i / per, r = i % per;
+    const int l = (int)(r / (2 * L - 1));
+    const double f = ((n & 1) ? -1.0 : 1.0) * sqrt((2.0 * l + 1.0) / (16.0 * pi * pi * pi));
     W2<Real> v = flmn[(b * (2 * N - 1) + (N - 1 + n)) * per + r];
     v.x = (Real)(v.x * f);
     v.y = (Real)(v.y * f);
