@@ -231,11 +231,16 @@ struct LatSmem {
   }
   __host__ __device__ static size_t l_bytes() { return (size_t)R * NRT * sizeof(Real); }
   __host__ __device__ static size_t stage_bytes(int Qp) { return h_bytes(Qp) + d_bytes(Qp) + l_bytes(); }
-  __host__ __device__ static size_t total(int Qp) { return red_bytes() + 2 * stage_bytes(Qp) + 16; }
+  __host__ __device__ static size_t seed_area() {
+    return ((size_t)QA * QT * T * 2 * sizeof(Real) + 15) & ~(size_t)15;
+  }
+  __host__ __device__ static size_t total(int Qp) {
+    return red_bytes() + 2 * stage_bytes(Qp) + seed_area() + 16;
+  }
 };
 
 template <typename Real, bool FWD, bool DUAL, int T, int K, int QA, int QT, int R>
-__global__ void __launch_bounds__(QA* QT)
+__global__ void __launch_bounds__(QA* QT, sizeof(Real) == 4 ? 4 : 3)
     lat_kernel(const LatParams p) {
   using Cfg = LatCfg<Real, FWD, DUAL, T, K, QA, QT, R>;
   using Acc = typename Cfg::Acc;
@@ -247,7 +252,9 @@ __global__ void __launch_bounds__(QA* QT)
   const int Qp = p.Qp;
   Acc* buf = reinterpret_cast<Acc*>(smem_raw);
   unsigned char* stage_base = smem_raw + SM::red_bytes();
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(stage_base + 2 * SM::stage_bytes(Qp));
+  SeedT<Real>* seed_sm = reinterpret_cast<SeedT<Real>*>(stage_base + 2 * SM::stage_bytes(Qp));
+  uint64_t* mbar =
+      reinterpret_cast<uint64_t*>(stage_base + 2 * SM::stage_bytes(Qp) + SM::seed_area());
 
   const int tid = threadIdx.x;
   const int ql = tid % QA;
@@ -267,16 +274,27 @@ __global__ void __launch_bounds__(QA* QT)
   (void)n;
 
   Real v[K][T], w[K][T], sc[K][T];
-  int ex[K][T];
+  // exponents, two 16-bit values per register (only read on the renormalisation path)
+  constexpr int TE = (T + 1) / 2;
+  int ex2[K][TE];
 #pragma unroll
-  for (int k = 0; k < K; ++k)
+  for (int k = 0; k < K; ++k) {
 #pragma unroll
     for (int i = 0; i < T; ++i) {
       v[k][i] = Real(0);
       w[k][i] = Real(0);
       sc[k][i] = Real(0);
-      ex[k][i] = 0;
     }
+#pragma unroll
+    for (int i = 0; i < TE; ++i) ex2[k][i] = 0;
+  }
+  auto ex_get = [&](int k, int i) -> int {
+    return (int)(short)((ex2[k][i >> 1] >> ((i & 1) * 16)) & 0xffff);
+  };
+  auto ex_set = [&](int k, int i, int e) {
+    const int sh = (i & 1) * 16;
+    ex2[k][i >> 1] = (ex2[k][i >> 1] & ~(0xffff << sh)) | ((e & 0xffff) << sh);
+  };
 
   const Real* __restrict__ Hc = reinterpret_cast<const Real*>(p.H) + (size_t)j * TR * Qp;
   const SeedT<Real>* __restrict__ seeds =
@@ -297,14 +315,15 @@ __global__ void __launch_bounds__(QA* QT)
   if (nlam > NRT) nlam = NRT;
 
   // even-aligned chunk boundaries: chunk k covers m in [clo(k), clo(k+1)-1]
+  // chunk boundaries aligned to the group length R (a power of two)
   auto clo = [&](int k) -> int {
     const int x = j + C * QA * k;
-    return k == 0 ? 0 : (x & ~1);
+    return k == 0 ? 0 : (x & ~(R - 1));
   };
-  const int mtop = lmax | 1;  // odd, >= lmax
+  const int mtop = lmax | (R - 1);  // == R-1 (mod R), >= lmax
   int ktop = (lmax - j) / (C * QA);
   if (ktop > K - 1) ktop = K - 1;
-  const int ngroups = (mtop + R) / R;
+  const int ngroups = (mtop + 1) / R;
 
   // group g covers steps m = mtop - g R ... mtop - g R - R + 1 (table rows ascending)
   auto issue = [&](int g) {
@@ -348,7 +367,6 @@ __global__ void __launch_bounds__(QA* QT)
     if (ngroups > 1) issue(1);
   }
 
-  int gstep = 0;    // steps done in the current group
   int grp = 0;      // current group
   int mgrp = mtop;  // m of the first step of the current group
   const Real* Hs = nullptr;
@@ -372,7 +390,7 @@ __global__ void __launch_bounds__(QA* QT)
         if (m < 0 || m >= L || r >= p.nrings) continue;
         const Acc* row = buf + ((s * T + i) * QT + qq) * (QA + 1);
         Acc a = zero_acc<Acc>();
-#pragma unroll
+#pragma unroll 4
         for (int x = 0; x < QA; ++x) acc_add(a, row[x]);
         using R2 = typename Cfg::R2;
         R2* ftm = reinterpret_cast<R2*>(p.out) + ((size_t)b * p.nrows + p.ring_row[r]) * p.ncol;
@@ -409,7 +427,7 @@ __global__ void __launch_bounds__(QA* QT)
         const int l = j + C * q;
         if (m < 0 || m >= L || l >= L || l < m) continue;
         Acc a = zero_acc<Acc>();
-#pragma unroll
+#pragma unroll 4
         for (int y = 0; y < QT; ++y) acc_add(a, buf[((s * K + k) * QT + y) * QA + x]);
         Acc* out = reinterpret_cast<Acc*>(p.out) +
                    ((((size_t)b * p.nhalf + half) * C + j) * L + m) * Qp + q;
@@ -433,16 +451,18 @@ __global__ void __launch_bounds__(QA* QT)
           if (fabs(v[k][i]) > trig) {
             v[k][i] *= down;
             w[k][i] *= down;
-            ex[k][i] += 1;
-            sc[k][i] = ex[k][i] >= 0 ? Real(1) : Real(0);
+            const int e = ex_get(k, i) + 1;
+            ex_set(k, i, e);
+            sc[k][i] = e >= 0 ? Real(1) : Real(0);
           }
     }
   };
 
-  // one recursion step at m; CUR holds dt_m, PRV holds dt_{m+1} and receives dt_{m-1}
-#define S2B_STEP(CUR, PRV, KC)                                                         \
+  // one recursion step at m (S = step index inside the group, compile-time);
+  // CUR holds dt_m, PRV holds dt_{m+1} and receives dt_{m-1}
+#define S2B_STEP(CUR, PRV, KC, S)                                                      \
   {                                                                                    \
-    const int srow = R - 1 - gstep;                                                    \
+    constexpr int srow = R - 1 - (S);                                                  \
     const Real* Hrow = Hs + srow * Qp;                                                 \
     Real lam[T];                                                                       \
     _Pragma("unroll") for (int i = 0; i < T; ++i) lam[i] = Ls_[srow * NRT + qt * T + i]; \
@@ -454,17 +474,20 @@ __global__ void __launch_bounds__(QA* QT)
     } else {                                                                           \
       _Pragma("unroll") for (int i = 0; i < T; ++i) accT[i] = zero_acc<Acc>();         \
     }                                                                                  \
-    _Pragma("unroll") for (int k = KC; k < K; ++k) {                                   \
-      const int q = ql + QA * k;                                                       \
-      const int l = j + C * q;                                                         \
-      if (k == KC && l == m) {                                                         \
+    if (rem == 0) {                                                                    \
+      /* CTA-uniform: some lane's slot KC reaches l == m on this step */              \
+      if (lkc == m) {                                                                  \
         _Pragma("unroll") for (int i = 0; i < T; ++i) {                                \
-          CUR[k][i] = sdv[i];                                                          \
-          PRV[k][i] = Real(0);                                                         \
-          ex[k][i] = sde[i];                                                           \
-          sc[k][i] = sde[i] >= 0 ? Real(1) : Real(0);                                  \
+          const SeedT<Real> sd = seed_sm[tid * T + i];                                 \
+          CUR[KC][i] = sd.v;                                                           \
+          PRV[KC][i] = Real(0);                                                        \
+          ex_set(KC, i, sd.e);                                                         \
+          sc[KC][i] = sd.e >= 0 ? Real(1) : Real(0);                                   \
         }                                                                              \
       }                                                                                \
+    }                                                                                  \
+    _Pragma("unroll") for (int k = KC; k < K; ++k) {                                   \
+      const int q = ql + QA * k;                                                       \
       const Real h = Hrow[q];                                                          \
       Acc fk;                                                                          \
       if constexpr (!FWD) fk = Ds[srow * Qp + q];                                      \
@@ -477,62 +500,57 @@ __global__ void __launch_bounds__(QA* QT)
           acc_fma(accK, x, gin[i]);                                                    \
         PRV[k][i] = fma(lam[i] * h, CUR[k][i], -PRV[k][i]);                            \
       }                                                                                \
-      if constexpr (FWD) buf[(((gstep)*K + k) * QT + qt) * QA + ql] = accK;            \
+      if constexpr (FWD) buf[((srow_b(S) * K + k) * QT + qt) * QA + ql] = accK;        \
     }                                                                                  \
-    if constexpr (FWD) {                                                               \
-      _Pragma("unroll") for (int k = 0; k < KC; ++k)                                   \
-          buf[(((gstep)*K + k) * QT + qt) * QA + ql] = zero_acc<Acc>();                \
-    } else {                                                                           \
+    if constexpr (!FWD) {                                                              \
       _Pragma("unroll") for (int i = 0; i < T; ++i)                                    \
-          buf[(((gstep)*T + i) * QT + qt) * (QA + 1) + ql] = accT[i];                  \
+          buf[((srow_b(S) * T + i) * QT + qt) * (QA + 1) + ql] = accT[i];              \
     }                                                                                  \
-    ++gstep;                                                                           \
     --m;                                                                               \
+    rem = rem == 0 ? C - 1 : rem - 1;                                                  \
   }
+#define srow_b(S) (S)
 
   int m = mtop;
-  Real sdv[T];
-  int sde[T];
+  int rem = (mtop - j) % C;  // (m - j) mod C; activation possible only when 0
 #pragma unroll
   for (int kc = K - 1; kc >= 0; --kc) {
     if (kc > ktop) continue;
     // seeds of slot kc for this thread (activated when m reaches l)
-    {
-      const int q = ql + QA * kc;
-      const int l = j + C * q;
+    const int qkc = ql + QA * kc;
+    const int lkc = j + C * qkc;
 #pragma unroll
-      for (int i = 0; i < T; ++i) {
-        SeedT<Real> sd{Real(0), 0};
-        if (l < L && rbase + i < p.nrings) sd = seeds[(size_t)q * p.nrings + rbase + i];
-        sdv[i] = sd.v;
-        sde[i] = sd.e;
-      }
+    for (int i = 0; i < T; ++i) {
+      SeedT<Real> sd{Real(0), 0};
+      if (lkc < L && rbase + i < p.nrings) sd = seeds[(size_t)qkc * p.nrings + rbase + i];
+      seed_sm[tid * T + i] = sd;  // thread-private slot
     }
     const int lo = clo(kc);
     while (m >= lo) {
-      if (gstep == 0) {
-        const bool ok = mbar_wait(&mbar[grp & 1], (grp >> 1) & 1);
-        if (!__syncthreads_and(ok)) {
-          if (tid == 0) atomicExch(p.status, 1);
-          return;
-        }
+      // one reduction group of R steps per iteration
+      const bool ok = mbar_wait(&mbar[grp & 1], (grp >> 1) & 1);
+      if (!__syncthreads_and(ok)) {
+        if (tid == 0) atomicExch(p.status, 1);
+        return;
+      }
+      {
         unsigned char* st = stage_base + (size_t)(grp & 1) * SM::stage_bytes(Qp);
         Hs = reinterpret_cast<const Real*>(st);
         Ds = reinterpret_cast<const Acc*>(st + SM::h_bytes(Qp));
         Ls_ = reinterpret_cast<const Real*>(st + SM::h_bytes(Qp) + SM::d_bytes(Qp));
       }
-      S2B_STEP(v, w, kc)
-      S2B_STEP(w, v, kc)
-      if (gstep == R) {
-        flush(R);
-        gstep = 0;
-        mgrp = m;
-        ++grp;
-        if (tid == 0 && grp + 1 < ngroups) issue(grp + 1);
-      }
+      static_assert(R == 4, "the group body below is written for R = 4");
+      S2B_STEP(v, w, kc, 0)
+      S2B_STEP(w, v, kc, 1)
+      S2B_STEP(v, w, kc, 2)
+      S2B_STEP(w, v, kc, 3)
+      flush(R);
+      mgrp = m;
+      ++grp;
+      if (tid == 0 && grp + 1 < ngroups) issue(grp + 1);
     }
   }
-  if (gstep > 0) flush(gstep);
+#undef srow_b
 #undef S2B_STEP
 }
 

@@ -244,9 +244,19 @@ __global__ void inv_rows_kernel(RowsParams<Real> p) {
 
 template <typename Real, typename Val>
 __device__ __forceinline__ void store_spectra(const RowsParams<Real>& p, int b, int t, Val val) {
-  // G [b][half][m + kPadLo][Gs]: rows m < 0 and m = L are zero pads
+  // G [b][half][m + kPadLo][Gs]: rows m outside [0, L) and columns >= nrows are zero
   using R2 = typename C2<Real>::t;
   const int L = p.L;
+  if (t == p.nrows - 1 && p.Gs > p.nrows) {
+    const int halves = p.dual ? 1 : p.nhalf, per = p.dual ? 2 : 1;
+    R2* o2 = reinterpret_cast<R2*>(p.out);
+    const int padc = p.Gs - p.nrows;
+    for (int x = threadIdx.x; x < halves * p.TR * padc * per; x += blockDim.x) {
+      const int c = x % (padc * per);
+      const int rowi = x / (padc * per);
+      o2[(((size_t)b * halves * p.TR + rowi) * p.Gs + p.nrows) * per + c] = czero<R2>();
+    }
+  }
   if (p.dual) {
     using R4 = std::conditional_t<sizeof(Real) == 4, float4, double4>;
     R4* out = reinterpret_cast<R4*>(p.out);
@@ -417,13 +427,19 @@ __global__ void mw_cols_kernel(ColsParams<Real> p) {
       out[(((size_t)b * p.nhalf + 1) * p.TR + mr) * p.Gs + row] = u;
     }
   }
-  // zero pad rows (m < 0 and m = L), written once per map by the m = 0 column
+  // zero pad rows (m outside [0, L)) and pad columns (>= 2L+1), once per map (m = 0 CTA)
   if (m == 0) {
     const int per = p.dual ? 2 : 1;
     const int halves = p.dual ? 1 : p.nhalf;
+    const int padc = p.Gs - nout;
+    for (int x = threadIdx.x; x < halves * p.TR * padc * per; x += blockDim.x) {
+      const int c = x % (padc * per);
+      const int rowi = x / (padc * per);
+      out[(((size_t)b * halves * p.TR + rowi) * p.Gs + nout) * per + c] = czero<R2>();
+    }
     for (int h = 0; h < halves; ++h)
-      for (int pr = 0; pr < kPadLo + 1; ++pr) {
-        const int mr = pr < kPadLo ? pr : p.TR - 1;
+      for (int pr = 0; pr < 2 * kPadLo; ++pr) {
+        const int mr = pr < kPadLo ? pr : L + pr;  // rows m < 0 and m >= L
         R2* base = out + (((size_t)b * halves + h) * p.TR + mr) * p.Gs * per;
         for (int x = threadIdx.x; x < p.Gs * per; x += blockDim.x) base[x] = czero<R2>();
       }

@@ -32,11 +32,11 @@ struct Scaling<double> {
   static constexpr double kDown = 0x1p-800;
 };
 
-// Coefficient tables indexed by m are stored with kPadLo zero rows below m = 0
-// and one zero row above m = L - 1 (rows m in [-kPadLo, L]), so that every
-// R-step group of the latitudinal kernel is one fixed-size contiguous copy.
+// Coefficient tables indexed by m are stored with kPadLo zero rows on both
+// sides of 0 <= m < L (row = m + kPadLo), so that every R-step group of the
+// latitudinal kernel is one fixed-size contiguous copy.
 constexpr int kPadLo = 8;
-__host__ __device__ inline int tab_rows(int L) { return L + kPadLo + 1; }
+__host__ __device__ inline int tab_rows(int L) { return L + 2 * kPadLo; }
 __host__ __device__ inline int round4(int x) { return (x + 3) & ~3; }
 
 // One recursed ring (pole rings are handled separately, in closed form).
