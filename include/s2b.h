@@ -108,6 +108,22 @@ int s2b_wigner_inverse(s2b_plan* plan, const void* flmn, void* f, void* workspac
 int s2b_wigner_forward(s2b_plan* plan, const void* f, void* flmn, void* workspace,
                        size_t workspace_bytes, void* stream);
 
+/* Precompute-kernel path (spin plans only). The kernel table has the upstream
+ * layout K [ntheta_k][L][M] with M = 2L-1 (or L when reality), real in the
+ * plan precision (complex for HEALPix, phases folded in); forward tables carry
+ * the quadrature weights and, for mw/mwss, the 2L+1 rings of the MWSS grid at 2L.
+ * s2b_kernel_size     <- s2fft/precompute_transforms/construct.py:16-161 (table size)
+ * s2b_kernel_build    <- construct.py:16-161 (spin_spherical_kernel), built on the device
+ * s2b_precompute_inverse <- s2fft/precompute_transforms/spherical.py:87-149
+ * s2b_precompute_forward <- s2fft/precompute_transforms/spherical.py:314-380
+ * Workspace: s2b_workspace_size(plan, forward, ...). */
+int s2b_kernel_size(const s2b_plan* plan, int forward, size_t* bytes);
+int s2b_kernel_build(s2b_plan* plan, int forward, void* kernel, void* stream);
+int s2b_precompute_inverse(s2b_plan* plan, const void* kernel, const void* flm, void* f,
+                           void* workspace, size_t workspace_bytes, void* stream);
+int s2b_precompute_forward(s2b_plan* plan, const void* kernel, const void* f, void* flm,
+                           void* workspace, size_t workspace_bytes, void* stream);
+
 /* Device status of the plan (synchronous): *status != 0 after a bounded
  * wait inside a kernel ran out (the kernel then skipped its work); returns
  * S2B_ERR_TIMEOUT in that case. No upstream counterpart (upstream exits the

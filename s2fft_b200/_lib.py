@@ -47,6 +47,10 @@ _SIGS = {
     "s2b_wigner_inverse": [ctypes.c_void_p] * 4 + [ctypes.c_size_t, ctypes.c_void_p],
     "s2b_wigner_forward": [ctypes.c_void_p] * 4 + [ctypes.c_size_t, ctypes.c_void_p],
     "s2b_plan_status": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)],
+    "s2b_kernel_size": [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)],
+    "s2b_kernel_build": [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
+    "s2b_precompute_inverse": [ctypes.c_void_p] * 5 + [ctypes.c_size_t, ctypes.c_void_p],
+    "s2b_precompute_forward": [ctypes.c_void_p] * 5 + [ctypes.c_size_t, ctypes.c_void_p],
     "s2b_plan_set_events": [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
     "s2b_fma_probe": [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
 }

@@ -26,6 +26,7 @@
 #include "s2b_internal.h"
 #include "s2b_stages.h"
 #include "s2b_wigner.h"
+#include "s2b_precompute.h"
 
 using namespace s2b;
 using cd = std::complex<double>;
@@ -349,6 +350,11 @@ struct s2b_plan {
   void* chirp = nullptr;
   void* bf = nullptr;
   int row_desc = 0, col_d1 = 0, col_d2 = 0, maxM = 2, M1 = 2, M2 = 2;
+  // precompute path: ring colatitudes of the kernel tables, table width
+  double* kth_inv = nullptr;
+  double* kth_fwd = nullptr;
+  int knth_inv = 0, knth_fwd = 0, kM = 0;
+  size_t ws_pre_fwd = 0;
   // Wigner: one spin transform plan per n, gamma-DFT buffers
   std::vector<s2b_plan*> subs;
   size_t ws_w_fban = 0, ws_w_tmp = 0, ws_w_sub = 0;
@@ -611,6 +617,19 @@ static int build_plan(s2b_plan* p) {
   if ((size_t)p->maxM * 2 * p->rsz > maxsmem || (size_t)(p->M1 + p->M2) * 2 * p->rsz > maxsmem)
     return fail(S2B_ERR_INVALID, "band-limit too large for the shared-memory ring FFT");
 
+  // ---- precompute-kernel geometry (tables include the pole rings)
+  {
+    std::vector<double> thk = thetas(L, d.sampling, d.nside);
+    p->knth_inv = (int)thk.size();
+    if ((rc = upload(p, &p->kth_inv, thk))) return rc;
+    std::vector<double> thf = (d.sampling == S2B_MW || d.sampling == S2B_MWSS)
+                                  ? thetas(2 * L, S2B_MWSS, 0)
+                                  : thk;
+    p->knth_fwd = (int)thf.size();
+    if ((rc = upload(p, &p->kth_fwd, thf))) return rc;
+    p->kM = d.reality ? L : 2 * L - 1;
+  }
+
   // ---- workspace layout
   const size_t c2 = 2 * p->rsz;
   const size_t acc = p->dual ? 2 * c2 : c2;
@@ -624,6 +643,7 @@ static int build_plan(s2b_plan* p) {
   const size_t fel = d.reality ? p->rsz : c2;
   p->ws_iter_f = d.iter > 0 ? B * (size_t)p->npix * fel : 0;
   p->ws_iter_flm = d.iter > 0 ? B * (size_t)L * (2 * L - 1) * c2 : 0;
+  p->ws_pre_fwd = B * (size_t)p->knth_fwd * p->kM * c2;
   S2B_CK(cudaDeviceSynchronize());
   return S2B_OK;
 }
@@ -631,6 +651,9 @@ static int build_plan(s2b_plan* p) {
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 static size_t inv_ws(const s2b_plan* p) { return align256(p->ws_inv_F) + align256(p->ws_inv_ftm); }
+static size_t pre_fwd_ws(const s2b_plan* p) {
+  return align256(p->ws_fwd_cols) + align256(p->ws_pre_fwd);
+}
 static size_t fwd_ws(const s2b_plan* p) {
   size_t once = align256(p->ws_fwd_cols) + align256(p->ws_fwd_G) + align256(p->ws_fwd_acc);
   if (p->d.iter > 0)
@@ -855,6 +878,138 @@ static int run_forward(s2b_plan* p, const void* f, void* flm, char* ws, cudaStre
 }
 
 // ----------------------------------------------------------------------------
+// Precompute-kernel transforms (s2fft/precompute_transforms/spherical.py)
+// ----------------------------------------------------------------------------
+static size_t kernel_bytes(const s2b_plan* p, bool forward) {
+  const int nth = forward ? p->knth_fwd : p->knth_inv;
+  const size_t el = (p->d.sampling == S2B_HEALPIX ? 2 : 1) * p->rsz;
+  return (size_t)nth * p->d.L * p->kM * el;
+}
+
+static int build_kernel(s2b_plan* p, bool forward, void* K, cudaStream_t s) {
+  const s2b_desc& d = p->d;
+  KernelTableParams kp{};
+  kp.L = d.L;
+  kp.spin = d.spin;
+  kp.reality = d.reality;
+  kp.forward = forward;
+  kp.complex_out = d.sampling == S2B_HEALPIX;
+  kp.nth = forward ? p->knth_fwd : p->knth_inv;
+  kp.theta = forward ? p->kth_fwd : p->kth_inv;
+  kp.weights = forward ? p->fwd_weights : nullptr;
+  kp.phi0 = d.sampling == S2B_HEALPIX ? p->hp_phi0 : nullptr;
+  kp.lbin = p->lbin;
+  kp.out = K;
+  S2B_CK(launch_kernel_table(p->fp64, kp, s));
+  return S2B_OK;
+}
+
+template <typename Real>
+static int run_pre_inverse(s2b_plan* p, const void* K, const void* flm, void* f, char* ws,
+                           cudaStream_t s) {
+  const s2b_desc& d = p->d;
+  const int L = d.L;
+  void* ftm = ws;
+  const size_t ftm_bytes = (size_t)d.batch * p->nth * p->inv_ncol * 2 * p->rsz;
+  S2B_CK(cudaMemsetAsync(ftm, 0, ftm_bytes, s));
+  PreContractParams cp{};
+  cp.L = L;
+  cp.nth = p->nth;
+  cp.M = p->kM;
+  cp.batch = d.batch;
+  cp.mshift = d.reality ? L - 1 : 0;
+  cp.mo = p->inv_mo + cp.mshift;
+  cp.ncol = p->inv_ncol;
+  cp.sign = (d.spin & 1) ? -1.0 : 1.0;
+  cp.K = K;
+  cp.in = flm;
+  cp.out = ftm;
+  S2B_CK(launch_pre_contract(p->fp64, false, d.sampling == S2B_HEALPIX, cp, s));
+  RowsParams<Real> rp{};
+  rp.L = L;
+  rp.nrows = p->nth;
+  rp.ncol = p->inv_ncol;
+  rp.mo = p->inv_mo;
+  rp.reality = d.reality;
+  rp.real_out = d.reality;
+  rp.scale = 1.0;
+  rp.desc = d.sampling == S2B_HEALPIX ? p->descs : p->descs + p->row_desc;
+  rp.ring_desc = d.sampling == S2B_HEALPIX ? p->ring_desc : nullptr;
+  rp.ring_off = p->ring_off;
+  rp.out_batch_stride = p->npix;
+  rp.phi0 = nullptr;  // the HEALPix phases are folded into the kernel table
+  rp.tb = tables<Real>(p);
+  rp.in = ftm;
+  rp.out = f;
+  S2B_CK(launch_inv_rows<Real>(rp, p->nth, d.batch, p->maxM, s));
+  return S2B_OK;
+}
+
+template <typename Real>
+static int run_pre_forward(s2b_plan* p, const void* K, const void* f, void* flm, char* ws,
+                           cudaStream_t s) {
+  const s2b_desc& d = p->d;
+  const int L = d.L;
+  char* cols = ws;
+  char* raw = cols + align256(p->ws_fwd_cols);
+  const int m0 = d.reality ? 0 : -(L - 1);
+  RowsParams<Real> rp{};
+  rp.L = L;
+  rp.nrows = p->nth;
+  rp.mo = p->fwd_mode == 2 ? 1 : 0;
+  rp.real_in = d.reality;
+  rp.scale = 1.0;
+  rp.desc = d.sampling == S2B_HEALPIX ? p->descs : p->descs + p->row_desc;
+  rp.ring_desc = d.sampling == S2B_HEALPIX ? p->ring_desc : nullptr;
+  rp.ring_off = p->ring_off;
+  rp.out_batch_stride = p->npix;
+  rp.tb = tables<Real>(p);
+  rp.in = f;
+  rp.M = p->kM;
+  rp.m0 = m0;
+  if (p->fwd_mode == 0) {
+    rp.mode = FWD_TO_RAW;
+    rp.out = raw;
+    S2B_CK(launch_fwd_rows<Real>(rp, p->nth, d.batch, p->maxM, s));
+  } else {
+    rp.mode = FWD_TO_COLS;
+    rp.out = cols;
+    S2B_CK(launch_fwd_rows<Real>(rp, p->nth, d.batch, p->maxM, s));
+    ColsParams<Real> cp{};
+    cp.L = L;
+    cp.spin = d.spin;
+    cp.mw = p->fwd_mode == 1;
+    cp.nin = p->nth;
+    cp.raw = 1;
+    cp.M = p->kM;
+    cp.m0 = m0;
+    cp.scale = p->fwd_mode == 1 ? (2.0 * L) / (2.0 * L - 1.0) : 1.0;
+    cp.d1 = p->descs + p->col_d1;
+    cp.d2 = p->descs + p->col_d2;
+    cp.weights = p->fwd_weights;
+    cp.tb = tables<Real>(p);
+    cp.in = cols;
+    cp.out = raw;
+    const int ncm = p->fwd_mode == 1 ? 2 * L - 1 : 2 * L;
+    S2B_CK(launch_mw_cols<Real>(cp, ncm, d.batch, p->M1, p->M2, s));
+  }
+  S2B_CK(cudaMemsetAsync(flm, 0, (size_t)d.batch * L * (2 * L - 1) * 2 * p->rsz, s));
+  PreContractParams cp{};
+  cp.L = L;
+  cp.nth = p->knth_fwd;
+  cp.M = p->kM;
+  cp.batch = d.batch;
+  cp.mshift = L - 1 + m0;
+  cp.sign = (d.spin & 1) ? -1.0 : 1.0;
+  cp.K = K;
+  cp.in = raw;
+  cp.out = flm;
+  S2B_CK(launch_pre_contract(p->fp64, true, d.sampling == S2B_HEALPIX, cp, s));
+  if (d.reality) S2B_CK(launch_reality_mirror(p->fp64, flm, d.batch, L, s));
+  return S2B_OK;
+}
+
+// ----------------------------------------------------------------------------
 // Wigner (SO(3)) transforms: 2N-1 spin transforms + gamma DFT
 // (s2fft/transforms/wigner.py:110-196, 442-533)
 // ----------------------------------------------------------------------------
@@ -975,7 +1130,7 @@ int s2b_plan_destroy(s2b_plan* p) {
 
 int s2b_workspace_size(const s2b_plan* p, int forward, size_t* bytes) {
   if (!p || !bytes) return fail(S2B_ERR_INVALID, "plan and bytes must be non-NULL");
-  *bytes = p->d.N > 0 ? wigner_ws(p) : (forward ? fwd_ws(p) : inv_ws(p));
+  *bytes = p->d.N > 0 ? wigner_ws(p) : (forward ? std::max(fwd_ws(p), pre_fwd_ws(p)) : inv_ws(p));
   return S2B_OK;
 }
 
@@ -995,10 +1150,49 @@ int s2b_forward(s2b_plan* p, const void* f, void* flm, void* ws, size_t ws_bytes
   int rc;
   if ((rc = check_ptr(flm, "flm")) || (rc = check_ptr(f, "f")) || (rc = check_ptr(ws, "workspace")))
     return rc;
-  if (ws_bytes < fwd_ws(p)) return fail(S2B_ERR_WORKSPACE, "workspace too small");
+  if (ws_bytes < fwd_ws(p)) return fail(S2B_ERR_WORKSPACE, "workspace too small");  // spin path
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   return p->fp64 ? run_forward<double>(p, f, flm, (char*)ws, s)
                  : run_forward<float>(p, f, flm, (char*)ws, s);
+}
+
+int s2b_kernel_size(const s2b_plan* p, int forward, size_t* bytes) {
+  if (!p || !bytes || p->d.N > 0) return fail(S2B_ERR_INVALID, "bad plan or bytes");
+  *bytes = kernel_bytes(p, forward != 0);
+  return S2B_OK;
+}
+
+int s2b_kernel_build(s2b_plan* p, int forward, void* K, void* stream) {
+  if (!p || p->d.N > 0) return fail(S2B_ERR_INVALID, "bad plan");
+  int rc;
+  if ((rc = check_ptr(K, "kernel"))) return rc;
+  return build_kernel(p, forward != 0, K, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int s2b_precompute_inverse(s2b_plan* p, const void* K, const void* flm, void* f, void* ws,
+                           size_t ws_bytes, void* stream) {
+  if (!p || p->d.N > 0) return fail(S2B_ERR_INVALID, "bad plan");
+  int rc;
+  if ((rc = check_ptr(K, "kernel")) || (rc = check_ptr(flm, "flm")) || (rc = check_ptr(f, "f")) ||
+      (rc = check_ptr(ws, "workspace")))
+    return rc;
+  if (ws_bytes < inv_ws(p)) return fail(S2B_ERR_WORKSPACE, "workspace too small");
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  return p->fp64 ? run_pre_inverse<double>(p, K, flm, f, (char*)ws, s)
+                 : run_pre_inverse<float>(p, K, flm, f, (char*)ws, s);
+}
+
+int s2b_precompute_forward(s2b_plan* p, const void* K, const void* f, void* flm, void* ws,
+                           size_t ws_bytes, void* stream) {
+  if (!p || p->d.N > 0) return fail(S2B_ERR_INVALID, "bad plan");
+  int rc;
+  if ((rc = check_ptr(K, "kernel")) || (rc = check_ptr(flm, "flm")) || (rc = check_ptr(f, "f")) ||
+      (rc = check_ptr(ws, "workspace")))
+    return rc;
+  if (ws_bytes < pre_fwd_ws(p)) return fail(S2B_ERR_WORKSPACE, "workspace too small");
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  return p->fp64 ? run_pre_forward<double>(p, K, f, flm, (char*)ws, s)
+                 : run_pre_forward<float>(p, K, f, flm, (char*)ws, s);
 }
 
 int s2b_wigner_inverse(s2b_plan* p, const void* flmn, void* f, void* ws, size_t ws_bytes,

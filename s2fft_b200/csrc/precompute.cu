@@ -1,0 +1,289 @@
+// Precompute-kernel path: build the Wigner-d kernel table on the device and
+// contract it against ring spectra.
+//
+// Table (the upstream layout, s2fft/precompute_transforms/construct.py:16-161):
+//   K[t][l][mi] = d^l_{m,-s}(theta_t) sqrt((2l+1)/4pi) [x w_t if forward]
+//                 [x exp(-+i m phi0_t) for HEALPix], m = m0 + mi,
+// m0 = 0 when reality (spin 0) else -(L-1). Real for equiangular samplings,
+// complex (interleaved) for HEALPix.
+//
+// Construction: one thread per (ring, l) runs the three-term recursion in m in
+// double (from the edge m = +-l inwards, both halves, spin n = -s and the
+// d^l_{-m,n} = (-1)^(m-n) d^l_{m,-n} symmetry), with a scaled exponent so the
+// polar seeds do not underflow; rows of K are written contiguously in m.
+// Pole rings use the closed forms d^l_{m,n}(0) = delta_{m,n},
+// d^l_{m,n}(pi) = (-1)^(l-n) delta_{m,-n}.
+//
+// Contractions (s2fft/precompute_transforms/spherical.py:87-149, 314-380):
+//   inverse: ftm[b][t][m] = (-1)^s sum_l K[t][l][m] flm[b][l][m]
+//   forward: flm[b][l][m] = (-1)^s sum_t K[t][l][m] ftm[b][t][m]
+// streamed so that every K element is read from HBM once per group of maps.
+#include <cuda_runtime.h>
+
+#include <type_traits>
+
+#include "s2b_precompute.h"
+
+namespace s2b {
+
+template <typename Real>
+using P2 = std::conditional_t<sizeof(Real) == 4, float2, double2>;
+
+static int pgrid(long n, int threads) {
+  long b = (n + threads - 1) / threads;
+  if (b > 1048576) b = 1048576;
+  return b < 1 ? 1 : (int)b;
+}
+
+// ---------------------------------------------------------------------------
+// table construction
+// ---------------------------------------------------------------------------
+template <typename Real>
+__global__ void kernel_table_kernel(KernelTableParams p) {
+  const long total = (long)p.nth * p.L;
+  const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (idx >= total) return;
+  const int t = (int)(idx / p.L);
+  const int l = (int)(idx % p.L);
+  const int L = p.L;
+  const int s = p.spin;
+  const int as = s < 0 ? -s : s;
+  const double th = p.theta[t];
+  const double nl = sqrt((2.0 * l + 1.0) / (4.0 * 3.141592653589793));
+  const double w = p.weights ? p.weights[t] : 1.0;
+  const int m0 = p.reality ? 0 : -(L - 1);
+  const int M = L - m0;
+  Real* rowr = nullptr;
+  P2<Real>* rowc = nullptr;
+  if (p.complex_out)
+    rowc = reinterpret_cast<P2<Real>*>(p.out) + ((size_t)t * L + l) * M;
+  else
+    rowr = reinterpret_cast<Real*>(p.out) + ((size_t)t * L + l) * M;
+  auto store = [&](int m, double d) {
+    const int mi = m - m0;
+    if (mi < 0 || mi >= M) return;
+    const double v = d * nl * w;
+    if (p.complex_out) {
+      double sn = 0.0, cs = 1.0;
+      if (p.phi0) sincos((p.forward ? -1.0 : 1.0) * (double)m * p.phi0[t], &sn, &cs);
+      P2<Real> o;
+      o.x = (Real)(v * cs);
+      o.y = (Real)(v * sn);
+      rowc[mi] = o;
+    } else {
+      rowr[mi] = (Real)v;
+    }
+  };
+  // zero the row first (entries with |m| > l, l < |s| stay zero)
+  for (int mi = 0; mi < M; ++mi) {
+    if (p.complex_out) {
+      P2<Real> z;
+      z.x = 0;
+      z.y = 0;
+      rowc[mi] = z;
+    } else {
+      rowr[mi] = Real(0);
+    }
+  }
+  if (l < as) return;
+  const bool north = th < 1e-12, south = th > 3.141592653589793 - 1e-12;
+  if (north) {  // d^l_{m,-s}(0) = delta_{m,-s}
+    store(-s, 1.0);
+    return;
+  }
+  if (south) {  // d^l_{m,-s}(pi) = (-1)^(l+s) delta_{m,s}
+    store(s, ((l + s) & 1) ? -1.0 : 1.0);
+    return;
+  }
+  const double c = cos(th), sn = sin(th);
+  const double lc = log2(cos(th / 2.0)), ls = log2(sin(th / 2.0));
+  const double lb = p.lbin[l];
+  constexpr double kS = 800.0, kTh = 0x1p400, kDn = 0x1p-800, kSig = -200.0;
+  for (int half = 0; half < 2; ++half) {
+    if (p.reality && half == 1) break;
+    const int n = half == 0 ? -s : s;  // recursion for d^l_{m,n}, m from l down
+    // seed d^l_{l,n}
+    const double lg = lb + (double)(l + n) * lc + (double)(l - n) * ls;
+    int e = 0;
+    if (lg < kSig) e = -(int)ceil((kSig - lg) / kS);
+    double v = ((((l - n) & 1) ? -1.0 : 1.0)) * exp2(lg - kS * (double)e);
+    double wv = 0.0;  // d_{m+1}
+    const int mlast = half == 0 ? 0 : 1;
+    for (int m = l; m >= mlast; --m) {
+      const double val = e == 0 ? v : 0.0;
+      if (half == 0)
+        store(m, val);
+      else  // d^l_{-m,-s} = (-1)^(m+s) d^l_{m,s}
+        store(-m, (((m + s) % 2 + 2) % 2 ? -1.0 : 1.0) * val);
+      if (m == mlast) break;
+      // d_{m-1} = (lambda d_m - f_{m+1} d_{m+1}) / f_m
+      const double lam = 2.0 * ((double)n - (double)m * c) / sn;
+      const double fm = sqrt((double)(l + m) * (double)(l - m + 1));
+      const double fp = sqrt((double)(l + m + 1) * (double)(l - m));
+      const double nv = (lam * v - fp * wv) / fm;
+      wv = v;
+      v = nv;
+      if (fabs(v) > kTh && e < 0) {
+        v *= kDn;
+        wv *= kDn;
+        e += 1;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// streaming contractions; threads run along mi (contiguous in K and in the data)
+// ---------------------------------------------------------------------------
+// inverse: out ftm [b][t][mo + mi] (ncol columns) = sgn * sum_l K[t][l][mi] flm[b][l][m0 + L-1 + mi]
+template <typename Real, bool CPLX>
+__global__ void pre_inverse_kernel(PreContractParams p) {
+  using C = P2<Real>;
+  constexpr int BB = 8;  // maps per pass
+  const int M = p.M;
+  const int mi = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t = blockIdx.y;
+  const int b0 = blockIdx.z * BB;
+  if (mi >= M) return;
+  const int L = p.L;
+  const int col = p.mshift + mi;  // flm column L-1+m
+  double ar[BB], ai[BB];
+#pragma unroll
+  for (int x = 0; x < BB; ++x) ar[x] = ai[x] = 0.0;
+  const C* flm = reinterpret_cast<const C*>(p.in);
+  for (int l = 0; l < L; ++l) {
+    double kr, ki = 0.0;
+    if (CPLX) {
+      const C k = reinterpret_cast<const C*>(p.K)[((size_t)t * L + l) * M + mi];
+      kr = k.x;
+      ki = k.y;
+    } else {
+      kr = reinterpret_cast<const Real*>(p.K)[((size_t)t * L + l) * M + mi];
+    }
+#pragma unroll
+    for (int x = 0; x < BB; ++x) {
+      if (b0 + x >= p.batch) break;
+      const C f = flm[((size_t)(b0 + x) * L + l) * (2 * L - 1) + col];
+      ar[x] += kr * f.x - ki * f.y;
+      ai[x] += kr * f.y + ki * f.x;
+    }
+  }
+  C* out = reinterpret_cast<C*>(p.out);
+#pragma unroll
+  for (int x = 0; x < BB; ++x) {
+    if (b0 + x >= p.batch) break;
+    C o;
+    o.x = (Real)(p.sign * ar[x]);
+    o.y = (Real)(p.sign * ai[x]);
+    out[((size_t)(b0 + x) * p.nth + t) * p.ncol + p.mo + mi] = o;
+  }
+}
+
+// forward: out flm [b][l][L-1+m] = sgn * sum_t K[t][l][mi] ftm[b][t][mi] (ftm row width M)
+template <typename Real, bool CPLX>
+__global__ void pre_forward_kernel(PreContractParams p) {
+  using C = P2<Real>;
+  constexpr int BB = 8;
+  const int M = p.M;
+  const int mi = blockIdx.x * blockDim.x + threadIdx.x;
+  const int l = blockIdx.y;
+  const int b0 = blockIdx.z * BB;
+  if (mi >= M) return;
+  const int L = p.L;
+  double ar[BB], ai[BB];
+#pragma unroll
+  for (int x = 0; x < BB; ++x) ar[x] = ai[x] = 0.0;
+  const C* ftm = reinterpret_cast<const C*>(p.in);
+  for (int t = 0; t < p.nth; ++t) {
+    double kr, ki = 0.0;
+    if (CPLX) {
+      const C k = reinterpret_cast<const C*>(p.K)[((size_t)t * L + l) * M + mi];
+      kr = k.x;
+      ki = k.y;
+    } else {
+      kr = reinterpret_cast<const Real*>(p.K)[((size_t)t * L + l) * M + mi];
+    }
+#pragma unroll
+    for (int x = 0; x < BB; ++x) {
+      if (b0 + x >= p.batch) break;
+      const C f = ftm[((size_t)(b0 + x) * p.nth + t) * M + mi];
+      ar[x] += kr * f.x - ki * f.y;
+      ai[x] += kr * f.y + ki * f.x;
+    }
+  }
+  C* out = reinterpret_cast<C*>(p.out);
+#pragma unroll
+  for (int x = 0; x < BB; ++x) {
+    if (b0 + x >= p.batch) break;
+    C o;
+    o.x = (Real)(p.sign * ar[x]);
+    o.y = (Real)(p.sign * ai[x]);
+    out[((size_t)(b0 + x) * L + l) * (2 * L - 1) + p.mshift + mi] = o;
+  }
+}
+
+// reality mirror flm[b][l][L-1-m] = (-1)^m conj(flm[b][l][L-1+m]), m >= 1
+template <typename Real>
+__global__ void reality_mirror_kernel(void* flm, int B, int L) {
+  using C = P2<Real>;
+  const long total = (long)B * L * (L - 1);
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
+       i += (long)gridDim.x * blockDim.x) {
+    const int m = 1 + (int)(i % (L - 1));
+    const long bl = i / (L - 1);
+    C* row = reinterpret_cast<C*>(flm) + bl * (2 * L - 1);
+    C v = row[L - 1 + m];
+    const Real sg = (m & 1) ? Real(-1) : Real(1);
+    C o;
+    o.x = sg * v.x;
+    o.y = -sg * v.y;
+    row[L - 1 - m] = o;
+  }
+}
+
+cudaError_t launch_kernel_table(bool fp64, const KernelTableParams& p, cudaStream_t s) {
+  const long total = (long)p.nth * p.L;
+  if (fp64)
+    kernel_table_kernel<double><<<pgrid(total, 128), 128, 0, s>>>(p);
+  else
+    kernel_table_kernel<float><<<pgrid(total, 128), 128, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pre_contract(bool fp64, bool forward, bool cplx, const PreContractParams& p,
+                                cudaStream_t s) {
+  const int threads = 128;
+  dim3 grid((p.M + threads - 1) / threads, forward ? p.L : p.nth, (p.batch + 7) / 8);
+#define S2B_LAUNCH(R, C)                                                   \
+  if (forward)                                                             \
+    pre_forward_kernel<R, C><<<grid, threads, 0, s>>>(p);                  \
+  else                                                                     \
+    pre_inverse_kernel<R, C><<<grid, threads, 0, s>>>(p);
+  if (fp64) {
+    if (cplx) {
+      S2B_LAUNCH(double, true)
+    } else {
+      S2B_LAUNCH(double, false)
+    }
+  } else {
+    if (cplx) {
+      S2B_LAUNCH(float, true)
+    } else {
+      S2B_LAUNCH(float, false)
+    }
+  }
+#undef S2B_LAUNCH
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reality_mirror(bool fp64, void* flm, int B, int L, cudaStream_t s) {
+  if (L < 2) return cudaSuccess;
+  const long total = (long)B * L * (L - 1);
+  if (fp64)
+    reality_mirror_kernel<double><<<pgrid(total, 256) > 65535 ? 65535 : pgrid(total, 256), 256, 0, s>>>(flm, B, L);
+  else
+    reality_mirror_kernel<float><<<pgrid(total, 256) > 65535 ? 65535 : pgrid(total, 256), 256, 0, s>>>(flm, B, L);
+  return cudaGetLastError();
+}
+
+}  // namespace s2b

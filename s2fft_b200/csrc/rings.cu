@@ -316,6 +316,15 @@ __global__ void fwd_rows_kernel(RowsParams<Real> p) {
   dft_run<Real>(s, d, p.tb, false, load);
   const double w = p.weights ? p.weights[t] : 1.0;
   const double phi0 = p.phi0 ? p.phi0[t] : 0.0;
+  if (p.mode == FWD_TO_RAW) {
+    R2* out = reinterpret_cast<R2*>(p.out);
+    for (int mi = threadIdx.x; mi < p.M; mi += blockDim.x) {
+      const int m = p.m0 + mi;
+      R2 x = dft_get<Real>(s, d, p.tb, false, pmod(m, n));
+      out[((size_t)b * p.nrows + t) * p.M + mi] = cscale(x, (Real)p.scale);
+    }
+    return;
+  }
   if (p.mode == FWD_TO_COLS) {
     // Fc[b][m + mshift][t] = scale * X_m for m in [mlo, L-1]
     R2* out = reinterpret_cast<R2*>(p.out);
@@ -411,6 +420,16 @@ __global__ void mw_cols_kernel(ColsParams<Real> p) {
   const int nout = 2 * L + 1;
   const int am = m < 0 ? -m : m;
   R2* out = reinterpret_cast<R2*>(p.out);
+  if (p.raw) {
+    if (m < p.m0) return;
+    for (int t = threadIdx.x; t < nout; t += blockDim.x) {
+      R2 u = dft_get<Real>(s2, d2, p.tb, true, t);
+      u.x = (Real)((double)u.x * p.scale);
+      u.y = (Real)((double)u.y * p.scale);
+      out[((size_t)b * nout + t) * p.M + (m - p.m0)] = u;
+    }
+    return;
+  }
   for (int t = threadIdx.x; t < nout; t += blockDim.x) {
     R2 u = dft_get<Real>(s2, d2, p.tb, true, t);
     const double f = p.scale * p.weights[t];

@@ -27,7 +27,7 @@ struct FFTTables {
   const R2* bfilt;
 };
 
-enum RowsMode { FWD_TO_SPECTRA = 0, FWD_TO_COLS = 1 };
+enum RowsMode { FWD_TO_SPECTRA = 0, FWD_TO_COLS = 1, FWD_TO_RAW = 2 };
 
 template <typename Real>
 struct RowsParams {
@@ -41,6 +41,7 @@ struct RowsParams {
   int dual, nhalf;      // forward spectra layout
   int TR, Gs;           // forward spectra: table rows (m + kPadLo) and row stride
   int mode;             // RowsMode
+  int M, m0;            // FWD_TO_RAW: out [B][nrows][M] holds X_m for m = m0 .. m0+M-1
   double scale;
   const FFTDesc* desc;  // transform descriptors
   const int* ring_desc; // per ring index into desc (nullptr: desc[0] for all)
@@ -60,6 +61,7 @@ struct ColsParams {
   int nin;              // rings of the input columns
   int dual, nhalf;
   int TR, Gs;           // spectra table rows and row stride
+  int raw, M, m0;       // raw = 1: out [B][2L+1][M] unweighted, m = m0 .. m0+M-1
   double scale;         // overall factor of the chain
   const FFTDesc* d1;    // theta DFT over the periodic extension (2L-1 or 2L)
   const FFTDesc* d2;    // inverse DFT of length 4L

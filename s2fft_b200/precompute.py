@@ -1,0 +1,131 @@
+"""Drop-in precompute-kernel transforms on one B200.
+
+Mirrors upstream ``s2fft.precompute_transforms.spherical.inverse`` / ``forward``
+(s2fft/precompute_transforms/spherical.py:19-84, 226-311) and
+``construct.spin_spherical_kernel`` (construct.py:16-161). The kernel table
+K[t, l, m] has the upstream layout and meaning; here it is built on the device
+and returned as a torch tensor (an upstream numpy kernel is accepted too).
+"""
+
+from __future__ import annotations
+
+import ctypes
+from warnings import warn
+
+import numpy as np
+import torch
+
+from . import _lib
+from .spherical import _check_method, _device, _dtypes, _ret, _to_device, f_shape
+
+
+def _plan(dev, L, spin, nside, s, reality, precision, B):
+    return _lib.get_plan(dev, L=L, spin=spin, nside=nside or 0, sampling=_lib.SAMPLING[s],
+                         reality=int(bool(reality)), L_lower=0,
+                         precision=_lib.PRECISION[precision], batch=B, iter=0, N=0)
+
+
+def _kernel_shape(L, s, nside, reality, forward):
+    M = L if reality else 2 * L - 1
+    if forward and s in ("mw", "mwss"):
+        nth = 2 * L + 1
+    else:
+        nth = f_shape(L, s, nside)[0] if s != "healpix" else 4 * nside - 1
+    return nth, L, M
+
+
+def _reality(reality, spin):
+    if reality and spin != 0:
+        warn("Reality acceleration only supports spin 0 fields. Defering to complex transform.",
+             stacklevel=3)
+        return False
+    return reality
+
+
+def spin_spherical_kernel(L: int, spin: int = 0, reality: bool = False, sampling: str = "mw",
+                          nside: int = None, forward: bool = True, recursion: str = "auto",
+                          precision: str = "f64"):
+    """Kernel K[t, l, m] built on the device (torch tensor on the current CUDA device)."""
+    s = sampling.lower()
+    reality = _reality(reality, spin)
+    _, rdt = _dtypes(precision)
+    cdt = _dtypes(precision)[0]
+    dev = _device()
+    plan = _plan(dev, L, spin, nside, s, reality, precision, 1)
+    shape = _kernel_shape(L, s, nside, reality, forward)
+    K = torch.empty(shape, dtype=cdt if s == "healpix" else rdt, device=dev)
+    n = ctypes.c_size_t()
+    _lib.check(_lib.lib().s2b_kernel_size(plan.ptr, int(forward), ctypes.byref(n)))
+    assert n.value == K.numel() * K.element_size()
+    _lib.check(_lib.lib().s2b_kernel_build(plan.ptr, int(forward), K.data_ptr(),
+                                           _lib.stream_handle(dev)))
+    return K
+
+
+def _kernel_tensor(kernel, L, s, nside, reality, forward, precision, spin, dev):
+    cdt, rdt = _dtypes(precision)
+    if kernel is None:
+        return spin_spherical_kernel(L, spin, reality, s, nside, forward, precision=precision)
+    want = cdt if s == "healpix" else rdt
+    if isinstance(kernel, np.ndarray):
+        kernel = torch.from_numpy(np.ascontiguousarray(kernel))
+    return kernel.to(device=dev, dtype=want).contiguous()
+
+
+def inverse(flm, L: int, spin: int = 0, kernel=None, sampling: str = "mw",
+            reality: bool = False, method: str = "cuda", nside: int = None,
+            precision: str = "f64"):
+    """Inverse spin SHT through a precomputed kernel (upstream spherical.py:19-84)."""
+    _check_method(method)
+    s = sampling.lower()
+    reality = _reality(reality, spin)
+    cdt, rdt = _dtypes(precision)
+    x, was_np, odev = _to_device(flm, cdt, _device())
+    bs = tuple(x.shape[:-2])
+    B = int(np.prod(bs)) if bs else 1
+    K = _kernel_tensor(kernel, L, s, nside, reality, False, precision, spin, x.device)
+    plan = _plan(x.device, L, spin, nside, s, reality, precision, B)
+    out = torch.empty(bs + f_shape(L, s, nside), dtype=rdt if reality else cdt, device=x.device)
+    ws = plan.workspace(False)
+    _lib.check(_lib.lib().s2b_precompute_inverse(plan.ptr, K.data_ptr(), x.data_ptr(),
+                                                 out.data_ptr(), ws.data_ptr(), ws.numel(),
+                                                 _lib.stream_handle(x.device)))
+    return _ret(out, was_np, odev)
+
+
+def _forward_once(x, K, L, spin, s, nside, reality, precision):
+    cdt, _ = _dtypes(precision)
+    nd = len(f_shape(L, s, nside))
+    bs = tuple(x.shape[:-nd])
+    B = int(np.prod(bs)) if bs else 1
+    plan = _plan(x.device, L, spin, nside, s, reality, precision, B)
+    out = torch.empty(bs + (L, 2 * L - 1), dtype=cdt, device=x.device)
+    ws = plan.workspace(True)
+    _lib.check(_lib.lib().s2b_precompute_forward(plan.ptr, K.data_ptr(), x.data_ptr(),
+                                                 out.data_ptr(), ws.data_ptr(), ws.numel(),
+                                                 _lib.stream_handle(x.device)))
+    return out
+
+
+def forward(f, L: int, spin: int = 0, kernel=None, sampling: str = "mw",
+            reality: bool = False, method: str = "cuda", nside: int = None, iter: int = 0,
+            precision: str = "f64"):
+    """Forward spin SHT through a precomputed kernel (upstream spherical.py:226-311)."""
+    _check_method(method)
+    s = sampling.lower()
+    reality = _reality(reality, spin)
+    cdt, rdt = _dtypes(precision)
+    if reality:
+        if isinstance(f, torch.Tensor) and f.is_complex():
+            f = f.real
+        elif isinstance(f, np.ndarray) and np.iscomplexobj(f):
+            f = np.real(f)
+    x, was_np, odev = _to_device(f, rdt if reality else cdt, _device())
+    K = _kernel_tensor(kernel, L, s, nside, reality, True, precision, spin, x.device)
+    flm = _forward_once(x, K, L, spin, s, nside, reality, precision)
+    if iter:
+        Ki = spin_spherical_kernel(L, spin, reality, s, nside, False, precision=precision)
+        for _ in range(iter):
+            fr = inverse(flm, L, spin, Ki, s, reality, method, nside, precision)
+            flm = flm + _forward_once(x - fr, K, L, spin, s, nside, reality, precision)
+    return _ret(flm, was_np, odev)

@@ -146,3 +146,44 @@ def test_device_status_clean(s2b):
 
     for key, plan in list(_lib._plans.items()):
         assert plan.status() == 0
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_golden_precompute(s2b, golden, precision):
+    import torch
+
+    data, index = golden
+    tol = TOL64 if precision == "f64" else TOL32
+    for c in [c for c in index["cases"] if c["kind"] == "precompute"]:
+        n = c["name"]
+        L, sp, ns, smp = c["L"], c["spin"], c["nside"], c["sampling"]
+        kin = s2b.precompute.spin_spherical_kernel(L, sp, False, smp, ns, False,
+                                                   precision=precision)
+        kfw = s2b.precompute.spin_spherical_kernel(L, sp, False, smp, ns, True,
+                                                   precision=precision)
+        assert relerr(kin.cpu().numpy(), data[f"{n}/kernel_inv"]) < tol, (n, "kin")
+        assert relerr(kfw.cpu().numpy(), data[f"{n}/kernel_fwd"]) < tol, (n, "kfw")
+        f = s2b.precompute.inverse(data[f"{n}/flm"], L, sp, kin, smp, False, nside=ns,
+                                   precision=precision)
+        assert relerr(f, data[f"{n}/f"]) < tol, (n, relerr(f, data[f"{n}/f"]))
+        g = s2b.precompute.forward(data[f"{n}/f"], L, sp, kfw, smp, False, nside=ns,
+                                   precision=precision)
+        assert relerr(g, data[f"{n}/flm_fwd"]) < tol, (n, relerr(g, data[f"{n}/flm_fwd"]))
+        # the upstream numpy kernel is accepted as well
+        g2 = s2b.precompute.forward(data[f"{n}/f"], L, sp, data[f"{n}/kernel_fwd"], smp, False,
+                                    nside=ns, precision=precision)
+        assert relerr(g2, data[f"{n}/flm_fwd"]) < tol
+        torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("sampling", ["mw", "gl", "healpix"])
+def test_precompute_reality_batch(s2b, rng, sampling):
+    L, nside = (16, 8) if sampling == "healpix" else (24, None)
+    flms = np.stack([oracle.signal.generate_flm(rng, L, 0, 0, True) for _ in range(3)])
+    ref = np.stack([np.real(oracle.spherical.inverse(x, L, 0, nside, sampling, True))
+                    for x in flms])
+    f = s2b.precompute.inverse(flms, L, 0, None, sampling, True, nside=nside)
+    assert relerr(f, ref) < TOL64
+    if sampling != "healpix":
+        g = s2b.precompute.forward(ref, L, 0, None, sampling, True, nside=nside)
+        assert relerr(g, flms) < TOL64
