@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libs2b.so")
 
 SAMPLING = {"mw": 0, "mwss": 1, "dh": 2, "gl": 3, "healpix": 4}
-PRECISION = {"f64": 0, "f32": 1}
+PRECISION = {"f64": 0, "f32": 1, "bf16x3": 2}
 
 S2B_OK = 0
 STATUS = {1: "invalid argument", 2: "CUDA error", 3: "workspace too small",

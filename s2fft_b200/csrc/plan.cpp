@@ -27,6 +27,7 @@
 #include "s2b_stages.h"
 #include "s2b_wigner.h"
 #include "s2b_precompute.h"
+#include "s2b_tc.h"
 
 using namespace s2b;
 using cd = std::complex<double>;
@@ -46,6 +47,8 @@ static int fail(int code, const std::string& msg) {
   } while (0)
 
 static const double kPi = 3.14159265358979323846;
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 // ----------------------------------------------------------------------------
 // sampling geometry and quadrature (double)
@@ -314,6 +317,7 @@ struct DevBuf {
 struct s2b_plan {
   s2b_desc d;
   bool fp64;
+  bool tc;      // S2B_BF16X3: tensor-core precompute forward
   size_t rsz;   // sizeof(Real)
   int nth;      // rings of the sampling
   int nphi;     // equiangular ring length
@@ -414,6 +418,7 @@ static int build_plan(s2b_plan* p) {
   const s2b_desc& d = p->d;
   const int L = d.L;
   p->fp64 = d.precision == S2B_F64;
+  p->tc = d.precision == S2B_BF16X3;
   p->rsz = p->fp64 ? 8 : 4;
   p->nth = ntheta(L, d.sampling, d.nside);
   p->nphi = d.sampling == S2B_HEALPIX ? 0 : nphi_equiang(L, d.sampling);
@@ -644,11 +649,11 @@ static int build_plan(s2b_plan* p) {
   p->ws_iter_f = d.iter > 0 ? B * (size_t)p->npix * fel : 0;
   p->ws_iter_flm = d.iter > 0 ? B * (size_t)L * (2 * L - 1) * c2 : 0;
   p->ws_pre_fwd = B * (size_t)p->knth_fwd * p->kM * c2;
+  if (p->tc) p->ws_pre_fwd = align256(p->ws_pre_fwd) + tc_packed_b_bytes(p->knth_fwd, d.batch, p->kM);
   S2B_CK(cudaDeviceSynchronize());
   return S2B_OK;
 }
 
-static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 static size_t inv_ws(const s2b_plan* p) { return align256(p->ws_inv_F) + align256(p->ws_inv_ftm); }
 static size_t pre_fwd_ws(const s2b_plan* p) {
@@ -882,6 +887,7 @@ static int run_forward(s2b_plan* p, const void* f, void* flm, char* ws, cudaStre
 // ----------------------------------------------------------------------------
 static size_t kernel_bytes(const s2b_plan* p, bool forward) {
   const int nth = forward ? p->knth_fwd : p->knth_inv;
+  if (p->tc && forward) return tc_packed_a_bytes(nth, p->d.L, p->kM);
   const size_t el = (p->d.sampling == S2B_HEALPIX ? 2 : 1) * p->rsz;
   return (size_t)nth * p->d.L * p->kM * el;
 }
@@ -900,6 +906,19 @@ static int build_kernel(s2b_plan* p, bool forward, void* K, cudaStream_t s) {
   kp.phi0 = d.sampling == S2B_HEALPIX ? p->hp_phi0 : nullptr;
   kp.lbin = p->lbin;
   kp.out = K;
+  if (p->tc && forward) {
+    // float table in a temporary buffer, then split into bf16 hi/lo and packed for the MMA
+    const size_t tb = (size_t)kp.nth * d.L * p->kM * sizeof(float);
+    void* tmp = nullptr;
+    S2B_CK(cudaMalloc(&tmp, tb));
+    kp.out = tmp;
+    cudaError_t e = launch_kernel_table(false, kp, s);
+    if (e == cudaSuccess) e = launch_tc_pack_a((const float*)tmp, kp.nth, d.L, p->kM, K, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(tmp);
+    S2B_CK(e);
+    return S2B_OK;
+  }
   S2B_CK(launch_kernel_table(p->fp64, kp, s));
   return S2B_OK;
 }
@@ -994,6 +1013,26 @@ static int run_pre_forward(s2b_plan* p, const void* K, const void* f, void* flm,
     S2B_CK(launch_mw_cols<Real>(cp, ncm, d.batch, p->M1, p->M2, s));
   }
   S2B_CK(cudaMemsetAsync(flm, 0, (size_t)d.batch * L * (2 * L - 1) * 2 * p->rsz, s));
+  if (p->tc) {
+    char* bp = raw + align256((size_t)d.batch * p->knth_fwd * p->kM * 2 * p->rsz);
+    S2B_CK(launch_tc_pack_b(raw, d.batch, p->knth_fwd, p->kM, bp, s));
+    TcParams tp{};
+    tp.L = L;
+    tp.nth = p->knth_fwd;
+    tp.M = p->kM;
+    tp.B = d.batch;
+    tp.mshift = L - 1 + m0;
+    tp.sign = (d.spin & 1) ? -1.f : 1.f;
+    tp.Ap = reinterpret_cast<const __nv_bfloat16*>(K);
+    tp.Bp = reinterpret_cast<const __nv_bfloat16*>(bp);
+    tp.out = reinterpret_cast<float2*>(flm);
+    tp.status = p->status;
+    if (p->ev_begin[1]) S2B_CK(cudaEventRecord(p->ev_begin[1], s));
+    S2B_CK(launch_tc_forward(tp, s));
+    if (p->ev_end[1]) S2B_CK(cudaEventRecord(p->ev_end[1], s));
+    if (d.reality) S2B_CK(launch_reality_mirror(false, flm, d.batch, L, s));
+    return S2B_OK;
+  }
   PreContractParams cp{};
   cp.L = L;
   cp.nth = p->knth_fwd;
@@ -1097,8 +1136,10 @@ int s2b_plan_create(const s2b_desc* desc, s2b_plan** out) {
     if (d.nside < 1) return fail(S2B_ERR_INVALID, "healpix sampling needs nside >= 1");
     if (d.L < 2 * d.nside) return fail(S2B_ERR_INVALID, "healpix requires L >= 2*nside");
   }
-  if (d.precision != S2B_F64 && d.precision != S2B_F32)
+  if (d.precision != S2B_F64 && d.precision != S2B_F32 && d.precision != S2B_BF16X3)
     return fail(S2B_ERR_INVALID, "unknown precision");
+  if (d.precision == S2B_BF16X3 && (d.sampling == S2B_HEALPIX || d.N > 0))
+    return fail(S2B_ERR_INVALID, "BF16x3 plans support the equiangular precompute path");
   if (d.reality && d.spin != 0) return fail(S2B_ERR_INVALID, "reality requires spin 0");
   if (std::abs(d.spin) >= d.L) return fail(S2B_ERR_INVALID, "|spin| must be < L");
   if (d.L_lower < 0 || d.L_lower >= d.L) return fail(S2B_ERR_INVALID, "0 <= L_lower < L");

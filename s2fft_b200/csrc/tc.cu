@@ -1,0 +1,334 @@
+// Batched precompute-kernel forward contraction on the 5th-generation tensor
+// cores (tcgen05), with 3-term BF16 split operands and FP32 accumulation.
+//
+// For every m column the forward precompute transform is a dense product
+//   flm[b][l][m] = (-1)^s sum_t K[t][l][m] ftm[b][t][m]
+// (s2fft/precompute_transforms/spherical.py:314-380, einsum "tlm,tm->lm"),
+// which over a batch of maps is a GEMM D[l][n] = sum_t A[l][t] B[n][t] with
+// n = 2 b + {re, im}. Each operand x is split as x = hi + lo (both bf16) and
+//   D ~= A_hi B_hi + A_hi B_lo + A_lo B_hi,
+// accumulated in FP32 in tensor memory.
+//
+// Operands are packed once into the no-swizzle K-major core-matrix layout the
+// MMA reads directly (8 rows x 16 bytes per core matrix; tile [r/8][k/8][r%8][k%8]),
+// so every pipeline stage is four contiguous 1-D bulk copies (TMA engine, no
+// multicast). CTA = 4 consecutive m columns x 128 l rows; 4 accumulators of
+// 128 x 128 FP32 occupy the 512 TMEM columns. One thread produces and issues;
+// all waits are bounded and TMEM is always released.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "s2b_tc.h"
+
+namespace s2b {
+
+namespace {
+
+constexpr int kTileR = 128;              // rows of a tile (l for A, n for B)
+constexpr int kTileK = 64;               // K (t) per stage
+constexpr int kBlk = kTileR * kTileK;    // elements per operand block
+constexpr int kBlkBytes = kBlk * 2;      // 16 KB (bf16)
+constexpr int kStageBytes = 4 * kBlkBytes;  // A_hi, A_lo, B_hi, B_lo
+constexpr int kStages = 3;
+constexpr int kMPerCta = 4;
+constexpr unsigned kTmemCols = 512;
+
+__device__ __forceinline__ uint32_t su32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// byte offset of element (r, k) inside a packed block
+__host__ __device__ __forceinline__ int core_off(int r, int k) {
+  return (((r >> 3) * (kTileK / 8) + (k >> 3)) * 64 + (r & 7) * 8 + (k & 7)) * 2;
+}
+
+__device__ __forceinline__ void mb_init(uint64_t* mb, unsigned c) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(mb)), "r"(c) : "memory");
+}
+__device__ __forceinline__ void mb_expect(uint64_t* mb, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(mb)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mb_wait(uint64_t* mb, unsigned parity) {
+  for (int it = 0; it < (1 << 22); ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(su32(mb)), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, unsigned bytes, uint64_t* mb) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          su32(dst)),
+      "l"(src), "r"(bytes), "r"(su32(mb))
+      : "memory");
+}
+
+// shared-memory matrix descriptor: no swizzle, K-major, LBO = 128 B (next 8 k),
+// SBO = 1024 B (next 8 rows), Blackwell descriptor version 1
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+  d |= (uint64_t)((128u >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((1024u >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46;
+  return d;
+}
+
+// instruction descriptor: D f32, A/B bf16, both K-major, N = 128, M = 128
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((128u >> 3) << 17) |
+                            ((128u >> 4) << 24);
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+      "l"(a), "l"(b), "r"(kIdesc), "r"(acc)
+      : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint64_t* mb) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   su32(mb))
+               : "memory");
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// packing: K[t][l][mi] (float) -> Ap[mi][lt][tc][hi/lo][block]
+// ---------------------------------------------------------------------------
+__global__ void pack_kernel_a(const float* __restrict__ K, int nth, int L, int M, int nlt, int ntc,
+                              __nv_bfloat16* __restrict__ out) {
+  const long total = (long)M * nlt * ntc * kBlk;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
+       i += (long)gridDim.x * blockDim.x) {
+    const int e = (int)(i % kBlk);
+    long rest = i / kBlk;
+    const int tc = (int)(rest % ntc);
+    rest /= ntc;
+    const int lt = (int)(rest % nlt);
+    const int mi = (int)(rest / nlt);
+    const int r = e / kTileK, k = e % kTileK;
+    const int l = lt * kTileR + r, t = tc * kTileK + k;
+    float x = 0.f;
+    if (l < L && t < nth) x = K[((size_t)t * L + l) * M + mi];
+    const __nv_bfloat16 hi = __float2bfloat16_rn(x);
+    const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+    __nv_bfloat16* blk = out + (((size_t)mi * nlt + lt) * ntc + tc) * 2 * kBlk;
+    const int off = core_off(r, k) / 2;
+    blk[off] = hi;
+    blk[kBlk + off] = lo;
+  }
+}
+
+// raw spectra [b][t][mi] (complex float) -> Bp[mi][bg][tc][hi/lo][block], n = 2 (b - 64 bg) + c
+__global__ void pack_kernel_b(const float2* __restrict__ X, int B, int nth, int M, int nbg, int ntc,
+                              __nv_bfloat16* __restrict__ out) {
+  const long total = (long)M * nbg * ntc * kBlk;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
+       i += (long)gridDim.x * blockDim.x) {
+    const int e = (int)(i % kBlk);
+    long rest = i / kBlk;
+    const int tc = (int)(rest % ntc);
+    rest /= ntc;
+    const int bg = (int)(rest % nbg);
+    const int mi = (int)(rest / nbg);
+    const int n = e / kTileK, k = e % kTileK;
+    const int b = bg * 64 + (n >> 1), t = tc * kTileK + k;
+    float x = 0.f;
+    if (b < B && t < nth) {
+      const float2 v = X[((size_t)b * nth + t) * M + mi];
+      x = (n & 1) ? v.y : v.x;
+    }
+    const __nv_bfloat16 hi = __float2bfloat16_rn(x);
+    const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+    __nv_bfloat16* blk = out + (((size_t)mi * nbg + bg) * ntc + tc) * 2 * kBlk;
+    const int off = core_off(n, k) / 2;
+    blk[off] = hi;
+    blk[kBlk + off] = lo;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// the MMA kernel: grid (ceil(M/4), nlt, nbg), 128 threads
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128, 1) tc_forward_kernel(TcParams p) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
+  uint64_t* empty = full + kStages;
+  uint64_t* done = empty + kStages;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int mg = blockIdx.x, lt = blockIdx.y, bg = blockIdx.z;
+  const int mi0 = mg * kMPerCta;
+  const int nm = min(kMPerCta, p.M - mi0);
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     su32(tmem_slot)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mb_init(&full[s], 1);
+      mb_init(&empty[s], 1);
+    }
+    mb_init(done, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  // work items: (j, tc) for j < nm, tc < ntc; skip m columns whose l tile is all zero
+  const int ntc = p.ntc;
+  const int niter = nm * ntc;
+  bool ok = true;
+  if (tid == 0) {
+    auto produce = [&](int it) {
+      const int j = it / ntc, tc = it % ntc;
+      const int s = it % kStages;
+      unsigned char* st = smem + (size_t)s * kStageBytes;
+      const __nv_bfloat16* a =
+          p.Ap + ((((size_t)(mi0 + j) * p.nlt + lt) * ntc + tc) * 2 * kBlk);
+      const __nv_bfloat16* b =
+          p.Bp + ((((size_t)(mi0 + j) * p.nbg + bg) * ntc + tc) * 2 * kBlk);
+      mb_expect(&full[s], kStageBytes);
+      bulk_copy(st, a, 2 * kBlkBytes, &full[s]);
+      bulk_copy(st + 2 * kBlkBytes, b, 2 * kBlkBytes, &full[s]);
+    };
+    for (int it = 0; it < niter + kStages - 1 && ok; ++it) {
+      if (it < niter) {
+        const int s = it % kStages;
+        if (it >= kStages) ok = mb_wait(&empty[s], ((it / kStages) - 1) & 1);
+        if (!ok) break;
+        produce(it);
+      }
+      const int k = it - (kStages - 1);
+      if (k >= 0 && k < niter) {
+        const int s = k % kStages;
+        ok = mb_wait(&full[s], (k / kStages) & 1);
+        if (!ok) break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int j = k / ntc, tc = k % ntc;
+        const uint32_t d = tmem + (uint32_t)(j * 128);
+        const uint32_t st = su32(smem + (size_t)s * kStageBytes);
+        const uint32_t ahi = st, alo = st + kBlkBytes, bhi = st + 2 * kBlkBytes,
+                       blo = st + 3 * kBlkBytes;
+#pragma unroll
+        for (int kk = 0; kk < kTileK / 16; ++kk) {
+          const uint32_t o = kk * 256;  // two core matrices (16 k) per MMA
+          mma_bf16(d, sdesc(ahi + o), sdesc(bhi + o), (tc > 0 || kk > 0) ? 1u : 0u);
+          mma_bf16(d, sdesc(ahi + o), sdesc(blo + o), 1u);
+          mma_bf16(d, sdesc(alo + o), sdesc(bhi + o), 1u);
+        }
+        mma_commit(&empty[s]);
+      }
+    }
+    if (ok) mma_commit(done);
+    if (!ok) atomicExch(p.status, 1);
+  }
+  __syncwarp();
+  // everyone waits for the accumulators (bounded); on failure skip the epilogue
+  bool good = mb_wait(done, 0);
+  good = __syncthreads_and(good) != 0;
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (good) {
+    // lane (row l) of this warp's TMEM quarter; 32 columns per load
+    const int l = lt * kTileR + warp * 32 + lane;
+    for (int q = 0; q < 4; ++q) {  // 16 maps per pass
+      float v[kMPerCta][32];
+#pragma unroll
+      for (int j = 0; j < kMPerCta; ++j) {
+        const uint32_t addr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(j * 128 + q * 32);
+        uint32_t r[32];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+            "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+              "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+              "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+              "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+              "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+              "=r"(r[31])
+            : "r"(addr)
+            : "memory");
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int x = 0; x < 32; ++x) v[j][x] = __uint_as_float(r[x]);
+      }
+      if (l < p.L) {
+        for (int x = 0; x < 16; ++x) {
+          const int b = bg * 64 + q * 16 + x;
+          if (b >= p.B) break;
+          float2* row = p.out + ((size_t)b * p.L + l) * (2 * p.L - 1) + p.mshift + mi0;
+#pragma unroll
+          for (int j = 0; j < kMPerCta; ++j)
+            if (j < nm) row[j] = make_float2(p.sign * v[j][2 * x], p.sign * v[j][2 * x + 1]);
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTmemCols)
+                 : "memory");
+}
+
+size_t tc_packed_a_bytes(int nth, int L, int M) {
+  const int nlt = (L + kTileR - 1) / kTileR, ntc = (nth + kTileK - 1) / kTileK;
+  return (size_t)M * nlt * ntc * 2 * kBlkBytes;
+}
+size_t tc_packed_b_bytes(int nth, int B, int M) {
+  const int nbg = (B + 63) / 64, ntc = (nth + kTileK - 1) / kTileK;
+  return (size_t)M * nbg * ntc * 2 * kBlkBytes;
+}
+
+static int tgrid(long n) {
+  long b = (n + 255) / 256;
+  if (b > 1048576) b = 1048576;
+  return b < 1 ? 1 : (int)b;
+}
+
+cudaError_t launch_tc_pack_a(const float* K, int nth, int L, int M, void* out, cudaStream_t s) {
+  const int nlt = (L + kTileR - 1) / kTileR, ntc = (nth + kTileK - 1) / kTileK;
+  const long total = (long)M * nlt * ntc * kBlk;
+  pack_kernel_a<<<tgrid(total), 256, 0, s>>>(K, nth, L, M, nlt, ntc, (__nv_bfloat16*)out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tc_pack_b(const void* X, int B, int nth, int M, void* out, cudaStream_t s) {
+  const int nbg = (B + 63) / 64, ntc = (nth + kTileK - 1) / kTileK;
+  const long total = (long)M * nbg * ntc * kBlk;
+  pack_kernel_b<<<tgrid(total), 256, 0, s>>>((const float2*)X, B, nth, M, nbg, ntc,
+                                             (__nv_bfloat16*)out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tc_forward(TcParams p, cudaStream_t s) {
+  p.nlt = (p.L + kTileR - 1) / kTileR;
+  p.ntc = (p.nth + kTileK - 1) / kTileK;
+  p.nbg = (p.B + 63) / 64;
+  const size_t smem = (size_t)kStages * kStageBytes + 1024;
+  cudaError_t e = cudaFuncSetAttribute(tc_forward_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  dim3 grid((p.M + kMPerCta - 1) / kMPerCta, p.nlt, p.nbg);
+  tc_forward_kernel<<<grid, 128, smem, s>>>(p);
+  return cudaGetLastError();
+}
+
+}  // namespace s2b

@@ -1,5 +1,8 @@
 """Drop-in precompute-kernel transforms on one B200.
 
+Precision "bf16x3" runs the forward contraction on the tcgen05 tensor cores
+with 3-term bf16 split operands (its forward kernel is an opaque packed buffer).
+
 Mirrors upstream ``s2fft.precompute_transforms.spherical.inverse`` / ``forward``
 (s2fft/precompute_transforms/spherical.py:19-84, 226-311) and
 ``construct.spin_spherical_kernel`` (construct.py:16-161). The kernel table
@@ -52,11 +55,15 @@ def spin_spherical_kernel(L: int, spin: int = 0, reality: bool = False, sampling
     cdt = _dtypes(precision)[0]
     dev = _device()
     plan = _plan(dev, L, spin, nside, s, reality, precision, 1)
-    shape = _kernel_shape(L, s, nside, reality, forward)
-    K = torch.empty(shape, dtype=cdt if s == "healpix" else rdt, device=dev)
     n = ctypes.c_size_t()
     _lib.check(_lib.lib().s2b_kernel_size(plan.ptr, int(forward), ctypes.byref(n)))
-    assert n.value == K.numel() * K.element_size()
+    if precision == "bf16x3" and forward:
+        # packed bf16 hi/lo operand tiles for the tensor-core contraction (opaque)
+        K = torch.empty(n.value, dtype=torch.uint8, device=dev)
+    else:
+        shape = _kernel_shape(L, s, nside, reality, forward)
+        K = torch.empty(shape, dtype=cdt if s == "healpix" else rdt, device=dev)
+        assert n.value == K.numel() * K.element_size()
     _lib.check(_lib.lib().s2b_kernel_build(plan.ptr, int(forward), K.data_ptr(),
                                            _lib.stream_handle(dev)))
     return K
@@ -66,6 +73,10 @@ def _kernel_tensor(kernel, L, s, nside, reality, forward, precision, spin, dev):
     cdt, rdt = _dtypes(precision)
     if kernel is None:
         return spin_spherical_kernel(L, spin, reality, s, nside, forward, precision=precision)
+    if precision == "bf16x3" and forward:
+        if not (isinstance(kernel, torch.Tensor) and kernel.dtype == torch.uint8):
+            raise ValueError("bf16x3 forward needs the packed kernel from spin_spherical_kernel")
+        return kernel.to(dev)
     want = cdt if s == "healpix" else rdt
     if isinstance(kernel, np.ndarray):
         kernel = torch.from_numpy(np.ascontiguousarray(kernel))

@@ -94,7 +94,7 @@ def _ret(t, was_numpy, dev):
 
 def _dtypes(precision):
     if precision not in _lib.PRECISION:
-        raise ValueError("precision must be 'f64' or 'f32'")
+        raise ValueError("precision must be 'f64', 'f32' or 'bf16x3'")
     return (torch.complex128, torch.float64) if precision == "f64" else (torch.complex64,
                                                                           torch.float32)
 

@@ -187,3 +187,22 @@ def test_precompute_reality_batch(s2b, rng, sampling):
     if sampling != "healpix":
         g = s2b.precompute.forward(ref, L, 0, None, sampling, True, nside=nside)
         assert relerr(g, flms) < TOL64
+
+
+@pytest.mark.parametrize("spin", [2, -2])
+def test_bf16x3_tensor_core_forward(s2b, rng, spin):
+    """Batched precompute forward on tcgen05 (bf16 x3 split, FP32 accumulation)."""
+    L, B = 40, 70  # two groups of 64 maps
+    flms = np.stack([oracle.signal.generate_flm(rng, L, 0, spin, False) for _ in range(B)])
+    f = np.stack([oracle.spherical.inverse(x, L, spin, None, "gl") for x in flms])
+    K = s2b.precompute.spin_spherical_kernel(L, spin, False, "gl", None, True,
+                                             precision="bf16x3")
+    g = s2b.precompute.forward(f, L, spin, K, "gl", precision="bf16x3")
+    err = relerr(g, flms)
+    assert err < 5e-5, err
+    g32 = s2b.precompute.forward(f, L, spin, None, "gl", precision="f32")
+    assert relerr(g32, flms) < TOL32
+    from s2fft_b200 import _lib
+
+    for plan in list(_lib._plans.values()):
+        assert plan.status() == 0
