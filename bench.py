@@ -42,6 +42,10 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--L", type=int, default=1024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the secondary configurations (batched tensor-core, HEALPix)")
+    ap.add_argument("--tc-profile", action="store_true",
+                    help="small tensor-core case for ncu (GL L=256, 64 maps)")
     ap.add_argument("--cpu-budget", type=float, default=25.0,
                     help="seconds of host work for the CPU baseline sample")
     ap.add_argument("--profile-case", action="store_true",
@@ -263,6 +267,109 @@ def run_ours(args, rank, world, torch, dist):
 
 
 # ---------------------------------------------------------------------------
+# secondary configurations (extra fields of the JSON line)
+# ---------------------------------------------------------------------------
+def _time(torch, fn, steps, warmup, flush):
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    tot = 0.0
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        tot += e0.elapsed_time(e1)
+    return tot / steps
+
+
+def run_batched_precompute(torch, L=512, B=64, steps=5, warmup=2):
+    """GL sampling, spin +-2, 64 maps: precompute forward, FP32 SIMT vs BF16x3 tcgen05."""
+    import s2fft_b200
+    from s2fft_b200 import _lib
+
+    import oracle
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    out = {"workload": f"precompute forward, GL, L={L}, {B} maps, spin +-2", "maps": B}
+    for spin in (2, -2):
+        rng = np.random.default_rng(1000 + spin)
+        flm = np.stack([oracle.signal.generate_flm_full_complex(rng, L, 0, spin)
+                        for _ in range(B)])
+        x64 = torch.from_numpy(flm).to(dev)
+        f64 = s2fft_b200.inverse(x64, L, spin, None, "gl")  # seeded maps from the inverse
+        K64 = s2fft_b200.precompute.spin_spherical_kernel(L, spin, False, "gl", None, True)
+        ref = s2fft_b200.precompute.forward(f64, L, spin, K64, "gl")
+        del K64
+        torch.cuda.empty_cache()
+        res = {}
+        for prec in ("f32", "bf16x3"):
+            K = s2fft_b200.precompute.spin_spherical_kernel(L, spin, False, "gl", None, True,
+                                                            precision=prec)
+            f32 = f64.to(torch.complex64)
+            plan = _lib.get_plan(dev, L=L, spin=spin, nside=0, sampling=_lib.SAMPLING["gl"],
+                                 reality=0, L_lower=0, precision=_lib.PRECISION[prec],
+                                 batch=B, iter=0, N=0)
+            ev = [torch.cuda.Event(True), torch.cuda.Event(True)]
+            for e in ev:
+                e.record()
+            ms = _time(torch, lambda: s2fft_b200.precompute.forward(f32, L, spin, K, "gl",
+                                                                    precision=prec),
+                       steps, warmup, flush)
+            _lib.check(_lib.lib().s2b_plan_set_events(plan.ptr, 1, ev[0].cuda_event,
+                                                      ev[1].cuda_event))
+            g = s2fft_b200.precompute.forward(f32, L, spin, K, "gl", precision=prec)
+            torch.cuda.synchronize()
+            _lib.check(_lib.lib().s2b_plan_set_events(plan.ptr, 1, None, None))
+            kern_ms = ev[0].elapsed_time(ev[1]) if prec == "bf16x3" else None
+            d = (g.to(torch.complex128) - ref).abs()
+            mx = ref.abs().max().item()
+            res[prec] = {"maps_per_s": B / (ms * 1e-3), "ms_per_batch": ms,
+                         "max_rel_err": d.max().item() / mx,
+                         "rms_rel_err": (d.pow(2).mean().sqrt() / ref.abs().pow(2).mean().sqrt()).item()}
+            if kern_ms:
+                res[prec]["contraction_ms"] = kern_ms
+                nth = L
+                flops = 2.0 * L * nth * (2 * L - 1) * 2 * B  # algorithmic (one product per term)
+                res[prec]["contraction_tflops_algorithmic"] = flops / (kern_ms * 1e-3) / 1e12
+                kbytes = L * nth * (2 * L - 1) * 4.0
+                res[prec]["kernel_table_gbs"] = kbytes / (kern_ms * 1e-3) / 1e9
+            del K
+            torch.cuda.empty_cache()
+        out[f"spin{spin:+d}"] = res
+    return out
+
+
+def run_healpix_iter(torch, nside=256, L=512, steps=5, warmup=2):
+    """HEALPix nside=256, L=512, real signal: inverse + forward with 3 refinement iterations."""
+    import s2fft_b200
+
+    import oracle
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    rng = np.random.default_rng(7)
+    flm = torch.from_numpy(oracle.signal.generate_flm(rng, L, 0, 0, True)).to(dev)
+    out = {"workload": f"healpix nside={nside} L={L} reality, forward iter=3"}
+    for prec in ("f32", "f64"):
+        x = flm.to(torch.complex64 if prec == "f32" else torch.complex128)
+        f = s2fft_b200.inverse(x, L, 0, nside, "healpix", reality=True, precision=prec)
+        ms_inv = _time(torch, lambda: s2fft_b200.inverse(x, L, 0, nside, "healpix", reality=True,
+                                                         precision=prec), steps, warmup, flush)
+        ms_fwd = _time(torch, lambda: s2fft_b200.forward(f, L, 0, nside, "healpix", reality=True,
+                                                         iter=3, precision=prec),
+                       steps, warmup, flush)
+        g = s2fft_b200.forward(f, L, 0, nside, "healpix", reality=True, iter=3, precision=prec)
+        err = ((g.to(torch.complex128) - flm).abs().max() / flm.abs().max()).item()
+        out[prec] = {"inverse_ms": ms_inv, "forward_iter3_ms": ms_fwd,
+                     "roundtrip_max_rel_err": err}
+    return out
+
+
+# ---------------------------------------------------------------------------
 # CPU reference: the float64 numpy restatement of the upstream algorithm
 # (oracle/), on a bounded sample: the first k m-steps of every latitudinal
 # recursion on all rings (rings split over host processes), plus the full
@@ -387,6 +494,10 @@ def main():
         dist = tdist
     else:
         torch.cuda.set_device(0)
+    if args.tc_profile:
+        print(json.dumps(run_batched_precompute(torch, L=args.L if args.L != 1024 else 256, B=64,
+                                                steps=1, warmup=1)))
+        return
     if args.profile_case:
         args.steps, args.warmup = 2, 1
     r = run_ours(args, rank, world, torch, dist)
@@ -432,6 +543,9 @@ def main():
             "e2e": {"value": r["e2e"], "unit": UNIT, "h2d_bytes_per_step": r["h2d"],
                     "d2h_bytes_per_step": r["d2h"]},
             "gpu_launches": 8 * args.steps}
+    if not args.profile_case and not args.no_extra:
+        line["batched_precompute"] = run_batched_precompute(torch)
+        line["healpix_iter3"] = run_healpix_iter(torch)
     if not args.no_cpu_baseline and not args.profile_case:
         c = cpu_sample(args.L, args.cpu_budget)
         line["cpu_baseline"] = {"value": c["value"], "unit": UNIT, "cores": c["cores"],

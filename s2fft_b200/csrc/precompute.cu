@@ -133,92 +133,134 @@ __global__ void kernel_table_kernel(KernelTableParams p) {
 }
 
 // ---------------------------------------------------------------------------
-// streaming contractions; threads run along mi (contiguous in K and in the data)
+// streaming contractions; threads run along mi (contiguous in K and in the data).
+// Register tiles: each thread owns RT rows of the output (t for the inverse, l
+// for the forward) for BB maps, so every data element loaded is reused RT times
+// and every K element BB times. Accumulation in the plan precision.
 // ---------------------------------------------------------------------------
-// inverse: out ftm [b][t][mo + mi] (ncol columns) = sgn * sum_l K[t][l][mi] flm[b][l][m0 + L-1 + mi]
+constexpr int kRT = 4, kBB = 8;
+
+// inverse: ftm[b][t][mo + mi] = sgn * sum_l K[t][l][mi] flm[b][l][mshift + mi]
 template <typename Real, bool CPLX>
 __global__ void pre_inverse_kernel(PreContractParams p) {
   using C = P2<Real>;
-  constexpr int BB = 8;  // maps per pass
   const int M = p.M;
   const int mi = blockIdx.x * blockDim.x + threadIdx.x;
-  const int t = blockIdx.y;
-  const int b0 = blockIdx.z * BB;
+  const int t0 = blockIdx.y * kRT;
+  const int b0 = blockIdx.z * kBB;
   if (mi >= M) return;
   const int L = p.L;
-  const int col = p.mshift + mi;  // flm column L-1+m
-  double ar[BB], ai[BB];
+  Real ar[kRT][kBB], ai[kRT][kBB];
 #pragma unroll
-  for (int x = 0; x < BB; ++x) ar[x] = ai[x] = 0.0;
+  for (int r = 0; r < kRT; ++r)
+#pragma unroll
+    for (int x = 0; x < kBB; ++x) ar[r][x] = ai[r][x] = Real(0);
   const C* flm = reinterpret_cast<const C*>(p.in);
   for (int l = 0; l < L; ++l) {
-    double kr, ki = 0.0;
-    if (CPLX) {
-      const C k = reinterpret_cast<const C*>(p.K)[((size_t)t * L + l) * M + mi];
-      kr = k.x;
-      ki = k.y;
-    } else {
-      kr = reinterpret_cast<const Real*>(p.K)[((size_t)t * L + l) * M + mi];
+    C f[kBB];
+#pragma unroll
+    for (int x = 0; x < kBB; ++x) {
+      f[x].x = f[x].y = Real(0);
+      if (b0 + x < p.batch) f[x] = flm[((size_t)(b0 + x) * L + l) * (2 * L - 1) + p.mshift + mi];
     }
 #pragma unroll
-    for (int x = 0; x < BB; ++x) {
-      if (b0 + x >= p.batch) break;
-      const C f = flm[((size_t)(b0 + x) * L + l) * (2 * L - 1) + col];
-      ar[x] += kr * f.x - ki * f.y;
-      ai[x] += kr * f.y + ki * f.x;
+    for (int r = 0; r < kRT; ++r) {
+      const int t = t0 + r;
+      if (t >= p.nth) break;
+      Real kr, ki = Real(0);
+      if (CPLX) {
+        const C k = reinterpret_cast<const C*>(p.K)[((size_t)t * L + l) * M + mi];
+        kr = k.x;
+        ki = k.y;
+      } else {
+        kr = reinterpret_cast<const Real*>(p.K)[((size_t)t * L + l) * M + mi];
+      }
+#pragma unroll
+      for (int x = 0; x < kBB; ++x) {
+        ar[r][x] = fma(kr, f[x].x, ar[r][x]);
+        ai[r][x] = fma(kr, f[x].y, ai[r][x]);
+        if (CPLX) {
+          ar[r][x] = fma(-ki, f[x].y, ar[r][x]);
+          ai[r][x] = fma(ki, f[x].x, ai[r][x]);
+        }
+      }
     }
   }
   C* out = reinterpret_cast<C*>(p.out);
 #pragma unroll
-  for (int x = 0; x < BB; ++x) {
-    if (b0 + x >= p.batch) break;
-    C o;
-    o.x = (Real)(p.sign * ar[x]);
-    o.y = (Real)(p.sign * ai[x]);
-    out[((size_t)(b0 + x) * p.nth + t) * p.ncol + p.mo + mi] = o;
+  for (int r = 0; r < kRT; ++r) {
+    const int t = t0 + r;
+    if (t >= p.nth) break;
+#pragma unroll
+    for (int x = 0; x < kBB; ++x) {
+      if (b0 + x >= p.batch) break;
+      C o;
+      o.x = (Real)(p.sign * ar[r][x]);
+      o.y = (Real)(p.sign * ai[r][x]);
+      out[((size_t)(b0 + x) * p.nth + t) * p.ncol + p.mo + mi] = o;
+    }
   }
 }
 
-// forward: out flm [b][l][L-1+m] = sgn * sum_t K[t][l][mi] ftm[b][t][mi] (ftm row width M)
+// forward: flm[b][l][mshift + mi] = sgn * sum_t K[t][l][mi] ftm[b][t][mi]
 template <typename Real, bool CPLX>
 __global__ void pre_forward_kernel(PreContractParams p) {
   using C = P2<Real>;
-  constexpr int BB = 8;
   const int M = p.M;
   const int mi = blockIdx.x * blockDim.x + threadIdx.x;
-  const int l = blockIdx.y;
-  const int b0 = blockIdx.z * BB;
+  const int l0 = blockIdx.y * kRT;
+  const int b0 = blockIdx.z * kBB;
   if (mi >= M) return;
   const int L = p.L;
-  double ar[BB], ai[BB];
+  Real ar[kRT][kBB], ai[kRT][kBB];
 #pragma unroll
-  for (int x = 0; x < BB; ++x) ar[x] = ai[x] = 0.0;
+  for (int r = 0; r < kRT; ++r)
+#pragma unroll
+    for (int x = 0; x < kBB; ++x) ar[r][x] = ai[r][x] = Real(0);
   const C* ftm = reinterpret_cast<const C*>(p.in);
   for (int t = 0; t < p.nth; ++t) {
-    double kr, ki = 0.0;
-    if (CPLX) {
-      const C k = reinterpret_cast<const C*>(p.K)[((size_t)t * L + l) * M + mi];
-      kr = k.x;
-      ki = k.y;
-    } else {
-      kr = reinterpret_cast<const Real*>(p.K)[((size_t)t * L + l) * M + mi];
+    C f[kBB];
+#pragma unroll
+    for (int x = 0; x < kBB; ++x) {
+      f[x].x = f[x].y = Real(0);
+      if (b0 + x < p.batch) f[x] = ftm[((size_t)(b0 + x) * p.nth + t) * M + mi];
     }
 #pragma unroll
-    for (int x = 0; x < BB; ++x) {
-      if (b0 + x >= p.batch) break;
-      const C f = ftm[((size_t)(b0 + x) * p.nth + t) * M + mi];
-      ar[x] += kr * f.x - ki * f.y;
-      ai[x] += kr * f.y + ki * f.x;
+    for (int r = 0; r < kRT; ++r) {
+      const int l = l0 + r;
+      if (l >= L) break;
+      Real kr, ki = Real(0);
+      if (CPLX) {
+        const C k = reinterpret_cast<const C*>(p.K)[((size_t)t * L + l) * M + mi];
+        kr = k.x;
+        ki = k.y;
+      } else {
+        kr = reinterpret_cast<const Real*>(p.K)[((size_t)t * L + l) * M + mi];
+      }
+#pragma unroll
+      for (int x = 0; x < kBB; ++x) {
+        ar[r][x] = fma(kr, f[x].x, ar[r][x]);
+        ai[r][x] = fma(kr, f[x].y, ai[r][x]);
+        if (CPLX) {
+          ar[r][x] = fma(-ki, f[x].y, ar[r][x]);
+          ai[r][x] = fma(ki, f[x].x, ai[r][x]);
+        }
+      }
     }
   }
   C* out = reinterpret_cast<C*>(p.out);
 #pragma unroll
-  for (int x = 0; x < BB; ++x) {
-    if (b0 + x >= p.batch) break;
-    C o;
-    o.x = (Real)(p.sign * ar[x]);
-    o.y = (Real)(p.sign * ai[x]);
-    out[((size_t)(b0 + x) * L + l) * (2 * L - 1) + p.mshift + mi] = o;
+  for (int r = 0; r < kRT; ++r) {
+    const int l = l0 + r;
+    if (l >= L) break;
+#pragma unroll
+    for (int x = 0; x < kBB; ++x) {
+      if (b0 + x >= p.batch) break;
+      C o;
+      o.x = (Real)(p.sign * ar[r][x]);
+      o.y = (Real)(p.sign * ai[r][x]);
+      out[((size_t)(b0 + x) * L + l) * (2 * L - 1) + p.mshift + mi] = o;
+    }
   }
 }
 
@@ -252,8 +294,9 @@ cudaError_t launch_kernel_table(bool fp64, const KernelTableParams& p, cudaStrea
 
 cudaError_t launch_pre_contract(bool fp64, bool forward, bool cplx, const PreContractParams& p,
                                 cudaStream_t s) {
-  const int threads = 128;
-  dim3 grid((p.M + threads - 1) / threads, forward ? p.L : p.nth, (p.batch + 7) / 8);
+  const int threads = 64;
+  dim3 grid((p.M + threads - 1) / threads, ((forward ? p.L : p.nth) + kRT - 1) / kRT,
+            (p.batch + kBB - 1) / kBB);
 #define S2B_LAUNCH(R, C)                                                   \
   if (forward)                                                             \
     pre_forward_kernel<R, C><<<grid, threads, 0, s>>>(p);                  \
