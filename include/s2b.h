@@ -5,10 +5,12 @@
  * (S2B_OK == 0) and never exits the process; s2b_last_error() gives the
  * message of the last failure on the calling thread.
  *
- * Device buffers are caller-owned. Inputs are never modified. Execution is
- * stream-ordered on the given cudaStream_t (passed as void*), performs no
- * device allocation and no host synchronisation, so it can be captured in a
- * CUDA graph once the plan exists.
+ * Device buffers are caller-owned. Inputs are never modified. The transform
+ * calls (s2b_inverse, s2b_forward, s2b_wigner_*, s2b_precompute_*) are
+ * stream-ordered on the given cudaStream_t (passed as void*) and perform no
+ * device allocation and no host synchronisation, so they can be captured in a
+ * CUDA graph once the plan exists. Plan creation allocates the plan's tables;
+ * s2b_kernel_build with S2B_BF16X3 allocates and frees a temporary table.
  *
  * Array layouts (row-major, innermost last), for B = desc.batch maps:
  *   flm   [B][L][2L-1]           complex, index [l][L-1+m]
@@ -24,10 +26,6 @@
  *                   + transforms/otf_recursions.py:15-171 (inverse_latitudinal_step)
  *   s2b_forward  <- s2fft/transforms/spherical.py:352-464 (forward, incl. iter refinement)
  *                   + transforms/otf_recursions.py:432-588 (forward_latitudinal_step)
- *   s2b_healpix_fft / s2b_healpix_ifft
- *                <- lib/src/extensions.cc:26-100 (XLA custom call healpix_fft_cuda:
- *                   healpix_forward / healpix_backward) and
- *                   s2fft/utils/healpix_ffts.py:187-423 (healpix_fft / healpix_ifft)
  *   s2b_plan_create <- lib/src/extensions.cc:115-149 (build_healpix_fft_descriptor,
  *                   plan cache init) and recursions/price_mcewen.py:118-255
  *                   (generate_precomputes_jax: per-plan recursion tables)
