@@ -139,6 +139,32 @@ int s2b_plan_status(s2b_plan* plan, int* status);
  * benchmark to time the dominant kernel on the launching stream. */
 int s2b_plan_set_events(s2b_plan* plan, int forward, void* ev_begin, void* ev_end);
 
+/* Spin inverse transform for callers that may not allocate device memory:
+ * code running inside a host application or framework that owns every device
+ * allocation (a plugin handed only its input and output buffers, a custom
+ * call whose memory budget was fixed ahead of time), or code on a path where
+ * an allocation would synchronise the device. Same plan, layouts, result and
+ * errors as s2b_inverse, but instead of a caller-provided workspace it uses a
+ * fixed scratch array of S2B_NOALLOC_SCRATCH_BYTES that the library holds on
+ * every GPU it is loaded on, until the process exits. It calls no
+ * cudaMalloc/cudaFree or other allocating routine.
+ *   - Plans whose inverse workspace (s2b_workspace_size(plan, 0, ...)) exceeds
+ *     S2B_NOALLOC_SCRATCH_BYTES are rejected with S2B_ERR_WORKSPACE. 32 MiB
+ *     covers one mw-sampled map up to L ~ 1000 in float32 and L ~ 700 in
+ *     float64; dh, with twice the rings, reaches about 5/6 of that.
+ *   - The first call on a device (the current device, which must be the
+ *     plan's) looks up the array's device address with cudaGetSymbolAddress;
+ *     make that first call before any stream capture on that device.
+ *   - Every call on a device shares the one array: calls that can overlap on
+ *     the GPU (different streams, threads or plans without ordering between
+ *     them) race and corrupt each other's results. Order them on one stream.
+ *   - Leftover contents from earlier calls are harmless: each call zeroes
+ *     the accumulation rows it sums into and overwrites the rest before use.
+ * No counterpart in the reference: upstream transforms always receive their
+ * temporaries from the JAX/XLA allocator. */
+#define S2B_NOALLOC_SCRATCH_BYTES ((size_t)32 << 20)
+int s2b_inverse_noalloc(s2b_plan* plan, const void* flm, void* f, void* stream);
+
 /* Peak-rate probe: a fused multiply-add chain kernel (float when fp64 == 0,
  * double otherwise) over `blocks` CTAs of 256 threads, `iters` iterations of 8
  * independent FMA chains per thread, writing one value per thread to `out`

@@ -39,6 +39,9 @@ static int fail(int code, const std::string& msg) {
   return code;
 }
 
+// Lets other translation units of the library report through s2b_last_error().
+int s2b::set_last_error(int code, const char* msg) { return fail(code, msg); }
+
 #define S2B_CK(call)                                                                    \
   do {                                                                                  \
     cudaError_t _e = (call);                                                            \

@@ -85,6 +85,9 @@ int lat_nclass(bool fp64, int L);
 cudaError_t launch_lambda(bool fp64, int L, int spin, int nhalf, const RingInfo* rings, int nrings,
                           int Ls, void* lam, cudaStream_t s);
 int lat_qp(bool fp64, int L);
+
+// Records msg as the calling thread's s2b_last_error() text and returns code.
+int set_last_error(int code, const char* msg);
 size_t seed_bytes(bool fp64, int L, int nhalf, int nrings);
 
 }  // namespace s2b
