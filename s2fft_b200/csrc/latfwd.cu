@@ -1,0 +1,377 @@
+// Forward latitudinal step (projection of weighted ring spectra onto flm),
+// restart formulation of the Price-McEwen m-recursion.
+//
+// Same recursion and projection as upstream s2fft
+// (s2fft/transforms/otf_recursions.py:432-588, forward_latitudinal_step;
+// coefficients s2fft/recursions/price_mcewen.py:118-255): for every (theta, l)
+// the values d^l_{m,n}(theta), n = -spin, are generated from m = l towards
+// m = 0 and flm[l, m] accumulates d * G(theta, m) over the rings.
+//
+// B200 formulation (own design):
+//  * A state (theta, l) is only started where d first becomes significant
+//    (|d| >= 2^floor going down from m = l). The start values are computed
+//    once per plan in double (fwd_start_kernel); the transform itself then runs
+//    the monic recursion dt_{m-1} = lambda_m h_{l,m} dt_m - dt_{m+1} in the plan
+//    precision with no exponent bookkeeping, no gating multiply and no
+//    renormalisation: once significant, |dt| stays within [2^-110, 2^10].
+//  * Starts are taken per (ring, block of 32 consecutive l) at the largest first
+//    significant m of the block, rounded up to a group start m = 3 (mod 4), so a
+//    whole warp starts a ring together. Degrees of the block below that start
+//    begin with the exact continuation of the recursion above m = l
+//    (h_{l,m} = 0 for m > l gives dt_{l+2j} = (-1)^j dt_l, dt_{l+2j+1} = 0).
+//  * CTA tile: W warps x T rings (rings shared by the lanes of a warp, so the
+//    spectra and lambda loads are shared-memory broadcasts) x two l blocks
+//    (lane = l within the block, blocks p and NB-1-p for balance). The sum over
+//    the T rings of a thread stays in registers; warps' partial sums meet in
+//    shared memory every R = 4 steps and are added to flm with vector atomics.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <type_traits>
+
+#include "s2b_dev.h"
+#include "s2b_latfwd.h"
+
+namespace s2b {
+
+// ---------------------------------------------------------------------------
+// Start table. One warp per (half, block, ring); lane = degree within the block.
+// Double arithmetic with a running power-of-two exponent (value = v * 2^E).
+// ---------------------------------------------------------------------------
+template <typename Real>
+__global__ void fwd_start_kernel(const FwdStartParams p) {
+  using R2 = typename Vec<Real>::t2;
+  const int lane = threadIdx.x & 31;
+  const long wid = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5;
+  const long nw = (long)p.nhalf * p.NB * p.nrings;
+  if (wid >= nw) return;  // uniform per warp
+  const int r = (int)(wid % p.nrings);
+  const int blk = (int)((wid / p.nrings) % p.NB);
+  const int half = (int)(wid / ((long)p.nrings * p.NB));
+  const int n = half == 0 ? -p.spin : p.spin;
+  const int an = n < 0 ? -n : n;
+  const int L = p.L;
+  const int l = blk * kFwdBlock + lane;
+  const bool valid = l < L && l >= p.L0 && l >= an;
+  const RingInfo ri = p.rings[r];
+  const int fl = (int)p.floor_log2;
+
+  double lg = 0.0;
+  if (valid) lg = p.lbin[l] + (double)(l + n) * ri.lc + (double)(l - n) * ri.ls;
+  const double sgn = ((l - n) & 1) ? -1.0 : 1.0;
+
+  // one step of the monic recursion at m: (v, w) = (dt_m, dt_{m+1}) -> (dt_{m-1}, dt_m)
+  auto step = [&](double& v, double& w, int& E, int m) {
+    const double lam = fma(-(double)m, ri.B, (double)n * ri.A);
+    double h = 1.0;
+    if (m < l) {
+      const double f = sqrt((double)(l + m + 1) * (double)(l - m));
+      h = p.g[(size_t)m * L + l] / (f * p.g[(size_t)(m + 1) * L + l]);
+    }
+    const double nv = lam * h * v - w;
+    w = v;
+    v = nv;
+    if (fabs(v) > 0x1p200) {
+      v *= 0x1p-200;
+      w *= 0x1p-200;
+      E += 200;
+    }
+  };
+
+  // pass 1: first m (going down from l) with |d_m| = |dt_m| g_{l,m} >= 2^fl
+  int ms = -1;
+  if (valid) {
+    int E = (int)floor(lg);
+    double v = sgn * exp2(lg - (double)E), w = 0.0;
+    for (int m = l; m >= 0; --m) {
+      if (fabs(v) * p.g[(size_t)m * L + l] >= ldexp(1.0, fl - E)) {
+        ms = m;
+        break;
+      }
+      if (m == 0) break;
+      step(v, w, E, m);
+    }
+  }
+  // pass 2: common start of the block on this ring, aligned to a group start
+  int M = __reduce_max_sync(0xffffffffu, ms);
+  if (M >= 0) M |= 3;
+
+  // pass 3: (dt_M, dt_{M+1}) of this degree
+  double cur = 0.0, prv = 0.0;
+  if (valid && M >= 0) {
+    if (M >= l) {
+      const double dl = sgn * exp2(lg);
+      const int dlt = M - l;
+      if ((dlt & 1) == 0)
+        cur = ((dlt >> 1) & 1) ? -dl : dl;
+      else
+        prv = (((dlt + 1) >> 1) & 1) ? -dl : dl;
+    } else {
+      int E = (int)floor(lg);
+      double v = sgn * exp2(lg - (double)E), w = 0.0;
+      for (int m = l; m > M; --m) step(v, w, E, m);
+      cur = ldexp(v, E);
+      prv = ldexp(w, E);
+    }
+  }
+  R2 o;
+  o.x = (Real)cur;
+  o.y = (Real)prv;
+  reinterpret_cast<R2*>(p.Vst)[wid * kFwdBlock + lane] = o;
+  if (lane == 0) p.Mst[wid] = M;
+}
+
+size_t fwd_start_bytes(bool fp64, int L, int nhalf, int nrings) {
+  return (size_t)nhalf * fwd_nblocks(L) * nrings * kFwdBlock * 2 * (fp64 ? 8 : 4);
+}
+
+cudaError_t launch_fwd_start(bool fp64, const FwdStartParams& p, cudaStream_t s) {
+  const long warps = (long)p.nhalf * p.NB * p.nrings;
+  const int threads = 128;
+  const long blocks = (warps * 32 + threads - 1) / threads;
+  if (blocks > 0x7fffffffL) return cudaErrorInvalidValue;
+  if (fp64)
+    fwd_start_kernel<double><<<(unsigned)blocks, threads, 0, s>>>(p);
+  else
+    fwd_start_kernel<float><<<(unsigned)blocks, threads, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Main kernel
+// ---------------------------------------------------------------------------
+template <typename Real, bool DUAL, int T, int W, int R>
+struct Fwd2Layout {
+  using Acc = std::conditional_t<DUAL, typename Vec<Real>::t4, typename Vec<Real>::t2>;
+  static constexpr int NRT = W * T;  // rings per CTA
+  static constexpr int NT = W * 32;
+  // stage: h rows [2 blocks][R][32] | spectra rows [R][NRT] | lambda rows [R][NRT]
+  static constexpr size_t h_bytes = 2 * R * kFwdBlock * sizeof(Real);
+  static constexpr size_t g_bytes = (size_t)R * NRT * sizeof(Acc);
+  static constexpr size_t l_bytes = (size_t)R * NRT * sizeof(Real);
+  static constexpr size_t stage_bytes = h_bytes + g_bytes + l_bytes;
+  // partial sums [R][W][2][32]
+  static constexpr size_t buf_bytes = (size_t)R * W * 2 * kFwdBlock * sizeof(Acc);
+  static constexpr size_t act_bytes = (size_t)W * 2 * T * sizeof(int);
+  static constexpr size_t total = 2 * stage_bytes + buf_bytes + act_bytes + 16 + 16;
+  static_assert(stage_bytes % 16 == 0 && buf_bytes % 16 == 0 && act_bytes % 16 == 0, "align");
+  static_assert(2 * T <= 32, "act table is held by the first 2T lanes");
+};
+
+// One recursion step over the T rings of slot k: cur = dt_m, prv = dt_{m+1} -> dt_{m-1};
+// a += dt_m * G(theta_i, m) over the rings.
+template <typename Real, typename Acc, int T>
+__device__ __forceinline__ void fwd_slot_step(Real (&cur)[T], Real (&prv)[T], Real h,
+                                              const Real* __restrict__ lrow,
+                                              const Acc* __restrict__ grow, Acc& a) {
+#pragma unroll
+  for (int i = 0; i < T; ++i) {
+    const Real x = cur[i];
+    acc_fma(a, x, grow[i]);
+    prv[i] = fma(lrow[i] * h, x, -prv[i]);
+  }
+}
+
+template <typename Real, bool DUAL, int T, int W, int R>
+__global__ void __launch_bounds__(W * 32, sizeof(Real) == 4 ? 4 : 3)
+    lat_fwd2_kernel(const Fwd2Params p) {
+  using Lay = Fwd2Layout<Real, DUAL, T, W, R>;
+  using Acc = typename Lay::Acc;
+  using R2 = typename Vec<Real>::t2;
+  constexpr int NRT = Lay::NRT;
+  constexpr int NT = Lay::NT;
+  static_assert(R == 4, "the group body below is written for R = 4");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  unsigned char* stage_base = smem_raw;
+  Acc* buf = reinterpret_cast<Acc*>(smem_raw + 2 * Lay::stage_bytes);
+  int* act = reinterpret_cast<int*>(smem_raw + 2 * Lay::stage_bytes + Lay::buf_bytes);
+  int* mk = act + W * 2 * T;  // CTA-wide first m per slot (2 ints)
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(mk) + 16);
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int wp = tid >> 5;
+  const int L = p.L;
+  const int NB = p.NB;
+  const int TR = tab_rows(L);
+  const int Lp = NB * kFwdBlock;
+  // ring tiles from the equator outwards: the largest tiles are scheduled first
+  const int ntiles = (p.nrings + NRT - 1) / NRT;
+  const int mid = ntiles >> 1;
+  const int t = (int)blockIdx.x;
+  const int tile = (t & 1) ? mid - 1 - (t >> 1) : mid + (t >> 1);
+  const int r0 = tile * NRT;
+  const int kb0 = (int)blockIdx.y, kb1 = NB - 1 - (int)blockIdx.y;
+  const int half = (int)(blockIdx.z % p.nhalf);
+  const int b = (int)(blockIdx.z / p.nhalf);
+
+  // start m of every (slot, ring) of this warp: lane < 2T holds (k, i) = (lane / T, lane % T)
+  int a_m = -1;
+  if (lane < 2 * T) {
+    const int k = lane / T, i = lane % T;
+    const int r = r0 + wp * T + i;
+    if (r < p.nrings) a_m = p.Mst[((size_t)half * NB + (k ? kb1 : kb0)) * p.nrings + r];
+    act[(wp * 2 + k) * T + i] = a_m;
+  }
+  const int mt0 = __reduce_max_sync(0xffffffffu, lane < T ? a_m : -1);
+  const int mt1 = __reduce_max_sync(0xffffffffu, (lane >= T && lane < 2 * T) ? a_m : -1);
+  if (tid == 0) {
+    mk[0] = -1;
+    mk[1] = -1;
+  }
+  // zero both stages once: columns beyond a copy's extent then read as zeros
+  for (size_t x = tid * 16; x < 2 * Lay::stage_bytes; x += (size_t)NT * 16)
+    *reinterpret_cast<uint4*>(stage_base + x) = make_uint4(0, 0, 0, 0);
+  __syncthreads();
+  if (lane == 0) {
+    atomicMax(&mk[0], mt0);
+    atomicMax(&mk[1], mt1);
+  }
+  if (tid == 0) {
+    mbar_init(&mbar[0], 1);
+    mbar_init(&mbar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  const int mc0 = mk[0], mc1 = mk[1];
+  const int mtop = mc0 > mc1 ? mc0 : mc1;
+  if (mtop < 0) return;  // nothing significant in this tile (uniform)
+  const int ngroups = (mtop + 1) / R;
+
+  const Real* __restrict__ Hb = reinterpret_cast<const Real*>(p.Hb);
+  const Acc* __restrict__ Gin =
+      reinterpret_cast<const Acc*>(p.G) + ((size_t)b * p.nhalf + half) * TR * p.Gs;
+  const Real* __restrict__ lamh = reinterpret_cast<const Real*>(p.lam) + (size_t)half * TR * p.Ls;
+  const R2* __restrict__ Vst = reinterpret_cast<const R2*>(p.Vst);
+  Acc* __restrict__ out = reinterpret_cast<Acc*>(p.acc) + ((size_t)b * p.nhalf + half) * L * Lp;
+  int ncopy = p.Gs - r0;
+  if (ncopy > NRT) ncopy = NRT;
+  int nlam = p.Ls - r0;
+  if (nlam > NRT) nlam = NRT;
+
+  auto issue = [&](int g) {
+    unsigned char* st = stage_base + (size_t)(g & 1) * Lay::stage_bytes;
+    const int row0 = mtop - g * R - R + 1 + kPadLo;
+    constexpr unsigned hb = R * kFwdBlock * sizeof(Real);
+    const unsigned bytes = 2 * hb + (unsigned)(R * ncopy * sizeof(Acc)) +
+                           (unsigned)(R * nlam * sizeof(Real));
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(&mbar[g & 1], bytes);
+    bulk_g2s(st, Hb + ((size_t)kb0 * TR + row0) * kFwdBlock, hb, &mbar[g & 1]);
+    bulk_g2s(st + hb, Hb + ((size_t)kb1 * TR + row0) * kFwdBlock, hb, &mbar[g & 1]);
+    unsigned char* gdst = st + Lay::h_bytes;
+#pragma unroll
+    for (int s = 0; s < R; ++s)
+      bulk_g2s(gdst + (size_t)s * NRT * sizeof(Acc), Gin + (size_t)(row0 + s) * p.Gs + r0,
+               (unsigned)(ncopy * sizeof(Acc)), &mbar[g & 1]);
+    unsigned char* ldst = st + Lay::h_bytes + Lay::g_bytes;
+#pragma unroll
+    for (int s = 0; s < R; ++s)
+      bulk_g2s(ldst + (size_t)s * NRT * sizeof(Real), lamh + (size_t)(row0 + s) * p.Ls + r0,
+               (unsigned)(nlam * sizeof(Real)), &mbar[g & 1]);
+  };
+  if (tid == 0) {
+    issue(0);
+    if (ngroups > 1) issue(1);
+  }
+
+  Real v[2][T], w[2][T];
+#pragma unroll
+  for (int k = 0; k < 2; ++k)
+#pragma unroll
+    for (int i = 0; i < T; ++i) {
+      v[k][i] = Real(0);
+      w[k][i] = Real(0);
+    }
+  int next_act = mt0 > mt1 ? mt0 : mt1;  // warp-uniform
+  const int kb[2] = {kb0, kb1};
+  const int mtw[2] = {mt0, mt1};
+
+  for (int grp = 0; grp < ngroups; ++grp) {
+    const int mgrp = mtop - grp * R;
+    const bool ok = mbar_wait(&mbar[grp & 1], (grp >> 1) & 1);
+    // start the (slot, ring) states whose first m is this group's first m
+    if (mgrp == next_act) {
+#pragma unroll
+      for (int k = 0; k < 2; ++k)
+#pragma unroll
+        for (int i = 0; i < T; ++i)
+          if (act[(wp * 2 + k) * T + i] == mgrp) {
+            const R2 sv = Vst[(((size_t)half * NB + kb[k]) * p.nrings + r0 + wp * T + i) *
+                                  kFwdBlock + lane];
+            v[k][i] = sv.x;
+            w[k][i] = sv.y;
+          }
+      next_act = __reduce_max_sync(0xffffffffu, (lane < 2 * T && a_m < mgrp) ? a_m : -1);
+    }
+    const unsigned char* st = stage_base + (size_t)(grp & 1) * Lay::stage_bytes;
+    const Real* hS = reinterpret_cast<const Real*>(st);
+    const Acc* gS = reinterpret_cast<const Acc*>(st + Lay::h_bytes) + wp * T;
+    const Real* lS = reinterpret_cast<const Real*>(st + Lay::h_bytes + Lay::g_bytes) + wp * T;
+
+#define S2B_FWD2_STEP(CUR, PRV, S)                                                       \
+  {                                                                                      \
+    constexpr int srow = R - 1 - (S);                                                    \
+    const int m = mgrp - (S);                                                            \
+    _Pragma("unroll") for (int k = 0; k < 2; ++k) {                                      \
+      Acc a = zero_acc<Acc>();                                                           \
+      if (m <= mtw[k])                                                                   \
+        fwd_slot_step<Real, Acc, T>(CUR[k], PRV[k], hS[(k * R + srow) * kFwdBlock + lane], \
+                                    lS + srow * NRT, gS + srow * NRT, a);                \
+      buf[(((S) * W + wp) * 2 + k) * kFwdBlock + lane] = a;                              \
+    }                                                                                    \
+  }
+    S2B_FWD2_STEP(v, w, 0)
+    S2B_FWD2_STEP(w, v, 1)
+    S2B_FWD2_STEP(v, w, 2)
+    S2B_FWD2_STEP(w, v, 3)
+#undef S2B_FWD2_STEP
+
+    if (!__syncthreads_and(ok)) {
+      if (tid == 0) {
+        atomicExch(p.status, 1);
+        mbar_wait(&mbar[(grp + 1) & 1], ((grp + 1) >> 1) & 1);
+      }
+      return;
+    }
+    // warps' partial sums -> flm accumulator
+    for (int it = tid; it < R * 2 * kFwdBlock; it += NT) {
+      const int S = it / (2 * kFwdBlock);
+      const int k = (it / kFwdBlock) & 1;
+      const int ln = it % kFwdBlock;
+      const int m = mgrp - S;
+      const int l = (k ? kb1 : kb0) * kFwdBlock + ln;
+      if (m < 0 || m > (k ? mc1 : mc0) || l >= L || l < m) continue;
+      Acc s = buf[((S * W + 0) * 2 + k) * kFwdBlock + ln];
+#pragma unroll
+      for (int x = 1; x < W; ++x) acc_add(s, buf[((S * W + x) * 2 + k) * kFwdBlock + ln]);
+      red_add(out + (size_t)m * Lp + l, s);
+    }
+    __syncthreads();
+    if (tid == 0 && grp + 2 < ngroups) issue(grp + 2);
+  }
+}
+
+template <typename Real, bool DUAL, int T, int W>
+static cudaError_t launch_fwd2_cfg(const Fwd2Params& p, cudaStream_t s) {
+  using Lay = Fwd2Layout<Real, DUAL, T, W, 4>;
+  auto kern = lat_fwd2_kernel<Real, DUAL, T, W, 4>;
+  cudaError_t err =
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::total);
+  if (err != cudaSuccess) return err;
+  const int ntiles = (p.nrings + Lay::NRT - 1) / Lay::NRT;
+  dim3 grid(ntiles, p.NB / 2, p.nhalf * p.batch);
+  kern<<<grid, Lay::NT, Lay::total, s>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fwd2(bool fp64, bool dual, const Fwd2Params& p, cudaStream_t s) {
+  if (p.nrings <= 0) return cudaSuccess;
+  if (!fp64)
+    return dual ? launch_fwd2_cfg<float, true, 16, 4>(p, s)
+                : launch_fwd2_cfg<float, false, 16, 4>(p, s);
+  return dual ? launch_fwd2_cfg<double, true, 8, 4>(p, s)
+              : launch_fwd2_cfg<double, false, 8, 4>(p, s);
+}
+
+}  // namespace s2b

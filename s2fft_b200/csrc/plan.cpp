@@ -28,6 +28,7 @@
 #include "s2b_wigner.h"
 #include "s2b_precompute.h"
 #include "s2b_tc.h"
+#include "s2b_latfwd.h"
 
 using namespace s2b;
 using cd = std::complex<double>;
@@ -347,6 +348,11 @@ struct s2b_plan {
   double* lbin = nullptr;
   double* gtab = nullptr;
   void* htab = nullptr;
+  // forward recursion, restart formulation: h by 32-degree block, start tables
+  int fwd_NB = 0;
+  void* fwd_Hb = nullptr;   // [NB][tab_rows][32]
+  int* fwd_Mst = nullptr;   // [nhalf][NB][fwd rings]
+  void* fwd_Vst = nullptr;  // [nhalf][NB][fwd rings][32] (dt_M, dt_{M+1})
   double* fwd_weights = nullptr;   // per MWSS(2L) ring (mw/mwss) or per ring
   int* status = nullptr;           // device status word (timed-out waits)
   double* hp_phi0 = nullptr;
@@ -484,6 +490,32 @@ static int build_plan(s2b_plan* p) {
     rc = upload(p, &p->lbin, lb);
     if (rc) return rc;
   }
+  {
+    // h_{l,m} by 32-degree block (zero for m > l and for l >= L)
+    const int NB = fwd_nblocks(L), TR = p->TR;
+    p->fwd_NB = NB;
+    const size_t n = (size_t)NB * TR * kFwdBlock;
+    if (p->fp64) {
+      std::vector<double> hb(n, 0.0);
+      for (int l = 0; l < L; ++l)
+        for (int m = 0; m <= l; ++m)
+          hb[((size_t)(l / kFwdBlock) * TR + m + kPadLo) * kFwdBlock + l % kFwdBlock] =
+              h[(size_t)m * L + l];
+      double* dp = nullptr;
+      rc = upload(p, &dp, hb);
+      p->fwd_Hb = dp;
+    } else {
+      std::vector<float> hb(n, 0.0f);
+      for (int l = 0; l < L; ++l)
+        for (int m = 0; m <= l; ++m)
+          hb[((size_t)(l / kFwdBlock) * TR + m + kPadLo) * kFwdBlock + l % kFwdBlock] =
+              (float)h[(size_t)m * L + l];
+      float* fp = nullptr;
+      rc = upload(p, &fp, hb);
+      p->fwd_Hb = fp;
+    }
+    if (rc) return rc;
+  }
 
   // ---- inverse geometry: rings of the sampling, poles in closed form
   std::vector<double> th = thetas(L, d.sampling, d.nside);
@@ -562,6 +594,30 @@ static int build_plan(s2b_plan* p) {
                           p->lbin, p->inv_seeds, 0));
     S2B_CK(launch_seeds(p->fp64, L, d.L_lower, d.spin, p->nhalf, p->fwd_rings, p->fwd_nrings,
                         p->lbin, p->fwd_seeds, 0));
+  }
+
+  // ---- forward start tables (device kernel, double arithmetic)
+  if (p->fwd_nrings > 0) {
+    const size_t nst = (size_t)p->nhalf * p->fwd_NB * p->fwd_nrings;
+    S2B_CK(cudaMalloc(&p->fwd_Mst, nst * sizeof(int)));
+    p->allocs.push_back(p->fwd_Mst);
+    S2B_CK(cudaMalloc(&p->fwd_Vst, fwd_start_bytes(p->fp64, L, p->nhalf, p->fwd_nrings)));
+    p->allocs.push_back(p->fwd_Vst);
+    FwdStartParams fp{};
+    fp.L = L;
+    fp.L0 = d.L_lower;
+    fp.spin = d.spin;
+    fp.nhalf = p->nhalf;
+    fp.nrings = p->fwd_nrings;
+    fp.NB = p->fwd_NB;
+    // contributions below 2^-40 (float) / 2^-70 (double) of |d| <= 1 are dropped
+    fp.floor_log2 = p->fp64 ? -70.0 : -40.0;
+    fp.rings = p->fwd_rings;
+    fp.lbin = p->lbin;
+    fp.g = p->gtab;
+    fp.Mst = p->fwd_Mst;
+    fp.Vst = p->fwd_Vst;
+    S2B_CK(launch_fwd_start(p->fp64, fp, 0));
   }
 
   // ---- lambda(theta, m) tables (double, rounded once to the plan precision)
@@ -647,7 +703,7 @@ static int build_plan(s2b_plan* p) {
   const int ncm = p->fwd_mode == 1 ? 2 * L - 1 : 2 * L;
   p->ws_fwd_cols = p->fwd_mode ? B * (size_t)ncm * p->nth * c2 : 0;
   p->ws_fwd_G = B * p->nhalf * (size_t)p->TR * p->Gs * acc;
-  p->ws_fwd_acc = B * p->nhalf * p->nclass * (size_t)L * p->Q * acc;
+  p->ws_fwd_acc = B * p->nhalf * (size_t)L * ((size_t)p->fwd_NB * kFwdBlock) * acc;
   const size_t fel = d.reality ? p->rsz : c2;
   p->ws_iter_f = d.iter > 0 ? B * (size_t)p->npix * fel : 0;
   p->ws_iter_flm = d.iter > 0 ? B * (size_t)L * (2 * L - 1) * c2 : 0;
@@ -820,26 +876,23 @@ static int run_forward_once(s2b_plan* p, const void* f, void* flm, char* ws, cud
     const int ncm = p->fwd_mode == 1 ? 2 * L - 1 : 2 * L;
     S2B_CK(launch_mw_cols<Real>(cp, ncm, d.batch, p->M1, p->M2, s));
   }
-  LatParams lp{};
+  Fwd2Params lp{};
   lp.L = L;
-  lp.L0 = d.L_lower;
-  lp.spin = d.spin;
   lp.nrings = p->fwd_nrings;
   lp.nhalf = p->nhalf;
   lp.batch = d.batch;
-  lp.rings = p->fwd_rings;
-  lp.ring_row = p->fwd_ring_row;
-  lp.seeds = p->fwd_seeds;
-  lp.H = p->htab;
-  lp.in = G;
-  lp.out = acc;
-  lp.nrows = p->fwd_nrows;
-  lp.Gs = p->Gs;
-  lp.status = p->status;
+  lp.NB = p->fwd_NB;
+  lp.Mst = p->fwd_Mst;
+  lp.Vst = p->fwd_Vst;
+  lp.Hb = p->fwd_Hb;
   lp.lam = p->fwd_lam;
   lp.Ls = p->fwd_Ls;
+  lp.G = G;
+  lp.Gs = p->Gs;
+  lp.acc = acc;
+  lp.status = p->status;
   if (p->ev_begin[1]) S2B_CK(cudaEventRecord(p->ev_begin[1], s));
-  S2B_CK(launch_latitudinal(p->fp64, true, p->dual, lp, s));
+  S2B_CK(launch_fwd2(p->fp64, p->dual, lp, s));
   if (p->ev_end[1]) S2B_CK(cudaEventRecord(p->ev_end[1], s));
   StageParams sp{};
   sp.L = L;
@@ -858,6 +911,7 @@ static int run_forward_once(s2b_plan* p, const void* f, void* flm, char* ws, cud
   sp.g = p->gtab;
   sp.G = G;
   sp.acc = acc;
+  sp.Lp = p->fwd_NB * kFwdBlock;
   sp.flm_out = flm;
   S2B_CK(launch_epilogue(p->fp64, sp, s));
   return S2B_OK;

@@ -1,0 +1,118 @@
+// Device helpers shared by the latitudinal kernels: vector accumulators,
+// global reductions, and 1-D bulk asynchronous copies global -> shared
+// completed on an mbarrier (no multicast). Waits are bounded.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <type_traits>
+
+namespace s2b {
+
+template <typename Real>
+struct Vec;
+template <>
+struct Vec<float> {
+  using t2 = float2;
+  using t4 = float4;
+};
+template <>
+struct Vec<double> {
+  using t2 = double2;
+  using t4 = double4;
+};
+
+template <typename T2>
+__device__ __forceinline__ void red_add(T2* addr, T2 v);
+template <>
+__device__ __forceinline__ void red_add<float2>(float2* addr, float2 v) {
+  atomicAdd(addr, v);  // red.global.add.v2.f32 (sm_90+)
+}
+template <>
+__device__ __forceinline__ void red_add<double2>(double2* addr, double2 v) {
+  atomicAdd(&addr->x, v.x);
+  atomicAdd(&addr->y, v.y);
+}
+template <>
+__device__ __forceinline__ void red_add<float4>(float4* addr, float4 v) {
+  atomicAdd(addr, v);  // red.global.add.v4.f32 (sm_90+)
+}
+template <>
+__device__ __forceinline__ void red_add<double4>(double4* addr, double4 v) {
+  atomicAdd(&addr->x, v.x);
+  atomicAdd(&addr->y, v.y);
+  atomicAdd(&addr->z, v.z);
+  atomicAdd(&addr->w, v.w);
+}
+
+template <typename A>
+__device__ __forceinline__ A zero_acc() {
+  A a;
+  a.x = 0;
+  a.y = 0;
+  if constexpr (sizeof(A) == 4 * sizeof(a.x)) {
+    a.z = 0;
+    a.w = 0;
+  }
+  return a;
+}
+
+template <typename A>
+__device__ __forceinline__ void acc_add(A& a, const A& b) {
+  a.x += b.x;
+  a.y += b.y;
+  if constexpr (sizeof(A) == 4 * sizeof(a.x)) {
+    a.z += b.z;
+    a.w += b.w;
+  }
+}
+
+// a += x * f (component-wise)
+template <typename A, typename Real>
+__device__ __forceinline__ void acc_fma(A& a, Real x, const A& f) {
+  a.x = fma(x, f.x, a.x);
+  a.y = fma(x, f.y, a.y);
+  if constexpr (sizeof(A) == 4 * sizeof(Real)) {
+    a.z = fma(x, f.z, a.z);
+    a.w = fma(x, f.w, a.w);
+  }
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* ptr) {
+  return (uint32_t)__cvta_generic_to_shared(ptr);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* mb, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mb)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* mb, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mb)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes,
+                                         uint64_t* mb) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(mb))
+      : "memory");
+}
+// Bounded wait for the phase with the given parity; false when it ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* mb, unsigned parity) {
+  const uint32_t a = smem_u32(mb);
+  for (int it = 0; it < (1 << 22); ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+}  // namespace s2b

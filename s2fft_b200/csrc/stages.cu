@@ -158,24 +158,27 @@ __global__ void epilogue_kernel(StageParams p) {
     double re = 0.0, im = 0.0;
     if (l >= lmin && am <= l) {
       const int j = l % C, q = l / C;
+      // offset of (m, l) in one [batch][half] slice of the forward sums, in R2/R4 units
+      const size_t cell = p.Lp > 0 ? (size_t)am * p.Lp + l : ((size_t)j * L + am) * Q + q;
+      const size_t slice = p.Lp > 0 ? (size_t)L * p.Lp : (size_t)C * L * Q;
       const double g = p.g[(size_t)am * L + l];
       double ar = 0.0, ai = 0.0;
       bool conj_mirror = false;
       if (p.dual) {
         const R2* A = reinterpret_cast<const R2*>(p.acc);
-        const R2 a = A[((((size_t)b * C + j) * L + am) * Q + q) * 2 + (m < 0 ? 1 : 0)];
+        const R2 a = A[((size_t)b * slice + cell) * 2 + (m < 0 ? 1 : 0)];
         ar = a.x;
         ai = a.y;
       } else if (m >= 0 || p.nhalf > 1) {
         const int half = m >= 0 ? 0 : 1;
         const R2* A = reinterpret_cast<const R2*>(p.acc);
-        const R2 a = A[((((size_t)b * p.nhalf + half) * C + j) * L + am) * Q + q];
+        const R2 a = A[((size_t)b * p.nhalf + half) * slice + cell];
         ar = a.x;
         ai = a.y;
       } else {
         // reality: flm[l, -m] = (-1)^m conj(flm[l, m])
         const R2* A = reinterpret_cast<const R2*>(p.acc);
-        const R2 a = A[(((size_t)b * C + j) * L + am) * Q + q];
+        const R2 a = A[(size_t)b * slice + cell];
         ar = a.x;
         ai = a.y;
         conj_mirror = true;
