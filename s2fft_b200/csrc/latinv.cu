@@ -1,0 +1,311 @@
+// Inverse latitudinal step (synthesis of ring spectra from flm), blocked tiling.
+//
+// Same recursion and projection as upstream s2fft
+// (s2fft/transforms/otf_recursions.py:15-171, inverse_latitudinal_step;
+// coefficients s2fft/recursions/price_mcewen.py:118-255):
+// ftm[theta, m] = sum_l d^l_{m,n}(theta) flm'[l, m], n = -spin, with d generated
+// by the m-recursion from the seeds d^l_{l,n}(theta).
+//
+// B200 formulation (own design):
+//  * lanes run along theta (T rings per lane), and every lane of a warp holds the
+//    same K = 16 degrees (8 consecutive ones from each of the CTA's two 32-degree
+//    blocks p and NB-1-p, so all warps stay busy), so the coefficient loads h_{l,m} and
+//    flm'[l, m] are shared-memory broadcasts and the sum over l stays in
+//    registers over 16 terms before warps' partial sums meet in shared memory;
+//  * states carry the monic mantissa and an exponent (value = v 2^(kScale e)) as
+//    in the seed table; the exponent lives in the gating operand itself: sc = 1
+//    once the state is significant (e >= 0), otherwise sc is the negative
+//    denormal with integer mantissa -e, so x = v * sc stays below 2^-70 and the
+//    exponent costs no register;
+//  * a state is loaded from its seed at kernel start and placed at the first
+//    group start M >= l with the exact continuation of the recursion above m = l
+//    (h_{l,m} = 0 for m > l: dt_{l+2j} = (-1)^j dt_l, dt_{l+2j+1} = 0), so the
+//    warp needs no activation logic; a block's degrees are skipped until the
+//    recursion reaches the block. Partial sums meet every R = 8 steps.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <type_traits>
+
+#include "s2b_dev.h"
+#include "s2b_latfwd.h"
+
+namespace s2b {
+
+template <typename Real>
+struct SigBits;
+template <>
+struct SigBits<float> {
+  // sc for an exponent e < 0 / exponent of a gating operand that is not 1
+  __device__ static float enc(int e) { return __int_as_float((int)(0x80000000u | (unsigned)(-e))); }
+  __device__ static int dec(float sc) { return -(__float_as_int(sc) & 0x7fffff); }
+};
+template <>
+struct SigBits<double> {
+  __device__ static double enc(int e) {
+    return __longlong_as_double((long long)(0x8000000000000000ull | (unsigned long long)(-e)));
+  }
+  __device__ static int dec(double sc) { return -(int)(__double_as_longlong(sc) & 0xfffffff); }
+};
+
+template <typename Real, bool DUAL, int T, int W, int R>
+struct Inv2Layout {
+  using Acc = std::conditional_t<DUAL, typename Vec<Real>::t4, typename Vec<Real>::t2>;
+  static constexpr int K = 16;       // degrees per warp
+  static constexpr int NRT = 32 * T; // rings per CTA
+  static constexpr int NT = W * 32;
+  // stage: h rows [2 blocks][R][32] | coefficient rows [2 blocks][R][32] | lambda [R][NRT]
+  static constexpr size_t h_bytes = 2 * R * kFwdBlock * sizeof(Real);
+  static constexpr size_t f_bytes = 2 * R * kFwdBlock * sizeof(Acc);
+  static constexpr size_t l_bytes = (size_t)R * NRT * sizeof(Real);
+  static constexpr size_t stage_bytes = h_bytes + f_bytes + l_bytes;
+  static constexpr size_t buf_bytes = (size_t)R * W * NRT * sizeof(Acc);
+  static constexpr size_t total = 2 * stage_bytes + buf_bytes + 16;
+  static_assert(W == 4, "two warps per 32-degree block, two blocks per CTA");
+  static_assert(stage_bytes % 16 == 0 && buf_bytes % 16 == 0, "align");
+};
+
+template <typename Real, bool DUAL, int T, int W, int R>
+__global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p) {
+  using Lay = Inv2Layout<Real, DUAL, T, W, R>;
+  using Acc = typename Lay::Acc;
+  using R2 = typename Vec<Real>::t2;
+  using SB = SigBits<Real>;
+  constexpr int K = Lay::K;
+  constexpr int NRT = Lay::NRT;
+  constexpr int NT = Lay::NT;
+  static_assert(R == 8, "the group body below is written for R = 8");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  unsigned char* stage_base = smem_raw;
+  Acc* buf = reinterpret_cast<Acc*>(smem_raw + 2 * Lay::stage_bytes);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_raw + 2 * Lay::stage_bytes + Lay::buf_bytes);
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int wp = tid >> 5;
+  const int L = p.L;
+  const int NB = p.NB;
+  const int TR = tab_rows(L);
+  const int r0 = (int)blockIdx.x * NRT;
+  const int kb0 = (int)blockIdx.y, kb1 = NB - 1 - (int)blockIdx.y;
+  const int half = (int)(blockIdx.z % p.nhalf);
+  const int b = (int)(blockIdx.z / p.nhalf);
+
+  // degrees of this warp: slot k < 8 -> l = 32 kb0 + 8 wp + k, slot k >= 8 -> 32 kb1 + 8 wp + k - 8,
+  // so every warp works on both blocks of the CTA
+  const int col0 = wp * (K / 2);
+  auto slot_l = [&](int k) { return (k < K / 2 ? kb0 : kb1) * kFwdBlock + col0 + (k % (K / 2)); };
+  // first group start of each block (all states of a block join the recursion there)
+  int Mb[2];
+#pragma unroll
+  for (int x = 0; x < 2; ++x) {
+    const int base = (x ? kb1 : kb0) * kFwdBlock;
+    const int top = base + kFwdBlock - 1 < L ? base + kFwdBlock - 1 : L - 1;
+    Mb[x] = base < L ? (top | (R - 1)) : -1;
+  }
+  const int mtop = Mb[0] > Mb[1] ? Mb[0] : Mb[1];
+  if (mtop < 0) return;  // padding pair (uniform)
+  const int ngroups = (mtop + 1) / R;
+
+  // states from the seeds, placed at the block's first group start
+  Real v[K][T], w[K][T], sc[K][T];
+  {
+    const SeedT<Real>* __restrict__ seeds = reinterpret_cast<const SeedT<Real>*>(p.seeds);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int l = slot_l(k);
+      const int M = Mb[k / (K / 2)];
+#pragma unroll
+      for (int i = 0; i < T; ++i) {
+        const int r = r0 + lane * T + i;
+        SeedT<Real> sd{Real(0), 0};
+        if (l < L && r < p.nrings)
+          sd = seeds[(((size_t)half * p.C + l % p.C) * p.Qp + l / p.C) * p.nrings + r];
+        const int dlt = M - l;
+        Real cur = Real(0), prv = Real(0);
+        if ((dlt & 1) == 0)
+          cur = ((dlt >> 1) & 1) ? -sd.v : sd.v;
+        else
+          prv = (((dlt + 1) >> 1) & 1) ? -sd.v : sd.v;
+        v[k][i] = cur;
+        w[k][i] = prv;
+        sc[k][i] = sd.e >= 0 ? Real(1) : SB::enc(sd.e);
+      }
+    }
+  }
+
+  const Real* __restrict__ Hb = reinterpret_cast<const Real*>(p.Hb);
+  const Acc* __restrict__ Fin =
+      reinterpret_cast<const Acc*>(p.F) + ((size_t)b * p.nhalf + half) * NB * TR * kFwdBlock;
+  const Real* __restrict__ lamh = reinterpret_cast<const Real*>(p.lam) + (size_t)half * TR * p.Ls;
+  int nlam = p.Ls - r0;
+  if (nlam > NRT) nlam = NRT;
+
+  auto issue = [&](int g) {
+    unsigned char* st = stage_base + (size_t)(g & 1) * Lay::stage_bytes;
+    const int row0 = mtop - g * R - R + 1 + kPadLo;
+    constexpr unsigned hb = R * kFwdBlock * sizeof(Real);
+    constexpr unsigned fb = R * kFwdBlock * sizeof(Acc);
+    const unsigned bytes = 2 * hb + 2 * fb + (unsigned)(R * nlam * sizeof(Real));
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(&mbar[g & 1], bytes);
+    bulk_g2s(st, Hb + ((size_t)kb0 * TR + row0) * kFwdBlock, hb, &mbar[g & 1]);
+    bulk_g2s(st + hb, Hb + ((size_t)kb1 * TR + row0) * kFwdBlock, hb, &mbar[g & 1]);
+    bulk_g2s(st + Lay::h_bytes, Fin + ((size_t)kb0 * TR + row0) * kFwdBlock, fb, &mbar[g & 1]);
+    bulk_g2s(st + Lay::h_bytes + fb, Fin + ((size_t)kb1 * TR + row0) * kFwdBlock, fb,
+             &mbar[g & 1]);
+    unsigned char* ldst = st + Lay::h_bytes + Lay::f_bytes;
+#pragma unroll
+    for (int s = 0; s < R; ++s)
+      bulk_g2s(ldst + (size_t)s * NRT * sizeof(Real), lamh + (size_t)(row0 + s) * p.Ls + r0,
+               (unsigned)(nlam * sizeof(Real)), &mbar[g & 1]);
+  };
+  for (size_t x = tid * 16; x < 2 * Lay::stage_bytes; x += (size_t)NT * 16)
+    *reinterpret_cast<uint4*>(stage_base + x) = make_uint4(0, 0, 0, 0);
+  __syncthreads();
+  if (tid == 0) {
+    mbar_init(&mbar[0], 1);
+    mbar_init(&mbar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0) {
+    issue(0);
+    if (ngroups > 1) issue(1);
+  }
+  // highest degree of the CTA: partial sums above it are zero
+  int lmax = -1;
+  if (kb0 * kFwdBlock < L) lmax = kb0 * kFwdBlock + kFwdBlock - 1;
+  if (kb1 * kFwdBlock < L && kb1 * kFwdBlock + kFwdBlock - 1 > lmax)
+    lmax = kb1 * kFwdBlock + kFwdBlock - 1;
+  if (lmax > L - 1) lmax = L - 1;
+
+  for (int grp = 0; grp < ngroups; ++grp) {
+    const int mgrp = mtop - grp * R;
+    const bool ok = mbar_wait(&mbar[grp & 1], (grp >> 1) & 1);
+    const unsigned char* st = stage_base + (size_t)(grp & 1) * Lay::stage_bytes;
+    const Real* hS = reinterpret_cast<const Real*>(st) + col0;
+    const Acc* fS = reinterpret_cast<const Acc*>(st + Lay::h_bytes) + col0;
+    const Real* lS = reinterpret_cast<const Real*>(st + Lay::h_bytes + Lay::f_bytes) + lane * T;
+
+#define S2B_INV2_STEP(CUR, PRV, S)                                                      \
+  {                                                                                     \
+    constexpr int srow = R - 1 - (S);                                                   \
+    const int m = mgrp - (S);                                                           \
+    Real lam[T];                                                                        \
+    _Pragma("unroll") for (int i = 0; i < T; ++i) lam[i] = lS[srow * NRT + i];          \
+    Acc a[2][T]; /* one partial sum per block: two independent FMA chains */            \
+    _Pragma("unroll") for (int i = 0; i < T; ++i) {                                     \
+      a[0][i] = zero_acc<Acc>();                                                        \
+      a[1][i] = zero_acc<Acc>();                                                        \
+    }                                                                                   \
+    _Pragma("unroll") for (int x = 1; x >= 0; --x) {                                    \
+      if (m <= Mb[x]) {                                                                 \
+        _Pragma("unroll") for (int kk = 0; kk < K / 2; ++kk) {                          \
+          const int k = x * (K / 2) + kk;                                               \
+          const int so = (x * R + srow) * kFwdBlock + kk;                               \
+          const Real h = hS[so];                                                        \
+          const Acc f = fS[so];                                                         \
+          _Pragma("unroll") for (int i = 0; i < T; ++i) {                               \
+            const Real xv = CUR[k][i] * sc[k][i];                                       \
+            acc_fma(a[x][i], xv, f);                                                    \
+            PRV[k][i] = fma(lam[i] * h, CUR[k][i], -PRV[k][i]);                         \
+          }                                                                             \
+        }                                                                               \
+      }                                                                                 \
+    }                                                                                   \
+    _Pragma("unroll") for (int i = 0; i < T; ++i) {                                     \
+      acc_add(a[0][i], a[1][i]);                                                        \
+      buf[((S) * W + wp) * NRT + lane * T + i] = a[0][i];                               \
+    }                                                                                   \
+  }
+    S2B_INV2_STEP(v, w, 0)
+    S2B_INV2_STEP(w, v, 1)
+    S2B_INV2_STEP(v, w, 2)
+    S2B_INV2_STEP(w, v, 3)
+    S2B_INV2_STEP(v, w, 4)
+    S2B_INV2_STEP(w, v, 5)
+    S2B_INV2_STEP(v, w, 6)
+    S2B_INV2_STEP(w, v, 7)
+#undef S2B_INV2_STEP
+
+    if (!__syncthreads_and(ok)) {
+      if (tid == 0) {
+        atomicExch(p.status, 1);
+        mbar_wait(&mbar[(grp + 1) & 1], ((grp + 1) >> 1) & 1);
+      }
+      return;
+    }
+    // warps' partial sums -> ring spectra
+    for (int it = tid; it < R * NRT; it += NT) {
+      const int S = it / NRT;
+      const int rr = it % NRT;
+      const int m = mgrp - S;
+      const int r = r0 + rr;
+      if (m < 0 || m > lmax || r >= p.nrings) continue;
+      Acc s = buf[(S * W + 0) * NRT + rr];
+#pragma unroll
+      for (int x = 1; x < W; ++x) acc_add(s, buf[(S * W + x) * NRT + rr]);
+      R2* ftm = reinterpret_cast<R2*>(p.ftm) + ((size_t)b * p.nrows + p.ring_row[r]) * p.ncol;
+      R2 ap;
+      ap.x = s.x;
+      ap.y = s.y;
+      if constexpr (DUAL) {
+        R2 an;
+        an.x = s.z;
+        an.y = s.w;
+        red_add(ftm + (L - 1 + m + p.mo), ap);
+        if (m > 0) red_add(ftm + (L - 1 - m + p.mo), an);
+      } else {
+        if (half == 0)
+          red_add(ftm + (L - 1 + m + p.mo), ap);
+        else if (m > 0)
+          red_add(ftm + (L - 1 - m + p.mo), ap);
+      }
+    }
+    __syncthreads();
+    if (tid == 0 && grp + 2 < ngroups) issue(grp + 2);
+    // renormalise states whose mantissa grew past the trigger (only states below
+    // significance grow that far)
+    Real mx = Real(0);
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+#pragma unroll
+      for (int i = 0; i < T; ++i) mx = fmax(mx, fabs(v[k][i]));
+    const Real trig = Scaling<Real>::kTrig;
+    if (mx > trig) {
+      const Real down = Scaling<Real>::kDown;
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+#pragma unroll
+        for (int i = 0; i < T; ++i)
+          if (fabs(v[k][i]) > trig) {
+            v[k][i] *= down;
+            w[k][i] *= down;
+            const int e = SB::dec(sc[k][i]) + 1;
+            sc[k][i] = e >= 0 ? Real(1) : SB::enc(e);
+          }
+    }
+  }
+}
+
+template <typename Real, bool DUAL, int T>
+static cudaError_t launch_inv2_cfg(const Inv2Params& p, cudaStream_t s) {
+  using Lay = Inv2Layout<Real, DUAL, T, 4, 8>;
+  auto kern = lat_inv2_kernel<Real, DUAL, T, 4, 8>;
+  cudaError_t err =
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::total);
+  if (err != cudaSuccess) return err;
+  dim3 grid((p.nrings + Lay::NRT - 1) / Lay::NRT, p.NB / 2, p.nhalf * p.batch);
+  kern<<<grid, Lay::NT, Lay::total, s>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_inv2(bool fp64, bool dual, const Inv2Params& p, cudaStream_t s) {
+  if (p.nrings <= 0) return cudaSuccess;
+  if (!fp64)
+    return dual ? launch_inv2_cfg<float, true, 2>(p, s) : launch_inv2_cfg<float, false, 2>(p, s);
+  return dual ? launch_inv2_cfg<double, true, 1>(p, s) : launch_inv2_cfg<double, false, 1>(p, s);
+}
+
+}  // namespace s2b

@@ -35,11 +35,6 @@
 
 namespace s2b {
 
-template <typename Real>
-struct SeedT {
-  Real v;
-  int e;
-};
 
 // ---------------------------------------------------------------------------
 // Seeds d^l_{l,n}(theta) = (-1)^(l-n) sqrt(binom(2l, l+n)) cos^(l+n)(t/2) sin^(l-n)(t/2)

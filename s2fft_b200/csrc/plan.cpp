@@ -771,31 +771,34 @@ static int run_inverse(s2b_plan* p, const void* flm, void* f, char* ws, cudaStre
   sp.flm = flm;
   sp.F = F;
   sp.ftm = ftm;
+  // blocked coefficient table for the latitudinal kernel: [NB][row][32], l = 32 block + column
+  sp.nclass = p->fwd_NB;
+  sp.Q = kFwdBlock;
+  sp.Lp = p->fwd_NB * kFwdBlock;
   S2B_CK(launch_prologue(p->fp64, sp, s));
   S2B_CK(launch_poles(p->fp64, sp, s));
   if (p->inv_nrings > 0) {
-    LatParams lp{};
+    Inv2Params lp{};
     lp.L = L;
-    lp.L0 = d.L_lower;
-    lp.spin = d.spin;
     lp.nrings = p->inv_nrings;
     lp.nhalf = p->nhalf;
     lp.batch = d.batch;
-    lp.rings = p->inv_rings;
-    lp.ring_row = p->inv_ring_row;
+    lp.NB = p->fwd_NB;
+    lp.C = p->nclass;
+    lp.Qp = p->Q;
     lp.seeds = p->inv_seeds;
-    lp.H = p->htab;
-    lp.in = F;
-    lp.out = ftm;
+    lp.Hb = p->fwd_Hb;
+    lp.lam = p->inv_lam;
+    lp.Ls = p->inv_Ls;
+    lp.F = F;
+    lp.ftm = ftm;
+    lp.ring_row = p->inv_ring_row;
     lp.nrows = p->nth;
     lp.ncol = p->inv_ncol;
     lp.mo = p->inv_mo;
-    lp.reality = d.reality;
     lp.status = p->status;
-    lp.lam = p->inv_lam;
-    lp.Ls = p->inv_Ls;
     if (p->ev_begin[0]) S2B_CK(cudaEventRecord(p->ev_begin[0], s));
-    S2B_CK(launch_latitudinal(p->fp64, false, p->dual, lp, s));
+    S2B_CK(launch_inv2(p->fp64, p->dual, lp, s));
     if (p->ev_end[0]) S2B_CK(cudaEventRecord(p->ev_end[0], s));
   }
   RowsParams<Real> rp{};

@@ -39,6 +39,22 @@ struct Fwd2Params {
   int* status;
 };
 
+// Inverse latitudinal step, blocked layout (latinv.cu).
+struct Inv2Params {
+  int L, nrings, nhalf, batch, NB;
+  int C, Qp;                // seed table geometry: [nhalf][C][Qp][nrings], l = j + C q
+  const void* seeds;        // {mantissa, exponent} of d^l_{l,n}(theta)
+  const void* Hb;           // [NB][tab_rows][32]
+  const void* lam;          // [nhalf][tab_rows][Ls]
+  int Ls;
+  const void* F;            // [batch][nhalf][NB][tab_rows][32] coefficients (Real4 when dual)
+  void* ftm;                // [batch][nrows][ncol] ring spectra, accumulated with atomics
+  const int* ring_row;
+  int nrows, ncol, mo;
+  int* status;
+};
+cudaError_t launch_inv2(bool fp64, bool dual, const Inv2Params& p, cudaStream_t s);
+
 cudaError_t launch_fwd_start(bool fp64, const FwdStartParams& p, cudaStream_t s);
 cudaError_t launch_fwd2(bool fp64, bool dual, const Fwd2Params& p, cudaStream_t s);
 size_t fwd_start_bytes(bool fp64, int L, int nhalf, int nrings);

@@ -12,7 +12,8 @@ struct StageParams {
   int nhalf, dual;
   int nrows, ncol, mo;  // ftm / G row count, ftm columns, column offset
   int pole_south, pole_north;  // rows of the closed-form pole rings (-1: none)
-  int Lp;               // forward sums layout: 0 = [C][m][Q] classes, > 0 = [m][Lp] by degree
+  int Lp;               // 0: class layouts (l = j + C q); > 0: blocked layouts, inverse table
+                        // F [C blocks][m][Q = 32] with l = 32 j + q, forward sums [m][Lp] by l
   const double* g;      // [m][l] monic scale g_{l,m}
   const void* flm;      // inverse input  [b][L][2L-1]
   void* F;              // inverse recursion table

@@ -43,7 +43,7 @@ __global__ void prologue_kernel(StageParams p) {
     r /= C;
     const int half = (int)(r % p.nhalf);
     const int b = (int)(r / p.nhalf);
-    const int l = j + C * q;
+    const int l = p.Lp > 0 ? j * Q + q : j + C * q;  // blocked: l = 32 block + column
     const int as = p.spin < 0 ? -p.spin : p.spin;
     const bool ok = m >= 0 && m < L && l < L && l >= m && l >= p.L0 && l >= as;
     double g = 0.0;
