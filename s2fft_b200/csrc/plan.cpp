@@ -678,7 +678,8 @@ static int build_plan(s2b_plan* p) {
   if ((rc = upload_complex(p, &p->chirp, fb.chirp))) return rc;
   if ((rc = upload_complex(p, &p->bf, fb.bf))) return rc;
   const size_t maxsmem = (size_t)227 * 1024;
-  if ((size_t)p->maxM * 2 * p->rsz > maxsmem || (size_t)(p->M1 + p->M2) * 2 * p->rsz > maxsmem)
+  auto padded = [](int M) { return (size_t)M + (size_t)(M >> 3); };  // ring FFT buffer layout
+  if (padded(p->maxM) * 2 * p->rsz > maxsmem || (padded(p->M1) + padded(p->M2)) * 2 * p->rsz > maxsmem)
     return fail(S2B_ERR_INVALID, "band-limit too large for the shared-memory ring FFT");
 
   // ---- precompute-kernel geometry (tables include the pole rings)

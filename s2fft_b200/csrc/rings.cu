@@ -77,41 +77,96 @@ __device__ __forceinline__ R2 czero() {
   return r;
 }
 
-// tw[k] = exp(-2 pi i k / M), k < M/2. DIF: natural order in, bit-reversed out.
-template <typename R2>
-__device__ void fft_dif(R2* s, int M, const R2* __restrict__ tw, bool inv) {
-  for (int half = M >> 1, stride = 1; half >= 1; half >>= 1, stride <<= 1) {
-    __syncthreads();
-    for (int t = threadIdx.x; t < (M >> 1); t += blockDim.x) {
-      const int pos = t & (half - 1);
-      const int i0 = ((t - pos) << 1) + pos;
-      const int i1 = i0 + half;
-      const R2 a = s[i0], b = s[i1];
-      R2 w = tw[pos * stride];
-      if (inv) w.y = -w.y;
-      s[i0] = cadd(a, b);
-      s[i1] = cmul(csub(a, b), w);
+// Shared-memory layout of a transform buffer: one padding slot per 8 elements,
+// so that the contiguous 8-element groups of the last DIF / first DIT pass fall
+// into distinct banks. A buffer for length M holds M + M/8 elements.
+__device__ __forceinline__ int pidx(int e) { return e + (e >> 3); }
+__host__ __device__ inline int padded_len(int M) { return M + (M >> 3); }
+
+// Radix-2 butterflies fused NS <= 3 stages per pass: a thread loads the 2^NS
+// elements base + a q that NS consecutive stages combine, runs the stages in
+// registers and writes them back in place (same data order as plain radix-2),
+// so a length-4096 transform takes 4 passes and 4 barriers instead of 12.
+// tw[k] = exp(-2 pi i k / M), k < M/2.
+//
+// DIF stage of span hs: (x, x + hs) -> (x + y, (x - y) w), w = tw[(x mod hs) M / (2 hs)],
+// spans decreasing (h, h/2, ...); DIT stage: (x, x + hs) -> (x + y w, x - y w), spans
+// increasing (q, 2q, ...). In both, the pass covers elements base + a q, a < 2^NS.
+template <int NS, bool DIF, typename R2>
+__device__ __forceinline__ void fft_pass(R2* s, int M, int q, const R2* __restrict__ tw, bool inv,
+                                         const R2* __restrict__ post) {
+  constexpr int NA = 1 << NS;
+  const int h = q << (NS - 1);  // largest span of the pass
+  for (int g = threadIdx.x; g < (M >> NS); g += blockDim.x) {
+    const int r = g % q;
+    const int base = (g / q) * (2 * h) + r;
+    R2 x[NA];
+#pragma unroll
+    for (int a = 0; a < NA; ++a) x[a] = s[pidx(base + a * q)];
+#pragma unroll
+    for (int j = 0; j < NS; ++j) {
+      const int sj = DIF ? (1 << (NS - 1 - j)) : (1 << j);  // pair distance in units of q
+      const int stride = M / (2 * sj * q);
+#pragma unroll
+      for (int a = 0; a < NA; ++a) {
+        if (a & sj) continue;
+        R2 w = tw[(r + (a & (sj - 1)) * q) * stride];
+        if (inv) w.y = -w.y;
+        if (DIF) {
+          const R2 u = x[a], v = x[a + sj];
+          x[a] = cadd(u, v);
+          x[a + sj] = cmul(csub(u, v), w);
+        } else {
+          const R2 u = x[a];
+          const R2 v = cmul(x[a + sj], w);
+          x[a] = cadd(u, v);
+          x[a + sj] = csub(u, v);
+        }
+      }
     }
+#pragma unroll
+    for (int a = 0; a < NA; ++a) {
+      const int e = base + a * q;
+      s[pidx(e)] = post ? cmul(x[a], post[e]) : x[a];
+    }
+  }
+}
+
+// DIF: natural order in, bit-reversed out; if post != nullptr the output element
+// e (bit-reversed position) is multiplied by post[e] in the last pass.
+template <typename R2>
+__device__ void fft_dif(R2* s, int M, int logM, const R2* __restrict__ tw, bool inv,
+                        const R2* __restrict__ post = nullptr) {
+  for (int done = 0; done < logM;) {
+    const int ns = logM - done < 3 ? logM - done : 3;
+    const int q = M >> (done + ns);  // span of the last fused stage
+    const R2* pp = done + ns == logM ? post : nullptr;
+    __syncthreads();
+    if (ns == 3)
+      fft_pass<3, true>(s, M, q, tw, inv, pp);
+    else if (ns == 2)
+      fft_pass<2, true>(s, M, q, tw, inv, pp);
+    else
+      fft_pass<1, true>(s, M, q, tw, inv, pp);
+    done += ns;
   }
   __syncthreads();
 }
 
 // DIT: bit-reversed order in, natural out.
 template <typename R2>
-__device__ void fft_dit(R2* s, int M, const R2* __restrict__ tw, bool inv) {
-  for (int half = 1, stride = M >> 1; half < M; half <<= 1, stride >>= 1) {
+__device__ void fft_dit(R2* s, int M, int logM, const R2* __restrict__ tw, bool inv) {
+  for (int done = 0; done < logM;) {
+    const int ns = logM - done < 3 ? logM - done : 3;
+    const int q = 1 << done;  // span of the first fused stage
     __syncthreads();
-    for (int t = threadIdx.x; t < (M >> 1); t += blockDim.x) {
-      const int pos = t & (half - 1);
-      const int i0 = ((t - pos) << 1) + pos;
-      const int i1 = i0 + half;
-      R2 w = tw[pos * stride];
-      if (inv) w.y = -w.y;
-      const R2 a = s[i0];
-      const R2 b = cmul(s[i1], w);
-      s[i0] = cadd(a, b);
-      s[i1] = csub(a, b);
-    }
+    if (ns == 3)
+      fft_pass<3, false>(s, M, q, tw, inv, (const R2*)nullptr);
+    else if (ns == 2)
+      fft_pass<2, false>(s, M, q, tw, inv, (const R2*)nullptr);
+    else
+      fft_pass<1, false>(s, M, q, tw, inv, (const R2*)nullptr);
+    done += ns;
   }
   __syncthreads();
 }
@@ -136,18 +191,17 @@ __device__ void dft_run(typename C2<Real>::t* s, const FFTDesc& d, const FFTTabl
         if (inv) x = cconj(x);
         x = cmul(x, ch[k]);
       }
-      s[k] = x;
+      s[pidx(k)] = x;
     }
-    fft_dif(s, d.M, tw, false);
-    for (int k = threadIdx.x; k < d.M; k += blockDim.x) s[k] = cmul(s[k], bf[k]);
-    fft_dit(s, d.M, tw, true);
+    fft_dif(s, d.M, d.logM, tw, false, bf);
+    fft_dit(s, d.M, d.logM, tw, true);
   } else {
     for (int k = threadIdx.x; k < d.M; k += blockDim.x) {
       R2 x = load(k);
       if (inv) x = cconj(x);
-      s[k] = x;
+      s[pidx(k)] = x;
     }
-    fft_dif(s, d.M, tw, false);
+    fft_dif(s, d.M, d.logM, tw, false);
   }
 }
 
@@ -159,9 +213,9 @@ __device__ __forceinline__ typename C2<Real>::t dft_get(const typename C2<Real>:
   using R2 = typename C2<Real>::t;
   R2 x;
   if (d.bluestein)
-    x = cmul(s[j], tb.chirp[d.chirp_off + j]);
+    x = cmul(s[pidx(j)], tb.chirp[d.chirp_off + j]);
   else
-    x = s[bitrev(j, d.logM)];
+    x = s[pidx(bitrev(j, d.logM))];
   return inv ? cconj(x) : x;
 }
 
@@ -373,7 +427,7 @@ __global__ void mw_cols_kernel(ColsParams<Real> p) {
   const FFTDesc d1 = *p.d1;
   const FFTDesc d2 = *p.d2;
   R2* s1 = reinterpret_cast<R2*>(smem_raw);
-  R2* s2 = s1 + d1.M;
+  R2* s2 = s1 + padded_len(d1.M);
   const int L = p.L;
   const int mlo = p.mw ? -(L - 1) : -L;
   const int ncm = L - mlo;
@@ -482,7 +536,7 @@ __global__ void mw_cols_kernel(ColsParams<Real> p) {
 // launchers
 // ---------------------------------------------------------------------------
 static int fft_threads(int M) {
-  int t = M / 2;
+  int t = M / 8;
   if (t > 512) t = 512;
   if (t < 32) t = 32;
   return t;
@@ -492,7 +546,7 @@ template <typename Real>
 cudaError_t launch_inv_rows(const RowsParams<Real>& p, int nrings, int batch, int maxM,
                             cudaStream_t s) {
   using R2 = typename C2<Real>::t;
-  const size_t smem = (size_t)maxM * sizeof(R2);
+  const size_t smem = (size_t)padded_len(maxM) * sizeof(R2);
   cudaError_t e = cudaFuncSetAttribute(inv_rows_kernel<Real>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -504,7 +558,7 @@ template <typename Real>
 cudaError_t launch_fwd_rows(const RowsParams<Real>& p, int nrings, int batch, int maxM,
                             cudaStream_t s) {
   using R2 = typename C2<Real>::t;
-  const size_t smem = (size_t)maxM * sizeof(R2);
+  const size_t smem = (size_t)padded_len(maxM) * sizeof(R2);
   cudaError_t e = cudaFuncSetAttribute(fwd_rows_kernel<Real>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -516,7 +570,7 @@ template <typename Real>
 cudaError_t launch_mw_cols(const ColsParams<Real>& p, int ncm, int batch, int M1, int M2,
                            cudaStream_t s) {
   using R2 = typename C2<Real>::t;
-  const size_t smem = (size_t)(M1 + M2) * sizeof(R2);
+  const size_t smem = (size_t)(padded_len(M1) + padded_len(M2)) * sizeof(R2);
   cudaError_t e = cudaFuncSetAttribute(mw_cols_kernel<Real>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
