@@ -363,6 +363,7 @@ struct s2b_plan {
   void* chirp = nullptr;
   void* bf = nullptr;
   int row_desc = 0, col_d1 = 0, col_d2 = 0, maxM = 2, M1 = 2, M2 = 2;
+  void* col_ph = nullptr;  // column chain: chirp * half-sample phase / n1 per 4L-bin
   // precompute path: ring colatitudes of the kernel tables, table width
   double* kth_inv = nullptr;
   double* kth_fwd = nullptr;
@@ -677,6 +678,23 @@ static int build_plan(s2b_plan* p) {
   if ((rc = upload_complex(p, &p->tw, fb.tw))) return rc;
   if ((rc = upload_complex(p, &p->chirp, fb.chirp))) return rc;
   if ((rc = upload_complex(p, &p->bf, fb.bf))) return rc;
+  if (p->fwd_mode != 0) {
+    // factor applied to theta-DFT bin pp (stored at k = pp mod 4L) before the
+    // inverse 4L DFT: Bluestein output chirp, MW half-sample shift exp(-i pp pi/(2L-1)),
+    // and 1/n1
+    const FFTDesc& d1 = fb.descs[p->col_d1];
+    const int n1 = d1.n, n2 = 4 * L;
+    const int plo = p->fwd_mode == 1 ? -(L - 1) : -L, phi = L - 1;
+    std::vector<cd> ph(n2, cd(0.0, 0.0));
+    for (int pp = plo; pp <= phi; ++pp) {
+      const int j = ((pp % n1) + n1) % n1;
+      cd f(1.0 / n1, 0.0);
+      if (d1.bluestein) f *= fb.chirp[d1.chirp_off + j];
+      if (p->fwd_mode == 1) f *= std::polar(1.0, -kPi * (double)pp / (2.0 * L - 1.0));
+      ph[(pp + n2) % n2] = f;
+    }
+    if ((rc = upload_complex(p, &p->col_ph, ph))) return rc;
+  }
   const size_t maxsmem = (size_t)227 * 1024;
   auto padded = [](int M) { return (size_t)M + (size_t)(M >> 3); };  // ring FFT buffer layout
   if (padded(p->maxM) * 2 * p->rsz > maxsmem || (padded(p->M1) + padded(p->M2)) * 2 * p->rsz > maxsmem)
@@ -873,6 +891,7 @@ static int run_forward_once(s2b_plan* p, const void* f, void* flm, char* ws, cud
     cp.scale = p->fwd_mode == 1 ? (2.0 * L) / (2.0 * L - 1.0) : 1.0;
     cp.d1 = p->descs + p->col_d1;
     cp.d2 = p->descs + p->col_d2;
+    cp.ph = p->col_ph;
     cp.weights = p->fwd_weights;
     cp.tb = tables<Real>(p);
     cp.in = cols;
@@ -1066,6 +1085,7 @@ static int run_pre_forward(s2b_plan* p, const void* K, const void* f, void* flm,
     cp.scale = p->fwd_mode == 1 ? (2.0 * L) / (2.0 * L - 1.0) : 1.0;
     cp.d1 = p->descs + p->col_d1;
     cp.d2 = p->descs + p->col_d2;
+    cp.ph = p->col_ph;
     cp.weights = p->fwd_weights;
     cp.tb = tables<Real>(p);
     cp.in = cols;

@@ -92,26 +92,64 @@ __host__ __device__ inline int padded_len(int M) { return M + (M >> 3); }
 // DIF stage of span hs: (x, x + hs) -> (x + y, (x - y) w), w = tw[(x mod hs) M / (2 hs)],
 // spans decreasing (h, h/2, ...); DIT stage: (x, x + hs) -> (x + y w, x - y w), spans
 // increasing (q, 2q, ...). In both, the pass covers elements base + a q, a < 2^NS.
+// Every twiddle of a pass derives from one table entry b = tw[r M / (2h)]
+// (h = largest span of the pass, r = position of the group): the stage whose
+// pairs are sj q apart uses b^(2^(NS-1)/sj) * exp(-i pi k / sj), k = a mod sj,
+// i.e. powers of b times constant roots of unity of order <= 8.
+template <int S, typename R2>
+__device__ __forceinline__ R2 root_rot(R2 w, int k, bool inv) {
+  // w * exp(-i pi k / S) (conjugate rotation when inv), k < S, S in {1, 2, 4}
+  using Real = decltype(w.x);
+  if (S == 1 || k == 0) return w;
+  const Real c = Real(0.70710678118654752440);
+  R2 o;
+  if (S == 2 || k == 2) {  // -i (or +i)
+    o.x = inv ? -w.y : w.y;
+    o.y = inv ? w.x : -w.x;
+    return o;
+  }
+  if (k == 1) {  // (1 - i)/sqrt2  (inv: (1 + i)/sqrt2)
+    o.x = inv ? (w.x - w.y) * c : (w.x + w.y) * c;
+    o.y = inv ? (w.x + w.y) * c : (w.y - w.x) * c;
+    return o;
+  }
+  // k == 3: (-1 - i)/sqrt2  (inv: (-1 + i)/sqrt2)
+  o.x = inv ? (-w.x - w.y) * c : (w.y - w.x) * c;
+  o.y = inv ? (w.x - w.y) * c : (-w.x - w.y) * c;
+  return o;
+}
+
 template <int NS, bool DIF, typename R2>
 __device__ __forceinline__ void fft_pass(R2* s, int M, int q, const R2* __restrict__ tw, bool inv,
                                          const R2* __restrict__ post) {
   constexpr int NA = 1 << NS;
   const int h = q << (NS - 1);  // largest span of the pass
+  const int s0 = M / (2 * h);
   for (int g = threadIdx.x; g < (M >> NS); g += blockDim.x) {
     const int r = g % q;
     const int base = (g / q) * (2 * h) + r;
     R2 x[NA];
 #pragma unroll
     for (int a = 0; a < NA; ++a) x[a] = s[pidx(base + a * q)];
+    R2 bp[3];  // b, b^2, b^4
+    bp[0] = tw[r * s0];
+    if (inv) bp[0].y = -bp[0].y;
+    bp[1] = cmul(bp[0], bp[0]);
+    bp[2] = cmul(bp[1], bp[1]);
 #pragma unroll
     for (int j = 0; j < NS; ++j) {
       const int sj = DIF ? (1 << (NS - 1 - j)) : (1 << j);  // pair distance in units of q
-      const int stride = M / (2 * sj * q);
+      const int pw = DIF ? j : NS - 1 - j;                  // power index: b^(2^pw)
 #pragma unroll
       for (int a = 0; a < NA; ++a) {
         if (a & sj) continue;
-        R2 w = tw[(r + (a & (sj - 1)) * q) * stride];
-        if (inv) w.y = -w.y;
+        R2 w;
+        if (sj == 4)
+          w = root_rot<4>(bp[pw], a & 3, inv);
+        else if (sj == 2)
+          w = root_rot<2>(bp[pw], a & 1, inv);
+        else
+          w = bp[pw];
         if (DIF) {
           const R2 u = x[a], v = x[a + sj];
           x[a] = cadd(u, v);
@@ -451,24 +489,14 @@ __global__ void mw_cols_kernel(ColsParams<Real> p) {
   const int plo = p.mw ? -(L - 1) : -L;
   const int phi = L - 1;
   const int n2 = d2.n;  // 4L
-  const double inv_n1 = 1.0 / (double)n1;
+  const R2* __restrict__ ph = reinterpret_cast<const R2*>(p.ph);
   auto load2 = [&](int k) -> R2 {
-    // k = p mod 4L for p in [plo, phi]
-    int pp = k <= phi ? k : k - n2;
+    // k = pp mod 4L for pp in [plo, phi]; ph is zero outside
+    const int pp = k <= phi ? k : k - n2;
     if (pp < plo || pp > phi) return czero<R2>();
-    R2 g = dft_get<Real>(s1, d1, p.tb, false, pmod(pp, n1));
-    double re = (double)g.x * inv_n1, im = (double)g.y * inv_n1;
-    if (p.mw) {
-      double sn, cs;
-      sincospi(-(double)pp / (double)(2 * L - 1), &sn, &cs);
-      const double r2 = re * cs - im * sn;
-      im = re * sn + im * cs;
-      re = r2;
-    }
-    R2 o;
-    o.x = (Real)re;
-    o.y = (Real)im;
-    return o;
+    const int j = pmod(pp, n1);
+    const R2 g = d1.bluestein ? s1[pidx(j)] : s1[pidx(bitrev(j, d1.logM))];
+    return cmul(g, ph[k]);
   };
   dft_run<Real>(s2, d2, p.tb, true, load2);
   const int nout = 2 * L + 1;

@@ -66,6 +66,7 @@ struct ColsParams {
   const FFTDesc* d1;    // theta DFT over the periodic extension (2L-1 or 2L)
   const FFTDesc* d2;    // inverse DFT of length 4L
   const double* weights;// 2L+1 MWSS(2L) transform weights
+  const void* ph;       // [4L] complex factor of theta-DFT bin p (at p mod 4L), 0 outside
   FFTTables<Real> tb;
   const void* in;       // Fc [B][ncm][nin]
   void* out;            // G  [B][half][m + kPadLo][Gs]; MWSS(2L) ring t -> row t-1,
