@@ -15,7 +15,7 @@
 //    precision with no exponent bookkeeping, no gating multiply and no
 //    renormalisation: once significant, |dt| stays within [2^-110, 2^10].
 //  * Starts are taken per (ring, block of 32 consecutive l) at the largest first
-//    significant m of the block, rounded up to a group start m = 3 (mod 4), so a
+//    significant m of the block, rounded up to a group start (m = -1 mod R), so a
 //    whole warp starts a ring together. Degrees of the block below that start
 //    begin with the exact continuation of the recursion above m = l
 //    (h_{l,m} = 0 for m > l gives dt_{l+2j} = (-1)^j dt_l, dt_{l+2j+1} = 0).
@@ -23,7 +23,7 @@
 //    spectra and lambda loads are shared-memory broadcasts) x two l blocks
 //    (lane = l within the block, blocks p and NB-1-p for balance). The sum over
 //    the T rings of a thread stays in registers; warps' partial sums meet in
-//    shared memory every R = 4 steps and are added to flm with vector atomics.
+//    shared memory every R steps and are added to flm with vector atomics.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -94,7 +94,7 @@ __global__ void fwd_start_kernel(const FwdStartParams p) {
   }
   // pass 2: common start of the block on this ring, aligned to a group start
   int M = __reduce_max_sync(0xffffffffu, ms);
-  if (M >= 0) M |= 3;
+  if (M >= 0) M |= p.group - 1;
 
   // pass 3: (dt_M, dt_{M+1}) of this degree
   double cur = 0.0, prv = 0.0;
@@ -155,7 +155,7 @@ struct Fwd2Layout {
   static constexpr size_t act_bytes = (size_t)W * 2 * T * sizeof(int);
   static constexpr size_t total = 2 * stage_bytes + buf_bytes + act_bytes + 16 + 16;
   static_assert(stage_bytes % 16 == 0 && buf_bytes % 16 == 0 && act_bytes % 16 == 0, "align");
-  static_assert(2 * T <= 32, "act table is held by the first 2T lanes");
+  static_assert((2 * T) % 32 == 0 || 2 * T < 32, "act entries are spread over the lanes");
 };
 
 // One recursion step over the T rings of slot k: cur = dt_m, prv = dt_{m+1} -> dt_{m-1};
@@ -180,7 +180,8 @@ __global__ void __launch_bounds__(W * 32, sizeof(Real) == 4 ? 4 : 3)
   using R2 = typename Vec<Real>::t2;
   constexpr int NRT = Lay::NRT;
   constexpr int NT = Lay::NT;
-  static_assert(R == 4, "the group body below is written for R = 4");
+  static_assert(R == 4 || R == 8, "the group body below is written for R = 4 or 8");
+  constexpr int U = (2 * T + 31) / 32;  // act entries per lane: entry e = lane + 32 u -> (k, i) = (e / T, e % T)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char* stage_base = smem_raw;
   Acc* buf = reinterpret_cast<Acc*>(smem_raw + 2 * Lay::stage_bytes);
@@ -206,15 +207,21 @@ __global__ void __launch_bounds__(W * 32, sizeof(Real) == 4 ? 4 : 3)
   const int b = (int)(blockIdx.z / p.nhalf);
 
   // start m of every (slot, ring) of this warp: lane < 2T holds (k, i) = (lane / T, lane % T)
-  int a_m = -1;
-  if (lane < 2 * T) {
-    const int k = lane / T, i = lane % T;
-    const int r = r0 + wp * T + i;
-    if (r < p.nrings) a_m = p.Mst[((size_t)half * NB + (k ? kb1 : kb0)) * p.nrings + r];
-    act[(wp * 2 + k) * T + i] = a_m;
+  int a_m[U];
+  int mt0 = -1, mt1 = -1;
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    const int e = lane + 32 * u;
+    a_m[u] = -1;
+    if (e < 2 * T) {
+      const int k = e / T, i = e % T;
+      const int r = r0 + wp * T + i;
+      if (r < p.nrings) a_m[u] = p.Mst[((size_t)half * NB + (k ? kb1 : kb0)) * p.nrings + r];
+      act[(wp * 2 + k) * T + i] = a_m[u];
+    }
+    mt0 = max(mt0, __reduce_max_sync(0xffffffffu, (e < T) ? a_m[u] : -1));
+    mt1 = max(mt1, __reduce_max_sync(0xffffffffu, (e >= T && e < 2 * T) ? a_m[u] : -1));
   }
-  const int mt0 = __reduce_max_sync(0xffffffffu, lane < T ? a_m : -1);
-  const int mt1 = __reduce_max_sync(0xffffffffu, (lane >= T && lane < 2 * T) ? a_m : -1);
   if (tid == 0) {
     mk[0] = -1;
     mk[1] = -1;
@@ -302,7 +309,11 @@ __global__ void __launch_bounds__(W * 32, sizeof(Real) == 4 ? 4 : 3)
             v[k][i] = sv.x;
             w[k][i] = sv.y;
           }
-      next_act = __reduce_max_sync(0xffffffffu, (lane < 2 * T && a_m < mgrp) ? a_m : -1);
+      int na = -1;
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (lane + 32 * u < 2 * T && a_m[u] < mgrp && a_m[u] > na) na = a_m[u];
+      next_act = __reduce_max_sync(0xffffffffu, na);
     }
     const unsigned char* st = stage_base + (size_t)(grp & 1) * Lay::stage_bytes;
     const Real* hS = reinterpret_cast<const Real*>(st);
@@ -325,6 +336,12 @@ __global__ void __launch_bounds__(W * 32, sizeof(Real) == 4 ? 4 : 3)
     S2B_FWD2_STEP(w, v, 1)
     S2B_FWD2_STEP(v, w, 2)
     S2B_FWD2_STEP(w, v, 3)
+    if constexpr (R == 8) {
+      S2B_FWD2_STEP(v, w, 4)
+      S2B_FWD2_STEP(w, v, 5)
+      S2B_FWD2_STEP(v, w, 6)
+      S2B_FWD2_STEP(w, v, 7)
+    }
 #undef S2B_FWD2_STEP
 
     if (!__syncthreads_and(ok)) {
@@ -352,10 +369,10 @@ __global__ void __launch_bounds__(W * 32, sizeof(Real) == 4 ? 4 : 3)
   }
 }
 
-template <typename Real, bool DUAL, int T, int W>
+template <typename Real, bool DUAL, int T, int W, int R>
 static cudaError_t launch_fwd2_cfg(const Fwd2Params& p, cudaStream_t s) {
-  using Lay = Fwd2Layout<Real, DUAL, T, W, 4>;
-  auto kern = lat_fwd2_kernel<Real, DUAL, T, W, 4>;
+  using Lay = Fwd2Layout<Real, DUAL, T, W, R>;
+  auto kern = lat_fwd2_kernel<Real, DUAL, T, W, R>;
   cudaError_t err =
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::total);
   if (err != cudaSuccess) return err;
@@ -365,13 +382,15 @@ static cudaError_t launch_fwd2_cfg(const Fwd2Params& p, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+int fwd_group(bool fp64) { return fp64 ? 4 : 8; }
+
 cudaError_t launch_fwd2(bool fp64, bool dual, const Fwd2Params& p, cudaStream_t s) {
   if (p.nrings <= 0) return cudaSuccess;
   if (!fp64)
-    return dual ? launch_fwd2_cfg<float, true, 16, 4>(p, s)
-                : launch_fwd2_cfg<float, false, 16, 4>(p, s);
-  return dual ? launch_fwd2_cfg<double, true, 8, 4>(p, s)
-              : launch_fwd2_cfg<double, false, 8, 4>(p, s);
+    return dual ? launch_fwd2_cfg<float, true, 16, 4, 8>(p, s)
+                : launch_fwd2_cfg<float, false, 16, 4, 8>(p, s);
+  return dual ? launch_fwd2_cfg<double, true, 8, 4, 4>(p, s)
+              : launch_fwd2_cfg<double, false, 8, 4, 4>(p, s);
 }
 
 }  // namespace s2b

@@ -613,6 +613,7 @@ static int build_plan(s2b_plan* p) {
     fp.NB = p->fwd_NB;
     // contributions below 2^-40 (float) / 2^-70 (double) of |d| <= 1 are dropped
     fp.floor_log2 = p->fp64 ? -70.0 : -40.0;
+    fp.group = fwd_group(p->fp64);
     fp.rings = p->fwd_rings;
     fp.lbin = p->lbin;
     fp.g = p->gtab;

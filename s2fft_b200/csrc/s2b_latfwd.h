@@ -13,12 +13,13 @@ constexpr int kFwdBlock = 32;
 __host__ __device__ inline int fwd_nblocks(int L) { return 2 * ((L + 2 * kFwdBlock - 1) / (2 * kFwdBlock)); }
 
 // Start table of the forward recursion.
-//   Mst [nhalf][NB][nrings]      first m of the recursion for (ring, block); m = 3 (mod 4),
+//   Mst [nhalf][NB][nrings]      first m of the recursion for (ring, block), a group start,
 //                                 -1 when no degree of the block is significant on the ring
 //   Vst [nhalf][NB][nrings][32]  (dt_M, dt_{M+1}) of each degree of the block, monic form
 struct FwdStartParams {
   int L, L0, spin, nhalf, nrings, NB;
   double floor_log2;        // |d| below 2^floor_log2 is dropped from the projection
+  int group;                // steps per group of the main kernel (starts are group starts)
   const RingInfo* rings;
   const double* lbin;       // log2 sqrt(binom(2l, l+|s|))
   const double* g;          // [m][l] monic scale
@@ -58,5 +59,6 @@ cudaError_t launch_inv2(bool fp64, bool dual, const Inv2Params& p, cudaStream_t 
 cudaError_t launch_fwd_start(bool fp64, const FwdStartParams& p, cudaStream_t s);
 cudaError_t launch_fwd2(bool fp64, bool dual, const Fwd2Params& p, cudaStream_t s);
 size_t fwd_start_bytes(bool fp64, int L, int nhalf, int nrings);
+int fwd_group(bool fp64);  // steps per group of the forward kernel
 
 }  // namespace s2b
