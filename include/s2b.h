@@ -92,7 +92,8 @@ const char* s2b_last_error(void);
 int s2b_plan_create(const s2b_desc* desc, s2b_plan** plan);
 int s2b_plan_destroy(s2b_plan* plan);
 
-/* Bytes of device workspace an execute call needs (0 allowed). */
+/* Bytes of device workspace an execute call needs (0 allowed); forward selects the
+ * call: 0 s2b_inverse, 1 s2b_forward, 2 s2b_inverse_adjoint, 3 s2b_forward_adjoint. */
 int s2b_workspace_size(const s2b_plan* plan, int forward, size_t* bytes);
 
 /* Spin spherical-harmonic transforms. */
@@ -100,6 +101,20 @@ int s2b_inverse(s2b_plan* plan, const void* flm, void* f, void* workspace,
                 size_t workspace_bytes, void* stream);
 int s2b_forward(s2b_plan* plan, const void* f, void* flm, void* workspace,
                 size_t workspace_bytes, void* stream);
+
+/* Adjoints (conjugate transposes) of the spin transforms, for reverse-mode
+ * differentiation: for a complex-linear map y = A x the gradient of a real
+ * loss is A^H applied to the gradient of y. Layouts as s2b_inverse /
+ * s2b_forward (g_f has the shape of f, g_flm of flm); complex plans only
+ * (reality = 0); s2b_forward_adjoint is the adjoint of the single-pass forward
+ * (desc.iter is ignored). Workspace: s2b_workspace_size(plan, 2 | 3, ...).
+ * Replace the custom VJP rules of s2fft/transforms/spherical.py:306-324 and
+ * 711-729 (latitudinal steps) together with JAX's autodiff of the ring FFTs and
+ * the MW/MWSS resampling (s2fft/utils/resampling.py). */
+int s2b_inverse_adjoint(s2b_plan* plan, const void* g_f, void* g_flm, void* workspace,
+                        size_t workspace_bytes, void* stream);
+int s2b_forward_adjoint(s2b_plan* plan, const void* g_flm, void* g_f, void* workspace,
+                        size_t workspace_bytes, void* stream);
 
 /* Wigner transforms on SO(3) (plan with desc.N > 0; desc.spin is ignored):
  *   flmn [B][2N-1][L][2L-1] <-> f [B][2N-1][ntheta][nphi] (or [B][2N-1][12 nside^2]);

@@ -54,6 +54,8 @@ _SIGS = {
     "s2b_plan_set_events": [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
     "s2b_fma_probe": [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
     "s2b_inverse_noalloc": [ctypes.c_void_p] * 4,
+    "s2b_inverse_adjoint": [ctypes.c_void_p] * 4 + [ctypes.c_size_t, ctypes.c_void_p],
+    "s2b_forward_adjoint": [ctypes.c_void_p] * 4 + [ctypes.c_size_t, ctypes.c_void_p],
 }
 
 
@@ -96,7 +98,8 @@ class Plan:
         self._ws = {}
 
     def workspace(self, forward):
-        key = int(bool(forward))
+        """Workspace of a call: 0 inverse, 1 forward, 2 inverse adjoint, 3 forward adjoint."""
+        key = int(forward)
         if key not in self._ws:
             n = ctypes.c_size_t()
             check(lib().s2b_workspace_size(self.ptr, key, ctypes.byref(n)))

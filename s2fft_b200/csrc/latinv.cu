@@ -180,6 +180,31 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
     lmax = kb1 * kFwdBlock + kFwdBlock - 1;
   if (lmax > L - 1) lmax = L - 1;
 
+  // rescale states whose mantissa grew past the trigger (only states below significance
+  // grow that far). Run every 4 steps: near the poles the monic state can grow by ~2^15 per
+  // step, so 4 steps from just below the trigger (2^48) stay inside the float range.
+  auto renorm = [&]() {
+    Real mx = Real(0);
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+#pragma unroll
+      for (int i = 0; i < T; ++i) mx = fmax(mx, fabs(v[k][i]));
+    const Real trig = Scaling<Real>::kTrig;
+    if (mx > trig) {
+      const Real down = Scaling<Real>::kDown;
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+#pragma unroll
+        for (int i = 0; i < T; ++i)
+          if (fabs(v[k][i]) > trig) {
+            v[k][i] *= down;
+            w[k][i] *= down;
+            const int e = SB::dec(sc[k][i]) + 1;
+            sc[k][i] = e >= 0 ? Real(1) : SB::enc(e);
+          }
+    }
+  };
+
   for (int grp = 0; grp < ngroups; ++grp) {
     const int mgrp = mtop - grp * R;
     const bool ok = mbar_wait(&mbar[grp & 1], (grp >> 1) & 1);
@@ -224,6 +249,7 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
     S2B_INV2_STEP(v, w, 2)
     S2B_INV2_STEP(w, v, 3)
     if constexpr (R == 8) {
+      renorm();
       S2B_INV2_STEP(v, w, 4)
       S2B_INV2_STEP(w, v, 5)
       S2B_INV2_STEP(v, w, 6)
@@ -267,27 +293,7 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
     }
     __syncthreads();
     if (tid == 0 && grp + 2 < ngroups) issue(grp + 2);
-    // renormalise states whose mantissa grew past the trigger (only states below
-    // significance grow that far)
-    Real mx = Real(0);
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-#pragma unroll
-      for (int i = 0; i < T; ++i) mx = fmax(mx, fabs(v[k][i]));
-    const Real trig = Scaling<Real>::kTrig;
-    if (mx > trig) {
-      const Real down = Scaling<Real>::kDown;
-#pragma unroll
-      for (int k = 0; k < K; ++k)
-#pragma unroll
-        for (int i = 0; i < T; ++i)
-          if (fabs(v[k][i]) > trig) {
-            v[k][i] *= down;
-            w[k][i] *= down;
-            const int e = SB::dec(sc[k][i]) + 1;
-            sc[k][i] = e >= 0 ? Real(1) : SB::enc(e);
-          }
-    }
+    renorm();
   }
 }
 
@@ -306,9 +312,9 @@ static cudaError_t launch_inv2_cfg(const Inv2Params& p, cudaStream_t s) {
 cudaError_t launch_inv2(bool fp64, bool dual, const Inv2Params& p, cudaStream_t s) {
   if (p.nrings <= 0) return cudaSuccess;
   if (!fp64)
-    // 2 rings per lane, 8-step groups (measured at L=1024: 0.43 ms; 1 ring per lane is
-    // the same, 4-step groups 10-15 % slower)
-    return dual ? launch_inv2_cfg<float, true, 2, 8>(p, s) : launch_inv2_cfg<float, false, 2, 8>(p, s);
+    // 2 rings per lane, 4-step groups: near the poles a float mantissa can grow by ~2^60
+    // in 4 steps, so the renormalisation check must run at least every 4 steps
+    return dual ? launch_inv2_cfg<float, true, 2, 4>(p, s) : launch_inv2_cfg<float, false, 2, 4>(p, s);
   return dual ? launch_inv2_cfg<double, true, 1, 8>(p, s) : launch_inv2_cfg<double, false, 1, 8>(p, s);
 }
 

@@ -364,11 +364,23 @@ struct s2b_plan {
   void* bf = nullptr;
   int row_desc = 0, col_d1 = 0, col_d2 = 0, maxM = 2, M1 = 2, M2 = 2;
   void* col_ph = nullptr;  // column chain: chirp * half-sample phase / n1 per 4L-bin
+  // adjoints: projection over the inverse rings (start tables), ring -> column map of the
+  // adjoint spectra (recursed rings first, then north / south pole), adjoint chain table
+  int* adj_Mst = nullptr;
+  void* adj_Vst = nullptr;
+  int* adj_col = nullptr;
+  int adj_Gs = 4, adj_pole_s = -1, adj_pole_n = -1;
+  void* col_ph_adj = nullptr;
+  size_t ws_adj_G = 0, ws_adj_y = 0;
   // precompute path: ring colatitudes of the kernel tables, table width
   double* kth_inv = nullptr;
   double* kth_fwd = nullptr;
   int knth_inv = 0, knth_fwd = 0, kM = 0;
   size_t ws_pre_fwd = 0;
+  // float plans with |spin| >= 4: the on-the-fly transforms run on this float64 plan (the
+  // float m-recursion through the evanescent zone |m| < |s| near the poles is not accurate
+  // enough); inputs and outputs are converted at the boundary
+  s2b_plan* shadow = nullptr;
   // Wigner: one spin transform plan per n, gamma-DFT buffers
   std::vector<s2b_plan*> subs;
   size_t ws_w_fban = 0, ws_w_tmp = 0, ws_w_sub = 0;
@@ -545,6 +557,19 @@ static int build_plan(s2b_plan* p) {
     p->inv_mo = (d.sampling == S2B_MWSS || d.sampling == S2B_HEALPIX) ? 1 : 0;
     if ((rc = upload(p, &p->inv_rings, ri))) return rc;
     if ((rc = upload(p, &p->inv_ring_row, rr))) return rc;
+    std::vector<int> col(p->nth, 0);
+    for (int r = 0; r < (int)rr.size(); ++r) col[rr[r]] = r;
+    int next = p->inv_nrings;
+    if (p->inv_pole_n >= 0) {
+      p->adj_pole_n = next;
+      col[p->inv_pole_n] = next++;
+    }
+    if (p->inv_pole_s >= 0) {
+      p->adj_pole_s = next;
+      col[p->inv_pole_s] = next++;
+    }
+    p->adj_Gs = round4(p->nth);
+    if ((rc = upload(p, &p->adj_col, col))) return rc;
   }
   // ---- forward geometry
   {
@@ -621,6 +646,29 @@ static int build_plan(s2b_plan* p) {
     fp.Vst = p->fwd_Vst;
     S2B_CK(launch_fwd_start(p->fp64, fp, 0));
   }
+  // ---- adjoint of the inverse: the forward projection over the inverse rings
+  if (p->inv_nrings > 0) {
+    const size_t nst = (size_t)p->nhalf * p->fwd_NB * p->inv_nrings;
+    S2B_CK(cudaMalloc(&p->adj_Mst, nst * sizeof(int)));
+    p->allocs.push_back(p->adj_Mst);
+    S2B_CK(cudaMalloc(&p->adj_Vst, fwd_start_bytes(p->fp64, L, p->nhalf, p->inv_nrings)));
+    p->allocs.push_back(p->adj_Vst);
+    FwdStartParams fp{};
+    fp.L = L;
+    fp.L0 = d.L_lower;
+    fp.spin = d.spin;
+    fp.nhalf = p->nhalf;
+    fp.nrings = p->inv_nrings;
+    fp.NB = p->fwd_NB;
+    fp.floor_log2 = p->fp64 ? -70.0 : -40.0;
+    fp.group = fwd_group(p->fp64);
+    fp.rings = p->inv_rings;
+    fp.lbin = p->lbin;
+    fp.g = p->gtab;
+    fp.Mst = p->adj_Mst;
+    fp.Vst = p->adj_Vst;
+    S2B_CK(launch_fwd_start(p->fp64, fp, 0));
+  }
 
   // ---- lambda(theta, m) tables (double, rounded once to the plan precision)
   {
@@ -695,6 +743,13 @@ static int build_plan(s2b_plan* p) {
       ph[(pp + n2) % n2] = f;
     }
     if ((rc = upload_complex(p, &p->col_ph, ph))) return rc;
+    std::vector<cd> pa(n2, cd(0.0, 0.0));
+    for (int pp = plo; pp <= phi; ++pp) {
+      cd f(1.0 / n1, 0.0);
+      if (p->fwd_mode == 1) f *= std::polar(1.0, kPi * (double)pp / (2.0 * L - 1.0));
+      pa[(pp + n2) % n2] = f;
+    }
+    if ((rc = upload_complex(p, &p->col_ph_adj, pa))) return rc;
   }
   const size_t maxsmem = (size_t)227 * 1024;
   auto padded = [](int M) { return (size_t)M + (size_t)(M >> 3); };  // ring FFT buffer layout
@@ -727,6 +782,8 @@ static int build_plan(s2b_plan* p) {
   const size_t fel = d.reality ? p->rsz : c2;
   p->ws_iter_f = d.iter > 0 ? B * (size_t)p->npix * fel : 0;
   p->ws_iter_flm = d.iter > 0 ? B * (size_t)L * (2 * L - 1) * c2 : 0;
+  p->ws_adj_G = B * p->nhalf * (size_t)p->TR * p->adj_Gs * acc;
+  p->ws_adj_y = p->fwd_mode ? B * (size_t)(2 * L + 1) * (2 * L - 1) * c2 : 0;
   p->ws_pre_fwd = B * (size_t)p->knth_fwd * p->kM * c2;
   if (p->tc) p->ws_pre_fwd = align256(p->ws_pre_fwd) + tc_packed_b_bytes(p->knth_fwd, d.batch, p->kM);
   S2B_CK(cudaDeviceSynchronize());
@@ -735,6 +792,13 @@ static int build_plan(s2b_plan* p) {
 
 
 static size_t inv_ws(const s2b_plan* p) { return align256(p->ws_inv_F) + align256(p->ws_inv_ftm); }
+static size_t inv_adj_ws(const s2b_plan* p) {
+  return align256(p->ws_adj_G) + align256(p->ws_fwd_acc);
+}
+static size_t fwd_adj_ws(const s2b_plan* p) {
+  return p->fwd_mode ? align256(p->ws_inv_F) + align256(p->ws_adj_y) + align256(p->ws_inv_ftm)
+                     : inv_ws(p);
+}
 static size_t pre_fwd_ws(const s2b_plan* p) {
   return align256(p->ws_fwd_cols) + align256(p->ws_pre_fwd);
 }
@@ -765,7 +829,8 @@ static int check_ptr(const void* ptr, const char* what) {
 }
 
 template <typename Real>
-static int run_inverse(s2b_plan* p, const void* flm, void* f, char* ws, cudaStream_t s) {
+static int run_inverse(s2b_plan* p, const void* flm, void* f, char* ws, cudaStream_t s,
+                       const double* ring_w = nullptr) {
   const s2b_desc& d = p->d;
   const int L = d.L;
   void* F = ws;
@@ -836,8 +901,171 @@ static int run_inverse(s2b_plan* p, const void* flm, void* f, char* ws, cudaStre
   rp.out_batch_stride = p->npix;
   rp.phi0 = d.sampling == S2B_HEALPIX ? p->hp_phi0 : nullptr;
   rp.tb = tables<Real>(p);
+  rp.weights = ring_w;
   rp.in = ftm;
   rp.out = f;
+  S2B_CK(launch_inv_rows<Real>(rp, p->nth, d.batch, p->maxM, s));
+  return S2B_OK;
+}
+
+// Adjoint (conjugate transpose) of the inverse: unweighted ring DFTs of g_f, the forward
+// projection over the inverse rings, and the pole rings in closed form.
+template <typename Real>
+static int run_inverse_adjoint(s2b_plan* p, const void* gf, void* gflm, char* ws,
+                               cudaStream_t s) {
+  const s2b_desc& d = p->d;
+  const int L = d.L;
+  char* G = ws;
+  char* acc = G + align256(p->ws_adj_G);
+  S2B_CK(cudaMemsetAsync(acc, 0, p->ws_fwd_acc, s));
+  RowsParams<Real> rp{};
+  rp.L = L;
+  rp.nrows = p->nth;
+  rp.dual = p->dual;
+  rp.nhalf = p->nhalf;
+  rp.TR = p->TR;
+  rp.Gs = p->adj_Gs;
+  rp.scale = 1.0;
+  rp.desc = p->descs + p->row_desc;
+  if (d.sampling == S2B_HEALPIX) {
+    rp.desc = p->descs;
+    rp.ring_desc = p->ring_desc;
+    rp.phi0 = p->hp_phi0;
+  }
+  rp.ring_off = p->ring_off;
+  rp.out_batch_stride = p->npix;
+  rp.tb = tables<Real>(p);
+  rp.mode = FWD_TO_SPECTRA;
+  rp.col_of_ring = p->adj_col;
+  rp.in = gf;
+  rp.out = G;
+  S2B_CK(launch_fwd_rows<Real>(rp, p->nth, d.batch, p->maxM, s));
+  if (p->inv_nrings > 0) {
+    Fwd2Params lp{};
+    lp.L = L;
+    lp.nrings = p->inv_nrings;
+    lp.nhalf = p->nhalf;
+    lp.batch = d.batch;
+    lp.NB = p->fwd_NB;
+    lp.Mst = p->adj_Mst;
+    lp.Vst = p->adj_Vst;
+    lp.Hb = p->fwd_Hb;
+    lp.lam = p->inv_lam;
+    lp.Ls = p->inv_Ls;
+    lp.G = G;
+    lp.Gs = p->adj_Gs;
+    lp.acc = acc;
+    lp.status = p->status;
+    S2B_CK(launch_fwd2(p->fp64, p->dual, lp, s));
+  }
+  StageParams sp{};
+  sp.L = L;
+  sp.L0 = d.L_lower;
+  sp.spin = d.spin;
+  sp.batch = d.batch;
+  sp.nclass = p->nclass;
+  sp.Q = p->Q;
+  sp.TR = p->TR;
+  sp.Gs = p->adj_Gs;
+  sp.nhalf = p->nhalf;
+  sp.dual = p->dual;
+  sp.nrows = p->nth;
+  sp.pole_south = p->adj_pole_s;
+  sp.pole_north = p->adj_pole_n;
+  sp.g = p->gtab;
+  sp.G = G;
+  sp.acc = acc;
+  sp.Lp = p->fwd_NB * kFwdBlock;
+  sp.flm_out = gflm;
+  S2B_CK(launch_epilogue(p->fp64, sp, s));
+  return S2B_OK;
+}
+
+// Adjoint of the (single-pass) forward. Direct samplings: the inverse followed by the ring
+// quadrature weights. MW / MWSS: the inverse projection onto the MWSS(2L) rings, the adjoint
+// of the column resampling chain, then unnormalised inverse ring DFTs.
+template <typename Real>
+static int run_forward_adjoint(s2b_plan* p, const void* gflm, void* gf, char* ws,
+                               cudaStream_t s) {
+  const s2b_desc& d = p->d;
+  const int L = d.L;
+  if (p->fwd_mode == 0) return run_inverse<Real>(p, gflm, gf, ws, s, p->fwd_weights);
+  char* F = ws;
+  char* y = F + align256(p->ws_inv_F);
+  char* ftm2 = y + align256(p->ws_adj_y);
+  S2B_CK(cudaMemsetAsync(y, 0, p->ws_adj_y, s));
+  StageParams sp{};
+  sp.L = L;
+  sp.L0 = d.L_lower;
+  sp.spin = d.spin;
+  sp.batch = d.batch;
+  sp.nclass = p->fwd_NB;
+  sp.Q = kFwdBlock;
+  sp.Lp = p->fwd_NB * kFwdBlock;
+  sp.TR = p->TR;
+  sp.nhalf = p->nhalf;
+  sp.dual = p->dual;
+  sp.nrows = 2 * L + 1;
+  sp.ncol = 2 * L - 1;
+  sp.mo = 0;
+  sp.pole_south = p->fwd_pole_s;
+  sp.pole_north = p->fwd_pole_n;
+  sp.g = p->gtab;
+  sp.flm = gflm;
+  sp.F = F;
+  sp.ftm = y;
+  S2B_CK(launch_prologue(p->fp64, sp, s));
+  S2B_CK(launch_poles(p->fp64, sp, s));
+  Inv2Params lp{};
+  lp.L = L;
+  lp.nrings = p->fwd_nrings;
+  lp.nhalf = p->nhalf;
+  lp.batch = d.batch;
+  lp.NB = p->fwd_NB;
+  lp.C = p->nclass;
+  lp.Qp = p->Q;
+  lp.seeds = p->fwd_seeds;
+  lp.Hb = p->fwd_Hb;
+  lp.lam = p->fwd_lam;
+  lp.Ls = p->fwd_Ls;
+  lp.F = F;
+  lp.ftm = y;
+  lp.ring_row = p->fwd_ring_row;
+  lp.nrows = 2 * L + 1;
+  lp.ncol = 2 * L - 1;
+  lp.mo = 0;
+  lp.status = p->status;
+  S2B_CK(launch_inv2(p->fp64, p->dual, lp, s));
+  ColsParams<Real> cp{};
+  cp.L = L;
+  cp.spin = d.spin;
+  cp.mw = p->fwd_mode == 1;
+  cp.nin = p->nth;
+  cp.dual = p->dual;
+  cp.nhalf = p->nhalf;
+  cp.TR = p->TR;
+  cp.scale = p->fwd_mode == 1 ? (2.0 * L) / (2.0 * L - 1.0) : 1.0;
+  cp.d1 = p->descs + p->col_d1;
+  cp.d2 = p->descs + p->col_d2;
+  cp.weights = p->fwd_weights;
+  cp.ph_adj = p->col_ph_adj;
+  cp.tb = tables<Real>(p);
+  cp.in = y;
+  cp.out = ftm2;
+  const int ncm = p->fwd_mode == 1 ? 2 * L - 1 : 2 * L;
+  S2B_CK(launch_mw_cols_adj<Real>(cp, ncm, d.batch, p->M1, p->M2, p->inv_ncol, p->inv_mo, s));
+  RowsParams<Real> rp{};
+  rp.L = L;
+  rp.nrows = p->nth;
+  rp.ncol = p->inv_ncol;
+  rp.mo = p->inv_mo;
+  rp.scale = 1.0;
+  rp.desc = p->descs + p->row_desc;
+  rp.ring_off = p->ring_off;
+  rp.out_batch_stride = p->npix;
+  rp.tb = tables<Real>(p);
+  rp.in = ftm2;
+  rp.out = gf;
   S2B_CK(launch_inv_rows<Real>(rp, p->nth, d.batch, p->maxM, s));
   return S2B_OK;
 }
@@ -1134,6 +1362,55 @@ static int run_pre_forward(s2b_plan* p, const void* K, const void* f, void* flm,
 // Wigner (SO(3)) transforms: 2N-1 spin transforms + gamma DFT
 // (s2fft/transforms/wigner.py:110-196, 442-533)
 // ----------------------------------------------------------------------------
+// Workspace of a call of the given kind (0 inverse, 1 forward, 2 inverse adjoint,
+// 3 forward adjoint) on a spin plan, including the float64 shadow's conversion buffers.
+static size_t ws_of(const s2b_plan* p, int kind) {
+  if (p->shadow) {
+    const s2b_desc& d = p->d;
+    const size_t nflm = (size_t)d.batch * d.L * (2 * d.L - 1) * 2;
+    const size_t nf = (size_t)d.batch * p->npix * (d.reality ? 1 : 2);
+    return align256(nflm * 8) + align256(nf * 8) + ws_of(p->shadow, kind);
+  }
+  switch (kind) {
+    case 0: return inv_ws(p);
+    case 1: return std::max(fwd_ws(p), pre_fwd_ws(p));
+    case 2: return inv_adj_ws(p);
+    default: return fwd_adj_ws(p);
+  }
+}
+
+// One spin-transform call of the given kind on the plan's own precision, or, for plans with a
+// float64 shadow, on the shadow with float <-> double conversion of input and output.
+static int exec_call(s2b_plan* p, int kind, const void* in, void* out, char* ws, cudaStream_t s) {
+  if (p->shadow) {
+    const s2b_desc& d = p->d;
+    const size_t nflm = (size_t)d.batch * d.L * (2 * d.L - 1) * 2;
+    const size_t nf = (size_t)d.batch * p->npix * (d.reality ? 1 : 2);
+    const bool in_flm = kind == 0 || kind == 3;
+    const size_t nin = in_flm ? nflm : nf, nout = in_flm ? nf : nflm;
+    char* a = ws;                          // converted input
+    char* b = a + align256(nin * 8);       // float64 output
+    char* w2 = a + align256(nflm * 8) + align256(nf * 8);  // the shadow's workspace
+    S2B_CK(launch_cast(true, in, a, (long)nin, s));
+    const int rc = exec_call(p->shadow, kind, a, b, w2, s);
+    if (rc) return rc;
+    S2B_CK(launch_cast(false, b, out, (long)nout, s));
+    return S2B_OK;
+  }
+  switch (kind) {
+    case 0:
+      return p->fp64 ? run_inverse<double>(p, in, out, ws, s) : run_inverse<float>(p, in, out, ws, s);
+    case 1:
+      return p->fp64 ? run_forward<double>(p, in, out, ws, s) : run_forward<float>(p, in, out, ws, s);
+    case 2:
+      return p->fp64 ? run_inverse_adjoint<double>(p, in, out, ws, s)
+                     : run_inverse_adjoint<float>(p, in, out, ws, s);
+    default:
+      return p->fp64 ? run_forward_adjoint<double>(p, in, out, ws, s)
+                     : run_forward_adjoint<float>(p, in, out, ws, s);
+  }
+}
+
 static int build_wigner(s2b_plan* p) {
   const s2b_desc& d = p->d;
   p->fp64 = d.precision == S2B_F64;
@@ -1152,7 +1429,7 @@ static int build_wigner(s2b_plan* p) {
     const int rc = s2b_plan_create(&sd, &sub);
     if (rc) return rc;
     p->subs.push_back(sub);
-    p->ws_w_sub = std::max(p->ws_w_sub, std::max(inv_ws(sub), fwd_ws(sub)));
+    p->ws_w_sub = std::max(p->ws_w_sub, std::max(ws_of(sub, 0), ws_of(sub, 1)));
   }
   const size_t c2 = 2 * p->rsz;
   p->ws_w_fban = (size_t)(2 * d.N - 1) * d.batch * p->npix * c2;
@@ -1178,8 +1455,7 @@ static int run_wigner(s2b_plan* p, bool forward, const void* in, void* out, char
       s2b_plan* sub = p->subs[n - n0];
       S2B_CK(launch_gather_n(p->fp64, in, tmp, d.batch, d.N, d.L, n, s));
       char* dst = fban + (size_t)(d.N - 1 + n) * slice;
-      rc = p->fp64 ? run_inverse<double>(sub, tmp, dst, subws, s)
-                   : run_inverse<float>(sub, tmp, dst, subws, s);
+      rc = exec_call(sub, 0, tmp, dst, subws, s);
       if (rc) return rc;
     }
     S2B_CK(launch_gamma_inverse(p->fp64, fban, out, d.batch, d.N, p->npix, d.reality, s));
@@ -1189,8 +1465,7 @@ static int run_wigner(s2b_plan* p, bool forward, const void* in, void* out, char
   for (int n = n0; n < d.N; ++n) {
     s2b_plan* sub = p->subs[n - n0];
     const char* src = fban + (size_t)(d.N - 1 + n) * slice;
-    rc = p->fp64 ? run_forward<double>(sub, src, tmp, subws, s)
-                 : run_forward<float>(sub, src, tmp, subws, s);
+    rc = exec_call(sub, 1, src, tmp, subws, s);
     if (rc) return rc;
     S2B_CK(launch_scatter_n(p->fp64, tmp, out, d.batch, d.N, d.L, n, d.L_lower, s));
   }
@@ -1232,8 +1507,14 @@ int s2b_plan_create(const s2b_desc* desc, s2b_plan** out) {
   if (d.N > 0 && d.iter != 0) return fail(S2B_ERR_INVALID, "iter is not used by Wigner plans");
   s2b_plan* p = new s2b_plan();
   p->d = d;
-  const int rc = d.N > 0 ? build_wigner(p) : build_plan(p);
+  int rc = d.N > 0 ? build_wigner(p) : build_plan(p);
+  if (!rc && d.N == 0 && d.precision != S2B_F64 && std::abs(d.spin) >= 4) {
+    s2b_desc d64 = d;
+    d64.precision = S2B_F64;
+    rc = s2b_plan_create(&d64, &p->shadow);
+  }
   if (rc) {
+    if (p->shadow) s2b_plan_destroy(p->shadow);
     for (s2b_plan* sp : p->subs) s2b_plan_destroy(sp);
     for (void* a : p->allocs) cudaFree(a);
     delete p;
@@ -1245,6 +1526,7 @@ int s2b_plan_create(const s2b_desc* desc, s2b_plan** out) {
 
 int s2b_plan_destroy(s2b_plan* p) {
   if (!p) return S2B_OK;
+  if (p->shadow) s2b_plan_destroy(p->shadow);
   for (s2b_plan* sp : p->subs) s2b_plan_destroy(sp);
   for (void* a : p->allocs) cudaFree(a);
   delete p;
@@ -1253,7 +1535,11 @@ int s2b_plan_destroy(s2b_plan* p) {
 
 int s2b_workspace_size(const s2b_plan* p, int forward, size_t* bytes) {
   if (!p || !bytes) return fail(S2B_ERR_INVALID, "plan and bytes must be non-NULL");
-  *bytes = p->d.N > 0 ? wigner_ws(p) : (forward ? std::max(fwd_ws(p), pre_fwd_ws(p)) : inv_ws(p));
+  if (forward < 0 || forward > 3) return fail(S2B_ERR_INVALID, "direction must be 0..3");
+  if (p->d.N > 0)
+    *bytes = wigner_ws(p);
+  else
+    *bytes = ws_of(p, forward);
   return S2B_OK;
 }
 
@@ -1262,10 +1548,8 @@ int s2b_inverse(s2b_plan* p, const void* flm, void* f, void* ws, size_t ws_bytes
   int rc;
   if ((rc = check_ptr(flm, "flm")) || (rc = check_ptr(f, "f")) || (rc = check_ptr(ws, "workspace")))
     return rc;
-  if (ws_bytes < inv_ws(p)) return fail(S2B_ERR_WORKSPACE, "workspace too small");
-  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  return p->fp64 ? run_inverse<double>(p, flm, f, (char*)ws, s)
-                 : run_inverse<float>(p, flm, f, (char*)ws, s);
+  if (ws_bytes < ws_of(p, 0)) return fail(S2B_ERR_WORKSPACE, "workspace too small");
+  return exec_call(p, 0, flm, f, (char*)ws, reinterpret_cast<cudaStream_t>(stream));
 }
 
 int s2b_forward(s2b_plan* p, const void* f, void* flm, void* ws, size_t ws_bytes, void* stream) {
@@ -1273,10 +1557,32 @@ int s2b_forward(s2b_plan* p, const void* f, void* flm, void* ws, size_t ws_bytes
   int rc;
   if ((rc = check_ptr(flm, "flm")) || (rc = check_ptr(f, "f")) || (rc = check_ptr(ws, "workspace")))
     return rc;
-  if (ws_bytes < fwd_ws(p)) return fail(S2B_ERR_WORKSPACE, "workspace too small");  // spin path
-  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  return p->fp64 ? run_forward<double>(p, f, flm, (char*)ws, s)
-                 : run_forward<float>(p, f, flm, (char*)ws, s);
+  if (ws_bytes < ws_of(p, 1)) return fail(S2B_ERR_WORKSPACE, "workspace too small");
+  return exec_call(p, 1, f, flm, (char*)ws, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int s2b_inverse_adjoint(s2b_plan* p, const void* g_f, void* g_flm, void* ws, size_t ws_bytes,
+                        void* stream) {
+  if (!p || p->d.N > 0) return fail(S2B_ERR_INVALID, "plan is NULL or a Wigner plan");
+  if (p->d.reality) return fail(S2B_ERR_INVALID, "adjoints are defined for complex plans (reality = 0)");
+  int rc;
+  if ((rc = check_ptr(g_f, "g_f")) || (rc = check_ptr(g_flm, "g_flm")) ||
+      (rc = check_ptr(ws, "workspace")))
+    return rc;
+  if (ws_bytes < ws_of(p, 2)) return fail(S2B_ERR_WORKSPACE, "workspace too small");
+  return exec_call(p, 2, g_f, g_flm, (char*)ws, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int s2b_forward_adjoint(s2b_plan* p, const void* g_flm, void* g_f, void* ws, size_t ws_bytes,
+                        void* stream) {
+  if (!p || p->d.N > 0) return fail(S2B_ERR_INVALID, "plan is NULL or a Wigner plan");
+  if (p->d.reality) return fail(S2B_ERR_INVALID, "adjoints are defined for complex plans (reality = 0)");
+  int rc;
+  if ((rc = check_ptr(g_flm, "g_flm")) || (rc = check_ptr(g_f, "g_f")) ||
+      (rc = check_ptr(ws, "workspace")))
+    return rc;
+  if (ws_bytes < ws_of(p, 3)) return fail(S2B_ERR_WORKSPACE, "workspace too small");
+  return exec_call(p, 3, g_flm, g_f, (char*)ws, reinterpret_cast<cudaStream_t>(stream));
 }
 
 int s2b_kernel_size(const s2b_plan* p, int forward, size_t* bytes) {
@@ -1338,19 +1644,22 @@ int s2b_wigner_forward(s2b_plan* p, const void* f, void* flmn, void* ws, size_t 
   return run_wigner(p, true, f, flmn, (char*)ws, reinterpret_cast<cudaStream_t>(stream));
 }
 
+static int plan_status_word(const s2b_plan* p, int* out) {
+  int st = 0;
+  if (p->status) S2B_CK(cudaMemcpy(&st, p->status, sizeof(int), cudaMemcpyDeviceToHost));
+  *out |= st;
+  int rc;
+  if (p->shadow && (rc = plan_status_word(p->shadow, out))) return rc;
+  for (const s2b_plan* sp : p->subs)
+    if ((rc = plan_status_word(sp, out))) return rc;
+  return S2B_OK;
+}
+
 int s2b_plan_status(s2b_plan* p, int* status) {
   if (!p || !status) return fail(S2B_ERR_INVALID, "plan and status must be non-NULL");
   *status = 0;
-  for (s2b_plan* sp : p->subs) {
-    int st = 0;
-    S2B_CK(cudaMemcpy(&st, sp->status, sizeof(int), cudaMemcpyDeviceToHost));
-    *status |= st;
-  }
-  if (p->status) {
-    int st = 0;
-    S2B_CK(cudaMemcpy(&st, p->status, sizeof(int), cudaMemcpyDeviceToHost));
-    *status |= st;
-  }
+  const int rc = plan_status_word(p, status);
+  if (rc) return rc;
   if (*status) return fail(S2B_ERR_TIMEOUT, "a bounded device wait gave up");
   return S2B_OK;
 }

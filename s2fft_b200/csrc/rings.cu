@@ -322,7 +322,7 @@ __global__ void inv_rows_kernel(RowsParams<Real> p) {
     return acc;
   };
   dft_run<Real>(s, d, p.tb, true, load);
-  const Real scale = (Real)p.scale;
+  const Real scale = (Real)(p.scale * (p.weights ? p.weights[t] : 1.0));
   if (p.real_out) {
     Real* out = reinterpret_cast<Real*>(p.out) + (size_t)b * p.out_batch_stride + p.ring_off[t];
     for (int j = threadIdx.x; j < n; j += blockDim.x)
@@ -339,6 +339,7 @@ __device__ __forceinline__ void store_spectra(const RowsParams<Real>& p, int b, 
   // G [b][half][m + kPadLo][Gs]: rows m outside [0, L) and columns >= nrows are zero
   using R2 = typename C2<Real>::t;
   const int L = p.L;
+  const int col = p.col_of_ring ? p.col_of_ring[t] : t;
   if (t == p.nrows - 1 && p.Gs > p.nrows) {
     const int halves = p.dual ? 1 : p.nhalf, per = p.dual ? 2 : 1;
     R2* o2 = reinterpret_cast<R2*>(p.out);
@@ -364,16 +365,16 @@ __device__ __forceinline__ void store_spectra(const RowsParams<Real>& p, int b, 
       o.y = a.y;
       o.z = c.x;
       o.w = c.y;
-      out[((size_t)b * p.TR + mr) * p.Gs + t] = o;
+      out[((size_t)b * p.TR + mr) * p.Gs + col] = o;
     }
   } else {
     R2* out = reinterpret_cast<R2*>(p.out);
     for (int mr = threadIdx.x; mr < p.TR; mr += blockDim.x) {
       const int m = mr - kPadLo;
       const bool ok = m >= 0 && m < L;
-      out[(((size_t)b * p.nhalf + 0) * p.TR + mr) * p.Gs + t] = ok ? val(m) : czero<R2>();
+      out[(((size_t)b * p.nhalf + 0) * p.TR + mr) * p.Gs + col] = ok ? val(m) : czero<R2>();
       if (p.nhalf > 1)
-        out[(((size_t)b * p.nhalf + 1) * p.TR + mr) * p.Gs + t] =
+        out[(((size_t)b * p.nhalf + 1) * p.TR + mr) * p.Gs + col] =
             (ok && m > 0) ? val(-m) : czero<R2>();
     }
   }
@@ -561,6 +562,71 @@ __global__ void mw_cols_kernel(ColsParams<Real> p) {
 }
 
 // ---------------------------------------------------------------------------
+// Adjoint of the MW / MWSS column chain (one CTA per (m column, map)): the
+// conjugate transpose of mw_cols_kernel, step by step in reverse order:
+//   y (2L+1 MWSS(2L) ring values) * scale * weights -> zero-padded DFT over 4L
+//   -> bins p in [plo, phi] times conj(half-sample phase) / n1 -> unnormalised
+//   inverse DFT over the n1-point extended circle -> fold the extension back
+//   onto the input rings with the parity (-1)^(m+s).
+// ---------------------------------------------------------------------------
+template <typename Real>
+__global__ void mw_cols_adj_kernel(ColsParams<Real> p, int ncol_out, int mo_out) {
+  using R2 = typename C2<Real>::t;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const FFTDesc d1 = *p.d1;
+  const FFTDesc d2 = *p.d2;
+  R2* s1 = reinterpret_cast<R2*>(smem_raw);
+  R2* s2 = s1 + padded_len(d1.M);
+  const int L = p.L;
+  const int mlo = p.mw ? -(L - 1) : -L;
+  const int mi = blockIdx.x;
+  const int b = blockIdx.y;
+  const int m = mlo + mi;
+  R2* out = reinterpret_cast<R2*>(p.out) + (size_t)b * p.nin * ncol_out + (L - 1 + m + mo_out);
+  if (m < -(L - 1)) {  // MWSS m = -L: the forward chain output of this column is never used
+    for (int t = threadIdx.x; t < p.nin; t += blockDim.x) out[(size_t)t * ncol_out] = czero<R2>();
+    return;
+  }
+  const int nout = 2 * L + 1;
+  const R2* y = reinterpret_cast<const R2*>(p.in) + (size_t)b * nout * (2 * L - 1) + (L - 1 + m);
+  auto load2 = [&](int t) -> R2 {
+    if (t >= nout) return czero<R2>();
+    const int row = t == 0 ? 2 * L - 1 : (t == 2 * L ? 2 * L : t - 1);
+    const R2 v = y[(size_t)row * (2 * L - 1)];
+    const double f = p.scale * p.weights[t];
+    R2 o;
+    o.x = (Real)((double)v.x * f);
+    o.y = (Real)((double)v.y * f);
+    return o;
+  };
+  dft_run<Real>(s2, d2, p.tb, false, load2);  // DFT over 4L
+  const int plo = p.mw ? -(L - 1) : -L;
+  const int phi = L - 1;
+  const int n1 = d1.n;
+  const int n2 = d2.n;
+  const R2* __restrict__ pha = reinterpret_cast<const R2*>(p.ph_adj);
+  auto load1 = [&](int j) -> R2 {
+    const int pp = j <= phi ? j : j - n1;  // the bin p in [plo, phi] with p = j (mod n1)
+    if (pp < plo) return czero<R2>();
+    const int k = (pp + n2) % n2;
+    return cmul(dft_get<Real>(s2, d2, p.tb, false, k), pha[k]);
+  };
+  dft_run<Real>(s1, d1, p.tb, true, load1);  // unnormalised inverse DFT over n1
+  const int par = ((m + p.spin) % 2 + 2) % 2;
+  const Real sgn = par ? Real(-1) : Real(1);
+  for (int t = threadIdx.x; t < p.nin; t += blockDim.x) {
+    R2 x = dft_get<Real>(s1, d1, p.tb, true, t);
+    if (p.mw) {
+      if (t <= L - 2) x = cadd(x, cscale(dft_get<Real>(s1, d1, p.tb, true, 2 * L - 2 - t), sgn));
+    } else {
+      if (t >= 1 && t <= L - 1)
+        x = cadd(x, cscale(dft_get<Real>(s1, d1, p.tb, true, 2 * L - t), sgn));
+    }
+    out[(size_t)t * ncol_out] = x;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
 static int fft_threads(int M) {
@@ -606,6 +672,23 @@ cudaError_t launch_mw_cols(const ColsParams<Real>& p, int ncm, int batch, int M1
   return cudaGetLastError();
 }
 
+template <typename Real>
+cudaError_t launch_mw_cols_adj(const ColsParams<Real>& p, int ncm, int batch, int M1, int M2,
+                               int ncol_out, int mo_out, cudaStream_t s) {
+  using R2 = typename C2<Real>::t;
+  const size_t smem = (size_t)(padded_len(M1) + padded_len(M2)) * sizeof(R2);
+  cudaError_t e = cudaFuncSetAttribute(mw_cols_adj_kernel<Real>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  mw_cols_adj_kernel<Real><<<dim3(ncm, batch), fft_threads(M1 > M2 ? M1 : M2), smem, s>>>(
+      p, ncol_out, mo_out);
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_mw_cols_adj<float>(const ColsParams<float>&, int, int, int, int, int,
+                                               int, cudaStream_t);
+template cudaError_t launch_mw_cols_adj<double>(const ColsParams<double>&, int, int, int, int, int,
+                                                int, cudaStream_t);
 template cudaError_t launch_inv_rows<float>(const RowsParams<float>&, int, int, int, cudaStream_t);
 template cudaError_t launch_inv_rows<double>(const RowsParams<double>&, int, int, int, cudaStream_t);
 template cudaError_t launch_fwd_rows<float>(const RowsParams<float>&, int, int, int, cudaStream_t);

@@ -47,8 +47,10 @@ struct RowsParams {
   const int* ring_desc; // per ring index into desc (nullptr: desc[0] for all)
   const long* ring_off; // element offset of ring t inside one map
   long out_batch_stride;// elements per map of the pixel-space array (f)
-  const double* weights;// forward: quadrature weight per ring (nullptr: 1)
+  const double* weights;// forward: quadrature weight per ring; inverse: output factor per ring
+                        // (nullptr: 1)
   const double* phi0;   // HEALPix ring phase (nullptr: none)
+  const int* col_of_ring; // forward spectra: column of ring t (nullptr: t)
   FFTTables<Real> tb;
   const void* in;
   void* out;
@@ -67,6 +69,7 @@ struct ColsParams {
   const FFTDesc* d2;    // inverse DFT of length 4L
   const double* weights;// 2L+1 MWSS(2L) transform weights
   const void* ph;       // [4L] complex factor of theta-DFT bin p (at p mod 4L), 0 outside
+  const void* ph_adj;   // [4L] adjoint chain: conj(half-sample phase) / n1 (at p mod 4L)
   FFTTables<Real> tb;
   const void* in;       // Fc [B][ncm][nin]
   void* out;            // G  [B][half][m + kPadLo][Gs]; MWSS(2L) ring t -> row t-1,
@@ -85,4 +88,10 @@ cudaError_t launch_fwd_rows(const RowsParams<Real>& p, int nrings, int batch, in
 template <typename Real>
 cudaError_t launch_mw_cols(const ColsParams<Real>& p, int ncm, int batch, int M1, int M2,
                            cudaStream_t s);
+// Adjoint of the column chain: in = [B][2L+1][2L-1] values on the MWSS(2L) rings (row t-1 for
+// ring t = 1..2L-1, north pole row 2L-1, south pole row 2L; column L-1+m), out = the
+// transposed column spectra [B][nin][ncol_out] (column L-1+m+mo_out) that inv_rows reads.
+template <typename Real>
+cudaError_t launch_mw_cols_adj(const ColsParams<Real>& p, int ncm, int batch, int M1, int M2,
+                               int ncol_out, int mo_out, cudaStream_t s);
 }  // namespace s2b

@@ -188,15 +188,16 @@ __global__ void epilogue_kernel(StageParams p) {
       if (m < 0 && !conj_mirror) f *= ((am + p.spin) % 2 + 2) % 2 ? -1.0 : 1.0;
       re = f * ar;
       im = f * ai;
-      // closed-form pole rings (MWSS(2L) grid of the mw / mwss forward)
-      if (p.pole_south >= 0 && !conj_mirror) {
-        if (m == p.spin) {
+      // closed-form pole rings (each present pole: theta = pi contributes at m = s, theta = 0 at
+      // m = -s)
+      if (!conj_mirror) {
+        if (p.pole_south >= 0 && m == p.spin) {
           const R2 s = spectrum_at<Real>(p, b, p.pole_south, m);
           const double sg = ((l - p.spin) % 2 + 2) % 2 ? -1.0 : 1.0;
           re += sg * s.x;
           im += sg * s.y;
         }
-        if (m == -p.spin) {
+        if (p.pole_north >= 0 && m == -p.spin) {
           const R2 s = spectrum_at<Real>(p, b, p.pole_north, m);
           re += s.x;
           im += s.y;
@@ -271,6 +272,24 @@ cudaError_t launch_epilogue(bool fp64, const StageParams& p, cudaStream_t s) {
     epilogue_kernel<double><<<grid_for(total), 256, 0, s>>>(p);
   else
     epilogue_kernel<float><<<grid_for(total), 256, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+__global__ void cast_f2d_kernel(const float* __restrict__ in, double* __restrict__ out, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    out[i] = (double)in[i];
+}
+__global__ void cast_d2f_kernel(const double* __restrict__ in, float* __restrict__ out, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    out[i] = (float)in[i];
+}
+
+cudaError_t launch_cast(bool to64, const void* in, void* out, long n, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  if (to64)
+    cast_f2d_kernel<<<grid_for(n), 256, 0, s>>>((const float*)in, (double*)out, n);
+  else
+    cast_d2f_kernel<<<grid_for(n), 256, 0, s>>>((const double*)in, (float*)out, n);
   return cudaGetLastError();
 }
 

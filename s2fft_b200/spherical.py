@@ -13,6 +13,12 @@ bookkeeping and weights; complex64 arrays).
 
 Inputs may be numpy arrays (returned as numpy) or torch tensors (returned as
 torch tensors on the same device). A leading batch dimension is accepted.
+
+Differentiation: when a torch input requires grad, the transforms run as
+``torch.autograd.Function``s whose backward passes call the adjoint kernels
+(``s2b_inverse_adjoint`` / ``s2b_forward_adjoint``, recomputing the Wigner-d
+recursion instead of storing it); refinement iterations are composed from the
+single passes. Complex transforms only (``reality=False``).
 """
 
 from __future__ import annotations
@@ -99,6 +105,60 @@ def _dtypes(precision):
                                                                           torch.float32)
 
 
+class _InverseFn(torch.autograd.Function):
+    """f = inverse(flm); backward applies the adjoint kernel (s2b_inverse_adjoint)."""
+
+    @staticmethod
+    def forward(ctx, flm, plan, f_shape_full, out_dtype):
+        out = torch.empty(f_shape_full, dtype=out_dtype, device=flm.device)
+        ws = plan.workspace(0)
+        _lib.check(_lib.lib().s2b_inverse(plan.ptr, flm.data_ptr(), out.data_ptr(),
+                                          ws.data_ptr(), ws.numel(),
+                                          _lib.stream_handle(flm.device)))
+        ctx.plan = plan
+        ctx.in_shape = flm.shape
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        g = g.contiguous()
+        gflm = torch.empty(ctx.in_shape, dtype=g.dtype, device=g.device)
+        ws = ctx.plan.workspace(2)
+        _lib.check(_lib.lib().s2b_inverse_adjoint(ctx.plan.ptr, g.data_ptr(), gflm.data_ptr(),
+                                                  ws.data_ptr(), ws.numel(),
+                                                  _lib.stream_handle(g.device)))
+        return gflm, None, None, None
+
+
+class _ForwardFn(torch.autograd.Function):
+    """flm = forward(f) (single pass); backward applies s2b_forward_adjoint."""
+
+    @staticmethod
+    def forward(ctx, f, plan, flm_shape_full, out_dtype):
+        out = torch.empty(flm_shape_full, dtype=out_dtype, device=f.device)
+        ws = plan.workspace(1)
+        _lib.check(_lib.lib().s2b_forward(plan.ptr, f.data_ptr(), out.data_ptr(),
+                                          ws.data_ptr(), ws.numel(),
+                                          _lib.stream_handle(f.device)))
+        ctx.plan = plan
+        ctx.in_shape = f.shape
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        g = g.contiguous()
+        gf = torch.empty(ctx.in_shape, dtype=g.dtype, device=g.device)
+        ws = ctx.plan.workspace(3)
+        _lib.check(_lib.lib().s2b_forward_adjoint(ctx.plan.ptr, g.data_ptr(), gf.data_ptr(),
+                                                  ws.data_ptr(), ws.numel(),
+                                                  _lib.stream_handle(g.device)))
+        return gf, None, None, None
+
+
+def _needs_grad(x):
+    return isinstance(x, torch.Tensor) and x.requires_grad and torch.is_grad_enabled()
+
+
 def inverse(flm, L: int, spin: int = 0, nside: int = None, sampling: str = "mw",
             method: str = "cuda", reality: bool = False, precomps=None, spmd: bool = False,
             L_lower: int = 0, _ssht_backend: int = 1, precision: str = "f64"):
@@ -115,6 +175,11 @@ def inverse(flm, L: int, spin: int = 0, nside: int = None, sampling: str = "mw",
     plan = _lib.get_plan(x.device, L=L, spin=spin, nside=nside or 0, sampling=_lib.SAMPLING[s],
                          reality=int(bool(reality)), L_lower=L_lower,
                          precision=_lib.PRECISION[precision], batch=B, iter=0, N=0)
+    if _needs_grad(x):
+        if reality:
+            raise NotImplementedError("gradients are available for complex transforms (reality=False)")
+        return _ret(_InverseFn.apply(x, plan, batch_shape + f_shape(L, s, nside), cdt),
+                    was_np, odev)
     out = torch.empty(batch_shape + f_shape(L, s, nside), dtype=rdt if reality else cdt,
                       device=x.device)
     ws = plan.workspace(False)
@@ -150,6 +215,19 @@ def forward(f, L: int, spin: int = 0, nside: int = None, sampling: str = "mw",
         raise ValueError(f"f must have trailing shape {fs}, got {tuple(x.shape)}")
     batch_shape = tuple(x.shape[:-nd])
     B = int(np.prod(batch_shape)) if batch_shape else 1
+    if _needs_grad(x):
+        if reality:
+            raise NotImplementedError("gradients are available for complex transforms (reality=False)")
+        # refinement flm <- flm + F(f - I(flm)) composed from the differentiable single passes
+        kw = dict(L=L, spin=spin, nside=nside or 0, sampling=_lib.SAMPLING[s], reality=0,
+                  L_lower=L_lower, precision=_lib.PRECISION[precision], batch=B, N=0)
+        p0 = _lib.get_plan(x.device, iter=0, **kw)
+        flm_shape = batch_shape + (L, 2 * L - 1)
+        y = _ForwardFn.apply(x, p0, flm_shape, cdt)
+        for _ in range(int(iter)):
+            r = x - _InverseFn.apply(y, p0, batch_shape + fs, cdt)
+            y = y + _ForwardFn.apply(r, p0, flm_shape, cdt)
+        return _ret(y, was_np, odev)
     plan = _lib.get_plan(x.device, L=L, spin=spin, nside=nside or 0, sampling=_lib.SAMPLING[s],
                          reality=int(bool(reality)), L_lower=L_lower,
                          precision=_lib.PRECISION[precision], batch=B, iter=int(iter), N=0)

@@ -4,6 +4,14 @@ Same call surface as upstream ``s2fft.wigner.inverse`` / ``forward``
 (s2fft/transforms/wigner.py:13-107, 346-439): ``(flmn|f, L, N, nside, sampling,
 method, reality, precomps, L_lower)``. The transform is 2N-1 spin (-n)
 transforms run by ``libs2b.so`` plus a DFT over gamma.
+
+When a torch input requires grad, the transform is composed from the
+differentiable spin transforms (whose backward passes run the adjoint kernels)
+and a gamma DFT written as a dense (2N-1) x (2N-1) product.
+
+Difference from upstream: upstream's recursive methods raise ``Warning`` for
+N >= 8 (wigner.py:87-88); here the limit is the spin transforms' own (|spin| < 8),
+so N <= 8 is accepted.
 """
 
 from __future__ import annotations
@@ -12,7 +20,8 @@ import numpy as np
 import torch
 
 from . import _lib
-from .spherical import _check_method, _device, _dtypes, _ret, _to_device, f_shape
+from . import spherical as _sph
+from .spherical import _check_method, _device, _dtypes, _needs_grad, _ret, _to_device, f_shape
 
 
 def so3_f_shape(L, N, sampling="mw", nside=None):
@@ -27,8 +36,8 @@ def _check(L, N, nside, sampling, L_lower):
     s = sampling.lower()
     if s not in _lib.SAMPLING:
         raise ValueError(f"Sampling scheme sampling={sampling} not supported")
-    if N >= 8:
-        # upstream raises Warning for the recursive methods (wigner.py:87-88, 419-420)
+    if N > 8:
+        # spins -(N-1) .. N-1 must stay below 8 (upstream warns from N = 8, wigner.py:87-88)
         raise Warning("Recursive transform may provide lower precision beyond N ~ 8")
     if N < 1 or N > L:
         raise ValueError("1 <= N <= L required")
@@ -47,6 +56,57 @@ def _plan(dev, L, N, nside, s, reality, L_lower, precision, B):
                          precision=_lib.PRECISION[precision], batch=B, iter=0, N=N)
 
 
+def _gamma_phases(N, sign, device, dtype):
+    """P[k, j] = exp(sign 2 pi i (j - (N-1)) k / (2N-1)), k, j < 2N-1."""
+    G = 2 * N - 1
+    k = np.arange(G)[:, None]
+    n = np.arange(G)[None, :] - (N - 1)
+    ph = np.exp(sign * 2j * np.pi * ((n * k) % G) / G)
+    return torch.from_numpy(ph).to(device=device, dtype=dtype)
+
+
+def _lnorm(L, n, L_lower, device, dtype, inverse):
+    l = np.arange(L, dtype=np.float64)
+    if inverse:
+        v = (-1.0) ** n * np.sqrt((2 * l + 1) / (16 * np.pi ** 3))
+    else:
+        v = (-1.0) ** n * np.sqrt(4 * np.pi / (2 * l + 1))
+        v[:L_lower] = 0.0
+    return torch.from_numpy(v).to(device=device, dtype=dtype)[:, None]
+
+
+def _inverse_composed(x, L, N, nside, s, L_lower, precision):
+    """Differentiable inverse: 2N-1 spin(-n) inverses and the gamma inverse DFT
+    (s2fft/transforms/wigner.py:110-196)."""
+    rdt = x.real.dtype
+    fs = []
+    for j in range(2 * N - 1):
+        n = j - (N - 1)
+        t = x[..., j, :, :] * _lnorm(L, n, L_lower, x.device, rdt, True)
+        fs.append(_sph.inverse(t, L, -n, nside, s, L_lower=L_lower, precision=precision))
+    gdim = len(f_shape(L, s, nside))
+    fban = torch.stack(fs, dim=-gdim - 1)  # [.., 2N-1 (n), grid]
+    P = _gamma_phases(N, +1, x.device, x.dtype)
+    return torch.movedim(torch.tensordot(fban, P, dims=([-gdim - 1], [1])), -1, -gdim - 1)
+
+
+def _forward_composed(x, L, N, nside, s, L_lower, precision):
+    """Differentiable forward: gamma DFT times 2 pi/(2N-1), spin(-n) forwards
+    (s2fft/transforms/wigner.py:442-533)."""
+    rdt = x.real.dtype
+    gdim = len(f_shape(L, s, nside))
+    P = _gamma_phases(N, -1, x.device, x.dtype) * (2 * np.pi / (2 * N - 1))
+    # fban[.., j, grid] = sum_k P[k, j] f[.., k, grid]
+    fban = torch.movedim(torch.tensordot(x, P, dims=([-gdim - 1], [0])), -1, -gdim - 1)
+    out = []
+    for j in range(2 * N - 1):
+        n = j - (N - 1)
+        fb = fban.select(-gdim - 1, j)
+        flm = _sph.forward(fb, L, -n, nside, s, L_lower=L_lower, precision=precision)
+        out.append(flm * _lnorm(L, n, L_lower, x.device, rdt, False))
+    return torch.stack(out, dim=-3)
+
+
 def inverse(flmn, L: int, N: int, nside: int = None, sampling: str = "mw",
             method: str = "cuda", reality: bool = False, precomps=None, L_lower: int = 0,
             _ssht_backend: int = 1, precision: str = "f64"):
@@ -59,6 +119,10 @@ def inverse(flmn, L: int, N: int, nside: int = None, sampling: str = "mw",
         raise ValueError(f"flmn must have trailing shape {flmn_shape(L, N)}")
     bs = tuple(x.shape[:-3])
     B = int(np.prod(bs)) if bs else 1
+    if _needs_grad(x):
+        if reality:
+            raise NotImplementedError("gradients are available for complex transforms (reality=False)")
+        return _ret(_inverse_composed(x, L, N, nside, s, L_lower, precision), was_np, odev)
     plan = _plan(x.device, L, N, nside, s, reality, L_lower, precision, B)
     out = torch.empty(bs + so3_f_shape(L, N, s, nside), dtype=rdt if reality else cdt,
                       device=x.device)
@@ -87,6 +151,10 @@ def forward(f, L: int, N: int, nside: int = None, sampling: str = "mw", method: 
         raise ValueError(f"f must have trailing shape {fs}")
     bs = tuple(x.shape[:-len(fs)])
     B = int(np.prod(bs)) if bs else 1
+    if _needs_grad(x):
+        if reality:
+            raise NotImplementedError("gradients are available for complex transforms (reality=False)")
+        return _ret(_forward_composed(x, L, N, nside, s, L_lower, precision), was_np, odev)
     plan = _plan(x.device, L, N, nside, s, reality, L_lower, precision, B)
     out = torch.empty(bs + flmn_shape(L, N), dtype=cdt, device=x.device)
     ws = plan.workspace(True)

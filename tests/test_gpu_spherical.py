@@ -206,3 +206,18 @@ def test_bf16x3_tensor_core_forward(s2b, rng, spin):
 
     for plan in list(_lib._plans.values()):
         assert plan.status() == 0
+
+
+@pytest.mark.parametrize("sampling", ["mw", "gl", "mwss"])
+@pytest.mark.parametrize("spin", [4, -5, 7, -7])
+def test_f32_high_spin(s2b, rng, sampling, spin):
+    """float32 plans with |spin| >= 4 run the recursion on a float64 plan internally; the
+    float32 result must still meet the float32 tolerance."""
+    L = 48
+    flm = oracle.signal.generate_flm(rng, L, 0, spin, False)
+    ref = oracle.spherical.inverse(flm, L, spin, None, sampling)
+    f = s2b.inverse(flm, L, spin, None, sampling, precision="f32")
+    assert f.dtype == np.complex64
+    assert relerr(f, ref) < TOL32, relerr(f, ref)
+    g = s2b.forward(ref, L, spin, None, sampling, precision="f32")
+    assert relerr(g, flm) < TOL32, relerr(g, flm)
