@@ -231,6 +231,10 @@ def run_ours(args, rank, world, torch, dist):
     # mixed-path coefficient error against the float64 path (itself <= 1e-10 of the oracle)
     err_mixed = float((y32.to(torch.complex128) - y64).abs().max().item()
                       / y64.abs().max().item())
+    # a throughput number is only meaningful for a correct transform
+    if not (np.isfinite(err_mixed) and np.isfinite(err32) and err_mixed < 1e-4 and err64 < 1e-9):
+        raise RuntimeError(f"transform error out of bounds: mixed {err_mixed}, f32 round trip "
+                           f"{err32}, f64 round trip {err64}")
 
     # end to end through the public API with pinned host buffers
     host_in = torch.from_numpy(flm_np.astype(np.complex64)).pin_memory()
