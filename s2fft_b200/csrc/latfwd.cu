@@ -386,9 +386,16 @@ int fwd_group(bool fp64) { return fp64 ? 4 : 8; }
 
 cudaError_t launch_fwd2(bool fp64, bool dual, const Fwd2Params& p, cudaStream_t s) {
   if (p.nrings <= 0) return cudaSuccess;
-  if (!fp64)
+  if (!fp64) {
+    if (p.tile == 1)
+      return dual ? launch_fwd2_cfg<float, true, 8, 4, 8>(p, s)
+                  : launch_fwd2_cfg<float, false, 8, 4, 8>(p, s);
     return dual ? launch_fwd2_cfg<float, true, 16, 4, 8>(p, s)
                 : launch_fwd2_cfg<float, false, 16, 4, 8>(p, s);
+  }
+  if (p.tile == 1)
+    return dual ? launch_fwd2_cfg<double, true, 4, 4, 4>(p, s)
+                : launch_fwd2_cfg<double, false, 4, 4, 4>(p, s);
   return dual ? launch_fwd2_cfg<double, true, 8, 4, 4>(p, s)
               : launch_fwd2_cfg<double, false, 8, 4, 4>(p, s);
 }

@@ -311,10 +311,13 @@ static cudaError_t launch_inv2_cfg(const Inv2Params& p, cudaStream_t s) {
 
 cudaError_t launch_inv2(bool fp64, bool dual, const Inv2Params& p, cudaStream_t s) {
   if (p.nrings <= 0) return cudaSuccess;
-  if (!fp64)
-    // 2 rings per lane, 4-step groups: near the poles a float mantissa can grow by ~2^60
-    // in 4 steps, so the renormalisation check must run at least every 4 steps
+  if (!fp64) {
+    // 2 rings per lane (tile 1: one), 4-step groups: near the poles a float mantissa can
+    // grow by ~2^60 in 4 steps, so the renormalisation check must run at least every 4 steps
+    if (p.tile == 1)
+      return dual ? launch_inv2_cfg<float, true, 1, 4>(p, s) : launch_inv2_cfg<float, false, 1, 4>(p, s);
     return dual ? launch_inv2_cfg<float, true, 2, 4>(p, s) : launch_inv2_cfg<float, false, 2, 4>(p, s);
+  }
   return dual ? launch_inv2_cfg<double, true, 1, 8>(p, s) : launch_inv2_cfg<double, false, 1, 8>(p, s);
 }
 

@@ -385,6 +385,7 @@ struct s2b_plan {
   std::vector<s2b_plan*> subs;
   size_t ws_w_fban = 0, ws_w_tmp = 0, ws_w_sub = 0;
   // optional events recorded around the latitudinal launch ([0] inverse, [1] forward)
+  int tile_fwd = 0, tile_inv = 0;  // latitudinal tile variants (s2b_plan_set_tuning)
   cudaEvent_t ev_begin[2] = {nullptr, nullptr};
   cudaEvent_t ev_end[2] = {nullptr, nullptr};
   // workspace layout (bytes)
@@ -882,6 +883,7 @@ static int run_inverse(s2b_plan* p, const void* flm, void* f, char* ws, cudaStre
     lp.ncol = p->inv_ncol;
     lp.mo = p->inv_mo;
     lp.status = p->status;
+    lp.tile = p->tile_inv;
     if (p->ev_begin[0]) S2B_CK(cudaEventRecord(p->ev_begin[0], s));
     S2B_CK(launch_inv2(p->fp64, p->dual, lp, s));
     if (p->ev_end[0]) S2B_CK(cudaEventRecord(p->ev_end[0], s));
@@ -1143,6 +1145,7 @@ static int run_forward_once(s2b_plan* p, const void* f, void* flm, char* ws, cud
   lp.Gs = p->Gs;
   lp.acc = acc;
   lp.status = p->status;
+  lp.tile = p->tile_fwd;
   if (p->ev_begin[1]) S2B_CK(cudaEventRecord(p->ev_begin[1], s));
   S2B_CK(launch_fwd2(p->fp64, p->dual, lp, s));
   if (p->ev_end[1]) S2B_CK(cudaEventRecord(p->ev_end[1], s));
@@ -1661,6 +1664,18 @@ int s2b_plan_status(s2b_plan* p, int* status) {
   const int rc = plan_status_word(p, status);
   if (rc) return rc;
   if (*status) return fail(S2B_ERR_TIMEOUT, "a bounded device wait gave up");
+  return S2B_OK;
+}
+
+int s2b_plan_set_tuning(s2b_plan* p, int key, int value) {
+  if (!p || (key != 0 && key != 1) || (value != 0 && value != 1))
+    return fail(S2B_ERR_INVALID, "key must be 0 (forward) or 1 (inverse), value 0 or 1");
+  if (key == 0)
+    p->tile_fwd = value;
+  else
+    p->tile_inv = value;
+  if (p->shadow) s2b_plan_set_tuning(p->shadow, key, value);
+  for (s2b_plan* sp : p->subs) s2b_plan_set_tuning(sp, key, value);
   return S2B_OK;
 }
 

@@ -38,6 +38,7 @@ struct Fwd2Params {
   int Gs;
   void* acc;                // [batch][nhalf][L (m)][NB*32 (l)] projected sums (Real4 when dual)
   int* status;
+  int tile;                 // 0: default rings per warp, 1: half of it (more CTAs)
 };
 
 // Inverse latitudinal step, blocked layout (latinv.cu).
@@ -53,6 +54,7 @@ struct Inv2Params {
   const int* ring_row;
   int nrows, ncol, mo;
   int* status;
+  int tile;                 // 0: default rings per lane, 1: one ring per lane (more CTAs)
 };
 cudaError_t launch_inv2(bool fp64, bool dual, const Inv2Params& p, cudaStream_t s);
 
