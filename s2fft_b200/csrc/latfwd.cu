@@ -382,7 +382,10 @@ static cudaError_t launch_fwd2_cfg(const Fwd2Params& p, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-int fwd_group(bool fp64) { return fp64 ? 4 : 8; }
+int fwd_group(bool fp64) {
+  (void)fp64;
+  return 8;  // start tables serve 8-step groups (and 4-step ones: 7 = 3 mod 4)
+}
 
 cudaError_t launch_fwd2(bool fp64, bool dual, const Fwd2Params& p, cudaStream_t s) {
   if (p.nrings <= 0) return cudaSuccess;

@@ -12,16 +12,13 @@
 //    blocks p and NB-1-p, so all warps stay busy), so the coefficient loads h_{l,m} and
 //    flm'[l, m] are shared-memory broadcasts and the sum over l stays in
 //    registers over 16 terms before warps' partial sums meet in shared memory;
-//  * states carry the monic mantissa and an exponent (value = v 2^(kScale e)) as
-//    in the seed table; the exponent lives in the gating operand itself: sc = 1
-//    once the state is significant (e >= 0), otherwise sc is the negative
-//    denormal with integer mantissa -e, so x = v * sc stays below 2^-70 and the
-//    exponent costs no register;
-//  * a state is loaded from its seed at kernel start and placed at the first
-//    group start M >= l with the exact continuation of the recursion above m = l
-//    (h_{l,m} = 0 for m > l: dt_{l+2j} = (-1)^j dt_l, dt_{l+2j+1} = 0), so the
-//    warp needs no activation logic; a block's degrees are skipped until the
-//    recursion reaches the block. Partial sums meet every R = 8 steps.
+//  * restart at first significance, as in the forward kernel: per (ring, 32-degree
+//    block) the recursion starts at the block's first significant group start M with
+//    the double-precision start values (d~_M, d~_{M+1}) of every degree (degrees below
+//    M begin with the exact continuation above m = l); the loop runs the plain monic
+//    recursion with no exponent, no gating multiply and no renormalisation, and a
+//    block's degrees are skipped until the recursion reaches the block on any ring of
+//    the CTA. A lane starts its (ring, block) states when the group start equals M.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -31,22 +28,6 @@
 #include "s2b_latfwd.h"
 
 namespace s2b {
-
-template <typename Real>
-struct SigBits;
-template <>
-struct SigBits<float> {
-  // sc for an exponent e < 0 / exponent of a gating operand that is not 1
-  __device__ static float enc(int e) { return __int_as_float((int)(0x80000000u | (unsigned)(-e))); }
-  __device__ static int dec(float sc) { return -(__float_as_int(sc) & 0x7fffff); }
-};
-template <>
-struct SigBits<double> {
-  __device__ static double enc(int e) {
-    return __longlong_as_double((long long)(0x8000000000000000ull | (unsigned long long)(-e)));
-  }
-  __device__ static int dec(double sc) { return -(int)(__double_as_longlong(sc) & 0xfffffff); }
-};
 
 template <typename Real, bool DUAL, int T, int W, int R>
 struct Inv2Layout {
@@ -70,7 +51,6 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
   using Lay = Inv2Layout<Real, DUAL, T, W, R>;
   using Acc = typename Lay::Acc;
   using R2 = typename Vec<Real>::t2;
-  using SB = SigBits<Real>;
   constexpr int K = Lay::K;
   constexpr int NRT = Lay::NRT;
   constexpr int NT = Lay::NT;
@@ -94,45 +74,34 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
   // degrees of this warp: slot k < 8 -> l = 32 kb0 + 8 wp + k, slot k >= 8 -> 32 kb1 + 8 wp + k - 8,
   // so every warp works on both blocks of the CTA
   const int col0 = wp * (K / 2);
-  auto slot_l = [&](int k) { return (k < K / 2 ? kb0 : kb1) * kFwdBlock + col0 + (k % (K / 2)); };
-  // first group start of each block (all states of a block join the recursion there)
+  // first group start of every (ring, block) state of this lane, and per block the
+  // earliest one over the CTA (all warps hold the same rings)
+  int Ms[2][T];
   int Mb[2];
 #pragma unroll
   for (int x = 0; x < 2; ++x) {
-    const int base = (x ? kb1 : kb0) * kFwdBlock;
-    const int top = base + kFwdBlock - 1 < L ? base + kFwdBlock - 1 : L - 1;
-    Mb[x] = base < L ? (top | (R - 1)) : -1;
+    int mx = -1;
+#pragma unroll
+    for (int i = 0; i < T; ++i) {
+      const int r = r0 + lane * T + i;
+      Ms[x][i] = r < p.nrings ? p.Mst[((size_t)half * NB + (x ? kb1 : kb0)) * p.nrings + r] : -1;
+      mx = Ms[x][i] > mx ? Ms[x][i] : mx;
+    }
+    Mb[x] = __reduce_max_sync(0xffffffffu, mx);
   }
   const int mtop = Mb[0] > Mb[1] ? Mb[0] : Mb[1];
-  if (mtop < 0) return;  // padding pair (uniform)
+  if (mtop < 0) return;  // nothing significant in this tile (uniform)
   const int ngroups = (mtop + 1) / R;
+  const R2* __restrict__ Vst = reinterpret_cast<const R2*>(p.Vst);
 
-  // states from the seeds, placed at the block's first group start
-  Real v[K][T], w[K][T], sc[K][T];
-  {
-    const SeedT<Real>* __restrict__ seeds = reinterpret_cast<const SeedT<Real>*>(p.seeds);
+  Real v[K][T], w[K][T];
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const int l = slot_l(k);
-      const int M = Mb[k / (K / 2)];
+  for (int k = 0; k < K; ++k)
 #pragma unroll
-      for (int i = 0; i < T; ++i) {
-        const int r = r0 + lane * T + i;
-        SeedT<Real> sd{Real(0), 0};
-        if (l < L && r < p.nrings)
-          sd = seeds[(((size_t)half * p.C + l % p.C) * p.Qp + l / p.C) * p.nrings + r];
-        const int dlt = M - l;
-        Real cur = Real(0), prv = Real(0);
-        if ((dlt & 1) == 0)
-          cur = ((dlt >> 1) & 1) ? -sd.v : sd.v;
-        else
-          prv = (((dlt + 1) >> 1) & 1) ? -sd.v : sd.v;
-        v[k][i] = cur;
-        w[k][i] = prv;
-        sc[k][i] = sd.e >= 0 ? Real(1) : SB::enc(sd.e);
-      }
+    for (int i = 0; i < T; ++i) {
+      v[k][i] = Real(0);
+      w[k][i] = Real(0);
     }
-  }
 
   const Real* __restrict__ Hb = reinterpret_cast<const Real*>(p.Hb);
   const Acc* __restrict__ Fin =
@@ -180,34 +149,24 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
     lmax = kb1 * kFwdBlock + kFwdBlock - 1;
   if (lmax > L - 1) lmax = L - 1;
 
-  // rescale states whose mantissa grew past the trigger (only states below significance
-  // grow that far). Run every 4 steps: near the poles the monic state can grow by ~2^15 per
-  // step, so 4 steps from just below the trigger (2^48) stay inside the float range.
-  auto renorm = [&]() {
-    Real mx = Real(0);
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-#pragma unroll
-      for (int i = 0; i < T; ++i) mx = fmax(mx, fabs(v[k][i]));
-    const Real trig = Scaling<Real>::kTrig;
-    if (mx > trig) {
-      const Real down = Scaling<Real>::kDown;
-#pragma unroll
-      for (int k = 0; k < K; ++k)
-#pragma unroll
-        for (int i = 0; i < T; ++i)
-          if (fabs(v[k][i]) > trig) {
-            v[k][i] *= down;
-            w[k][i] *= down;
-            const int e = SB::dec(sc[k][i]) + 1;
-            sc[k][i] = e >= 0 ? Real(1) : SB::enc(e);
-          }
-    }
-  };
-
   for (int grp = 0; grp < ngroups; ++grp) {
     const int mgrp = mtop - grp * R;
     const bool ok = mbar_wait(&mbar[grp & 1], (grp >> 1) & 1);
+    // start the (ring, block) states whose first group start is this group's
+#pragma unroll
+    for (int x = 0; x < 2; ++x)
+#pragma unroll
+      for (int i = 0; i < T; ++i)
+        if (Ms[x][i] == mgrp) {
+          const R2* src = Vst + (((size_t)half * NB + (x ? kb1 : kb0)) * p.nrings + r0 + lane * T + i) *
+                                    kFwdBlock + col0;
+#pragma unroll
+          for (int kk = 0; kk < K / 2; ++kk) {
+            const R2 sv = src[kk];
+            v[x * (K / 2) + kk][i] = sv.x;
+            w[x * (K / 2) + kk][i] = sv.y;
+          }
+        }
     const unsigned char* st = stage_base + (size_t)(grp & 1) * Lay::stage_bytes;
     const Real* hS = reinterpret_cast<const Real*>(st) + col0;
     const Acc* fS = reinterpret_cast<const Acc*>(st + Lay::h_bytes) + col0;
@@ -232,8 +191,7 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
           const Real h = hS[so];                                                        \
           const Acc f = fS[so];                                                         \
           _Pragma("unroll") for (int i = 0; i < T; ++i) {                               \
-            const Real xv = CUR[k][i] * sc[k][i];                                       \
-            acc_fma(a[x][i], xv, f);                                                    \
+            acc_fma(a[x][i], CUR[k][i], f);                                             \
             PRV[k][i] = fma(lam[i] * h, CUR[k][i], -PRV[k][i]);                         \
           }                                                                             \
         }                                                                               \
@@ -249,7 +207,6 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
     S2B_INV2_STEP(v, w, 2)
     S2B_INV2_STEP(w, v, 3)
     if constexpr (R == 8) {
-      renorm();
       S2B_INV2_STEP(v, w, 4)
       S2B_INV2_STEP(w, v, 5)
       S2B_INV2_STEP(v, w, 6)
@@ -293,7 +250,6 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
     }
     __syncthreads();
     if (tid == 0 && grp + 2 < ngroups) issue(grp + 2);
-    renorm();
   }
 }
 
@@ -312,11 +268,10 @@ static cudaError_t launch_inv2_cfg(const Inv2Params& p, cudaStream_t s) {
 cudaError_t launch_inv2(bool fp64, bool dual, const Inv2Params& p, cudaStream_t s) {
   if (p.nrings <= 0) return cudaSuccess;
   if (!fp64) {
-    // 2 rings per lane (tile 1: one), 4-step groups: near the poles a float mantissa can
-    // grow by ~2^60 in 4 steps, so the renormalisation check must run at least every 4 steps
+    // 2 rings per lane (tile 1: one), 8-step groups (the start tables' alignment)
     if (p.tile == 1)
-      return dual ? launch_inv2_cfg<float, true, 1, 4>(p, s) : launch_inv2_cfg<float, false, 1, 4>(p, s);
-    return dual ? launch_inv2_cfg<float, true, 2, 4>(p, s) : launch_inv2_cfg<float, false, 2, 4>(p, s);
+      return dual ? launch_inv2_cfg<float, true, 1, 8>(p, s) : launch_inv2_cfg<float, false, 1, 8>(p, s);
+    return dual ? launch_inv2_cfg<float, true, 2, 8>(p, s) : launch_inv2_cfg<float, false, 2, 8>(p, s);
   }
   return dual ? launch_inv2_cfg<double, true, 1, 8>(p, s) : launch_inv2_cfg<double, false, 1, 8>(p, s);
 }

@@ -340,8 +340,6 @@ struct s2b_plan {
   int* inv_ring_row = nullptr;
   RingInfo* fwd_rings = nullptr;
   int* fwd_ring_row = nullptr;
-  void* inv_seeds = nullptr;
-  void* fwd_seeds = nullptr;
   void* inv_lam = nullptr;
   void* fwd_lam = nullptr;
   int inv_Ls = 4, fwd_Ls = 4;
@@ -364,10 +362,10 @@ struct s2b_plan {
   void* bf = nullptr;
   int row_desc = 0, col_d1 = 0, col_d2 = 0, maxM = 2, M1 = 2, M2 = 2;
   void* col_ph = nullptr;  // column chain: chirp * half-sample phase / n1 per 4L-bin
-  // adjoints: projection over the inverse rings (start tables), ring -> column map of the
+  // start tables of the inverse rings (inverse and its adjoint), ring -> column map of the
   // adjoint spectra (recursed rings first, then north / south pole), adjoint chain table
-  int* adj_Mst = nullptr;
-  void* adj_Vst = nullptr;
+  int* inv_Mst = nullptr;
+  void* inv_Vst = nullptr;
   int* adj_col = nullptr;
   int adj_Gs = 4, adj_pole_s = -1, adj_pole_n = -1;
   void* col_ph_adj = nullptr;
@@ -608,21 +606,6 @@ static int build_plan(s2b_plan* p) {
   p->allocs.push_back(p->status);
   S2B_CK(cudaMemset(p->status, 0, sizeof(int)));
 
-  // ---- seeds (device kernel, double arithmetic)
-  {
-    const size_t bi = seed_bytes(p->fp64, L, p->nhalf, p->inv_nrings);
-    const size_t bf = seed_bytes(p->fp64, L, p->nhalf, p->fwd_nrings);
-    S2B_CK(cudaMalloc(&p->inv_seeds, std::max<size_t>(bi, 16)));
-    p->allocs.push_back(p->inv_seeds);
-    S2B_CK(cudaMalloc(&p->fwd_seeds, std::max<size_t>(bf, 16)));
-    p->allocs.push_back(p->fwd_seeds);
-    if (p->inv_nrings > 0)
-      S2B_CK(launch_seeds(p->fp64, L, d.L_lower, d.spin, p->nhalf, p->inv_rings, p->inv_nrings,
-                          p->lbin, p->inv_seeds, 0));
-    S2B_CK(launch_seeds(p->fp64, L, d.L_lower, d.spin, p->nhalf, p->fwd_rings, p->fwd_nrings,
-                        p->lbin, p->fwd_seeds, 0));
-  }
-
   // ---- forward start tables (device kernel, double arithmetic)
   if (p->fwd_nrings > 0) {
     const size_t nst = (size_t)p->nhalf * p->fwd_NB * p->fwd_nrings;
@@ -637,8 +620,8 @@ static int build_plan(s2b_plan* p) {
     fp.nhalf = p->nhalf;
     fp.nrings = p->fwd_nrings;
     fp.NB = p->fwd_NB;
-    // contributions below 2^-40 (float) / 2^-70 (double) of |d| <= 1 are dropped
-    fp.floor_log2 = p->fp64 ? -70.0 : -40.0;
+    // contributions below 2^-32 (float) / 2^-70 (double) of |d| <= 1 are dropped
+    fp.floor_log2 = p->fp64 ? -70.0 : -32.0;
     fp.group = fwd_group(p->fp64);
     fp.rings = p->fwd_rings;
     fp.lbin = p->lbin;
@@ -647,13 +630,13 @@ static int build_plan(s2b_plan* p) {
     fp.Vst = p->fwd_Vst;
     S2B_CK(launch_fwd_start(p->fp64, fp, 0));
   }
-  // ---- adjoint of the inverse: the forward projection over the inverse rings
+  // ---- start tables of the inverse rings (inverse kernel and adjoint of the inverse)
   if (p->inv_nrings > 0) {
     const size_t nst = (size_t)p->nhalf * p->fwd_NB * p->inv_nrings;
-    S2B_CK(cudaMalloc(&p->adj_Mst, nst * sizeof(int)));
-    p->allocs.push_back(p->adj_Mst);
-    S2B_CK(cudaMalloc(&p->adj_Vst, fwd_start_bytes(p->fp64, L, p->nhalf, p->inv_nrings)));
-    p->allocs.push_back(p->adj_Vst);
+    S2B_CK(cudaMalloc(&p->inv_Mst, nst * sizeof(int)));
+    p->allocs.push_back(p->inv_Mst);
+    S2B_CK(cudaMalloc(&p->inv_Vst, fwd_start_bytes(p->fp64, L, p->nhalf, p->inv_nrings)));
+    p->allocs.push_back(p->inv_Vst);
     FwdStartParams fp{};
     fp.L = L;
     fp.L0 = d.L_lower;
@@ -661,13 +644,13 @@ static int build_plan(s2b_plan* p) {
     fp.nhalf = p->nhalf;
     fp.nrings = p->inv_nrings;
     fp.NB = p->fwd_NB;
-    fp.floor_log2 = p->fp64 ? -70.0 : -40.0;
+    fp.floor_log2 = p->fp64 ? -70.0 : -32.0;
     fp.group = fwd_group(p->fp64);
     fp.rings = p->inv_rings;
     fp.lbin = p->lbin;
     fp.g = p->gtab;
-    fp.Mst = p->adj_Mst;
-    fp.Vst = p->adj_Vst;
+    fp.Mst = p->inv_Mst;
+    fp.Vst = p->inv_Vst;
     S2B_CK(launch_fwd_start(p->fp64, fp, 0));
   }
 
@@ -870,9 +853,8 @@ static int run_inverse(s2b_plan* p, const void* flm, void* f, char* ws, cudaStre
     lp.nhalf = p->nhalf;
     lp.batch = d.batch;
     lp.NB = p->fwd_NB;
-    lp.C = p->nclass;
-    lp.Qp = p->Q;
-    lp.seeds = p->inv_seeds;
+    lp.Mst = p->inv_Mst;
+    lp.Vst = p->inv_Vst;
     lp.Hb = p->fwd_Hb;
     lp.lam = p->inv_lam;
     lp.Ls = p->inv_Ls;
@@ -949,8 +931,8 @@ static int run_inverse_adjoint(s2b_plan* p, const void* gf, void* gflm, char* ws
     lp.nhalf = p->nhalf;
     lp.batch = d.batch;
     lp.NB = p->fwd_NB;
-    lp.Mst = p->adj_Mst;
-    lp.Vst = p->adj_Vst;
+    lp.Mst = p->inv_Mst;
+    lp.Vst = p->inv_Vst;
     lp.Hb = p->fwd_Hb;
     lp.lam = p->inv_lam;
     lp.Ls = p->inv_Ls;
@@ -1024,9 +1006,8 @@ static int run_forward_adjoint(s2b_plan* p, const void* gflm, void* gf, char* ws
   lp.nhalf = p->nhalf;
   lp.batch = d.batch;
   lp.NB = p->fwd_NB;
-  lp.C = p->nclass;
-  lp.Qp = p->Q;
-  lp.seeds = p->fwd_seeds;
+  lp.Mst = p->fwd_Mst;
+  lp.Vst = p->fwd_Vst;
   lp.Hb = p->fwd_Hb;
   lp.lam = p->fwd_lam;
   lp.Ls = p->fwd_Ls;

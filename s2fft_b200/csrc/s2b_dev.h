@@ -23,13 +23,6 @@ struct Vec<double> {
   using t4 = double4;
 };
 
-// Recursion seed: mantissa and exponent (value = v * 2^(kScale e), see Scaling).
-template <typename Real>
-struct SeedT {
-  Real v;
-  int e;
-};
-
 template <typename T2>
 __device__ __forceinline__ void red_add(T2* addr, T2 v);
 template <>

@@ -44,8 +44,8 @@ struct Fwd2Params {
 // Inverse latitudinal step, blocked layout (latinv.cu).
 struct Inv2Params {
   int L, nrings, nhalf, batch, NB;
-  int C, Qp;                // seed table geometry: [nhalf][C][Qp][nrings], l = j + C q
-  const void* seeds;        // {mantissa, exponent} of d^l_{l,n}(theta)
+  const int* Mst;           // start tables of these rings (FwdStartParams layout)
+  const void* Vst;
   const void* Hb;           // [NB][tab_rows][32]
   const void* lam;          // [nhalf][tab_rows][Ls]
   int Ls;
