@@ -267,7 +267,7 @@ __device__ __forceinline__ int pmod(int a, int n) {
 // One CTA per (ring, map). Column c of ftm holds m = c - (L-1) - mo.
 // ---------------------------------------------------------------------------
 template <typename Real>
-__global__ void inv_rows_kernel(RowsParams<Real> p) {
+__global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) inv_rows_kernel(RowsParams<Real> p) {
   using R2 = typename C2<Real>::t;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R2* s = reinterpret_cast<R2*>(smem_raw);
@@ -386,7 +386,7 @@ __device__ __forceinline__ void store_spectra(const RowsParams<Real>& p, int b, 
 // the MW/MWSS resampling chain, the transposed raw spectra Fc [B][ncolm][nrows].
 // ---------------------------------------------------------------------------
 template <typename Real>
-__global__ void fwd_rows_kernel(RowsParams<Real> p) {
+__global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) fwd_rows_kernel(RowsParams<Real> p) {
   using R2 = typename C2<Real>::t;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R2* s = reinterpret_cast<R2*>(smem_raw);
@@ -460,7 +460,7 @@ __global__ void fwd_rows_kernel(RowsParams<Real> p) {
 //   reduces to the overall factor 2L/(2L-1) in the phi-Fourier domain.
 // ---------------------------------------------------------------------------
 template <typename Real>
-__global__ void mw_cols_kernel(ColsParams<Real> p) {
+__global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) mw_cols_kernel(ColsParams<Real> p) {
   using R2 = typename C2<Real>::t;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const FFTDesc d1 = *p.d1;
@@ -570,7 +570,7 @@ __global__ void mw_cols_kernel(ColsParams<Real> p) {
 //   onto the input rings with the parity (-1)^(m+s).
 // ---------------------------------------------------------------------------
 template <typename Real>
-__global__ void mw_cols_adj_kernel(ColsParams<Real> p, int ncol_out, int mo_out) {
+__global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) mw_cols_adj_kernel(ColsParams<Real> p, int ncol_out, int mo_out) {
   using R2 = typename C2<Real>::t;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const FFTDesc d1 = *p.d1;
@@ -644,6 +644,9 @@ cudaError_t launch_inv_rows(const RowsParams<Real>& p, int nrings, int batch, in
   cudaError_t e = cudaFuncSetAttribute(inv_rows_kernel<Real>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(inv_rows_kernel<Real>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           cudaSharedmemCarveoutMaxShared);
+  if (e != cudaSuccess) return e;
   inv_rows_kernel<Real><<<dim3(nrings, batch), fft_threads(maxM), smem, s>>>(p);
   return cudaGetLastError();
 }
@@ -655,6 +658,9 @@ cudaError_t launch_fwd_rows(const RowsParams<Real>& p, int nrings, int batch, in
   const size_t smem = (size_t)padded_len(maxM) * sizeof(R2);
   cudaError_t e = cudaFuncSetAttribute(fwd_rows_kernel<Real>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(fwd_rows_kernel<Real>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
   fwd_rows_kernel<Real><<<dim3(nrings, batch), fft_threads(maxM), smem, s>>>(p);
   return cudaGetLastError();
@@ -668,6 +674,9 @@ cudaError_t launch_mw_cols(const ColsParams<Real>& p, int ncm, int batch, int M1
   cudaError_t e = cudaFuncSetAttribute(mw_cols_kernel<Real>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(mw_cols_kernel<Real>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           cudaSharedmemCarveoutMaxShared);
+  if (e != cudaSuccess) return e;
   mw_cols_kernel<Real><<<dim3(ncm, batch), fft_threads(M1 > M2 ? M1 : M2), smem, s>>>(p);
   return cudaGetLastError();
 }
@@ -679,6 +688,9 @@ cudaError_t launch_mw_cols_adj(const ColsParams<Real>& p, int ncm, int batch, in
   const size_t smem = (size_t)(padded_len(M1) + padded_len(M2)) * sizeof(R2);
   cudaError_t e = cudaFuncSetAttribute(mw_cols_adj_kernel<Real>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(mw_cols_adj_kernel<Real>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
   mw_cols_adj_kernel<Real><<<dim3(ncm, batch), fft_threads(M1 > M2 ? M1 : M2), smem, s>>>(
       p, ncol_out, mo_out);
