@@ -236,27 +236,56 @@ def run_ours(args, rank, world, torch, dist):
         raise RuntimeError(f"transform error out of bounds: mixed {err_mixed}, f32 round trip "
                            f"{err32}, f64 round trip {err64}")
 
-    # end to end through the public API with pinned host buffers
-    host_in = torch.from_numpy(flm_np.astype(np.complex64)).pin_memory()
-    host_out = torch.empty_like(host_in).pin_memory()
-    for _ in range(2):
-        xd = host_in.to(dev, non_blocking=True)
-        yd = s2fft_b200.forward(s2fft_b200.inverse(xd, L, precision="f32"), L, precision="f32")
-        host_out.copy_(yd, non_blocking=True)
-    torch.cuda.synchronize()
-    e_steps = max(3, steps // 2)
-    evs = []
-    for _ in range(e_steps):
-        flush.zero_()
-        e = [torch.cuda.Event(True) for _ in range(2)]
-        e[0].record()
-        xd = host_in.to(dev, non_blocking=True)
-        yd = s2fft_b200.forward(s2fft_b200.inverse(xd, L, precision="f32"), L, precision="f32")
-        host_out.copy_(yd, non_blocking=True)
-        e[1].record()
-        evs.append(e)
-    torch.cuda.synchronize()
-    e2e_ms = sum(a.elapsed_time(b) for a, b in evs)
+    # end to end through the public API with pinned host buffers: each step copies its
+    # coefficients host -> device, runs inverse + forward and copies the result back. The
+    # copies run on their own streams with double-buffered pinned memory, so step i's
+    # transfers overlap the compute of its neighbours (as a pipelined user would do); the
+    # timed region spans the whole job, first upload and last download included, with an L2
+    # flush on the compute stream before every step.
+    nb = 2
+    host_in = [torch.from_numpy(flm_np.astype(np.complex64)).pin_memory() for _ in range(nb)]
+    host_out = [torch.empty_like(host_in[0]).pin_memory() for _ in range(nb)]
+    dev_in = [torch.empty(host_in[0].shape, dtype=torch.complex64, device=dev) for _ in range(nb)]
+    comp = torch.cuda.current_stream(dev)
+    up, down = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+
+    def e2e_job(nsteps):
+        ev_up = [torch.cuda.Event() for _ in range(nb)]
+        ev_done = [torch.cuda.Event() for _ in range(nb)]
+        ev_read = [torch.cuda.Event() for _ in range(nb)]
+        start, end = torch.cuda.Event(True), torch.cuda.Event(True)
+        start.record(comp)
+        up.wait_stream(comp)
+        down.wait_stream(comp)
+        for i in range(nsteps):
+            j = i % nb
+            if i >= nb:
+                up.wait_event(ev_read[j])  # compute of step i-nb has consumed dev_in[j]
+            with torch.cuda.stream(up):
+                dev_in[j].copy_(host_in[j], non_blocking=True)
+                ev_up[j].record(up)
+            comp.wait_event(ev_up[j])
+            flush.zero_()
+            yd = s2fft_b200.forward(s2fft_b200.inverse(dev_in[j], L, precision="f32"), L,
+                                    precision="f32")
+            ev_read[j].record(comp)
+            ev_done[j].record(comp)
+            down.wait_event(ev_done[j])
+            with torch.cuda.stream(down):
+                host_out[j].copy_(yd, non_blocking=True)
+            yd.record_stream(down)
+        comp.wait_stream(up)
+        comp.wait_stream(down)
+        end.record(comp)
+        torch.cuda.synchronize()
+        return start.elapsed_time(end), yd
+
+    e2e_job(2)
+    e_steps = max(8, steps)
+    e2e_ms, y_last = e2e_job(e_steps)
+    j_last = (e_steps - 1) % nb
+    if not torch.equal(host_out[j_last], y_last.cpu()):
+        raise RuntimeError("pipelined end-to-end result differs from the device result")
 
     t = torch.tensor([ms32, ms64, e2e_ms], dtype=torch.float64, device=dev)
     if dist is not None:
@@ -267,7 +296,7 @@ def run_ours(args, rank, world, torch, dist):
     e2e = world * e_steps / (e2e_ms * 1e-3)
     return dict(value=value, value64=value64, e2e=e2e, ms32=ms32 / steps, lat32=lat32,
                 lat64=lat64, err32=err32, err64=err64, err_mixed=err_mixed, clocks=clk,
-                T_inv=T_inv, T_fwd=T_fwd, h2d=host_in.numel() * 8, d2h=host_out.numel() * 8)
+                T_inv=T_inv, T_fwd=T_fwd, h2d=host_in[0].numel() * 8, d2h=host_out[0].numel() * 8)
 
 
 # ---------------------------------------------------------------------------
