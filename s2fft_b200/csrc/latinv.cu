@@ -41,7 +41,9 @@ struct Inv2Layout {
   static constexpr size_t l_bytes = (size_t)R * NRT * sizeof(Real);
   static constexpr size_t stage_bytes = h_bytes + f_bytes + l_bytes;
   static constexpr size_t buf_bytes = (size_t)R * W * NRT * sizeof(Acc);
-  static constexpr size_t total = 2 * stage_bytes + buf_bytes + 16;
+  // start values of the CTA's states: [2 blocks][NRT rings][32] (d~_M, d~_{M+1})
+  static constexpr size_t v_bytes = (size_t)2 * NRT * kFwdBlock * 2 * sizeof(Real);
+  static constexpr size_t total = 2 * stage_bytes + buf_bytes + v_bytes + 32;
   static_assert(W == 4, "two warps per 32-degree block, two blocks per CTA");
   static_assert(stage_bytes % 16 == 0 && buf_bytes % 16 == 0, "align");
 };
@@ -58,7 +60,10 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char* stage_base = smem_raw;
   Acc* buf = reinterpret_cast<Acc*>(smem_raw + 2 * Lay::stage_bytes);
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_raw + 2 * Lay::stage_bytes + Lay::buf_bytes);
+  const typename Vec<Real>::t2* vS = reinterpret_cast<const typename Vec<Real>::t2*>(
+      smem_raw + 2 * Lay::stage_bytes + Lay::buf_bytes);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_raw + 2 * Lay::stage_bytes + Lay::buf_bytes +
+                                               Lay::v_bytes);  // [0], [1] stages, [2] start values
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -135,13 +140,26 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
   if (tid == 0) {
     mbar_init(&mbar[0], 1);
     mbar_init(&mbar[1], 1);
+    mbar_init(&mbar[2], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
   if (tid == 0) {
+    // the start values of both blocks for this CTA's rings, once
+    int nr = p.nrings - r0;
+    if (nr > NRT) nr = NRT;
+    const unsigned vb = (unsigned)(nr * kFwdBlock * sizeof(R2));
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(&mbar[2], 2 * vb);
+#pragma unroll
+    for (int x = 0; x < 2; ++x)
+      bulk_g2s(const_cast<R2*>(vS) + (size_t)x * NRT * kFwdBlock,
+               Vst + (((size_t)half * NB + (x ? kb1 : kb0)) * p.nrings + r0) * kFwdBlock, vb,
+               &mbar[2]);
     issue(0);
     if (ngroups > 1) issue(1);
   }
+  const bool vok = mbar_wait(&mbar[2], 0);
   // highest degree of the CTA: partial sums above it are zero
   int lmax = -1;
   if (kb0 * kFwdBlock < L) lmax = kb0 * kFwdBlock + kFwdBlock - 1;
@@ -158,8 +176,7 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
 #pragma unroll
       for (int i = 0; i < T; ++i)
         if (Ms[x][i] == mgrp) {
-          const R2* src = Vst + (((size_t)half * NB + (x ? kb1 : kb0)) * p.nrings + r0 + lane * T + i) *
-                                    kFwdBlock + col0;
+          const R2* src = vS + ((size_t)x * NRT + lane * T + i) * kFwdBlock + col0;
 #pragma unroll
           for (int kk = 0; kk < K / 2; ++kk) {
             const R2 sv = src[kk];
@@ -214,7 +231,7 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
     }
 #undef S2B_INV2_STEP
 
-    if (!__syncthreads_and(ok)) {
+    if (!__syncthreads_and(ok && vok)) {
       if (tid == 0) {
         atomicExch(p.status, 1);
         mbar_wait(&mbar[(grp + 1) & 1], ((grp + 1) >> 1) & 1);
