@@ -393,6 +393,7 @@ cudaError_t launch_fwd2(bool fp64, bool dual, const Fwd2Params& p, cudaStream_t 
     if (p.tile == 1)
       return dual ? launch_fwd2_cfg<float, true, 8, 4, 8>(p, s)
                   : launch_fwd2_cfg<float, false, 8, 4, 8>(p, s);
+    // 16 rings x 4 warps (measured at L=1024: 0.46 ms; 2 warps 0.52 ms, 15 rings 0.52 ms)
     return dual ? launch_fwd2_cfg<float, true, 16, 4, 8>(p, s)
                 : launch_fwd2_cfg<float, false, 16, 4, 8>(p, s);
   }
