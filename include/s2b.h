@@ -116,6 +116,18 @@ int s2b_inverse_adjoint(s2b_plan* plan, const void* g_f, void* g_flm, void* work
 int s2b_forward_adjoint(s2b_plan* plan, const void* g_flm, void* g_f, void* workspace,
                         size_t workspace_bytes, void* stream);
 
+/* HEALPix ring FFTs alone (plan with sampling S2B_HEALPIX; spin is ignored):
+ *   f [B][12 nside^2] (complex, or real when desc.reality) <-> ftm [B][4 nside - 1][2L]
+ * complex, column c holding m = c - L: per ring FFT (no normalisation), fftshift and
+ * periodic extension to 2L columns; the inverse folds each row onto its ring length and
+ * inverse-FFTs without normalisation. No ring phase shifts. For real maps the rings of 2L
+ * pixels keep m >= 0 only, and the inverse returns real maps (Hermitian spectra).
+ * Replace s2fft/utils/healpix_ffts.py:187-423 (healpix_fft / healpix_ifft) and the XLA
+ * custom call lib/src/extensions.cc:26-100 (healpix_fft_cuda: healpix_forward /
+ * healpix_backward), which leaves reality aside. No workspace. */
+int s2b_healpix_fft(s2b_plan* plan, const void* f, void* ftm, void* stream);
+int s2b_healpix_ifft(s2b_plan* plan, const void* ftm, void* f, void* stream);
+
 /* Wigner transforms on SO(3) (plan with desc.N > 0; desc.spin is ignored):
  *   flmn [B][2N-1][L][2L-1] <-> f [B][2N-1][ntheta][nphi] (or [B][2N-1][12 nside^2]);
  *   f real when desc.reality (then flmn obeys the SO(3) conjugate symmetry).

@@ -54,6 +54,8 @@ _SIGS = {
     "s2b_plan_set_events": [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
     "s2b_fma_probe": [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
     "s2b_inverse_noalloc": [ctypes.c_void_p] * 4,
+    "s2b_healpix_fft": [ctypes.c_void_p] * 4,
+    "s2b_healpix_ifft": [ctypes.c_void_p] * 4,
     "s2b_plan_set_tuning": [ctypes.c_void_p, ctypes.c_int, ctypes.c_int],
     "s2b_inverse_adjoint": [ctypes.c_void_p] * 4 + [ctypes.c_size_t, ctypes.c_void_p],
     "s2b_forward_adjoint": [ctypes.c_void_p] * 4 + [ctypes.c_size_t, ctypes.c_void_p],

@@ -892,6 +892,55 @@ static int run_inverse(s2b_plan* p, const void* flm, void* f, char* ws, cudaStre
   return S2B_OK;
 }
 
+// HEALPix ring FFTs alone (s2fft/utils/healpix_ffts.py:187-423): per ring FFT, fftshift and
+// periodic extension to 2L columns (column c holds m = c - L), and the inverse with spectral
+// folding; no ring phases, no normalisation in either direction.
+template <typename Real>
+static int run_healpix_fft(s2b_plan* p, const void* f, void* ftm, cudaStream_t s) {
+  const s2b_desc& d = p->d;
+  RowsParams<Real> rp{};
+  rp.L = d.L;
+  rp.nrows = p->nth;
+  rp.real_in = d.reality;
+  rp.reality = d.reality;
+  rp.mode = FWD_TO_RAW;
+  rp.M = 2 * d.L;
+  rp.m0 = -d.L;
+  rp.scale = 1.0;
+  rp.desc = p->descs;
+  rp.ring_desc = p->ring_desc;
+  rp.ring_off = p->ring_off;
+  rp.out_batch_stride = p->npix;
+  rp.tb = tables<Real>(p);
+  rp.in = f;
+  rp.out = ftm;
+  S2B_CK(launch_fwd_rows<Real>(rp, p->nth, d.batch, p->maxM, s));
+  return S2B_OK;
+}
+
+template <typename Real>
+static int run_healpix_ifft(s2b_plan* p, const void* ftm, void* f, cudaStream_t s) {
+  const s2b_desc& d = p->d;
+  RowsParams<Real> rp{};
+  rp.L = d.L;
+  rp.nrows = p->nth;
+  rp.ncol = 2 * d.L;
+  rp.mo = 1;
+  rp.reality = d.reality;
+  rp.rings_real_2L = 1;
+  rp.real_out = d.reality;
+  rp.scale = 1.0;
+  rp.desc = p->descs;
+  rp.ring_desc = p->ring_desc;
+  rp.ring_off = p->ring_off;
+  rp.out_batch_stride = p->npix;
+  rp.tb = tables<Real>(p);
+  rp.in = ftm;
+  rp.out = f;
+  S2B_CK(launch_inv_rows<Real>(rp, p->nth, d.batch, p->maxM, s));
+  return S2B_OK;
+}
+
 // Adjoint (conjugate transpose) of the inverse: unweighted ring DFTs of g_f, the forward
 // projection over the inverse rings, and the pole rings in closed form.
 template <typename Real>
@@ -1567,6 +1616,24 @@ int s2b_forward_adjoint(s2b_plan* p, const void* g_flm, void* g_f, void* ws, siz
     return rc;
   if (ws_bytes < ws_of(p, 3)) return fail(S2B_ERR_WORKSPACE, "workspace too small");
   return exec_call(p, 3, g_flm, g_f, (char*)ws, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int s2b_healpix_fft(s2b_plan* p, const void* f, void* ftm, void* stream) {
+  if (!p || p->d.N > 0 || p->d.sampling != S2B_HEALPIX)
+    return fail(S2B_ERR_INVALID, "plan must be a HEALPix spin plan");
+  int rc;
+  if ((rc = check_ptr(f, "f")) || (rc = check_ptr(ftm, "ftm"))) return rc;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  return p->fp64 ? run_healpix_fft<double>(p, f, ftm, s) : run_healpix_fft<float>(p, f, ftm, s);
+}
+
+int s2b_healpix_ifft(s2b_plan* p, const void* ftm, void* f, void* stream) {
+  if (!p || p->d.N > 0 || p->d.sampling != S2B_HEALPIX)
+    return fail(S2B_ERR_INVALID, "plan must be a HEALPix spin plan");
+  int rc;
+  if ((rc = check_ptr(f, "f")) || (rc = check_ptr(ftm, "ftm"))) return rc;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  return p->fp64 ? run_healpix_ifft<double>(p, ftm, f, s) : run_healpix_ifft<float>(p, ftm, f, s);
 }
 
 int s2b_kernel_size(const s2b_plan* p, int forward, size_t* bytes) {

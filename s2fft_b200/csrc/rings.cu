@@ -278,10 +278,13 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) inv_rows_kerne
   const R2* row = reinterpret_cast<const R2*>(p.in) + ((size_t)b * p.nrows + t) * p.ncol;
   const int L = p.L;
   const double phi0 = p.phi0 ? p.phi0[t] : 0.0;
+  // the Hermitian mirror applies on every ring, or (rings_real_2L) only on rings of 2L
+  // pixels, where the rows hold the rfft half spectrum; other rings then use the full row
+  const bool mirror = p.reality && (!p.rings_real_2L || n == 2 * p.L);
   // coefficient C_m with the HEALPix phase exp(+i m phi0) and reality mirror
   auto coef = [&](int m) -> R2 {
     R2 c;
-    if (p.reality && m < 0) {
+    if (mirror && m < 0) {
       c = cconj(row[L - 1 - m + p.mo]);
       if (p.phi0) {
         double sn, cs;
@@ -304,7 +307,7 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) inv_rows_kerne
     }
     return c;
   };
-  const int mlo = p.reality ? -(L - 1) : -(L - 1) - p.mo;  // lowest m present
+  const int mlo = mirror ? -(L - 1) : -(L - 1) - p.mo;  // lowest m present
   const int mhi = L - 1;
   auto load = [&](int k) -> R2 {
     // X_k = sum of C_m over m == k (mod n), m in [mlo, mhi]
@@ -414,6 +417,9 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) fwd_rows_kerne
     for (int mi = threadIdx.x; mi < p.M; mi += blockDim.x) {
       const int m = p.m0 + mi;
       R2 x = dft_get<Real>(s, d, p.tb, false, pmod(m, n));
+      // real input on a ring of 2L pixels keeps m >= 0 only (the rfft half spectrum,
+      // s2fft/utils/healpix_ffts.py:212-216)
+      if (p.real_in && p.reality && n == 2 * L && m < 0) x = czero<R2>();
       out[((size_t)b * p.nrows + t) * p.M + mi] = cscale(x, (Real)p.scale);
     }
     return;

@@ -36,6 +36,7 @@ struct RowsParams {
   int ncol;             // inverse: columns of ftm
   int mo;               // column offset (1 for mwss / healpix)
   int reality;          // inverse: fill m < 0 by conjugate symmetry
+  int rings_real_2L;    // inverse, reality: mirror only on rings of 2L pixels (healpix_ifft)
   int real_out;         // inverse: write the real part only
   int real_in;          // forward: real input map
   int dual, nhalf;      // forward spectra layout

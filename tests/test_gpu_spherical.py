@@ -221,3 +221,27 @@ def test_f32_high_spin(s2b, rng, sampling, spin):
     assert relerr(f, ref) < TOL32, relerr(f, ref)
     g = s2b.forward(ref, L, spin, None, sampling, precision="f32")
     assert relerr(g, flm) < TOL32, relerr(g, flm)
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+@pytest.mark.parametrize("L,nside", [(16, 8), (24, 8), (32, 16)])
+def test_healpix_ring_ffts(s2b, rng, precision, L, nside):
+    """healpix_fft / healpix_ifft against the oracle's restatement of upstream's numpy
+    versions (complex and real maps)."""
+    tol = TOL64 if precision == "f64" else TOL32
+    npix = 12 * nside * nside
+    f = rng.normal(size=npix) + 1j * rng.normal(size=npix)
+    ftm = s2b.healpix_ffts.healpix_fft(f, L, nside, precision=precision)
+    ref = oracle.healpix.healpix_fft(f, L, nside)
+    assert relerr(ftm, ref) < tol
+    back = s2b.healpix_ffts.healpix_ifft(ref, L, nside, precision=precision)
+    assert relerr(back, oracle.healpix.healpix_ifft(ref, L, nside)) < tol
+    fr = rng.normal(size=npix)
+    ftr = s2b.healpix_ffts.healpix_fft(fr, L, nside, reality=True, precision=precision)
+    refr = oracle.healpix.healpix_fft(fr, L, nside, reality=True)
+    assert relerr(ftr, refr) < tol
+    # real inverse of Hermitian spectra (those of a real map)
+    spec = oracle.healpix.healpix_fft(fr, L, nside)
+    rr = s2b.healpix_ffts.healpix_ifft(spec, L, nside, reality=True, precision=precision)
+    assert rr.dtype in (np.float64, np.float32)
+    assert relerr(rr, np.real(oracle.healpix.healpix_ifft(spec, L, nside, reality=True))) < tol
