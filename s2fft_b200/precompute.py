@@ -80,7 +80,12 @@ def _kernel_tensor(kernel, L, s, nside, reality, forward, precision, spin, dev):
     want = cdt if s == "healpix" else rdt
     if isinstance(kernel, np.ndarray):
         kernel = torch.from_numpy(np.ascontiguousarray(kernel))
-    return kernel.to(device=dev, dtype=want).contiguous()
+    return _aligned(kernel.to(device=dev, dtype=want).contiguous())
+
+
+def _aligned(t):
+    # the C ABI takes 16-byte aligned operands (a slice of a stacked kernel may not be)
+    return t if t.data_ptr() % 16 == 0 else t.clone()
 
 
 def inverse(flm, L: int, spin: int = 0, kernel=None, sampling: str = "mw",
@@ -140,3 +145,115 @@ def forward(f, L: int, spin: int = 0, kernel=None, sampling: str = "mw",
             fr = inverse(flm, L, spin, Ki, s, reality, method, nside, precision)
             flm = flm + _forward_once(x - fr, K, L, spin, s, nside, reality, precision)
     return _ret(flm, was_np, odev)
+
+
+# ---------------------------------------------------------------------------------------
+# Precompute-kernel Wigner (SO(3)) transforms
+# (s2fft/precompute_transforms/wigner.py:13-467, construct.py:332-470)
+# ---------------------------------------------------------------------------------------
+def _wigner_ns(N, reality):
+    return range(0 if reality else -(N - 1), N)
+
+
+def _wigner_l_factor(L, N, n, forward, dev, dtype):
+    l = np.arange(L, dtype=np.float64)
+    if forward:
+        v = (-1.0) ** n * (2 * np.pi / (2 * N - 1)) / np.sqrt((2 * l + 1) / (4 * np.pi))
+    else:
+        v = (-1.0) ** n * np.sqrt((2 * l + 1) / (16 * np.pi ** 3))
+    return torch.from_numpy(v).to(device=dev, dtype=dtype)[None, :, None]
+
+
+def wigner_kernel(L: int, N: int, reality: bool = False, sampling: str = "mw",
+                  nside: int = None, forward: bool = False, mode: str = "auto",
+                  precision: str = "f64"):
+    """Wigner-d kernel K[n, t, l, m] in the upstream layout (construct.py:332-470):
+    d^l_{m,n}(theta_t) (2l+1)/(8 pi^2) for the inverse, d^l_{m,n}(theta_t) w_t 2pi/(2N-1)
+    for the forward (MWSS(2L) rings for mw / mwss), HEALPix ring phases folded in;
+    n >= 0 only when ``reality``. Built on the device from the spin kernels of spin -n
+    (``mode`` is accepted for signature compatibility: the recursion is always the
+    on-device one)."""
+    s = sampling.lower()
+    if precision == "bf16x3":
+        raise ValueError("Wigner kernels are built in f64 or f32")
+    dev = _device()
+    slabs = []
+    for n in _wigner_ns(N, reality):
+        K = spin_spherical_kernel(L, -n, False, s, nside, forward, precision=precision)
+        slabs.append(K * _wigner_l_factor(L, N, n, forward, dev, K.real.dtype))
+    return torch.stack(slabs)
+
+
+def _wigner_kernel_tensor(kernel, L, N, s, nside, reality, forward, precision, dev):
+    if kernel is None:
+        return wigner_kernel(L, N, reality, s, nside, forward, precision=precision)
+    cdt, rdt = _dtypes(precision)
+    want = cdt if s == "healpix" else rdt
+    if isinstance(kernel, np.ndarray):
+        kernel = torch.from_numpy(np.ascontiguousarray(kernel))
+    return kernel.to(device=dev, dtype=want).contiguous()
+
+
+def wigner_inverse(flmn, L: int, N: int, kernel=None, sampling: str = "mw",
+                   reality: bool = False, method: str = "cuda", nside: int = None,
+                   precision: str = "f64"):
+    """Inverse Wigner transform through a precomputed kernel
+    (upstream precompute_transforms/wigner.py:13-221): per n the contraction with the
+    kernel slice and the phi FFT (the spin precompute inverse of spin -n), then the
+    unnormalised inverse DFT over gamma."""
+    _check_method(method)
+    s = sampling.lower()
+    cdt, rdt = _dtypes(precision)
+    x, was_np, odev = _to_device(flmn, cdt, _device())
+    K = _wigner_kernel_tensor(kernel, L, N, s, nside, reality, False, precision, x.device)
+    G = 2 * N - 1
+    fs = []
+    for j, n in enumerate(_wigner_ns(N, reality)):
+        fs.append(inverse(x[..., N - 1 + n, :, :], L, -n, K[j], s, False, method, nside,
+                          precision))
+    gdim = len(f_shape(L, s, nside))
+    fban = torch.stack(fs, dim=-gdim - 1)
+    ns = np.array(list(_wigner_ns(N, reality)))
+    k = np.arange(G)
+    P = np.exp(2j * np.pi * np.outer(ns, k) / G)  # [n, k]
+    if reality:
+        P[ns > 0] *= 2.0
+    Pt = torch.from_numpy(P).to(device=x.device, dtype=cdt)
+    f = torch.movedim(torch.tensordot(fban, Pt, dims=([-gdim - 1], [0])), -1, -gdim - 1)
+    if reality:
+        f = f.real.contiguous()
+    return _ret(f, was_np, odev)
+
+
+def wigner_forward(f, L: int, N: int, kernel=None, sampling: str = "mw",
+                   reality: bool = False, method: str = "cuda", nside: int = None,
+                   precision: str = "f64"):
+    """Forward Wigner transform through a precomputed kernel
+    (upstream precompute_transforms/wigner.py:224-371): unnormalised DFT over gamma, then
+    per n the spin precompute forward of spin -n (MW / MWSS resampling, phi FFT and the
+    contraction with the kernel slice); n < 0 from the conjugate symmetry when ``reality``."""
+    _check_method(method)
+    s = sampling.lower()
+    cdt, rdt = _dtypes(precision)
+    x, was_np, odev = _to_device(f, cdt, _device())
+    K = _wigner_kernel_tensor(kernel, L, N, s, nside, reality, True, precision, x.device)
+    G = 2 * N - 1
+    gdim = len(f_shape(L, s, nside))
+    ns = np.array(list(_wigner_ns(N, reality)))
+    P = np.exp(-2j * np.pi * np.outer(np.arange(G), ns) / G)  # [k, n]
+    Pt = torch.from_numpy(P).to(device=x.device, dtype=cdt)
+    fin = x.real.to(cdt) if reality else x
+    fban = torch.movedim(torch.tensordot(fin, Pt, dims=([-gdim - 1], [0])), -1, -gdim - 1)
+    bs = tuple(x.shape[:-gdim - 1])
+    out = torch.zeros(bs + (G, L, 2 * L - 1), dtype=cdt, device=x.device)
+    for j, n in enumerate(ns):
+        fb = fban.select(-gdim - 1, j).contiguous()
+        out[..., N - 1 + n, :, :] = forward(fb, L, int(-n), K[j], s, False, method, nside,
+                                            0, precision)
+    if reality:
+        m = torch.arange(-(L - 1), L, device=x.device)
+        sm = ((-1.0) ** m.abs()).to(cdt)
+        for n in range(1, N):
+            out[..., N - 1 - n, :, :] = (-1.0) ** n * torch.flip(
+                out[..., N - 1 + n, :, :].conj(), dims=(-1,)) * sm
+    return _ret(out, was_np, odev)

@@ -77,17 +77,22 @@ def _device():
     return torch.device("cuda", torch.cuda.current_device())
 
 
+def _aligned(t):
+    # the C ABI takes 16-byte aligned operands; a view into a larger tensor may not be
+    return t if t.data_ptr() % 16 == 0 else t.clone()
+
+
 def _to_device(x, dtype, device):
-    """(tensor on device, was_numpy, original device)."""
+    """(contiguous, 16-byte aligned tensor on device, was_numpy, original device)."""
     if isinstance(x, np.ndarray):
         t = torch.from_numpy(np.ascontiguousarray(x))
-        return t.to(device=device, dtype=dtype).contiguous(), True, None
+        return _aligned(t.to(device=device, dtype=dtype).contiguous()), True, None
     if isinstance(x, torch.Tensor):
         dev = x.device
         t = x.to(device=device if dev.type != "cuda" else dev, dtype=dtype).contiguous()
-        return t, False, dev
+        return _aligned(t), False, dev
     t = torch.as_tensor(np.asarray(x))
-    return t.to(device=device, dtype=dtype).contiguous(), True, None
+    return _aligned(t.to(device=device, dtype=dtype).contiguous()), True, None
 
 
 def _ret(t, was_numpy, dev):

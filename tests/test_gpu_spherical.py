@@ -245,3 +245,25 @@ def test_healpix_ring_ffts(s2b, rng, precision, L, nside):
     rr = s2b.healpix_ffts.healpix_ifft(spec, L, nside, reality=True, precision=precision)
     assert rr.dtype in (np.float64, np.float32)
     assert relerr(rr, np.real(oracle.healpix.healpix_ifft(spec, L, nside, reality=True))) < tol
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_precompute_wigner_golden(s2b, golden, rng, precision):
+    """Precompute-kernel Wigner transforms against upstream's golden SO(3) vectors, and the
+    kernel-based HEALPix transform against the on-the-fly one."""
+    data, index = golden
+    tol = TOL64 if precision == "f64" else TOL32
+    for c in [c for c in index["cases"] if c["kind"] == "wigner"]:
+        n, L, N, smp, real = c["name"], c["L"], c["N"], c["sampling"], c["reality"]
+        f = s2b.precompute.wigner_inverse(data[f"{n}/flmn"], L, N, None, smp, real,
+                                          precision=precision)
+        ref = np.real(data[f"{n}/f"]) if real else data[f"{n}/f"]
+        assert relerr(f, ref) < tol, (n, relerr(f, ref))
+        g = s2b.precompute.wigner_forward(ref, L, N, None, smp, real, precision=precision)
+        assert relerr(g, data[f"{n}/flmn_fwd"]) < tol, (n, relerr(g, data[f"{n}/flmn_fwd"]))
+    L, N, nside = 16, 3, 8
+    flmn = oracle.signal.generate_flmn(rng, L, N)
+    K = s2b.precompute.wigner_kernel(L, N, False, "healpix", nside, False, precision=precision)
+    f = s2b.precompute.wigner_inverse(flmn, L, N, K, "healpix", nside=nside, precision=precision)
+    ref = s2b.wigner.inverse(flmn, L, N, nside, "healpix", precision=precision)
+    assert relerr(f, ref) < tol
