@@ -358,7 +358,7 @@ __global__ void __launch_bounds__(W * 32, sizeof(Real) == 4 ? 4 : 3)
       const int ln = it % kFwdBlock;
       const int m = mgrp - S;
       const int l = (k ? kb1 : kb0) * kFwdBlock + ln;
-      if (m < 0 || m > (k ? mc1 : mc0) || l >= L || l < m) continue;
+      if (m < p.mlo || m > (k ? mc1 : mc0) || l >= L || l < m) continue;
       Acc s = buf[((S * W + 0) * 2 + k) * kFwdBlock + ln];
 #pragma unroll
       for (int x = 1; x < W; ++x) acc_add(s, buf[((S * W + x) * 2 + k) * kFwdBlock + ln]);

@@ -244,7 +244,7 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
       const int rr = it % NRT;
       const int m = mgrp - S;
       const int r = r0 + rr;
-      if (m < 0 || m > lmax || r >= p.nrings) continue;
+      if (m < p.mlo || m > lmax || r >= p.nrings) continue;
       Acc s = buf[(S * W + 0) * NRT + rr];
 #pragma unroll
       for (int x = 1; x < W; ++x) acc_add(s, buf[(S * W + x) * NRT + rr]);

@@ -29,6 +29,7 @@
 #include "s2b_precompute.h"
 #include "s2b_tc.h"
 #include "s2b_latfwd.h"
+#include "s2b_lowm.h"
 
 using namespace s2b;
 using cd = std::complex<double>;
@@ -375,13 +376,14 @@ struct s2b_plan {
   double* kth_fwd = nullptr;
   int knth_inv = 0, knth_fwd = 0, kM = 0;
   size_t ws_pre_fwd = 0;
-  // float plans with |spin| >= 4: the on-the-fly transforms run on this float64 plan (the
-  // float m-recursion through the evanescent zone |m| < |s| near the poles is not accurate
-  // enough); inputs and outputs are converted at the boundary
-  s2b_plan* shadow = nullptr;
   // Wigner: one spin transform plan per n, gamma-DFT buffers
   std::vector<s2b_plan*> subs;
   size_t ws_w_fban = 0, ws_w_tmp = 0, ws_w_sub = 0;
+  // Wigner: the spin transforms of different n run concurrently on internal streams, forked
+  // from and joined back to the caller's stream with events; one workspace slice per stream
+  int nwstream = 0;
+  cudaStream_t wstream[4] = {};
+  cudaEvent_t wfork = nullptr, wjoin[4] = {};
   // optional events recorded around the latitudinal launch ([0] inverse, [1] forward)
   int tile_fwd = 0, tile_inv = 0;  // latitudinal tile variants (s2b_plan_set_tuning)
   cudaEvent_t ev_begin[2] = {nullptr, nullptr};
@@ -812,6 +814,54 @@ static int check_ptr(const void* ptr, const char* what) {
   return S2B_OK;
 }
 
+// Orders m < |spin| are left out of the latitudinal kernels and added by the degree
+// recursion (lowm.cu): the m-recursion is unstable below m = n cos(theta) on rings where
+// n cos(theta) > 0, a range that lies inside m < |spin|.
+static int lowm_orders(const s2b_plan* p) { return p->d.spin < 0 ? -p->d.spin : p->d.spin; }
+
+static int run_lowm_synth(const s2b_plan* p, const Inv2Params& lp, const RingInfo* rings,
+                          cudaStream_t s) {
+  if (lp.mlo <= 0 || lp.nrings <= 0) return S2B_OK;
+  LowmParams q{};
+  q.L = lp.L;
+  q.spin = p->d.spin;
+  q.nhalf = lp.nhalf;
+  q.batch = lp.batch;
+  q.nrings = lp.nrings;
+  q.NB = lp.NB;
+  q.mlo = lp.mlo;
+  q.rings = rings;
+  q.g = p->gtab;
+  q.F = lp.F;
+  q.ftm = lp.ftm;
+  q.ring_row = lp.ring_row;
+  q.nrows = lp.nrows;
+  q.ncol = lp.ncol;
+  q.mo = lp.mo;
+  S2B_CK(launch_lowm_synth(p->fp64, q, s));
+  return S2B_OK;
+}
+
+static int run_lowm_project(const s2b_plan* p, const Fwd2Params& lp, const RingInfo* rings,
+                            cudaStream_t s) {
+  if (lp.mlo <= 0 || lp.nrings <= 0) return S2B_OK;
+  LowmParams q{};
+  q.L = lp.L;
+  q.spin = p->d.spin;
+  q.nhalf = lp.nhalf;
+  q.batch = lp.batch;
+  q.nrings = lp.nrings;
+  q.NB = lp.NB;
+  q.mlo = lp.mlo;
+  q.rings = rings;
+  q.g = p->gtab;
+  q.G = lp.G;
+  q.Gs = lp.Gs;
+  q.acc = lp.acc;
+  S2B_CK(launch_lowm_project(p->fp64, q, s));
+  return S2B_OK;
+}
+
 template <typename Real>
 static int run_inverse(s2b_plan* p, const void* flm, void* f, char* ws, cudaStream_t s,
                        const double* ring_w = nullptr) {
@@ -866,9 +916,11 @@ static int run_inverse(s2b_plan* p, const void* flm, void* f, char* ws, cudaStre
     lp.mo = p->inv_mo;
     lp.status = p->status;
     lp.tile = p->tile_inv;
+    lp.mlo = lowm_orders(p);
     if (p->ev_begin[0]) S2B_CK(cudaEventRecord(p->ev_begin[0], s));
     S2B_CK(launch_inv2(p->fp64, p->dual, lp, s));
     if (p->ev_end[0]) S2B_CK(cudaEventRecord(p->ev_end[0], s));
+    if (int rc_ = run_lowm_synth(p, lp, p->inv_rings, s)) return rc_;
   }
   RowsParams<Real> rp{};
   rp.L = L;
@@ -989,7 +1041,9 @@ static int run_inverse_adjoint(s2b_plan* p, const void* gf, void* gflm, char* ws
     lp.Gs = p->adj_Gs;
     lp.acc = acc;
     lp.status = p->status;
+    lp.mlo = lowm_orders(p);
     S2B_CK(launch_fwd2(p->fp64, p->dual, lp, s));
+    if (int rc_ = run_lowm_project(p, lp, p->inv_rings, s)) return rc_;
   }
   StageParams sp{};
   sp.L = L;
@@ -1067,7 +1121,9 @@ static int run_forward_adjoint(s2b_plan* p, const void* gflm, void* gf, char* ws
   lp.ncol = 2 * L - 1;
   lp.mo = 0;
   lp.status = p->status;
+  lp.mlo = lowm_orders(p);
   S2B_CK(launch_inv2(p->fp64, p->dual, lp, s));
+  if (int rc_ = run_lowm_synth(p, lp, p->fwd_rings, s)) return rc_;
   ColsParams<Real> cp{};
   cp.L = L;
   cp.spin = d.spin;
@@ -1176,9 +1232,11 @@ static int run_forward_once(s2b_plan* p, const void* f, void* flm, char* ws, cud
   lp.acc = acc;
   lp.status = p->status;
   lp.tile = p->tile_fwd;
+  lp.mlo = lowm_orders(p);
   if (p->ev_begin[1]) S2B_CK(cudaEventRecord(p->ev_begin[1], s));
   S2B_CK(launch_fwd2(p->fp64, p->dual, lp, s));
   if (p->ev_end[1]) S2B_CK(cudaEventRecord(p->ev_end[1], s));
+  if (int rc_ = run_lowm_project(p, lp, p->fwd_rings, s)) return rc_;
   StageParams sp{};
   sp.L = L;
   sp.L0 = d.L_lower;
@@ -1396,14 +1454,8 @@ static int run_pre_forward(s2b_plan* p, const void* K, const void* f, void* flm,
 // (s2fft/transforms/wigner.py:110-196, 442-533)
 // ----------------------------------------------------------------------------
 // Workspace of a call of the given kind (0 inverse, 1 forward, 2 inverse adjoint,
-// 3 forward adjoint) on a spin plan, including the float64 shadow's conversion buffers.
+// 3 forward adjoint) on a spin plan.
 static size_t ws_of(const s2b_plan* p, int kind) {
-  if (p->shadow) {
-    const s2b_desc& d = p->d;
-    const size_t nflm = (size_t)d.batch * d.L * (2 * d.L - 1) * 2;
-    const size_t nf = (size_t)d.batch * p->npix * (d.reality ? 1 : 2);
-    return align256(nflm * 8) + align256(nf * 8) + ws_of(p->shadow, kind);
-  }
   switch (kind) {
     case 0: return inv_ws(p);
     case 1: return std::max(fwd_ws(p), pre_fwd_ws(p));
@@ -1412,24 +1464,8 @@ static size_t ws_of(const s2b_plan* p, int kind) {
   }
 }
 
-// One spin-transform call of the given kind on the plan's own precision, or, for plans with a
-// float64 shadow, on the shadow with float <-> double conversion of input and output.
+// One spin-transform call of the given kind in the plan's precision.
 static int exec_call(s2b_plan* p, int kind, const void* in, void* out, char* ws, cudaStream_t s) {
-  if (p->shadow) {
-    const s2b_desc& d = p->d;
-    const size_t nflm = (size_t)d.batch * d.L * (2 * d.L - 1) * 2;
-    const size_t nf = (size_t)d.batch * p->npix * (d.reality ? 1 : 2);
-    const bool in_flm = kind == 0 || kind == 3;
-    const size_t nin = in_flm ? nflm : nf, nout = in_flm ? nf : nflm;
-    char* a = ws;                          // converted input
-    char* b = a + align256(nin * 8);       // float64 output
-    char* w2 = a + align256(nflm * 8) + align256(nf * 8);  // the shadow's workspace
-    S2B_CK(launch_cast(true, in, a, (long)nin, s));
-    const int rc = exec_call(p->shadow, kind, a, b, w2, s);
-    if (rc) return rc;
-    S2B_CK(launch_cast(false, b, out, (long)nout, s));
-    return S2B_OK;
-  }
   switch (kind) {
     case 0:
       return p->fp64 ? run_inverse<double>(p, in, out, ws, s) : run_inverse<float>(p, in, out, ws, s);
@@ -1467,42 +1503,64 @@ static int build_wigner(s2b_plan* p) {
   const size_t c2 = 2 * p->rsz;
   p->ws_w_fban = (size_t)(2 * d.N - 1) * d.batch * p->npix * c2;
   p->ws_w_tmp = (size_t)d.batch * d.L * (2 * d.L - 1) * c2;
+  p->nwstream = std::min<int>(4, (int)p->subs.size());
+  if (p->nwstream > 1) {
+    S2B_CK(cudaEventCreateWithFlags(&p->wfork, cudaEventDisableTiming));
+    for (int k = 0; k < p->nwstream; ++k) {
+      S2B_CK(cudaStreamCreateWithFlags(&p->wstream[k], cudaStreamNonBlocking));
+      S2B_CK(cudaEventCreateWithFlags(&p->wjoin[k], cudaEventDisableTiming));
+    }
+  }
   return S2B_OK;
 }
 
+// fban | per stream: (tmp | sub-transform workspace)
+static size_t wigner_slot(const s2b_plan* p) { return align256(p->ws_w_tmp) + align256(p->ws_w_sub); }
 static size_t wigner_ws(const s2b_plan* p) {
-  return align256(p->ws_w_fban) + align256(p->ws_w_tmp) + align256(p->ws_w_sub);
+  return align256(p->ws_w_fban) + (size_t)std::max(1, p->nwstream) * wigner_slot(p);
 }
 
 static int run_wigner(s2b_plan* p, bool forward, const void* in, void* out, char* ws,
                       cudaStream_t s) {
   const s2b_desc& d = p->d;
   const int n0 = d.reality ? 0 : -(d.N - 1);
+  const int K = p->nwstream > 1 ? p->nwstream : 1;
   char* fban = ws;
-  char* tmp = fban + align256(p->ws_w_fban);
-  char* subws = tmp + align256(p->ws_w_tmp);
   const size_t slice = (size_t)d.batch * p->npix * 2 * p->rsz;
   int rc;
-  if (!forward) {
-    for (int n = n0; n < d.N; ++n) {
-      s2b_plan* sub = p->subs[n - n0];
-      S2B_CK(launch_gather_n(p->fp64, in, tmp, d.batch, d.N, d.L, n, s));
-      char* dst = fban + (size_t)(d.N - 1 + n) * slice;
-      rc = exec_call(sub, 0, tmp, dst, subws, s);
-      if (rc) return rc;
-    }
-    S2B_CK(launch_gamma_inverse(p->fp64, fban, out, d.batch, d.N, p->npix, d.reality, s));
-    return S2B_OK;
+  if (forward) S2B_CK(launch_gamma_forward(p->fp64, in, fban, d.batch, d.N, p->npix, d.reality, s));
+  if (K > 1) {
+    S2B_CK(cudaEventRecord(p->wfork, s));
+    for (int k = 0; k < K; ++k) S2B_CK(cudaStreamWaitEvent(p->wstream[k], p->wfork, 0));
   }
-  S2B_CK(launch_gamma_forward(p->fp64, in, fban, d.batch, d.N, p->npix, d.reality, s));
   for (int n = n0; n < d.N; ++n) {
+    const int k = (n - n0) % K;
+    cudaStream_t sk = K > 1 ? p->wstream[k] : s;
+    char* tmp = fban + align256(p->ws_w_fban) + (size_t)k * wigner_slot(p);
+    char* subws = tmp + align256(p->ws_w_tmp);
     s2b_plan* sub = p->subs[n - n0];
-    const char* src = fban + (size_t)(d.N - 1 + n) * slice;
-    rc = exec_call(sub, 1, src, tmp, subws, s);
-    if (rc) return rc;
-    S2B_CK(launch_scatter_n(p->fp64, tmp, out, d.batch, d.N, d.L, n, d.L_lower, s));
+    char* band = fban + (size_t)(d.N - 1 + n) * slice;
+    if (!forward) {
+      S2B_CK(launch_gather_n(p->fp64, in, tmp, d.batch, d.N, d.L, n, sk));
+      rc = exec_call(sub, 0, tmp, band, subws, sk);
+      if (rc) return rc;
+    } else {
+      rc = exec_call(sub, 1, band, tmp, subws, sk);
+      if (rc) return rc;
+      S2B_CK(launch_scatter_n(p->fp64, tmp, out, d.batch, d.N, d.L, n, d.L_lower, sk));
+    }
   }
-  if (d.reality) S2B_CK(launch_wigner_mirror(p->fp64, out, d.batch, d.N, d.L, s));
+  if (K > 1) {
+    for (int k = 0; k < K; ++k) {
+      S2B_CK(cudaEventRecord(p->wjoin[k], p->wstream[k]));
+      S2B_CK(cudaStreamWaitEvent(s, p->wjoin[k], 0));
+    }
+  }
+  if (!forward) {
+    S2B_CK(launch_gamma_inverse(p->fp64, fban, out, d.batch, d.N, p->npix, d.reality, s));
+  } else if (d.reality) {
+    S2B_CK(launch_wigner_mirror(p->fp64, out, d.batch, d.N, d.L, s));
+  }
   return S2B_OK;
 }
 
@@ -1541,16 +1599,8 @@ int s2b_plan_create(const s2b_desc* desc, s2b_plan** out) {
   s2b_plan* p = new s2b_plan();
   p->d = d;
   int rc = d.N > 0 ? build_wigner(p) : build_plan(p);
-  if (!rc && d.N == 0 && d.precision != S2B_F64 && std::abs(d.spin) >= 4) {
-    s2b_desc d64 = d;
-    d64.precision = S2B_F64;
-    rc = s2b_plan_create(&d64, &p->shadow);
-  }
   if (rc) {
-    if (p->shadow) s2b_plan_destroy(p->shadow);
-    for (s2b_plan* sp : p->subs) s2b_plan_destroy(sp);
-    for (void* a : p->allocs) cudaFree(a);
-    delete p;
+    s2b_plan_destroy(p);
     return rc;
   }
   *out = p;
@@ -1559,9 +1609,13 @@ int s2b_plan_create(const s2b_desc* desc, s2b_plan** out) {
 
 int s2b_plan_destroy(s2b_plan* p) {
   if (!p) return S2B_OK;
-  if (p->shadow) s2b_plan_destroy(p->shadow);
   for (s2b_plan* sp : p->subs) s2b_plan_destroy(sp);
   for (void* a : p->allocs) cudaFree(a);
+  for (int k = 0; k < 4; ++k) {
+    if (p->wstream[k]) cudaStreamDestroy(p->wstream[k]);
+    if (p->wjoin[k]) cudaEventDestroy(p->wjoin[k]);
+  }
+  if (p->wfork) cudaEventDestroy(p->wfork);
   delete p;
   return S2B_OK;
 }
@@ -1700,7 +1754,6 @@ static int plan_status_word(const s2b_plan* p, int* out) {
   if (p->status) S2B_CK(cudaMemcpy(&st, p->status, sizeof(int), cudaMemcpyDeviceToHost));
   *out |= st;
   int rc;
-  if (p->shadow && (rc = plan_status_word(p->shadow, out))) return rc;
   for (const s2b_plan* sp : p->subs)
     if ((rc = plan_status_word(sp, out))) return rc;
   return S2B_OK;
@@ -1722,7 +1775,6 @@ int s2b_plan_set_tuning(s2b_plan* p, int key, int value) {
     p->tile_fwd = value;
   else
     p->tile_inv = value;
-  if (p->shadow) s2b_plan_set_tuning(p->shadow, key, value);
   for (s2b_plan* sp : p->subs) s2b_plan_set_tuning(sp, key, value);
   return S2B_OK;
 }

@@ -39,6 +39,7 @@ struct Fwd2Params {
   void* acc;                // [batch][nhalf][L (m)][NB*32 (l)] projected sums (Real4 when dual)
   int* status;
   int tile;                 // 0: default rings per warp, 1: half of it (more CTAs)
+  int mlo;                  // orders m < mlo are left to the degree recursion (lowm.cu)
 };
 
 // Inverse latitudinal step, blocked layout (latinv.cu).
@@ -55,6 +56,7 @@ struct Inv2Params {
   int nrows, ncol, mo;
   int* status;
   int tile;                 // 0: default rings per lane, 1: one ring per lane (more CTAs)
+  int mlo;                  // orders m < mlo are left to the degree recursion (lowm.cu)
 };
 cudaError_t launch_inv2(bool fp64, bool dual, const Inv2Params& p, cudaStream_t s);
 

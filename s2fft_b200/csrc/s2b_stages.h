@@ -28,7 +28,5 @@ cudaError_t launch_poles(bool fp64, const StageParams& p, cudaStream_t s);
 cudaError_t launch_epilogue(bool fp64, const StageParams& p, cudaStream_t s);
 cudaError_t launch_axpy(bool fp64, long n, double a, const void* x, void* y, cudaStream_t s);
 cudaError_t launch_sub(bool fp64, long n, const void* x, const void* y, void* z, cudaStream_t s);
-// float <-> double element copy (n reals)
-cudaError_t launch_cast(bool to64, const void* in, void* out, long n, cudaStream_t s);
 
 }  // namespace s2b

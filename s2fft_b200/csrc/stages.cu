@@ -275,24 +275,6 @@ cudaError_t launch_epilogue(bool fp64, const StageParams& p, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-__global__ void cast_f2d_kernel(const float* __restrict__ in, double* __restrict__ out, long n) {
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-    out[i] = (double)in[i];
-}
-__global__ void cast_d2f_kernel(const double* __restrict__ in, float* __restrict__ out, long n) {
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-    out[i] = (float)in[i];
-}
-
-cudaError_t launch_cast(bool to64, const void* in, void* out, long n, cudaStream_t s) {
-  if (n <= 0) return cudaSuccess;
-  if (to64)
-    cast_f2d_kernel<<<grid_for(n), 256, 0, s>>>((const float*)in, (double*)out, n);
-  else
-    cast_d2f_kernel<<<grid_for(n), 256, 0, s>>>((const double*)in, (float*)out, n);
-  return cudaGetLastError();
-}
-
 cudaError_t launch_axpy(bool fp64, long n, double a, const void* x, void* y, cudaStream_t s) {
   if (fp64)
     axpy_kernel<double><<<grid_for(n), 256, 0, s>>>(n, a, (const double2*)x, (double2*)y);

@@ -83,12 +83,26 @@ __global__ void wigner_mirror_kernel(W2<Real>* flmn, int B, int N, int L) {
   }
 }
 
+// exp(sign 2 pi i ((j * k) mod G) / G) for j, k < G, one table per CTA in shared memory
+// (G = 2N - 1 <= 2L - 1; computed in double, kept in double)
+__device__ inline void gamma_phases(double2* tab, int G, double sign) {
+  for (int x = threadIdx.x; x < G * G; x += blockDim.x) {
+    const int j = x / G, k = x % G;
+    double sn, cs;
+    sincospi(sign * 2.0 * (double)((j * k) % G) / (double)G, &sn, &cs);
+    tab[x] = make_double2(cs, sn);
+  }
+  __syncthreads();
+}
+
 // Inverse gamma DFT: f[b][k][p] = sum_n fban[n][b][p] exp(+2 pi i n k / (2N-1)),
 // n in [-(N-1), N-1]; reality: real output from n >= 0 (irfft semantics).
 template <typename Real>
 __global__ void gamma_inverse_kernel(const W2<Real>* fban, void* f, int B, int N, long npix,
                                      int reality) {
+  extern __shared__ double2 tab[];  // [n mod G][k]
   const int G = 2 * N - 1;
+  gamma_phases(tab, G, 1.0);
   const long total = (long)B * npix;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
        i += (long)gridDim.x * blockDim.x) {
@@ -97,13 +111,12 @@ __global__ void gamma_inverse_kernel(const W2<Real>* fban, void* f, int B, int N
       double re = 0.0, im = 0.0;
       for (int n = reality ? 0 : -(N - 1); n < N; ++n) {
         const W2<Real> x = fban[((long)(N - 1 + n) * B + b) * npix + px];
-        double sn, cs;
-        sincospi(2.0 * (double)(((long)n * k) % G) / (double)G, &sn, &cs);
+        const double2 e = tab[((n + G) % G) * G + k];
         double xr = x.x, xi = x.y;
         if (reality && n == 0) xi = 0.0;
         const double w = (reality && n > 0) ? 2.0 : 1.0;
-        re += w * (xr * cs - xi * sn);
-        im += w * (xr * sn + xi * cs);
+        re += w * (xr * e.x - xi * e.y);
+        im += w * (xr * e.y + xi * e.x);
       }
       if (reality) {
         reinterpret_cast<Real*>(f)[(b * G + k) * npix + px] = (Real)re;
@@ -122,7 +135,9 @@ __global__ void gamma_inverse_kernel(const W2<Real>* fban, void* f, int B, int N
 template <typename Real>
 __global__ void gamma_forward_kernel(const void* f, W2<Real>* fban, int B, int N, long npix,
                                      int reality) {
+  extern __shared__ double2 tab[];
   const int G = 2 * N - 1;
+  gamma_phases(tab, G, -1.0);
   const long total = (long)B * npix;
   const double sc = 2.0 * 3.141592653589793 / (double)G;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
@@ -140,10 +155,9 @@ __global__ void gamma_forward_kernel(const void* f, W2<Real>* fban, int B, int N
           xr = x.x;
           xi = x.y;
         }
-        double sn, cs;
-        sincospi(-2.0 * (double)((((long)n * k) % G + G) % G) / (double)G, &sn, &cs);
-        re += xr * cs - xi * sn;
-        im += xr * sn + xi * cs;
+        const double2 e = tab[((n + G) % G) * G + k];
+        re += xr * e.x - xi * e.y;
+        im += xr * e.y + xi * e.x;
       }
       W2<Real> o;
       o.x = (Real)(sc * re);
@@ -185,19 +199,21 @@ cudaError_t launch_wigner_mirror(bool fp64, void* flmn, int B, int N, int L, cud
 
 cudaError_t launch_gamma_inverse(bool fp64, const void* fban, void* f, int B, int N, long npix,
                                  int reality, cudaStream_t s) {
+  const size_t sm = (size_t)(2 * N - 1) * (2 * N - 1) * sizeof(double2);
   if (fp64)
-    gamma_inverse_kernel<double><<<wgrid((long)B * npix), 256, 0, s>>>((const double2*)fban, f, B, N, npix, reality);
+    gamma_inverse_kernel<double><<<wgrid((long)B * npix), 256, sm, s>>>((const double2*)fban, f, B, N, npix, reality);
   else
-    gamma_inverse_kernel<float><<<wgrid((long)B * npix), 256, 0, s>>>((const float2*)fban, f, B, N, npix, reality);
+    gamma_inverse_kernel<float><<<wgrid((long)B * npix), 256, sm, s>>>((const float2*)fban, f, B, N, npix, reality);
   return cudaGetLastError();
 }
 
 cudaError_t launch_gamma_forward(bool fp64, const void* f, void* fban, int B, int N, long npix,
                                  int reality, cudaStream_t s) {
+  const size_t sm = (size_t)(2 * N - 1) * (2 * N - 1) * sizeof(double2);
   if (fp64)
-    gamma_forward_kernel<double><<<wgrid((long)B * npix), 256, 0, s>>>(f, (double2*)fban, B, N, npix, reality);
+    gamma_forward_kernel<double><<<wgrid((long)B * npix), 256, sm, s>>>(f, (double2*)fban, B, N, npix, reality);
   else
-    gamma_forward_kernel<float><<<wgrid((long)B * npix), 256, 0, s>>>(f, (float2*)fban, B, N, npix, reality);
+    gamma_forward_kernel<float><<<wgrid((long)B * npix), 256, sm, s>>>(f, (float2*)fban, B, N, npix, reality);
   return cudaGetLastError();
 }
 

@@ -65,6 +65,31 @@ def test_adjoint_dot_products(s2b, rng, sampling, spin, precision):
     assert abs(lhs - rhs) <= TOL[precision] * max(abs(lhs), 1e-30) * 10, (lhs, rhs)
 
 
+@pytest.mark.parametrize("sampling", ["mw", "dh"])
+@pytest.mark.parametrize("spin", [-7, 6])
+def test_adjoint_dot_products_high_spin(s2b, rng, sampling, spin):
+    """The adjoints at L=256 and |spin| > 4, where orders m < |spin| run on the degree
+    recursion (both directions and both halves)."""
+    import torch
+
+    L = 256
+    shape = s2b.f_shape(L, sampling)
+    x = torch.tensor(oracle.signal.generate_flm(rng, L, 0, spin), device="cuda",
+                     requires_grad=True)
+    y = torch.tensor(rng.normal(size=shape) + 1j * rng.normal(size=shape), device="cuda")
+    f = s2b.inverse(x, L, spin, None, sampling)
+    (gx,) = torch.autograd.grad(f, x, grad_outputs=y)
+    lhs, rhs = _vdot(f.detach(), y), _vdot(x.detach(), gx)
+    assert abs(lhs - rhs) <= 1e-10 * abs(lhs), (lhs, rhs)
+    fin = torch.tensor(rng.normal(size=shape) + 1j * rng.normal(size=shape), device="cuda",
+                       requires_grad=True)
+    h = torch.tensor(oracle.signal.generate_flm(rng, L, 0, spin), device="cuda")
+    flm = s2b.forward(fin, L, spin, None, sampling)
+    (gf,) = torch.autograd.grad(flm, fin, grad_outputs=h)
+    lhs, rhs = _vdot(flm.detach(), h), _vdot(fin.detach(), gf)
+    assert abs(lhs - rhs) <= 1e-10 * abs(lhs), (lhs, rhs)
+
+
 def _fd_check(loss_fn, x, grad, coords, tol):
     """Central differences on the real and imaginary part of each coordinate."""
     import torch

@@ -5,11 +5,14 @@ Tolerances: float64 path <= 1e-10 relative to max|ref| (upstream's own round tri
 error at these sizes is ~1e-13); mixed float32 path <= 1e-5.
 """
 
+import json
+import os
+
 import numpy as np
 import pytest
 
 import oracle
-from tests.conftest import relerr
+from tests.conftest import GOLDEN_DIR, relerr
 
 pytestmark = pytest.mark.gpu
 
@@ -211,8 +214,8 @@ def test_bf16x3_tensor_core_forward(s2b, rng, spin):
 @pytest.mark.parametrize("sampling", ["mw", "gl", "mwss"])
 @pytest.mark.parametrize("spin", [4, -5, 7, -7])
 def test_f32_high_spin(s2b, rng, sampling, spin):
-    """float32 plans with |spin| >= 4 run the recursion on a float64 plan internally; the
-    float32 result must still meet the float32 tolerance."""
+    """float32 plans at |spin| >= 4 (orders m < |spin| by the degree recursion) against the
+    float64 oracle."""
     L = 48
     flm = oracle.signal.generate_flm(rng, L, 0, spin, False)
     ref = oracle.spherical.inverse(flm, L, spin, None, sampling)
@@ -267,3 +270,39 @@ def test_precompute_wigner_golden(s2b, golden, rng, precision):
     f = s2b.precompute.wigner_inverse(flmn, L, N, K, "healpix", nside=nside, precision=precision)
     ref = s2b.wigner.inverse(flmn, L, N, nside, "healpix", precision=precision)
     assert relerr(f, ref) < tol
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_high_spin_exact_near_poles(s2b, precision):
+    """Unit coefficients at orders |m| < |spin| on the rings nearest the poles against exact
+    values (Wigner's sum in 60 digits, tests/golden/make_high_spin.py). Upstream's
+    m-recursion runs through a decaying range there and loses digits (e.g. the oracle's
+    L=128 spin -7 round trip is off by 7e-6); the degree recursion keeps full precision."""
+    data = np.load(os.path.join(GOLDEN_DIR, "high_spin.npz"))
+    with open(os.path.join(GOLDEN_DIR, "high_spin.json")) as fh:
+        index = json.load(fh)
+    tol = TOL64 * 1e-2 if precision == "f64" else TOL32
+    for c in index:
+        L, spin = c["L"], c["spin"]
+        phi = 2.0 * np.pi * np.arange(2 * L - 1) / (2 * L - 1)
+        vals = data[c["name"] + "/values"]
+        for k, (l, m) in enumerate(c["lm"]):
+            flm = np.zeros((L, 2 * L - 1), dtype=np.complex128)
+            flm[l, L - 1 + m] = 1.0
+            f = s2b.inverse(flm, L, spin, None, "mw", precision=precision)
+            scale = np.sqrt((2 * l + 1) / (4 * np.pi))
+            for j, t in enumerate(c["rings"]):
+                err = np.max(np.abs(f[t] - vals[k, j] * np.exp(1j * m * phi))) / scale
+                assert err < tol, (L, spin, l, m, t, err)
+
+
+@pytest.mark.parametrize("sampling", ["mw", "gl"])
+@pytest.mark.parametrize("spin", [5, -7, -15, -40])
+def test_high_spin_round_trip_L256(s2b, rng, sampling, spin):
+    """forward(inverse(flm)) = flm at L=256 (exact quadrature) for large spins."""
+    L = 256
+    flm = oracle.signal.generate_flm(rng, L, 0, spin, False)
+    for prec, tol in (("f64", TOL64), ("f32", TOL32)):
+        f = s2b.inverse(flm, L, spin, None, sampling, precision=prec)
+        g = s2b.forward(f, L, spin, None, sampling, precision=prec)
+        assert relerr(g, flm) < tol, (prec, relerr(g, flm))
