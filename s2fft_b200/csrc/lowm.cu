@@ -8,18 +8,10 @@
 // rounding errors grow like the dominant solution (first MW ring at L = 512, n = 7:
 // d^7_{0,7} = 1.2e-18 comes out as 6.0 in double). The range lies inside m < |s| on every
 // ring, so the latitudinal kernels leave the orders m < |s| out and the kernels below add
-// them. For fixed (m, n) the degree recursion
-//   d^{l+1} = a_l (cos(theta) - m n / (l (l + 1))) d^l - b_l d^{l-1},
-//   a_l = (2l + 1)(l + 1) / q_l,  q_l = sqrt(((l + 1)^2 - m^2)((l + 1)^2 - n^2)),
-//   b_l = (l + 1) sqrt((l^2 - m^2)(l^2 - n^2)) / (l q_l),
-// started at l = |n| from the closed form
-//   d^j_{m,j} = sqrt(C(2j, j+m)) cos^{j+m}(theta/2) sin^{j-m}(theta/2),
-//   d^j_{m,-j} = (-1)^{m+j} sqrt(C(2j, j-m)) cos^{j-m}(theta/2) sin^{j+m}(theta/2),
-// runs in the growing or oscillating direction for every theta and is stable (it is the
-// degree recursion of Kostelec & Rockmore, J. Fourier Anal. Appl. 14 (2008) 145-179).
-// All arithmetic is double, with a running power-of-two exponent for the small values
-// near the poles; the values enter the sums in the monic form dt = d / g_{l,m} of the
-// tables they complete.
+// them by the degree recursion at fixed (m, n) (s2b_degree.h), which is stable for every
+// theta. All arithmetic is double, with a running power-of-two exponent for the small
+// values near the poles; the values enter the sums in the monic form dt = d / g_{l,m} of
+// the tables they complete.
 //
 // Cost: |s| orders out of L, one thread per (ring, order, half, map); the degree loop is
 // sequential per thread, its coefficients are shared per CTA in shared memory.
@@ -27,6 +19,7 @@
 
 #include <cstdint>
 
+#include "s2b_degree.h"
 #include "s2b_dev.h"
 #include "s2b_lowm.h"
 
@@ -51,11 +44,10 @@ __device__ void lowm_fill(LowmChunk& ch, const double* __restrict__ g, int L, in
     const int l = l0 + i;
     double a = 0.0, c = 0.0, b = 0.0, ig = 0.0;
     if (l < L) {
-      const double ld = (double)l, l1 = ld + 1.0, mm = (double)m * m, nn = (double)n * n;
-      const double q = sqrt((l1 * l1 - mm) * (l1 * l1 - nn));
-      a = (2.0 * ld + 1.0) * l1 / q;
-      c = (double)m * (double)n / (ld * l1);
-      b = l1 * sqrt((ld * ld - mm) * (ld * ld - nn)) / (ld * q);
+      const DegreeCoef k = degree_coef(l, m, n);
+      a = k.a;
+      c = k.c;
+      b = k.b;
       ig = 1.0 / g[(size_t)m * L + l];
     }
     ch.a[i] = a;
@@ -65,31 +57,10 @@ __device__ void lowm_fill(LowmChunk& ch, const double* __restrict__ g, int L, in
   }
 }
 
-// d^{|n|}_{m,n}(theta) = v 2^E for |m| < |n|.
-__device__ void lowm_seed(const RingInfo& ri, int m, int n, double& v, int& E) {
-  const int j = n < 0 ? -n : n;
-  const int kc = n > 0 ? j + m : j - m;  // power of cos(theta/2)
-  const int ks = 2 * j - kc;             // power of sin(theta/2)
-  const double lb = 0.5 * (lgamma(2.0 * j + 1.0) - lgamma(kc + 1.0) - lgamma(ks + 1.0)) *
-                    1.4426950408889634;  // log2 sqrt(binom(2j, kc))
-  const double lg = lb + (double)kc * ri.lc + (double)ks * ri.ls;
-  E = (int)floor(lg);
-  v = exp2(lg - (double)E);
-  if (n < 0 && ((m + j) & 1)) v = -v;
-}
-
-// one degree step; values above 2^64 are rescaled into the exponent
+// one degree step with the chunk's coefficients
 __device__ __forceinline__ void lowm_step(const LowmChunk& ch, int i, double ct, double& cur,
                                           double& prv, int& E, double& sc) {
-  const double nx = ch.a[i] * (ct - ch.c[i]) * cur - ch.b[i] * prv;
-  prv = cur;
-  cur = nx;
-  if (fabs(cur) > 0x1p64) {
-    cur *= 0x1p-64;
-    prv *= 0x1p-64;
-    E += 64;
-    sc = ldexp(1.0, E);
-  }
+  degree_step(ch.a[i], ch.c[i], ch.b[i], ct, cur, prv, E, sc);
 }
 
 template <typename Real>
@@ -110,7 +81,7 @@ __global__ void __launch_bounds__(kLowmRings) lowm_synth_kernel(const LowmParams
   const double ct = ri.B / ri.A;  // cos(theta)
   double cur = 0.0, prv = 0.0, sx = 0.0, sy = 0.0;
   int E = 0;
-  if (live) lowm_seed(ri, m, n, cur, E);
+  if (live) degree_seed(ri.lc, ri.ls, m, n, cur, E);
   double sc = ldexp(1.0, E);
   const R2* __restrict__ F =
       reinterpret_cast<const R2*>(p.F) + (size_t)(b * p.nhalf + half) * p.NB * TR * 32;
@@ -169,7 +140,7 @@ __global__ void __launch_bounds__(kLowmRings) lowm_project_kernel(const LowmPara
         p.G)[(((size_t)b * p.nhalf + half) * TR + m + kPadLo) * p.Gs + r];
     gx = x.x;
     gy = x.y;
-    lowm_seed(ri, m, n, cur, E);
+    degree_seed(ri.lc, ri.ls, m, n, cur, E);
   }
   double sc = ldexp(1.0, E);
   R2* __restrict__ acc =

@@ -22,6 +22,7 @@
 
 #include <type_traits>
 
+#include "s2b_degree.h"
 #include "s2b_precompute.h"
 
 namespace s2b {
@@ -128,6 +129,57 @@ __global__ void kernel_table_kernel(KernelTableParams p) {
         wv *= kDn;
         e += 1;
       }
+    }
+  }
+}
+
+// Orders |m| < |s| of the table by the degree recursion (s2b_degree.h): the m-recursion
+// above runs, on rings with n cos(theta) > 0, through a range below m = n cos(theta) where
+// d^l_{m,n} decays as m decreases and loses digits there; that range lies inside |m| < |s|.
+// One thread per (ring, half, order) overwrites those entries for every l (poles keep
+// their closed forms).
+template <typename Real>
+__global__ void kernel_table_lowm_kernel(KernelTableParams p) {
+  const int as = p.spin < 0 ? -p.spin : p.spin;
+  const long total = (long)p.nth * 2 * as;
+  const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (idx >= total) return;
+  const int t = (int)(idx / (2 * as));
+  const int half = (int)((idx / as) % 2);
+  const int m = (int)(idx % as);
+  if (half == 1 && (m == 0 || p.reality)) return;  // order 0 and m >= 0 tables: half 0 only
+  const int L = p.L, s = p.spin;
+  const double th = p.theta[t];
+  if (th < 1e-12 || th > 3.141592653589793 - 1e-12) return;
+  const int n = half == 0 ? -s : s;
+  const int col = half == 0 ? m : -m;  // d^l_{-m,-s} = (-1)^(m+s) d^l_{m,s}
+  const double sgn = (half == 1 && ((m + s) % 2 + 2) % 2) ? -1.0 : 1.0;
+  const double w = p.weights ? p.weights[t] : 1.0;
+  const int m0 = p.reality ? 0 : -(L - 1);
+  const int M = L - m0;
+  const int mi = col - m0;
+  if (mi < 0 || mi >= M) return;
+  double ph_c = 1.0, ph_s = 0.0;
+  if (p.complex_out && p.phi0) sincos((p.forward ? -1.0 : 1.0) * (double)col * p.phi0[t], &ph_s, &ph_c);
+  const double ct = cos(th);
+  double cur, prv = 0.0;
+  int E;
+  degree_seed(log2(cos(th / 2.0)), log2(sin(th / 2.0)), m, n, cur, E);
+  double sc = ldexp(1.0, E);
+  for (int l = as; l < L; ++l) {
+    const double v = sgn * cur * sc * sqrt((2.0 * l + 1.0) / (4.0 * 3.141592653589793)) * w;
+    const size_t at = ((size_t)t * L + l) * M + mi;
+    if (p.complex_out) {
+      P2<Real> o;
+      o.x = (Real)(v * ph_c);
+      o.y = (Real)(v * ph_s);
+      reinterpret_cast<P2<Real>*>(p.out)[at] = o;
+    } else {
+      reinterpret_cast<Real*>(p.out)[at] = (Real)v;
+    }
+    if (l + 1 < L) {
+      const DegreeCoef k = degree_coef(l, m, n);
+      degree_step(k.a, k.c, k.b, ct, cur, prv, E, sc);
     }
   }
 }
@@ -289,6 +341,13 @@ cudaError_t launch_kernel_table(bool fp64, const KernelTableParams& p, cudaStrea
     kernel_table_kernel<double><<<pgrid(total, 128), 128, 0, s>>>(p);
   else
     kernel_table_kernel<float><<<pgrid(total, 128), 128, 0, s>>>(p);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || p.spin == 0) return e;
+  const long low = (long)p.nth * 2 * (p.spin < 0 ? -p.spin : p.spin);
+  if (fp64)
+    kernel_table_lowm_kernel<double><<<pgrid(low, 128), 128, 0, s>>>(p);
+  else
+    kernel_table_lowm_kernel<float><<<pgrid(low, 128), 128, 0, s>>>(p);
   return cudaGetLastError();
 }
 

@@ -306,3 +306,21 @@ def test_high_spin_round_trip_L256(s2b, rng, sampling, spin):
         f = s2b.inverse(flm, L, spin, None, sampling, precision=prec)
         g = s2b.forward(f, L, spin, None, sampling, precision=prec)
         assert relerr(g, flm) < tol, (prec, relerr(g, flm))
+
+
+@pytest.mark.parametrize("sampling", ["mw", "healpix"])
+def test_precompute_high_spin(s2b, rng, sampling):
+    """Precompute kernels at spin -7 (orders |m| < 7 by the degree recursion) against the
+    on-the-fly transforms, and the exact near-pole values through the kernel inverse."""
+    L, spin, nside = (128, -7, None) if sampling == "mw" else (64, -7, 32)
+    flm = oracle.signal.generate_flm(rng, L, 0, spin, False)
+    kin = s2b.precompute.spin_spherical_kernel(L, spin, False, sampling, nside, False)
+    kfw = s2b.precompute.spin_spherical_kernel(L, spin, False, sampling, nside, True)
+    f = s2b.precompute.inverse(flm, L, spin, kin, sampling, False, nside=nside)
+    f_otf = s2b.inverse(flm, L, spin, nside, sampling)
+    assert relerr(f, f_otf) < TOL64, relerr(f, f_otf)
+    g = s2b.precompute.forward(f_otf, L, spin, kfw, sampling, False, nside=nside)
+    g_otf = s2b.forward(f_otf, L, spin, nside, sampling)
+    assert relerr(g, g_otf) < TOL64, relerr(g, g_otf)
+    if sampling == "mw":
+        assert relerr(g, flm) < TOL64, relerr(g, flm)
