@@ -159,10 +159,12 @@ int s2b_precompute_forward(s2b_plan* plan, const void* kernel, const void* f, vo
  * process on CUDA errors, lib/include/hresult.h:26-33). */
 int s2b_plan_status(s2b_plan* plan, int* status);
 
-/* Tile variant of the latitudinal kernels for later calls on this plan (and its
- * sub-plans): key 0 = forward (value 0: 16 rings per warp in float / 8 in double;
- * 1: half of that, twice the CTAs), key 1 = inverse (value 0: 2 rings per lane in
- * float; 1: one ring per lane). Results are identical; only the speed differs, which
+/* Launch shape of the latitudinal kernels for later calls on this plan (and its
+ * sub-plans): key 0 = forward tile (value 0: 16 rings per warp in float / 8 in double;
+ * 1: half of that, twice the CTAs), key 1 = inverse tile (value 0: 2 rings per lane in
+ * float; 1: one ring per lane), key 2 = inverse segments along m (value 1, 2 or 4: each
+ * CTA's m-range split into that many independently restarted parts; the default
+ * depends on the grid size). Results agree to rounding; only the speed differs, which
  * depends on band-limit, batch and sampling. Used by the autotuner of the batched
  * front-end. No upstream counterpart. */
 int s2b_plan_set_tuning(s2b_plan* plan, int key, int value);

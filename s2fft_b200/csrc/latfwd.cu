@@ -96,12 +96,14 @@ __global__ void fwd_start_kernel(const FwdStartParams p) {
   int M = __reduce_max_sync(0xffffffffu, ms);
   if (M >= 0) M |= p.group - 1;
 
-  // pass 3: (dt_M, dt_{M+1}) of this degree
-  double cur = 0.0, prv = 0.0;
-  if (valid && M >= 0) {
-    if (M >= l) {
+  // pass 3: (dt_X, dt_{X+1}) of this degree for a start X >= 0
+  auto start_pair = [&](int X, double& cur, double& prv) {
+    cur = 0.0;
+    prv = 0.0;
+    if (!valid) return;
+    if (X >= l) {
       const double dl = sgn * exp2(lg);
-      const int dlt = M - l;
+      const int dlt = X - l;
       if ((dlt & 1) == 0)
         cur = ((dlt >> 1) & 1) ? -dl : dl;
       else
@@ -109,16 +111,39 @@ __global__ void fwd_start_kernel(const FwdStartParams p) {
     } else {
       int E = (int)floor(lg);
       double v = sgn * exp2(lg - (double)E), w = 0.0;
-      for (int m = l; m > M; --m) step(v, w, E, m);
+      for (int m = l; m > X; --m) step(v, w, E, m);
       cur = ldexp(v, E);
       prv = ldexp(w, E);
     }
-  }
+  };
+  double cur = 0.0, prv = 0.0;
+  if (M >= 0) start_pair(M, cur, prv);
   R2 o;
   o.x = (Real)cur;
   o.y = (Real)prv;
   reinterpret_cast<R2*>(p.Vst)[wid * kFwdBlock + lane] = o;
   if (lane == 0) p.Mst[wid] = M;
+  if (p.Mst1) {
+    // restart tables of the inverse kernel's m-split, one per inner boundary
+    const int q = blk < p.NB - 1 - blk ? blk : p.NB - 1 - blk;
+    const size_t nst = (size_t)p.nhalf * p.NB * p.nrings;
+    for (int k = 1; k < kInvSegMax; ++k) {
+      const int bk = inv_mbound(L, p.NB, q, k);
+      int Mk = M;
+      double ck = cur, pk = prv;
+      if (M >= bk) {
+        Mk = bk > 0 ? bk - 1 : -1;
+        ck = 0.0;
+        pk = 0.0;
+        if (Mk >= 0) start_pair(Mk, ck, pk);
+      }
+      R2 ok;
+      ok.x = (Real)ck;
+      ok.y = (Real)pk;
+      reinterpret_cast<R2*>(p.Vst1)[((k - 1) * nst + wid) * kFwdBlock + lane] = ok;
+      if (lane == 0) p.Mst1[(k - 1) * nst + wid] = Mk;
+    }
+  }
 }
 
 size_t fwd_start_bytes(bool fp64, int L, int nhalf, int nrings) {

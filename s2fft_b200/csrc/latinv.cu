@@ -72,7 +72,16 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
   const int NB = p.NB;
   const int TR = tab_rows(L);
   const int r0 = (int)blockIdx.x * NRT;
-  const int kb0 = (int)blockIdx.y, kb1 = NB - 1 - (int)blockIdx.y;
+  // blockIdx.y = block pair + NB/2 * segment; segment seg of nseg spans the boundaries
+  // g = seg * kInvSegMax / nseg and g + kInvSegMax / nseg (inv_mbound)
+  const int npair = NB / 2;
+  const int q = (int)blockIdx.y % npair, seg = (int)blockIdx.y / npair;
+  const int kb0 = q, kb1 = NB - 1 - q;
+  const int nseg = p.Mst1 ? p.nseg : 1;
+  const int gstep = kInvSegMax / nseg, g0 = seg * gstep;
+  const size_t nst = (size_t)p.nhalf * NB * p.nrings;
+  const int* __restrict__ Mtab = g0 ? p.Mst1 + (size_t)(g0 - 1) * nst : p.Mst;
+  const int mbot = inv_mbound(L, NB, q, g0 + gstep);  // lowest m of the segment
   const int half = (int)(blockIdx.z % p.nhalf);
   const int b = (int)(blockIdx.z / p.nhalf);
 
@@ -89,15 +98,17 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
 #pragma unroll
     for (int i = 0; i < T; ++i) {
       const int r = r0 + lane * T + i;
-      Ms[x][i] = r < p.nrings ? p.Mst[((size_t)half * NB + (x ? kb1 : kb0)) * p.nrings + r] : -1;
+      Ms[x][i] = r < p.nrings ? Mtab[((size_t)half * NB + (x ? kb1 : kb0)) * p.nrings + r] : -1;
       mx = Ms[x][i] > mx ? Ms[x][i] : mx;
     }
     Mb[x] = __reduce_max_sync(0xffffffffu, mx);
   }
   const int mtop = Mb[0] > Mb[1] ? Mb[0] : Mb[1];
-  if (mtop < 0) return;  // nothing significant in this tile (uniform)
-  const int ngroups = (mtop + 1) / R;
-  const R2* __restrict__ Vst = reinterpret_cast<const R2*>(p.Vst);
+  if (mtop < mbot) return;  // nothing significant in this tile and segment (uniform)
+  const int ngroups = (mtop + 1 - mbot) / R;  // mtop = -1 mod 8, mbot = 0 mod 8
+  const R2* __restrict__ Vst =
+      g0 ? reinterpret_cast<const R2*>(p.Vst1) + (size_t)(g0 - 1) * nst * kFwdBlock
+         : reinterpret_cast<const R2*>(p.Vst);
 
   Real v[K][T], w[K][T];
 #pragma unroll
@@ -277,13 +288,15 @@ static cudaError_t launch_inv2_cfg(const Inv2Params& p, cudaStream_t s) {
   cudaError_t err =
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::total);
   if (err != cudaSuccess) return err;
-  dim3 grid((p.nrings + Lay::NRT - 1) / Lay::NRT, p.NB / 2, p.nhalf * p.batch);
+  dim3 grid((p.nrings + Lay::NRT - 1) / Lay::NRT, (p.NB / 2) * (p.Mst1 ? p.nseg : 1),
+            p.nhalf * p.batch);
   kern<<<grid, Lay::NT, Lay::total, s>>>(p);
   return cudaGetLastError();
 }
 
 cudaError_t launch_inv2(bool fp64, bool dual, const Inv2Params& p, cudaStream_t s) {
   if (p.nrings <= 0) return cudaSuccess;
+  if (p.Mst1 && !(p.nseg == 1 || p.nseg == 2 || p.nseg == 4)) return cudaErrorInvalidValue;
   if (!fp64) {
     // 2 rings per lane (tile 1: one), 8-step groups (the start tables' alignment)
     if (p.tile == 1)

@@ -367,6 +367,9 @@ struct s2b_plan {
   // adjoint spectra (recursed rings first, then north / south pole), adjoint chain table
   int* inv_Mst = nullptr;
   void* inv_Vst = nullptr;
+  int* inv_Mst1 = nullptr;  // restart tables of the inverse kernel's m-split
+  void* inv_Vst1 = nullptr;
+  int inv_nseg = 1;         // segments along m of the inverse kernel (1, 2, 4)
   int* adj_col = nullptr;
   int adj_Gs = 4, adj_pole_s = -1, adj_pole_n = -1;
   void* col_ph_adj = nullptr;
@@ -639,6 +642,18 @@ static int build_plan(s2b_plan* p) {
     p->allocs.push_back(p->inv_Mst);
     S2B_CK(cudaMalloc(&p->inv_Vst, fwd_start_bytes(p->fp64, L, p->nhalf, p->inv_nrings)));
     p->allocs.push_back(p->inv_Vst);
+    S2B_CK(cudaMalloc(&p->inv_Mst1, (kInvSegMax - 1) * nst * sizeof(int)));
+    p->allocs.push_back(p->inv_Mst1);
+    S2B_CK(cudaMalloc(&p->inv_Vst1, (kInvSegMax - 1) *
+                                        fwd_start_bytes(p->fp64, L, p->nhalf, p->inv_nrings)));
+    p->allocs.push_back(p->inv_Vst1);
+    // segments along m: enough CTAs for about two waves of 3 per SM on 148 SMs
+    {
+      const long rings_per_cta = p->fp64 ? 32 : 64;
+      const long ctas = (p->inv_nrings + rings_per_cta - 1) / rings_per_cta * (p->fwd_NB / 2) *
+                        p->nhalf * d.batch;
+      p->inv_nseg = ctas >= 888 ? 1 : (2 * ctas >= 888 ? 2 : 4);
+    }
     FwdStartParams fp{};
     fp.L = L;
     fp.L0 = d.L_lower;
@@ -653,6 +668,8 @@ static int build_plan(s2b_plan* p) {
     fp.g = p->gtab;
     fp.Mst = p->inv_Mst;
     fp.Vst = p->inv_Vst;
+    fp.Mst1 = p->inv_Mst1;
+    fp.Vst1 = p->inv_Vst1;
     S2B_CK(launch_fwd_start(p->fp64, fp, 0));
   }
 
@@ -905,6 +922,9 @@ static int run_inverse(s2b_plan* p, const void* flm, void* f, char* ws, cudaStre
     lp.NB = p->fwd_NB;
     lp.Mst = p->inv_Mst;
     lp.Vst = p->inv_Vst;
+    lp.Mst1 = p->inv_Mst1;
+    lp.Vst1 = p->inv_Vst1;
+    lp.nseg = p->inv_nseg;
     lp.Hb = p->fwd_Hb;
     lp.lam = p->inv_lam;
     lp.Ls = p->inv_Ls;
@@ -1769,12 +1789,19 @@ int s2b_plan_status(s2b_plan* p, int* status) {
 }
 
 int s2b_plan_set_tuning(s2b_plan* p, int key, int value) {
-  if (!p || (key != 0 && key != 1) || (value != 0 && value != 1))
-    return fail(S2B_ERR_INVALID, "key must be 0 (forward) or 1 (inverse), value 0 or 1");
+  if (!p) return fail(S2B_ERR_INVALID, "plan must be non-NULL");
+  const bool tile = (key == 0 || key == 1) && (value == 0 || value == 1);
+  const bool seg = key == 2 && (value == 1 || value == 2 || value == 4);
+  if (!tile && !seg)
+    return fail(S2B_ERR_INVALID,
+                "key 0 (forward tile) or 1 (inverse tile) takes 0 or 1; key 2 (inverse segments "
+                "along m) takes 1, 2 or 4");
   if (key == 0)
     p->tile_fwd = value;
-  else
+  else if (key == 1)
     p->tile_inv = value;
+  else
+    p->inv_nseg = value;
   for (s2b_plan* sp : p->subs) s2b_plan_set_tuning(sp, key, value);
   return S2B_OK;
 }

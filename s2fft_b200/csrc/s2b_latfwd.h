@@ -12,6 +12,27 @@ namespace s2b {
 constexpr int kFwdBlock = 32;
 __host__ __device__ inline int fwd_nblocks(int L) { return 2 * ((L + 2 * kFwdBlock - 1) / (2 * kFwdBlock)); }
 
+// Split of the inverse kernel along m: block pair q (blocks q and NB-1-q) runs as up to
+// kInvSegMax segments with about the same number of block-steps each (m from the pair's top
+// degree down: one block above the lower block's top degree, two below). Boundary k of
+// kInvSegMax (k = 0..kInvSegMax, decreasing in k, boundary kInvSegMax = 0) is a multiple
+// of 8, so every segment starts on a group boundary; a run with S segments (S dividing
+// kInvSegMax) uses every (kInvSegMax / S)-th boundary. Segment k >= 1 restarts the states
+// begun above its top boundary b from exact values at m = b - 1.
+constexpr int kInvSegMax = 4;
+__host__ __device__ inline int inv_mbound(int L, int NB, int q, int k) {
+  int top = (NB - 1 - q) * 32 + 31;
+  if (top > L - 1) top = L - 1;
+  if (k <= 0) return top + 1;
+  if (k >= kInvSegMax) return 0;
+  int lo = q * 32 + 32;
+  if (lo > top + 1) lo = top + 1;
+  const int w1 = top + 1 - lo, W = w1 + 2 * lo, t = (int)((long)k * W / kInvSegMax);
+  int b = t <= w1 ? top + 1 - t : lo - (t - w1) / 2;
+  b &= ~7;
+  return b < 0 ? 0 : b;
+}
+
 // Start table of the forward recursion.
 //   Mst [nhalf][NB][nrings]      first m of the recursion for (ring, block), a group start,
 //                                 -1 when no degree of the block is significant on the ring
@@ -25,6 +46,10 @@ struct FwdStartParams {
   const double* g;          // [m][l] monic scale
   int* Mst;
   void* Vst;
+  // optional restart tables of the inverse kernel's m-split, [kInvSegMax - 1][table]: for
+  // boundary k (inv_mbound) states with M >= b restart at b - 1 (b > 0), others keep M
+  int* Mst1;
+  void* Vst1;
 };
 
 struct Fwd2Params {
@@ -47,6 +72,9 @@ struct Inv2Params {
   int L, nrings, nhalf, batch, NB;
   const int* Mst;           // start tables of these rings (FwdStartParams layout)
   const void* Vst;
+  const int* Mst1;          // restart tables of the m-split (nullptr: one segment)
+  const void* Vst1;
+  int nseg;                 // segments along m: 1, 2 or 4 (with Mst1)
   const void* Hb;           // [NB][tab_rows][32]
   const void* lam;          // [nhalf][tab_rows][Ls]
   int Ls;
