@@ -420,7 +420,9 @@ def run_batched_uneven(torch, nmaps=256, steps=3, warmup=1, seed=4242):
             "sequential_maps_per_s": nmaps / (ms_seq * 1e-3), "sequential_ms": ms_seq,
             "max_rel_err_vs_unbatched": worst, "max_rel_roundtrip_err": rt,
             "tiles": {"forward_half": sum(g.tiles[0] for g in b.groups),
-                      "inverse_one_ring": sum(g.tiles[1] for g in b.groups)}}
+                      "inverse_one_ring": sum(g.tiles[1] & 1 for g in b.groups),
+                      "inverse_segments": {str(n): sum(g.tiles[2] == n for g in b.groups)
+                                           for n in (1, 2, 4)}}}
 
 
 def run_healpix_iter(torch, nside=256, L=512, steps=5, warmup=2):

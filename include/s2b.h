@@ -161,10 +161,11 @@ int s2b_plan_status(s2b_plan* plan, int* status);
 
 /* Launch shape of the latitudinal kernels for later calls on this plan (and its
  * sub-plans): key 0 = forward tile (value 0: 16 rings per warp in float / 8 in double;
- * 1: half of that, twice the CTAs), key 1 = inverse tile (value 0: 2 rings per lane in
- * float; 1: one ring per lane), key 2 = inverse segments along m (value 1, 2 or 4: each
- * CTA's m-range split into that many independently restarted parts; the default
- * depends on the grid size). Results agree to rounding; only the speed differs, which
+ * 1: half of that, twice the CTAs), key 1 = inverse tile (value bit 0: one ring per
+ * lane instead of two in float; bit 1: start values read from global memory instead of
+ * staged in shared memory), key 2 = inverse segments along m (value 1, 2 or 4: each
+ * CTA's m-range split into that many independently restarted parts; default 4).
+ * Results agree to rounding; only the speed differs, which
  * depends on band-limit, batch and sampling. Used by the autotuner of the batched
  * front-end. No upstream counterpart. */
 int s2b_plan_set_tuning(s2b_plan* plan, int key, int value);

@@ -5,8 +5,9 @@ A workload mixes band-limits, spins and samplings. Maps that share
 the group size, so each kernel of the chain processes the whole group in one
 launch. Groups run concurrently on several CUDA streams (largest first), the
 whole inverse + forward of all groups is captured once in a CUDA graph and
-replayed on every call, and an autotuner picks each group's latitudinal tile
-variant (``s2b_plan_set_tuning``) by timing the variants on the group itself.
+replayed on every call, and an autotuner picks each group's latitudinal launch
+shapes (``s2b_plan_set_tuning``: tiles, inverse segments along m) by timing them
+on the group itself.
 
 Only the host-side scheduling is new here; every transform runs the same
 kernels as :func:`s2fft_b200.inverse` / :func:`s2fft_b200.forward`, so each
@@ -46,7 +47,7 @@ class _Group:
     flm_out: torch.Tensor = None
     ws_inv: torch.Tensor = None
     ws_fwd: torch.Tensor = None
-    tiles: tuple = (0, 0)
+    tiles: tuple = (0, 0, 1)  # (forward tile, inverse tile, inverse segments along m)
 
     def work(self):
         nth = f_shape(self.L, self.sampling, self.nside)[0] if self.sampling != "healpix" \
@@ -148,8 +149,8 @@ class BatchedSHT:
 
     # -- autotuner --------------------------------------------------------------------
     def tune(self, reps=3):
-        """Per group, time both tile variants of the inverse and the forward latitudinal
-        kernels on the group itself and keep the faster ones."""
+        """Per group, time the launch shapes of the inverse (tile x segments along m) and the
+        forward (tile) latitudinal kernels on the group itself and keep the fastest."""
         lib = _lib.lib()
         stream = torch.cuda.current_stream(self.device)
         h = ctypes.c_void_p(stream.cuda_stream)
@@ -164,24 +165,34 @@ class BatchedSHT:
             e1.synchronize()
             return e0.elapsed_time(e1)
 
+        inv = [(t, n) for t in (2, 3) for n in (2, 4)]  # (tile, segments along m)
         for g in self.groups:
-            best = []
-            for key, call in ((1, lambda: _lib.check(lib.s2b_inverse(
-                    g.plan.ptr, g.flm_in.data_ptr(), g.f.data_ptr(), g.ws_inv.data_ptr(),
-                    g.ws_inv.numel(), h))),
-                              (0, lambda: _lib.check(lib.s2b_forward(
-                    g.plan.ptr, g.f.data_ptr(), g.flm_out.data_ptr(), g.ws_fwd.data_ptr(),
-                    g.ws_fwd.numel(), h)))):
-                t = []
-                for v in (0, 1):
-                    _lib.check(lib.s2b_plan_set_tuning(g.plan.ptr, key, v))
-                    t.append(timed(call))
-                v = int(np.argmin(t))
-                _lib.check(lib.s2b_plan_set_tuning(g.plan.ptr, key, v))
-                best.append(v)
-            g.tiles = (best[1], best[0])  # (forward, inverse)
+            def call_inv():
+                _lib.check(lib.s2b_inverse(g.plan.ptr, g.flm_in.data_ptr(), g.f.data_ptr(),
+                                           g.ws_inv.data_ptr(), g.ws_inv.numel(), h))
+
+            def call_fwd():
+                _lib.check(lib.s2b_forward(g.plan.ptr, g.f.data_ptr(), g.flm_out.data_ptr(),
+                                           g.ws_fwd.data_ptr(), g.ws_fwd.numel(), h))
+
+            t = []
+            for tile, nseg in inv:
+                _lib.check(lib.s2b_plan_set_tuning(g.plan.ptr, 1, tile))
+                _lib.check(lib.s2b_plan_set_tuning(g.plan.ptr, 2, nseg))
+                t.append(timed(call_inv))
+            tile_inv, nseg = inv[int(np.argmin(t))]
+            _lib.check(lib.s2b_plan_set_tuning(g.plan.ptr, 1, tile_inv))
+            _lib.check(lib.s2b_plan_set_tuning(g.plan.ptr, 2, nseg))
+            t = []
+            for v in (0, 1):
+                _lib.check(lib.s2b_plan_set_tuning(g.plan.ptr, 0, v))
+                t.append(timed(call_fwd))
+            tile_fwd = int(np.argmin(t))
+            _lib.check(lib.s2b_plan_set_tuning(g.plan.ptr, 0, tile_fwd))
+            g.tiles = (tile_fwd, tile_inv, nseg)
         torch.cuda.synchronize(self.device)
 
     def summary(self):
         return [dict(L=g.L, spin=g.spin, sampling=g.sampling, maps=len(g.members),
-                     forward_tile=g.tiles[0], inverse_tile=g.tiles[1]) for g in self.groups]
+                     forward_tile=g.tiles[0], inverse_tile=g.tiles[1], inverse_segments=g.tiles[2])
+                for g in self.groups]

@@ -29,7 +29,7 @@
 
 namespace s2b {
 
-template <typename Real, bool DUAL, int T, int W, int R>
+template <typename Real, bool DUAL, int T, int W, int R, bool VST>
 struct Inv2Layout {
   using Acc = std::conditional_t<DUAL, typename Vec<Real>::t4, typename Vec<Real>::t2>;
   static constexpr int K = 16;       // degrees per warp
@@ -42,15 +42,17 @@ struct Inv2Layout {
   static constexpr size_t stage_bytes = h_bytes + f_bytes + l_bytes;
   static constexpr size_t buf_bytes = (size_t)R * W * NRT * sizeof(Acc);
   // start values of the CTA's states: [2 blocks][NRT rings][32] (d~_M, d~_{M+1})
-  static constexpr size_t v_bytes = (size_t)2 * NRT * kFwdBlock * 2 * sizeof(Real);
+  // (VST: staged by bulk copy; otherwise each lane reads its own from global memory, which
+  // leaves room for one more CTA per SM)
+  static constexpr size_t v_bytes = VST ? (size_t)2 * NRT * kFwdBlock * 2 * sizeof(Real) : 0;
   static constexpr size_t total = 2 * stage_bytes + buf_bytes + v_bytes + 32;
   static_assert(W == 4, "two warps per 32-degree block, two blocks per CTA");
   static_assert(stage_bytes % 16 == 0 && buf_bytes % 16 == 0, "align");
 };
 
-template <typename Real, bool DUAL, int T, int W, int R>
+template <typename Real, bool DUAL, int T, int W, int R, bool VST>
 __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p) {
-  using Lay = Inv2Layout<Real, DUAL, T, W, R>;
+  using Lay = Inv2Layout<Real, DUAL, T, W, R, VST>;
   using Acc = typename Lay::Acc;
   using R2 = typename Vec<Real>::t2;
   constexpr int K = Lay::K;
@@ -156,21 +158,24 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
   }
   __syncthreads();
   if (tid == 0) {
-    // the start values of both blocks for this CTA's rings, once
-    int nr = p.nrings - r0;
-    if (nr > NRT) nr = NRT;
-    const unsigned vb = (unsigned)(nr * kFwdBlock * sizeof(R2));
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    mbar_expect_tx(&mbar[2], 2 * vb);
+    if constexpr (VST) {
+      // the start values of both blocks for this CTA's rings, once
+      int nr = p.nrings - r0;
+      if (nr > NRT) nr = NRT;
+      const unsigned vb = (unsigned)(nr * kFwdBlock * sizeof(R2));
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_expect_tx(&mbar[2], 2 * vb);
 #pragma unroll
-    for (int x = 0; x < 2; ++x)
-      bulk_g2s(const_cast<R2*>(vS) + (size_t)x * NRT * kFwdBlock,
-               Vst + (((size_t)half * NB + (x ? kb1 : kb0)) * p.nrings + r0) * kFwdBlock, vb,
-               &mbar[2]);
+      for (int x = 0; x < 2; ++x)
+        bulk_g2s(const_cast<R2*>(vS) + (size_t)x * NRT * kFwdBlock,
+                 Vst + (((size_t)half * NB + (x ? kb1 : kb0)) * p.nrings + r0) * kFwdBlock, vb,
+                 &mbar[2]);
+    }
     issue(0);
     if (ngroups > 1) issue(1);
   }
-  const bool vok = mbar_wait(&mbar[2], 0);
+  bool vok = true;
+  if constexpr (VST) vok = mbar_wait(&mbar[2], 0);
   // highest degree of the CTA: partial sums above it are zero
   int lmax = -1;
   if (kb0 * kFwdBlock < L) lmax = kb0 * kFwdBlock + kFwdBlock - 1;
@@ -187,7 +192,10 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
 #pragma unroll
       for (int i = 0; i < T; ++i)
         if (Ms[x][i] == mgrp) {
-          const R2* src = vS + ((size_t)x * NRT + lane * T + i) * kFwdBlock + col0;
+          const R2* src =
+              VST ? vS + ((size_t)x * NRT + lane * T + i) * kFwdBlock + col0
+                  : Vst + (((size_t)half * NB + (x ? kb1 : kb0)) * p.nrings + r0 + lane * T + i) *
+                              kFwdBlock + col0;
 #pragma unroll
           for (int kk = 0; kk < K / 2; ++kk) {
             const R2 sv = src[kk];
@@ -281,10 +289,10 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
   }
 }
 
-template <typename Real, bool DUAL, int T, int R>
+template <typename Real, bool DUAL, int T, int R, bool VST>
 static cudaError_t launch_inv2_cfg(const Inv2Params& p, cudaStream_t s) {
-  using Lay = Inv2Layout<Real, DUAL, T, 4, R>;
-  auto kern = lat_inv2_kernel<Real, DUAL, T, 4, R>;
+  using Lay = Inv2Layout<Real, DUAL, T, 4, R, VST>;
+  auto kern = lat_inv2_kernel<Real, DUAL, T, 4, R, VST>;
   cudaError_t err =
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::total);
   if (err != cudaSuccess) return err;
@@ -294,16 +302,28 @@ static cudaError_t launch_inv2_cfg(const Inv2Params& p, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+template <typename Real, int T, bool VST>
+static cudaError_t launch_inv2_dual(bool dual, const Inv2Params& p, cudaStream_t s) {
+  return dual ? launch_inv2_cfg<Real, true, T, 8, VST>(p, s)
+              : launch_inv2_cfg<Real, false, T, 8, VST>(p, s);
+}
+
 cudaError_t launch_inv2(bool fp64, bool dual, const Inv2Params& p, cudaStream_t s) {
   if (p.nrings <= 0) return cudaSuccess;
   if (p.Mst1 && !(p.nseg == 1 || p.nseg == 2 || p.nseg == 4)) return cudaErrorInvalidValue;
+  // tile bit 0: one ring per lane (float; double always has one); bit 1: start values read
+  // from global memory instead of staged in shared memory. 8-step groups (the start tables'
+  // alignment).
+  const bool vst = (p.tile & 2) == 0;
   if (!fp64) {
-    // 2 rings per lane (tile 1: one), 8-step groups (the start tables' alignment)
-    if (p.tile == 1)
-      return dual ? launch_inv2_cfg<float, true, 1, 8>(p, s) : launch_inv2_cfg<float, false, 1, 8>(p, s);
-    return dual ? launch_inv2_cfg<float, true, 2, 8>(p, s) : launch_inv2_cfg<float, false, 2, 8>(p, s);
+    if (p.tile & 1)
+      return vst ? launch_inv2_dual<float, 1, true>(dual, p, s)
+                 : launch_inv2_dual<float, 1, false>(dual, p, s);
+    return vst ? launch_inv2_dual<float, 2, true>(dual, p, s)
+               : launch_inv2_dual<float, 2, false>(dual, p, s);
   }
-  return dual ? launch_inv2_cfg<double, true, 1, 8>(p, s) : launch_inv2_cfg<double, false, 1, 8>(p, s);
+  return vst ? launch_inv2_dual<double, 1, true>(dual, p, s)
+             : launch_inv2_dual<double, 1, false>(dual, p, s);
 }
 
 }  // namespace s2b

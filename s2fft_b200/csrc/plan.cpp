@@ -647,13 +647,11 @@ static int build_plan(s2b_plan* p) {
     S2B_CK(cudaMalloc(&p->inv_Vst1, (kInvSegMax - 1) *
                                         fwd_start_bytes(p->fp64, L, p->nhalf, p->inv_nrings)));
     p->allocs.push_back(p->inv_Vst1);
-    // segments along m: enough CTAs for about two waves of 3 per SM on 148 SMs
-    {
-      const long rings_per_cta = p->fp64 ? 32 : 64;
-      const long ctas = (p->inv_nrings + rings_per_cta - 1) / rings_per_cta * (p->fwd_NB / 2) *
-                        p->nhalf * d.batch;
-      p->inv_nseg = ctas >= 888 ? 1 : (2 * ctas >= 888 ? 2 : 4);
-    }
+    // launch shape of the inverse kernel, measured at L = 256 ... 2048 (MW, float and
+    // double): four segments along m, start values read from global memory (shared memory
+    // for 3 CTAs per SM), two rings per lane in float from L = 1024 and one below
+    p->inv_nseg = kInvSegMax;
+    p->tile_inv = (!p->fp64 && L >= 1024) ? 2 : 3;
     FwdStartParams fp{};
     fp.L = L;
     fp.L0 = d.L_lower;
@@ -1790,12 +1788,12 @@ int s2b_plan_status(s2b_plan* p, int* status) {
 
 int s2b_plan_set_tuning(s2b_plan* p, int key, int value) {
   if (!p) return fail(S2B_ERR_INVALID, "plan must be non-NULL");
-  const bool tile = (key == 0 || key == 1) && (value == 0 || value == 1);
+  const bool tile = (key == 0 && (value == 0 || value == 1)) || (key == 1 && value >= 0 && value <= 3);
   const bool seg = key == 2 && (value == 1 || value == 2 || value == 4);
   if (!tile && !seg)
     return fail(S2B_ERR_INVALID,
-                "key 0 (forward tile) or 1 (inverse tile) takes 0 or 1; key 2 (inverse segments "
-                "along m) takes 1, 2 or 4");
+                "key 0 (forward tile) takes 0 or 1, key 1 (inverse tile) 0 to 3, key 2 (inverse "
+                "segments along m) 1, 2 or 4");
   if (key == 0)
     p->tile_fwd = value;
   else if (key == 1)
