@@ -10,8 +10,10 @@ differentiable spin transforms (whose backward passes run the adjoint kernels)
 and a gamma DFT written as a dense (2N-1) x (2N-1) product.
 
 Difference from upstream: upstream's recursive methods raise ``Warning`` for
-N >= 8 (wigner.py:87-88); here the limit is the spin transforms' own (|spin| < 8),
-so N <= 8 is accepted.
+N >= 8 (wigner.py:87-88); here N = 8 is accepted and ``Warning`` is raised from
+N = 9. The spin transforms stay accurate for any spin (orders m < |spin| run on
+the degree recursion), so the limit only keeps the drop-in raising where upstream
+would for larger N.
 """
 
 from __future__ import annotations
@@ -37,7 +39,7 @@ def _check(L, N, nside, sampling, L_lower):
     if s not in _lib.SAMPLING:
         raise ValueError(f"Sampling scheme sampling={sampling} not supported")
     if N > 8:
-        # spins -(N-1) .. N-1 must stay below 8 (upstream warns from N = 8, wigner.py:87-88)
+        # upstream warns from N = 8 (wigner.py:87-88); N = 8 is accepted here
         raise Warning("Recursive transform may provide lower precision beyond N ~ 8")
     if N < 1 or N > L:
         raise ValueError("1 <= N <= L required")
