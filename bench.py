@@ -53,6 +53,21 @@ def parse_args():
     return ap.parse_args()
 
 
+def seeded_flm(rng, L, spin=0, reality=False):
+    """Band-limited synthetic coefficients flm[l, L-1+m]: Re and Im ~ N(0,1) for every
+    |m| <= l with max(|spin|) <= l < L; with reality, m = 0 real and
+    flm[l, -m] = (-1)^m conj(flm[l, m])."""
+    flm = np.zeros((L, 2 * L - 1), dtype=np.complex128)
+    for el in range(abs(spin), L):
+        n = 2 * el + 1
+        flm[el, L - 1 - el: L + el] = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+        if reality:
+            flm[el, L - 1] = flm[el, L - 1].real
+            m = np.arange(1, el + 1)
+            flm[el, L - 1 - m] = (-1.0) ** m * np.conj(flm[el, L - 1 + m])
+    return flm
+
+
 def triples(L, nrings, spin=0, reality=False):
     """(theta, l, m) terms with max(|m|, |s|) <= l < L, summed over rings."""
     ms = np.arange(0 if reality else -(L - 1), L)
@@ -158,14 +173,14 @@ def run_ours(args, rank, world, torch, dist):
     import s2fft_b200
     from s2fft_b200 import _lib
 
-    import oracle  # only to draw the seeded coefficients (same generator as upstream)
-
     L = args.L
     dev = torch.device("cuda", torch.cuda.current_device())
     rng = np.random.default_rng(8966433580120847635 + rank)
-    flm_np = oracle.signal.generate_flm_full_complex(rng, L)
+    flm_np = seeded_flm(rng, L)
     nrings_inv, nrings_fwd = L, 2 * L - 1
     T_inv, T_fwd = triples(L, nrings_inv), triples(L, nrings_fwd)
+    # executed: the forward's 2L-1 rings run as L ring pairs (the equator pairs with itself)
+    T_fwd_exec = triples(L, (nrings_fwd + 1) // 2)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)  # > 126 MB L2
 
     def plans(precision):
@@ -296,7 +311,7 @@ def run_ours(args, rank, world, torch, dist):
     e2e = world * e_steps / (e2e_ms * 1e-3)
     return dict(value=value, value64=value64, e2e=e2e, ms32=ms32 / steps, lat32=lat32,
                 lat64=lat64, err32=err32, err64=err64, err_mixed=err_mixed, clocks=clk,
-                T_inv=T_inv, T_fwd=T_fwd, h2d=host_in[0].numel() * 8, d2h=host_out[0].numel() * 8)
+                T_inv=T_inv, T_fwd=T_fwd, T_fwd_exec=T_fwd_exec, h2d=host_in[0].numel() * 8, d2h=host_out[0].numel() * 8)
 
 
 # ---------------------------------------------------------------------------
@@ -323,15 +338,12 @@ def run_batched_precompute(torch, L=512, B=64, steps=5, warmup=2):
     import s2fft_b200
     from s2fft_b200 import _lib
 
-    import oracle
-
     dev = torch.device("cuda", torch.cuda.current_device())
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     out = {"workload": f"precompute forward, GL, L={L}, {B} maps, spin +-2", "maps": B}
     for spin in (2, -2):
         rng = np.random.default_rng(1000 + spin)
-        flm = np.stack([oracle.signal.generate_flm_full_complex(rng, L, 0, spin)
-                        for _ in range(B)])
+        flm = np.stack([seeded_flm(rng, L, spin) for _ in range(B)])
         x64 = torch.from_numpy(flm).to(dev)
         f64 = s2fft_b200.inverse(x64, L, spin, None, "gl")  # seeded maps from the inverse
         K64 = s2fft_b200.precompute.spin_spherical_kernel(L, spin, False, "gl", None, True)
@@ -383,14 +395,12 @@ def run_batched_uneven(torch, nmaps=256, steps=3, warmup=1, seed=4242):
     import s2fft_b200
     from s2fft_b200.batch import BatchedSHT
 
-    import oracle
-
     rng = np.random.default_rng(seed)
     Ls = [64, 128, 256, 512, 1024]
     smps = ["mw", "mwss", "dh", "gl"]
     specs = [(int(rng.choice(Ls)), int(rng.integers(0, 4)), str(rng.choice(smps)))
              for _ in range(nmaps)]
-    flms = [oracle.signal.generate_flm_full_complex(rng, L, 0, sp) for L, sp, _ in specs]
+    flms = [seeded_flm(rng, L, sp) for L, sp, _ in specs]
     b = BatchedSHT(specs, precision="f32")
     b.load(flms)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
@@ -429,12 +439,10 @@ def run_healpix_iter(torch, nside=256, L=512, steps=5, warmup=2):
     """HEALPix nside=256, L=512, real signal: inverse + forward with 3 refinement iterations."""
     import s2fft_b200
 
-    import oracle
-
     dev = torch.device("cuda", torch.cuda.current_device())
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     rng = np.random.default_rng(7)
-    flm = torch.from_numpy(oracle.signal.generate_flm(rng, L, 0, 0, True)).to(dev)
+    flm = torch.from_numpy(seeded_flm(rng, L, 0, True)).to(dev)
     out = {"workload": f"healpix nside={nside} L={L} reality, forward iter=3"}
     for prec in ("f32", "f64"):
         x = flm.to(torch.complex64 if prec == "f32" else torch.complex128)
@@ -615,6 +623,14 @@ def main():
                          "peak_source": "measured FMA-chain probe (MEASURED_PEAKS.json has no "
                                         "FP32-SIMT figure)",
                          "flops_per_launch": FLOPS_PER_TRIPLE * r["T_fwd"],
+                         # the spin-0 forward runs on the equator-symmetric MWSS(2L) rings: one
+                         # recursion and one projection per ring pair (theta, pi - theta) serve
+                         # both rings (d(pi - theta) = (-1)^(l+m) d(theta)), so it executes
+                         # about half the algorithmic flops; frac above 1 comes from that
+                         "symmetric_ring_pairs": True,
+                         "executed_flops_per_launch": FLOPS_PER_TRIPLE * r["T_fwd_exec"],
+                         "executed_frac": FLOPS_PER_TRIPLE * r["T_fwd_exec"]
+                         / (lat_fwd_ms * 1e-3) / 1e12 / fp32_peak,
                          "launch_ms": lat_fwd_ms,
                          "inverse": {"achieved": ach_inv, "frac": ach_inv / fp32_peak,
                                      "launch_ms": lat_inv_ms}},

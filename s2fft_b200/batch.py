@@ -149,8 +149,9 @@ class BatchedSHT:
 
     # -- autotuner --------------------------------------------------------------------
     def tune(self, reps=3):
-        """Per group, time the launch shapes of the inverse (tile x segments along m) and the
-        forward (tile) latitudinal kernels on the group itself and keep the fastest."""
+        """Per group, time the launch shapes of the inverse and the forward latitudinal
+        kernels (tile x segments along m; forward segments apply to the equator-symmetric
+        forward) on the group itself and keep the fastest."""
         lib = _lib.lib()
         stream = torch.cuda.current_stream(self.device)
         h = ctypes.c_void_p(stream.cuda_stream)
@@ -184,11 +185,14 @@ class BatchedSHT:
             _lib.check(lib.s2b_plan_set_tuning(g.plan.ptr, 1, tile_inv))
             _lib.check(lib.s2b_plan_set_tuning(g.plan.ptr, 2, nseg))
             t = []
-            for v in (0, 1):
+            fwd = [(v, n) for v in (0, 1) for n in (2, 4)]  # (tile, segments along m)
+            for v, n in fwd:
                 _lib.check(lib.s2b_plan_set_tuning(g.plan.ptr, 0, v))
+                _lib.check(lib.s2b_plan_set_tuning(g.plan.ptr, 3, n))
                 t.append(timed(call_fwd))
-            tile_fwd = int(np.argmin(t))
+            tile_fwd, nseg_fwd = fwd[int(np.argmin(t))]
             _lib.check(lib.s2b_plan_set_tuning(g.plan.ptr, 0, tile_fwd))
+            _lib.check(lib.s2b_plan_set_tuning(g.plan.ptr, 3, nseg_fwd))
             g.tiles = (tile_fwd, tile_inv, nseg)
         torch.cuda.synchronize(self.device)
 

@@ -165,14 +165,15 @@ cudaError_t launch_fwd_start(bool fp64, const FwdStartParams& p, cudaStream_t s)
 // ---------------------------------------------------------------------------
 // Main kernel
 // ---------------------------------------------------------------------------
-template <typename Real, bool DUAL, int T, int W, int R>
+template <typename Real, bool DUAL, int T, int W, int R, bool SYM>
 struct Fwd2Layout {
   using Acc = std::conditional_t<DUAL, typename Vec<Real>::t4, typename Vec<Real>::t2>;
   static constexpr int NRT = W * T;  // rings per CTA
   static constexpr int NT = W * 32;
   // stage: h rows [2 blocks][R][32] | spectra rows [R][NRT] | lambda rows [R][NRT]
   static constexpr size_t h_bytes = 2 * R * kFwdBlock * sizeof(Real);
-  static constexpr size_t g_bytes = (size_t)R * NRT * sizeof(Acc);
+  static constexpr int GM = SYM ? 2 : 1;  // spectra per ring: G, or (E, O) of a ring pair
+  static constexpr size_t g_bytes = (size_t)R * NRT * GM * sizeof(Acc);
   static constexpr size_t l_bytes = (size_t)R * NRT * sizeof(Real);
   static constexpr size_t stage_bytes = h_bytes + g_bytes + l_bytes;
   // partial sums [R][W][2][32]
@@ -186,14 +187,14 @@ struct Fwd2Layout {
 // One recursion step over the T rings of one slot: cur = dt_m, prv = dt_{m+1} -> dt_{m-1};
 // a += dt_m G(theta_i, m) over the rings (float: measured faster than the paired form
 // below, which trades shared-memory loads for registers).
-template <typename Real, typename Acc, int T>
+template <typename Real, typename Acc, int T, int GS>
 __device__ __forceinline__ void fwd_slot_step(Real (&cur)[T], Real (&prv)[T], Real h,
                                               const Real* __restrict__ lrow,
                                               const Acc* __restrict__ grow, Acc& a) {
 #pragma unroll
   for (int i = 0; i < T; ++i) {
     const Real x = cur[i];
-    acc_fma(a, x, grow[i]);
+    acc_fma(a, x, grow[GS * i]);
     prv[i] = fma(lrow[i] * h, x, -prv[i]);
   }
 }
@@ -203,7 +204,7 @@ __device__ __forceinline__ void fwd_slot_step(Real (&cur)[T], Real (&prv)[T], Re
 // cur = dt_m, prv = dt_{m+1} -> dt_{m-1}; a_k += dt_m G(theta_i, m) over the rings. The
 // spectrum and lambda of a ring are loaded once for both slots (they do not depend on the
 // degree), lambda as 16-byte vectors.
-template <typename Real, typename Acc, int T, bool K0, bool K1>
+template <typename Real, typename Acc, int T, int GS, bool K0, bool K1>
 __device__ __forceinline__ void fwd_pair_step(Real (&c0)[T], Real (&p0)[T], Real (&c1)[T],
                                               Real (&p1)[T], Real h0, Real h1,
                                               const Real* __restrict__ lrow,
@@ -227,7 +228,7 @@ __device__ __forceinline__ void fwd_pair_step(Real (&c0)[T], Real (&p0)[T], Real
 #pragma unroll
     for (int j = 0; j < VL; ++j) {
       const int i = i0 + j;
-      const Acc g = grow[i];
+      const Acc g = grow[GS * i];
       if constexpr (K0) {
         const Real x = c0[i];
         acc_fma(a0, x, g);
@@ -242,10 +243,11 @@ __device__ __forceinline__ void fwd_pair_step(Real (&c0)[T], Real (&p0)[T], Real
   }
 }
 
-template <typename Real, bool DUAL, int T, int W, int R>
 // 3 CTAs per SM: the shared-memory footprint (two stages + partial sums) allows no more
+template <typename Real, bool DUAL, int T, int W, int R, bool SYM>
 __global__ void __launch_bounds__(W * 32, 3) lat_fwd2_kernel(const Fwd2Params p) {
-  using Lay = Fwd2Layout<Real, DUAL, T, W, R>;
+  using Lay = Fwd2Layout<Real, DUAL, T, W, R, SYM>;
+  constexpr int GM = Lay::GM;
   using Acc = typename Lay::Acc;
   using R2 = typename Vec<Real>::t2;
   constexpr int NRT = Lay::NRT;
@@ -270,11 +272,21 @@ __global__ void __launch_bounds__(W * 32, 3) lat_fwd2_kernel(const Fwd2Params p)
   const int ntiles = (p.nrings + NRT - 1) / NRT;
   const int mid = ntiles >> 1;
   const int t = (int)blockIdx.x;
-  const int tile = (t & 1) ? mid - 1 - (t >> 1) : mid + (t >> 1);
+  // (symmetric mode: the rings run from the pole to the equator, so the largest tiles last)
+  const int tile = SYM ? ntiles - 1 - t : ((t & 1) ? mid - 1 - (t >> 1) : mid + (t >> 1));
+  const int RS = p.tab_stride ? p.tab_stride : p.nrings;  // ring stride of the start tables
   const int r0 = tile * NRT;
-  const int kb0 = (int)blockIdx.y, kb1 = NB - 1 - (int)blockIdx.y;
+  // blockIdx.y = block pair + NB/2 * segment along m (boundaries of inv_mbound)
+  const int npair = NB / 2;
+  const int q = (int)blockIdx.y % npair, seg = (int)blockIdx.y / npair;
+  const int kb0 = q, kb1 = NB - 1 - q;
+  const int nseg = p.Mst1 ? p.nseg : 1;
+  const int gstep = kInvSegMax / nseg, g0 = seg * gstep;
   const int half = (int)(blockIdx.z % p.nhalf);
   const int b = (int)(blockIdx.z / p.nhalf);
+
+  const size_t nst = (size_t)p.nhalf * NB * RS;  // entries of one start table
+  const int* __restrict__ Mtab = g0 ? p.Mst1 + (size_t)(g0 - 1) * nst : p.Mst;
 
   // start m of every (slot, ring) of this warp: lane < 2T holds (k, i) = (lane / T, lane % T)
   int a_m[U];
@@ -286,7 +298,7 @@ __global__ void __launch_bounds__(W * 32, 3) lat_fwd2_kernel(const Fwd2Params p)
     if (e < 2 * T) {
       const int k = e / T, i = e % T;
       const int r = r0 + wp * T + i;
-      if (r < p.nrings) a_m[u] = p.Mst[((size_t)half * NB + (k ? kb1 : kb0)) * p.nrings + r];
+      if (r < p.nrings) a_m[u] = Mtab[((size_t)half * NB + (k ? kb1 : kb0)) * RS + r];
       act[(wp * 2 + k) * T + i] = a_m[u];
     }
     mt0 = max(mt0, __reduce_max_sync(0xffffffffu, (e < T) ? a_m[u] : -1));
@@ -312,14 +324,17 @@ __global__ void __launch_bounds__(W * 32, 3) lat_fwd2_kernel(const Fwd2Params p)
   __syncthreads();
   const int mc0 = mk[0], mc1 = mk[1];
   const int mtop = mc0 > mc1 ? mc0 : mc1;
-  if (mtop < 0) return;  // nothing significant in this tile (uniform)
-  const int ngroups = (mtop + 1) / R;
+  const int mbot = inv_mbound(L, NB, q, g0 + gstep);  // lowest m of the segment
+  if (mtop < mbot) return;  // nothing significant in this tile and segment (uniform)
+  const int ngroups = (mtop + 1 - mbot) / R;  // mtop = -1 mod 8, mbot = 0 mod 8
 
   const Real* __restrict__ Hb = reinterpret_cast<const Real*>(p.Hb);
   const Acc* __restrict__ Gin =
-      reinterpret_cast<const Acc*>(p.G) + ((size_t)b * p.nhalf + half) * TR * p.Gs;
+      reinterpret_cast<const Acc*>(p.G) + ((size_t)b * p.nhalf + half) * TR * p.Gs * GM;
   const Real* __restrict__ lamh = reinterpret_cast<const Real*>(p.lam) + (size_t)half * TR * p.Ls;
-  const R2* __restrict__ Vst = reinterpret_cast<const R2*>(p.Vst);
+  const R2* __restrict__ Vst =
+      g0 ? reinterpret_cast<const R2*>(p.Vst1) + (size_t)(g0 - 1) * nst * kFwdBlock
+         : reinterpret_cast<const R2*>(p.Vst);
   Acc* __restrict__ out = reinterpret_cast<Acc*>(p.acc) + ((size_t)b * p.nhalf + half) * L * Lp;
   int ncopy = p.Gs - r0;
   if (ncopy > NRT) ncopy = NRT;
@@ -330,7 +345,7 @@ __global__ void __launch_bounds__(W * 32, 3) lat_fwd2_kernel(const Fwd2Params p)
     unsigned char* st = stage_base + (size_t)(g & 1) * Lay::stage_bytes;
     const int row0 = mtop - g * R - R + 1 + kPadLo;
     constexpr unsigned hb = R * kFwdBlock * sizeof(Real);
-    const unsigned bytes = 2 * hb + (unsigned)(R * ncopy * sizeof(Acc)) +
+    const unsigned bytes = 2 * hb + (unsigned)(R * ncopy * GM * sizeof(Acc)) +
                            (unsigned)(R * nlam * sizeof(Real));
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     mbar_expect_tx(&mbar[g & 1], bytes);
@@ -339,8 +354,9 @@ __global__ void __launch_bounds__(W * 32, 3) lat_fwd2_kernel(const Fwd2Params p)
     unsigned char* gdst = st + Lay::h_bytes;
 #pragma unroll
     for (int s = 0; s < R; ++s)
-      bulk_g2s(gdst + (size_t)s * NRT * sizeof(Acc), Gin + (size_t)(row0 + s) * p.Gs + r0,
-               (unsigned)(ncopy * sizeof(Acc)), &mbar[g & 1]);
+      bulk_g2s(gdst + (size_t)s * NRT * GM * sizeof(Acc),
+               Gin + ((size_t)(row0 + s) * p.Gs + r0) * GM, (unsigned)(ncopy * GM * sizeof(Acc)),
+               &mbar[g & 1]);
     unsigned char* ldst = st + Lay::h_bytes + Lay::g_bytes;
 #pragma unroll
     for (int s = 0; s < R; ++s)
@@ -374,7 +390,7 @@ __global__ void __launch_bounds__(W * 32, 3) lat_fwd2_kernel(const Fwd2Params p)
 #pragma unroll
         for (int i = 0; i < T; ++i)
           if (act[(wp * 2 + k) * T + i] == mgrp) {
-            const R2 sv = Vst[(((size_t)half * NB + kb[k]) * p.nrings + r0 + wp * T + i) *
+            const R2 sv = Vst[(((size_t)half * NB + kb[k]) * RS + r0 + wp * T + i) *
                                   kFwdBlock + lane];
             v[k][i] = sv.x;
             w[k][i] = sv.y;
@@ -387,7 +403,7 @@ __global__ void __launch_bounds__(W * 32, 3) lat_fwd2_kernel(const Fwd2Params p)
     }
     const unsigned char* st = stage_base + (size_t)(grp & 1) * Lay::stage_bytes;
     const Real* hS = reinterpret_cast<const Real*>(st);
-    const Acc* gS = reinterpret_cast<const Acc*>(st + Lay::h_bytes) + wp * T;
+    const Acc* gS = reinterpret_cast<const Acc*>(st + Lay::h_bytes) + wp * T * GM;
     const Real* lS = reinterpret_cast<const Real*>(st + Lay::h_bytes + Lay::g_bytes) + wp * T;
 
 #define S2B_FWD2_STEP(CUR, PRV, S)                                                        \
@@ -396,24 +412,25 @@ __global__ void __launch_bounds__(W * 32, 3) lat_fwd2_kernel(const Fwd2Params p)
     const int m = mgrp - (S);                                                             \
     const bool k0 = m <= mtw[0], k1 = m <= mtw[1];                                        \
     const Real* lr = lS + srow * NRT;                                                     \
-    const Acc* gr = gS + srow * NRT;                                                      \
+    /* symmetric mode: E where l + m is even, O where odd (l = 32 block + lane) */        \
+    const Acc* gr = gS + srow * NRT * GM + (SYM ? ((lane + m) & 1) : 0);                  \
     Acc a0 = zero_acc<Acc>(), a1 = zero_acc<Acc>();                                       \
     if constexpr (sizeof(Real) == 8) {                                                    \
       const Real h0 = k0 ? hS[(0 * R + srow) * kFwdBlock + lane] : Real(0);               \
       const Real h1 = k1 ? hS[(1 * R + srow) * kFwdBlock + lane] : Real(0);               \
       /* an inactive slot's states are still zero, so both-slot steps serve k0 alone */   \
       if (k0)                                                                             \
-        fwd_pair_step<Real, Acc, T, true, true>(CUR[0], PRV[0], CUR[1], PRV[1], h0, h1,   \
+        fwd_pair_step<Real, Acc, T, GM, true, true>(CUR[0], PRV[0], CUR[1], PRV[1], h0, h1,   \
                                                 lr, gr, a0, a1);                          \
       else if (k1)                                                                        \
-        fwd_pair_step<Real, Acc, T, false, true>(CUR[0], PRV[0], CUR[1], PRV[1], h0, h1,  \
+        fwd_pair_step<Real, Acc, T, GM, false, true>(CUR[0], PRV[0], CUR[1], PRV[1], h0, h1,  \
                                                  lr, gr, a0, a1);                         \
     } else {                                                                              \
       if (k0)                                                                             \
-        fwd_slot_step<Real, Acc, T>(CUR[0], PRV[0], hS[(0 * R + srow) * kFwdBlock + lane], \
+        fwd_slot_step<Real, Acc, T, GM>(CUR[0], PRV[0], hS[(0 * R + srow) * kFwdBlock + lane], \
                                     lr, gr, a0);                                          \
       if (k1)                                                                             \
-        fwd_slot_step<Real, Acc, T>(CUR[1], PRV[1], hS[(1 * R + srow) * kFwdBlock + lane], \
+        fwd_slot_step<Real, Acc, T, GM>(CUR[1], PRV[1], hS[(1 * R + srow) * kFwdBlock + lane], \
                                     lr, gr, a1);                                          \
     }                                                                                     \
     /* the flush reads a slot's rows only where the slot is active somewhere in the CTA */ \
@@ -454,17 +471,23 @@ __global__ void __launch_bounds__(W * 32, 3) lat_fwd2_kernel(const Fwd2Params p)
   }
 }
 
-template <typename Real, bool DUAL, int T, int W, int R>
+template <typename Real, bool DUAL, int T, int W, int R, bool SYM>
 static cudaError_t launch_fwd2_cfg(const Fwd2Params& p, cudaStream_t s) {
-  using Lay = Fwd2Layout<Real, DUAL, T, W, R>;
-  auto kern = lat_fwd2_kernel<Real, DUAL, T, W, R>;
+  using Lay = Fwd2Layout<Real, DUAL, T, W, R, SYM>;
+  auto kern = lat_fwd2_kernel<Real, DUAL, T, W, R, SYM>;
   cudaError_t err =
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::total);
   if (err != cudaSuccess) return err;
   const int ntiles = (p.nrings + Lay::NRT - 1) / Lay::NRT;
-  dim3 grid(ntiles, p.NB / 2, p.nhalf * p.batch);
+  dim3 grid(ntiles, (p.NB / 2) * (p.Mst1 ? p.nseg : 1), p.nhalf * p.batch);
   kern<<<grid, Lay::NT, Lay::total, s>>>(p);
   return cudaGetLastError();
+}
+
+template <typename Real, int T, int R, bool SYM>
+static cudaError_t launch_fwd2_dual(bool dual, const Fwd2Params& p, cudaStream_t s) {
+  return dual ? launch_fwd2_cfg<Real, true, T, 4, R, SYM>(p, s)
+              : launch_fwd2_cfg<Real, false, T, 4, R, SYM>(p, s);
 }
 
 int fwd_group(bool fp64) {
@@ -472,21 +495,22 @@ int fwd_group(bool fp64) {
   return 8;  // start tables serve 8-step groups (and 4-step ones: 7 = 3 mod 4)
 }
 
+// float: 16 rings x 4 warps (measured at L=1024: 0.46 ms; 2 warps 0.52 ms, 15 rings
+// 0.52 ms), tile 1: 8 rings; double: 8 rings, tile 1: 4 rings
+template <bool SYM>
+static cudaError_t launch_fwd2_prec(bool fp64, bool dual, const Fwd2Params& p, cudaStream_t s) {
+  if (!fp64)
+    return p.tile == 1 ? launch_fwd2_dual<float, 8, 8, SYM>(dual, p, s)
+                       : launch_fwd2_dual<float, 16, 8, SYM>(dual, p, s);
+  return p.tile == 1 ? launch_fwd2_dual<double, 4, 4, SYM>(dual, p, s)
+                     : launch_fwd2_dual<double, 8, 4, SYM>(dual, p, s);
+}
+
 cudaError_t launch_fwd2(bool fp64, bool dual, const Fwd2Params& p, cudaStream_t s) {
   if (p.nrings <= 0) return cudaSuccess;
-  if (!fp64) {
-    if (p.tile == 1)
-      return dual ? launch_fwd2_cfg<float, true, 8, 4, 8>(p, s)
-                  : launch_fwd2_cfg<float, false, 8, 4, 8>(p, s);
-    // 16 rings x 4 warps (measured at L=1024: 0.46 ms; 2 warps 0.52 ms, 15 rings 0.52 ms)
-    return dual ? launch_fwd2_cfg<float, true, 16, 4, 8>(p, s)
-                : launch_fwd2_cfg<float, false, 16, 4, 8>(p, s);
-  }
-  if (p.tile == 1)
-    return dual ? launch_fwd2_cfg<double, true, 4, 4, 4>(p, s)
-                : launch_fwd2_cfg<double, false, 4, 4, 4>(p, s);
-  return dual ? launch_fwd2_cfg<double, true, 8, 4, 4>(p, s)
-              : launch_fwd2_cfg<double, false, 8, 4, 4>(p, s);
+  if (p.Mst1 && !(p.nseg == 1 || p.nseg == 2 || p.nseg == 4)) return cudaErrorInvalidValue;
+  return p.sym ? launch_fwd2_prec<true>(fp64, dual, p, s)
+               : launch_fwd2_prec<false>(fp64, dual, p, s);
 }
 
 }  // namespace s2b

@@ -393,6 +393,15 @@ struct s2b_plan {
   cudaEvent_t ev_end[2] = {nullptr, nullptr};
   // workspace layout (bytes)
   size_t ws_inv_F, ws_inv_ftm, ws_fwd_cols, ws_fwd_G, ws_fwd_acc, ws_iter_f, ws_iter_flm;
+  // equator-symmetric forward (spin 0, MW/MWSS): ring-pair spectra (E, O), Gs2 pairs per row
+  int fwd_sym = 0, Gs2 = 0;
+  size_t ws_fwd_G2 = 0;
+  // start and restart tables of the symmetric forward (the L northern rings and the equator)
+  int* sym_Mst = nullptr;
+  void* sym_Vst = nullptr;
+  int* sym_Mst1 = nullptr;
+  void* sym_Vst1 = nullptr;
+  int fwd_nseg = 1;  // segments along m of the forward kernel (1, 2, 4)
 };
 
 template <typename T>
@@ -582,6 +591,9 @@ static int build_plan(s2b_plan* p) {
     std::vector<double> w = transform_weights(L, d.sampling, d.nside);
     if (d.sampling == S2B_MW || d.sampling == S2B_MWSS) {
       p->fwd_mode = d.sampling == S2B_MW ? 1 : 2;
+      // the MWSS(2L) rings t and 2L - t mirror each other: spin 0 projects ring pairs
+      p->fwd_sym = d.spin == 0 ? 1 : 0;
+      p->Gs2 = round4(L);
       std::vector<double> th2 = thetas(2 * L, S2B_MWSS, 0);
       p->fwd_nrows = 2 * L + 1;
       p->fwd_pole_n = 2 * L - 1;  // rows 0..2L-2: rings t = 1..2L-1; then the two poles
@@ -634,6 +646,38 @@ static int build_plan(s2b_plan* p) {
     fp.Mst = p->fwd_Mst;
     fp.Vst = p->fwd_Vst;
     S2B_CK(launch_fwd_start(p->fp64, fp, 0));
+  }
+  // ---- start and restart tables of the symmetric forward: rings t = 1..L of the MWSS(2L) grid
+  if (p->fwd_sym) {
+    const size_t nst = (size_t)p->nhalf * p->fwd_NB * L;
+    const size_t vb = fwd_start_bytes(p->fp64, L, p->nhalf, L);
+    S2B_CK(cudaMalloc(&p->sym_Mst, kInvSegMax * nst * sizeof(int)));
+    p->allocs.push_back(p->sym_Mst);
+    S2B_CK(cudaMalloc(&p->sym_Vst, kInvSegMax * vb));
+    p->allocs.push_back(p->sym_Vst);
+    p->sym_Mst1 = p->sym_Mst + nst;
+    p->sym_Vst1 = static_cast<char*>(p->sym_Vst) + vb;
+    FwdStartParams fp{};
+    fp.L = L;
+    fp.L0 = d.L_lower;
+    fp.spin = d.spin;
+    fp.nhalf = p->nhalf;
+    fp.nrings = L;
+    fp.NB = p->fwd_NB;
+    fp.floor_log2 = p->fp64 ? -70.0 : -32.0;
+    fp.group = fwd_group(p->fp64);
+    fp.rings = p->fwd_rings;
+    fp.lbin = p->lbin;
+    fp.g = p->gtab;
+    fp.Mst = p->sym_Mst;
+    fp.Vst = p->sym_Vst;
+    fp.Mst1 = p->sym_Mst1;
+    fp.Vst1 = p->sym_Vst1;
+    S2B_CK(launch_fwd_start(p->fp64, fp, 0));
+    // launch shape measured at L = 256 ... 2048 (MW and MWSS, float and double): four
+    // segments along m; float takes 8 ring pairs per warp up to L = 512, 16 above
+    p->fwd_nseg = kInvSegMax;
+    p->tile_fwd = (!p->fp64 && L <= 512) ? 1 : 0;
   }
   // ---- start tables of the inverse rings (inverse kernel and adjoint of the inverse)
   if (p->inv_nrings > 0) {
@@ -780,6 +824,7 @@ static int build_plan(s2b_plan* p) {
   p->ws_fwd_cols = p->fwd_mode ? B * (size_t)ncm * p->nth * c2 : 0;
   p->ws_fwd_G = B * p->nhalf * (size_t)p->TR * p->Gs * acc;
   p->ws_fwd_acc = B * p->nhalf * (size_t)L * ((size_t)p->fwd_NB * kFwdBlock) * acc;
+  p->ws_fwd_G2 = p->fwd_sym ? B * p->nhalf * (size_t)p->TR * p->Gs2 * 2 * acc : 0;
   const size_t fel = d.reality ? p->rsz : c2;
   p->ws_iter_f = d.iter > 0 ? B * (size_t)p->npix * fel : 0;
   p->ws_iter_flm = d.iter > 0 ? B * (size_t)L * (2 * L - 1) * c2 : 0;
@@ -803,8 +848,12 @@ static size_t fwd_adj_ws(const s2b_plan* p) {
 static size_t pre_fwd_ws(const s2b_plan* p) {
   return align256(p->ws_fwd_cols) + align256(p->ws_pre_fwd);
 }
+static size_t fwd_once_ws(const s2b_plan* p) {
+  return align256(p->ws_fwd_cols) + align256(p->ws_fwd_G) + align256(p->ws_fwd_acc) +
+         align256(p->ws_fwd_G2);
+}
 static size_t fwd_ws(const s2b_plan* p) {
-  size_t once = align256(p->ws_fwd_cols) + align256(p->ws_fwd_G) + align256(p->ws_fwd_acc);
+  size_t once = fwd_once_ws(p);
   if (p->d.iter > 0)
     once = std::max(once, inv_ws(p)) + align256(p->ws_iter_f) + align256(p->ws_iter_flm);
   return once;
@@ -1183,6 +1232,7 @@ static int run_forward_once(s2b_plan* p, const void* f, void* flm, char* ws, cud
   char* cols = ws;
   char* G = cols + align256(p->ws_fwd_cols);
   char* acc = G + align256(p->ws_fwd_G);
+  char* G2 = acc + align256(p->ws_fwd_acc);
   S2B_CK(cudaMemsetAsync(acc, 0, p->ws_fwd_acc, s));
   RowsParams<Real> rp{};
   rp.L = L;
@@ -1231,6 +1281,8 @@ static int run_forward_once(s2b_plan* p, const void* f, void* flm, char* ws, cud
     cp.tb = tables<Real>(p);
     cp.in = cols;
     cp.out = G;
+    cp.out2 = p->fwd_sym ? G2 : nullptr;
+    cp.Gs2 = p->Gs2;
     const int ncm = p->fwd_mode == 1 ? 2 * L - 1 : 2 * L;
     S2B_CK(launch_mw_cols<Real>(cp, ncm, d.batch, p->M1, p->M2, s));
   }
@@ -1251,6 +1303,18 @@ static int run_forward_once(s2b_plan* p, const void* f, void* flm, char* ws, cud
   lp.status = p->status;
   lp.tile = p->tile_fwd;
   lp.mlo = lowm_orders(p);
+  if (p->fwd_sym) {
+    // ring pairs: the first L forward rings (t = 1..L) with their mirrors folded into G2
+    lp.sym = 1;
+    lp.nrings = L;
+    lp.Mst = p->sym_Mst;
+    lp.Vst = p->sym_Vst;
+    lp.Mst1 = p->sym_Mst1;
+    lp.Vst1 = p->sym_Vst1;
+    lp.nseg = p->fwd_nseg;
+    lp.G = G2;
+    lp.Gs = p->Gs2;
+  }
   if (p->ev_begin[1]) S2B_CK(cudaEventRecord(p->ev_begin[1], s));
   S2B_CK(launch_fwd2(p->fp64, p->dual, lp, s));
   if (p->ev_end[1]) S2B_CK(cudaEventRecord(p->ev_end[1], s));
@@ -1284,9 +1348,7 @@ static int run_forward(s2b_plan* p, const void* f, void* flm, char* ws, cudaStre
   int rc = run_forward_once<Real>(p, f, flm, ws, s);
   if (rc || d.iter <= 0) return rc;
   // Jacobi refinement: flm += F(f - I(flm))   (iterative_refinement.py:9-46)
-  const size_t scratch = std::max(align256(p->ws_fwd_cols) + align256(p->ws_fwd_G) +
-                                      align256(p->ws_fwd_acc),
-                                  inv_ws(p));
+  const size_t scratch = std::max(fwd_once_ws(p), inv_ws(p));
   char* fr = ws + scratch;
   char* dflm = fr + align256(p->ws_iter_f);
   const long nf = (long)d.batch * p->npix * (d.reality ? 1 : 2);
@@ -1789,17 +1851,19 @@ int s2b_plan_status(s2b_plan* p, int* status) {
 int s2b_plan_set_tuning(s2b_plan* p, int key, int value) {
   if (!p) return fail(S2B_ERR_INVALID, "plan must be non-NULL");
   const bool tile = (key == 0 && (value == 0 || value == 1)) || (key == 1 && value >= 0 && value <= 3);
-  const bool seg = key == 2 && (value == 1 || value == 2 || value == 4);
+  const bool seg = (key == 2 || key == 3) && (value == 1 || value == 2 || value == 4);
   if (!tile && !seg)
     return fail(S2B_ERR_INVALID,
-                "key 0 (forward tile) takes 0 or 1, key 1 (inverse tile) 0 to 3, key 2 (inverse "
-                "segments along m) 1, 2 or 4");
+                "key 0 (forward tile) takes 0 or 1, key 1 (inverse tile) 0 to 3, keys 2 and 3 "
+                "(inverse / forward segments along m) 1, 2 or 4");
   if (key == 0)
     p->tile_fwd = value;
   else if (key == 1)
     p->tile_inv = value;
-  else
+  else if (key == 2)
     p->inv_nseg = value;
+  else
+    p->fwd_nseg = value;
   for (s2b_plan* sp : p->subs) s2b_plan_set_tuning(sp, key, value);
   return S2B_OK;
 }

@@ -519,11 +519,68 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) mw_cols_kernel
     }
     return;
   }
-  for (int t = threadIdx.x; t < nout; t += blockDim.x) {
+  auto weighted = [&](int t) -> R2 {
     R2 u = dft_get<Real>(s2, d2, p.tb, true, t);
     const double f = p.scale * p.weights[t];
     u.x = (Real)((double)u.x * f);
     u.y = (Real)((double)u.y * f);
+    return u;
+  };
+  if (p.out2) {
+    // ring pairs (t, 2L - t) as (E, O), in the layout of out with a trailing pair axis
+    R2* o2 = reinterpret_cast<R2*>(p.out2);
+    const size_t mr = (size_t)(am + kPadLo);
+    const int per = p.dual ? 2 : 1;
+    const size_t rowbase =
+        p.dual ? ((size_t)b * p.TR + mr) * p.Gs2 : ((size_t)b * p.nhalf * p.TR + mr) * p.Gs2;
+    if (p.dual || m >= 0) {
+      for (int q = threadIdx.x; q < L; q += blockDim.x) {
+        const R2 un = weighted(q + 1);
+        R2 e = un, o = czero<R2>();
+        if (q < L - 1) {
+          const R2 us = weighted(2 * L - 1 - q);
+          e.x = un.x + us.x;
+          e.y = un.y + us.y;
+          o.x = un.x - us.x;
+          o.y = un.y - us.y;
+        }
+        o2[((rowbase + q) * 2 + 0) * per + (m < 0 ? 1 : 0)] = e;
+        o2[((rowbase + q) * 2 + 1) * per + (m < 0 ? 1 : 0)] = o;
+      }
+    }
+    // the pole rows stay in out (read by the epilogue)
+    if (threadIdx.x < 2) {
+      const int t = threadIdx.x == 0 ? 0 : 2 * L;
+      const int row = t == 0 ? 2 * L - 1 : 2 * L;
+      const R2 u = weighted(t);
+      if (p.dual)
+        out[(((size_t)b * p.TR + mr) * p.Gs + row) * 2 + (m < 0 ? 1 : 0)] = u;
+      else if (m >= 0)
+        out[(((size_t)b * p.nhalf + 0) * p.TR + mr) * p.Gs + row] = u;
+    }
+    if (m == 0) {
+      // zero pad rows (m outside [0, L)), pad pair columns (>= L) and, in the dual layout,
+      // the unused -m half of m = 0 (spin 0: one half)
+      const int rowlen = p.Gs2 * 2 * per;  // R2 entries per m row
+      R2* ob = o2 + (size_t)b * p.TR * rowlen;
+      for (int x = threadIdx.x; x < 2 * kPadLo * rowlen; x += blockDim.x) {
+        const int pr = x / rowlen;
+        const int mrow = pr < kPadLo ? pr : L + pr;
+        ob[(size_t)mrow * rowlen + x % rowlen] = czero<R2>();
+      }
+      const int padq = p.Gs2 - L;
+      for (int x = threadIdx.x; x < L * padq * 2 * per; x += blockDim.x) {
+        const int mrow = kPadLo + x / (padq * 2 * per);
+        ob[(size_t)mrow * rowlen + L * 2 * per + x % (padq * 2 * per)] = czero<R2>();
+      }
+      if (p.dual)
+        for (int x = threadIdx.x; x < L * 2; x += blockDim.x)
+          ob[(size_t)kPadLo * rowlen + x * 2 + 1] = czero<R2>();
+    }
+    return;
+  }
+  for (int t = threadIdx.x; t < nout; t += blockDim.x) {
+    const R2 u = weighted(t);
     const int row = t == 0 ? 2 * L - 1 : (t == 2 * L ? 2 * L : t - 1);  // poles after the recursed rings
     const size_t mr = (size_t)(am + kPadLo);
     if (p.dual) {

@@ -75,6 +75,11 @@ struct ColsParams {
   const void* in;       // Fc [B][ncm][nin]
   void* out;            // G  [B][half][m + kPadLo][Gs]; MWSS(2L) ring t -> row t-1,
                         // north pole -> row 2L-1, south pole -> row 2L
+  // equator-symmetric output (spin 0): when set, the recursed rings go to out2 as ring
+  // pairs q = 0..L-1 (rings t = q+1 and 2L-1-q) with (E, O) = G(t) +- G(2L-t) (the equator
+  // q = L-1: (G, 0)), [B][half][m + kPadLo][Gs2][2], and only the pole rows to out
+  void* out2;
+  int Gs2;
 };
 
 }  // namespace s2b

@@ -65,6 +65,17 @@ struct Fwd2Params {
   int* status;
   int tile;                 // 0: default rings per warp, 1: half of it (more CTAs)
   int mlo;                  // orders m < mlo are left to the degree recursion (lowm.cu)
+  // equator-symmetric mode (spin 0): the nrings rings are the northern members of ring
+  // pairs (theta, pi - theta) plus the equator, G holds per pair (E, O) = G(theta) +- G(pi -
+  // theta) (E = G, O = 0 for the equator) and Gs counts pairs; d^l_{m,0}(pi - theta) =
+  // (-1)^(l+m) d^l_{m,0}(theta), so degree l projects E where l + m is even, O where odd
+  int sym;
+  int tab_stride;           // ring stride of Mst / Vst (0: nrings)
+  // split along m as in the inverse kernel (inv_mbound): restart tables
+  // [kInvSegMax - 1][table] (nullptr: one segment) and the number of segments (1, 2, 4)
+  const int* Mst1;
+  const void* Vst1;
+  int nseg;
 };
 
 // Inverse latitudinal step, blocked layout (latinv.cu).
