@@ -120,19 +120,20 @@ __device__ __forceinline__ R2 root_rot(R2 w, int k, bool inv) {
 }
 
 template <int NS, bool DIF, typename R2>
-__device__ __forceinline__ void fft_pass(R2* s, int M, int q, const R2* __restrict__ tw, bool inv,
+__device__ __forceinline__ void fft_pass(R2* s, int M, int lq, const R2* __restrict__ tw, bool inv,
                                          const R2* __restrict__ post) {
   constexpr int NA = 1 << NS;
+  const int q = 1 << lq;        // q = 2^lq: group position and index by shifts and masks
   const int h = q << (NS - 1);  // largest span of the pass
-  const int s0 = M / (2 * h);
+  const int ls0 = __ffs(M) - 1 - lq - NS;  // log2(M / (2 h))
   for (int g = threadIdx.x; g < (M >> NS); g += blockDim.x) {
-    const int r = g % q;
-    const int base = (g / q) * (2 * h) + r;
+    const int r = g & (q - 1);
+    const int base = ((g >> lq) << (lq + NS)) + r;
     R2 x[NA];
 #pragma unroll
     for (int a = 0; a < NA; ++a) x[a] = s[pidx(base + a * q)];
     R2 bp[3];  // b, b^2, b^4
-    bp[0] = tw[r * s0];
+    bp[0] = tw[r << ls0];
     if (inv) bp[0].y = -bp[0].y;
     bp[1] = cmul(bp[0], bp[0]);
     bp[2] = cmul(bp[1], bp[1]);
@@ -177,15 +178,15 @@ __device__ void fft_dif(R2* s, int M, int logM, const R2* __restrict__ tw, bool 
                         const R2* __restrict__ post = nullptr) {
   for (int done = 0; done < logM;) {
     const int ns = logM - done < 3 ? logM - done : 3;
-    const int q = M >> (done + ns);  // span of the last fused stage
+    const int lq = logM - done - ns;  // log2 of the span of the last fused stage
     const R2* pp = done + ns == logM ? post : nullptr;
     __syncthreads();
     if (ns == 3)
-      fft_pass<3, true>(s, M, q, tw, inv, pp);
+      fft_pass<3, true>(s, M, lq, tw, inv, pp);
     else if (ns == 2)
-      fft_pass<2, true>(s, M, q, tw, inv, pp);
+      fft_pass<2, true>(s, M, lq, tw, inv, pp);
     else
-      fft_pass<1, true>(s, M, q, tw, inv, pp);
+      fft_pass<1, true>(s, M, lq, tw, inv, pp);
     done += ns;
   }
   __syncthreads();
@@ -196,14 +197,14 @@ template <typename R2>
 __device__ void fft_dit(R2* s, int M, int logM, const R2* __restrict__ tw, bool inv) {
   for (int done = 0; done < logM;) {
     const int ns = logM - done < 3 ? logM - done : 3;
-    const int q = 1 << done;  // span of the first fused stage
+    const int lq = done;  // log2 of the span of the first fused stage
     __syncthreads();
     if (ns == 3)
-      fft_pass<3, false>(s, M, q, tw, inv, (const R2*)nullptr);
+      fft_pass<3, false>(s, M, lq, tw, inv, (const R2*)nullptr);
     else if (ns == 2)
-      fft_pass<2, false>(s, M, q, tw, inv, (const R2*)nullptr);
+      fft_pass<2, false>(s, M, lq, tw, inv, (const R2*)nullptr);
     else
-      fft_pass<1, false>(s, M, q, tw, inv, (const R2*)nullptr);
+      fft_pass<1, false>(s, M, lq, tw, inv, (const R2*)nullptr);
     done += ns;
   }
   __syncthreads();
