@@ -394,7 +394,7 @@ struct s2b_plan {
   // workspace layout (bytes)
   size_t ws_inv_F, ws_inv_ftm, ws_fwd_cols, ws_fwd_G, ws_fwd_acc, ws_iter_f, ws_iter_flm;
   // equator-symmetric forward (spin 0, MW/MWSS): ring-pair spectra (E, O), Gs2 pairs per row
-  int fwd_sym = 0, Gs2 = 0;
+  int fwd_sym = 0, Gs2 = 0, sym_npair = 0;
   size_t ws_fwd_G2 = 0;
   // start and restart tables of the symmetric forward (the L northern rings and the equator)
   int* sym_Mst = nullptr;
@@ -593,6 +593,7 @@ static int build_plan(s2b_plan* p) {
       p->fwd_mode = d.sampling == S2B_MW ? 1 : 2;
       // the MWSS(2L) rings t and 2L - t mirror each other: spin 0 projects ring pairs
       p->fwd_sym = d.spin == 0 ? 1 : 0;
+      p->sym_npair = L;
       p->Gs2 = round4(L);
       std::vector<double> th2 = thetas(2 * L, S2B_MWSS, 0);
       p->fwd_nrows = 2 * L + 1;
@@ -610,6 +611,15 @@ static int build_plan(s2b_plan* p) {
       for (int t = 0; t < p->nth; ++t) {
         ri.push_back(ring_info(th[t]));
         rr.push_back(t);
+      }
+      // spin 0 on a ring set symmetric about the equator (GL, DH, HEALPix): ring pairs
+      bool symmetric = d.spin == 0 && p->nth >= 2;
+      for (int t = 0; symmetric && t < p->nth; ++t)
+        symmetric = std::fabs(th[t] + th[p->nth - 1 - t] - kPi) < 1e-12;
+      if (symmetric) {
+        p->fwd_sym = 1;
+        p->sym_npair = (p->nth + 1) / 2;
+        p->Gs2 = round4(p->sym_npair);
       }
     }
     p->fwd_nrings = (int)ri.size();
@@ -647,10 +657,10 @@ static int build_plan(s2b_plan* p) {
     fp.Vst = p->fwd_Vst;
     S2B_CK(launch_fwd_start(p->fp64, fp, 0));
   }
-  // ---- start and restart tables of the symmetric forward: rings t = 1..L of the MWSS(2L) grid
+  // ---- start and restart tables of the symmetric forward: the northern rings and the equator
   if (p->fwd_sym) {
-    const size_t nst = (size_t)p->nhalf * p->fwd_NB * L;
-    const size_t vb = fwd_start_bytes(p->fp64, L, p->nhalf, L);
+    const size_t nst = (size_t)p->nhalf * p->fwd_NB * p->sym_npair;
+    const size_t vb = fwd_start_bytes(p->fp64, L, p->nhalf, p->sym_npair);
     S2B_CK(cudaMalloc(&p->sym_Mst, kInvSegMax * nst * sizeof(int)));
     p->allocs.push_back(p->sym_Mst);
     S2B_CK(cudaMalloc(&p->sym_Vst, kInvSegMax * vb));
@@ -662,7 +672,7 @@ static int build_plan(s2b_plan* p) {
     fp.L0 = d.L_lower;
     fp.spin = d.spin;
     fp.nhalf = p->nhalf;
-    fp.nrings = L;
+    fp.nrings = p->sym_npair;
     fp.NB = p->fwd_NB;
     fp.floor_log2 = p->fp64 ? -70.0 : -32.0;
     fp.group = fwd_group(p->fp64);
@@ -1260,6 +1270,21 @@ static int run_forward_once(s2b_plan* p, const void* f, void* flm, char* ws, cud
     rp.weights = p->fwd_weights;
     rp.out = G;
     S2B_CK(launch_fwd_rows<Real>(rp, p->nth, d.batch, p->maxM, s));
+    if (p->fwd_sym) {
+      FoldParams fo{};
+      fo.L = L;
+      fo.nhalf = p->nhalf;
+      fo.dual = p->dual;
+      fo.TR = p->TR;
+      fo.Gs = p->Gs;
+      fo.Gs2 = p->Gs2;
+      fo.nrows = p->nth;
+      fo.npair = p->sym_npair;
+      fo.batch = d.batch;
+      fo.G = G;
+      fo.G2 = G2;
+      S2B_CK(launch_fold_pairs(p->fp64, fo, s));
+    }
   } else {
     rp.mode = FWD_TO_COLS;
     rp.out = cols;
@@ -1304,9 +1329,9 @@ static int run_forward_once(s2b_plan* p, const void* f, void* flm, char* ws, cud
   lp.tile = p->tile_fwd;
   lp.mlo = lowm_orders(p);
   if (p->fwd_sym) {
-    // ring pairs: the first L forward rings (t = 1..L) with their mirrors folded into G2
+    // ring pairs: the northern forward rings (and the equator) with their mirrors folded in
     lp.sym = 1;
-    lp.nrings = L;
+    lp.nrings = p->sym_npair;
     lp.Mst = p->sym_Mst;
     lp.Vst = p->sym_Vst;
     lp.Mst1 = p->sym_Mst1;

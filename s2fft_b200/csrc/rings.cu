@@ -761,6 +761,51 @@ cudaError_t launch_mw_cols_adj(const ColsParams<Real>& p, int ncm, int batch, in
   return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Ring-pair fold (equator-symmetric forward): one thread per (map, half, row, pair, component)
+// ---------------------------------------------------------------------------
+template <typename Real>
+__global__ void fold_pairs_kernel(FoldParams p) {
+  using R2 = typename C2<Real>::t;
+  const int per = p.dual ? 2 : 1;  // Real2 entries of one spectrum (dual: +m and -m)
+  const int halves = p.dual ? 1 : p.nhalf;
+  const long total = (long)p.batch * halves * p.TR * p.Gs2 * per;
+  const R2* G = reinterpret_cast<const R2*>(p.G);
+  R2* G2 = reinterpret_cast<R2*>(p.G2);
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
+       i += (long)gridDim.x * blockDim.x) {
+    const int c = (int)(i % per);
+    const int q = (int)((i / per) % p.Gs2);
+    const long row = i / ((long)per * p.Gs2);  // (b, half, m row)
+    const int mrow = (int)(row % p.TR);
+    R2 e = czero<R2>(), o = czero<R2>();
+    if (q < p.npair && mrow >= kPadLo && mrow < p.L + kPadLo) {
+      const int qm = p.nrows - 1 - q;  // mirror ring
+      const R2 a = G[(row * p.Gs + q) * per + c];
+      e = a;
+      if (qm != q) {
+        const R2 z = G[(row * p.Gs + qm) * per + c];
+        e = cadd(a, z);
+        o = csub(a, z);
+      }
+    }
+    G2[((row * p.Gs2 + q) * 2 + 0) * per + c] = e;
+    G2[((row * p.Gs2 + q) * 2 + 1) * per + c] = o;
+  }
+}
+
+cudaError_t launch_fold_pairs(bool fp64, const FoldParams& p, cudaStream_t s) {
+  const long total = (long)p.batch * (p.dual ? 1 : p.nhalf) * p.TR * p.Gs2 * (p.dual ? 2 : 1);
+  long blocks = (total + 255) / 256;
+  if (blocks > 65535L * 8) blocks = 65535L * 8;
+  if (blocks < 1) blocks = 1;
+  if (fp64)
+    fold_pairs_kernel<double><<<(unsigned)blocks, 256, 0, s>>>(p);
+  else
+    fold_pairs_kernel<float><<<(unsigned)blocks, 256, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
 template cudaError_t launch_mw_cols_adj<float>(const ColsParams<float>&, int, int, int, int, int,
                                                int, cudaStream_t);
 template cudaError_t launch_mw_cols_adj<double>(const ColsParams<double>&, int, int, int, int, int,

@@ -85,6 +85,17 @@ struct ColsParams {
 }  // namespace s2b
 
 namespace s2b {
+// Ring-pair fold of the forward spectra for the equator-symmetric forward (spin 0):
+// G [B][half][m + kPadLo][Gs] over nrows rings in theta order (ring t and nrows-1-t mirror
+// each other) -> G2 [B][half][m + kPadLo][Gs2][2] with (E, O) = G(q) +- G(nrows-1-q) for
+// q < npair = ceil(nrows / 2) (the middle ring of an odd count: (G, 0)); zero elsewhere.
+struct FoldParams {
+  int L, nhalf, dual, TR, Gs, Gs2, nrows, npair, batch;
+  const void* G;
+  void* G2;
+};
+cudaError_t launch_fold_pairs(bool fp64, const FoldParams& p, cudaStream_t s);
+
 template <typename Real>
 cudaError_t launch_inv_rows(const RowsParams<Real>& p, int nrings, int batch, int maxM,
                             cudaStream_t s);
