@@ -29,7 +29,7 @@
 
 namespace s2b {
 
-template <typename Real, bool DUAL, int T, int W, int R, bool VST>
+template <typename Real, bool DUAL, int T, int W, int R, bool VST, bool SYM>
 struct Inv2Layout {
   using Acc = std::conditional_t<DUAL, typename Vec<Real>::t4, typename Vec<Real>::t2>;
   static constexpr int K = 16;       // degrees per warp
@@ -40,7 +40,8 @@ struct Inv2Layout {
   static constexpr size_t f_bytes = 2 * R * kFwdBlock * sizeof(Acc);
   static constexpr size_t l_bytes = (size_t)R * NRT * sizeof(Real);
   static constexpr size_t stage_bytes = h_bytes + f_bytes + l_bytes;
-  static constexpr size_t buf_bytes = (size_t)R * W * NRT * sizeof(Acc);
+  static constexpr int NE = SYM ? 2 : 1;  // partial sums per lane slot: (E, O) of a ring pair
+  static constexpr size_t buf_bytes = (size_t)R * W * NRT * NE * sizeof(Acc);
   // start values of the CTA's states: [2 blocks][NRT rings][32] (d~_M, d~_{M+1})
   // (VST: staged by bulk copy; otherwise each lane reads its own from global memory, which
   // leaves room for one more CTA per SM)
@@ -50,9 +51,32 @@ struct Inv2Layout {
   static_assert(stage_bytes % 16 == 0 && buf_bytes % 16 == 0, "align");
 };
 
-template <typename Real, bool DUAL, int T, int W, int R, bool VST>
+// Adds a ring's partial spectrum for order m to its ftm row: column L-1+m+mo (half 0), and
+// L-1-m+mo for the second half or, in the dual layout, the -m components.
+template <bool DUAL, typename R2, typename Acc>
+__device__ __forceinline__ void inv2_store(R2* ftm, const Acc& s, int L, int m, int mo,
+                                           int half) {
+  R2 ap;
+  ap.x = s.x;
+  ap.y = s.y;
+  if constexpr (DUAL) {
+    R2 an;
+    an.x = s.z;
+    an.y = s.w;
+    red_add(ftm + (L - 1 + m + mo), ap);
+    if (m > 0) red_add(ftm + (L - 1 - m + mo), an);
+  } else {
+    if (half == 0)
+      red_add(ftm + (L - 1 + m + mo), ap);
+    else if (m > 0)
+      red_add(ftm + (L - 1 - m + mo), ap);
+  }
+}
+
+template <typename Real, bool DUAL, int T, int W, int R, bool VST, bool SYM>
 __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p) {
-  using Lay = Inv2Layout<Real, DUAL, T, W, R, VST>;
+  using Lay = Inv2Layout<Real, DUAL, T, W, R, VST, SYM>;
+  constexpr int NE = Lay::NE;
   using Acc = typename Lay::Acc;
   using R2 = typename Vec<Real>::t2;
   constexpr int K = Lay::K;
@@ -81,7 +105,8 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
   const int kb0 = q, kb1 = NB - 1 - q;
   const int nseg = p.Mst1 ? p.nseg : 1;
   const int gstep = kInvSegMax / nseg, g0 = seg * gstep;
-  const size_t nst = (size_t)p.nhalf * NB * p.nrings;
+  const int RS = p.tab_stride ? p.tab_stride : p.nrings;  // table stride = rings of the set
+  const size_t nst = (size_t)p.nhalf * NB * RS;
   const int* __restrict__ Mtab = g0 ? p.Mst1 + (size_t)(g0 - 1) * nst : p.Mst;
   const int mbot = inv_mbound(L, NB, q, g0 + gstep);  // lowest m of the segment
   const int half = (int)(blockIdx.z % p.nhalf);
@@ -100,7 +125,7 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
 #pragma unroll
     for (int i = 0; i < T; ++i) {
       const int r = r0 + lane * T + i;
-      Ms[x][i] = r < p.nrings ? Mtab[((size_t)half * NB + (x ? kb1 : kb0)) * p.nrings + r] : -1;
+      Ms[x][i] = r < p.nrings ? Mtab[((size_t)half * NB + (x ? kb1 : kb0)) * RS + r] : -1;
       mx = Ms[x][i] > mx ? Ms[x][i] : mx;
     }
     Mb[x] = __reduce_max_sync(0xffffffffu, mx);
@@ -168,7 +193,7 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
 #pragma unroll
       for (int x = 0; x < 2; ++x)
         bulk_g2s(const_cast<R2*>(vS) + (size_t)x * NRT * kFwdBlock,
-                 Vst + (((size_t)half * NB + (x ? kb1 : kb0)) * p.nrings + r0) * kFwdBlock, vb,
+                 Vst + (((size_t)half * NB + (x ? kb1 : kb0)) * RS + r0) * kFwdBlock, vb,
                  &mbar[2]);
     }
     issue(0);
@@ -194,7 +219,7 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
         if (Ms[x][i] == mgrp) {
           const R2* src =
               VST ? vS + ((size_t)x * NRT + lane * T + i) * kFwdBlock + col0
-                  : Vst + (((size_t)half * NB + (x ? kb1 : kb0)) * p.nrings + r0 + lane * T + i) *
+                  : Vst + (((size_t)half * NB + (x ? kb1 : kb0)) * RS + r0 + lane * T + i) *
                               kFwdBlock + col0;
 #pragma unroll
           for (int kk = 0; kk < K / 2; ++kk) {
@@ -214,7 +239,8 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
     const int m = mgrp - (S);                                                           \
     Real lam[T];                                                                        \
     _Pragma("unroll") for (int i = 0; i < T; ++i) lam[i] = lS[srow * NRT + i];          \
-    Acc a[2][T]; /* one partial sum per block: two independent FMA chains */            \
+    /* two independent FMA chains: one per block, or (symmetric) one per degree parity */ \
+    Acc a[2][T];                                                                        \
     _Pragma("unroll") for (int i = 0; i < T; ++i) {                                     \
       a[0][i] = zero_acc<Acc>();                                                        \
       a[1][i] = zero_acc<Acc>();                                                        \
@@ -227,15 +253,23 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
           const Real h = hS[so];                                                        \
           const Acc f = fS[so];                                                         \
           _Pragma("unroll") for (int i = 0; i < T; ++i) {                               \
-            acc_fma(a[x][i], CUR[k][i], f);                                             \
+            acc_fma(a[SYM ? (kk & 1) : x][i], CUR[k][i], f);                            \
             PRV[k][i] = fma(lam[i] * h, CUR[k][i], -PRV[k][i]);                         \
           }                                                                             \
         }                                                                               \
       }                                                                                 \
     }                                                                                   \
     _Pragma("unroll") for (int i = 0; i < T; ++i) {                                     \
-      acc_add(a[0][i], a[1][i]);                                                        \
-      buf[((S) * W + wp) * NRT + lane * T + i] = a[0][i];                               \
+      if constexpr (SYM) {                                                              \
+        /* l = 32 block + 8 warp + kk: l + m even for kk = m mod 2 */                   \
+        const int pe = m & 1;                                                           \
+        Acc* e = buf + (((S) * W + wp) * NRT + lane * T + i) * 2;                       \
+        e[0] = pe ? a[1][i] : a[0][i];                                                  \
+        e[1] = pe ? a[0][i] : a[1][i];                                                  \
+      } else {                                                                          \
+        acc_add(a[0][i], a[1][i]);                                                      \
+        buf[((S) * W + wp) * NRT + lane * T + i] = a[0][i];                             \
+      }                                                                                 \
     }                                                                                   \
   }
     S2B_INV2_STEP(v, w, 0)
@@ -264,35 +298,37 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
       const int m = mgrp - S;
       const int r = r0 + rr;
       if (m < p.mlo || m > lmax || r >= p.nrings) continue;
-      Acc s = buf[(S * W + 0) * NRT + rr];
+      Acc s = buf[((S * W + 0) * NRT + rr) * NE];
 #pragma unroll
-      for (int x = 1; x < W; ++x) acc_add(s, buf[(S * W + x) * NRT + rr]);
-      R2* ftm = reinterpret_cast<R2*>(p.ftm) + ((size_t)b * p.nrows + p.ring_row[r]) * p.ncol;
-      R2 ap;
-      ap.x = s.x;
-      ap.y = s.y;
-      if constexpr (DUAL) {
-        R2 an;
-        an.x = s.z;
-        an.y = s.w;
-        red_add(ftm + (L - 1 + m + p.mo), ap);
-        if (m > 0) red_add(ftm + (L - 1 - m + p.mo), an);
-      } else {
-        if (half == 0)
-          red_add(ftm + (L - 1 + m + p.mo), ap);
-        else if (m > 0)
-          red_add(ftm + (L - 1 - m + p.mo), ap);
+      for (int x = 1; x < W; ++x) acc_add(s, buf[((S * W + x) * NRT + rr) * NE]);
+      if constexpr (SYM) {
+        // ring r gets E + O, its mirror E - O (the equator, its own mirror, E + O once)
+        Acc o = buf[((S * W + 0) * NRT + rr) * NE + 1];
+#pragma unroll
+        for (int x = 1; x < W; ++x) acc_add(o, buf[((S * W + x) * NRT + rr) * NE + 1]);
+        const int rm = RS - 1 - r;
+        if (rm != r) {
+          Acc d = s;
+          acc_fma(d, Real(-1), o);
+          inv2_store<DUAL>(reinterpret_cast<R2*>(p.ftm) +
+                               ((size_t)b * p.nrows + p.ring_row[rm]) * p.ncol,
+                           d, L, m, p.mo, half);
+        }
+        acc_add(s, o);
       }
+      inv2_store<DUAL>(
+          reinterpret_cast<R2*>(p.ftm) + ((size_t)b * p.nrows + p.ring_row[r]) * p.ncol, s, L,
+          m, p.mo, half);
     }
     __syncthreads();
     if (tid == 0 && grp + 2 < ngroups) issue(grp + 2);
   }
 }
 
-template <typename Real, bool DUAL, int T, int R, bool VST>
+template <typename Real, bool DUAL, int T, int R, bool VST, bool SYM>
 static cudaError_t launch_inv2_cfg(const Inv2Params& p, cudaStream_t s) {
-  using Lay = Inv2Layout<Real, DUAL, T, 4, R, VST>;
-  auto kern = lat_inv2_kernel<Real, DUAL, T, 4, R, VST>;
+  using Lay = Inv2Layout<Real, DUAL, T, 4, R, VST, SYM>;
+  auto kern = lat_inv2_kernel<Real, DUAL, T, 4, R, VST, SYM>;
   cudaError_t err =
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::total);
   if (err != cudaSuccess) return err;
@@ -302,28 +338,34 @@ static cudaError_t launch_inv2_cfg(const Inv2Params& p, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-template <typename Real, int T, bool VST>
+template <typename Real, int T, bool VST, bool SYM>
 static cudaError_t launch_inv2_dual(bool dual, const Inv2Params& p, cudaStream_t s) {
-  return dual ? launch_inv2_cfg<Real, true, T, 8, VST>(p, s)
-              : launch_inv2_cfg<Real, false, T, 8, VST>(p, s);
+  return dual ? launch_inv2_cfg<Real, true, T, 8, VST, SYM>(p, s)
+              : launch_inv2_cfg<Real, false, T, 8, VST, SYM>(p, s);
+}
+
+// tile bit 0: one ring per lane (float; double always has one); bit 1: start values read
+// from global memory instead of staged in shared memory. 8-step groups (the start tables'
+// alignment).
+template <bool SYM>
+static cudaError_t launch_inv2_prec(bool fp64, bool dual, const Inv2Params& p, cudaStream_t s) {
+  const bool vst = (p.tile & 2) == 0;
+  if (!fp64) {
+    if (p.tile & 1)
+      return vst ? launch_inv2_dual<float, 1, true, SYM>(dual, p, s)
+                 : launch_inv2_dual<float, 1, false, SYM>(dual, p, s);
+    return vst ? launch_inv2_dual<float, 2, true, SYM>(dual, p, s)
+               : launch_inv2_dual<float, 2, false, SYM>(dual, p, s);
+  }
+  return vst ? launch_inv2_dual<double, 1, true, SYM>(dual, p, s)
+             : launch_inv2_dual<double, 1, false, SYM>(dual, p, s);
 }
 
 cudaError_t launch_inv2(bool fp64, bool dual, const Inv2Params& p, cudaStream_t s) {
   if (p.nrings <= 0) return cudaSuccess;
   if (p.Mst1 && !(p.nseg == 1 || p.nseg == 2 || p.nseg == 4)) return cudaErrorInvalidValue;
-  // tile bit 0: one ring per lane (float; double always has one); bit 1: start values read
-  // from global memory instead of staged in shared memory. 8-step groups (the start tables'
-  // alignment).
-  const bool vst = (p.tile & 2) == 0;
-  if (!fp64) {
-    if (p.tile & 1)
-      return vst ? launch_inv2_dual<float, 1, true>(dual, p, s)
-                 : launch_inv2_dual<float, 1, false>(dual, p, s);
-    return vst ? launch_inv2_dual<float, 2, true>(dual, p, s)
-               : launch_inv2_dual<float, 2, false>(dual, p, s);
-  }
-  return vst ? launch_inv2_dual<double, 1, true>(dual, p, s)
-             : launch_inv2_dual<double, 1, false>(dual, p, s);
+  return p.sym ? launch_inv2_prec<true>(fp64, dual, p, s)
+               : launch_inv2_prec<false>(fp64, dual, p, s);
 }
 
 }  // namespace s2b

@@ -370,6 +370,8 @@ struct s2b_plan {
   int* inv_Mst1 = nullptr;  // restart tables of the inverse kernel's m-split
   void* inv_Vst1 = nullptr;
   int inv_nseg = 1;         // segments along m of the inverse kernel (1, 2, 4)
+  // equator-symmetric inverse (spin 0, rings symmetric about the equator): ring pairs
+  int inv_sym = 0, inv_npair = 0;
   int* adj_col = nullptr;
   int adj_Gs = 4, adj_pole_s = -1, adj_pole_n = -1;
   void* col_ph_adj = nullptr;
@@ -566,6 +568,15 @@ static int build_plan(s2b_plan* p) {
       rr.push_back(t);
     }
     p->inv_nrings = (int)ri.size();
+    // spin 0 on a recursed ring set symmetric about the equator (MWSS inner rings, GL, DH,
+    // HEALPix; not MW): ring r and inv_nrings - 1 - r share one recursion
+    {
+      bool symmetric = d.spin == 0 && p->inv_nrings >= 2;
+      for (int r = 0; symmetric && r < p->inv_nrings; ++r)
+        symmetric = std::fabs(th[rr[r]] + th[rr[p->inv_nrings - 1 - r]] - kPi) < 1e-12;
+      p->inv_sym = symmetric ? 1 : 0;
+      p->inv_npair = (p->inv_nrings + 1) / 2;
+    }
     p->inv_ncol = (d.sampling == S2B_MWSS || d.sampling == S2B_HEALPIX) ? 2 * L : 2 * L - 1;
     p->inv_mo = (d.sampling == S2B_MWSS || d.sampling == S2B_HEALPIX) ? 1 : 0;
     if ((rc = upload(p, &p->inv_rings, ri))) return rc;
@@ -706,6 +717,9 @@ static int build_plan(s2b_plan* p) {
     // for 3 CTAs per SM), two rings per lane in float from L = 1024 and one below
     p->inv_nseg = kInvSegMax;
     p->tile_inv = (!p->fp64 && L >= 1024) ? 2 : 3;
+    // symmetric inverse: one ring pair per lane (two would double the partial sums in
+    // shared memory and drop to 2 CTAs per SM; measured slower at L = 256 ... 2048)
+    if (p->inv_sym) p->tile_inv = 3;
     FwdStartParams fp{};
     fp.L = L;
     fp.L0 = d.L_lower;
@@ -982,6 +996,11 @@ static int run_inverse(s2b_plan* p, const void* flm, void* f, char* ws, cudaStre
     lp.Mst1 = p->inv_Mst1;
     lp.Vst1 = p->inv_Vst1;
     lp.nseg = p->inv_nseg;
+    if (p->inv_sym) {
+      lp.sym = 1;
+      lp.nrings = p->inv_npair;
+      lp.tab_stride = p->inv_nrings;
+    }
     lp.Hb = p->fwd_Hb;
     lp.lam = p->inv_lam;
     lp.Ls = p->inv_Ls;

@@ -86,6 +86,11 @@ struct Inv2Params {
   const int* Mst1;          // restart tables of the m-split (nullptr: one segment)
   const void* Vst1;
   int nseg;                 // segments along m: 1, 2 or 4 (with Mst1)
+  // equator-symmetric mode (spin 0): the nrings rings are the northern members of ring
+  // pairs (ring q and tab_stride - 1 - q) plus the equator; a lane sums the degrees with
+  // l + m even (E) and odd (O) apart and adds E + O to ring q and E - O to its mirror
+  int sym;
+  int tab_stride;           // ring stride of the start tables and ring count (0: nrings)
   const void* Hb;           // [NB][tab_rows][32]
   const void* lam;          // [nhalf][tab_rows][Ls]
   int Ls;
