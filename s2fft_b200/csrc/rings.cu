@@ -123,9 +123,8 @@ template <int NS, bool DIF, typename R2>
 __device__ __forceinline__ void fft_pass(R2* s, int M, int lq, const R2* __restrict__ tw, bool inv,
                                          const R2* __restrict__ post) {
   constexpr int NA = 1 << NS;
-  const int q = 1 << lq;        // q = 2^lq: group position and index by shifts and masks
-  const int h = q << (NS - 1);  // largest span of the pass
-  const int ls0 = __ffs(M) - 1 - lq - NS;  // log2(M / (2 h))
+  const int q = 1 << lq;  // q = 2^lq: group position and index by shifts and masks
+  const int ls0 = __ffs(M) - 1 - lq - NS;  // log2(M / (2 h)), h = q 2^(NS-1) the largest span
   for (int g = threadIdx.x; g < (M >> NS); g += blockDim.x) {
     const int r = g & (q - 1);
     const int base = ((g >> lq) << (lq + NS)) + r;
