@@ -165,9 +165,11 @@ cudaError_t launch_fwd_start(bool fp64, const FwdStartParams& p, cudaStream_t s)
 // ---------------------------------------------------------------------------
 // Main kernel
 // ---------------------------------------------------------------------------
-template <typename Real, bool DUAL, int T, int W, int R, bool SYM>
+// SYM: 0 one recursion per ring; 1 spin-0 ring pairs; 2 spin != 0 ring pairs (cross: the
+// partial sums carry this half's projection and the other half's mirrored one)
+template <typename Real, bool DUAL, int T, int W, int R, int SYM>
 struct Fwd2Layout {
-  using Acc = std::conditional_t<DUAL, typename Vec<Real>::t4, typename Vec<Real>::t2>;
+  using Acc = std::conditional_t<DUAL || SYM == 2, typename Vec<Real>::t4, typename Vec<Real>::t2>;
   static constexpr int NRT = W * T;  // rings per CTA
   static constexpr int NT = W * 32;
   // stage: h rows [2 blocks][R][32] | spectra rows [R][NRT] | lambda rows [R][NRT]
@@ -244,7 +246,7 @@ __device__ __forceinline__ void fwd_pair_step(Real (&c0)[T], Real (&p0)[T], Real
 }
 
 // 3 CTAs per SM: the shared-memory footprint (two stages + partial sums) allows no more
-template <typename Real, bool DUAL, int T, int W, int R, bool SYM>
+template <typename Real, bool DUAL, int T, int W, int R, int SYM>
 __global__ void __launch_bounds__(W * 32, 3) lat_fwd2_kernel(const Fwd2Params p) {
   using Lay = Fwd2Layout<Real, DUAL, T, W, R, SYM>;
   constexpr int GM = Lay::GM;
@@ -464,14 +466,27 @@ __global__ void __launch_bounds__(W * 32, 3) lat_fwd2_kernel(const Fwd2Params p)
       Acc s = buf[((S * W + 0) * 2 + k) * kFwdBlock + ln];
 #pragma unroll
       for (int x = 1; x < W; ++x) acc_add(s, buf[((S * W + x) * 2 + k) * kFwdBlock + ln]);
-      red_add(out + (size_t)m * Lp + l, s);
+      if constexpr (SYM == 2) {
+        // this half's projection and the other half's mirrored one
+        using R2o = typename Vec<Real>::t2;
+        R2o own, oth;
+        own.x = s.x;
+        own.y = s.y;
+        oth.x = s.z;
+        oth.y = s.w;
+        R2o* o2 = reinterpret_cast<R2o*>(p.acc);
+        red_add(o2 + (((size_t)b * p.nhalf + half) * L + m) * Lp + l, own);
+        red_add(o2 + (((size_t)b * p.nhalf + (1 - half)) * L + m) * Lp + l, oth);
+      } else {
+        red_add(out + (size_t)m * Lp + l, s);
+      }
     }
     __syncthreads();
     if (tid == 0 && grp + 2 < ngroups) issue(grp + 2);
   }
 }
 
-template <typename Real, bool DUAL, int T, int W, int R, bool SYM>
+template <typename Real, bool DUAL, int T, int W, int R, int SYM>
 static cudaError_t launch_fwd2_cfg(const Fwd2Params& p, cudaStream_t s) {
   using Lay = Fwd2Layout<Real, DUAL, T, W, R, SYM>;
   auto kern = lat_fwd2_kernel<Real, DUAL, T, W, R, SYM>;
@@ -484,10 +499,15 @@ static cudaError_t launch_fwd2_cfg(const Fwd2Params& p, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-template <typename Real, int T, int R, bool SYM>
+template <typename Real, int T, int R, int SYM>
 static cudaError_t launch_fwd2_dual(bool dual, const Fwd2Params& p, cudaStream_t s) {
-  return dual ? launch_fwd2_cfg<Real, true, T, 4, R, SYM>(p, s)
-              : launch_fwd2_cfg<Real, false, T, 4, R, SYM>(p, s);
+  if constexpr (SYM == 2) {  // spin != 0: never the dual layout
+    if (dual) return cudaErrorInvalidValue;
+    return launch_fwd2_cfg<Real, false, T, 4, R, 2>(p, s);
+  } else {
+    return dual ? launch_fwd2_cfg<Real, true, T, 4, R, SYM>(p, s)
+                : launch_fwd2_cfg<Real, false, T, 4, R, SYM>(p, s);
+  }
 }
 
 int fwd_group(bool fp64) {
@@ -497,7 +517,7 @@ int fwd_group(bool fp64) {
 
 // float: 16 rings x 4 warps (measured at L=1024: 0.46 ms; 2 warps 0.52 ms, 15 rings
 // 0.52 ms), tile 1: 8 rings; double: 8 rings, tile 1: 4 rings
-template <bool SYM>
+template <int SYM>
 static cudaError_t launch_fwd2_prec(bool fp64, bool dual, const Fwd2Params& p, cudaStream_t s) {
   if (!fp64)
     return p.tile == 1 ? launch_fwd2_dual<float, 8, 8, SYM>(dual, p, s)
@@ -509,8 +529,8 @@ static cudaError_t launch_fwd2_prec(bool fp64, bool dual, const Fwd2Params& p, c
 cudaError_t launch_fwd2(bool fp64, bool dual, const Fwd2Params& p, cudaStream_t s) {
   if (p.nrings <= 0) return cudaSuccess;
   if (p.Mst1 && !(p.nseg == 1 || p.nseg == 2 || p.nseg == 4)) return cudaErrorInvalidValue;
-  return p.sym ? launch_fwd2_prec<true>(fp64, dual, p, s)
-               : launch_fwd2_prec<false>(fp64, dual, p, s);
+  if (p.sym && p.cross) return launch_fwd2_prec<2>(fp64, dual, p, s);
+  return p.sym ? launch_fwd2_prec<1>(fp64, dual, p, s) : launch_fwd2_prec<0>(fp64, dual, p, s);
 }
 
 }  // namespace s2b

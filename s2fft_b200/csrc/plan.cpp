@@ -397,6 +397,7 @@ struct s2b_plan {
   size_t ws_inv_F, ws_inv_ftm, ws_fwd_cols, ws_fwd_G, ws_fwd_acc, ws_iter_f, ws_iter_flm;
   // equator-symmetric forward (spin 0, MW/MWSS): ring-pair spectra (E, O), Gs2 pairs per row
   int fwd_sym = 0, Gs2 = 0, sym_npair = 0;
+  int fwd_cross = 0;  // spin != 0: ring pairs serve both halves (fold of G into G2)
   size_t ws_fwd_G2 = 0;
   // start and restart tables of the symmetric forward (the L northern rings and the equator)
   int* sym_Mst = nullptr;
@@ -603,7 +604,8 @@ static int build_plan(s2b_plan* p) {
     if (d.sampling == S2B_MW || d.sampling == S2B_MWSS) {
       p->fwd_mode = d.sampling == S2B_MW ? 1 : 2;
       // the MWSS(2L) rings t and 2L - t mirror each other: spin 0 projects ring pairs
-      p->fwd_sym = d.spin == 0 ? 1 : 0;
+      p->fwd_sym = 1;
+      p->fwd_cross = d.spin != 0 ? 1 : 0;
       p->sym_npair = L;
       p->Gs2 = round4(L);
       std::vector<double> th2 = thetas(2 * L, S2B_MWSS, 0);
@@ -624,11 +626,12 @@ static int build_plan(s2b_plan* p) {
         rr.push_back(t);
       }
       // spin 0 on a ring set symmetric about the equator (GL, DH, HEALPix): ring pairs
-      bool symmetric = d.spin == 0 && p->nth >= 2;
+      bool symmetric = p->nth >= 2;
       for (int t = 0; symmetric && t < p->nth; ++t)
         symmetric = std::fabs(th[t] + th[p->nth - 1 - t] - kPi) < 1e-12;
       if (symmetric) {
         p->fwd_sym = 1;
+        p->fwd_cross = d.spin != 0 ? 1 : 0;
         p->sym_npair = (p->nth + 1) / 2;
         p->Gs2 = round4(p->sym_npair);
       }
@@ -695,10 +698,11 @@ static int build_plan(s2b_plan* p) {
     fp.Mst1 = p->sym_Mst1;
     fp.Vst1 = p->sym_Vst1;
     S2B_CK(launch_fwd_start(p->fp64, fp, 0));
-    // launch shape measured at L = 256 ... 2048 (MW and MWSS, float and double): four
-    // segments along m; float takes 8 ring pairs per warp up to L = 512, 16 above
+    // launch shape measured at L = 256 ... 2048 (MW, MWSS, GL, DH, float and double): four
+    // segments along m; spin-0 float takes 8 ring pairs per warp up to L = 512, 16 above
+    // (spin != 0: 16 throughout)
     p->fwd_nseg = kInvSegMax;
-    p->tile_fwd = (!p->fp64 && L <= 512) ? 1 : 0;
+    p->tile_fwd = (!p->fp64 && L <= 512 && !p->fwd_cross) ? 1 : 0;
   }
   // ---- start tables of the inverse rings (inverse kernel and adjoint of the inverse)
   if (p->inv_nrings > 0) {
@@ -848,7 +852,10 @@ static int build_plan(s2b_plan* p) {
   p->ws_fwd_cols = p->fwd_mode ? B * (size_t)ncm * p->nth * c2 : 0;
   p->ws_fwd_G = B * p->nhalf * (size_t)p->TR * p->Gs * acc;
   p->ws_fwd_acc = B * p->nhalf * (size_t)L * ((size_t)p->fwd_NB * kFwdBlock) * acc;
-  p->ws_fwd_G2 = p->fwd_sym ? B * p->nhalf * (size_t)p->TR * p->Gs2 * 2 * acc : 0;
+  // (E, O) per pair: Real4 in the dual and the cross layouts, Real2 otherwise
+  p->ws_fwd_G2 = p->fwd_sym ? B * p->nhalf * (size_t)p->TR * p->Gs2 * 2 *
+                                  (p->fwd_cross ? 2 * c2 : acc)
+                            : 0;
   const size_t fel = d.reality ? p->rsz : c2;
   p->ws_iter_f = d.iter > 0 ? B * (size_t)p->npix * fel : 0;
   p->ws_iter_flm = d.iter > 0 ? B * (size_t)L * (2 * L - 1) * c2 : 0;
@@ -1300,6 +1307,7 @@ static int run_forward_once(s2b_plan* p, const void* f, void* flm, char* ws, cud
       fo.nrows = p->nth;
       fo.npair = p->sym_npair;
       fo.batch = d.batch;
+      fo.cross = p->fwd_cross;
       fo.G = G;
       fo.G2 = G2;
       S2B_CK(launch_fold_pairs(p->fp64, fo, s));
@@ -1325,10 +1333,25 @@ static int run_forward_once(s2b_plan* p, const void* f, void* flm, char* ws, cud
     cp.tb = tables<Real>(p);
     cp.in = cols;
     cp.out = G;
-    cp.out2 = p->fwd_sym ? G2 : nullptr;
+    cp.out2 = (p->fwd_sym && !p->fwd_cross) ? G2 : nullptr;
     cp.Gs2 = p->Gs2;
     const int ncm = p->fwd_mode == 1 ? 2 * L - 1 : 2 * L;
     S2B_CK(launch_mw_cols<Real>(cp, ncm, d.batch, p->M1, p->M2, s));
+    if (p->fwd_cross) {
+      FoldParams fo{};
+      fo.L = L;
+      fo.nhalf = p->nhalf;
+      fo.TR = p->TR;
+      fo.Gs = p->Gs;
+      fo.Gs2 = p->Gs2;
+      fo.nrows = p->fwd_nrings;  // rows 0..2L-2: the recursed MWSS(2L) rings in theta order
+      fo.npair = p->sym_npair;
+      fo.batch = d.batch;
+      fo.cross = 1;
+      fo.G = G;
+      fo.G2 = G2;
+      S2B_CK(launch_fold_pairs(p->fp64, fo, s));
+    }
   }
   Fwd2Params lp{};
   lp.L = L;
@@ -1347,9 +1370,11 @@ static int run_forward_once(s2b_plan* p, const void* f, void* flm, char* ws, cud
   lp.status = p->status;
   lp.tile = p->tile_fwd;
   lp.mlo = lowm_orders(p);
+  const Fwd2Params lp_all = lp;  // every ring and G: the low orders (lowm.cu) run on these
   if (p->fwd_sym) {
     // ring pairs: the northern forward rings (and the equator) with their mirrors folded in
     lp.sym = 1;
+    lp.cross = p->fwd_cross;
     lp.nrings = p->sym_npair;
     lp.Mst = p->sym_Mst;
     lp.Vst = p->sym_Vst;
@@ -1362,7 +1387,7 @@ static int run_forward_once(s2b_plan* p, const void* f, void* flm, char* ws, cud
   if (p->ev_begin[1]) S2B_CK(cudaEventRecord(p->ev_begin[1], s));
   S2B_CK(launch_fwd2(p->fp64, p->dual, lp, s));
   if (p->ev_end[1]) S2B_CK(cudaEventRecord(p->ev_end[1], s));
-  if (int rc_ = run_lowm_project(p, lp, p->fwd_rings, s)) return rc_;
+  if (int rc_ = run_lowm_project(p, lp_all, p->fwd_rings, s)) return rc_;
   StageParams sp{};
   sp.L = L;
   sp.L0 = d.L_lower;

@@ -793,7 +793,46 @@ __global__ void fold_pairs_kernel(FoldParams p) {
   }
 }
 
+// cross mode: one thread per (map, half, row, pair)
+template <typename Real>
+__global__ void fold_cross_kernel(FoldParams p) {
+  using R2 = typename C2<Real>::t;
+  const long total = (long)p.batch * 2 * p.TR * p.Gs2;
+  const R2* G = reinterpret_cast<const R2*>(p.G);
+  R2* G2 = reinterpret_cast<R2*>(p.G2);
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
+       i += (long)gridDim.x * blockDim.x) {
+    const int q = (int)(i % p.Gs2);
+    const long row = i / p.Gs2;  // (b, half, m row)
+    const int mrow = (int)(row % p.TR);
+    const int half = (int)((row / p.TR) % 2);
+    const long orow = row + (half ? -1L : 1L) * p.TR;  // the other half, same map and m
+    R2 a = czero<R2>(), z = czero<R2>();
+    if (q < p.npair && mrow >= kPadLo && mrow < p.L + kPadLo) {
+      const int qm = p.nrows - 1 - q;
+      a = G[row * p.Gs + q];
+      if (qm != q) z = G[orow * p.Gs + qm];
+    }
+    R2* e = G2 + (row * p.Gs2 + q) * 4;  // two Real4 = four Real2
+    e[0] = a;
+    e[1] = z;
+    e[2] = a;
+    e[3] = cscale(z, Real(-1));
+  }
+}
+
 cudaError_t launch_fold_pairs(bool fp64, const FoldParams& p, cudaStream_t s) {
+  if (p.cross) {
+    const long total = (long)p.batch * 2 * p.TR * p.Gs2;
+    long blocks = (total + 255) / 256;
+    if (blocks > 65535L * 8) blocks = 65535L * 8;
+    if (blocks < 1) blocks = 1;
+    if (fp64)
+      fold_cross_kernel<double><<<(unsigned)blocks, 256, 0, s>>>(p);
+    else
+      fold_cross_kernel<float><<<(unsigned)blocks, 256, 0, s>>>(p);
+    return cudaGetLastError();
+  }
   const long total = (long)p.batch * (p.dual ? 1 : p.nhalf) * p.TR * p.Gs2 * (p.dual ? 2 : 1);
   long blocks = (total + 255) / 256;
   if (blocks > 65535L * 8) blocks = 65535L * 8;

@@ -89,8 +89,12 @@ namespace s2b {
 // G [B][half][m + kPadLo][Gs] over nrows rings in theta order (ring t and nrows-1-t mirror
 // each other) -> G2 [B][half][m + kPadLo][Gs2][2] with (E, O) = G(q) +- G(nrows-1-q) for
 // q < npair = ceil(nrows / 2) (the middle ring of an odd count: (G, 0)); zero elsewhere.
+// Cross mode (spin != 0, two halves, one Real2 per spectrum): G2 [B][half][m + kPadLo][Gs2][2]
+// of Real4 {G_h(q), +-G_{1-h}(nrows-1-q)}, + for the first entry (l + m even), - for the
+// second; the middle ring's second component is 0 (the other half counts it itself).
 struct FoldParams {
   int L, nhalf, dual, TR, Gs, Gs2, nrows, npair, batch;
+  int cross;
   const void* G;
   void* G2;
 };

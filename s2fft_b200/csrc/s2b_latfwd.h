@@ -70,6 +70,10 @@ struct Fwd2Params {
   // theta) (E = G, O = 0 for the equator) and Gs counts pairs; d^l_{m,0}(pi - theta) =
   // (-1)^(l+m) d^l_{m,0}(theta), so degree l projects E where l + m is even, O where odd
   int sym;
+  // with sym, spin != 0: d^l_{m,n}(pi - theta) = (-1)^(l+m) d^l_{m,-n}(theta), so this half's
+  // recursion also serves the other half's mirrored ring: G holds per pair and parity the
+  // Real4 {G_h(theta), +-G_{1-h}(pi - theta)} and both halves' sums are updated
+  int cross;
   int tab_stride;           // ring stride of Mst / Vst (0: nrings)
   // split along m as in the inverse kernel (inv_mbound): restart tables
   // [kInvSegMax - 1][table] (nullptr: one segment) and the number of segments (1, 2, 4)
