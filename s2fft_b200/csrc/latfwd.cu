@@ -96,11 +96,20 @@ __global__ void fwd_start_kernel(const FwdStartParams p) {
   int M = __reduce_max_sync(0xffffffffu, ms);
   if (M >= 0) M |= p.group - 1;
 
-  // pass 3: (dt_X, dt_{X+1}) of this degree for a start X >= 0
+  // pass 3: (dt_X, dt_{X+1}) of this degree at the start X = M and, for the inverse kernel's
+  // m-split, at the restarts X = b - 1 of the boundaries b <= M; the points are requested in
+  // decreasing order, so one walk down from m = l serves them all (starts at or above l
+  // take the exact continuation above m = l)
+  int E3 = 0, mc = l;
+  double v3 = 0.0, w3 = 0.0;
+  if (valid) {
+    E3 = (int)floor(lg);
+    v3 = sgn * exp2(lg - (double)E3);
+  }
   auto start_pair = [&](int X, double& cur, double& prv) {
     cur = 0.0;
     prv = 0.0;
-    if (!valid) return;
+    if (!valid || X < 0) return;
     if (X >= l) {
       const double dl = sgn * exp2(lg);
       const int dlt = X - l;
@@ -108,23 +117,24 @@ __global__ void fwd_start_kernel(const FwdStartParams p) {
         cur = ((dlt >> 1) & 1) ? -dl : dl;
       else
         prv = (((dlt + 1) >> 1) & 1) ? -dl : dl;
-    } else {
-      int E = (int)floor(lg);
-      double v = sgn * exp2(lg - (double)E), w = 0.0;
-      for (int m = l; m > X; --m) step(v, w, E, m);
-      cur = ldexp(v, E);
-      prv = ldexp(w, E);
+      return;
     }
+    while (mc > X) {
+      step(v3, w3, E3, mc);
+      --mc;
+    }
+    cur = ldexp(v3, E3);
+    prv = ldexp(w3, E3);
   };
   double cur = 0.0, prv = 0.0;
-  if (M >= 0) start_pair(M, cur, prv);
+  start_pair(M, cur, prv);
   R2 o;
   o.x = (Real)cur;
   o.y = (Real)prv;
   reinterpret_cast<R2*>(p.Vst)[wid * kFwdBlock + lane] = o;
   if (lane == 0) p.Mst[wid] = M;
   if (p.Mst1) {
-    // restart tables of the inverse kernel's m-split, one per inner boundary
+    // restart tables of the m-split, one per inner boundary (boundaries decrease with k)
     const int q = blk < p.NB - 1 - blk ? blk : p.NB - 1 - blk;
     const size_t nst = (size_t)p.nhalf * p.NB * p.nrings;
     for (int k = 1; k < kInvSegMax; ++k) {
@@ -133,9 +143,7 @@ __global__ void fwd_start_kernel(const FwdStartParams p) {
       double ck = cur, pk = prv;
       if (M >= bk) {
         Mk = bk > 0 ? bk - 1 : -1;
-        ck = 0.0;
-        pk = 0.0;
-        if (Mk >= 0) start_pair(Mk, ck, pk);
+        start_pair(Mk, ck, pk);
       }
       R2 ok;
       ok.x = (Real)ck;

@@ -146,23 +146,6 @@ static std::vector<double> thetas(int L, int sampling, int nside) {
 }
 
 // exact DFT helper on the host (used only at plan time for small tables)
-static std::vector<cd> dft_exact(const std::vector<cd>& x) {
-  const int n = (int)x.size();
-  std::vector<cd> tw(n);
-  for (int k = 0; k < n; ++k) tw[k] = cd(std::cos(-2.0 * kPi * k / n), std::sin(-2.0 * kPi * k / n));
-  std::vector<cd> X(n);
-  for (int j = 0; j < n; ++j) {
-    cd s = 0;
-    long idx = 0;
-    for (int k = 0; k < n; ++k) {
-      s += x[k] * tw[idx];
-      idx += j;
-      if (idx >= n) idx -= n;
-    }
-    X[j] = s;
-  }
-  return X;
-}
 
 static cd mw_weight(int m) {
   if (m == 1) return cd(0, kPi / 2);
@@ -170,6 +153,8 @@ static cd mw_weight(int m) {
   if (m % 2 == 0) return cd(2.0 / (1.0 - (double)m * m), 0);
   return 0;
 }
+
+static std::vector<cd> dft_host(std::vector<cd> x);
 
 // transform weights (quadrature.py:7-50); MW/MWSS use the MWSS grid at 2L
 static std::vector<double> transform_weights(int L, int sampling, int nside) {
@@ -182,7 +167,7 @@ static std::vector<double> transform_weights(int L, int sampling, int nside) {
     const int n = 2 * Lp;
     std::vector<cd> ws(n);
     for (int k = 0; k < n; ++k) ws[k] = w[(k + n / 2) % n];
-    std::vector<cd> W = dft_exact(ws);
+    std::vector<cd> W = dft_host(ws);
     std::vector<double> wr(n);
     for (int k = 0; k < n; ++k) wr[k] = W[k].real() / n;
     q.assign(wr.begin(), wr.begin() + Lp + 1);
@@ -240,6 +225,35 @@ static void fft_pow2_host(std::vector<cd>& a) {
         a[i + k + len / 2] = u - v;
       }
   }
+}
+
+// DFT X_j = sum_k x_k exp(-2 pi i jk / n) of any length in O(n log n): the power-of-two FFT
+// directly, other lengths by Bluestein's chirp-z convolution (chirp angles reduced modulo
+// 2n, so the error stays at the level of the FFTs).
+static std::vector<cd> dft_host(std::vector<cd> x) {
+  const int n = (int)x.size();
+  if (n <= 1) return x;
+  if ((n & (n - 1)) == 0) {
+    fft_pow2_host(x);
+    return x;
+  }
+  int M = 1;
+  while (M < 2 * n - 1) M <<= 1;
+  std::vector<cd> c(n), a(M, 0.0), bf(M, 0.0);
+  for (int k = 0; k < n; ++k) {
+    const long kk = ((long)k * k) % (2L * n);
+    c[k] = cd(std::cos(kPi * kk / n), -std::sin(kPi * kk / n));  // exp(-i pi k^2 / n)
+    a[k] = x[k] * c[k];
+    bf[k] = std::conj(c[k]);
+    if (k > 0) bf[M - k] = std::conj(c[k]);
+  }
+  fft_pow2_host(a);
+  fft_pow2_host(bf);
+  for (int k = 0; k < M; ++k) a[k] = std::conj(a[k] * bf[k]);  // inverse FFT by conjugation
+  fft_pow2_host(a);
+  std::vector<cd> X(n);
+  for (int k = 0; k < n; ++k) X[k] = c[k] * std::conj(a[k]) / (double)M;
+  return X;
 }
 
 static int ilog2(int x) {
