@@ -603,12 +603,13 @@ def main():
     lat_inv_ms, lat_fwd_ms = r["lat32"]
     ach_fwd = FLOPS_PER_TRIPLE * r["T_fwd"] / (lat_fwd_ms * 1e-3) / 1e12
     ach_inv = FLOPS_PER_TRIPLE * r["T_inv"] / (lat_inv_ms * 1e-3) / 1e12
-    traffic = None
+    traffic = {"inverse": None, "forward": None}
     tpath = os.path.join(ROOT, "profiles", "latitudinal_traffic.txt")
     if os.path.exists(tpath):
         for ln in open(tpath):
-            if ln.startswith(f"L={args.L} forward_f32 bytes_per_launch="):
-                traffic = float(ln.split("=")[-1])
+            for k in traffic:
+                if ln.startswith(f"L={args.L} {k}_f32 bytes_per_launch="):
+                    traffic[k] = float(ln.split("=")[-1])
     line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms32"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -617,24 +618,32 @@ def main():
             "roundtrip_rel_err_f64": r["err64"],
             "fp64_path": {"value": r["value64"], "unit": UNIT,
                           "speedup_mixed_over_fp64": r["value"] / r["value64"]},
-            "roofline": {"bound": "fp32", "kernel": "latitudinal forward (recursion+projection)",
-                         "achieved": ach_fwd, "peak": fp32_peak, "unit": "TFLOP/s",
-                         "frac": ach_fwd / fp32_peak, "traffic": traffic,
+            # the dominant kernel of the step: the inverse latitudinal (recursion + synthesis);
+            # the forward one is reported beside it
+            "roofline": {"bound": "fp32", "kernel": "latitudinal inverse (recursion+synthesis)",
+                         "achieved": ach_inv, "peak": fp32_peak, "unit": "TFLOP/s",
+                         "frac": ach_inv / fp32_peak, "traffic": traffic["inverse"],
                          "peak_source": "measured FMA-chain probe (MEASURED_PEAKS.json has no "
                                         "FP32-SIMT figure)",
-                         "flops_per_launch": FLOPS_PER_TRIPLE * r["T_fwd"],
-                         # the spin-0 forward runs on the equator-symmetric MWSS(2L) rings: one
-                         # recursion and one projection per ring pair (theta, pi - theta) serve
-                         # both rings (d(pi - theta) = (-1)^(l+m) d(theta)), so it executes
-                         # about half the algorithmic flops; frac above 1 comes from that
-                         "symmetric_ring_pairs": True,
-                         "executed_flops_per_launch": FLOPS_PER_TRIPLE * r["T_fwd_exec"],
-                         "executed_frac": FLOPS_PER_TRIPLE * r["T_fwd_exec"]
-                         / (lat_fwd_ms * 1e-3) / 1e12 / fp32_peak,
-                         "launch_ms": lat_fwd_ms,
-                         "inverse": {"achieved": ach_inv, "frac": ach_inv / fp32_peak,
-                                     "launch_ms": lat_inv_ms}},
-            "fp64_roofline": {"achieved": FLOPS_PER_TRIPLE * r["T_fwd"] / (r["lat64"][1] * 1e-3)
+                         "flops_per_launch": FLOPS_PER_TRIPLE * r["T_inv"],
+                         "launch_ms": lat_inv_ms,
+                         "forward": {
+                             "kernel": "latitudinal forward (recursion+projection)",
+                             "achieved": ach_fwd, "frac": ach_fwd / fp32_peak,
+                             "traffic": traffic["forward"],
+                             "flops_per_launch": FLOPS_PER_TRIPLE * r["T_fwd"],
+                             "launch_ms": lat_fwd_ms,
+                             # the spin-0 forward runs on the equator-symmetric MWSS(2L) rings:
+                             # one recursion and one projection per ring pair (theta, pi -
+                             # theta) serve both rings (d(pi - theta) = (-1)^(l+m) d(theta)),
+                             # so it executes about half the algorithmic flops; its frac above
+                             # 1 comes from that
+                             "symmetric_ring_pairs": True,
+                             "executed_flops_per_launch": FLOPS_PER_TRIPLE * r["T_fwd_exec"],
+                             "executed_frac": FLOPS_PER_TRIPLE * r["T_fwd_exec"]
+                             / (lat_fwd_ms * 1e-3) / 1e12 / fp32_peak}},
+            "fp64_roofline": {"kernel": "latitudinal inverse",
+                              "achieved": FLOPS_PER_TRIPLE * r["T_inv"] / (r["lat64"][0] * 1e-3)
                               / 1e12, "peak": fp64_peak, "unit": "TFLOP/s"},
             "hbm_peak_gbs": peaks.get("hbm_gbs"), "peaks_source": kind,
             "clocks": r["clocks"],
