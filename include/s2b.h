@@ -204,6 +204,26 @@ int s2b_plan_set_events(s2b_plan* plan, int forward, void* ev_begin, void* ev_en
 #define S2B_NOALLOC_SCRATCH_BYTES ((size_t)32 << 20)
 int s2b_inverse_noalloc(s2b_plan* plan, const void* flm, void* f, void* stream);
 
+/* Rotation of spherical-harmonic coefficients by the Euler angles (alpha, beta, gamma):
+ *   flm'[l, m] = exp(-i m alpha) sum_n d^l_{m,n}(beta) exp(-i n gamma) flm[l, n],
+ * replaces s2fft.utils.rotation.rotate_flms (s2fft/utils/rotation.py:9-64). flm and out
+ * are [batch][L][2L-1] complex (double for precision S2B_F64, float for S2B_F32); the
+ * arithmetic is double in both. dl == NULL: the Wigner-d planes at beta are generated
+ * on the device by Risbo's recursion (upstream s2fft/recursions/risbo.py:4-120);
+ * otherwise dl holds them in the layout of upstream's generate_rotate_dls,
+ * [L][2L-1][2L-1] float64 with d^l_{m,n} at [l][L-1+m][L-1+n]. The workspace
+ * (s2b_rotate_workspace_size(L) bytes, caller-owned) holds two planes and the phase
+ * tables. Stream-ordered; no allocation. */
+size_t s2b_rotate_workspace_size(int L);
+int s2b_rotate_flms(int L, int batch, int precision, double alpha, double beta, double gamma,
+                    const void* flm, void* out, const double* dl, void* ws, size_t ws_bytes,
+                    void* stream);
+
+/* The planes d^l_{m,n}(beta), 0 <= l < L, in the layout of upstream's
+ * generate_rotate_dls (s2fft/utils/rotation.py:75-96): dl[l][L-1+m][L-1+n] float64,
+ * zero where |m| > l or |n| > l (the call clears dl first). */
+int s2b_rotate_dls(int L, double beta, double* dl, void* ws, size_t ws_bytes, void* stream);
+
 /* Peak-rate probe: a fused multiply-add chain kernel (float when fp64 == 0,
  * double otherwise) over `blocks` CTAs of 256 threads, `iters` iterations of 8
  * independent FMA chains per thread, writing one value per thread to `out`

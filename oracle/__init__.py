@@ -3,7 +3,8 @@
 TEST INFRASTRUCTURE ONLY. This package is a float64 numpy restatement of the
 upstream s2fft algorithm for the transform path (sampling geometry, quadrature,
 resampling, HEALPix ring FFTs, the Price-McEwen latitudinal recursion, the
-spherical and Wigner front-ends and the precompute-kernel transforms). Each
+spherical and Wigner front-ends, the precompute-kernel transforms and the rotation of
+coefficients). Each
 function cites the upstream file:line it follows.
 
 It is imported only by ``tests/``, by ``__graft_entry__.smoke()`` and by the
@@ -22,6 +23,7 @@ from . import (  # noqa: F401
     quadrature,
     recursion,
     resampling,
+    rotation,
     samples,
     signal,
     spherical,

@@ -59,6 +59,11 @@ _SIGS = {
     "s2b_plan_set_tuning": [ctypes.c_void_p, ctypes.c_int, ctypes.c_int],
     "s2b_inverse_adjoint": [ctypes.c_void_p] * 4 + [ctypes.c_size_t, ctypes.c_void_p],
     "s2b_forward_adjoint": [ctypes.c_void_p] * 4 + [ctypes.c_size_t, ctypes.c_void_p],
+    "s2b_rotate_flms": [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                        ctypes.c_double, ctypes.c_double] + [ctypes.c_void_p] * 4
+                       + [ctypes.c_size_t, ctypes.c_void_p],
+    "s2b_rotate_dls": [ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
+                       ctypes.c_size_t, ctypes.c_void_p],
 }
 
 
@@ -77,6 +82,8 @@ def lib():
                 fn.restype = ctypes.c_int
             handle.s2b_last_error.argtypes = []
             handle.s2b_last_error.restype = ctypes.c_char_p
+            handle.s2b_rotate_workspace_size.argtypes = [ctypes.c_int]
+            handle.s2b_rotate_workspace_size.restype = ctypes.c_size_t
             _lib = handle
     return _lib
 

@@ -99,3 +99,20 @@ def test_signal_generator(golden):
                                   data["gen/flmn_L6_N3"])
     np.testing.assert_array_equal(oracle.signal.generate_flmn(r2, 6, 3, 0, True),
                                   data["gen/flmn_L6_N3_real"])
+
+
+def test_rotation_matches_upstream_risbo():
+    """oracle.rotation against upstream's own Risbo recursion and rotate_flms contraction
+    (tests/golden/make_rotation.py)."""
+    import os
+
+    from tests.conftest import GOLDEN_DIR
+
+    d = np.load(os.path.join(GOLDEN_DIR, "rotation.npz"))
+    for k in range(3):
+        L = int(d[f"r{k}/L"])
+        rot = tuple(d[f"r{k}/rotation"])
+        dl = oracle.rotation.generate_rotate_dls(L, rot[1])
+        assert np.abs(dl - d[f"r{k}/dls"]).max() < 1e-13
+        r = oracle.rotation.rotate_flms(d[f"r{k}/flm"], L, rot)
+        assert np.abs(r - d[f"r{k}/rotated"]).max() < 1e-13 * np.abs(d[f"r{k}/rotated"]).max()
