@@ -18,6 +18,7 @@ golden vectors produced by the upstream numpy code itself
 """
 
 from . import (  # noqa: F401
+    fourier_wigner,
     healpix,
     precompute,
     quadrature,

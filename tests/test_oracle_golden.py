@@ -116,3 +116,61 @@ def test_rotation_matches_upstream_risbo():
         assert np.abs(dl - d[f"r{k}/dls"]).max() < 1e-13
         r = oracle.rotation.rotate_flms(d[f"r{k}/flm"], L, rot)
         assert np.abs(r - d[f"r{k}/rotated"]).max() < 1e-13 * np.abs(d[f"r{k}/rotated"]).max()
+
+
+def _fw_golden():
+    import json
+    import os
+
+    from tests.conftest import GOLDEN_DIR
+
+    d = np.load(os.path.join(GOLDEN_DIR, "fourier_wigner.npz"))
+    with open(os.path.join(GOLDEN_DIR, "fourier_wigner.json")) as fh:
+        return d, json.load(fh)["cases"]
+
+
+def test_fourier_wigner_matches_upstream():
+    """oracle.fourier_wigner against upstream's numpy Fourier-Wigner transforms and
+    fourier_wigner_kernel (tests/golden/make_fourier_wigner.py), atol 1e-12 as upstream's
+    tests/test_fourier_wigner.py."""
+    fw = oracle.fourier_wigner
+    d, cases = _fw_golden()
+    for L in (8, 16):
+        delta, quads = fw.fourier_wigner_kernel(L)
+        assert np.abs(delta - d[f"kernel_L{L}/delta"]).max() < 1e-13
+        assert np.abs(quads - d[f"kernel_L{L}/quads"]).max() < 1e-13
+    seen = 0
+    for c in cases:
+        if c["kind"] != "fourier_wigner":
+            continue
+        n, L, N, s, r = c["name"], c["L"], c["N"], c["sampling"], c["reality"]
+        f = fw.inverse_transform(d[f"{n}/flmn"], L, N, None, r, s)
+        np.testing.assert_allclose(f, d[f"{n}/f"], atol=1e-12)
+        g = fw.forward_transform(d[f"{n}/f"], L, N, None, r, s)
+        np.testing.assert_allclose(g, d[f"{n}/flmn_fwd"], atol=1e-12)
+        # the forward inverts the inverse on band-limited inputs
+        np.testing.assert_allclose(d[f"{n}/flmn_fwd"], d[f"{n}/flmn"], atol=1e-12)
+        seen += 1
+    assert seen == 10
+
+
+def test_spin_subset_ops_match_upstream():
+    """wigner_subset_to_s2 / s2_to_wigner_subset / so3_to_wigner_subset against upstream
+    custom_ops (batch 2, channels 3, mixed spins)."""
+    fw = oracle.fourier_wigner
+    d, cases = _fw_golden()
+    for c in cases:
+        if c["kind"] != "subset_ops":
+            continue
+        n, L, N, s, sp = c["name"], c["L"], c["N"], c["sampling"], np.array(c["spins"])
+        DW = fw.fourier_wigner_kernel(L)
+        np.testing.assert_allclose(fw.wigner_subset_to_s2(d[f"{n}/flmn"], sp, DW, L, s),
+                                   d[f"{n}/fs"], atol=1e-12)
+        np.testing.assert_allclose(fw.s2_to_wigner_subset(d[f"{n}/fs"], sp, DW, L, s),
+                                   d[f"{n}/back"], atol=1e-12)
+        np.testing.assert_allclose(fw.so3_to_wigner_subset(d[f"{n}/fso3"], sp, DW, L, N, s),
+                                   d[f"{n}/sub"], atol=1e-12)
+    with pytest.raises(ValueError):
+        fw.wigner_subset_to_s2(d["ops0/flmn"], np.array([0, 1]), DW, 8, "mw")
+    with pytest.raises(ValueError):
+        fw.inverse_transform(d["fw0/flmn"], 8, 2, None, False, "gl")
