@@ -224,6 +224,59 @@ int s2b_rotate_flms(int L, int batch, int precision, double alpha, double beta, 
  * zero where |m| > l or |n| > l (the call clears dl first). */
 int s2b_rotate_dls(int L, double beta, double* dl, void* ws, size_t ws_bytes, void* stream);
 
+/* Fourier-Wigner transforms on SO(3) and the spin-subset lifting ops (mw / mwss only).
+ * A plan holds the FFT tables of one (L, sampling, precision); it is independent of N,
+ * of the batch and of the spin subset. Layouts (complex interleaved, double for S2B_F64,
+ * float for S2B_F32):
+ *   flmn  [batch][2N-1][L][2L-1]            f [batch][2N-1][ntheta][nphi] (real if reality)
+ *   spin-subset coefficients [batch][nspins][L][2L-1], maps [batch][nspins][ntheta][nphi],
+ *   SO(3) signals for s2b_fw_so3_to_subset [batch][ngamma][ntheta][nphi].
+ * delta = [L][2L-1][2L-1] float64 planes Delta^l_{a,b} = d^l_{a,b}(pi/2) (upstream layout,
+ * e.g. from s2b_rotate_dls(L, pi/2, ...)); quads = [4L-3] complex128 upsampled quadrature
+ * weights (s2b_fw_quads). Spins satisfy |spin| <= L-1 (slice n = -spin; a slice with |n|
+ * > L-1 comes out zero). Pointers 16-byte aligned, workspace 256-byte aligned, of
+ * s2b_fw_workspace_size bytes for the operation (enum s2b_fw_op). Stream-ordered; no
+ * allocation or synchronisation outside plan creation.
+ * Replace upstream:
+ *   s2b_fw_plan_create / s2b_fw_quads
+ *            <- s2fft/precompute_transforms/construct.py:614-639 (fourier_wigner_kernel)
+ *   s2b_fw_inverse  <- s2fft/precompute_transforms/fourier_wigner.py:13-88
+ *   s2b_fw_forward  <- s2fft/precompute_transforms/fourier_wigner.py:177-333
+ *   s2b_fw_subset_to_s2  <- s2fft/precompute_transforms/custom_ops.py:5-83
+ *   s2b_fw_s2_to_subset  <- s2fft/precompute_transforms/custom_ops.py:251-333
+ *   s2b_fw_so3_to_subset <- s2fft/precompute_transforms/custom_ops.py:168-205 */
+typedef struct s2b_fw_plan s2b_fw_plan;
+enum s2b_fw_op {
+  S2B_FW_INVERSE = 0,
+  S2B_FW_FORWARD = 1,
+  S2B_FW_SUBSET_TO_S2 = 2,
+  S2B_FW_S2_TO_SUBSET = 3,
+  S2B_FW_SO3_TO_SUBSET = 4
+};
+int s2b_fw_plan_create(int L, int sampling, int precision, s2b_fw_plan** plan);
+int s2b_fw_plan_destroy(s2b_fw_plan* plan);
+int s2b_fw_quads(s2b_fw_plan* plan, void* quads, void* stream);
+/* N and reality are used by the full transforms, nspins by the subset ops. */
+size_t s2b_fw_workspace_size(const s2b_fw_plan* plan, int op, int batch, int N, int reality,
+                             int nspins);
+int s2b_fw_inverse(s2b_fw_plan* plan, int batch, int N, int reality, const double* delta,
+                   const void* flmn, void* f, void* workspace, size_t workspace_bytes,
+                   void* stream);
+int s2b_fw_forward(s2b_fw_plan* plan, int batch, int N, int reality, const double* delta,
+                   const void* quads, const void* f, void* flmn, void* workspace,
+                   size_t workspace_bytes, void* stream);
+/* spins: device int32 [nspins]. */
+int s2b_fw_subset_to_s2(s2b_fw_plan* plan, int batch, int nspins, const int* spins,
+                        const double* delta, const void* flmn, void* f, void* workspace,
+                        size_t workspace_bytes, void* stream);
+int s2b_fw_s2_to_subset(s2b_fw_plan* plan, int batch, int nspins, const int* spins,
+                        const double* delta, const void* quads, const void* f, void* flmn,
+                        void* workspace, size_t workspace_bytes, void* stream);
+int s2b_fw_so3_to_subset(s2b_fw_plan* plan, int batch, int ngamma, int nspins,
+                         const int* spins, const double* delta, const void* quads,
+                         const void* f, void* flmn, void* workspace, size_t workspace_bytes,
+                         void* stream);
+
 /* Peak-rate probe: a fused multiply-add chain kernel (float when fp64 == 0,
  * double otherwise) over `blocks` CTAs of 256 threads, `iters` iterations of 8
  * independent FMA chains per thread, writing one value per thread to `out`

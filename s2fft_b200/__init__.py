@@ -6,8 +6,9 @@ for sm_100a and exposed through the C ABI of ``libs2b.so`` (``include/s2b.h``).
 """
 
 from . import _lib  # noqa: F401
-from . import batch, healpix_ffts, precompute, rotation, wigner  # noqa: F401
+from . import (batch, custom_ops, fourier_wigner, healpix_ffts, precompute,  # noqa: F401
+               rotation, wigner)
 from .spherical import f_shape, flm_shape, forward, inverse  # noqa: F401
 
 __all__ = ["forward", "inverse", "f_shape", "flm_shape", "wigner", "precompute", "batch",
-           "healpix_ffts", "rotation"]
+           "healpix_ffts", "rotation", "fourier_wigner", "custom_ops"]

@@ -1,0 +1,957 @@
+// Fourier-Wigner SO(3) transforms and the spin-subset lifting ops.
+//
+// Replaces upstream s2fft:
+//   precompute_transforms/fourier_wigner.py:13-88    inverse_transform
+//   precompute_transforms/fourier_wigner.py:177-333  forward_transform
+//   precompute_transforms/construct.py:614-639       fourier_wigner_kernel (quadrature part;
+//                                                    the Delta planes come from s2b_rotate_dls)
+//   precompute_transforms/custom_ops.py:5-83         wigner_subset_to_s2
+//   precompute_transforms/custom_ops.py:168-205      so3_to_wigner_subset
+//   precompute_transforms/custom_ops.py:251-333      s2_to_wigner_subset
+//
+// Every operation is a chain over "slices": one slice is one azimuthal index n of one
+// map (a spin -n field). With Delta^l = d^l(pi/2) and c_l = (2l+1)/(8 pi^2):
+//
+//   inverse: Y[a, m] = i^(n-m) e^{i a theta0} sum_l c_l Delta^l_{a,m} Delta^l_{a,n} F[l, m]
+//            (fw_contract_kernel<INV>), a DFT over a keeping the sampled rings
+//            (fw_cols_inv_kernel), a DFT over m per ring (fw_rows_inv_kernel); the full
+//            transform then sums over n (gamma DFT, fw_gamma_kernel).
+//   forward: the gamma DFT (fw_gamma_kernel, or fw_gamma_subset_kernel for a spin subset), a DFT
+//            per ring (fw_rows_fwd_kernel), per column m the periodic extension of beta to
+//            [0, 2pi), its DFT, the quadrature as a product with the 4L-3 upsampled weights
+//            between an inverse and a forward DFT of length 4L-3 (fw_cols_fwd_kernel), and
+//            H[l, m] = (2pi)^2 i^(m-n) sum_b G[b, m] Delta^l_{b,m} Delta^l_{b,n}
+//            (fw_contract_kernel<FWD>).
+//
+// Frequencies are stored "value mod length", which is what upstream's fftshift /
+// ifftshift pairs amount to. The FFTs are the block DFTs of s2b_fft_dev.h (one CTA per
+// row or column, radix-2 or Bluestein in shared memory).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "s2b.h"
+#include "s2b_fft.h"
+#include "s2b_fft_dev.h"
+#include "s2b_internal.h"
+#include "s2b_wigner.h"  // launch_wigner_mirror
+
+namespace s2b {
+
+// Slice bookkeeping. Slice e belongs to group g = e / S and has slot k = e % S; its
+// azimuthal index is n = nlist ? nsign * nlist[k] : n0 + k. In the coefficient array
+// (flmn) the slice sits at slot Soff + k of a group of Stot slots.
+struct FWSlices {
+  int S, Stot, Soff, n0, nsign;
+  const int* nlist;
+};
+
+__device__ __forceinline__ int fw_n(const FWSlices& s, int k) {
+  return s.nlist ? s.nsign * __ldg(s.nlist + k) : s.n0 + k;
+}
+__device__ __forceinline__ long fw_coef_slice(const FWSlices& s, int e) {
+  return (long)(e / s.S) * s.Stot + s.Soff + e % s.S;
+}
+
+// z * i^k
+template <typename R2>
+__device__ __forceinline__ R2 mul_ipow(R2 z, int k) {
+  R2 o;
+  switch (k & 3) {
+    case 0: o = z; break;
+    case 1: o.x = -z.y; o.y = z.x; break;
+    case 2: o.x = -z.x; o.y = -z.y; break;
+    default: o.x = z.y; o.y = -z.x; break;
+  }
+  return o;
+}
+
+constexpr int kFwLanes = 128;  // threads of a contraction CTA, one m column each
+constexpr int kFwR = 4;        // output rows (a for the inverse, l for the forward) per thread
+constexpr int kFwE = 4;        // slices per thread
+constexpr int kFwQ = 32;       // summation indices staged per shared-memory chunk
+
+template <typename Real>
+struct FWContractParams {
+  int L, E;
+  int mwss;
+  FWSlices sl;
+  const double* delta;  // [L][2L-1][2L-1]
+  const void* in;       // INV: coefficients (slice layout fw_coef_slice); FWD: G [E][2L-1][2L-1]
+  void* out;            // INV: Y [E][2L-1][2L-1]; FWD: coefficients
+};
+
+// INV: out[e][a][m] = i^(n-m) e^{i a theta0} sum_{l} c_l D[l][a][m] D[l][a][n] F[e][l][m]
+// FWD: out[e][l][m] = (2pi)^2 i^(m-n) sum_{b} D[l][b][m] D[l][b][n] G[e][b][m]
+// (D[l][x][y] = Delta^l_{x,y}, zero where |x| > l or |y| > l.) Lanes run along m, each
+// thread keeps kFwR x kFwE complex sums; the n-column weights of a chunk of kFwQ summation
+// indices are staged in shared memory and read as broadcasts.
+template <typename Real, bool FWD>
+__global__ void __launch_bounds__(kFwLanes) fw_contract_kernel(FWContractParams<Real> p) {
+  using R2 = typename C2<Real>::t;
+  const int L = p.L, W = 2 * L - 1;
+  const int ci = blockIdx.x * kFwLanes + threadIdx.x;  // column index m + L - 1
+  const bool live = ci < W;
+  const int m = ci - (L - 1);
+  const int r0 = FWD ? blockIdx.y * kFwR : (int)blockIdx.y * kFwR - (L - 1);
+  const int rhi = L - 1;  // last output row (a or l)
+  const int e0 = blockIdx.z * kFwE;
+
+  __shared__ Real wn[kFwQ][kFwR][kFwE];
+  __shared__ int nsh[kFwE];
+  if (threadIdx.x < kFwE) {
+    const int e = e0 + threadIdx.x;
+    int n = e < p.E ? fw_n(p.sl, e % p.sl.S) : 0;
+    if (n > L - 1 || n < -(L - 1)) n = L;  // out of range: weights zero below
+    nsh[threadIdx.x] = n;
+  }
+  __syncthreads();
+
+  // summation range of the tile
+  int qlo, qhi;
+  int nmin = L;
+  for (int s = 0; s < kFwE; ++s)
+    if (e0 + s < p.E) nmin = min(nmin, abs(nsh[s]));
+  if (FWD) {
+    const int lmax = min(r0 + kFwR - 1, L - 1);
+    qlo = -lmax;
+    qhi = lmax;
+  } else {
+    int amin = L;
+    for (int j = 0; j < kFwR; ++j) {
+      const int a = r0 + j;
+      if (a <= rhi) amin = min(amin, abs(a));
+    }
+    const int cl = blockIdx.x * kFwLanes - (L - 1);
+    const int ch = min(cl + kFwLanes - 1, L - 1);
+    const int mmin = (cl <= 0 && ch >= 0) ? 0 : min(abs(cl), abs(ch));
+    qlo = max(max(amin, nmin), mmin);
+    qhi = L - 1;
+  }
+
+  R2 acc[kFwR][kFwE];
+#pragma unroll
+  for (int j = 0; j < kFwR; ++j)
+#pragma unroll
+    for (int s = 0; s < kFwE; ++s) acc[j][s] = czero<R2>();
+
+  const R2* X = reinterpret_cast<const R2*>(p.in);
+  long xoff[kFwE];
+#pragma unroll
+  for (int s = 0; s < kFwE; ++s) {
+    const int e = min(e0 + s, p.E - 1);
+    xoff[s] = FWD ? (long)e * W * W : fw_coef_slice(p.sl, e) * (long)L * W;
+  }
+
+  const double pi = 3.141592653589793;
+  for (int q0 = qlo; q0 <= qhi; q0 += kFwQ) {
+    // stage the n-column weights of this chunk
+    for (int t = threadIdx.x; t < kFwQ * kFwR * kFwE; t += kFwLanes) {
+      const int qq = t / (kFwR * kFwE), j = (t / kFwE) % kFwR, s = t % kFwE;
+      const int q = q0 + qq, r = r0 + j, n = nsh[s];
+      double w = 0.0;
+      if (q <= qhi && r <= rhi && n < L && e0 + s < p.E) {
+        if (FWD)  // D[l = r][b = q][n]
+          w = __ldg(p.delta + ((long)r * W + (q + L - 1)) * W + (n + L - 1));
+        else      // c_l D[l = q][a = r][n]
+          w = (2.0 * q + 1.0) / (8.0 * pi * pi) *
+              __ldg(p.delta + ((long)q * W + (r + L - 1)) * W + (n + L - 1));
+      }
+      wn[qq][j][s] = (Real)w;
+    }
+    __syncthreads();
+    const int qend = min(kFwQ, qhi - q0 + 1);
+    if (live) {
+      for (int qq = 0; qq < qend; ++qq) {
+        const int q = q0 + qq;
+        R2 x[kFwE];
+#pragma unroll
+        for (int s = 0; s < kFwE; ++s)
+          x[s] = FWD ? X[xoff[s] + (long)(q + L - 1) * W + ci] : X[xoff[s] + (long)q * W + ci];
+#pragma unroll
+        for (int j = 0; j < kFwR; ++j) {
+          const int r = r0 + j;
+          if (r > rhi) continue;
+          const Real w1 = FWD ? (Real)__ldg(p.delta + ((long)r * W + (q + L - 1)) * W + ci)
+                              : (Real)__ldg(p.delta + ((long)q * W + (r + L - 1)) * W + ci);
+#pragma unroll
+          for (int s = 0; s < kFwE; ++s) {
+            const Real w = w1 * wn[qq][j][s];
+            acc[j][s].x = fma(w, x[s].x, acc[j][s].x);
+            acc[j][s].y = fma(w, x[s].y, acc[j][s].y);
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (!live) return;
+
+  R2* O = reinterpret_cast<R2*>(p.out);
+#pragma unroll
+  for (int s = 0; s < kFwE; ++s) {
+    const int e = e0 + s;
+    if (e >= p.E) continue;
+    const int n = nsh[s] == L ? 0 : nsh[s];
+#pragma unroll
+    for (int j = 0; j < kFwR; ++j) {
+      const int r = r0 + j;
+      if (r > rhi) continue;
+      R2 v = acc[j][s];
+      if (FWD) {
+        const Real sc = (Real)(4.0 * pi * pi);
+        v = mul_ipow(v, m - n);
+        v.x *= sc;
+        v.y *= sc;
+        O[fw_coef_slice(p.sl, e) * (long)L * W + (long)r * W + ci] = v;
+      } else {
+        v = mul_ipow(v, n - m);
+        if (!p.mwss) {  // e^{i a pi / (2L-1)}
+          double sn, cs;
+          sincospi((double)r / (double)W, &sn, &cs);
+          const Real c = (Real)cs, sv = (Real)sn;
+          const R2 u = v;
+          v.x = u.x * c - u.y * sv;
+          v.y = u.x * sv + u.y * c;
+        }
+        O[(long)e * W * W + (long)(r + L - 1) * W + ci] = v;
+      }
+    }
+  }
+}
+
+template <typename Real>
+struct FWFftParams {
+  int L, mwss, ntheta, nphi, P, E;
+  FWSlices sl;
+  int nmajor, groups;  // map index of slice e: (Soff + e % S) * groups + e / S when nmajor
+  double scale;
+  FFTDesc dphi, dP;
+  FFTTables<Real> tb;
+  const void* quads;  // complex128 [4L-3]
+  const void* in;
+  void* out;
+};
+
+template <typename Real>
+__device__ __forceinline__ long fw_map_index(const FWFftParams<Real>& p, int e) {
+  return p.nmajor ? (long)(p.sl.Soff + e % p.sl.S) * p.groups + e / p.sl.S : (long)e;
+}
+
+// Inverse, beta: column m of Y[e] -> T[e][t][m] = sum_a Y[a][m] e^{+i a beta_t}, t < ntheta
+// (beta_t = 2 pi t / nphi; the theta0 shift is in Y).
+template <typename Real>
+__global__ void __launch_bounds__(512) fw_cols_inv_kernel(FWFftParams<Real> p) {
+  using R2 = typename C2<Real>::t;
+  extern __shared__ unsigned char fw_smem[];
+  R2* s = reinterpret_cast<R2*>(fw_smem);
+  const int L = p.L, W = 2 * L - 1, col = blockIdx.x, e = blockIdx.y;
+  const R2* Y = reinterpret_cast<const R2*>(p.in) + (long)e * W * W;
+  const int na = p.nphi;
+  dft_run<Real>(s, p.dphi, p.tb, true, [&](int k) {
+    const int a = k <= L - 1 ? k : k - na;
+    return a >= -(L - 1) ? Y[(long)(a + L - 1) * W + col] : czero<R2>();
+  });
+  R2* T = reinterpret_cast<R2*>(p.out) + (long)e * p.ntheta * W;
+  for (int t = threadIdx.x; t < p.ntheta; t += blockDim.x)
+    T[(long)t * W + col] = dft_get<Real>(s, p.dphi, p.tb, true, t);
+}
+
+// Inverse, alpha: ring t of T[e] -> map[t][p] = sum_m T[t][m] e^{+i m alpha_p}.
+template <typename Real>
+__global__ void __launch_bounds__(512) fw_rows_inv_kernel(FWFftParams<Real> p) {
+  using R2 = typename C2<Real>::t;
+  extern __shared__ unsigned char fw_smem[];
+  R2* s = reinterpret_cast<R2*>(fw_smem);
+  const int L = p.L, W = 2 * L - 1, t = blockIdx.x, e = blockIdx.y;
+  const R2* T = reinterpret_cast<const R2*>(p.in) + ((long)e * p.ntheta + t) * W;
+  const int np = p.nphi;
+  dft_run<Real>(s, p.dphi, p.tb, true, [&](int k) {
+    const int m = k <= L - 1 ? k : k - np;
+    return m >= -(L - 1) ? T[m + L - 1] : czero<R2>();
+  });
+  R2* o = reinterpret_cast<R2*>(p.out) + (fw_map_index(p, e) * p.ntheta + t) * np;
+  for (int j = threadIdx.x; j < np; j += blockDim.x) o[j] = dft_get<Real>(s, p.dphi, p.tb, true, j);
+}
+
+// Forward, alpha: ring t of map e -> S[e][t][m] = scale sum_p map[t][p] e^{-i m alpha_p},
+// |m| <= L-1.
+template <typename Real>
+__global__ void __launch_bounds__(512) fw_rows_fwd_kernel(FWFftParams<Real> p) {
+  using R2 = typename C2<Real>::t;
+  extern __shared__ unsigned char fw_smem[];
+  R2* s = reinterpret_cast<R2*>(fw_smem);
+  const int L = p.L, W = 2 * L - 1, t = blockIdx.x, e = blockIdx.y;
+  const int np = p.nphi;
+  const R2* f = reinterpret_cast<const R2*>(p.in) + (fw_map_index(p, e) * p.ntheta + t) * np;
+  dft_run<Real>(s, p.dphi, p.tb, false, [&](int k) { return f[k]; });
+  R2* S = reinterpret_cast<R2*>(p.out) + ((long)e * p.ntheta + t) * W;
+  const Real sc = (Real)p.scale;
+  for (int c = threadIdx.x; c < W; c += blockDim.x) {
+    const int m = c - (L - 1);
+    S[c] = cscale(dft_get<Real>(s, p.dphi, p.tb, false, pmod(m, np)), sc);
+  }
+}
+
+// Forward, beta: column m of S[e] -> G[e][b][m], |b| <= L-1 (fourier_wigner.py:258-292).
+// Shared memory: the DFT buffer (padded working length) and a buffer of 4L-3 values.
+template <typename Real>
+__global__ void __launch_bounds__(512) fw_cols_fwd_kernel(FWFftParams<Real> p, int bufM) {
+  using R2 = typename C2<Real>::t;
+  extern __shared__ unsigned char fw_smem[];
+  R2* s = reinterpret_cast<R2*>(fw_smem);
+  R2* tmp = s + padded_len(bufM);
+  const int L = p.L, W = 2 * L - 1, col = blockIdx.x, e = blockIdx.y;
+  const int m = col - (L - 1);
+  const int n = fw_n(p.sl, e % p.sl.S);
+  const Real sgn = ((abs(m) + abs(n)) & 1) ? Real(-1) : Real(1);
+  const int nth = p.ntheta, nx = p.nphi, P = p.P;
+  const R2* Sx = reinterpret_cast<const R2*>(p.in) + (long)e * nth * W;
+  // periodic extension to [0, 2pi): rows nth-1+j = sgn * rows nth-1-j, 1 <= j <= L-1
+  dft_run<Real>(s, p.dphi, p.tb, false, [&](int k) {
+    if (k < nth) return Sx[(long)k * W + col];
+    return cscale(Sx[(long)(2 * (nth - 1) - k) * W + col], sgn);
+  });
+  const int blo = p.mwss ? -L : -(L - 1);
+  const Real inx = (Real)(1.0 / nx);
+  for (int b = blo + (int)threadIdx.x; b <= L - 1; b += blockDim.x) {
+    R2 v = cscale(dft_get<Real>(s, p.dphi, p.tb, false, pmod(b, nx)), inx);
+    if (!p.mwss) {  // e^{-i b pi / (2L-1)}
+      double sn, cs;
+      sincospi(-(double)b / (double)W, &sn, &cs);
+      const R2 u = v;
+      v.x = u.x * (Real)cs - u.y * (Real)sn;
+      v.y = u.x * (Real)sn + u.y * (Real)cs;
+    }
+    tmp[b - blo] = v;
+  }
+  __syncthreads();
+  // zero-padded to 4L-3 and inverse DFT (the upsampled beta samples)
+  const int half = (P - 1) / 2;
+  dft_run<Real>(s, p.dP, p.tb, true, [&](int k) {
+    const int v = k <= half ? k : k - P;
+    return (v >= blo && v <= L - 1) ? tmp[v - blo] : czero<R2>();
+  });
+  const double2* qd = reinterpret_cast<const double2*>(p.quads);
+  for (int j = threadIdx.x; j < P; j += blockDim.x) {
+    const double2 q = qd[j];
+    R2 w;
+    w.x = (Real)q.x;
+    w.y = (Real)q.y;
+    tmp[j] = cmul(dft_get<Real>(s, p.dP, p.tb, true, j), w);
+  }
+  __syncthreads();
+  dft_run<Real>(s, p.dP, p.tb, false, [&](int k) { return tmp[k]; });
+  const Real iP = (Real)(1.0 / P);
+  R2* G = reinterpret_cast<R2*>(p.out) + (long)e * W * W;
+  for (int b = -(L - 1) + (int)threadIdx.x; b <= L - 1; b += blockDim.x)
+    G[(long)(b + L - 1) * W + col] = cscale(dft_get<Real>(s, p.dP, p.tb, false, pmod(b, P)), iP);
+}
+
+// Gamma DFT of the full transform, one thread per (map, pixel), kGamK outputs per pass.
+//   inverse: f[b][g][px] = sum_n x[N-1+n][b][px] e^{+2 pi i n g / G}, n in [-(N-1), N-1];
+//            reality: real output from n >= 0 (irfft: n = 0 real part, n > 0 doubled)
+//   forward: x[N-1+n][b][px] = (1/G) sum_g f[b][g][px] e^{-2 pi i n g / G}, n in [n0, N-1]
+// (fourier_wigner.py:80-87 and 241-248). A table of the G roots e^{2 pi i j / G} sits in
+// shared memory; the exponent n g is reduced mod G exactly.
+constexpr int kGamK = 8;
+
+template <typename Real, bool FWD>
+__global__ void fw_gamma_kernel(const void* in, void* out, int B, int N, long npix, int reality) {
+  using R2 = typename C2<Real>::t;
+  extern __shared__ double2 roots[];
+  const int G = 2 * N - 1;
+  for (int j = threadIdx.x; j < G; j += blockDim.x) {
+    double sn, cs;
+    sincospi(2.0 * (double)j / (double)G, &sn, &cs);
+    roots[j] = make_double2(cs, sn);
+  }
+  __syncthreads();
+  const long total = (long)B * npix;
+  const int nlo = reality ? 0 : -(N - 1);
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
+       i += (long)gridDim.x * blockDim.x) {
+    const long b = i / npix, px = i % npix;
+    if (!FWD) {
+      const R2* x = reinterpret_cast<const R2*>(in);
+      for (int g0 = 0; g0 < G; g0 += kGamK) {
+        double re[kGamK], im[kGamK];
+#pragma unroll
+        for (int u = 0; u < kGamK; ++u) re[u] = im[u] = 0.0;
+        for (int n = nlo; n < N; ++n) {
+          const R2 v = x[((long)(N - 1 + n) * B + b) * npix + px];
+          double vr = v.x, vi = v.y;
+          if (reality) {
+            if (n == 0) vi = 0.0;
+            else { vr *= 2.0; vi *= 2.0; }
+          }
+          const int step = ((n % G) + G) % G;
+          int r = (int)(((long)step * g0) % G);
+#pragma unroll
+          for (int u = 0; u < kGamK; ++u) {
+            const double2 w = roots[r];
+            re[u] += vr * w.x - vi * w.y;
+            im[u] += vr * w.y + vi * w.x;
+            r += step;
+            if (r >= G) r -= G;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < kGamK; ++u) {
+          const int g = g0 + u;
+          if (g >= G) break;
+          const long o = (b * G + g) * npix + px;
+          if (reality) {
+            reinterpret_cast<Real*>(out)[o] = (Real)re[u];
+          } else {
+            R2 w;
+            w.x = (Real)re[u];
+            w.y = (Real)im[u];
+            reinterpret_cast<R2*>(out)[o] = w;
+          }
+        }
+      }
+    } else {
+      R2* x = reinterpret_cast<R2*>(out);
+      for (int n0 = nlo; n0 < N; n0 += kGamK) {
+        double re[kGamK], im[kGamK];
+#pragma unroll
+        for (int u = 0; u < kGamK; ++u) re[u] = im[u] = 0.0;
+        for (int g = 0; g < G; ++g) {
+          double vr, vi;
+          const long o = (b * G + g) * npix + px;
+          if (reality) {
+            vr = reinterpret_cast<const Real*>(in)[o];
+            vi = 0.0;
+          } else {
+            const R2 v = reinterpret_cast<const R2*>(in)[o];
+            vr = v.x;
+            vi = v.y;
+          }
+          // e^{-2 pi i n g / G} = roots[(-n g) mod G]
+          const int step = (G - g % G) % G;  // (-g) mod G, advances with n
+          int r = (int)(((long)step * (((n0 % G) + G) % G)) % G);
+#pragma unroll
+          for (int u = 0; u < kGamK; ++u) {
+            const double2 w = roots[r];
+            re[u] += vr * w.x - vi * w.y;
+            im[u] += vr * w.y + vi * w.x;
+            r += step;
+            if (r >= G) r -= G;
+          }
+        }
+        const double sc = 1.0 / G;
+#pragma unroll
+        for (int u = 0; u < kGamK; ++u) {
+          const int n = n0 + u;
+          if (n >= N) break;
+          R2 w;
+          w.x = (Real)(re[u] * sc);
+          w.y = (Real)(im[u] * sc);
+          x[((long)(N - 1 + n) * B + b) * npix + px] = w;
+        }
+      }
+    }
+  }
+}
+
+// quads[j] = sum_{|k| <= 2L-2} w(-k) e^{+2 pi i k j / (4L-3)}, w the MW weights
+// (w(+-1) = +-i pi/2, w(even k) = 2/(1-k^2), else 0); construct.py:629-634.
+__global__ void fw_quads_kernel(int L, double2* quads) {
+  const int P = 4 * L - 3;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= P) return;
+  double re = 0.0, im = 0.0;
+  for (int k = -(2 * L - 2); k <= 2 * L - 2; ++k) {
+    const int mk = -k;
+    double wr = 0.0, wi = 0.0;
+    if (mk == 1)
+      wi = 1.5707963267948966;
+    else if (mk == -1)
+      wi = -1.5707963267948966;
+    else if ((mk & 1) == 0)
+      wr = 2.0 / (1.0 - (double)mk * (double)mk);
+    else
+      continue;
+    const long r = (((long)k * j) % P + P) % P;
+    double sn, cs;
+    sincospi(2.0 * (double)r / (double)P, &sn, &cs);
+    re += wr * cs - wi * sn;
+    im += wr * sn + wi * cs;
+  }
+  quads[j] = make_double2(re, im);
+}
+
+// Gamma DFT at a spin subset: x[g][k][px] = (1/G) sum_c f[g][c][px] e^{-2 pi i c n_k / G}
+// (n_k = -spin_k; custom_ops.py:200-204), f [O][G][npix], x [O][S][npix].
+template <typename Real>
+__global__ void fw_gamma_subset_kernel(const void* fin, void* xout, int O, int G, int S,
+                                       long npix, FWSlices sl) {
+  using R2 = typename C2<Real>::t;
+  const R2* f = reinterpret_cast<const R2*>(fin);
+  R2* x = reinterpret_cast<R2*>(xout);
+  const long total = (long)O * npix;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
+       i += (long)gridDim.x * blockDim.x) {
+    const long o = i / npix, px = i % npix;
+    for (int k = 0; k < S; ++k) {
+      const int n = fw_n(sl, k);
+      double re = 0.0, im = 0.0;
+      for (int c = 0; c < G; ++c) {
+        const R2 v = f[(o * G + c) * npix + px];
+        const long r = ((-(long)c * n) % G + G) % G;
+        double sn, cs;
+        sincospi(2.0 * (double)r / (double)G, &sn, &cs);
+        re += (double)v.x * cs - (double)v.y * sn;
+        im += (double)v.x * sn + (double)v.y * cs;
+      }
+      R2 out;
+      out.x = (Real)(re / G);
+      out.y = (Real)(im / G);
+      x[(o * S + k) * npix + px] = out;
+    }
+  }
+}
+
+}  // namespace s2b
+
+using namespace s2b;
+
+struct s2b_fw_plan {
+  int L, mwss, ntheta, nphi, P;
+  bool fp64;
+  int device;
+  std::vector<void*> allocs;
+  FFTSet fft;  // host[0]: length nphi, host[1]: length 4L-3
+  ~s2b_fw_plan() {
+    for (void* a : allocs) cudaFree(a);
+  }
+};
+
+namespace {
+
+int fw_fail(int code, const std::string& msg) { return s2b::set_last_error(code, msg.c_str()); }
+
+#define FW_CK(call)                                                                       \
+  do {                                                                                    \
+    cudaError_t _e = (call);                                                              \
+    if (_e != cudaSuccess)                                                                \
+      return fw_fail(S2B_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(_e));   \
+  } while (0)
+
+size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+bool aligned16(const void* p) { return p && ((uintptr_t)p & 15) == 0; }
+
+// Workspace regions: A (Y, G, or the gamma maps), B (T or S), C (spin-subset gamma maps).
+struct FWLayout {
+  size_t a, b, c;
+  size_t total() const { return a + b + c; }
+};
+
+FWLayout fw_layout(const s2b_fw_plan* p, long E, long nmaps_gamma, long E_subset_gamma) {
+  const size_t cs = p->fp64 ? 16 : 8;
+  const long W = 2L * p->L - 1;
+  const long npix = (long)p->ntheta * p->nphi;
+  FWLayout l;
+  l.a = al256(cs * (size_t)std::max(E * W * W, nmaps_gamma * npix));
+  l.b = al256(cs * (size_t)(E * p->ntheta * W));
+  l.c = al256(cs * (size_t)(E_subset_gamma * npix));
+  return l;
+}
+
+template <typename Real>
+FFTTables<Real> tables(const s2b_fw_plan* p) {
+  FFTTables<Real> t;
+  t.tw = reinterpret_cast<const typename FFTTables<Real>::R2*>(p->fft.tw);
+  t.chirp = reinterpret_cast<const typename FFTTables<Real>::R2*>(p->fft.chirp);
+  t.bfilt = reinterpret_cast<const typename FFTTables<Real>::R2*>(p->fft.bf);
+  return t;
+}
+
+int fft_threads_for(int M) {
+  int t = M / 8;
+  if (t > 512) t = 512;
+  if (t < 32) t = 32;
+  return t;
+}
+
+template <typename Real>
+FWFftParams<Real> fft_params(const s2b_fw_plan* p, int E, const FWSlices& sl) {
+  FWFftParams<Real> f{};
+  f.L = p->L;
+  f.mwss = p->mwss;
+  f.ntheta = p->ntheta;
+  f.nphi = p->nphi;
+  f.P = p->P;
+  f.E = E;
+  f.sl = sl;
+  f.nmajor = 0;
+  f.groups = 1;
+  f.scale = 1.0;
+  f.dphi = p->fft.host[0];
+  f.dP = p->fft.host[1];
+  f.tb = tables<Real>(p);
+  return f;
+}
+
+template <typename Real, typename K>
+cudaError_t launch_fft(K kernel, dim3 grid, int M, size_t smem, cudaStream_t st,
+                       const FWFftParams<Real>& f) {
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  kernel<<<grid, fft_threads_for(M), smem, st>>>(f);
+  return cudaGetLastError();
+}
+
+template <typename Real>
+int contract(const s2b_fw_plan* p, bool fwd, int E, const FWSlices& sl, const double* delta,
+             const void* in, void* out, cudaStream_t st) {
+  FWContractParams<Real> c{};
+  c.L = p->L;
+  c.E = E;
+  c.mwss = p->mwss;
+  c.sl = sl;
+  c.delta = delta;
+  c.in = in;
+  c.out = out;
+  const int W = 2 * p->L - 1;
+  const int rows = fwd ? p->L : W;
+  dim3 grid((W + kFwLanes - 1) / kFwLanes, (rows + kFwR - 1) / kFwR, (E + kFwE - 1) / kFwE);
+  if (grid.z > 65535) return fw_fail(S2B_ERR_INVALID, "too many slices in one call");
+  if (fwd)
+    fw_contract_kernel<Real, true><<<grid, kFwLanes, 0, st>>>(c);
+  else
+    fw_contract_kernel<Real, false><<<grid, kFwLanes, 0, st>>>(c);
+  FW_CK(cudaGetLastError());
+  return S2B_OK;
+}
+
+// sphere-side inverse chain: Y (region A) -> T (region B) -> maps
+template <typename Real>
+int inverse_chain(const s2b_fw_plan* p, int E, const FWSlices& sl, const double* delta,
+                  const void* coef, void* maps, int nmajor, int groups, char* ws,
+                  const FWLayout& lay, cudaStream_t st) {
+  using R2 = typename C2<Real>::t;
+  void* A = ws;
+  void* B = ws + lay.a;
+  int rc = contract<Real>(p, false, E, sl, delta, coef, A, st);
+  if (rc) return rc;
+  FWFftParams<Real> f = fft_params<Real>(p, E, sl);
+  const int M = f.dphi.M;
+  const size_t smem = (size_t)padded_len(M) * sizeof(R2);
+  f.in = A;
+  f.out = B;
+  FW_CK(launch_fft<Real>(fw_cols_inv_kernel<Real>, dim3(2 * p->L - 1, E), M, smem, st, f));
+  f.in = B;
+  f.out = maps;
+  f.nmajor = nmajor;
+  f.groups = groups;
+  FW_CK(launch_fft<Real>(fw_rows_inv_kernel<Real>, dim3(p->ntheta, E), M, smem, st, f));
+  return S2B_OK;
+}
+
+// sphere-side forward chain: maps -> S (region B) -> G (region A) -> coefficients
+template <typename Real>
+int forward_chain(const s2b_fw_plan* p, int E, const FWSlices& sl, const double* delta,
+                  const void* quads, const void* maps, void* coef, int nmajor, int groups,
+                  double scale, char* ws, const FWLayout& lay, cudaStream_t st) {
+  using R2 = typename C2<Real>::t;
+  void* A = ws;
+  void* B = ws + lay.a;
+  FWFftParams<Real> f = fft_params<Real>(p, E, sl);
+  f.quads = quads;
+  const int M = f.dphi.M;
+  f.in = maps;
+  f.out = B;
+  f.nmajor = nmajor;
+  f.groups = groups;
+  f.scale = scale;
+  FW_CK(launch_fft<Real>(fw_rows_fwd_kernel<Real>, dim3(p->ntheta, E), M,
+                         (size_t)padded_len(M) * sizeof(R2), st, f));
+  f.in = B;
+  f.out = A;
+  f.nmajor = 0;
+  f.scale = 1.0;
+  const int bufM = std::max(f.dphi.M, f.dP.M);
+  const size_t smem = (size_t)(padded_len(bufM) + p->P) * sizeof(R2);
+  FW_CK(cudaFuncSetAttribute(fw_cols_fwd_kernel<Real>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  fw_cols_fwd_kernel<Real><<<dim3(2 * p->L - 1, E), fft_threads_for(bufM), smem, st>>>(f, bufM);
+  FW_CK(cudaGetLastError());
+  return contract<Real>(p, true, E, sl, delta, A, coef, st);
+}
+
+template <typename Real>
+int gamma_dft(bool fwd, const void* in, void* out, int B, int N, long npix, int reality,
+              cudaStream_t st) {
+  const long tot = (long)B * npix;
+  const int blocks = (int)std::min<long>((tot + 255) / 256, 4L * 148 * 8);
+  const size_t smem = (size_t)(2 * N - 1) * sizeof(double2);
+  if (fwd)
+    fw_gamma_kernel<Real, true><<<blocks, 256, smem, st>>>(in, out, B, N, npix, reality);
+  else
+    fw_gamma_kernel<Real, false><<<blocks, 256, smem, st>>>(in, out, B, N, npix, reality);
+  FW_CK(cudaGetLastError());
+  return S2B_OK;
+}
+
+int check_plan(const s2b_fw_plan* p) {
+  if (!p) return fw_fail(S2B_ERR_INVALID, "NULL Fourier-Wigner plan");
+  int dev = -1;
+  FW_CK(cudaGetDevice(&dev));
+  if (dev != p->device)
+    return fw_fail(S2B_ERR_INVALID, "the current device is not the plan's device");
+  return S2B_OK;
+}
+
+int check_ptrs(std::initializer_list<const void*> ptrs) {
+  for (const void* q : ptrs)
+    if (!aligned16(q)) return fw_fail(S2B_ERR_ALIGN, "NULL or misaligned (16-byte) pointer");
+  return S2B_OK;
+}
+
+// slices run along gridDim.y of the FFT kernels
+int check_slices(long E) {
+  if (E > 65535) return fw_fail(S2B_ERR_INVALID, "more than 65535 slices in one call");
+  return S2B_OK;
+}
+
+int check_ws(const FWLayout& lay, const void* ws, size_t bytes) {
+  if (bytes < lay.total())
+    return fw_fail(S2B_ERR_WORKSPACE, "Fourier-Wigner workspace too small: need " +
+                                          std::to_string(lay.total()) + " bytes");
+  if (lay.total() && ((uintptr_t)ws & 255))
+    return fw_fail(S2B_ERR_ALIGN, "Fourier-Wigner workspace must be 256-byte aligned");
+  return S2B_OK;
+}
+
+FWSlices full_slices(int N, int reality) {
+  FWSlices s{};
+  s.S = reality ? N : 2 * N - 1;
+  s.Stot = 2 * N - 1;
+  s.Soff = reality ? N - 1 : 0;
+  s.n0 = reality ? 0 : -(N - 1);
+  s.nsign = 1;
+  s.nlist = nullptr;
+  return s;
+}
+
+FWSlices spin_slices(int nspins, const int* spins) {
+  FWSlices s{};
+  s.S = nspins;
+  s.Stot = nspins;
+  s.Soff = 0;
+  s.n0 = 0;
+  s.nsign = -1;  // slice n = -spin
+  s.nlist = spins;
+  return s;
+}
+
+}  // namespace
+
+extern "C" {
+
+int s2b_fw_plan_create(int L, int sampling, int precision, s2b_fw_plan** plan) {
+  if (!plan) return fw_fail(S2B_ERR_INVALID, "plan is NULL");
+  *plan = nullptr;
+  if (L < 2) return fw_fail(S2B_ERR_INVALID, "Fourier-Wigner transforms need L >= 2");
+  if (sampling != S2B_MW && sampling != S2B_MWSS)
+    return fw_fail(S2B_ERR_INVALID, "Fourier-Wigner algorithm supports mw and mwss sampling only");
+  if (precision != S2B_F64 && precision != S2B_F32)
+    return fw_fail(S2B_ERR_INVALID, "Fourier-Wigner precision must be S2B_F64 or S2B_F32");
+  auto* p = new s2b_fw_plan();
+  p->L = L;
+  p->mwss = sampling == S2B_MWSS;
+  p->ntheta = p->mwss ? L + 1 : L;
+  p->nphi = p->mwss ? 2 * L : 2 * L - 1;
+  p->P = 4 * L - 3;
+  p->fp64 = precision == S2B_F64;
+  cudaError_t e = cudaGetDevice(&p->device);
+  if (e != cudaSuccess) {
+    delete p;
+    return fw_fail(S2B_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+  }
+  const int lens[2] = {p->nphi, p->P};
+  const int rc = build_fft_set(lens, 2, p->fp64, &p->allocs, &p->fft);
+  if (rc) {
+    delete p;
+    return rc;
+  }
+  // the column chain keeps a DFT buffer and 4L-3 values in shared memory
+  const size_t cs = p->fp64 ? 16 : 8;
+  const int bufM = std::max(p->fft.host[0].M, p->fft.host[1].M);
+  if ((padded_len(bufM) + (size_t)p->P) * cs > 227 * 1024) {
+    delete p;
+    return fw_fail(S2B_ERR_INVALID, "band-limit too large for the Fourier-Wigner beta chain");
+  }
+  *plan = p;
+  return S2B_OK;
+}
+
+int s2b_fw_plan_destroy(s2b_fw_plan* plan) {
+  delete plan;
+  return S2B_OK;
+}
+
+int s2b_fw_quads(s2b_fw_plan* plan, void* quads, void* stream) {
+  int rc;
+  if ((rc = check_plan(plan))) return rc;
+  if ((rc = check_ptrs({quads}))) return rc;
+  fw_quads_kernel<<<(plan->P + 127) / 128, 128, 0, (cudaStream_t)stream>>>(plan->L,
+                                                                           (double2*)quads);
+  FW_CK(cudaGetLastError());
+  return S2B_OK;
+}
+
+size_t s2b_fw_workspace_size(const s2b_fw_plan* plan, int op, int batch, int N, int reality,
+                             int nspins) {
+  if (!plan || batch < 1) return 0;
+  switch (op) {
+    case S2B_FW_INVERSE:
+    case S2B_FW_FORWARD: {
+      const long S = reality ? N : 2L * N - 1;
+      return fw_layout(plan, (long)batch * S, (long)batch * (2L * N - 1), 0).total();
+    }
+    case S2B_FW_SUBSET_TO_S2:
+    case S2B_FW_S2_TO_SUBSET:
+      return fw_layout(plan, (long)batch * nspins, 0, 0).total();
+    case S2B_FW_SO3_TO_SUBSET:
+      return fw_layout(plan, (long)batch * nspins, 0, (long)batch * nspins).total();
+    default:
+      return 0;
+  }
+}
+
+int s2b_fw_inverse(s2b_fw_plan* plan, int batch, int N, int reality, const double* delta,
+                   const void* flmn, void* f, void* ws, size_t ws_bytes, void* stream) {
+  int rc;
+  if ((rc = check_plan(plan))) return rc;
+  if (batch < 1 || N < 1 || N > plan->L)
+    return fw_fail(S2B_ERR_INVALID, "need batch >= 1 and 1 <= N <= L");
+  if ((rc = check_ptrs({delta, flmn, f}))) return rc;
+  const FWSlices sl = full_slices(N, reality);
+  const int E = batch * sl.S;
+  if ((rc = check_slices((long)batch * sl.S))) return rc;
+  const FWLayout lay = fw_layout(plan, E, (long)batch * (2L * N - 1), 0);
+  if ((rc = check_ws(lay, ws, ws_bytes))) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  char* w = (char*)ws;
+  // the per-n maps go to region A (after Y is consumed), n-major for the gamma DFT
+  if (plan->fp64)
+    rc = inverse_chain<double>(plan, E, sl, delta, flmn, w, 1, batch, w, lay, st);
+  else
+    rc = inverse_chain<float>(plan, E, sl, delta, flmn, w, 1, batch, w, lay, st);
+  if (rc) return rc;
+  const long npix = (long)plan->ntheta * plan->nphi;
+  return plan->fp64 ? gamma_dft<double>(false, w, f, batch, N, npix, reality, st)
+                    : gamma_dft<float>(false, w, f, batch, N, npix, reality, st);
+}
+
+int s2b_fw_forward(s2b_fw_plan* plan, int batch, int N, int reality, const double* delta,
+                   const void* quads, const void* f, void* flmn, void* ws, size_t ws_bytes,
+                   void* stream) {
+  int rc;
+  if ((rc = check_plan(plan))) return rc;
+  if (batch < 1 || N < 1 || N > plan->L)
+    return fw_fail(S2B_ERR_INVALID, "need batch >= 1 and 1 <= N <= L");
+  if ((rc = check_ptrs({delta, quads, f, flmn}))) return rc;
+  const FWSlices sl = full_slices(N, reality);
+  const int E = batch * sl.S;
+  if ((rc = check_slices((long)batch * sl.S))) return rc;
+  const FWLayout lay = fw_layout(plan, E, (long)batch * (2L * N - 1), 0);
+  if ((rc = check_ws(lay, ws, ws_bytes))) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  char* w = (char*)ws;
+  const long npix = (long)plan->ntheta * plan->nphi;
+  // gamma DFT into region A, n-major
+  rc = plan->fp64 ? gamma_dft<double>(true, f, w, batch, N, npix, reality, st)
+                  : gamma_dft<float>(true, f, w, batch, N, npix, reality, st);
+  if (rc) return rc;
+  const double scale = 1.0 / plan->nphi;
+  if (plan->fp64)
+    rc = forward_chain<double>(plan, E, sl, delta, quads, w, flmn, 1, batch, scale, w, lay, st);
+  else
+    rc = forward_chain<float>(plan, E, sl, delta, quads, w, flmn, 1, batch, scale, w, lay, st);
+  if (rc) return rc;
+  if (reality) FW_CK(launch_wigner_mirror(plan->fp64, flmn, batch, N, plan->L, st));
+  return S2B_OK;
+}
+
+int s2b_fw_subset_to_s2(s2b_fw_plan* plan, int batch, int nspins, const int* spins,
+                        const double* delta, const void* flmn, void* f, void* ws,
+                        size_t ws_bytes, void* stream) {
+  int rc;
+  if ((rc = check_plan(plan))) return rc;
+  if (batch < 1 || nspins < 1) return fw_fail(S2B_ERR_INVALID, "need batch >= 1 and nspins >= 1");
+  if (!spins) return fw_fail(S2B_ERR_INVALID, "spins is NULL");
+  if ((rc = check_ptrs({delta, flmn, f}))) return rc;
+  const FWSlices sl = spin_slices(nspins, spins);
+  const int E = batch * nspins;
+  if ((rc = check_slices((long)batch * nspins))) return rc;
+  const FWLayout lay = fw_layout(plan, E, 0, 0);
+  if ((rc = check_ws(lay, ws, ws_bytes))) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plan->fp64)
+    return inverse_chain<double>(plan, E, sl, delta, flmn, f, 0, 1, (char*)ws, lay, st);
+  return inverse_chain<float>(plan, E, sl, delta, flmn, f, 0, 1, (char*)ws, lay, st);
+}
+
+int s2b_fw_s2_to_subset(s2b_fw_plan* plan, int batch, int nspins, const int* spins,
+                        const double* delta, const void* quads, const void* f, void* flmn,
+                        void* ws, size_t ws_bytes, void* stream) {
+  int rc;
+  if ((rc = check_plan(plan))) return rc;
+  if (batch < 1 || nspins < 1) return fw_fail(S2B_ERR_INVALID, "need batch >= 1 and nspins >= 1");
+  if (!spins) return fw_fail(S2B_ERR_INVALID, "spins is NULL");
+  if ((rc = check_ptrs({delta, quads, f, flmn}))) return rc;
+  const FWSlices sl = spin_slices(nspins, spins);
+  const int E = batch * nspins;
+  if ((rc = check_slices((long)batch * nspins))) return rc;
+  const FWLayout lay = fw_layout(plan, E, 0, 0);
+  if ((rc = check_ws(lay, ws, ws_bytes))) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  const double scale = 1.0 / plan->nphi;
+  if (plan->fp64)
+    return forward_chain<double>(plan, E, sl, delta, quads, f, flmn, 0, 1, scale, (char*)ws,
+                                 lay, st);
+  return forward_chain<float>(plan, E, sl, delta, quads, f, flmn, 0, 1, scale, (char*)ws, lay,
+                              st);
+}
+
+int s2b_fw_so3_to_subset(s2b_fw_plan* plan, int batch, int ngamma, int nspins, const int* spins,
+                         const double* delta, const void* quads, const void* f, void* flmn,
+                         void* ws, size_t ws_bytes, void* stream) {
+  int rc;
+  if ((rc = check_plan(plan))) return rc;
+  if (batch < 1 || nspins < 1 || ngamma < 1)
+    return fw_fail(S2B_ERR_INVALID, "need batch, ngamma, nspins >= 1");
+  if (!spins) return fw_fail(S2B_ERR_INVALID, "spins is NULL");
+  if ((rc = check_ptrs({delta, quads, f, flmn}))) return rc;
+  const FWSlices sl = spin_slices(nspins, spins);
+  const int E = batch * nspins;
+  if ((rc = check_slices((long)batch * nspins))) return rc;
+  const FWLayout lay = fw_layout(plan, E, 0, E);
+  if ((rc = check_ws(lay, ws, ws_bytes))) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  char* w = (char*)ws;
+  void* C = w + lay.a + lay.b;
+  const long npix = (long)plan->ntheta * plan->nphi;
+  const long tot = (long)batch * npix;
+  const int blocks = (int)std::min<long>((tot + 255) / 256, 65535L);
+  if (plan->fp64)
+    fw_gamma_subset_kernel<double><<<blocks, 256, 0, st>>>(f, C, batch, ngamma, nspins, npix, sl);
+  else
+    fw_gamma_subset_kernel<float><<<blocks, 256, 0, st>>>(f, C, batch, ngamma, nspins, npix, sl);
+  FW_CK(cudaGetLastError());
+  const double scale = 1.0 / plan->nphi;
+  if (plan->fp64)
+    return forward_chain<double>(plan, E, sl, delta, quads, C, flmn, 0, 1, scale, w, lay, st);
+  return forward_chain<float>(plan, E, sl, delta, quads, C, flmn, 0, 1, scale, w, lay, st);
+}
+
+}  // extern "C"

@@ -1727,6 +1727,56 @@ static int run_wigner(s2b_plan* p, bool forward, const void* in, void* out, char
   return S2B_OK;
 }
 
+// FFT descriptors and tables for a list of lengths, in device memory owned by *allocs
+// (used by the Fourier-Wigner plans, which have no spin plan around them).
+template <typename T>
+static int upload_to(std::vector<void*>* allocs, T** dst, const std::vector<T>& src) {
+  *dst = nullptr;
+  if (src.empty()) return S2B_OK;
+  void* ptr = nullptr;
+  S2B_CK(cudaMalloc(&ptr, src.size() * sizeof(T)));
+  allocs->push_back(ptr);
+  S2B_CK(cudaMemcpy(ptr, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+  *dst = reinterpret_cast<T*>(ptr);
+  return S2B_OK;
+}
+
+static int upload_complex_to(std::vector<void*>* allocs, bool fp64, void** dst,
+                             const std::vector<cd>& src) {
+  if (fp64) {
+    std::vector<double2> v(src.size());
+    for (size_t i = 0; i < src.size(); ++i) v[i] = make_double2(src[i].real(), src[i].imag());
+    double2* d = nullptr;
+    const int rc = upload_to(allocs, &d, v);
+    *dst = d;
+    return rc;
+  }
+  std::vector<float2> v(src.size());
+  for (size_t i = 0; i < src.size(); ++i)
+    v[i] = make_float2((float)src[i].real(), (float)src[i].imag());
+  float2* d = nullptr;
+  const int rc = upload_to(allocs, &d, v);
+  *dst = d;
+  return rc;
+}
+
+int s2b::build_fft_set(const int* lengths, int count, bool fp64, std::vector<void*>* allocs,
+                       FFTSet* out) {
+  FFTBuild fb;
+  out->host.clear();
+  std::vector<int> idx(count);
+  for (int i = 0; i < count; ++i) {
+    if (lengths[i] < 2) return fail(S2B_ERR_INVALID, "FFT length must be >= 2");
+    idx[i] = fb.add(lengths[i]);
+  }
+  for (int i = 0; i < count; ++i) out->host.push_back(fb.descs[idx[i]]);
+  int rc;
+  if ((rc = upload_complex_to(allocs, fp64, &out->tw, fb.tw))) return rc;
+  if ((rc = upload_complex_to(allocs, fp64, &out->chirp, fb.chirp))) return rc;
+  if ((rc = upload_complex_to(allocs, fp64, &out->bf, fb.bf))) return rc;
+  return S2B_OK;
+}
+
 // ----------------------------------------------------------------------------
 // C ABI
 // ----------------------------------------------------------------------------

@@ -5,6 +5,9 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <vector>
+
+#include "s2b_fft.h"
 
 namespace s2b {
 
@@ -27,6 +30,19 @@ int lat_nclass(bool fp64, int L);
 cudaError_t launch_lambda(bool fp64, int L, int spin, int nhalf, const RingInfo* rings, int nrings,
                           int Ls, void* lam, cudaStream_t s);
 int lat_qp(bool fp64, int L);
+
+// FFT descriptors (host copies, in the order of the requested lengths; their table
+// offsets index tw / chirp / bf) and the device tables they refer to.
+struct FFTSet {
+  std::vector<FFTDesc> host;
+  void* tw = nullptr;
+  void* chirp = nullptr;
+  void* bf = nullptr;
+};
+// Builds the set for `count` lengths (each >= 2) in float or double; every device
+// allocation is appended to *allocs (the caller frees them).
+int build_fft_set(const int* lengths, int count, bool fp64, std::vector<void*>* allocs,
+                  FFTSet* out);
 
 // Records msg as the calling thread's s2b_last_error() text and returns code.
 int set_last_error(int code, const char* msg);

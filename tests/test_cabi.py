@@ -86,3 +86,18 @@ def test_no_cpu_fallback_without_gpu():
         pytest.skip("GPU present")
     with pytest.raises(RuntimeError, match="CUDA"):
         s2fft_b200.inverse(np.zeros((8, 15), complex), 8)
+
+
+def test_fourier_wigner_arguments_rejected_on_host(lib):
+    """s2b_fw_plan_create validates L, sampling and precision before any CUDA call."""
+    lib.s2b_fw_plan_create.restype = ctypes.c_int
+    lib.s2b_fw_workspace_size.restype = ctypes.c_size_t
+    lib.s2b_fw_workspace_size.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 5
+    for L, sampling, precision in ((1, 0, 0), (8, 2, 0), (8, 3, 0), (8, 4, 0), (8, 0, 2),
+                                   (8, 1, 7)):
+        p = ctypes.c_void_p()
+        assert lib.s2b_fw_plan_create(L, sampling, precision, ctypes.byref(p)) == 1
+        assert not p.value
+        assert lib.s2b_last_error()
+    assert lib.s2b_fw_plan_create(8, 0, 0, None) == 1
+    assert lib.s2b_fw_workspace_size(None, 0, 1, 2, 0, 1) == 0

@@ -1,0 +1,144 @@
+"""Fourier-Wigner transforms and spin-subset ops on the GPU against upstream's numpy code
+(tests/golden/fourier_wigner.npz, made by tests/golden/make_fourier_wigner.py) and the
+oracle. Tolerances: float64 atol 1e-12 (upstream's own tests/test_fourier_wigner.py),
+float32 relative 1e-5."""
+
+import json
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from tests.conftest import GOLDEN_DIR, relerr
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def fwg():
+    d = np.load(os.path.join(GOLDEN_DIR, "fourier_wigner.npz"))
+    with open(os.path.join(GOLDEN_DIR, "fourier_wigner.json")) as fh:
+        return d, json.load(fh)["cases"]
+
+
+@pytest.fixture(scope="module")
+def s2b():
+    import s2fft_b200
+
+    return s2fft_b200
+
+
+def test_kernel_matches_upstream(fwg, s2b):
+    d, _ = fwg
+    for L in (8, 16):
+        delta, quads = s2b.fourier_wigner.fourier_wigner_kernel(L)
+        assert np.abs(delta.cpu().numpy() - d[f"kernel_L{L}/delta"]).max() < 1e-13
+        assert np.abs(quads.cpu().numpy() - d[f"kernel_L{L}/quads"]).max() < 1e-13
+
+
+@pytest.mark.parametrize("use_upstream_precomps", [False, True])
+def test_transforms_match_upstream_f64(fwg, s2b, use_upstream_precomps):
+    d, cases = fwg
+    fw = s2b.fourier_wigner
+    seen = 0
+    for c in cases:
+        if c["kind"] != "fourier_wigner":
+            continue
+        n, L, N, s, r = c["name"], c["L"], c["N"], c["sampling"], c["reality"]
+        pre = (d[f"kernel_L{L}/delta"], d[f"kernel_L{L}/quads"]) if (
+            use_upstream_precomps and L in (8, 16)) else None
+        f = fw.inverse_transform(d[f"{n}/flmn"], L, N, pre, r, s)
+        np.testing.assert_allclose(f, d[f"{n}/f"], atol=1e-12, err_msg=n)
+        assert (f.dtype == np.float64) if r else (f.dtype == np.complex128)
+        g = fw.forward_transform(d[f"{n}/f"], L, N, pre, r, s)
+        np.testing.assert_allclose(g, d[f"{n}/flmn_fwd"], atol=1e-12, err_msg=n)
+        seen += 1
+    assert seen == 10
+
+
+def test_transforms_f32(fwg, s2b):
+    d, cases = fwg
+    fw = s2b.fourier_wigner
+    for c in cases:
+        if c["kind"] != "fourier_wigner":
+            continue
+        n, L, N, s, r = c["name"], c["L"], c["N"], c["sampling"], c["reality"]
+        f = fw.inverse_transform(d[f"{n}/flmn"], L, N, None, r, s, precision="f32")
+        assert f.dtype == (np.float32 if r else np.complex64)
+        assert relerr(f, d[f"{n}/f"]) < 1e-5, n
+        g = fw.forward_transform(d[f"{n}/f"], L, N, None, r, s, precision="f32")
+        assert relerr(g, d[f"{n}/flmn_fwd"]) < 1e-5, n
+
+
+def test_subset_ops_match_upstream(fwg, s2b):
+    d, cases = fwg
+    ops = s2b.custom_ops
+    for c in cases:
+        if c["kind"] != "subset_ops":
+            continue
+        n, L, N, s, sp = c["name"], c["L"], c["N"], c["sampling"], np.array(c["spins"])
+        DW = s2b.fourier_wigner.fourier_wigner_kernel(L)
+        np.testing.assert_allclose(ops.wigner_subset_to_s2(d[f"{n}/flmn"], sp, DW, L, s),
+                                   d[f"{n}/fs"], atol=1e-12)
+        np.testing.assert_allclose(ops.s2_to_wigner_subset(d[f"{n}/fs"], sp, DW, L, s),
+                                   d[f"{n}/back"], atol=1e-12)
+        np.testing.assert_allclose(ops.so3_to_wigner_subset(d[f"{n}/fso3"], sp, DW, L, N, s),
+                                   d[f"{n}/sub"], atol=1e-12)
+        for fn, x, ref in ((ops.wigner_subset_to_s2, d[f"{n}/flmn"], d[f"{n}/fs"]),
+                           (ops.s2_to_wigner_subset, d[f"{n}/fs"], d[f"{n}/back"])):
+            y = fn(x, sp, DW, L, s, precision="f32")
+            assert relerr(y, ref) < 1e-5, n
+        # device tensors in, device tensors out
+        t = torch.as_tensor(d[f"{n}/flmn"]).cuda()
+        y = ops.wigner_subset_to_s2(t, torch.as_tensor(sp), DW, L, s)
+        assert y.is_cuda and relerr(y.cpu().numpy(), d[f"{n}/fs"]) < 1e-12
+
+
+def test_errors(fwg, s2b):
+    d, _ = fwg
+    with pytest.raises(ValueError):
+        s2b.fourier_wigner.inverse_transform(d["fw0/flmn"], 8, 2, None, False, "gl")
+    with pytest.raises(ValueError):
+        s2b.fourier_wigner.forward_transform(d["fw0/f"], 8, 2, None, False, "healpix")
+    DW = s2b.fourier_wigner.fourier_wigner_kernel(8)
+    with pytest.raises(ValueError):
+        s2b.custom_ops.wigner_subset_to_s2(d["ops0/flmn"], np.array([0, 1]), DW, 8, "mw")
+    with pytest.raises(ValueError):
+        s2b.custom_ops.s2_to_wigner_subset(d["ops0/fs"], np.array([0, -2, 3]), DW, 8, "dh")
+
+
+@pytest.mark.parametrize("sampling,reality", [("mw", False), ("mwss", True)])
+def test_oracle_L40_and_batch(s2b, sampling, reality):
+    """L=40, N=6 against the oracle; a batch of three maps equals three single calls."""
+    L, N = 40, 6
+    rng = np.random.default_rng(5)
+    flmn = np.stack([oracle.signal.generate_flmn(rng, L, N, 0, reality) for _ in range(3)])
+    fw = s2b.fourier_wigner
+    f = fw.inverse_transform(flmn, L, N, None, reality, sampling)
+    ref = oracle.fourier_wigner.inverse_transform(flmn[1], L, N, None, reality, sampling)
+    assert relerr(f[1], ref) < 1e-12
+    for k in range(3):
+        fk = fw.inverse_transform(flmn[k], L, N, None, reality, sampling)
+        assert np.array_equal(fk, f[k])
+    g = fw.forward_transform(f, L, N, None, reality, sampling)
+    assert relerr(g, flmn) < 1e-11
+    gref = oracle.fourier_wigner.forward_transform(f[2], L, N, None, reality, sampling)
+    assert relerr(g[2], gref) < 1e-12
+
+
+def test_round_trip_L128_N8_and_recursion_agreement(s2b):
+    """MW L=128, N=8: forward(inverse(flmn)) = flmn, and the Fourier-Wigner inverse agrees
+    with the recursion-based Wigner inverse of this library."""
+    L, N = 128, 8
+    rng = np.random.default_rng(11)
+    flmn = oracle.signal.generate_flmn(rng, L, N, 0, False)
+    fw = s2b.fourier_wigner
+    f = fw.inverse_transform(flmn, L, N)
+    g = fw.forward_transform(f, L, N)
+    assert relerr(g, flmn) < 1e-10
+    f_rec = s2b.wigner.inverse(flmn, L, N, sampling="mw")
+    assert relerr(f, f_rec) < 1e-9
+    f32 = fw.inverse_transform(flmn, L, N, precision="f32")
+    assert relerr(f32, f) < 1e-5
