@@ -70,9 +70,15 @@ __device__ __forceinline__ R2 mul_ipow(R2 z, int k) {
 }
 
 constexpr int kFwLanes = 128;  // threads of a contraction CTA, one m column each
-constexpr int kFwR = 4;        // output rows (a for the inverse, l for the forward) per thread
-constexpr int kFwE = 4;        // slices per thread
 constexpr int kFwQ = 32;       // summation indices staged per shared-memory chunk
+
+// Output rows (a for the inverse, l for the forward) and slices per thread.
+template <typename Real>
+struct FWTile {
+  static constexpr int R = 4;
+  static constexpr int E = 4;
+  static constexpr int QU = sizeof(Real) == 4 ? 4 : 2;  // summation indices per load batch
+};
 
 template <typename Real>
 struct FWContractParams {
@@ -80,29 +86,34 @@ struct FWContractParams {
   int mwss;
   FWSlices sl;
   const double* delta;  // [L][2L-1][2L-1]
-  const void* in;       // INV: coefficients (slice layout fw_coef_slice); FWD: G [E][2L-1][2L-1]
+  const void* in;       // INV: coefficients (slice layout fw_coef_slice); FWD: Gf [E][L][2L-1]
   void* out;            // INV: Y [E][2L-1][2L-1]; FWD: coefficients
 };
 
-// INV: out[e][a][m] = i^(n-m) e^{i a theta0} sum_{l} c_l D[l][a][m] D[l][a][n] F[e][l][m]
-// FWD: out[e][l][m] = (2pi)^2 i^(m-n) sum_{b} D[l][b][m] D[l][b][n] G[e][b][m]
-// (D[l][x][y] = Delta^l_{x,y}, zero where |x| > l or |y| > l.) Lanes run along m, each
-// thread keeps kFwR x kFwE complex sums; the n-column weights of a chunk of kFwQ summation
-// indices are staged in shared memory and read as broadcasts.
+// With D[l][x][y] = Delta^l_{x,y} (zero where |x| > l or |y| > l) and the reflection
+// D[l][-x][y] = (-1)^(l+y) D[l][x][y] of the planes at pi/2, the products
+// D[l][x][m] D[l][x][n] are even or odd in x with (-1)^(m+n). Hence
+// INV: for a >= 0, P[e][a][m] = sum_l c_l D[l][a][m] D[l][a][n] F[e][l][m], and
+//      Y[a] = i^(n-m) e^{+i a theta0} P[a], Y[-a] = (-1)^(m+n) i^(n-m) e^{-i a theta0} P[a];
+// FWD: out[e][l][m] = (2pi)^2 i^(m-n) sum_{0 <= b <= l} D[l][b][m] D[l][b][n] Gf[e][b][m],
+//      where Gf[b] = G[b] + (-1)^(m+n) G[-b] (b > 0), Gf[0] = G[0] (fw_cols_fwd_kernel).
+// Lanes run along m; each thread keeps R x E complex sums. The n-column weights of a chunk
+// of kFwQ summation indices are staged in shared memory and read as broadcasts. The slice
+// tiles run along blockIdx.x, so the CTAs that read the same planes run together.
 template <typename Real, bool FWD>
 __global__ void __launch_bounds__(kFwLanes) fw_contract_kernel(FWContractParams<Real> p) {
   using R2 = typename C2<Real>::t;
+  constexpr int R = FWTile<Real>::R, E = FWTile<Real>::E, QU = FWTile<Real>::QU;
   const int L = p.L, W = 2 * L - 1;
-  const int ci = blockIdx.x * kFwLanes + threadIdx.x;  // column index m + L - 1
+  const int ci = blockIdx.y * kFwLanes + threadIdx.x;  // column index m + L - 1
   const bool live = ci < W;
   const int m = ci - (L - 1);
-  const int r0 = FWD ? blockIdx.y * kFwR : (int)blockIdx.y * kFwR - (L - 1);
-  const int rhi = L - 1;  // last output row (a or l)
-  const int e0 = blockIdx.z * kFwE;
+  const int r0 = blockIdx.z * R;  // first output row (a >= 0, or l)
+  const int e0 = blockIdx.x * E;
 
-  __shared__ Real wn[kFwQ][kFwR][kFwE];
-  __shared__ int nsh[kFwE];
-  if (threadIdx.x < kFwE) {
+  __shared__ Real wn[kFwQ][R][E];
+  __shared__ int nsh[E];
+  if (threadIdx.x < E) {
     const int e = e0 + threadIdx.x;
     int n = e < p.E ? fw_n(p.sl, e % p.sl.S) : 0;
     if (n > L - 1 || n < -(L - 1)) n = L;  // out of range: weights zero below
@@ -112,48 +123,42 @@ __global__ void __launch_bounds__(kFwLanes) fw_contract_kernel(FWContractParams<
 
   // summation range of the tile
   int qlo, qhi;
-  int nmin = L;
-  for (int s = 0; s < kFwE; ++s)
-    if (e0 + s < p.E) nmin = min(nmin, abs(nsh[s]));
   if (FWD) {
-    const int lmax = min(r0 + kFwR - 1, L - 1);
-    qlo = -lmax;
-    qhi = lmax;
+    qlo = 0;
+    qhi = min(r0 + R - 1, L - 1);
   } else {
-    int amin = L;
-    for (int j = 0; j < kFwR; ++j) {
-      const int a = r0 + j;
-      if (a <= rhi) amin = min(amin, abs(a));
-    }
-    const int cl = blockIdx.x * kFwLanes - (L - 1);
+    int nmin = L;
+    for (int s = 0; s < E; ++s)
+      if (e0 + s < p.E) nmin = min(nmin, abs(nsh[s]));
+    const int cl = blockIdx.y * kFwLanes - (L - 1);
     const int ch = min(cl + kFwLanes - 1, L - 1);
     const int mmin = (cl <= 0 && ch >= 0) ? 0 : min(abs(cl), abs(ch));
-    qlo = max(max(amin, nmin), mmin);
+    qlo = max(max(r0, nmin), mmin);
     qhi = L - 1;
   }
 
-  R2 acc[kFwR][kFwE];
+  R2 acc[R][E];
 #pragma unroll
-  for (int j = 0; j < kFwR; ++j)
+  for (int j = 0; j < R; ++j)
 #pragma unroll
-    for (int s = 0; s < kFwE; ++s) acc[j][s] = czero<R2>();
+    for (int s = 0; s < E; ++s) acc[j][s] = czero<R2>();
 
   const R2* X = reinterpret_cast<const R2*>(p.in);
-  long xoff[kFwE];
+  long xoff[E];
 #pragma unroll
-  for (int s = 0; s < kFwE; ++s) {
+  for (int s = 0; s < E; ++s) {
     const int e = min(e0 + s, p.E - 1);
-    xoff[s] = FWD ? (long)e * W * W : fw_coef_slice(p.sl, e) * (long)L * W;
+    xoff[s] = (FWD ? (long)e : fw_coef_slice(p.sl, e)) * (long)L * W;
   }
 
   const double pi = 3.141592653589793;
   for (int q0 = qlo; q0 <= qhi; q0 += kFwQ) {
     // stage the n-column weights of this chunk
-    for (int t = threadIdx.x; t < kFwQ * kFwR * kFwE; t += kFwLanes) {
-      const int qq = t / (kFwR * kFwE), j = (t / kFwE) % kFwR, s = t % kFwE;
+    for (int t = threadIdx.x; t < kFwQ * R * E; t += kFwLanes) {
+      const int qq = t / (R * E), j = (t / E) % R, s = t % E;
       const int q = q0 + qq, r = r0 + j, n = nsh[s];
       double w = 0.0;
-      if (q <= qhi && r <= rhi && n < L && e0 + s < p.E) {
+      if (q <= qhi && r <= L - 1 && n < L && e0 + s < p.E) {
         if (FWD)  // D[l = r][b = q][n]
           w = __ldg(p.delta + ((long)r * W + (q + L - 1)) * W + (n + L - 1));
         else      // c_l D[l = q][a = r][n]
@@ -165,23 +170,34 @@ __global__ void __launch_bounds__(kFwLanes) fw_contract_kernel(FWContractParams<
     __syncthreads();
     const int qend = min(kFwQ, qhi - q0 + 1);
     if (live) {
-      for (int qq = 0; qq < qend; ++qq) {
-        const int q = q0 + qq;
-        R2 x[kFwE];
+      // QU summation indices per step, all their loads issued before the arithmetic
+      // (rows past L-1 and indices past qhi read row L-1 / index qhi and get weight 0)
+      for (int qq0 = 0; qq0 < qend; qq0 += QU) {
+        R2 x[QU][E];
+        Real w1[QU][R];
 #pragma unroll
-        for (int s = 0; s < kFwE; ++s)
-          x[s] = FWD ? X[xoff[s] + (long)(q + L - 1) * W + ci] : X[xoff[s] + (long)q * W + ci];
+        for (int u = 0; u < QU; ++u) {
+          const int q = q0 + min(qq0 + u, qend - 1);
 #pragma unroll
-        for (int j = 0; j < kFwR; ++j) {
-          const int r = r0 + j;
-          if (r > rhi) continue;
-          const Real w1 = FWD ? (Real)__ldg(p.delta + ((long)r * W + (q + L - 1)) * W + ci)
-                              : (Real)__ldg(p.delta + ((long)q * W + (r + L - 1)) * W + ci);
+          for (int s = 0; s < E; ++s) x[u][s] = X[xoff[s] + (long)q * W + ci];
 #pragma unroll
-          for (int s = 0; s < kFwE; ++s) {
-            const Real w = w1 * wn[qq][j][s];
-            acc[j][s].x = fma(w, x[s].x, acc[j][s].x);
-            acc[j][s].y = fma(w, x[s].y, acc[j][s].y);
+          for (int j = 0; j < R; ++j) {
+            const int r = min(r0 + j, L - 1);
+            w1[u][j] = FWD ? (Real)__ldg(p.delta + ((long)r * W + (q + L - 1)) * W + ci)
+                           : (Real)__ldg(p.delta + ((long)q * W + (r + L - 1)) * W + ci);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < QU; ++u) {
+          if (qq0 + u >= qend) break;
+#pragma unroll
+          for (int j = 0; j < R; ++j) {
+#pragma unroll
+            for (int s = 0; s < E; ++s) {
+              const Real w = w1[u][j] * wn[qq0 + u][j][s];
+              acc[j][s].x = fma(w, x[u][s].x, acc[j][s].x);
+              acc[j][s].y = fma(w, x[u][s].y, acc[j][s].y);
+            }
           }
         }
       }
@@ -192,32 +208,41 @@ __global__ void __launch_bounds__(kFwLanes) fw_contract_kernel(FWContractParams<
 
   R2* O = reinterpret_cast<R2*>(p.out);
 #pragma unroll
-  for (int s = 0; s < kFwE; ++s) {
+  for (int s = 0; s < E; ++s) {
     const int e = e0 + s;
     if (e >= p.E) continue;
     const int n = nsh[s] == L ? 0 : nsh[s];
 #pragma unroll
-    for (int j = 0; j < kFwR; ++j) {
+    for (int j = 0; j < R; ++j) {
       const int r = r0 + j;
-      if (r > rhi) continue;
-      R2 v = acc[j][s];
+      if (r > L - 1) continue;
       if (FWD) {
         const Real sc = (Real)(4.0 * pi * pi);
-        v = mul_ipow(v, m - n);
+        R2 v = mul_ipow(acc[j][s], m - n);
         v.x *= sc;
         v.y *= sc;
         O[fw_coef_slice(p.sl, e) * (long)L * W + (long)r * W + ci] = v;
       } else {
-        v = mul_ipow(v, n - m);
-        if (!p.mwss) {  // e^{i a pi / (2L-1)}
+        const R2 v = mul_ipow(acc[j][s], n - m);
+        R2* Y = O + (long)e * W * W;
+        if (p.mwss) {
+          Y[(long)(r + L - 1) * W + ci] = v;
+          if (r > 0) Y[(long)(L - 1 - r) * W + ci] = (((m + n) & 1) ? cscale(v, Real(-1)) : v);
+        } else {  // e^{+-i a pi / (2L-1)}
           double sn, cs;
           sincospi((double)r / (double)W, &sn, &cs);
           const Real c = (Real)cs, sv = (Real)sn;
-          const R2 u = v;
-          v.x = u.x * c - u.y * sv;
-          v.y = u.x * sv + u.y * c;
+          R2 u;
+          u.x = v.x * c - v.y * sv;
+          u.y = v.x * sv + v.y * c;
+          Y[(long)(r + L - 1) * W + ci] = u;
+          if (r > 0) {
+            const Real sg = ((m + n) & 1) ? Real(-1) : Real(1);
+            u.x = sg * (v.x * c + v.y * sv);
+            u.y = sg * (v.y * c - v.x * sv);
+            Y[(long)(L - 1 - r) * W + ci] = u;
+          }
         }
-        O[(long)e * W * W + (long)(r + L - 1) * W + ci] = v;
       }
     }
   }
@@ -296,7 +321,8 @@ __global__ void __launch_bounds__(512) fw_rows_fwd_kernel(FWFftParams<Real> p) {
   }
 }
 
-// Forward, beta: column m of S[e] -> G[e][b][m], |b| <= L-1 (fourier_wigner.py:258-292).
+// Forward, beta: column m of S[e] -> G[b], |b| <= L-1 (fourier_wigner.py:258-292), stored
+// folded as Gf[e][b][m], 0 <= b <= L-1 (see fw_contract_kernel).
 // Shared memory: the DFT buffer (padded working length) and a buffer of 4L-3 values.
 template <typename Real>
 __global__ void __launch_bounds__(512) fw_cols_fwd_kernel(FWFftParams<Real> p, int bufM) {
@@ -345,13 +371,18 @@ __global__ void __launch_bounds__(512) fw_cols_fwd_kernel(FWFftParams<Real> p, i
   }
   __syncthreads();
   dft_run<Real>(s, p.dP, p.tb, false, [&](int k) { return tmp[k]; });
+  // folded rows b >= 0: Gf[b] = G[b] + (-1)^(m+n) G[-b] (b > 0), Gf[0] = G[0]
   const Real iP = (Real)(1.0 / P);
-  R2* G = reinterpret_cast<R2*>(p.out) + (long)e * W * W;
-  for (int b = -(L - 1) + (int)threadIdx.x; b <= L - 1; b += blockDim.x)
-    G[(long)(b + L - 1) * W + col] = cscale(dft_get<Real>(s, p.dP, p.tb, false, pmod(b, P)), iP);
+  R2* G = reinterpret_cast<R2*>(p.out) + (long)e * L * W;
+  for (int b = threadIdx.x; b <= L - 1; b += blockDim.x) {
+    R2 v = dft_get<Real>(s, p.dP, p.tb, false, b);
+    if (b > 0) v = cadd(v, cscale(dft_get<Real>(s, p.dP, p.tb, false, P - b), sgn));
+    G[(long)b * W + col] = cscale(v, iP);
+  }
 }
 
-// Gamma DFT of the full transform, one thread per (map, pixel), kGamK outputs per pass.
+// Gamma DFT of the full transform: one thread per (map, pixel) and block of kGamK outputs
+// (blockIdx.y).
 //   inverse: f[b][g][px] = sum_n x[N-1+n][b][px] e^{+2 pi i n g / G}, n in [-(N-1), N-1];
 //            reality: real output from n >= 0 (irfft: n = 0 real part, n > 0 doubled)
 //   forward: x[N-1+n][b][px] = (1/G) sum_g f[b][g][px] e^{-2 pi i n g / G}, n in [n0, N-1]
@@ -377,7 +408,8 @@ __global__ void fw_gamma_kernel(const void* in, void* out, int B, int N, long np
     const long b = i / npix, px = i % npix;
     if (!FWD) {
       const R2* x = reinterpret_cast<const R2*>(in);
-      for (int g0 = 0; g0 < G; g0 += kGamK) {
+      {
+        const int g0 = blockIdx.y * kGamK;
         double re[kGamK], im[kGamK];
 #pragma unroll
         for (int u = 0; u < kGamK; ++u) re[u] = im[u] = 0.0;
@@ -416,7 +448,8 @@ __global__ void fw_gamma_kernel(const void* in, void* out, int B, int N, long np
       }
     } else {
       R2* x = reinterpret_cast<R2*>(out);
-      for (int n0 = nlo; n0 < N; n0 += kGamK) {
+      {
+        const int n0 = nlo + (int)blockIdx.y * kGamK;
         double re[kGamK], im[kGamK];
 #pragma unroll
         for (int u = 0; u < kGamK; ++u) re[u] = im[u] = 0.0;
@@ -620,9 +653,8 @@ int contract(const s2b_fw_plan* p, bool fwd, int E, const FWSlices& sl, const do
   c.in = in;
   c.out = out;
   const int W = 2 * p->L - 1;
-  const int rows = fwd ? p->L : W;
-  dim3 grid((W + kFwLanes - 1) / kFwLanes, (rows + kFwR - 1) / kFwR, (E + kFwE - 1) / kFwE);
-  if (grid.z > 65535) return fw_fail(S2B_ERR_INVALID, "too many slices in one call");
+  constexpr int R = FWTile<Real>::R, Et = FWTile<Real>::E;
+  dim3 grid((E + Et - 1) / Et, (W + kFwLanes - 1) / kFwLanes, (p->L + R - 1) / R);
   if (fwd)
     fw_contract_kernel<Real, true><<<grid, kFwLanes, 0, st>>>(c);
   else
@@ -690,12 +722,18 @@ template <typename Real>
 int gamma_dft(bool fwd, const void* in, void* out, int B, int N, long npix, int reality,
               cudaStream_t st) {
   const long tot = (long)B * npix;
+  const int G = 2 * N - 1;
+  const int nout = fwd ? (reality ? N : G) : G;
+  const int chunks = (nout + kGamK - 1) / kGamK;
   const int blocks = (int)std::min<long>((tot + 255) / 256, 4L * 148 * 8);
-  const size_t smem = (size_t)(2 * N - 1) * sizeof(double2);
+  const size_t smem = (size_t)G * sizeof(double2);
+  if (chunks > 65535) return fw_fail(S2B_ERR_INVALID, "N too large for the gamma DFT");
   if (fwd)
-    fw_gamma_kernel<Real, true><<<blocks, 256, smem, st>>>(in, out, B, N, npix, reality);
+    fw_gamma_kernel<Real, true><<<dim3(blocks, chunks), 256, smem, st>>>(in, out, B, N, npix,
+                                                                        reality);
   else
-    fw_gamma_kernel<Real, false><<<blocks, 256, smem, st>>>(in, out, B, N, npix, reality);
+    fw_gamma_kernel<Real, false><<<dim3(blocks, chunks), 256, smem, st>>>(in, out, B, N, npix,
+                                                                         reality);
   FW_CK(cudaGetLastError());
   return S2B_OK;
 }
