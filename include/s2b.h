@@ -225,8 +225,9 @@ int s2b_rotate_flms(int L, int batch, int precision, double alpha, double beta, 
 int s2b_rotate_dls(int L, double beta, double* dl, void* ws, size_t ws_bytes, void* stream);
 
 /* Fourier-Wigner transforms on SO(3) and the spin-subset lifting ops (mw / mwss only).
- * A plan holds the FFT tables of one (L, sampling, precision); it is independent of N,
- * of the batch and of the spin subset. Layouts (complex interleaved, double for S2B_F64,
+ * A plan holds the FFT tables of one (L, N, sampling, precision), N the azimuthal
+ * band-limit of the full transforms (1 <= N <= L; the subset ops take any plan of the L,
+ * sampling and precision); it is independent of the batch and of the spin subset. Layouts (complex interleaved, double for S2B_F64,
  * float for S2B_F32):
  *   flmn  [batch][2N-1][L][2L-1]            f [batch][2N-1][ntheta][nphi] (real if reality)
  *   spin-subset coefficients [batch][nspins][L][2L-1], maps [batch][nspins][ntheta][nphi],
@@ -253,16 +254,17 @@ enum s2b_fw_op {
   S2B_FW_S2_TO_SUBSET = 3,
   S2B_FW_SO3_TO_SUBSET = 4
 };
-int s2b_fw_plan_create(int L, int sampling, int precision, s2b_fw_plan** plan);
+int s2b_fw_plan_create(int L, int N, int sampling, int precision, s2b_fw_plan** plan);
 int s2b_fw_plan_destroy(s2b_fw_plan* plan);
 int s2b_fw_quads(s2b_fw_plan* plan, void* quads, void* stream);
-/* N and reality are used by the full transforms, nspins by the subset ops. */
-size_t s2b_fw_workspace_size(const s2b_fw_plan* plan, int op, int batch, int N, int reality,
+/* reality is used by the full transforms, nspins by the subset ops. */
+size_t s2b_fw_workspace_size(const s2b_fw_plan* plan, int op, int batch, int reality,
                              int nspins);
-int s2b_fw_inverse(s2b_fw_plan* plan, int batch, int N, int reality, const double* delta,
+/* Full transforms with the plan's N. */
+int s2b_fw_inverse(s2b_fw_plan* plan, int batch, int reality, const double* delta,
                    const void* flmn, void* f, void* workspace, size_t workspace_bytes,
                    void* stream);
-int s2b_fw_forward(s2b_fw_plan* plan, int batch, int N, int reality, const double* delta,
+int s2b_fw_forward(s2b_fw_plan* plan, int batch, int reality, const double* delta,
                    const void* quads, const void* f, void* flmn, void* workspace,
                    size_t workspace_bytes, void* stream);
 /* spins: device int32 [nspins]. */

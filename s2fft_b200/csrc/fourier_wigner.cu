@@ -491,6 +491,59 @@ __global__ void fw_gamma_kernel(const void* in, void* out, int B, int N, long np
   }
 }
 
+// Gamma DFT by the block FFT (2N-1 >= kGamFFTMin): one CTA per (pixel, map), the
+// 2N-1 values of the pixel gathered with stride (map count x pixels). Same sums as
+// fw_gamma_kernel.
+constexpr int kGamFFTMin = 24;
+
+template <typename Real, bool FWD>
+__global__ void __launch_bounds__(512) fw_gamma_fft_kernel(const void* in, void* out, int B,
+                                                           int N, long npix, int reality,
+                                                           FFTDesc dg, FFTTables<Real> tb) {
+  using R2 = typename C2<Real>::t;
+  extern __shared__ unsigned char fw_smem[];
+  R2* s = reinterpret_cast<R2*>(fw_smem);
+  const long px = blockIdx.x;
+  const long b = blockIdx.y;
+  const int G = 2 * N - 1;
+  if (!FWD) {
+    const R2* x = reinterpret_cast<const R2*>(in);
+    dft_run<Real>(s, dg, tb, true, [&](int k) {
+      const int n = k <= N - 1 ? k : k - G;
+      if (!reality) return x[((long)(N - 1 + n) * B + b) * npix + px];
+      // Hermitian: x_{-n} = conj(x_n), the imaginary part of x_0 dropped (irfft)
+      R2 v = x[((long)(N - 1 + (n < 0 ? -n : n)) * B + b) * npix + px];
+      if (n < 0) v.y = -v.y;
+      if (n == 0) v.y = Real(0);
+      return v;
+    });
+    for (int g = threadIdx.x; g < G; g += blockDim.x) {
+      const R2 v = dft_get<Real>(s, dg, tb, true, g);
+      const long o = (b * G + g) * npix + px;
+      if (reality)
+        reinterpret_cast<Real*>(out)[o] = v.x;
+      else
+        reinterpret_cast<R2*>(out)[o] = v;
+    }
+  } else {
+    dft_run<Real>(s, dg, tb, false, [&](int k) {
+      const long o = (b * G + k) * npix + px;
+      if (reality) {
+        R2 v;
+        v.x = reinterpret_cast<const Real*>(in)[o];
+        v.y = Real(0);
+        return v;
+      }
+      return reinterpret_cast<const R2*>(in)[o];
+    });
+    R2* x = reinterpret_cast<R2*>(out);
+    const Real sc = (Real)(1.0 / G);
+    for (int n = (reality ? 0 : -(N - 1)) + (int)threadIdx.x; n < N; n += blockDim.x)
+      x[((long)(N - 1 + n) * B + b) * npix + px] =
+          cscale(dft_get<Real>(s, dg, tb, false, n < 0 ? n + G : n), sc);
+  }
+}
+
 // quads[j] = sum_{|k| <= 2L-2} w(-k) e^{+2 pi i k j / (4L-3)}, w the MW weights
 // (w(+-1) = +-i pi/2, w(even k) = 2/(1-k^2), else 0); construct.py:629-634.
 __global__ void fw_quads_kernel(int L, double2* quads) {
@@ -554,11 +607,12 @@ __global__ void fw_gamma_subset_kernel(const void* fin, void* xout, int O, int G
 using namespace s2b;
 
 struct s2b_fw_plan {
-  int L, mwss, ntheta, nphi, P;
+  int L, N, mwss, ntheta, nphi, P;
+  bool gamma_fft;  // fft.host[2] is the length-(2N-1) descriptor
   bool fp64;
   int device;
   std::vector<void*> allocs;
-  FFTSet fft;  // host[0]: length nphi, host[1]: length 4L-3
+  FFTSet fft;  // host[0]: length nphi, host[1]: length 4L-3, host[2]: 2N-1 (gamma_fft)
   ~s2b_fw_plan() {
     for (void* a : allocs) cudaFree(a);
   }
@@ -719,10 +773,31 @@ int forward_chain(const s2b_fw_plan* p, int E, const FWSlices& sl, const double*
 }
 
 template <typename Real>
-int gamma_dft(bool fwd, const void* in, void* out, int B, int N, long npix, int reality,
-              cudaStream_t st) {
-  const long tot = (long)B * npix;
+int gamma_dft(const s2b_fw_plan* p, bool fwd, const void* in, void* out, int B, int N,
+              long npix, int reality, cudaStream_t st) {
   const int G = 2 * N - 1;
+  if (p->gamma_fft && N == p->N) {
+    using R2 = typename C2<Real>::t;
+    const FFTDesc& dg = p->fft.host[2];
+    const size_t smem = (size_t)padded_len(dg.M) * sizeof(R2);
+    if (npix > 2147483647L || B > 65535)
+      return fw_fail(S2B_ERR_INVALID, "too many pixels or maps for the gamma FFT");
+    dim3 grid((unsigned)npix, B);
+    if (fwd) {
+      FW_CK(cudaFuncSetAttribute(fw_gamma_fft_kernel<Real, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      fw_gamma_fft_kernel<Real, true><<<grid, fft_threads_for(dg.M), smem, st>>>(
+          in, out, B, N, npix, reality, dg, tables<Real>(p));
+    } else {
+      FW_CK(cudaFuncSetAttribute(fw_gamma_fft_kernel<Real, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      fw_gamma_fft_kernel<Real, false><<<grid, fft_threads_for(dg.M), smem, st>>>(
+          in, out, B, N, npix, reality, dg, tables<Real>(p));
+    }
+    FW_CK(cudaGetLastError());
+    return S2B_OK;
+  }
+  const long tot = (long)B * npix;
   const int nout = fwd ? (reality ? N : G) : G;
   const int chunks = (nout + kGamK - 1) / kGamK;
   const int blocks = (int)std::min<long>((tot + 255) / 256, 4L * 148 * 8);
@@ -794,10 +869,11 @@ FWSlices spin_slices(int nspins, const int* spins) {
 
 extern "C" {
 
-int s2b_fw_plan_create(int L, int sampling, int precision, s2b_fw_plan** plan) {
+int s2b_fw_plan_create(int L, int N, int sampling, int precision, s2b_fw_plan** plan) {
   if (!plan) return fw_fail(S2B_ERR_INVALID, "plan is NULL");
   *plan = nullptr;
   if (L < 2) return fw_fail(S2B_ERR_INVALID, "Fourier-Wigner transforms need L >= 2");
+  if (N < 1 || N > L) return fw_fail(S2B_ERR_INVALID, "need 1 <= N <= L");
   if (sampling != S2B_MW && sampling != S2B_MWSS)
     return fw_fail(S2B_ERR_INVALID, "Fourier-Wigner algorithm supports mw and mwss sampling only");
   if (precision != S2B_F64 && precision != S2B_F32)
@@ -814,8 +890,10 @@ int s2b_fw_plan_create(int L, int sampling, int precision, s2b_fw_plan** plan) {
     delete p;
     return fw_fail(S2B_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
   }
-  const int lens[2] = {p->nphi, p->P};
-  const int rc = build_fft_set(lens, 2, p->fp64, &p->allocs, &p->fft);
+  p->N = N;
+  p->gamma_fft = 2 * N - 1 >= kGamFFTMin;
+  const int lens[3] = {p->nphi, p->P, 2 * N - 1};
+  const int rc = build_fft_set(lens, p->gamma_fft ? 3 : 2, p->fp64, &p->allocs, &p->fft);
   if (rc) {
     delete p;
     return rc;
@@ -846,9 +924,10 @@ int s2b_fw_quads(s2b_fw_plan* plan, void* quads, void* stream) {
   return S2B_OK;
 }
 
-size_t s2b_fw_workspace_size(const s2b_fw_plan* plan, int op, int batch, int N, int reality,
+size_t s2b_fw_workspace_size(const s2b_fw_plan* plan, int op, int batch, int reality,
                              int nspins) {
   if (!plan || batch < 1) return 0;
+  const int N = plan->N;
   switch (op) {
     case S2B_FW_INVERSE:
     case S2B_FW_FORWARD: {
@@ -865,12 +944,12 @@ size_t s2b_fw_workspace_size(const s2b_fw_plan* plan, int op, int batch, int N, 
   }
 }
 
-int s2b_fw_inverse(s2b_fw_plan* plan, int batch, int N, int reality, const double* delta,
+int s2b_fw_inverse(s2b_fw_plan* plan, int batch, int reality, const double* delta,
                    const void* flmn, void* f, void* ws, size_t ws_bytes, void* stream) {
   int rc;
   if ((rc = check_plan(plan))) return rc;
-  if (batch < 1 || N < 1 || N > plan->L)
-    return fw_fail(S2B_ERR_INVALID, "need batch >= 1 and 1 <= N <= L");
+  if (batch < 1) return fw_fail(S2B_ERR_INVALID, "need batch >= 1");
+  const int N = plan->N;
   if ((rc = check_ptrs({delta, flmn, f}))) return rc;
   const FWSlices sl = full_slices(N, reality);
   const int E = batch * sl.S;
@@ -886,17 +965,17 @@ int s2b_fw_inverse(s2b_fw_plan* plan, int batch, int N, int reality, const doubl
     rc = inverse_chain<float>(plan, E, sl, delta, flmn, w, 1, batch, w, lay, st);
   if (rc) return rc;
   const long npix = (long)plan->ntheta * plan->nphi;
-  return plan->fp64 ? gamma_dft<double>(false, w, f, batch, N, npix, reality, st)
-                    : gamma_dft<float>(false, w, f, batch, N, npix, reality, st);
+  return plan->fp64 ? gamma_dft<double>(plan, false, w, f, batch, N, npix, reality, st)
+                    : gamma_dft<float>(plan, false, w, f, batch, N, npix, reality, st);
 }
 
-int s2b_fw_forward(s2b_fw_plan* plan, int batch, int N, int reality, const double* delta,
+int s2b_fw_forward(s2b_fw_plan* plan, int batch, int reality, const double* delta,
                    const void* quads, const void* f, void* flmn, void* ws, size_t ws_bytes,
                    void* stream) {
   int rc;
   if ((rc = check_plan(plan))) return rc;
-  if (batch < 1 || N < 1 || N > plan->L)
-    return fw_fail(S2B_ERR_INVALID, "need batch >= 1 and 1 <= N <= L");
+  if (batch < 1) return fw_fail(S2B_ERR_INVALID, "need batch >= 1");
+  const int N = plan->N;
   if ((rc = check_ptrs({delta, quads, f, flmn}))) return rc;
   const FWSlices sl = full_slices(N, reality);
   const int E = batch * sl.S;
@@ -907,8 +986,8 @@ int s2b_fw_forward(s2b_fw_plan* plan, int batch, int N, int reality, const doubl
   char* w = (char*)ws;
   const long npix = (long)plan->ntheta * plan->nphi;
   // gamma DFT into region A, n-major
-  rc = plan->fp64 ? gamma_dft<double>(true, f, w, batch, N, npix, reality, st)
-                  : gamma_dft<float>(true, f, w, batch, N, npix, reality, st);
+  rc = plan->fp64 ? gamma_dft<double>(plan, true, f, w, batch, N, npix, reality, st)
+                  : gamma_dft<float>(plan, true, f, w, batch, N, npix, reality, st);
   if (rc) return rc;
   const double scale = 1.0 / plan->nphi;
   if (plan->fp64)

@@ -37,11 +37,11 @@ def _fwlib():
         if not _fw_sigs_done:
             vp, ci, sz = ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t
             sigs = {
-                "s2b_fw_plan_create": [ci, ci, ci, ctypes.POINTER(vp)],
+                "s2b_fw_plan_create": [ci, ci, ci, ci, ctypes.POINTER(vp)],
                 "s2b_fw_plan_destroy": [vp],
                 "s2b_fw_quads": [vp, vp, vp],
-                "s2b_fw_inverse": [vp, ci, ci, ci, vp, vp, vp, vp, sz, vp],
-                "s2b_fw_forward": [vp, ci, ci, ci, vp, vp, vp, vp, vp, sz, vp],
+                "s2b_fw_inverse": [vp, ci, ci, vp, vp, vp, vp, sz, vp],
+                "s2b_fw_forward": [vp, ci, ci, vp, vp, vp, vp, vp, sz, vp],
                 "s2b_fw_subset_to_s2": [vp, ci, ci, vp, vp, vp, vp, vp, sz, vp],
                 "s2b_fw_s2_to_subset": [vp, ci, ci, vp, vp, vp, vp, vp, vp, sz, vp],
                 "s2b_fw_so3_to_subset": [vp, ci, ci, ci, vp, vp, vp, vp, vp, vp, sz, vp],
@@ -50,7 +50,7 @@ def _fwlib():
                 fn = getattr(h, name)
                 fn.argtypes = argt
                 fn.restype = ci
-            h.s2b_fw_workspace_size.argtypes = [vp, ci, ci, ci, ci, ci]
+            h.s2b_fw_workspace_size.argtypes = [vp, ci, ci, ci, ci]
             h.s2b_fw_workspace_size.restype = sz
             _fw_sigs_done = True
     return h
@@ -60,19 +60,20 @@ OP_INVERSE, OP_FORWARD, OP_SUBSET_TO_S2, OP_S2_TO_SUBSET, OP_SO3_TO_SUBSET = ran
 
 
 class FWPlan:
-    """FFT tables of one (L, sampling, precision) on one device."""
+    """FFT tables of one (L, N, sampling, precision) on one device."""
 
-    def __init__(self, device, L, sampling, precision):
-        self.device, self.L, self.sampling, self.precision = device, L, sampling, precision
+    def __init__(self, device, L, N, sampling, precision):
+        self.device, self.L, self.N = device, L, N
+        self.sampling, self.precision = sampling, precision
         ptr = ctypes.c_void_p()
         with torch.cuda.device(device):
-            _lib.check(_fwlib().s2b_fw_plan_create(L, _lib.SAMPLING[sampling],
+            _lib.check(_fwlib().s2b_fw_plan_create(L, N, _lib.SAMPLING[sampling],
                                                    _lib.PRECISION[precision], ctypes.byref(ptr)))
         self.ptr = ptr
         self._ws = {}
 
-    def workspace(self, op, batch, N=1, reality=False, nspins=1):
-        n = int(_fwlib().s2b_fw_workspace_size(self.ptr, op, batch, N, int(bool(reality)),
+    def workspace(self, op, batch, reality=False, nspins=1):
+        n = int(_fwlib().s2b_fw_workspace_size(self.ptr, op, batch, int(bool(reality)),
                                                 nspins))
         cur = self._ws.get("ws")
         if cur is None or cur.numel() < n:
@@ -93,12 +94,12 @@ _kernels: dict = {}
 _plans_lock = threading.Lock()
 
 
-def get_plan(device, L, sampling, precision) -> FWPlan:
-    key = (str(device), L, sampling, precision)
+def get_plan(device, L, sampling, precision, N=1) -> FWPlan:
+    key = (str(device), L, N, sampling, precision)
     with _plans_lock:
         p = _plans.get(key)
         if p is None:
-            p = FWPlan(device, L, sampling, precision)
+            p = FWPlan(device, L, N, sampling, precision)
             _plans[key] = p
     return p
 
@@ -172,9 +173,9 @@ def inverse_transform(flmn, L: int, N: int, precomps=None, reality: bool = False
     rdt = torch.float64 if precision == "f64" else torch.float32
     out = torch.empty(bs + (2 * N - 1, nth, nph), dtype=rdt if reality else cdt,
                       device=x.device)
-    plan = get_plan(x.device, L, s, precision)
-    ws = plan.workspace(OP_INVERSE, B, N, reality)
-    _lib.check(_fwlib().s2b_fw_inverse(plan.ptr, B, N, int(bool(reality)), delta.data_ptr(),
+    plan = get_plan(x.device, L, s, precision, N)
+    ws = plan.workspace(OP_INVERSE, B, reality)
+    _lib.check(_fwlib().s2b_fw_inverse(plan.ptr, B, int(bool(reality)), delta.data_ptr(),
                                        x.data_ptr(), out.data_ptr(), ws.data_ptr(), ws.numel(),
                                        _lib.stream_handle(x.device)))
     return _ret(out, was_np, odev)
@@ -201,9 +202,9 @@ def forward_transform(f, L: int, N: int, precomps=None, reality: bool = False,
     B = int(np.prod(bs)) if bs else 1
     delta, quads = _precomps(precomps, L, x.device)
     out = torch.empty(bs + (2 * N - 1, L, 2 * L - 1), dtype=cdt, device=x.device)
-    plan = get_plan(x.device, L, s, precision)
-    ws = plan.workspace(OP_FORWARD, B, N, reality)
-    _lib.check(_fwlib().s2b_fw_forward(plan.ptr, B, N, int(bool(reality)), delta.data_ptr(),
+    plan = get_plan(x.device, L, s, precision, N)
+    ws = plan.workspace(OP_FORWARD, B, reality)
+    _lib.check(_fwlib().s2b_fw_forward(plan.ptr, B, int(bool(reality)), delta.data_ptr(),
                                        quads.data_ptr(), x.data_ptr(), out.data_ptr(),
                                        ws.data_ptr(), ws.numel(), _lib.stream_handle(x.device)))
     return _ret(out, was_np, odev)

@@ -92,12 +92,12 @@ def test_fourier_wigner_arguments_rejected_on_host(lib):
     """s2b_fw_plan_create validates L, sampling and precision before any CUDA call."""
     lib.s2b_fw_plan_create.restype = ctypes.c_int
     lib.s2b_fw_workspace_size.restype = ctypes.c_size_t
-    lib.s2b_fw_workspace_size.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 5
-    for L, sampling, precision in ((1, 0, 0), (8, 2, 0), (8, 3, 0), (8, 4, 0), (8, 0, 2),
-                                   (8, 1, 7)):
+    lib.s2b_fw_workspace_size.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 4
+    for L, N, sampling, precision in ((1, 1, 0, 0), (8, 2, 2, 0), (8, 2, 3, 0), (8, 2, 4, 0),
+                                      (8, 2, 0, 2), (8, 2, 1, 7), (8, 0, 0, 0), (8, 9, 1, 0)):
         p = ctypes.c_void_p()
-        assert lib.s2b_fw_plan_create(L, sampling, precision, ctypes.byref(p)) == 1
+        assert lib.s2b_fw_plan_create(L, N, sampling, precision, ctypes.byref(p)) == 1
         assert not p.value
         assert lib.s2b_last_error()
-    assert lib.s2b_fw_plan_create(8, 0, 0, None) == 1
-    assert lib.s2b_fw_workspace_size(None, 0, 1, 2, 0, 1) == 0
+    assert lib.s2b_fw_plan_create(8, 2, 0, 0, None) == 1
+    assert lib.s2b_fw_workspace_size(None, 0, 1, 0, 1) == 0
