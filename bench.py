@@ -459,6 +459,44 @@ def run_healpix_iter(torch, nside=256, L=512, steps=5, warmup=2):
     return out
 
 
+def run_so3(torch, L=128, N=8, steps=10, warmup=3):
+    """SO(3), MW, L=128, N=8, one complex signal: inverse + forward by the Fourier-Wigner
+    transforms (Delta-plane contraction + FFTs) and by the recursion-based Wigner
+    transforms (2N-1 spin transforms + gamma DFT), float32 and float64."""
+    import s2fft_b200
+    from s2fft_b200 import fourier_wigner as fw
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    rng = np.random.default_rng(8)
+    # slice n holds a spin -n field: zero below l = |n|
+    flmn = np.stack([seeded_flm(rng, L, n) for n in range(-(N - 1), N)])
+    flmn64 = torch.from_numpy(flmn).to(dev)
+    pre = fw.fourier_wigner_kernel(L)
+    ref_f = fw.inverse_transform(flmn64, L, N, pre)
+    out = {"workload": f"SO(3) mw L={L} N={N}, complex, inverse + forward, one signal"}
+    for prec in ("f32", "f64"):
+        x = flmn64.to(torch.complex64 if prec == "f32" else torch.complex128)
+        f = fw.inverse_transform(x, L, N, pre, precision=prec)
+        ms_fw = _time(torch, lambda: fw.forward_transform(
+            fw.inverse_transform(x, L, N, pre, precision=prec), L, N, pre, precision=prec),
+            steps, warmup, flush)
+        fr = s2fft_b200.wigner.inverse(x, L, N, sampling="mw", precision=prec)
+        ms_rec = _time(torch, lambda: s2fft_b200.wigner.forward(
+            s2fft_b200.wigner.inverse(x, L, N, sampling="mw", precision=prec), L, N,
+            sampling="mw", precision=prec), steps, warmup, flush)
+        g = fw.forward_transform(f, L, N, pre, precision=prec)
+        err_inv = ((f.to(torch.complex128) - ref_f).abs().max() / ref_f.abs().max()).item()
+        err_rt = ((g.to(torch.complex128) - flmn64).abs().max() / flmn64.abs().max()).item()
+        err_rec = ((fr.to(torch.complex128) - ref_f).abs().max() / ref_f.abs().max()).item()
+        out[prec] = {"fourier_wigner_ms": ms_fw, "fourier_wigner_per_s": 1e3 / ms_fw,
+                     "recursion_ms": ms_rec, "recursion_per_s": 1e3 / ms_rec,
+                     "inverse_max_rel_err_vs_fw_f64": err_inv,
+                     "roundtrip_max_rel_err": err_rt,
+                     "recursion_vs_fw_f64_max_rel": err_rec}
+    return out
+
+
 # ---------------------------------------------------------------------------
 # CPU reference: the float64 numpy restatement of the upstream algorithm
 # (oracle/), on a bounded sample: the first k m-steps of every latitudinal
@@ -654,6 +692,7 @@ def main():
         line["batched_precompute"] = run_batched_precompute(torch)
         line["healpix_iter3"] = run_healpix_iter(torch)
         line["batched_uneven"] = run_batched_uneven(torch)
+        line["so3_fourier_wigner"] = run_so3(torch)
     if not args.no_cpu_baseline and not args.profile_case:
         c = cpu_sample(args.L, args.cpu_budget)
         line["cpu_baseline"] = {"value": c["value"], "unit": UNIT, "cores": c["cores"],
