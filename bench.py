@@ -169,6 +169,17 @@ def simt_peak_tflops(torch, fp64):
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
+def job_rates(torch, ms, counts, world, dist=None, device="cpu"):
+    """Whole-job rates of the replicas: every timed leg i takes the slowest rank's time
+    (max over ranks, one all-reduce) and rate_i = world * counts_i / time_i. Returns
+    (max times in ms, rates per second)."""
+    t = torch.tensor([float(x) for x in ms], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    mx = t.tolist()
+    return mx, [world * c / (m * 1e-3) for c, m in zip(counts, mx)]
+
+
 def run_ours(args, rank, world, torch, dist):
     import s2fft_b200
     from s2fft_b200 import _lib
@@ -302,13 +313,8 @@ def run_ours(args, rank, world, torch, dist):
     if not torch.equal(host_out[j_last], y_last.cpu()):
         raise RuntimeError("pipelined end-to-end result differs from the device result")
 
-    t = torch.tensor([ms32, ms64, e2e_ms], dtype=torch.float64, device=dev)
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms32, ms64, e2e_ms = t.tolist()
-    value = world * steps / (ms32 * 1e-3)
-    value64 = world * max(3, steps // 4) / (ms64 * 1e-3)
-    e2e = world * e_steps / (e2e_ms * 1e-3)
+    (ms32, ms64, e2e_ms), (value, value64, e2e) = job_rates(
+        torch, [ms32, ms64, e2e_ms], [steps, max(3, steps // 4), e_steps], world, dist, dev)
     return dict(value=value, value64=value64, e2e=e2e, ms32=ms32 / steps, lat32=lat32,
                 lat64=lat64, err32=err32, err64=err64, err_mixed=err_mixed, clocks=clk,
                 T_inv=T_inv, T_fwd=T_fwd, T_fwd_exec=T_fwd_exec, h2d=host_in[0].numel() * 8, d2h=host_out[0].numel() * 8)

@@ -547,11 +547,13 @@ __global__ void __launch_bounds__(512) fw_gamma_fft_kernel(const void* in, void*
 // quads[j] = sum_{|k| <= 2L-2} w(-k) e^{+2 pi i k j / (4L-3)}, w the MW weights
 // (w(+-1) = +-i pi/2, w(even k) = 2/(1-k^2), else 0); construct.py:629-634.
 __global__ void fw_quads_kernel(int L, double2* quads) {
+  // one warp per output j, the 4L-3 terms split over the lanes and summed by shuffles
   const int P = 4 * L - 3;
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= P) return;
+  const int j = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (j >= P) return;  // whole warps leave together (blockDim is a multiple of 32)
   double re = 0.0, im = 0.0;
-  for (int k = -(2 * L - 2); k <= 2 * L - 2; ++k) {
+  for (int k = -(2 * L - 2) + lane; k <= 2 * L - 2; k += 32) {
     const int mk = -k;
     double wr = 0.0, wi = 0.0;
     if (mk == 1)
@@ -568,7 +570,11 @@ __global__ void fw_quads_kernel(int L, double2* quads) {
     re += wr * cs - wi * sn;
     im += wr * sn + wi * cs;
   }
-  quads[j] = make_double2(re, im);
+  for (int o = 16; o > 0; o >>= 1) {
+    re += __shfl_xor_sync(0xffffffffu, re, o);
+    im += __shfl_xor_sync(0xffffffffu, im, o);
+  }
+  if (lane == 0) quads[j] = make_double2(re, im);
 }
 
 // Gamma DFT at a spin subset: x[g][k][px] = (1/G) sum_c f[g][c][px] e^{-2 pi i c n_k / G}
@@ -918,8 +924,8 @@ int s2b_fw_quads(s2b_fw_plan* plan, void* quads, void* stream) {
   int rc;
   if ((rc = check_plan(plan))) return rc;
   if ((rc = check_ptrs({quads}))) return rc;
-  fw_quads_kernel<<<(plan->P + 127) / 128, 128, 0, (cudaStream_t)stream>>>(plan->L,
-                                                                           (double2*)quads);
+  fw_quads_kernel<<<(plan->P + 3) / 4, 128, 0, (cudaStream_t)stream>>>(plan->L,
+                                                                       (double2*)quads);
   FW_CK(cudaGetLastError());
   return S2B_OK;
 }
