@@ -18,8 +18,10 @@
 //            transform then sums over n (gamma DFT, fw_gamma_kernel).
 //   forward: the gamma DFT (fw_gamma_kernel, or fw_gamma_subset_kernel for a spin subset), a DFT
 //            per ring (fw_rows_fwd_kernel), per column m the periodic extension of beta to
-//            [0, 2pi), its DFT, the quadrature as a product with the 4L-3 upsampled weights
-//            between an inverse and a forward DFT of length 4L-3 (fw_cols_fwd_kernel), and
+//            [0, 2pi), its DFT, and the quadrature: upstream multiplies by 4L-3 upsampled
+//            weights between an inverse and a forward DFT of length 4L-3, a convolution
+//            that runs here on a power-of-two length Q >= 4L-1 with weights converted
+//            from the caller's (fw_cols_fwd_kernel, fw_quads_pow2_kernel), and
 //            H[l, m] = (2pi)^2 i^(m-n) sum_b G[b, m] Delta^l_{b,m} Delta^l_{b,n}
 //            (fw_contract_kernel<FWD>).
 //
@@ -256,7 +258,8 @@ struct FWFftParams {
   double scale;
   FFTDesc dphi, dP;
   FFTTables<Real> tb;
-  const void* quads;  // complex128 [4L-3]
+  const void* quads;  // complex128 [P]: the beta-convolution weights (quadsQ)
+  const void* wconv;  // complex128 [4L-3]: w[k], k = -(2L-2) .. 2L-2
   const void* in;
   void* out;
 };
@@ -323,7 +326,9 @@ __global__ void __launch_bounds__(512) fw_rows_fwd_kernel(FWFftParams<Real> p) {
 
 // Forward, beta: column m of S[e] -> G[b], |b| <= L-1 (fourier_wigner.py:258-292), stored
 // folded as Gf[e][b][m], 0 <= b <= L-1 (see fw_contract_kernel).
-// Shared memory: the DFT buffer (padded working length) and a buffer of 4L-3 values.
+// The quadrature is applied as a product between an inverse and a forward DFT of length
+// p.P = Q (power of two, >= 4L-1) with the weights p.quads = quadsQ (fw_quads_pow2_kernel).
+// Shared memory: the DFT buffer (padded working length) and a buffer of Q values.
 template <typename Real>
 __global__ void __launch_bounds__(512) fw_cols_fwd_kernel(FWFftParams<Real> p, int bufM) {
   using R2 = typename C2<Real>::t;
@@ -355,7 +360,17 @@ __global__ void __launch_bounds__(512) fw_cols_fwd_kernel(FWFftParams<Real> p, i
     tmp[b - blo] = v;
   }
   __syncthreads();
-  // zero-padded to 4L-3 and inverse DFT (the upsampled beta samples)
+  // mwss: on upstream's 4L-3 points the spectrum value at b = -L meets the weight at
+  // k = -(2L-2) again at b = L-1 (their distance is exactly 4L-3); kept for parity
+  R2 alias = czero<R2>();
+  if (p.mwss) {
+    const double2 w0 = reinterpret_cast<const double2*>(p.wconv)[0];  // w[-(2L-2)]
+    R2 w;
+    w.x = (Real)w0.x;
+    w.y = (Real)w0.y;
+    alias = cmul(tmp[0], w);
+  }
+  // zero-padded to Q and inverse DFT (the upsampled beta samples)
   const int half = (P - 1) / 2;
   dft_run<Real>(s, p.dP, p.tb, true, [&](int k) {
     const int v = k <= half ? k : k - P;
@@ -377,7 +392,9 @@ __global__ void __launch_bounds__(512) fw_cols_fwd_kernel(FWFftParams<Real> p, i
   for (int b = threadIdx.x; b <= L - 1; b += blockDim.x) {
     R2 v = dft_get<Real>(s, p.dP, p.tb, false, b);
     if (b > 0) v = cadd(v, cscale(dft_get<Real>(s, p.dP, p.tb, false, P - b), sgn));
-    G[(long)b * W + col] = cscale(v, iP);
+    v = cscale(v, iP);
+    if (b == L - 1) v = cadd(v, alias);
+    G[(long)b * W + col] = v;
   }
 }
 
@@ -577,6 +594,59 @@ __global__ void fw_quads_kernel(int L, double2* quads) {
   if (lane == 0) quads[j] = make_double2(re, im);
 }
 
+// The beta convolution of the forward runs on a power-of-two length Q >= 4L-1 instead of
+// the 4L-3 points of the weights: the product of the upsampled samples with quads between
+// an inverse and a forward DFT of length 4L-3 is the convolution of the beta spectrum with
+// w[k] = (1/(4L-3)) sum_j quads[j] e^{-2 pi i j k / (4L-3)}, |k| <= 2L-2, and on Q points the
+// same convolution needs quadsQ[j] = sum_k w[k] e^{+2 pi i k j / Q}. Q >= 4L-1 keeps the
+// wrapped terms off the 2L-1 kept outputs (the spectrum spans at most 2L values).
+// One warp per output; exponents reduced exactly.
+__global__ void fw_weights_from_quads_kernel(int L, const double2* __restrict__ quads,
+                                             double2* __restrict__ w) {
+  const int P = 4 * L - 3;
+  const int o = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (o >= P) return;
+  const int k = o - (2 * L - 2);
+  double re = 0.0, im = 0.0;
+  for (int j = lane; j < P; j += 32) {
+    const long r = ((-(long)j * k) % P + P) % P;
+    double sn, cs;
+    sincospi(2.0 * (double)r / (double)P, &sn, &cs);
+    const double2 q = quads[j];
+    re += q.x * cs - q.y * sn;
+    im += q.x * sn + q.y * cs;
+  }
+  for (int sh = 16; sh > 0; sh >>= 1) {
+    re += __shfl_xor_sync(0xffffffffu, re, sh);
+    im += __shfl_xor_sync(0xffffffffu, im, sh);
+  }
+  if (lane == 0) w[o] = make_double2(re / P, im / P);
+}
+
+__global__ void fw_quads_pow2_kernel(int L, int Q, const double2* __restrict__ w,
+                                     double2* __restrict__ quadsQ) {
+  const int P = 4 * L - 3;
+  const int j = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (j >= Q) return;
+  double re = 0.0, im = 0.0;
+  for (int o = lane; o < P; o += 32) {
+    const int k = o - (2 * L - 2);
+    const long r = (((long)k * j) % Q + Q) % Q;
+    double sn, cs;
+    sincospi(2.0 * (double)r / (double)Q, &sn, &cs);
+    const double2 v = w[o];
+    re += v.x * cs - v.y * sn;
+    im += v.x * sn + v.y * cs;
+  }
+  for (int sh = 16; sh > 0; sh >>= 1) {
+    re += __shfl_xor_sync(0xffffffffu, re, sh);
+    im += __shfl_xor_sync(0xffffffffu, im, sh);
+  }
+  if (lane == 0) quadsQ[j] = make_double2(re, im);
+}
+
 // Gamma DFT at a spin subset: x[g][k][px] = (1/G) sum_c f[g][c][px] e^{-2 pi i c n_k / G}
 // (n_k = -spin_k; custom_ops.py:200-204), f [O][G][npix], x [O][S][npix].
 template <typename Real>
@@ -613,12 +683,12 @@ __global__ void fw_gamma_subset_kernel(const void* fin, void* xout, int O, int G
 using namespace s2b;
 
 struct s2b_fw_plan {
-  int L, N, mwss, ntheta, nphi, P;
+  int L, N, mwss, ntheta, nphi, P, Q;  // P = 4L-3 weights, Q = pow2 >= 4L-1 beta convolution
   bool gamma_fft;  // fft.host[2] is the length-(2N-1) descriptor
   bool fp64;
   int device;
   std::vector<void*> allocs;
-  FFTSet fft;  // host[0]: length nphi, host[1]: length 4L-3, host[2]: 2N-1 (gamma_fft)
+  FFTSet fft;  // host[0]: length nphi, host[1]: length Q, host[2]: 2N-1 (gamma_fft)
   ~s2b_fw_plan() {
     for (void* a : allocs) cudaFree(a);
   }
@@ -640,9 +710,10 @@ size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
 bool aligned16(const void* p) { return p && ((uintptr_t)p & 15) == 0; }
 
 // Workspace regions: A (Y, G, or the gamma maps), B (T or S), C (spin-subset gamma maps).
+// D: the beta-convolution weights of the forward (w [4L-3], quadsQ [Q], complex double).
 struct FWLayout {
-  size_t a, b, c;
-  size_t total() const { return a + b + c; }
+  size_t a, b, c, d;
+  size_t total() const { return a + b + c + d; }
 };
 
 FWLayout fw_layout(const s2b_fw_plan* p, long E, long nmaps_gamma, long E_subset_gamma) {
@@ -653,6 +724,7 @@ FWLayout fw_layout(const s2b_fw_plan* p, long E, long nmaps_gamma, long E_subset
   l.a = al256(cs * (size_t)std::max(E * W * W, nmaps_gamma * npix));
   l.b = al256(cs * (size_t)(E * p->ntheta * W));
   l.c = al256(cs * (size_t)(E_subset_gamma * npix));
+  l.d = al256(sizeof(double2) * (size_t)(p->P + p->Q));
   return l;
 }
 
@@ -679,7 +751,7 @@ FWFftParams<Real> fft_params(const s2b_fw_plan* p, int E, const FWSlices& sl) {
   f.mwss = p->mwss;
   f.ntheta = p->ntheta;
   f.nphi = p->nphi;
-  f.P = p->P;
+  f.P = p->Q;  // length of the beta convolution (dP)
   f.E = E;
   f.sl = sl;
   f.nmajor = 0;
@@ -755,8 +827,16 @@ int forward_chain(const s2b_fw_plan* p, int E, const FWSlices& sl, const double*
   using R2 = typename C2<Real>::t;
   void* A = ws;
   void* B = ws + lay.a;
+  double2* wk = reinterpret_cast<double2*>(ws + lay.a + lay.b + lay.c);
+  double2* qQ = wk + p->P;
+  fw_weights_from_quads_kernel<<<(p->P + 3) / 4, 128, 0, st>>>(
+      p->L, reinterpret_cast<const double2*>(quads), wk);
+  FW_CK(cudaGetLastError());
+  fw_quads_pow2_kernel<<<(p->Q + 3) / 4, 128, 0, st>>>(p->L, p->Q, wk, qQ);
+  FW_CK(cudaGetLastError());
   FWFftParams<Real> f = fft_params<Real>(p, E, sl);
-  f.quads = quads;
+  f.quads = qQ;
+  f.wconv = wk;
   const int M = f.dphi.M;
   f.in = maps;
   f.out = B;
@@ -770,7 +850,7 @@ int forward_chain(const s2b_fw_plan* p, int E, const FWSlices& sl, const double*
   f.nmajor = 0;
   f.scale = 1.0;
   const int bufM = std::max(f.dphi.M, f.dP.M);
-  const size_t smem = (size_t)(padded_len(bufM) + p->P) * sizeof(R2);
+  const size_t smem = (size_t)(padded_len(bufM) + p->Q) * sizeof(R2);
   FW_CK(cudaFuncSetAttribute(fw_cols_fwd_kernel<Real>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   fw_cols_fwd_kernel<Real><<<dim3(2 * p->L - 1, E), fft_threads_for(bufM), smem, st>>>(f, bufM);
@@ -890,6 +970,8 @@ int s2b_fw_plan_create(int L, int N, int sampling, int precision, s2b_fw_plan** 
   p->ntheta = p->mwss ? L + 1 : L;
   p->nphi = p->mwss ? 2 * L : 2 * L - 1;
   p->P = 4 * L - 3;
+  p->Q = 1;
+  while (p->Q < 4 * L - 1) p->Q <<= 1;
   p->fp64 = precision == S2B_F64;
   cudaError_t e = cudaGetDevice(&p->device);
   if (e != cudaSuccess) {
@@ -898,16 +980,16 @@ int s2b_fw_plan_create(int L, int N, int sampling, int precision, s2b_fw_plan** 
   }
   p->N = N;
   p->gamma_fft = 2 * N - 1 >= kGamFFTMin;
-  const int lens[3] = {p->nphi, p->P, 2 * N - 1};
+  const int lens[3] = {p->nphi, p->Q, 2 * N - 1};
   const int rc = build_fft_set(lens, p->gamma_fft ? 3 : 2, p->fp64, &p->allocs, &p->fft);
   if (rc) {
     delete p;
     return rc;
   }
-  // the column chain keeps a DFT buffer and 4L-3 values in shared memory
+  // the column chain keeps a DFT buffer and Q values in shared memory
   const size_t cs = p->fp64 ? 16 : 8;
   const int bufM = std::max(p->fft.host[0].M, p->fft.host[1].M);
-  if ((padded_len(bufM) + (size_t)p->P) * cs > 227 * 1024) {
+  if ((padded_len(bufM) + (size_t)p->Q) * cs > 227 * 1024) {
     delete p;
     return fw_fail(S2B_ERR_INVALID, "band-limit too large for the Fourier-Wigner beta chain");
   }
