@@ -125,16 +125,17 @@ __global__ void __launch_bounds__(kFwLanes) fw_contract_kernel(FWContractParams<
 
   // summation range of the tile
   int qlo, qhi;
+  const int cl = blockIdx.y * kFwLanes - (L - 1);
+  const int ch = min(cl + kFwLanes - 1, L - 1);
+  const int mmin = (cl <= 0 && ch >= 0) ? 0 : min(abs(cl), abs(ch));  // least |m| of the CTA
   if (FWD) {
     qlo = 0;
     qhi = min(r0 + R - 1, L - 1);
+    if (mmin > qhi) qhi = -1;  // every D[l][b][m] of the tile is zero: write zeros
   } else {
     int nmin = L;
     for (int s = 0; s < E; ++s)
       if (e0 + s < p.E) nmin = min(nmin, abs(nsh[s]));
-    const int cl = blockIdx.y * kFwLanes - (L - 1);
-    const int ch = min(cl + kFwLanes - 1, L - 1);
-    const int mmin = (cl <= 0 && ch >= 0) ? 0 : min(abs(cl), abs(ch));
     qlo = max(max(r0, nmin), mmin);
     qhi = L - 1;
   }
