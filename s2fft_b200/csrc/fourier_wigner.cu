@@ -79,7 +79,7 @@ template <typename Real>
 struct FWTile {
   static constexpr int R = 4;
   static constexpr int E = 4;
-  static constexpr int QU = sizeof(Real) == 4 ? 4 : 2;  // summation indices per load batch
+  static constexpr int QU = 2;  // summation indices per load batch
 };
 
 template <typename Real>
