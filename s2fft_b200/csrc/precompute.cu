@@ -190,128 +190,112 @@ __global__ void kernel_table_lowm_kernel(KernelTableParams p) {
 // for the forward) for BB maps, so every data element loaded is reused RT times
 // and every K element BB times. Accumulation in the plan precision.
 // ---------------------------------------------------------------------------
-constexpr int kRT = 4, kBB = 8;
+// Register tile: RT output rows (t for the inverse, l for the forward) x BB maps per thread.
+template <typename Real>
+struct PreTile {
+  static constexpr int RT = sizeof(Real) == 4 ? 8 : 4;
+  static constexpr int BB = sizeof(Real) == 4 ? 8 : 4;
+  static constexpr int LANES = 64;  // columns mi per CTA
+};
 
-// inverse: ftm[b][t][mo + mi] = sgn * sum_l K[t][l][mi] flm[b][l][mshift + mi]
-template <typename Real, bool CPLX>
-__global__ void pre_inverse_kernel(PreContractParams p) {
+// Row tiles run along blockIdx.x and map tiles along blockIdx.y, so the CTAs resident at
+// one time cover every row and map tile of one or two column blocks (blockIdx.z): the K
+// columns and data columns of the block stay in L2 and come from DRAM about once. The
+// loads of two summation indices are issued ahead of their arithmetic.
+//
+// FWD = false (inverse): out[b][t][mo + mi] = sgn * sum_l K[t][l][mi] in[b][l][mshift + mi]
+// FWD = true (forward):  out[b][l][mshift + mi] = sgn * sum_t K[t][l][mi] in[b][t][mi]
+template <typename Real, bool CPLX, bool FWD>
+__global__ void pre_contract_kernel(PreContractParams p) {
   using C = P2<Real>;
+  constexpr int RT = PreTile<Real>::RT, BB = PreTile<Real>::BB;
   const int M = p.M;
-  const int mi = blockIdx.x * blockDim.x + threadIdx.x;
-  const int t0 = blockIdx.y * kRT;
-  const int b0 = blockIdx.z * kBB;
+  const int mi = blockIdx.z * blockDim.x + threadIdx.x;
+  const int r0 = blockIdx.x * RT;
+  const int b0 = blockIdx.y * BB;
   if (mi >= M) return;
   const int L = p.L;
-  Real ar[kRT][kBB], ai[kRT][kBB];
+  const int nrow = FWD ? L : p.nth;   // output rows
+  const int nsum = FWD ? p.nth : L;   // summation length
+  Real ar[RT][BB], ai[RT][BB];
 #pragma unroll
-  for (int r = 0; r < kRT; ++r)
+  for (int r = 0; r < RT; ++r)
 #pragma unroll
-    for (int x = 0; x < kBB; ++x) ar[r][x] = ai[r][x] = Real(0);
-  const C* flm = reinterpret_cast<const C*>(p.in);
-  for (int l = 0; l < L; ++l) {
-    C f[kBB];
+    for (int x = 0; x < BB; ++x) ar[r][x] = ai[r][x] = Real(0);
+  const C* in = reinterpret_cast<const C*>(p.in);
+  // data element (map x, summation index q) and kernel element (row r, index q)
+  auto dat = [&](int x, int q) -> C {
+    const int b = min(b0 + x, p.batch - 1);
+    return FWD ? in[((size_t)b * p.nth + q) * M + mi]
+               : in[((size_t)b * L + q) * (2 * L - 1) + p.mshift + mi];
+  };
+  auto ker = [&](int r, int q) -> C {
+    const int row = min(r0 + r, nrow - 1);
+    const size_t o = FWD ? ((size_t)q * L + row) * M + mi : ((size_t)row * L + q) * M + mi;
+    C k;
+    if (CPLX) {
+      k = reinterpret_cast<const C*>(p.K)[o];
+    } else {
+      k.x = reinterpret_cast<const Real*>(p.K)[o];
+      k.y = Real(0);
+    }
+    return k;
+  };
+  int q = 0;
+  for (; q + 1 < nsum; q += 2) {
+    C f[2][BB], k[2][RT];
 #pragma unroll
-    for (int x = 0; x < kBB; ++x) {
-      f[x].x = f[x].y = Real(0);
-      if (b0 + x < p.batch) f[x] = flm[((size_t)(b0 + x) * L + l) * (2 * L - 1) + p.mshift + mi];
+    for (int u = 0; u < 2; ++u) {
+#pragma unroll
+      for (int x = 0; x < BB; ++x) f[u][x] = dat(x, q + u);
+#pragma unroll
+      for (int r = 0; r < RT; ++r) k[u][r] = ker(r, q + u);
     }
 #pragma unroll
-    for (int r = 0; r < kRT; ++r) {
-      const int t = t0 + r;
-      if (t >= p.nth) break;
-      Real kr, ki = Real(0);
-      if (CPLX) {
-        const C k = reinterpret_cast<const C*>(p.K)[((size_t)t * L + l) * M + mi];
-        kr = k.x;
-        ki = k.y;
-      } else {
-        kr = reinterpret_cast<const Real*>(p.K)[((size_t)t * L + l) * M + mi];
-      }
+    for (int u = 0; u < 2; ++u)
 #pragma unroll
-      for (int x = 0; x < kBB; ++x) {
-        ar[r][x] = fma(kr, f[x].x, ar[r][x]);
-        ai[r][x] = fma(kr, f[x].y, ai[r][x]);
+      for (int r = 0; r < RT; ++r)
+#pragma unroll
+        for (int x = 0; x < BB; ++x) {
+          ar[r][x] = fma(k[u][r].x, f[u][x].x, ar[r][x]);
+          ai[r][x] = fma(k[u][r].x, f[u][x].y, ai[r][x]);
+          if (CPLX) {
+            ar[r][x] = fma(-k[u][r].y, f[u][x].y, ar[r][x]);
+            ai[r][x] = fma(k[u][r].y, f[u][x].x, ai[r][x]);
+          }
+        }
+  }
+  for (; q < nsum; ++q) {
+#pragma unroll
+    for (int r = 0; r < RT; ++r) {
+      const C k = ker(r, q);
+#pragma unroll
+      for (int x = 0; x < BB; ++x) {
+        const C f = dat(x, q);
+        ar[r][x] = fma(k.x, f.x, ar[r][x]);
+        ai[r][x] = fma(k.x, f.y, ai[r][x]);
         if (CPLX) {
-          ar[r][x] = fma(-ki, f[x].y, ar[r][x]);
-          ai[r][x] = fma(ki, f[x].x, ai[r][x]);
+          ar[r][x] = fma(-k.y, f.y, ar[r][x]);
+          ai[r][x] = fma(k.y, f.x, ai[r][x]);
         }
       }
     }
   }
   C* out = reinterpret_cast<C*>(p.out);
 #pragma unroll
-  for (int r = 0; r < kRT; ++r) {
-    const int t = t0 + r;
-    if (t >= p.nth) break;
+  for (int r = 0; r < RT; ++r) {
+    const int row = r0 + r;
+    if (row >= nrow) break;
 #pragma unroll
-    for (int x = 0; x < kBB; ++x) {
+    for (int x = 0; x < BB; ++x) {
       if (b0 + x >= p.batch) break;
       C o;
       o.x = (Real)(p.sign * ar[r][x]);
       o.y = (Real)(p.sign * ai[r][x]);
-      out[((size_t)(b0 + x) * p.nth + t) * p.ncol + p.mo + mi] = o;
-    }
-  }
-}
-
-// forward: flm[b][l][mshift + mi] = sgn * sum_t K[t][l][mi] ftm[b][t][mi]
-template <typename Real, bool CPLX>
-__global__ void pre_forward_kernel(PreContractParams p) {
-  using C = P2<Real>;
-  const int M = p.M;
-  const int mi = blockIdx.x * blockDim.x + threadIdx.x;
-  const int l0 = blockIdx.y * kRT;
-  const int b0 = blockIdx.z * kBB;
-  if (mi >= M) return;
-  const int L = p.L;
-  Real ar[kRT][kBB], ai[kRT][kBB];
-#pragma unroll
-  for (int r = 0; r < kRT; ++r)
-#pragma unroll
-    for (int x = 0; x < kBB; ++x) ar[r][x] = ai[r][x] = Real(0);
-  const C* ftm = reinterpret_cast<const C*>(p.in);
-  for (int t = 0; t < p.nth; ++t) {
-    C f[kBB];
-#pragma unroll
-    for (int x = 0; x < kBB; ++x) {
-      f[x].x = f[x].y = Real(0);
-      if (b0 + x < p.batch) f[x] = ftm[((size_t)(b0 + x) * p.nth + t) * M + mi];
-    }
-#pragma unroll
-    for (int r = 0; r < kRT; ++r) {
-      const int l = l0 + r;
-      if (l >= L) break;
-      Real kr, ki = Real(0);
-      if (CPLX) {
-        const C k = reinterpret_cast<const C*>(p.K)[((size_t)t * L + l) * M + mi];
-        kr = k.x;
-        ki = k.y;
-      } else {
-        kr = reinterpret_cast<const Real*>(p.K)[((size_t)t * L + l) * M + mi];
-      }
-#pragma unroll
-      for (int x = 0; x < kBB; ++x) {
-        ar[r][x] = fma(kr, f[x].x, ar[r][x]);
-        ai[r][x] = fma(kr, f[x].y, ai[r][x]);
-        if (CPLX) {
-          ar[r][x] = fma(-ki, f[x].y, ar[r][x]);
-          ai[r][x] = fma(ki, f[x].x, ai[r][x]);
-        }
-      }
-    }
-  }
-  C* out = reinterpret_cast<C*>(p.out);
-#pragma unroll
-  for (int r = 0; r < kRT; ++r) {
-    const int l = l0 + r;
-    if (l >= L) break;
-#pragma unroll
-    for (int x = 0; x < kBB; ++x) {
-      if (b0 + x >= p.batch) break;
-      C o;
-      o.x = (Real)(p.sign * ar[r][x]);
-      o.y = (Real)(p.sign * ai[r][x]);
-      out[((size_t)(b0 + x) * L + l) * (2 * L - 1) + p.mshift + mi] = o;
+      if (FWD)
+        out[((size_t)(b0 + x) * L + row) * (2 * L - 1) + p.mshift + mi] = o;
+      else
+        out[((size_t)(b0 + x) * p.nth + row) * p.ncol + p.mo + mi] = o;
     }
   }
 }
@@ -353,14 +337,17 @@ cudaError_t launch_kernel_table(bool fp64, const KernelTableParams& p, cudaStrea
 
 cudaError_t launch_pre_contract(bool fp64, bool forward, bool cplx, const PreContractParams& p,
                                 cudaStream_t s) {
-  const int threads = 64;
-  dim3 grid((p.M + threads - 1) / threads, ((forward ? p.L : p.nth) + kRT - 1) / kRT,
-            (p.batch + kBB - 1) / kBB);
+  const int threads = fp64 ? PreTile<double>::LANES : PreTile<float>::LANES;
+  const int nrow = forward ? p.L : p.nth;
+  const int RT = fp64 ? PreTile<double>::RT : PreTile<float>::RT;
+  const int BB = fp64 ? PreTile<double>::BB : PreTile<float>::BB;
+  dim3 grid((nrow + RT - 1) / RT, (p.batch + BB - 1) / BB, (p.M + threads - 1) / threads);
+  if (grid.y > 65535 || grid.z > 65535) return cudaErrorInvalidConfiguration;
 #define S2B_LAUNCH(R, C)                                                   \
   if (forward)                                                             \
-    pre_forward_kernel<R, C><<<grid, threads, 0, s>>>(p);                  \
+    pre_contract_kernel<R, C, true><<<grid, threads, 0, s>>>(p);           \
   else                                                                     \
-    pre_inverse_kernel<R, C><<<grid, threads, 0, s>>>(p);
+    pre_contract_kernel<R, C, false><<<grid, threads, 0, s>>>(p);
   if (fp64) {
     if (cplx) {
       S2B_LAUNCH(double, true)
