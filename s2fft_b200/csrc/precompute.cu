@@ -300,6 +300,148 @@ __global__ void pre_contract_kernel(PreContractParams p) {
   }
 }
 
+// Batched contraction (batch >= kGemmMinBatch): for every column mi an independent GEMM
+// (rows x maps, summed over q), computed by CTAs that own 8 consecutive columns, a tile of
+// 32 rows and a tile of 32 (float) or 16 (double) maps. Chunks of Q summation
+// indices of K and of the data are staged in shared memory with coalesced loads (the 8
+// columns of a row are one 32-byte sector of K) and prefetched into registers while the
+// previous chunk is consumed. Thread (column c, row group rg, map group bg) keeps 4 rows x
+// BT maps of complex sums. K rows are padded to 10 entries so that the four row groups of
+// a warp read distinct banks; the data reads of a warp are broadcasts.
+constexpr int kGemmMinBatch = 16;
+constexpr int kGemmMI = 8;      // columns per CTA
+constexpr int kGemmKP = 10;     // padded K row (entries)
+constexpr int kGemmRows = 32;   // rows per CTA (8 row groups x 4)
+
+template <typename Real>
+struct GemmTile {
+  static constexpr int BT = sizeof(Real) == 4 ? 8 : 4;  // maps per thread
+  static constexpr int MAPS = 4 * BT;                    // maps per CTA (4 map groups)
+};
+
+template <typename Real, bool CPLX, bool FWD>
+__global__ void __launch_bounds__(256, sizeof(Real) == 8 ? 2 : 1) pre_gemm_kernel(PreContractParams p) {
+  using C = P2<Real>;
+  using KT = std::conditional_t<CPLX, C, Real>;
+  constexpr int BT = GemmTile<Real>::BT, MAPS = GemmTile<Real>::MAPS;
+  constexpr int kGemmQ = sizeof(KT) >= 16 ? 4 : 8;  // summation indices per chunk (<= 48 KB)
+  constexpr int NK = kGemmQ * kGemmRows * kGemmMI;  // K entries per chunk
+  constexpr int ND = kGemmQ * MAPS * kGemmMI;       // data entries per chunk
+  constexpr int KPT = NK / 256, DPT = ND / 256;     // per thread
+  __shared__ KT Ks[kGemmQ][kGemmRows][kGemmKP];
+  __shared__ C Ds[kGemmQ][MAPS][kGemmMI];
+  const int tid = threadIdx.x;
+  const int c = tid & 7, rg = (tid >> 3) & 7, bg = tid >> 6;
+  const int L = p.L, M = p.M;
+  const int nrow = FWD ? L : p.nth;
+  const int nsum = FWD ? p.nth : L;
+  const int row0 = blockIdx.x * kGemmRows;
+  const int b0 = blockIdx.y * MAPS;
+  const int mi0 = blockIdx.z * kGemmMI;
+
+  // chunk loaders: element e of the chunk -> (q, row or map, column)
+  auto kload = [&](int q0, int e) -> KT {
+    const int cc = e & 7, rr = (e >> 3) % kGemmRows, qq = e / (8 * kGemmRows);
+    const int q = q0 + qq, row = row0 + rr, mi = mi0 + cc;
+    KT v{};
+    if (q < nsum && row < nrow && mi < M) {
+      const size_t o = FWD ? ((size_t)q * L + row) * M + mi : ((size_t)row * L + q) * M + mi;
+      v = reinterpret_cast<const KT*>(p.K)[o];
+    }
+    return v;
+  };
+  auto dload = [&](int q0, int e) -> C {
+    const int cc = e & 7, bb = (e >> 3) % MAPS, qq = e / (8 * MAPS);
+    const int q = q0 + qq, b = b0 + bb, mi = mi0 + cc;
+    C v;
+    v.x = v.y = Real(0);
+    if (q < nsum && b < p.batch && mi < M) {
+      const C* in = reinterpret_cast<const C*>(p.in);
+      v = FWD ? in[((size_t)b * p.nth + q) * M + mi]
+              : in[((size_t)b * L + q) * (2 * L - 1) + p.mshift + mi];
+    }
+    return v;
+  };
+
+  Real ar[4][BT], ai[4][BT];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int x = 0; x < BT; ++x) ar[r][x] = ai[r][x] = Real(0);
+
+  KT kreg[KPT];
+  C dreg[DPT];
+#pragma unroll
+  for (int i = 0; i < KPT; ++i) kreg[i] = kload(0, tid + i * 256);
+#pragma unroll
+  for (int i = 0; i < DPT; ++i) dreg[i] = dload(0, tid + i * 256);
+
+  for (int q0 = 0; q0 < nsum; q0 += kGemmQ) {
+    __syncthreads();  // the previous chunk is consumed
+#pragma unroll
+    for (int i = 0; i < KPT; ++i) {
+      const int e = tid + i * 256;
+      Ks[e / (8 * kGemmRows)][(e >> 3) % kGemmRows][e & 7] = kreg[i];
+    }
+#pragma unroll
+    for (int i = 0; i < DPT; ++i) {
+      const int e = tid + i * 256;
+      Ds[e / (8 * MAPS)][(e >> 3) % MAPS][e & 7] = dreg[i];
+    }
+    __syncthreads();
+    if (q0 + kGemmQ < nsum) {  // prefetch the next chunk
+#pragma unroll
+      for (int i = 0; i < KPT; ++i) kreg[i] = kload(q0 + kGemmQ, tid + i * 256);
+#pragma unroll
+      for (int i = 0; i < DPT; ++i) dreg[i] = dload(q0 + kGemmQ, tid + i * 256);
+    }
+#pragma unroll 4
+    for (int qq = 0; qq < kGemmQ; ++qq) {
+      KT k[4];
+      C d[BT];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) k[r] = Ks[qq][rg * 4 + r][c];
+#pragma unroll
+      for (int x = 0; x < BT; ++x) d[x] = Ds[qq][bg * BT + x][c];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int x = 0; x < BT; ++x) {
+          if constexpr (CPLX) {
+            ar[r][x] = fma(k[r].x, d[x].x, ar[r][x]);
+            ai[r][x] = fma(k[r].x, d[x].y, ai[r][x]);
+            ar[r][x] = fma(-k[r].y, d[x].y, ar[r][x]);
+            ai[r][x] = fma(k[r].y, d[x].x, ai[r][x]);
+          } else {
+            ar[r][x] = fma(k[r], d[x].x, ar[r][x]);
+            ai[r][x] = fma(k[r], d[x].y, ai[r][x]);
+          }
+        }
+    }
+  }
+
+  const int mi = mi0 + c;
+  if (mi >= M) return;
+  C* out = reinterpret_cast<C*>(p.out);
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int row = row0 + rg * 4 + r;
+    if (row >= nrow) break;
+#pragma unroll
+    for (int x = 0; x < BT; ++x) {
+      const int b = b0 + bg * BT + x;
+      if (b >= p.batch) break;
+      C o;
+      o.x = (Real)(p.sign * ar[r][x]);
+      o.y = (Real)(p.sign * ai[r][x]);
+      if (FWD)
+        out[((size_t)b * L + row) * (2 * L - 1) + p.mshift + mi] = o;
+      else
+        out[((size_t)b * p.nth + row) * p.ncol + p.mo + mi] = o;
+    }
+  }
+}
+
 // reality mirror flm[b][l][L-1-m] = (-1)^m conj(flm[b][l][L-1+m]), m >= 1
 template <typename Real>
 __global__ void reality_mirror_kernel(void* flm, int B, int L) {
@@ -337,8 +479,34 @@ cudaError_t launch_kernel_table(bool fp64, const KernelTableParams& p, cudaStrea
 
 cudaError_t launch_pre_contract(bool fp64, bool forward, bool cplx, const PreContractParams& p,
                                 cudaStream_t s) {
-  const int threads = fp64 ? PreTile<double>::LANES : PreTile<float>::LANES;
   const int nrow = forward ? p.L : p.nth;
+  if (p.batch >= kGemmMinBatch) {
+    const int maps = fp64 ? GemmTile<double>::MAPS : GemmTile<float>::MAPS;
+    dim3 g((nrow + kGemmRows - 1) / kGemmRows, (p.batch + maps - 1) / maps,
+           (p.M + kGemmMI - 1) / kGemmMI);
+    if (g.y > 65535 || g.z > 65535) return cudaErrorInvalidConfiguration;
+#define S2B_GEMM(R, C)                                                     \
+  if (forward)                                                             \
+    pre_gemm_kernel<R, C, true><<<g, 256, 0, s>>>(p);                      \
+  else                                                                     \
+    pre_gemm_kernel<R, C, false><<<g, 256, 0, s>>>(p);
+    if (fp64) {
+      if (cplx) {
+        S2B_GEMM(double, true)
+      } else {
+        S2B_GEMM(double, false)
+      }
+    } else {
+      if (cplx) {
+        S2B_GEMM(float, true)
+      } else {
+        S2B_GEMM(float, false)
+      }
+    }
+#undef S2B_GEMM
+    return cudaGetLastError();
+  }
+  const int threads = fp64 ? PreTile<double>::LANES : PreTile<float>::LANES;
   const int RT = fp64 ? PreTile<double>::RT : PreTile<float>::RT;
   const int BB = fp64 ? PreTile<double>::BB : PreTile<float>::BB;
   dim3 grid((nrow + RT - 1) / RT, (p.batch + BB - 1) / BB, (p.M + threads - 1) / threads);

@@ -367,3 +367,34 @@ def test_healpix_spin_exact(s2b, precision):
         assert relerr(f, data[f"{n}/f"]) < tol, (c, relerr(f, data[f"{n}/f"]))
         g = s2b.forward(data[f"{n}/f"], L, spin, nside, "healpix", precision=precision)
         assert relerr(g, data[f"{n}/flm_fwd"]) < tol, (c, relerr(g, data[f"{n}/flm_fwd"]))
+
+
+@pytest.mark.parametrize("precision,tol", [("f64", TOL64), ("f32", TOL32)])
+@pytest.mark.parametrize("sampling", ["gl", "healpix", "mwss"])
+def test_precompute_batched_contraction(s2b, rng, sampling, precision, tol):
+    """Batches of >= 16 maps take the shared-memory tiled contraction (partial column
+    blocks, partial map tiles, complex HEALPix kernels); it must agree with the per-map
+    path and with the oracle, in both directions."""
+    L, nside, spin = (16, 8, 0) if sampling == "healpix" else (19, None, 1)
+    B = 37
+    flms = np.stack([oracle.signal.generate_flm(rng, L, 0, spin, False) for _ in range(B)])
+    kin = s2b.precompute.spin_spherical_kernel(L, spin, False, sampling, nside, False,
+                                               precision=precision)
+    kfw = s2b.precompute.spin_spherical_kernel(L, spin, False, sampling, nside, True,
+                                               precision=precision)
+    f = s2b.precompute.inverse(flms, L, spin, kin, sampling, False, nside=nside,
+                               precision=precision)
+    for i in (0, 17, B - 1):
+        ref = oracle.spherical.inverse(flms[i], L, spin, nside, sampling)
+        assert relerr(f[i], ref) < tol
+        one = s2b.precompute.inverse(flms[i], L, spin, kin, sampling, False, nside=nside,
+                                     precision=precision)
+        assert relerr(f[i], one) < tol
+    g = s2b.precompute.forward(f, L, spin, kfw, sampling, False, nside=nside,
+                               precision=precision)
+    if sampling != "healpix":  # healpix forward is not exact without refinement
+        assert relerr(g, flms) < 10 * tol
+    for i in (3, B - 1):
+        one = s2b.precompute.forward(f[i], L, spin, kfw, sampling, False, nside=nside,
+                                     precision=precision)
+        assert relerr(g[i], one) < tol
