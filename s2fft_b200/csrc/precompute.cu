@@ -306,11 +306,9 @@ __global__ void pre_contract_kernel(PreContractParams p) {
 // indices of K and of the data are staged in shared memory with coalesced loads (the 8
 // columns of a row are one 32-byte sector of K) and prefetched into registers while the
 // previous chunk is consumed. Thread (column c, row group rg, map group bg) keeps 4 rows x
-// BT maps of complex sums. K rows are padded to 10 entries so that the four row groups of
-// a warp read distinct banks; the data reads of a warp are broadcasts.
+// BT maps of complex sums and reads them from shared memory with 16-byte loads.
 constexpr int kGemmMinBatch = 16;
 constexpr int kGemmMI = 8;      // columns per CTA
-constexpr int kGemmKP = 10;     // padded K row (entries)
 constexpr int kGemmRows = 32;   // rows per CTA (8 row groups x 4)
 
 template <typename Real>
@@ -319,17 +317,47 @@ struct GemmTile {
   static constexpr int MAPS = 4 * BT;                    // maps per CTA (4 map groups)
 };
 
+// n consecutive Real from 16-byte aligned shared memory by 16-byte loads
+template <int N, typename Real>
+__device__ __forceinline__ void lds_vec(Real (&dst)[N], const Real* src) {
+  if constexpr (sizeof(Real) == 4) {
+    static_assert(N % 4 == 0, "float vectors of 4");
+#pragma unroll
+    for (int i = 0; i < N / 4; ++i) {
+      const float4 v = reinterpret_cast<const float4*>(src)[i];
+      dst[4 * i] = v.x;
+      dst[4 * i + 1] = v.y;
+      dst[4 * i + 2] = v.z;
+      dst[4 * i + 3] = v.w;
+    }
+  } else {
+    static_assert(N % 2 == 0, "double vectors of 2");
+#pragma unroll
+    for (int i = 0; i < N / 2; ++i) {
+      const double2 v = reinterpret_cast<const double2*>(src)[i];
+      dst[2 * i] = v.x;
+      dst[2 * i + 1] = v.y;
+    }
+  }
+}
+
 template <typename Real, bool CPLX, bool FWD>
 __global__ void __launch_bounds__(256, sizeof(Real) == 8 ? 2 : 1) pre_gemm_kernel(PreContractParams p) {
   using C = P2<Real>;
   using KT = std::conditional_t<CPLX, C, Real>;
   constexpr int BT = GemmTile<Real>::BT, MAPS = GemmTile<Real>::MAPS;
-  constexpr int kGemmQ = sizeof(KT) >= 16 ? 4 : 8;  // summation indices per chunk (<= 48 KB)
-  constexpr int NK = kGemmQ * kGemmRows * kGemmMI;  // K entries per chunk
-  constexpr int ND = kGemmQ * MAPS * kGemmMI;       // data entries per chunk
-  constexpr int KPT = NK / 256, DPT = ND / 256;     // per thread
-  __shared__ KT Ks[kGemmQ][kGemmRows][kGemmKP];
-  __shared__ C Ds[kGemmQ][MAPS][kGemmMI];
+  constexpr int kGemmQ = sizeof(Real) == 8 ? 4 : 8;  // summation indices per chunk (<= 48 KB)
+  constexpr int KW = CPLX ? 2 : 1;                    // Real per K entry
+  constexpr int PAD = 16 / (int)sizeof(Real);         // 16 bytes: rows of a warp phase
+  constexpr int KS = kGemmRows * KW + PAD;            //   start on distinct bank groups
+  constexpr int DS = MAPS * 2 + PAD;
+  constexpr int NK = kGemmQ * kGemmRows * kGemmMI;    // K entries per chunk
+  constexpr int ND = kGemmQ * MAPS * kGemmMI;         // data entries per chunk
+  constexpr int KPT = NK / 256, DPT = ND / 256;       // per thread
+  // [q][column][rows] and [q][column][maps (re, im)]: a thread reads its 4 rows and BT maps
+  // of one column with 16-byte loads
+  __shared__ __align__(16) Real Ks[kGemmQ][kGemmMI][KS];
+  __shared__ __align__(16) Real Ds[kGemmQ][kGemmMI][DS];
   const int tid = threadIdx.x;
   const int c = tid & 7, rg = (tid >> 3) & 7, bg = tid >> 6;
   const int L = p.L, M = p.M;
@@ -339,7 +367,7 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 8 ? 2 : 1) pre_gemm_kerne
   const int b0 = blockIdx.y * MAPS;
   const int mi0 = blockIdx.z * kGemmMI;
 
-  // chunk loaders: element e of the chunk -> (q, row or map, column)
+  // chunk loaders: element e of the chunk -> (q, row or map, column), column fastest
   auto kload = [&](int q0, int e) -> KT {
     const int cc = e & 7, rr = (e >> 3) % kGemmRows, qq = e / (8 * kGemmRows);
     const int q = q0 + qq, row = row0 + rr, mi = mi0 + cc;
@@ -381,12 +409,20 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 8 ? 2 : 1) pre_gemm_kerne
 #pragma unroll
     for (int i = 0; i < KPT; ++i) {
       const int e = tid + i * 256;
-      Ks[e / (8 * kGemmRows)][(e >> 3) % kGemmRows][e & 7] = kreg[i];
+      Real* dst = &Ks[e / (8 * kGemmRows)][e & 7][((e >> 3) % kGemmRows) * KW];
+      if constexpr (CPLX) {
+        dst[0] = kreg[i].x;
+        dst[1] = kreg[i].y;
+      } else {
+        dst[0] = kreg[i];
+      }
     }
 #pragma unroll
     for (int i = 0; i < DPT; ++i) {
       const int e = tid + i * 256;
-      Ds[e / (8 * MAPS)][(e >> 3) % MAPS][e & 7] = dreg[i];
+      Real* dst = &Ds[e / (8 * MAPS)][e & 7][((e >> 3) % MAPS) * 2];
+      dst[0] = dreg[i].x;
+      dst[1] = dreg[i].y;
     }
     __syncthreads();
     if (q0 + kGemmQ < nsum) {  // prefetch the next chunk
@@ -395,26 +431,22 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 8 ? 2 : 1) pre_gemm_kerne
 #pragma unroll
       for (int i = 0; i < DPT; ++i) dreg[i] = dload(q0 + kGemmQ, tid + i * 256);
     }
-#pragma unroll 4
+#pragma unroll 2
     for (int qq = 0; qq < kGemmQ; ++qq) {
-      KT k[4];
-      C d[BT];
-#pragma unroll
-      for (int r = 0; r < 4; ++r) k[r] = Ks[qq][rg * 4 + r][c];
-#pragma unroll
-      for (int x = 0; x < BT; ++x) d[x] = Ds[qq][bg * BT + x][c];
+      Real k[4 * KW], d[2 * BT];
+      lds_vec(k, &Ks[qq][c][rg * 4 * KW]);
+      lds_vec(d, &Ds[qq][c][bg * BT * 2]);
 #pragma unroll
       for (int r = 0; r < 4; ++r)
 #pragma unroll
         for (int x = 0; x < BT; ++x) {
+          const Real kr = k[r * KW];
+          ar[r][x] = fma(kr, d[2 * x], ar[r][x]);
+          ai[r][x] = fma(kr, d[2 * x + 1], ai[r][x]);
           if constexpr (CPLX) {
-            ar[r][x] = fma(k[r].x, d[x].x, ar[r][x]);
-            ai[r][x] = fma(k[r].x, d[x].y, ai[r][x]);
-            ar[r][x] = fma(-k[r].y, d[x].y, ar[r][x]);
-            ai[r][x] = fma(k[r].y, d[x].x, ai[r][x]);
-          } else {
-            ar[r][x] = fma(k[r], d[x].x, ar[r][x]);
-            ai[r][x] = fma(k[r], d[x].y, ai[r][x]);
+            const Real ki = k[r * KW + 1];
+            ar[r][x] = fma(-ki, d[2 * x + 1], ar[r][x]);
+            ai[r][x] = fma(ki, d[2 * x], ai[r][x]);
           }
         }
     }
