@@ -129,31 +129,59 @@ __global__ void pack_kernel_a(const float* __restrict__ K, int nth, int L, int M
   }
 }
 
-// raw spectra [b][t][mi] (complex float) -> Bp[mi][bg][tc][hi/lo][block], n = 2 (b - 64 bg) + c
-__global__ void pack_kernel_b(const float2* __restrict__ X, int B, int nth, int M, int nbg, int ntc,
-                              __nv_bfloat16* __restrict__ out) {
-  const long total = (long)M * nbg * ntc * kBlk;
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
-       i += (long)gridDim.x * blockDim.x) {
-    const int e = (int)(i % kBlk);
-    long rest = i / kBlk;
-    const int tc = (int)(rest % ntc);
-    rest /= ntc;
-    const int bg = (int)(rest % nbg);
-    const int mi = (int)(rest / nbg);
-    const int n = e / kTileK, k = e % kTileK;
-    const int b = bg * 64 + (n >> 1), t = tc * kTileK + k;
-    float x = 0.f;
-    if (b < B && t < nth) {
-      const float2 v = X[((size_t)b * nth + t) * M + mi];
-      x = (n & 1) ? v.y : v.x;
+
+// raw spectra [b][t][mi] (complex float) -> Bp[mi][bg][tc][hi/lo][block], row
+// n = 2 (b - 64 bg) + (0: real, 1: imaginary part), through shared memory: a CTA takes 8 columns mi, one t chunk (64) and 8
+// maps (16 rows n), reads the spectra with 64-byte coalesced segments (the 8 columns of a
+// (b, t) pair), and writes every (column, core row group) as 1 KB of contiguous 16-byte
+// stores (8 consecutive k of one row per store, hi and lo).
+constexpr int kPackMaps = 8;
+constexpr int kPackCols = 8;
+constexpr int kPackTP = kTileK + 2;  // padded t row (float2)
+
+__global__ void __launch_bounds__(256) pack_kernel_b2(const float2* __restrict__ X, int B,
+                                                      int nth, int M, int nbg, int ntc,
+                                                      __nv_bfloat16* __restrict__ out) {
+  __shared__ __align__(16) float2 S[kPackCols][kPackMaps][kPackTP];
+  const int tid = threadIdx.x;
+  const int mi0 = blockIdx.x * kPackCols;
+  const int tc = blockIdx.y;
+  const int bg = blockIdx.z / (64 / kPackMaps), sub = blockIdx.z % (64 / kPackMaps);
+  const int bl0 = bg * 64 + sub * kPackMaps;  // first map of the CTA
+  for (int e = tid; e < kPackCols * kPackMaps * kTileK; e += 256) {
+    const int c = e & 7, tl = (e >> 3) % kTileK, bl = e / (8 * kTileK);
+    const int b = bl0 + bl, t = tc * kTileK + tl, mi = mi0 + c;
+    float2 v = make_float2(0.f, 0.f);
+    if (b < B && t < nth && mi < M) v = X[((size_t)b * nth + t) * M + mi];
+    S[c][bl][tl] = v;
+  }
+  __syncthreads();
+  // unit = 8 consecutive k of one row n of one column: id -> (c, row group, u), u fastest
+  for (int id = tid; id < kPackCols * 2 * 64; id += 256) {
+    const int u = id & 63, rgp = (id >> 6) & 1, c = id >> 7;
+    const int mi = mi0 + c;
+    if (mi >= M) continue;
+    const int nl = rgp * 8 + (u & 7);  // row within the CTA's 16 rows
+    const int kg = u >> 3;
+    const float4* src = reinterpret_cast<const float4*>(&S[c][nl >> 1][kg * 8]);
+    float x[8];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float4 w = src[j];  // two complex values
+      x[2 * j] = (nl & 1) ? w.y : w.x;
+      x[2 * j + 1] = (nl & 1) ? w.w : w.z;
     }
-    const __nv_bfloat16 hi = __float2bfloat16_rn(x);
-    const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+    __align__(16) __nv_bfloat16 hi[8], lo[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      hi[j] = __float2bfloat16_rn(x[j]);
+      lo[j] = __float2bfloat16_rn(x[j] - __bfloat162float(hi[j]));
+    }
+    const int n = sub * 16 + nl;
     __nv_bfloat16* blk = out + (((size_t)mi * nbg + bg) * ntc + tc) * 2 * kBlk;
-    const int off = core_off(n, k) / 2;
-    blk[off] = hi;
-    blk[kBlk + off] = lo;
+    const int off = core_off(n, kg * 8) / 2;
+    *reinterpret_cast<uint4*>(blk + off) = *reinterpret_cast<const uint4*>(hi);
+    *reinterpret_cast<uint4*>(blk + kBlk + off) = *reinterpret_cast<const uint4*>(lo);
   }
 }
 
@@ -313,8 +341,11 @@ cudaError_t launch_tc_pack_a(const float* K, int nth, int L, int M, void* out, c
 cudaError_t launch_tc_pack_b(const void* X, int B, int nth, int M, void* out, cudaStream_t s) {
   const int nbg = (B + 63) / 64, ntc = (nth + kTileK - 1) / kTileK;
   const long total = (long)M * nbg * ntc * kBlk;
-  pack_kernel_b<<<tgrid(total), 256, 0, s>>>((const float2*)X, B, nth, M, nbg, ntc,
-                                             (__nv_bfloat16*)out);
+  (void)total;
+  const dim3 grid((M + kPackCols - 1) / kPackCols, ntc, nbg * (64 / kPackMaps));
+  if (grid.y > 65535 || grid.z > 65535) return cudaErrorInvalidConfiguration;
+  pack_kernel_b2<<<grid, 256, 0, s>>>((const float2*)X, B, nth, M, nbg, ntc,
+                                      (__nv_bfloat16*)out);
   return cudaGetLastError();
 }
 
