@@ -340,13 +340,15 @@ def _time(torch, fn, steps, warmup, flush):
 
 
 def run_batched_precompute(torch, L=512, B=64, steps=5, warmup=2):
-    """GL sampling, spin +-2, 64 maps: precompute forward, FP32 SIMT vs BF16x3 tcgen05."""
+    """GL sampling, spin +-2, 64 maps: precompute forward and inverse, FP32 SIMT vs BF16x3
+    tcgen05."""
     import s2fft_b200
     from s2fft_b200 import _lib
 
     dev = torch.device("cuda", torch.cuda.current_device())
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
-    out = {"workload": f"precompute forward, GL, L={L}, {B} maps, spin +-2", "maps": B}
+    out = {"workload": f"precompute forward (and inverse), GL, L={L}, {B} maps, spin +-2",
+           "maps": B}
     for spin in (2, -2):
         rng = np.random.default_rng(1000 + spin)
         flm = np.stack([seeded_flm(rng, L, spin) for _ in range(B)])
@@ -389,6 +391,21 @@ def run_batched_precompute(torch, L=512, B=64, steps=5, warmup=2):
                 kbytes = L * nth * (2 * L - 1) * 4.0
                 res[prec]["kernel_table_gbs"] = kbytes / (kern_ms * 1e-3) / 1e9
             del K
+            torch.cuda.empty_cache()
+            # the inverse (flm -> maps) through the precomputed inverse kernel
+            Ki = s2fft_b200.precompute.spin_spherical_kernel(L, spin, False, "gl", None, False,
+                                                             precision=prec)
+            x32 = x64.to(torch.complex64)
+            ms_i = _time(torch, lambda: s2fft_b200.precompute.inverse(x32, L, spin, Ki, "gl",
+                                                                      precision=prec),
+                         steps, warmup, flush)
+            fi = s2fft_b200.precompute.inverse(x32, L, spin, Ki, "gl", precision=prec)
+            di = (fi.to(torch.complex128) - f64).abs()
+            res[prec]["inverse"] = {
+                "maps_per_s": B / (ms_i * 1e-3), "ms_per_batch": ms_i,
+                "max_rel_err": di.max().item() / f64.abs().max().item(),
+                "rms_rel_err": (di.pow(2).mean().sqrt() / f64.abs().pow(2).mean().sqrt()).item()}
+            del Ki
             torch.cuda.empty_cache()
         out[f"spin{spin:+d}"] = res
     return out

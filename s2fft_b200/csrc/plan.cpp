@@ -336,7 +336,7 @@ struct DevBuf {
 struct s2b_plan {
   s2b_desc d;
   bool fp64;
-  bool tc;      // S2B_BF16X3: tensor-core precompute forward
+  bool tc;      // S2B_BF16X3: tensor-core precompute contractions
   size_t rsz;   // sizeof(Real)
   int nth;      // rings of the sampling
   int nphi;     // equiangular ring length
@@ -394,7 +394,7 @@ struct s2b_plan {
   double* kth_inv = nullptr;
   double* kth_fwd = nullptr;
   int knth_inv = 0, knth_fwd = 0, kM = 0;
-  size_t ws_pre_fwd = 0;
+  size_t ws_pre_fwd = 0, ws_pre_inv = 0;
   // Wigner: one spin transform plan per n, gamma-DFT buffers
   std::vector<s2b_plan*> subs;
   size_t ws_w_fban = 0, ws_w_tmp = 0, ws_w_sub = 0;
@@ -877,12 +877,17 @@ static int build_plan(s2b_plan* p) {
   p->ws_adj_y = p->fwd_mode ? B * (size_t)(2 * L + 1) * (2 * L - 1) * c2 : 0;
   p->ws_pre_fwd = B * (size_t)p->knth_fwd * p->kM * c2;
   if (p->tc) p->ws_pre_fwd = align256(p->ws_pre_fwd) + tc_packed_b_bytes(p->knth_fwd, d.batch, p->kM);
+  p->ws_pre_inv = p->tc ? tc_packed_b_bytes(L, d.batch, p->kM) : 0;
   S2B_CK(cudaDeviceSynchronize());
   return S2B_OK;
 }
 
 
-static size_t inv_ws(const s2b_plan* p) { return align256(p->ws_inv_F) + align256(p->ws_inv_ftm); }
+static size_t inv_ws(const s2b_plan* p) {
+  // spin inverse: F and ftm; precompute inverse: ftm and (tensor cores) the packed flm
+  return std::max(align256(p->ws_inv_F) + align256(p->ws_inv_ftm),
+                  align256(p->ws_inv_ftm) + align256(p->ws_pre_inv));
+}
 static size_t inv_adj_ws(const s2b_plan* p) {
   return align256(p->ws_adj_G) + align256(p->ws_fwd_acc);
 }
@@ -1450,7 +1455,8 @@ static int run_forward(s2b_plan* p, const void* f, void* flm, char* ws, cudaStre
 // ----------------------------------------------------------------------------
 static size_t kernel_bytes(const s2b_plan* p, bool forward) {
   const int nth = forward ? p->knth_fwd : p->knth_inv;
-  if (p->tc && forward) return tc_packed_a_bytes(nth, p->d.L, p->kM);
+  if (p->tc) return forward ? tc_packed_a_bytes(nth, p->d.L, p->kM)
+                            : tc_packed_a_bytes(p->d.L, nth, p->kM);
   const size_t el = (p->d.sampling == S2B_HEALPIX ? 2 : 1) * p->rsz;
   return (size_t)nth * p->d.L * p->kM * el;
 }
@@ -1469,14 +1475,16 @@ static int build_kernel(s2b_plan* p, bool forward, void* K, cudaStream_t s) {
   kp.phi0 = d.sampling == S2B_HEALPIX ? p->hp_phi0 : nullptr;
   kp.lbin = p->lbin;
   kp.out = K;
-  if (p->tc && forward) {
+  if (p->tc) {
     // float table in a temporary buffer, then split into bf16 hi/lo and packed for the MMA
+    // (rows l and k = theta for the forward, rows theta and k = l for the inverse)
     const size_t tb = (size_t)kp.nth * d.L * p->kM * sizeof(float);
     void* tmp = nullptr;
     S2B_CK(cudaMalloc(&tmp, tb));
     kp.out = tmp;
     cudaError_t e = launch_kernel_table(false, kp, s);
-    if (e == cudaSuccess) e = launch_tc_pack_a((const float*)tmp, kp.nth, d.L, p->kM, K, s);
+    if (e == cudaSuccess)
+      e = launch_tc_pack_a((const float*)tmp, kp.nth, d.L, p->kM, forward ? 0 : 1, K, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     cudaFree(tmp);
     S2B_CK(e);
@@ -1506,7 +1514,32 @@ static int run_pre_inverse(s2b_plan* p, const void* K, const void* flm, void* f,
   cp.K = K;
   cp.in = flm;
   cp.out = ftm;
-  S2B_CK(launch_pre_contract(p->fp64, false, d.sampling == S2B_HEALPIX, cp, s));
+  if (p->tc) {
+    // per column: ftm[b][t] = sum_l K[t][l] flm[b][l] on the tensor cores (bf16 x3)
+    char* bp = ws + align256(ftm_bytes);
+    S2B_CK(launch_tc_pack_b(flm, d.batch, L, p->kM, (long)L * (2 * L - 1), 2 * L - 1,
+                            cp.mshift, bp, s));
+    TcParams tp{};
+    tp.L = L;
+    tp.nth = p->nth;
+    tp.M = p->kM;
+    tp.B = d.batch;
+    tp.rows = p->nth;
+    tp.kdim = L;
+    tp.sign = (float)cp.sign;
+    tp.Ap = reinterpret_cast<const __nv_bfloat16*>(K);
+    tp.Bp = reinterpret_cast<const __nv_bfloat16*>(bp);
+    tp.out = reinterpret_cast<float2*>(ftm);
+    tp.out_map = (long)p->nth * p->inv_ncol;
+    tp.out_row = p->inv_ncol;
+    tp.out_col0 = cp.mo;
+    tp.status = p->status;
+    if (p->ev_begin[0]) S2B_CK(cudaEventRecord(p->ev_begin[0], s));
+    S2B_CK(launch_tc_forward(tp, s));
+    if (p->ev_end[0]) S2B_CK(cudaEventRecord(p->ev_end[0], s));
+  } else {
+    S2B_CK(launch_pre_contract(p->fp64, false, d.sampling == S2B_HEALPIX, cp, s));
+  }
   RowsParams<Real> rp{};
   rp.L = L;
   rp.nrows = p->nth;
@@ -1579,13 +1612,18 @@ static int run_pre_forward(s2b_plan* p, const void* K, const void* f, void* flm,
   S2B_CK(cudaMemsetAsync(flm, 0, (size_t)d.batch * L * (2 * L - 1) * 2 * p->rsz, s));
   if (p->tc) {
     char* bp = raw + align256((size_t)d.batch * p->knth_fwd * p->kM * 2 * p->rsz);
-    S2B_CK(launch_tc_pack_b(raw, d.batch, p->knth_fwd, p->kM, bp, s));
+    S2B_CK(launch_tc_pack_b(raw, d.batch, p->knth_fwd, p->kM, (long)p->knth_fwd * p->kM, p->kM,
+                            0, bp, s));
     TcParams tp{};
     tp.L = L;
     tp.nth = p->knth_fwd;
     tp.M = p->kM;
     tp.B = d.batch;
-    tp.mshift = L - 1 + m0;
+    tp.rows = L;
+    tp.kdim = p->knth_fwd;
+    tp.out_map = (long)L * (2 * L - 1);
+    tp.out_row = 2 * L - 1;
+    tp.out_col0 = L - 1 + m0;
     tp.sign = (d.spin & 1) ? -1.f : 1.f;
     tp.Ap = reinterpret_cast<const __nv_bfloat16*>(K);
     tp.Bp = reinterpret_cast<const __nv_bfloat16*>(bp);

@@ -103,10 +103,11 @@ __device__ __forceinline__ void mma_commit(uint64_t* mb) {
 }  // namespace
 
 // ---------------------------------------------------------------------------
-// packing: K[t][l][mi] (float) -> Ap[mi][lt][tc][hi/lo][block]
+// packing: K[t][l][mi] (float) -> Ap[mi][rt][kc][hi/lo][block]; forward: rows l, k = t;
+// transposed (inverse): rows t, k = l
 // ---------------------------------------------------------------------------
 __global__ void pack_kernel_a(const float* __restrict__ K, int nth, int L, int M, int nlt, int ntc,
-                              __nv_bfloat16* __restrict__ out) {
+                              int transposed, __nv_bfloat16* __restrict__ out) {
   const long total = (long)M * nlt * ntc * kBlk;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
        i += (long)gridDim.x * blockDim.x) {
@@ -117,7 +118,8 @@ __global__ void pack_kernel_a(const float* __restrict__ K, int nth, int L, int M
     const int lt = (int)(rest % nlt);
     const int mi = (int)(rest / nlt);
     const int r = e / kTileK, k = e % kTileK;
-    const int l = lt * kTileR + r, t = tc * kTileK + k;
+    const int row = lt * kTileR + r, kk = tc * kTileK + k;
+    const int l = transposed ? kk : row, t = transposed ? row : kk;
     float x = 0.f;
     if (l < L && t < nth) x = K[((size_t)t * L + l) * M + mi];
     const __nv_bfloat16 hi = __float2bfloat16_rn(x);
@@ -130,8 +132,8 @@ __global__ void pack_kernel_a(const float* __restrict__ K, int nth, int L, int M
 }
 
 
-// raw spectra [b][t][mi] (complex float) -> Bp[mi][bg][tc][hi/lo][block], row
-// n = 2 (b - 64 bg) + (0: real, 1: imaginary part), through shared memory: a CTA takes 8 columns mi, one t chunk (64) and 8
+// data (map b, summation index t, column mi; complex float) -> Bp[mi][bg][tc][hi/lo][block],
+// row n = 2 (b - 64 bg) + (0: real, 1: imaginary part), through shared memory: a CTA takes 8 columns mi, one t chunk (64) and 8
 // maps (16 rows n), reads the spectra with 64-byte coalesced segments (the 8 columns of a
 // (b, t) pair), and writes every (column, core row group) as 1 KB of contiguous 16-byte
 // stores (8 consecutive k of one row per store, hi and lo).
@@ -140,7 +142,8 @@ constexpr int kPackCols = 8;
 constexpr int kPackTP = kTileK + 2;  // padded t row (float2)
 
 __global__ void __launch_bounds__(256) pack_kernel_b2(const float2* __restrict__ X, int B,
-                                                      int nth, int M, int nbg, int ntc,
+                                                      int kdim, int M, long in_map, int in_row,
+                                                      int in_col0, int nbg, int ntc,
                                                       __nv_bfloat16* __restrict__ out) {
   __shared__ __align__(16) float2 S[kPackCols][kPackMaps][kPackTP];
   const int tid = threadIdx.x;
@@ -152,7 +155,7 @@ __global__ void __launch_bounds__(256) pack_kernel_b2(const float2* __restrict__
     const int c = e & 7, tl = (e >> 3) % kTileK, bl = e / (8 * kTileK);
     const int b = bl0 + bl, t = tc * kTileK + tl, mi = mi0 + c;
     float2 v = make_float2(0.f, 0.f);
-    if (b < B && t < nth && mi < M) v = X[((size_t)b * nth + t) * M + mi];
+    if (b < B && t < kdim && mi < M) v = X[(size_t)b * in_map + (size_t)t * in_row + in_col0 + mi];
     S[c][bl][tl] = v;
   }
   __syncthreads();
@@ -296,11 +299,11 @@ __global__ void __launch_bounds__(128, 1) tc_forward_kernel(TcParams p) {
 #pragma unroll
         for (int x = 0; x < 32; ++x) v[j][x] = __uint_as_float(r[x]);
       }
-      if (l < p.L) {
+      if (l < p.rows) {
         for (int x = 0; x < 16; ++x) {
           const int b = bg * 64 + q * 16 + x;
           if (b >= p.B) break;
-          float2* row = p.out + ((size_t)b * p.L + l) * (2 * p.L - 1) + p.mshift + mi0;
+          float2* row = p.out + (size_t)b * p.out_map + (size_t)l * p.out_row + p.out_col0 + mi0;
 #pragma unroll
           for (int j = 0; j < kMPerCta; ++j)
             if (j < nm) row[j] = make_float2(p.sign * v[j][2 * x], p.sign * v[j][2 * x + 1]);
@@ -316,12 +319,12 @@ __global__ void __launch_bounds__(128, 1) tc_forward_kernel(TcParams p) {
                  : "memory");
 }
 
-size_t tc_packed_a_bytes(int nth, int L, int M) {
-  const int nlt = (L + kTileR - 1) / kTileR, ntc = (nth + kTileK - 1) / kTileK;
+size_t tc_packed_a_bytes(int kdim, int rows, int M) {
+  const int nlt = (rows + kTileR - 1) / kTileR, ntc = (kdim + kTileK - 1) / kTileK;
   return (size_t)M * nlt * ntc * 2 * kBlkBytes;
 }
-size_t tc_packed_b_bytes(int nth, int B, int M) {
-  const int nbg = (B + 63) / 64, ntc = (nth + kTileK - 1) / kTileK;
+size_t tc_packed_b_bytes(int kdim, int B, int M) {
+  const int nbg = (B + 63) / 64, ntc = (kdim + kTileK - 1) / kTileK;
   return (size_t)M * nbg * ntc * 2 * kBlkBytes;
 }
 
@@ -331,27 +334,29 @@ static int tgrid(long n) {
   return b < 1 ? 1 : (int)b;
 }
 
-cudaError_t launch_tc_pack_a(const float* K, int nth, int L, int M, void* out, cudaStream_t s) {
-  const int nlt = (L + kTileR - 1) / kTileR, ntc = (nth + kTileK - 1) / kTileK;
+cudaError_t launch_tc_pack_a(const float* K, int nth, int L, int M, int transposed, void* out,
+                             cudaStream_t s) {
+  const int rows = transposed ? nth : L, kdim = transposed ? L : nth;
+  const int nlt = (rows + kTileR - 1) / kTileR, ntc = (kdim + kTileK - 1) / kTileK;
   const long total = (long)M * nlt * ntc * kBlk;
-  pack_kernel_a<<<tgrid(total), 256, 0, s>>>(K, nth, L, M, nlt, ntc, (__nv_bfloat16*)out);
+  pack_kernel_a<<<tgrid(total), 256, 0, s>>>(K, nth, L, M, nlt, ntc, transposed,
+                                             (__nv_bfloat16*)out);
   return cudaGetLastError();
 }
 
-cudaError_t launch_tc_pack_b(const void* X, int B, int nth, int M, void* out, cudaStream_t s) {
-  const int nbg = (B + 63) / 64, ntc = (nth + kTileK - 1) / kTileK;
-  const long total = (long)M * nbg * ntc * kBlk;
-  (void)total;
+cudaError_t launch_tc_pack_b(const void* X, int B, int kdim, int M, long in_map, int in_row,
+                             int in_col0, void* out, cudaStream_t s) {
+  const int nbg = (B + 63) / 64, ntc = (kdim + kTileK - 1) / kTileK;
   const dim3 grid((M + kPackCols - 1) / kPackCols, ntc, nbg * (64 / kPackMaps));
   if (grid.y > 65535 || grid.z > 65535) return cudaErrorInvalidConfiguration;
-  pack_kernel_b2<<<grid, 256, 0, s>>>((const float2*)X, B, nth, M, nbg, ntc,
-                                      (__nv_bfloat16*)out);
+  pack_kernel_b2<<<grid, 256, 0, s>>>((const float2*)X, B, kdim, M, in_map, in_row, in_col0,
+                                      nbg, ntc, (__nv_bfloat16*)out);
   return cudaGetLastError();
 }
 
 cudaError_t launch_tc_forward(TcParams p, cudaStream_t s) {
-  p.nlt = (p.L + kTileR - 1) / kTileR;
-  p.ntc = (p.nth + kTileK - 1) / kTileK;
+  p.nlt = (p.rows + kTileR - 1) / kTileR;
+  p.ntc = (p.kdim + kTileK - 1) / kTileK;
   p.nbg = (p.B + 63) / 64;
   const size_t smem = (size_t)kStages * kStageBytes + 1024;
   cudaError_t e = cudaFuncSetAttribute(tc_forward_kernel,

@@ -1,7 +1,7 @@
 """Drop-in precompute-kernel transforms on one B200.
 
-Precision "bf16x3" runs the forward contraction on the tcgen05 tensor cores
-with 3-term bf16 split operands (its forward kernel is an opaque packed buffer).
+Precision "bf16x3" runs the contractions (forward and inverse) on the tcgen05 tensor
+cores with 3-term bf16 split operands (its kernels are opaque packed buffers).
 
 Mirrors upstream ``s2fft.precompute_transforms.spherical.inverse`` / ``forward``
 (s2fft/precompute_transforms/spherical.py:19-84, 226-311) and
@@ -57,7 +57,7 @@ def spin_spherical_kernel(L: int, spin: int = 0, reality: bool = False, sampling
     plan = _plan(dev, L, spin, nside, s, reality, precision, 1)
     n = ctypes.c_size_t()
     _lib.check(_lib.lib().s2b_kernel_size(plan.ptr, int(forward), ctypes.byref(n)))
-    if precision == "bf16x3" and forward:
+    if precision == "bf16x3":
         # packed bf16 hi/lo operand tiles for the tensor-core contraction (opaque)
         K = torch.empty(n.value, dtype=torch.uint8, device=dev)
     else:
@@ -73,9 +73,9 @@ def _kernel_tensor(kernel, L, s, nside, reality, forward, precision, spin, dev):
     cdt, rdt = _dtypes(precision)
     if kernel is None:
         return spin_spherical_kernel(L, spin, reality, s, nside, forward, precision=precision)
-    if precision == "bf16x3" and forward:
+    if precision == "bf16x3":
         if not (isinstance(kernel, torch.Tensor) and kernel.dtype == torch.uint8):
-            raise ValueError("bf16x3 forward needs the packed kernel from spin_spherical_kernel")
+            raise ValueError("bf16x3 needs the packed kernel from spin_spherical_kernel")
         return kernel.to(dev)
     want = cdt if s == "healpix" else rdt
     if isinstance(kernel, np.ndarray):

@@ -10,6 +10,7 @@ import os
 
 import numpy as np
 import pytest
+import torch
 
 import oracle
 from tests.conftest import GOLDEN_DIR, relerr
@@ -398,3 +399,26 @@ def test_precompute_batched_contraction(s2b, rng, sampling, precision, tol):
         one = s2b.precompute.forward(f[i], L, spin, kfw, sampling, False, nside=nside,
                                      precision=precision)
         assert relerr(g[i], one) < tol
+
+
+@pytest.mark.parametrize("sampling,spin,reality", [("gl", 2, False), ("mwss", -1, False),
+                                                   ("mw", 0, True), ("dh", 3, False)])
+def test_bf16x3_tensor_core_inverse(s2b, rng, sampling, spin, reality):
+    """Batched precompute inverse on tcgen05 (rows theta, K-dim l, bf16 x3 split, FP32
+    accumulation), 70 maps = two map groups, against the float64 transform."""
+    L, B = 40, 70
+    flms = np.stack([oracle.signal.generate_flm(rng, L, 0, spin, reality) for _ in range(B)])
+    K = s2b.precompute.spin_spherical_kernel(L, spin, reality, sampling, None, False,
+                                             precision="bf16x3")
+    assert K.dtype == torch.uint8
+    f = s2b.precompute.inverse(flms, L, spin, K, sampling, reality, precision="bf16x3")
+    ref = np.stack([oracle.spherical.inverse(flms[i], L, spin, None, sampling, reality)
+                    for i in (0, 37, B - 1)])
+    err = relerr(np.asarray(f)[[0, 37, B - 1]], ref)
+    assert err < 5e-5, err
+    f64 = s2b.precompute.inverse(flms, L, spin, None, sampling, reality)
+    assert relerr(f, f64) < 5e-5
+    from s2fft_b200 import _lib
+
+    for plan in list(_lib._plans.values()):
+        assert plan.status() == 0
