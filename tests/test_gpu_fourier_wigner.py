@@ -142,3 +142,44 @@ def test_round_trip_L128_N8_and_recursion_agreement(s2b):
     assert relerr(f, f_rec) < 1e-9
     f32 = fw.inverse_transform(flmn, L, N, precision="f32")
     assert relerr(f32, f) < 1e-5
+
+
+@pytest.mark.parametrize("L,N,sampling,reality", [(2, 1, "mw", False), (2, 2, "mwss", True),
+                                                  (3, 1, "mwss", False), (5, 5, "mw", True),
+                                                  (7, 3, "mwss", False)])
+def test_small_band_limits(s2b, L, N, sampling, reality):
+    """Tiny band-limits and N = 1 / N = L against the oracle (which is pinned to upstream)."""
+    rng = np.random.default_rng(L * 10 + N)
+    flmn = oracle.signal.generate_flmn(rng, L, N, 0, reality)
+    fw = s2b.fourier_wigner
+    f = fw.inverse_transform(flmn, L, N, None, reality, sampling)
+    ref = oracle.fourier_wigner.inverse_transform(flmn, L, N, None, reality, sampling)
+    np.testing.assert_allclose(f, ref, atol=1e-12)
+    g = fw.forward_transform(ref, L, N, None, reality, sampling)
+    gref = oracle.fourier_wigner.forward_transform(ref, L, N, None, reality, sampling)
+    np.testing.assert_allclose(g, gref, atol=1e-12)
+    np.testing.assert_allclose(g, flmn, atol=1e-12)
+
+
+def test_subset_ops_single_slice_and_f32_batches(s2b):
+    """One spin, one map, one channel; and a larger float32 batch against the float64 call."""
+    L = 12
+    rng = np.random.default_rng(3)
+    DW = s2b.fourier_wigner.fourier_wigner_kernel(L)
+    ops = s2b.custom_ops
+    for sampling in ("mw", "mwss"):
+        full = oracle.signal.generate_flmn(rng, L, 4, 0, False)
+        flmn = full[3 + 2][None, None, :, :, None]  # n = 2 -> spin -2
+        sp = np.array([-2])
+        fs = ops.wigner_subset_to_s2(flmn, sp, DW, L, sampling)
+        ref = oracle.fourier_wigner.wigner_subset_to_s2(
+            flmn, sp, oracle.fourier_wigner.fourier_wigner_kernel(L), L, sampling)
+        np.testing.assert_allclose(fs, ref, atol=1e-12)
+        back = ops.s2_to_wigner_subset(fs, sp, DW, L, sampling)
+        np.testing.assert_allclose(back, flmn, atol=1e-12)
+    x = (rng.standard_normal((5, 3, L, 2 * L - 1, 4))
+         + 1j * rng.standard_normal((5, 3, L, 2 * L - 1, 4)))
+    sp = np.array([0, 3, -5])
+    y64 = ops.wigner_subset_to_s2(x, sp, DW, L, "mw")
+    y32 = ops.wigner_subset_to_s2(x, sp, DW, L, "mw", precision="f32")
+    assert relerr(y32, y64) < 1e-5
