@@ -183,3 +183,37 @@ def test_subset_ops_single_slice_and_f32_batches(s2b):
     y64 = ops.wigner_subset_to_s2(x, sp, DW, L, "mw")
     y32 = ops.wigner_subset_to_s2(x, sp, DW, L, "mw", precision="f32")
     assert relerr(y32, y64) < 1e-5
+
+
+def test_c_abi_errors(s2b):
+    """The Fourier-Wigner entry points reject a short workspace, NULL or misaligned pointers
+    and too many slices with a status code (no launch)."""
+    import ctypes
+
+    from s2fft_b200 import _lib
+    from s2fft_b200 import fourier_wigner as fw
+
+    L, N = 8, 3
+    lib = fw._fwlib()
+    plan = fw.get_plan(torch.device("cuda", 0), L, "mw", "f64", N)
+    delta, quads = fw.fourier_wigner_kernel(L)
+    flmn = torch.zeros((2 * N - 1, L, 2 * L - 1), dtype=torch.complex128, device="cuda")
+    f = torch.empty((2 * N - 1, L, 2 * L - 1), dtype=torch.complex128, device="cuda")
+    need = int(lib.s2b_fw_workspace_size(plan.ptr, fw.OP_INVERSE, 1, 0, 1))
+    ws = torch.empty(need, dtype=torch.uint8, device="cuda")
+    st = _lib.stream_handle(torch.device("cuda", 0))
+    assert lib.s2b_fw_inverse(plan.ptr, 1, 0, delta.data_ptr(), flmn.data_ptr(), f.data_ptr(),
+                              ws.data_ptr(), need, st) == 0
+    assert lib.s2b_fw_inverse(plan.ptr, 1, 0, delta.data_ptr(), flmn.data_ptr(), f.data_ptr(),
+                              ws.data_ptr(), need - 1, st) == 3
+    assert lib.s2b_fw_inverse(plan.ptr, 1, 0, None, flmn.data_ptr(), f.data_ptr(),
+                              ws.data_ptr(), need, st) == 4
+    assert lib.s2b_fw_inverse(plan.ptr, 1, 0, delta.data_ptr(), flmn.data_ptr() + 8,
+                              f.data_ptr(), ws.data_ptr(), need, st) == 4
+    assert lib.s2b_fw_inverse(plan.ptr, 70000, 0, delta.data_ptr(), flmn.data_ptr(),
+                              f.data_ptr(), ws.data_ptr(), need, st) == 1
+    spins = torch.zeros(1, dtype=torch.int32, device="cuda")
+    assert lib.s2b_fw_subset_to_s2(plan.ptr, 1, 0, spins.data_ptr(), delta.data_ptr(),
+                                   flmn.data_ptr(), f.data_ptr(), ws.data_ptr(), need, st) == 1
+    assert lib.s2b_last_error()
+    torch.cuda.synchronize()
