@@ -64,7 +64,7 @@ enum s2b_sampling { S2B_MW = 0, S2B_MWSS = 1, S2B_DH = 2, S2B_GL = 3, S2B_HEALPI
 /* S2B_BF16X3: as S2B_F32, except that the precompute contractions (forward and
  *          inverse) run on the tcgen05 tensor cores with 3-term bf16 split operands
  *          (hi*hi + hi*lo + lo*hi) and FP32 accumulation; their kernel tables are the
- *          packed bf16 layouts produced by s2b_kernel_build (equiangular samplings). */
+ *          packed bf16 layouts produced by s2b_kernel_build (spin plans, every sampling). */
 enum s2b_precision { S2B_F64 = 0, S2B_F32 = 1, S2B_BF16X3 = 2 };
 
 typedef struct s2b_desc {

@@ -876,8 +876,10 @@ static int build_plan(s2b_plan* p) {
   p->ws_adj_G = B * p->nhalf * (size_t)p->TR * p->adj_Gs * acc;
   p->ws_adj_y = p->fwd_mode ? B * (size_t)(2 * L + 1) * (2 * L - 1) * c2 : 0;
   p->ws_pre_fwd = B * (size_t)p->knth_fwd * p->kM * c2;
-  if (p->tc) p->ws_pre_fwd = align256(p->ws_pre_fwd) + tc_packed_b_bytes(p->knth_fwd, d.batch, p->kM);
-  p->ws_pre_inv = p->tc ? tc_packed_b_bytes(L, d.batch, p->kM) : 0;
+  const int hpc = d.sampling == S2B_HEALPIX;  // complex kernel tables
+  if (p->tc)
+    p->ws_pre_fwd = align256(p->ws_pre_fwd) + tc_packed_b_bytes(p->knth_fwd, d.batch, p->kM, hpc);
+  p->ws_pre_inv = p->tc ? tc_packed_b_bytes(L, d.batch, p->kM, hpc) : 0;
   S2B_CK(cudaDeviceSynchronize());
   return S2B_OK;
 }
@@ -1455,8 +1457,9 @@ static int run_forward(s2b_plan* p, const void* f, void* flm, char* ws, cudaStre
 // ----------------------------------------------------------------------------
 static size_t kernel_bytes(const s2b_plan* p, bool forward) {
   const int nth = forward ? p->knth_fwd : p->knth_inv;
-  if (p->tc) return forward ? tc_packed_a_bytes(nth, p->d.L, p->kM)
-                            : tc_packed_a_bytes(p->d.L, nth, p->kM);
+  const int hpc = p->d.sampling == S2B_HEALPIX;
+  if (p->tc) return forward ? tc_packed_a_bytes(nth, p->d.L, p->kM, hpc)
+                            : tc_packed_a_bytes(p->d.L, nth, p->kM, hpc);
   const size_t el = (p->d.sampling == S2B_HEALPIX ? 2 : 1) * p->rsz;
   return (size_t)nth * p->d.L * p->kM * el;
 }
@@ -1478,13 +1481,14 @@ static int build_kernel(s2b_plan* p, bool forward, void* K, cudaStream_t s) {
   if (p->tc) {
     // float table in a temporary buffer, then split into bf16 hi/lo and packed for the MMA
     // (rows l and k = theta for the forward, rows theta and k = l for the inverse)
-    const size_t tb = (size_t)kp.nth * d.L * p->kM * sizeof(float);
+    const size_t tb = (size_t)kp.nth * d.L * p->kM * sizeof(float) * (kp.complex_out ? 2 : 1);
     void* tmp = nullptr;
     S2B_CK(cudaMalloc(&tmp, tb));
     kp.out = tmp;
     cudaError_t e = launch_kernel_table(false, kp, s);
     if (e == cudaSuccess)
-      e = launch_tc_pack_a((const float*)tmp, kp.nth, d.L, p->kM, forward ? 0 : 1, K, s);
+      e = launch_tc_pack_a((const float*)tmp, kp.nth, d.L, p->kM, forward ? 0 : 1,
+                           kp.complex_out ? 1 : 0, K, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     cudaFree(tmp);
     S2B_CK(e);
@@ -1517,8 +1521,9 @@ static int run_pre_inverse(s2b_plan* p, const void* K, const void* flm, void* f,
   if (p->tc) {
     // per column: ftm[b][t] = sum_l K[t][l] flm[b][l] on the tensor cores (bf16 x3)
     char* bp = ws + align256(ftm_bytes);
+    const int hpc = d.sampling == S2B_HEALPIX;
     S2B_CK(launch_tc_pack_b(flm, d.batch, L, p->kM, (long)L * (2 * L - 1), 2 * L - 1,
-                            cp.mshift, bp, s));
+                            cp.mshift, hpc, bp, s));
     TcParams tp{};
     tp.L = L;
     tp.nth = p->nth;
@@ -1526,6 +1531,7 @@ static int run_pre_inverse(s2b_plan* p, const void* K, const void* flm, void* f,
     tp.B = d.batch;
     tp.rows = p->nth;
     tp.kdim = L;
+    tp.cplx = hpc;
     tp.sign = (float)cp.sign;
     tp.Ap = reinterpret_cast<const __nv_bfloat16*>(K);
     tp.Bp = reinterpret_cast<const __nv_bfloat16*>(bp);
@@ -1612,8 +1618,9 @@ static int run_pre_forward(s2b_plan* p, const void* K, const void* f, void* flm,
   S2B_CK(cudaMemsetAsync(flm, 0, (size_t)d.batch * L * (2 * L - 1) * 2 * p->rsz, s));
   if (p->tc) {
     char* bp = raw + align256((size_t)d.batch * p->knth_fwd * p->kM * 2 * p->rsz);
+    const int hpc = d.sampling == S2B_HEALPIX;
     S2B_CK(launch_tc_pack_b(raw, d.batch, p->knth_fwd, p->kM, (long)p->knth_fwd * p->kM, p->kM,
-                            0, bp, s));
+                            0, hpc, bp, s));
     TcParams tp{};
     tp.L = L;
     tp.nth = p->knth_fwd;
@@ -1621,6 +1628,7 @@ static int run_pre_forward(s2b_plan* p, const void* K, const void* f, void* flm,
     tp.B = d.batch;
     tp.rows = L;
     tp.kdim = p->knth_fwd;
+    tp.cplx = hpc;
     tp.out_map = (long)L * (2 * L - 1);
     tp.out_row = 2 * L - 1;
     tp.out_col0 = L - 1 + m0;
@@ -1837,8 +1845,8 @@ int s2b_plan_create(const s2b_desc* desc, s2b_plan** out) {
   }
   if (d.precision != S2B_F64 && d.precision != S2B_F32 && d.precision != S2B_BF16X3)
     return fail(S2B_ERR_INVALID, "unknown precision");
-  if (d.precision == S2B_BF16X3 && (d.sampling == S2B_HEALPIX || d.N > 0))
-    return fail(S2B_ERR_INVALID, "BF16x3 plans support the equiangular precompute path");
+  if (d.precision == S2B_BF16X3 && d.N > 0)
+    return fail(S2B_ERR_INVALID, "BF16x3 plans support the precompute path of spin transforms");
   if (d.reality && d.spin != 0) return fail(S2B_ERR_INVALID, "reality requires spin 0");
   if (std::abs(d.spin) >= d.L) return fail(S2B_ERR_INVALID, "|spin| must be < L");
   if (d.L_lower < 0 || d.L_lower >= d.L) return fail(S2B_ERR_INVALID, "0 <= L_lower < L");

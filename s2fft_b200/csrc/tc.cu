@@ -107,7 +107,10 @@ __device__ __forceinline__ void mma_commit(uint64_t* mb) {
 // transposed (inverse): rows t, k = l
 // ---------------------------------------------------------------------------
 __global__ void pack_kernel_a(const float* __restrict__ K, int nth, int L, int M, int nlt, int ntc,
-                              int transposed, __nv_bfloat16* __restrict__ out) {
+                              int transposed, int cplx, __nv_bfloat16* __restrict__ out) {
+  // cplx: K is complex (float2) and the K dimension is doubled: chunks tc < ntc / 2 hold
+  // Re K, chunks tc >= ntc / 2 hold Im K of the same summation indices
+  const int nth_c = cplx ? ntc / 2 : ntc;
   const long total = (long)M * nlt * ntc * kBlk;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
        i += (long)gridDim.x * blockDim.x) {
@@ -118,10 +121,16 @@ __global__ void pack_kernel_a(const float* __restrict__ K, int nth, int L, int M
     const int lt = (int)(rest % nlt);
     const int mi = (int)(rest / nlt);
     const int r = e / kTileK, k = e % kTileK;
-    const int row = lt * kTileR + r, kk = tc * kTileK + k;
+    const int part = tc >= nth_c ? 1 : 0;  // 0: real, 1: imaginary (cplx only)
+    const int row = lt * kTileR + r, kk = (tc - part * nth_c) * kTileK + k;
     const int l = transposed ? kk : row, t = transposed ? row : kk;
     float x = 0.f;
-    if (l < L && t < nth) x = K[((size_t)t * L + l) * M + mi];
+    if (l < L && t < nth) {
+      const size_t o = ((size_t)t * L + l) * M + mi;
+      x = cplx ? (part ? reinterpret_cast<const float2*>(K)[o].y
+                       : reinterpret_cast<const float2*>(K)[o].x)
+               : K[o];
+    }
     const __nv_bfloat16 hi = __float2bfloat16_rn(x);
     const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
     __nv_bfloat16* blk = out + (((size_t)mi * nlt + lt) * ntc + tc) * 2 * kBlk;
@@ -143,17 +152,22 @@ constexpr int kPackTP = kTileK + 2;  // padded t row (float2)
 
 __global__ void __launch_bounds__(256) pack_kernel_b2(const float2* __restrict__ X, int B,
                                                       int kdim, int M, long in_map, int in_row,
-                                                      int in_col0, int nbg, int ntc,
+                                                      int in_col0, int nbg, int ntc, int cplx,
                                                       __nv_bfloat16* __restrict__ out) {
+  // cplx: chunks tc >= ntc / 2 repeat the summation indices of chunk tc - ntc / 2 with the
+  // rows (re, im) replaced by (-im, re), so that [Re K | Im K] x this gives the complex product
   __shared__ __align__(16) float2 S[kPackCols][kPackMaps][kPackTP];
   const int tid = threadIdx.x;
   const int mi0 = blockIdx.x * kPackCols;
   const int tc = blockIdx.y;
+  const int half = cplx ? ntc / 2 : ntc;
+  const int part = tc >= half ? 1 : 0;
+  const int tq = tc - part * half;  // chunk of summation indices
   const int bg = blockIdx.z / (64 / kPackMaps), sub = blockIdx.z % (64 / kPackMaps);
   const int bl0 = bg * 64 + sub * kPackMaps;  // first map of the CTA
   for (int e = tid; e < kPackCols * kPackMaps * kTileK; e += 256) {
     const int c = e & 7, tl = (e >> 3) % kTileK, bl = e / (8 * kTileK);
-    const int b = bl0 + bl, t = tc * kTileK + tl, mi = mi0 + c;
+    const int b = bl0 + bl, t = tq * kTileK + tl, mi = mi0 + c;
     float2 v = make_float2(0.f, 0.f);
     if (b < B && t < kdim && mi < M) v = X[(size_t)b * in_map + (size_t)t * in_row + in_col0 + mi];
     S[c][bl][tl] = v;
@@ -171,8 +185,13 @@ __global__ void __launch_bounds__(256) pack_kernel_b2(const float2* __restrict__
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const float4 w = src[j];  // two complex values
-      x[2 * j] = (nl & 1) ? w.y : w.x;
-      x[2 * j + 1] = (nl & 1) ? w.w : w.z;
+      if (part == 0) {
+        x[2 * j] = (nl & 1) ? w.y : w.x;
+        x[2 * j + 1] = (nl & 1) ? w.w : w.z;
+      } else {  // rows (-im, re)
+        x[2 * j] = (nl & 1) ? w.x : -w.y;
+        x[2 * j + 1] = (nl & 1) ? w.z : -w.w;
+      }
     }
     __align__(16) __nv_bfloat16 hi[8], lo[8];
 #pragma unroll
@@ -319,13 +338,13 @@ __global__ void __launch_bounds__(128, 1) tc_forward_kernel(TcParams p) {
                  : "memory");
 }
 
-size_t tc_packed_a_bytes(int kdim, int rows, int M) {
+size_t tc_packed_a_bytes(int kdim, int rows, int M, int cplx) {
   const int nlt = (rows + kTileR - 1) / kTileR, ntc = (kdim + kTileK - 1) / kTileK;
-  return (size_t)M * nlt * ntc * 2 * kBlkBytes;
+  return (size_t)M * nlt * ntc * (cplx ? 2 : 1) * 2 * kBlkBytes;
 }
-size_t tc_packed_b_bytes(int kdim, int B, int M) {
+size_t tc_packed_b_bytes(int kdim, int B, int M, int cplx) {
   const int nbg = (B + 63) / 64, ntc = (kdim + kTileK - 1) / kTileK;
-  return (size_t)M * nbg * ntc * 2 * kBlkBytes;
+  return (size_t)M * nbg * ntc * (cplx ? 2 : 1) * 2 * kBlkBytes;
 }
 
 static int tgrid(long n) {
@@ -334,29 +353,30 @@ static int tgrid(long n) {
   return b < 1 ? 1 : (int)b;
 }
 
-cudaError_t launch_tc_pack_a(const float* K, int nth, int L, int M, int transposed, void* out,
-                             cudaStream_t s) {
+cudaError_t launch_tc_pack_a(const float* K, int nth, int L, int M, int transposed, int cplx,
+                             void* out, cudaStream_t s) {
   const int rows = transposed ? nth : L, kdim = transposed ? L : nth;
-  const int nlt = (rows + kTileR - 1) / kTileR, ntc = (kdim + kTileK - 1) / kTileK;
+  const int nlt = (rows + kTileR - 1) / kTileR;
+  const int ntc = ((kdim + kTileK - 1) / kTileK) * (cplx ? 2 : 1);
   const long total = (long)M * nlt * ntc * kBlk;
-  pack_kernel_a<<<tgrid(total), 256, 0, s>>>(K, nth, L, M, nlt, ntc, transposed,
+  pack_kernel_a<<<tgrid(total), 256, 0, s>>>(K, nth, L, M, nlt, ntc, transposed, cplx,
                                              (__nv_bfloat16*)out);
   return cudaGetLastError();
 }
 
 cudaError_t launch_tc_pack_b(const void* X, int B, int kdim, int M, long in_map, int in_row,
-                             int in_col0, void* out, cudaStream_t s) {
-  const int nbg = (B + 63) / 64, ntc = (kdim + kTileK - 1) / kTileK;
+                             int in_col0, int cplx, void* out, cudaStream_t s) {
+  const int nbg = (B + 63) / 64, ntc = ((kdim + kTileK - 1) / kTileK) * (cplx ? 2 : 1);
   const dim3 grid((M + kPackCols - 1) / kPackCols, ntc, nbg * (64 / kPackMaps));
   if (grid.y > 65535 || grid.z > 65535) return cudaErrorInvalidConfiguration;
   pack_kernel_b2<<<grid, 256, 0, s>>>((const float2*)X, B, kdim, M, in_map, in_row, in_col0,
-                                      nbg, ntc, (__nv_bfloat16*)out);
+                                      nbg, ntc, cplx, (__nv_bfloat16*)out);
   return cudaGetLastError();
 }
 
 cudaError_t launch_tc_forward(TcParams p, cudaStream_t s) {
   p.nlt = (p.rows + kTileR - 1) / kTileR;
-  p.ntc = (p.kdim + kTileK - 1) / kTileK;
+  p.ntc = ((p.kdim + kTileK - 1) / kTileK) * (p.cplx ? 2 : 1);
   p.nbg = (p.B + 63) / 64;
   const size_t smem = (size_t)kStages * kStageBytes + 1024;
   cudaError_t e = cudaFuncSetAttribute(tc_forward_kernel,

@@ -422,3 +422,26 @@ def test_bf16x3_tensor_core_inverse(s2b, rng, sampling, spin, reality):
 
     for plan in list(_lib._plans.values()):
         assert plan.status() == 0
+
+
+@pytest.mark.parametrize("reality", [False, True])
+def test_bf16x3_tensor_core_healpix(s2b, rng, reality):
+    """HEALPix kernels are complex (ring phases folded in): on the tensor cores the K
+    dimension is doubled ([Re K | Im K] against [[Re x; Im x] | [-Im x; Re x]]). 70 maps,
+    both directions, against the float64 precompute path."""
+    L, nside, B = 16, 8, 70
+    flms = np.stack([oracle.signal.generate_flm(rng, L, 0, 0, reality) for _ in range(B)])
+    kin = s2b.precompute.spin_spherical_kernel(L, 0, reality, "healpix", nside, False,
+                                               precision="bf16x3")
+    f = s2b.precompute.inverse(flms, L, 0, kin, "healpix", reality, nside=nside,
+                               precision="bf16x3")
+    f64 = s2b.precompute.inverse(flms, L, 0, None, "healpix", reality, nside=nside)
+    assert relerr(f, f64) < 5e-5
+    ref = oracle.spherical.inverse(flms[5], L, 0, nside, "healpix", reality)
+    assert relerr(np.asarray(f)[5], ref) < 5e-5
+    kfw = s2b.precompute.spin_spherical_kernel(L, 0, reality, "healpix", nside, True,
+                                               precision="bf16x3")
+    g = s2b.precompute.forward(f64, L, 0, kfw, "healpix", reality, nside=nside,
+                               precision="bf16x3")
+    g64 = s2b.precompute.forward(f64, L, 0, None, "healpix", reality, nside=nside)
+    assert relerr(g, g64) < 5e-5
