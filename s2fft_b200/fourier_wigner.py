@@ -7,7 +7,7 @@
 factored through the planes Delta^l = d^l(pi/2) and FFTs over (alpha, beta, gamma).
 ``precomps`` is ``(delta, quads)`` as returned by ``fourier_wigner_kernel(L)``
 (construct.py:614-639); without it the kernel is built on the device for the call (and
-cached per device and L). Unlike upstream a leading batch dimension is accepted, and
+cached per device and L while the planes take at most 2 GiB). Unlike upstream a leading batch dimension is accepted, and
 ``precision="f32"`` runs the transform in float (the planes stay float64).
 """
 
@@ -131,6 +131,11 @@ def fourier_wigner_kernel(L: int):
     return delta, quads
 
 
+# planes built for calls without precomps are kept per (device, L) up to this size; larger
+# ones (L (2L-1)^2 float64: 2.1 GB at L=512, 34 GB at L=1024) are rebuilt on every call
+_KERNEL_CACHE_BYTES = 1 << 31
+
+
 def _precomps(precomps, L, dev):
     if precomps is None:
         key = (str(dev), L)
@@ -138,8 +143,9 @@ def _precomps(precomps, L, dev):
             k = _kernels.get(key)
         if k is None:
             k = fourier_wigner_kernel(L)
-            with _plans_lock:
-                _kernels[key] = k
+            if k[0].numel() * 8 <= _KERNEL_CACHE_BYTES:
+                with _plans_lock:
+                    _kernels[key] = k
         return k
     delta, quads = precomps
     delta, _, _ = _to_device(delta, torch.float64, dev)
