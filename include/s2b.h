@@ -153,6 +153,19 @@ int s2b_precompute_inverse(s2b_plan* plan, const void* kernel, const void* flm, 
 int s2b_precompute_forward(s2b_plan* plan, const void* kernel, const void* f, void* flm,
                            void* workspace, size_t workspace_bytes, void* stream);
 
+/* Adjoints (conjugate transposes) of the precompute transforms for reverse-mode
+ * differentiation, with the same kernel table and workspace as the call they invert the
+ * direction of: g_flm = A^H g_f for A = s2b_precompute_inverse, g_f = A^H g_flm for
+ * A = s2b_precompute_forward. Complex plans (reality = 0) with float or double tables
+ * (not S2B_BF16X3). Replace JAX's autodiff of upstream's precompute einsums and FFTs
+ * (s2fft/precompute_transforms/spherical.py:87-149, 314-380). */
+int s2b_precompute_inverse_adjoint(s2b_plan* plan, const void* kernel, const void* g_f,
+                                   void* g_flm, void* workspace, size_t workspace_bytes,
+                                   void* stream);
+int s2b_precompute_forward_adjoint(s2b_plan* plan, const void* kernel, const void* g_flm,
+                                   void* g_f, void* workspace, size_t workspace_bytes,
+                                   void* stream);
+
 /* Device status of the plan (synchronous): *status != 0 after a bounded
  * wait inside a kernel ran out (the kernel then skipped its work); returns
  * S2B_ERR_TIMEOUT in that case. No upstream counterpart (upstream exits the

@@ -59,6 +59,8 @@ _SIGS = {
     "s2b_plan_set_tuning": [ctypes.c_void_p, ctypes.c_int, ctypes.c_int],
     "s2b_inverse_adjoint": [ctypes.c_void_p] * 4 + [ctypes.c_size_t, ctypes.c_void_p],
     "s2b_forward_adjoint": [ctypes.c_void_p] * 4 + [ctypes.c_size_t, ctypes.c_void_p],
+    "s2b_precompute_inverse_adjoint": [ctypes.c_void_p] * 5 + [ctypes.c_size_t, ctypes.c_void_p],
+    "s2b_precompute_forward_adjoint": [ctypes.c_void_p] * 5 + [ctypes.c_size_t, ctypes.c_void_p],
     "s2b_rotate_flms": [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                         ctypes.c_double, ctypes.c_double] + [ctypes.c_void_p] * 4
                        + [ctypes.c_size_t, ctypes.c_void_p],

@@ -1658,6 +1658,105 @@ static int run_pre_forward(s2b_plan* p, const void* K, const void* f, void* flm,
   return S2B_OK;
 }
 
+// Adjoints of the precompute transforms (complex plans, float or double tables): the
+// conjugate-transposed contraction with the same kernel table, composed with the adjoints
+// of the ring stages (unnormalised ring DFTs for the inverse; for the forward, inverse
+// ring DFTs and, on mw / mwss, the adjoint of the resampling chain in its raw form).
+template <typename Real>
+static int run_pre_inverse_adjoint(s2b_plan* p, const void* K, const void* gf, void* gflm,
+                                   char* ws, cudaStream_t s) {
+  const s2b_desc& d = p->d;
+  const int L = d.L;
+  char* raw = ws;  // [B][nth][M] spectra of g_f, m = -(L-1) .. L-1
+  RowsParams<Real> rp{};
+  rp.L = L;
+  rp.nrows = p->nth;
+  rp.scale = 1.0;
+  rp.desc = d.sampling == S2B_HEALPIX ? p->descs : p->descs + p->row_desc;
+  rp.ring_desc = d.sampling == S2B_HEALPIX ? p->ring_desc : nullptr;
+  rp.ring_off = p->ring_off;
+  rp.out_batch_stride = p->npix;
+  rp.tb = tables<Real>(p);
+  rp.in = gf;
+  rp.out = raw;
+  rp.mode = FWD_TO_RAW;
+  rp.M = p->kM;
+  rp.m0 = -(L - 1);
+  S2B_CK(launch_fwd_rows<Real>(rp, p->nth, d.batch, p->maxM, s));
+  PreContractParams cp{};
+  cp.L = L;
+  cp.nth = p->nth;  // the inverse table has the sampling's rings (as s2b_precompute_inverse)
+  cp.M = p->kM;
+  cp.batch = d.batch;
+  cp.mshift = 0;
+  cp.sign = (d.spin & 1) ? -1.0 : 1.0;
+  cp.conj = 1;
+  cp.K = K;
+  cp.in = raw;
+  cp.out = gflm;
+  S2B_CK(launch_pre_contract(p->fp64, true, d.sampling == S2B_HEALPIX, cp, s));
+  return S2B_OK;
+}
+
+template <typename Real>
+static int run_pre_forward_adjoint(s2b_plan* p, const void* K, const void* gflm, void* gf,
+                                   char* ws, cudaStream_t s) {
+  const s2b_desc& d = p->d;
+  const int L = d.L;
+  char* cols = ws;
+  char* raw = cols + align256(p->ws_fwd_cols);  // [B][knth_fwd][M]
+  PreContractParams cp{};
+  cp.L = L;
+  cp.nth = p->knth_fwd;
+  cp.M = p->kM;
+  cp.batch = d.batch;
+  cp.mshift = 0;
+  cp.mo = 0;
+  cp.ncol = p->kM;
+  cp.sign = (d.spin & 1) ? -1.0 : 1.0;
+  cp.conj = 1;
+  cp.K = K;
+  cp.in = gflm;
+  cp.out = raw;
+  S2B_CK(launch_pre_contract(p->fp64, false, d.sampling == S2B_HEALPIX, cp, s));
+  RowsParams<Real> rp{};
+  rp.L = L;
+  rp.nrows = p->nth;
+  rp.scale = 1.0;
+  rp.desc = d.sampling == S2B_HEALPIX ? p->descs : p->descs + p->row_desc;
+  rp.ring_desc = d.sampling == S2B_HEALPIX ? p->ring_desc : nullptr;
+  rp.ring_off = p->ring_off;
+  rp.out_batch_stride = p->npix;
+  rp.tb = tables<Real>(p);
+  rp.out = gf;
+  if (p->fwd_mode == 0) {
+    rp.ncol = p->kM;
+    rp.mo = 0;
+    rp.in = raw;
+  } else {
+    ColsParams<Real> cc{};
+    cc.L = L;
+    cc.spin = d.spin;
+    cc.mw = p->fwd_mode == 1;
+    cc.nin = p->nth;
+    cc.raw = 1;
+    cc.scale = p->fwd_mode == 1 ? (2.0 * L) / (2.0 * L - 1.0) : 1.0;
+    cc.d1 = p->descs + p->col_d1;
+    cc.d2 = p->descs + p->col_d2;
+    cc.ph_adj = p->col_ph_adj;
+    cc.tb = tables<Real>(p);
+    cc.in = raw;
+    cc.out = cols;
+    const int ncm = p->fwd_mode == 1 ? 2 * L - 1 : 2 * L;
+    S2B_CK(launch_mw_cols_adj<Real>(cc, ncm, d.batch, p->M1, p->M2, p->inv_ncol, p->inv_mo, s));
+    rp.ncol = p->inv_ncol;
+    rp.mo = p->inv_mo;
+    rp.in = cols;
+  }
+  S2B_CK(launch_inv_rows<Real>(rp, p->nth, d.batch, p->maxM, s));
+  return S2B_OK;
+}
+
 // ----------------------------------------------------------------------------
 // Wigner (SO(3)) transforms: 2N-1 spin transforms + gamma DFT
 // (s2fft/transforms/wigner.py:110-196, 442-533)
@@ -1986,6 +2085,39 @@ int s2b_precompute_forward(s2b_plan* p, const void* K, const void* f, void* flm,
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   return p->fp64 ? run_pre_forward<double>(p, K, f, flm, (char*)ws, s)
                  : run_pre_forward<float>(p, K, f, flm, (char*)ws, s);
+}
+
+static int check_pre_adjoint(const s2b_plan* p) {
+  if (!p || p->d.N > 0) return fail(S2B_ERR_INVALID, "bad plan");
+  if (p->d.reality) return fail(S2B_ERR_INVALID, "adjoints are defined for complex plans (reality = 0)");
+  if (p->tc) return fail(S2B_ERR_INVALID, "adjoints need a float or double kernel table (not BF16x3)");
+  return S2B_OK;
+}
+
+int s2b_precompute_inverse_adjoint(s2b_plan* p, const void* K, const void* g_f, void* g_flm,
+                                   void* ws, size_t ws_bytes, void* stream) {
+  int rc;
+  if ((rc = check_pre_adjoint(p))) return rc;
+  if ((rc = check_ptr(K, "kernel")) || (rc = check_ptr(g_f, "g_f")) ||
+      (rc = check_ptr(g_flm, "g_flm")) || (rc = check_ptr(ws, "workspace")))
+    return rc;
+  if (ws_bytes < inv_ws(p)) return fail(S2B_ERR_WORKSPACE, "workspace too small");
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  return p->fp64 ? run_pre_inverse_adjoint<double>(p, K, g_f, g_flm, (char*)ws, s)
+                 : run_pre_inverse_adjoint<float>(p, K, g_f, g_flm, (char*)ws, s);
+}
+
+int s2b_precompute_forward_adjoint(s2b_plan* p, const void* K, const void* g_flm, void* g_f,
+                                   void* ws, size_t ws_bytes, void* stream) {
+  int rc;
+  if ((rc = check_pre_adjoint(p))) return rc;
+  if ((rc = check_ptr(K, "kernel")) || (rc = check_ptr(g_flm, "g_flm")) ||
+      (rc = check_ptr(g_f, "g_f")) || (rc = check_ptr(ws, "workspace")))
+    return rc;
+  if (ws_bytes < pre_fwd_ws(p)) return fail(S2B_ERR_WORKSPACE, "workspace too small");
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  return p->fp64 ? run_pre_forward_adjoint<double>(p, K, g_flm, g_f, (char*)ws, s)
+                 : run_pre_forward_adjoint<float>(p, K, g_flm, g_f, (char*)ws, s);
 }
 
 int s2b_wigner_inverse(s2b_plan* p, const void* flmn, void* f, void* ws, size_t ws_bytes,

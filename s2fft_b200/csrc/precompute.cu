@@ -235,6 +235,7 @@ __global__ void pre_contract_kernel(PreContractParams p) {
     C k;
     if (CPLX) {
       k = reinterpret_cast<const C*>(p.K)[o];
+      if (p.conj) k.y = -k.y;
     } else {
       k.x = reinterpret_cast<const Real*>(p.K)[o];
       k.y = Real(0);
@@ -375,6 +376,9 @@ __global__ void __launch_bounds__(256, sizeof(Real) == 8 ? 2 : 1) pre_gemm_kerne
     if (q < nsum && row < nrow && mi < M) {
       const size_t o = FWD ? ((size_t)q * L + row) * M + mi : ((size_t)row * L + q) * M + mi;
       v = reinterpret_cast<const KT*>(p.K)[o];
+      if constexpr (CPLX) {
+        if (p.conj) v.y = -v.y;
+      }
     }
     return v;
   };

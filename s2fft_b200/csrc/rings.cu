@@ -419,9 +419,11 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) mw_cols_adj_ke
   const R2* y = reinterpret_cast<const R2*>(p.in) + (size_t)b * nout * (2 * L - 1) + (L - 1 + m);
   auto load2 = [&](int t) -> R2 {
     if (t >= nout) return czero<R2>();
-    const int row = t == 0 ? 2 * L - 1 : (t == 2 * L ? 2 * L : t - 1);
+    // raw: rings in natural order and no weights (adjoint of the raw chain of the precompute
+    // path, whose kernel tables carry the weights)
+    const int row = p.raw ? t : (t == 0 ? 2 * L - 1 : (t == 2 * L ? 2 * L : t - 1));
     const R2 v = y[(size_t)row * (2 * L - 1)];
-    const double f = p.scale * p.weights[t];
+    const double f = p.raw ? p.scale : p.scale * p.weights[t];
     R2 o;
     o.x = (Real)((double)v.x * f);
     o.y = (Real)((double)v.y * f);

@@ -21,6 +21,7 @@ struct PreContractParams {
   int mo;                // inverse: ftm column of mi = 0
   int ncol;              // inverse: ftm row width
   double sign;           // (-1)^s
+  int conj;              // complex kernels: use conj(K) (adjoint transforms)
   const void* K;
   const void* in;
   void* out;

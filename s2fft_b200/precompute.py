@@ -88,10 +88,62 @@ def _aligned(t):
     return t if t.data_ptr() % 16 == 0 else t.clone()
 
 
+def _pre_call(name, plan, K, x, out, forward):
+    ws = plan.workspace(forward)
+    _lib.check(getattr(_lib.lib(), name)(plan.ptr, K.data_ptr(), x.data_ptr(), out.data_ptr(),
+                                         ws.data_ptr(), ws.numel(),
+                                         _lib.stream_handle(x.device)))
+    return out
+
+
+class _PreInverseFn(torch.autograd.Function):
+    """f = precompute inverse(flm); backward: s2b_precompute_inverse_adjoint."""
+
+    @staticmethod
+    def forward(ctx, x, plan, K, out_shape, cdt):
+        ctx.plan, ctx.K, ctx.in_shape = plan, K, x.shape
+        out = torch.empty(out_shape, dtype=cdt, device=x.device)
+        return _pre_call("s2b_precompute_inverse", plan, K, x, out, False)
+
+    @staticmethod
+    def backward(ctx, g):
+        g = g.contiguous()
+        gx = torch.empty(ctx.in_shape, dtype=g.dtype, device=g.device)
+        _pre_call("s2b_precompute_inverse_adjoint", ctx.plan, ctx.K, g, gx, False)
+        return gx, None, None, None, None
+
+
+class _PreForwardFn(torch.autograd.Function):
+    """flm = precompute forward(f) (one pass); backward: s2b_precompute_forward_adjoint."""
+
+    @staticmethod
+    def forward(ctx, x, plan, K, out_shape, cdt):
+        ctx.plan, ctx.K, ctx.in_shape = plan, K, x.shape
+        out = torch.empty(out_shape, dtype=cdt, device=x.device)
+        return _pre_call("s2b_precompute_forward", plan, K, x, out, True)
+
+    @staticmethod
+    def backward(ctx, g):
+        g = g.contiguous()
+        gx = torch.empty(ctx.in_shape, dtype=g.dtype, device=g.device)
+        _pre_call("s2b_precompute_forward_adjoint", ctx.plan, ctx.K, g, gx, True)
+        return gx, None, None, None, None
+
+
+def _needs_grad(x, reality, precision):
+    if not (isinstance(x, torch.Tensor) and x.requires_grad and torch.is_grad_enabled()):
+        return False
+    if reality or precision == "bf16x3":
+        raise NotImplementedError("precompute gradients need complex transforms "
+                                  "(reality=False) with f64 or f32 kernels")
+    return True
+
+
 def inverse(flm, L: int, spin: int = 0, kernel=None, sampling: str = "mw",
             reality: bool = False, method: str = "cuda", nside: int = None,
             precision: str = "f64"):
-    """Inverse spin SHT through a precomputed kernel (upstream spherical.py:19-84)."""
+    """Inverse spin SHT through a precomputed kernel (upstream spherical.py:19-84).
+    Differentiable in flm (complex transforms, f64 / f32 kernels)."""
     _check_method(method)
     s = sampling.lower()
     reality = _reality(reality, spin)
@@ -101,12 +153,11 @@ def inverse(flm, L: int, spin: int = 0, kernel=None, sampling: str = "mw",
     B = int(np.prod(bs)) if bs else 1
     K = _kernel_tensor(kernel, L, s, nside, reality, False, precision, spin, x.device)
     plan = _plan(x.device, L, spin, nside, s, reality, precision, B)
+    if _needs_grad(x, reality, precision):
+        return _ret(_PreInverseFn.apply(x, plan, K, bs + f_shape(L, s, nside), cdt), was_np,
+                    odev)
     out = torch.empty(bs + f_shape(L, s, nside), dtype=rdt if reality else cdt, device=x.device)
-    ws = plan.workspace(False)
-    _lib.check(_lib.lib().s2b_precompute_inverse(plan.ptr, K.data_ptr(), x.data_ptr(),
-                                                 out.data_ptr(), ws.data_ptr(), ws.numel(),
-                                                 _lib.stream_handle(x.device)))
-    return _ret(out, was_np, odev)
+    return _ret(_pre_call("s2b_precompute_inverse", plan, K, x, out, False), was_np, odev)
 
 
 def _forward_once(x, K, L, spin, s, nside, reality, precision):
@@ -115,12 +166,10 @@ def _forward_once(x, K, L, spin, s, nside, reality, precision):
     bs = tuple(x.shape[:-nd])
     B = int(np.prod(bs)) if bs else 1
     plan = _plan(x.device, L, spin, nside, s, reality, precision, B)
+    if _needs_grad(x, reality, precision):
+        return _PreForwardFn.apply(x, plan, K, bs + (L, 2 * L - 1), cdt)
     out = torch.empty(bs + (L, 2 * L - 1), dtype=cdt, device=x.device)
-    ws = plan.workspace(True)
-    _lib.check(_lib.lib().s2b_precompute_forward(plan.ptr, K.data_ptr(), x.data_ptr(),
-                                                 out.data_ptr(), ws.data_ptr(), ws.numel(),
-                                                 _lib.stream_handle(x.device)))
-    return out
+    return _pre_call("s2b_precompute_forward", plan, K, x, out, True)
 
 
 def forward(f, L: int, spin: int = 0, kernel=None, sampling: str = "mw",

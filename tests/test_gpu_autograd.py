@@ -199,3 +199,56 @@ def test_refinement_gradient_is_adjoint(s2b, rng):
     (gf,) = torch.autograd.grad(flm, fin, grad_outputs=h)
     lhs, rhs = _vdot(flm.detach(), h), _vdot(fin.detach(), gf)
     assert abs(lhs - rhs) <= 1e-10 * abs(lhs), (lhs, rhs)
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+@pytest.mark.parametrize("sampling", ["mw", "mwss", "dh", "gl", "healpix"])
+@pytest.mark.parametrize("spin", [0, -2])
+def test_precompute_adjoint_dot_products(s2b, rng, sampling, spin, precision):
+    """Precompute transforms (kernel tables) through s2b_precompute_inverse_adjoint /
+    s2b_precompute_forward_adjoint: <A x, y> = <x, A^H y> for a batch of 3 maps (small
+    batches use the register-tiled contraction) and of 20 maps (the shared-memory one)."""
+    import torch
+
+    L, nside = (16, 8) if sampling == "healpix" else (20, None)
+    cdt = torch.complex128 if precision == "f64" else torch.complex64
+    shape = s2b.f_shape(L, sampling, nside)
+    kin = s2b.precompute.spin_spherical_kernel(L, spin, False, sampling, nside, False,
+                                               precision=precision)
+    kfw = s2b.precompute.spin_spherical_kernel(L, spin, False, sampling, nside, True,
+                                               precision=precision)
+    for B in (3, 20):
+        x = torch.tensor(np.stack([oracle.signal.generate_flm(rng, L, 0, spin) for _ in range(B)]),
+                         dtype=cdt, device="cuda", requires_grad=True)
+        y = torch.tensor(rng.normal(size=(B,) + shape) + 1j * rng.normal(size=(B,) + shape),
+                         dtype=cdt, device="cuda")
+        f = s2b.precompute.inverse(x, L, spin, kin, sampling, nside=nside, precision=precision)
+        (gx,) = torch.autograd.grad(f, x, grad_outputs=y)
+        lhs, rhs = _vdot(f.detach(), y), _vdot(x.detach(), gx)
+        assert abs(lhs - rhs) <= TOL[precision] * max(abs(lhs), 1e-30) * 10, (B, lhs, rhs)
+
+        fin = torch.tensor(rng.normal(size=(B,) + shape) + 1j * rng.normal(size=(B,) + shape),
+                           dtype=cdt, device="cuda", requires_grad=True)
+        h = torch.tensor(np.stack([oracle.signal.generate_flm(rng, L, 0, spin) for _ in range(B)]),
+                         dtype=cdt, device="cuda")
+        flm = s2b.precompute.forward(fin, L, spin, kfw, sampling, nside=nside,
+                                     precision=precision)
+        (gf,) = torch.autograd.grad(flm, fin, grad_outputs=h)
+        lhs, rhs = _vdot(flm.detach(), h), _vdot(fin.detach(), gf)
+        assert abs(lhs - rhs) <= TOL[precision] * max(abs(lhs), 1e-30) * 10, (B, lhs, rhs)
+
+
+def test_precompute_gradient_matches_otf(s2b, rng):
+    """The precompute inverse's gradient equals the on-the-fly transform's (same map)."""
+    import torch
+
+    L = 24
+    x = torch.tensor(oracle.signal.generate_flm(rng, L, 0, 1), device="cuda",
+                     requires_grad=True)
+    g = torch.tensor(rng.normal(size=(L, 2 * L - 1)), device="cuda")
+    loss = (s2b.precompute.inverse(x, L, 1, None, "gl").real - g).pow(2).sum()
+    (g1,) = torch.autograd.grad(loss, x)
+    x2 = x.detach().clone().requires_grad_(True)
+    loss2 = (s2b.inverse(x2, L, 1, None, "gl").real - g).pow(2).sum()
+    (g2,) = torch.autograd.grad(loss2, x2)
+    assert relerr(g1.cpu().numpy(), g2.cpu().numpy()) < 1e-10
