@@ -280,6 +280,15 @@ int s2b_fw_inverse(s2b_fw_plan* plan, int batch, int reality, const double* delt
 int s2b_fw_forward(s2b_fw_plan* plan, int batch, int reality, const double* delta,
                    const void* quads, const void* f, void* flmn, void* workspace,
                    size_t workspace_bytes, void* stream);
+/* Adjoints (conjugate transposes) of s2b_fw_inverse / s2b_fw_forward for reverse-mode
+ * differentiation (complex signals): g_flmn = A^H g_f, g_f = A^H g_flmn, with the plan's N,
+ * the same delta / quads and the workspace of the transform they adjoin (reality = 0).
+ * Replace JAX's autodiff of upstream's fourier_wigner.py:13-333. */
+int s2b_fw_inverse_adjoint(s2b_fw_plan* plan, int batch, const double* delta, const void* g_f,
+                           void* g_flmn, void* workspace, size_t workspace_bytes, void* stream);
+int s2b_fw_forward_adjoint(s2b_fw_plan* plan, int batch, const double* delta, const void* quads,
+                           const void* g_flmn, void* g_f, void* workspace,
+                           size_t workspace_bytes, void* stream);
 /* spins: device int32 [nspins]. */
 int s2b_fw_subset_to_s2(s2b_fw_plan* plan, int batch, int nspins, const int* spins,
                         const double* delta, const void* flmn, void* f, void* workspace,

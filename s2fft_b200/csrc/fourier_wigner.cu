@@ -90,6 +90,11 @@ struct FWContractParams {
   const double* delta;  // [L][2L-1][2L-1]
   const void* in;       // INV: coefficients (slice layout fw_coef_slice); FWD: Gf [E][L][2L-1]
   void* out;            // INV: Y [E][2L-1][2L-1]; FWD: coefficients
+  // adjoints: INV with adj writes the rows a >= 0 only, [E][L][2L-1], times (2pi)^2 and
+  // i^(n-m) (the adjoint of the forward's last step); FWD with adj scales row l by c_l
+  // without phase (the adjoint of the inverse's first step; the phases come from
+  // fw_cols_inv_adj_kernel)
+  int adj;
 };
 
 // With D[l][x][y] = Delta^l_{x,y} (zero where |x| > l or |y| > l) and the reflection
@@ -164,8 +169,8 @@ __global__ void __launch_bounds__(kFwLanes) fw_contract_kernel(FWContractParams<
       if (q <= qhi && r <= L - 1 && n < L && e0 + s < p.E) {
         if (FWD)  // D[l = r][b = q][n]
           w = __ldg(p.delta + ((long)r * W + (q + L - 1)) * W + (n + L - 1));
-        else      // c_l D[l = q][a = r][n]
-          w = (2.0 * q + 1.0) / (8.0 * pi * pi) *
+        else      // c_l D[l = q][a = r][n]  (adjoint: (2pi)^2 D[l = q][a = r][n])
+          w = (p.adj ? 4.0 * pi * pi : (2.0 * q + 1.0) / (8.0 * pi * pi)) *
               __ldg(p.delta + ((long)q * W + (r + L - 1)) * W + (n + L - 1));
       }
       wn[qq][j][s] = (Real)w;
@@ -220,11 +225,18 @@ __global__ void __launch_bounds__(kFwLanes) fw_contract_kernel(FWContractParams<
       const int r = r0 + j;
       if (r > L - 1) continue;
       if (FWD) {
-        const Real sc = (Real)(4.0 * pi * pi);
-        R2 v = mul_ipow(acc[j][s], m - n);
-        v.x *= sc;
-        v.y *= sc;
+        R2 v;
+        if (p.adj) {
+          v = cscale(acc[j][s], (Real)((2.0 * r + 1.0) / (8.0 * pi * pi)));
+        } else {
+          const Real sc = (Real)(4.0 * pi * pi);
+          v = mul_ipow(acc[j][s], m - n);
+          v.x *= sc;
+          v.y *= sc;
+        }
         O[fw_coef_slice(p.sl, e) * (long)L * W + (long)r * W + ci] = v;
+      } else if (p.adj) {
+        O[(long)e * L * W + (long)r * W + ci] = mul_ipow(acc[j][s], n - m);
       } else {
         const R2 v = mul_ipow(acc[j][s], n - m);
         R2* Y = O + (long)e * W * W;
@@ -303,7 +315,9 @@ __global__ void __launch_bounds__(512) fw_rows_inv_kernel(FWFftParams<Real> p) {
     return m >= -(L - 1) ? T[m + L - 1] : czero<R2>();
   });
   R2* o = reinterpret_cast<R2*>(p.out) + (fw_map_index(p, e) * p.ntheta + t) * np;
-  for (int j = threadIdx.x; j < np; j += blockDim.x) o[j] = dft_get<Real>(s, p.dphi, p.tb, true, j);
+  const Real sc = (Real)p.scale;
+  for (int j = threadIdx.x; j < np; j += blockDim.x)
+    o[j] = cscale(dft_get<Real>(s, p.dphi, p.tb, true, j), sc);
 }
 
 // Forward, alpha: ring t of map e -> S[e][t][m] = scale sum_p map[t][p] e^{-i m alpha_p},
@@ -399,17 +413,126 @@ __global__ void __launch_bounds__(512) fw_cols_fwd_kernel(FWFftParams<Real> p, i
   }
 }
 
+// Adjoint of fw_cols_inv_kernel and of the phases / mirror of the inverse contraction:
+// column m of T[e] (ntheta rows) -> Y[a] = sum_t T[t] e^{-i a beta_t}, |a| <= L-1, then
+// Pf[a] = conj(ph(a)) Y[a] + (-1)^(m+n) conj(ph(-a)) Y[-a] (a > 0), Pf[0] = conj(ph(0)) Y[0],
+// ph(a) = i^(n-m) e^{i a theta0}; stored [E][L][2L-1] for the adjoint contraction.
+template <typename Real>
+__global__ void __launch_bounds__(512) fw_cols_inv_adj_kernel(FWFftParams<Real> p) {
+  using R2 = typename C2<Real>::t;
+  extern __shared__ unsigned char fw_smem[];
+  R2* s = reinterpret_cast<R2*>(fw_smem);
+  const int L = p.L, W = 2 * L - 1, col = blockIdx.x, e = blockIdx.y;
+  const int m = col - (L - 1);
+  const int n = fw_n(p.sl, e % p.sl.S);
+  const Real sgn = ((abs(m) + abs(n)) & 1) ? Real(-1) : Real(1);
+  const R2* T = reinterpret_cast<const R2*>(p.in) + (long)e * p.ntheta * W;
+  const int na = p.nphi;
+  dft_run<Real>(s, p.dphi, p.tb, false, [&](int k) {
+    return k < p.ntheta ? T[(long)k * W + col] : czero<R2>();
+  });
+  R2* Pf = reinterpret_cast<R2*>(p.out) + (long)e * L * W;
+  for (int a = threadIdx.x; a <= L - 1; a += blockDim.x) {
+    R2 yp = dft_get<Real>(s, p.dphi, p.tb, false, a);
+    R2 ym = a > 0 ? dft_get<Real>(s, p.dphi, p.tb, false, na - a) : czero<R2>();
+    if (!p.mwss) {  // e^{-i a theta0} on Y[a], e^{+i a theta0} on Y[-a]
+      double sn, cs;
+      sincospi((double)a / (double)W, &sn, &cs);
+      const Real c = (Real)cs, sv = (Real)sn;
+      const R2 u = yp, v = ym;
+      yp.x = u.x * c + u.y * sv;
+      yp.y = u.y * c - u.x * sv;
+      ym.x = v.x * c - v.y * sv;
+      ym.y = v.x * sv + v.y * c;
+    }
+    Pf[(long)a * W + col] = mul_ipow(cadd(yp, cscale(ym, sgn)), m - n);
+  }
+}
+
+// Adjoint of fw_cols_fwd_kernel: column m of Gf[e] ([E][L][2L-1]) -> S[e][t][m], t < ntheta.
+// Unfold (G[b] = Gf[b], G[-b] = (-1)^(m+n) Gf[b]), the convolution's adjoint (the same
+// length-Q chain with conj(quadsQ), plus the mwss wrap-around term's adjoint), the MW phase's
+// conjugate, (1/nx) times the inverse DFT of length nx, and the extension folded back.
+template <typename Real>
+__global__ void __launch_bounds__(512) fw_cols_fwd_adj_kernel(FWFftParams<Real> p, int bufM) {
+  using R2 = typename C2<Real>::t;
+  extern __shared__ unsigned char fw_smem[];
+  R2* s = reinterpret_cast<R2*>(fw_smem);
+  R2* tmp = s + padded_len(bufM);
+  const int L = p.L, W = 2 * L - 1, col = blockIdx.x, e = blockIdx.y;
+  const int m = col - (L - 1);
+  const int n = fw_n(p.sl, e % p.sl.S);
+  const Real sgn = ((abs(m) + abs(n)) & 1) ? Real(-1) : Real(1);
+  const int nth = p.ntheta, nx = p.nphi, P = p.P;
+  const R2* Gf = reinterpret_cast<const R2*>(p.in) + (long)e * L * W;
+  // G[b'] at b' mod P, |b'| <= L-1, zero elsewhere; inverse DFT of length P, times 1/P
+  const int half = (P - 1) / 2;
+  dft_run<Real>(s, p.dP, p.tb, true, [&](int k) {
+    const int v = k <= half ? k : k - P;
+    if (v >= 0 && v <= L - 1) return Gf[(long)v * W + col];
+    if (v < 0 && v >= -(L - 1)) return cscale(Gf[(long)(-v) * W + col], sgn);
+    return czero<R2>();
+  });
+  const double2* qd = reinterpret_cast<const double2*>(p.quads);
+  const Real iP = (Real)(1.0 / P);
+  for (int j = threadIdx.x; j < P; j += blockDim.x) {
+    const double2 q = qd[j];
+    R2 w;
+    w.x = (Real)q.x;
+    w.y = (Real)(-q.y);  // conj(quadsQ)
+    tmp[j] = cscale(cmul(dft_get<Real>(s, p.dP, p.tb, true, j), w), iP);
+  }
+  __syncthreads();
+  dft_run<Real>(s, p.dP, p.tb, false, [&](int k) { return tmp[k]; });
+  // B_adj[v], v in [blo, L-1] -> tmp[v - blo] (with the MW phase's conjugate)
+  const int blo = p.mwss ? -L : -(L - 1);
+  for (int v = blo + (int)threadIdx.x; v <= L - 1; v += blockDim.x) {
+    R2 x = dft_get<Real>(s, p.dP, p.tb, false, pmod(v, P));
+    if (p.mwss && v == -L) {  // adjoint of the wrap-around term B[-L] w[-(2L-2)] -> G[L-1]
+      const double2 w0 = reinterpret_cast<const double2*>(p.wconv)[0];
+      R2 cw;
+      cw.x = (Real)w0.x;
+      cw.y = (Real)(-w0.y);
+      x = cadd(x, cmul(Gf[(long)(L - 1) * W + col], cw));
+    }
+    if (!p.mwss) {  // conj(e^{-i v pi / (2L-1)})
+      double sn, cs;
+      sincospi((double)v / (double)W, &sn, &cs);
+      const R2 u = x;
+      x.x = u.x * (Real)cs - u.y * (Real)sn;
+      x.y = u.x * (Real)sn + u.y * (Real)cs;
+    }
+    tmp[v - blo] = x;
+  }
+  __syncthreads();
+  // (1/nx) inverse DFT of length nx over the bins v mod nx
+  dft_run<Real>(s, p.dphi, p.tb, true, [&](int k) {
+    const int v = k <= (nx - 1) / 2 ? k : k - nx;  // nx odd (mw): |v| <= L-1; even: -L..L-1
+    return (v >= blo && v <= L - 1) ? tmp[v - blo] : czero<R2>();
+  });
+  const Real inx = (Real)(1.0 / nx);
+  R2* S = reinterpret_cast<R2*>(p.out) + (long)e * nth * W;
+  for (int t = threadIdx.x; t < nth; t += blockDim.x) {
+    R2 x = dft_get<Real>(s, p.dphi, p.tb, true, t);
+    const int t2 = 2 * (nth - 1) - t;  // the extension row that copied ring t
+    if (t2 >= nth && t2 < nx) x = cadd(x, cscale(dft_get<Real>(s, p.dphi, p.tb, true, t2), sgn));
+    S[(long)t * W + col] = cscale(x, inx);
+  }
+}
+
 // Gamma DFT of the full transform: one thread per (map, pixel) and block of kGamK outputs
-// (blockIdx.y).
+// (blockIdx.y). The sums below are multiplied by `scale` (1 for the inverse, 1/G for the
+// forward in the transforms; the adjoints use G and 1/G).
 //   inverse: f[b][g][px] = sum_n x[N-1+n][b][px] e^{+2 pi i n g / G}, n in [-(N-1), N-1];
 //            reality: real output from n >= 0 (irfft: n = 0 real part, n > 0 doubled)
-//   forward: x[N-1+n][b][px] = (1/G) sum_g f[b][g][px] e^{-2 pi i n g / G}, n in [n0, N-1]
+//   forward: x[N-1+n][b][px] = sum_g f[b][g][px] e^{-2 pi i n g / G}, n in [n0, N-1]
 // (fourier_wigner.py:80-87 and 241-248). A table of the G roots e^{2 pi i j / G} sits in
 // shared memory; the exponent n g is reduced mod G exactly.
 constexpr int kGamK = 8;
 
 template <typename Real, bool FWD>
-__global__ void fw_gamma_kernel(const void* in, void* out, int B, int N, long npix, int reality) {
+__global__ void fw_gamma_kernel(const void* in, void* out, int B, int N, long npix, int reality,
+                                double scale) {
   using R2 = typename C2<Real>::t;
   extern __shared__ double2 roots[];
   const int G = 2 * N - 1;
@@ -455,11 +578,11 @@ __global__ void fw_gamma_kernel(const void* in, void* out, int B, int N, long np
           if (g >= G) break;
           const long o = (b * G + g) * npix + px;
           if (reality) {
-            reinterpret_cast<Real*>(out)[o] = (Real)re[u];
+            reinterpret_cast<Real*>(out)[o] = (Real)(re[u] * scale);
           } else {
             R2 w;
-            w.x = (Real)re[u];
-            w.y = (Real)im[u];
+            w.x = (Real)(re[u] * scale);
+            w.y = (Real)(im[u] * scale);
             reinterpret_cast<R2*>(out)[o] = w;
           }
         }
@@ -494,7 +617,7 @@ __global__ void fw_gamma_kernel(const void* in, void* out, int B, int N, long np
             if (r >= G) r -= G;
           }
         }
-        const double sc = 1.0 / G;
+        const double sc = scale;
 #pragma unroll
         for (int u = 0; u < kGamK; ++u) {
           const int n = n0 + u;
@@ -517,7 +640,8 @@ constexpr int kGamFFTMin = 24;
 template <typename Real, bool FWD>
 __global__ void __launch_bounds__(512) fw_gamma_fft_kernel(const void* in, void* out, int B,
                                                            int N, long npix, int reality,
-                                                           FFTDesc dg, FFTTables<Real> tb) {
+                                                           double scale, FFTDesc dg,
+                                                           FFTTables<Real> tb) {
   using R2 = typename C2<Real>::t;
   extern __shared__ unsigned char fw_smem[];
   R2* s = reinterpret_cast<R2*>(fw_smem);
@@ -536,7 +660,7 @@ __global__ void __launch_bounds__(512) fw_gamma_fft_kernel(const void* in, void*
       return v;
     });
     for (int g = threadIdx.x; g < G; g += blockDim.x) {
-      const R2 v = dft_get<Real>(s, dg, tb, true, g);
+      const R2 v = cscale(dft_get<Real>(s, dg, tb, true, g), (Real)scale);
       const long o = (b * G + g) * npix + px;
       if (reality)
         reinterpret_cast<Real*>(out)[o] = v.x;
@@ -555,7 +679,7 @@ __global__ void __launch_bounds__(512) fw_gamma_fft_kernel(const void* in, void*
       return reinterpret_cast<const R2*>(in)[o];
     });
     R2* x = reinterpret_cast<R2*>(out);
-    const Real sc = (Real)(1.0 / G);
+    const Real sc = (Real)scale;
     for (int n = (reality ? 0 : -(N - 1)) + (int)threadIdx.x; n < N; n += blockDim.x)
       x[((long)(N - 1 + n) * B + b) * npix + px] =
           cscale(dft_get<Real>(s, dg, tb, false, n < 0 ? n + G : n), sc);
@@ -776,8 +900,9 @@ cudaError_t launch_fft(K kernel, dim3 grid, int M, size_t smem, cudaStream_t st,
 
 template <typename Real>
 int contract(const s2b_fw_plan* p, bool fwd, int E, const FWSlices& sl, const double* delta,
-             const void* in, void* out, cudaStream_t st) {
+             const void* in, void* out, cudaStream_t st, int adj = 0) {
   FWContractParams<Real> c{};
+  c.adj = adj;
   c.L = p->L;
   c.E = E;
   c.mwss = p->mwss;
@@ -859,10 +984,77 @@ int forward_chain(const s2b_fw_plan* p, int E, const FWSlices& sl, const double*
   return contract<Real>(p, true, E, sl, delta, A, coef, st);
 }
 
+// Adjoint of inverse_chain (maps -> coefficients): alpha DFTs (rows_fwd, scale 1), the
+// beta adjoint with the phases and mirror (cols_inv_adj), the adjoint contraction.
+template <typename Real>
+int inverse_adjoint_chain(const s2b_fw_plan* p, int E, const FWSlices& sl, const double* delta,
+                          const void* maps, void* coef, int nmajor, int groups, char* ws,
+                          const FWLayout& lay, cudaStream_t st) {
+  using R2 = typename C2<Real>::t;
+  void* A = ws;
+  void* B = ws + lay.a;
+  FWFftParams<Real> f = fft_params<Real>(p, E, sl);
+  const int M = f.dphi.M;
+  const size_t smem = (size_t)padded_len(M) * sizeof(R2);
+  f.in = maps;
+  f.out = B;
+  f.nmajor = nmajor;
+  f.groups = groups;
+  f.scale = 1.0;
+  FW_CK(launch_fft<Real>(fw_rows_fwd_kernel<Real>, dim3(p->ntheta, E), M, smem, st, f));
+  f.in = B;
+  f.out = A;
+  f.nmajor = 0;
+  FW_CK(launch_fft<Real>(fw_cols_inv_adj_kernel<Real>, dim3(2 * p->L - 1, E), M, smem, st, f));
+  return contract<Real>(p, true, E, sl, delta, A, coef, st, 1);
+}
+
+// Adjoint of forward_chain (coefficients -> maps): the adjoint contraction, the beta-chain
+// adjoint (cols_fwd_adj) and inverse alpha DFTs times 1/nphi.
+template <typename Real>
+int forward_adjoint_chain(const s2b_fw_plan* p, int E, const FWSlices& sl, const double* delta,
+                          const void* quads, const void* coef, void* maps, int nmajor,
+                          int groups, char* ws, const FWLayout& lay, cudaStream_t st) {
+  using R2 = typename C2<Real>::t;
+  void* A = ws;
+  void* B = ws + lay.a;
+  double2* wk = reinterpret_cast<double2*>(ws + lay.a + lay.b + lay.c);
+  double2* qQ = wk + p->P;
+  fw_weights_from_quads_kernel<<<(p->P + 3) / 4, 128, 0, st>>>(
+      p->L, reinterpret_cast<const double2*>(quads), wk);
+  FW_CK(cudaGetLastError());
+  fw_quads_pow2_kernel<<<(p->Q + 3) / 4, 128, 0, st>>>(p->L, p->Q, wk, qQ);
+  FW_CK(cudaGetLastError());
+  int rc = contract<Real>(p, false, E, sl, delta, coef, A, st, 1);
+  if (rc) return rc;
+  FWFftParams<Real> f = fft_params<Real>(p, E, sl);
+  f.quads = qQ;
+  f.wconv = wk;
+  f.in = A;
+  f.out = B;
+  const int bufM = std::max(f.dphi.M, f.dP.M);
+  const size_t smem = (size_t)(padded_len(bufM) + p->Q) * sizeof(R2);
+  FW_CK(cudaFuncSetAttribute(fw_cols_fwd_adj_kernel<Real>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  fw_cols_fwd_adj_kernel<Real><<<dim3(2 * p->L - 1, E), fft_threads_for(bufM), smem, st>>>(f,
+                                                                                        bufM);
+  FW_CK(cudaGetLastError());
+  f.in = B;
+  f.out = maps;
+  f.nmajor = nmajor;
+  f.groups = groups;
+  f.scale = 1.0 / p->nphi;
+  const int M = f.dphi.M;
+  FW_CK(launch_fft<Real>(fw_rows_inv_kernel<Real>, dim3(p->ntheta, E), M,
+                         (size_t)padded_len(M) * sizeof(R2), st, f));
+  return S2B_OK;
+}
+
 template <typename Real>
 int gamma_dft(const s2b_fw_plan* p, bool fwd, const void* in, void* out, int B, int N,
-              long npix, int reality, cudaStream_t st) {
+              long npix, int reality, cudaStream_t st, double scale = -1.0) {
   const int G = 2 * N - 1;
+  if (scale < 0) scale = fwd ? 1.0 / G : 1.0;  // the transforms' own normalisation
   if (p->gamma_fft && N == p->N) {
     using R2 = typename C2<Real>::t;
     const FFTDesc& dg = p->fft.host[2];
@@ -874,12 +1066,12 @@ int gamma_dft(const s2b_fw_plan* p, bool fwd, const void* in, void* out, int B, 
       FW_CK(cudaFuncSetAttribute(fw_gamma_fft_kernel<Real, true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       fw_gamma_fft_kernel<Real, true><<<grid, fft_threads_for(dg.M), smem, st>>>(
-          in, out, B, N, npix, reality, dg, tables<Real>(p));
+          in, out, B, N, npix, reality, scale, dg, tables<Real>(p));
     } else {
       FW_CK(cudaFuncSetAttribute(fw_gamma_fft_kernel<Real, false>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       fw_gamma_fft_kernel<Real, false><<<grid, fft_threads_for(dg.M), smem, st>>>(
-          in, out, B, N, npix, reality, dg, tables<Real>(p));
+          in, out, B, N, npix, reality, scale, dg, tables<Real>(p));
     }
     FW_CK(cudaGetLastError());
     return S2B_OK;
@@ -892,10 +1084,10 @@ int gamma_dft(const s2b_fw_plan* p, bool fwd, const void* in, void* out, int B, 
   if (chunks > 65535) return fw_fail(S2B_ERR_INVALID, "N too large for the gamma DFT");
   if (fwd)
     fw_gamma_kernel<Real, true><<<dim3(blocks, chunks), 256, smem, st>>>(in, out, B, N, npix,
-                                                                        reality);
+                                                                        reality, scale);
   else
     fw_gamma_kernel<Real, false><<<dim3(blocks, chunks), 256, smem, st>>>(in, out, B, N, npix,
-                                                                         reality);
+                                                                         reality, scale);
   FW_CK(cudaGetLastError());
   return S2B_OK;
 }
@@ -1086,6 +1278,57 @@ int s2b_fw_forward(s2b_fw_plan* plan, int batch, int reality, const double* delt
   if (rc) return rc;
   if (reality) FW_CK(launch_wigner_mirror(plan->fp64, flmn, batch, N, plan->L, st));
   return S2B_OK;
+}
+
+int s2b_fw_inverse_adjoint(s2b_fw_plan* plan, int batch, const double* delta, const void* g_f,
+                           void* g_flmn, void* ws, size_t ws_bytes, void* stream) {
+  int rc;
+  if ((rc = check_plan(plan))) return rc;
+  if (batch < 1) return fw_fail(S2B_ERR_INVALID, "need batch >= 1");
+  const int N = plan->N;
+  if ((rc = check_ptrs({delta, g_f, g_flmn}))) return rc;
+  const FWSlices sl = full_slices(N, 0);
+  const int E = batch * sl.S;
+  if ((rc = check_slices((long)batch * sl.S))) return rc;
+  const FWLayout lay = fw_layout(plan, E, (long)batch * (2L * N - 1), 0);
+  if ((rc = check_ws(lay, ws, ws_bytes))) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  char* w = (char*)ws;
+  const long npix = (long)plan->ntheta * plan->nphi;
+  // adjoint of the inverse gamma DFT: the forward DFT without its 1/G, into region A
+  rc = plan->fp64 ? gamma_dft<double>(plan, true, g_f, w, batch, N, npix, 0, st, 1.0)
+                  : gamma_dft<float>(plan, true, g_f, w, batch, N, npix, 0, st, 1.0);
+  if (rc) return rc;
+  return plan->fp64
+             ? inverse_adjoint_chain<double>(plan, E, sl, delta, w, g_flmn, 1, batch, w, lay, st)
+             : inverse_adjoint_chain<float>(plan, E, sl, delta, w, g_flmn, 1, batch, w, lay, st);
+}
+
+int s2b_fw_forward_adjoint(s2b_fw_plan* plan, int batch, const double* delta, const void* quads,
+                           const void* g_flmn, void* g_f, void* ws, size_t ws_bytes,
+                           void* stream) {
+  int rc;
+  if ((rc = check_plan(plan))) return rc;
+  if (batch < 1) return fw_fail(S2B_ERR_INVALID, "need batch >= 1");
+  const int N = plan->N;
+  if ((rc = check_ptrs({delta, quads, g_flmn, g_f}))) return rc;
+  const FWSlices sl = full_slices(N, 0);
+  const int E = batch * sl.S;
+  if ((rc = check_slices((long)batch * sl.S))) return rc;
+  const FWLayout lay = fw_layout(plan, E, (long)batch * (2L * N - 1), 0);
+  if ((rc = check_ws(lay, ws, ws_bytes))) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  char* w = (char*)ws;
+  const long npix = (long)plan->ntheta * plan->nphi;
+  rc = plan->fp64 ? forward_adjoint_chain<double>(plan, E, sl, delta, quads, g_flmn, w, 1, batch,
+                                                  w, lay, st)
+                  : forward_adjoint_chain<float>(plan, E, sl, delta, quads, g_flmn, w, 1, batch,
+                                                 w, lay, st);
+  if (rc) return rc;
+  // adjoint of the forward gamma DFT (with its 1/G): the inverse DFT times 1/G
+  const double G = 2.0 * N - 1.0;
+  return plan->fp64 ? gamma_dft<double>(plan, false, w, g_f, batch, N, npix, 0, st, 1.0 / G)
+                    : gamma_dft<float>(plan, false, w, g_f, batch, N, npix, 0, st, 1.0 / G);
 }
 
 int s2b_fw_subset_to_s2(s2b_fw_plan* plan, int batch, int nspins, const int* spins,

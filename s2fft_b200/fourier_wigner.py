@@ -7,8 +7,11 @@
 factored through the planes Delta^l = d^l(pi/2) and FFTs over (alpha, beta, gamma).
 ``precomps`` is ``(delta, quads)`` as returned by ``fourier_wigner_kernel(L)``
 (construct.py:614-639); without it the kernel is built on the device for the call (and
-cached per device and L while the planes take at most 2 GiB). Unlike upstream a leading batch dimension is accepted, and
-``precision="f32"`` runs the transform in float (the planes stay float64).
+cached per device and L while the planes take at most 2 GiB). Unlike upstream a leading
+batch dimension is accepted, and ``precision="f32"`` runs the transform in float (the planes
+stay float64). Complex transforms are differentiable in their input through the adjoint
+entry points ``s2b_fw_inverse_adjoint`` / ``s2b_fw_forward_adjoint`` (upstream differentiates
+its JAX version by autodiff).
 """
 
 from __future__ import annotations
@@ -45,6 +48,8 @@ def _fwlib():
                 "s2b_fw_subset_to_s2": [vp, ci, ci, vp, vp, vp, vp, vp, sz, vp],
                 "s2b_fw_s2_to_subset": [vp, ci, ci, vp, vp, vp, vp, vp, vp, sz, vp],
                 "s2b_fw_so3_to_subset": [vp, ci, ci, ci, vp, vp, vp, vp, vp, vp, sz, vp],
+                "s2b_fw_inverse_adjoint": [vp, ci, vp, vp, vp, vp, sz, vp],
+                "s2b_fw_forward_adjoint": [vp, ci, vp, vp, vp, vp, vp, sz, vp],
             }
             for name, argt in sigs.items():
                 fn = getattr(h, name)
@@ -163,6 +168,62 @@ def _cdt(precision):
     return torch.complex128 if precision == "f64" else torch.complex64
 
 
+class _FWInverseFn(torch.autograd.Function):
+    """f = inverse_transform(flmn) (complex); backward: s2b_fw_inverse_adjoint."""
+
+    @staticmethod
+    def forward(ctx, x, plan, B, delta, out_shape, cdt):
+        ctx.plan, ctx.B, ctx.delta, ctx.in_shape = plan, B, delta, x.shape
+        out = torch.empty(out_shape, dtype=cdt, device=x.device)
+        ws = plan.workspace(OP_INVERSE, B, False)
+        _lib.check(_fwlib().s2b_fw_inverse(plan.ptr, B, 0, delta.data_ptr(), x.data_ptr(),
+                                           out.data_ptr(), ws.data_ptr(), ws.numel(),
+                                           _lib.stream_handle(x.device)))
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        g = g.contiguous()
+        gx = torch.empty(ctx.in_shape, dtype=g.dtype, device=g.device)
+        ws = ctx.plan.workspace(OP_INVERSE, ctx.B, False)
+        _lib.check(_fwlib().s2b_fw_inverse_adjoint(ctx.plan.ptr, ctx.B, ctx.delta.data_ptr(),
+                                                   g.data_ptr(), gx.data_ptr(), ws.data_ptr(),
+                                                   ws.numel(), _lib.stream_handle(g.device)))
+        return gx, None, None, None, None, None
+
+
+class _FWForwardFn(torch.autograd.Function):
+    """flmn = forward_transform(f) (complex); backward: s2b_fw_forward_adjoint."""
+
+    @staticmethod
+    def forward(ctx, x, plan, B, delta, quads, out_shape, cdt):
+        ctx.plan, ctx.B, ctx.delta, ctx.quads, ctx.in_shape = plan, B, delta, quads, x.shape
+        out = torch.empty(out_shape, dtype=cdt, device=x.device)
+        ws = plan.workspace(OP_FORWARD, B, False)
+        _lib.check(_fwlib().s2b_fw_forward(plan.ptr, B, 0, delta.data_ptr(), quads.data_ptr(),
+                                           x.data_ptr(), out.data_ptr(), ws.data_ptr(),
+                                           ws.numel(), _lib.stream_handle(x.device)))
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        g = g.contiguous()
+        gx = torch.empty(ctx.in_shape, dtype=g.dtype, device=g.device)
+        ws = ctx.plan.workspace(OP_FORWARD, ctx.B, False)
+        _lib.check(_fwlib().s2b_fw_forward_adjoint(
+            ctx.plan.ptr, ctx.B, ctx.delta.data_ptr(), ctx.quads.data_ptr(), g.data_ptr(),
+            gx.data_ptr(), ws.data_ptr(), ws.numel(), _lib.stream_handle(g.device)))
+        return gx, None, None, None, None, None, None
+
+
+def _needs_grad(x, reality):
+    if not (isinstance(x, torch.Tensor) and x.requires_grad and torch.is_grad_enabled()):
+        return False
+    if reality:
+        raise NotImplementedError("gradients are available for complex transforms (reality=False)")
+    return True
+
+
 def inverse_transform(flmn, L: int, N: int, precomps=None, reality: bool = False,
                       sampling: str = "mw", precision: str = "f64"):
     """flmn [..., 2N-1, L, 2L-1] -> f [..., 2N-1, ntheta, nphi] (real when reality)."""
@@ -180,6 +241,8 @@ def inverse_transform(flmn, L: int, N: int, precomps=None, reality: bool = False
     out = torch.empty(bs + (2 * N - 1, nth, nph), dtype=rdt if reality else cdt,
                       device=x.device)
     plan = get_plan(x.device, L, s, precision, N)
+    if _needs_grad(x, reality):
+        return _ret(_FWInverseFn.apply(x, plan, B, delta, out.shape, cdt), was_np, odev)
     ws = plan.workspace(OP_INVERSE, B, reality)
     _lib.check(_fwlib().s2b_fw_inverse(plan.ptr, B, int(bool(reality)), delta.data_ptr(),
                                        x.data_ptr(), out.data_ptr(), ws.data_ptr(), ws.numel(),
@@ -209,6 +272,8 @@ def forward_transform(f, L: int, N: int, precomps=None, reality: bool = False,
     delta, quads = _precomps(precomps, L, x.device)
     out = torch.empty(bs + (2 * N - 1, L, 2 * L - 1), dtype=cdt, device=x.device)
     plan = get_plan(x.device, L, s, precision, N)
+    if _needs_grad(x, reality):
+        return _ret(_FWForwardFn.apply(x, plan, B, delta, quads, out.shape, cdt), was_np, odev)
     ws = plan.workspace(OP_FORWARD, B, reality)
     _lib.check(_fwlib().s2b_fw_forward(plan.ptr, B, int(bool(reality)), delta.data_ptr(),
                                        quads.data_ptr(), x.data_ptr(), out.data_ptr(),

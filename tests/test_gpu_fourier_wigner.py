@@ -217,3 +217,54 @@ def test_c_abi_errors(s2b):
                                    flmn.data_ptr(), f.data_ptr(), ws.data_ptr(), need, st) == 1
     assert lib.s2b_last_error()
     torch.cuda.synchronize()
+
+
+def _vdot(a, b):
+    return complex((a.conj() * b).sum().item())
+
+
+@pytest.mark.parametrize("sampling", ["mw", "mwss"])
+@pytest.mark.parametrize("L,N", [(12, 3), (10, 10), (16, 13)])
+@pytest.mark.parametrize("precision,tol", [("f64", 1e-10), ("f32", 1e-5)])
+def test_adjoint_dot_products(s2b, sampling, L, N, precision, tol):
+    """Gradients through s2b_fw_inverse_adjoint / s2b_fw_forward_adjoint: for y = A x,
+    <A x, y> = <x, A^H y>, with two signals per call (N = 13 takes the gamma FFT)."""
+    rng = np.random.default_rng(L + 100 * N)
+    fw = s2b.fourier_wigner
+    cdt = torch.complex128 if precision == "f64" else torch.complex64
+    nth, nph = (L + 1, 2 * L) if sampling == "mwss" else (L, 2 * L - 1)
+    G = 2 * N - 1
+    x = torch.tensor(np.stack([oracle.signal.generate_flmn(rng, L, N, 0, False)
+                               for _ in range(2)]), dtype=cdt, device="cuda",
+                     requires_grad=True)
+    y = torch.tensor(rng.normal(size=(2, G, nth, nph)) + 1j * rng.normal(size=(2, G, nth, nph)),
+                     dtype=cdt, device="cuda")
+    f = fw.inverse_transform(x, L, N, None, False, sampling, precision=precision)
+    (gx,) = torch.autograd.grad(f, x, grad_outputs=y)
+    lhs, rhs = _vdot(f.detach(), y), _vdot(x.detach(), gx)
+    assert abs(lhs - rhs) <= tol * max(abs(lhs), 1e-30) * 10, (lhs, rhs)
+
+    fin = torch.tensor(rng.normal(size=(2, G, nth, nph)) + 1j * rng.normal(size=(2, G, nth, nph)),
+                       dtype=cdt, device="cuda", requires_grad=True)
+    h = torch.tensor(rng.normal(size=(2, G, L, 2 * L - 1))
+                     + 1j * rng.normal(size=(2, G, L, 2 * L - 1)), dtype=cdt, device="cuda")
+    flmn = fw.forward_transform(fin, L, N, None, False, sampling, precision=precision)
+    (gf,) = torch.autograd.grad(flmn, fin, grad_outputs=h)
+    lhs, rhs = _vdot(flmn.detach(), h), _vdot(fin.detach(), gf)
+    assert abs(lhs - rhs) <= tol * max(abs(lhs), 1e-30) * 10, (lhs, rhs)
+
+
+def test_gradient_matches_recursion_wigner(s2b):
+    """MW L=32 N=4: the gradient of ||inverse(flmn) - g||^2 by the Fourier-Wigner adjoint equals
+    the recursion-based Wigner transform's (its own adjoint kernels)."""
+    L, N = 32, 4
+    rng = np.random.default_rng(9)
+    x = torch.tensor(oracle.signal.generate_flmn(rng, L, N, 0, False), device="cuda",
+                     requires_grad=True)
+    g = torch.tensor(rng.normal(size=(2 * N - 1, L, 2 * L - 1)), device="cuda")
+    loss = (s2b.fourier_wigner.inverse_transform(x, L, N).real - g).pow(2).sum()
+    (g1,) = torch.autograd.grad(loss, x)
+    x2 = x.detach().clone().requires_grad_(True)
+    loss2 = (s2b.wigner.inverse(x2, L, N, sampling="mw").real - g).pow(2).sum()
+    (g2,) = torch.autograd.grad(loss2, x2)
+    assert relerr(g1.cpu().numpy(), g2.cpu().numpy()) < 1e-9
