@@ -301,6 +301,22 @@ int s2b_fw_so3_to_subset(s2b_fw_plan* plan, int batch, int ngamma, int nspins,
                          const void* f, void* flmn, void* workspace, size_t workspace_bytes,
                          void* stream);
 
+/* Adjoints of the three spin-subset ops (complex): same plan, spins, delta / quads and
+ * workspace as the op, input and output exchanged (g_flmn = A^H g_f for subset_to_s2,
+ * g_f = A^H g_flmn for s2_to_subset and so3_to_subset). Replace JAX's autodiff of
+ * upstream's custom_ops.py:5-333. */
+int s2b_fw_subset_to_s2_adjoint(s2b_fw_plan* plan, int batch, int nspins, const int* spins,
+                                const double* delta, const void* g_f, void* g_flmn,
+                                void* workspace, size_t workspace_bytes, void* stream);
+int s2b_fw_s2_to_subset_adjoint(s2b_fw_plan* plan, int batch, int nspins, const int* spins,
+                                const double* delta, const void* quads, const void* g_flmn,
+                                void* g_f, void* workspace, size_t workspace_bytes,
+                                void* stream);
+int s2b_fw_so3_to_subset_adjoint(s2b_fw_plan* plan, int batch, int ngamma, int nspins,
+                                 const int* spins, const double* delta, const void* quads,
+                                 const void* g_flmn, void* g_f, void* workspace,
+                                 size_t workspace_bytes, void* stream);
+
 /* Peak-rate probe: a fused multiply-add chain kernel (float when fp64 == 0,
  * double otherwise) over `blocks` CTAs of 256 threads, `iters` iterations of 8
  * independent FMA chains per thread, writing one value per thread to `out`

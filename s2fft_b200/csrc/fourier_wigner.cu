@@ -803,6 +803,37 @@ __global__ void fw_gamma_subset_kernel(const void* fin, void* xout, int O, int G
   }
 }
 
+// Adjoint of fw_gamma_subset_kernel: f[o][c][px] = (1/G) sum_k x[o][k][px] e^{+2 pi i c n_k / G}
+// for the G gamma samples c.
+template <typename Real>
+__global__ void fw_gamma_subset_adj_kernel(const void* xin, void* fout, int O, int G, int S,
+                                           long npix, FWSlices sl) {
+  using R2 = typename C2<Real>::t;
+  const R2* x = reinterpret_cast<const R2*>(xin);
+  R2* f = reinterpret_cast<R2*>(fout);
+  const long total = (long)O * npix;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
+       i += (long)gridDim.x * blockDim.x) {
+    const long o = i / npix, px = i % npix;
+    for (int c = 0; c < G; ++c) {
+      double re = 0.0, im = 0.0;
+      for (int k = 0; k < S; ++k) {
+        const int n = fw_n(sl, k);
+        const R2 v = x[(o * S + k) * npix + px];
+        const long r = (((long)c * n) % G + G) % G;
+        double sn, cs;
+        sincospi(2.0 * (double)r / (double)G, &sn, &cs);
+        re += (double)v.x * cs - (double)v.y * sn;
+        im += (double)v.x * sn + (double)v.y * cs;
+      }
+      R2 out;
+      out.x = (Real)(re / G);
+      out.y = (Real)(im / G);
+      f[(o * G + c) * npix + px] = out;
+    }
+  }
+}
+
 }  // namespace s2b
 
 using namespace s2b;
@@ -1401,6 +1432,84 @@ int s2b_fw_so3_to_subset(s2b_fw_plan* plan, int batch, int ngamma, int nspins, c
   if (plan->fp64)
     return forward_chain<double>(plan, E, sl, delta, quads, C, flmn, 0, 1, scale, w, lay, st);
   return forward_chain<float>(plan, E, sl, delta, quads, C, flmn, 0, 1, scale, w, lay, st);
+}
+
+// Adjoints of the spin-subset ops (same arguments, workspace and layouts as the op they
+// adjoin, with input and output exchanged).
+int s2b_fw_subset_to_s2_adjoint(s2b_fw_plan* plan, int batch, int nspins, const int* spins,
+                                const double* delta, const void* g_f, void* g_flmn, void* ws,
+                                size_t ws_bytes, void* stream) {
+  int rc;
+  if ((rc = check_plan(plan))) return rc;
+  if (batch < 1 || nspins < 1) return fw_fail(S2B_ERR_INVALID, "need batch >= 1 and nspins >= 1");
+  if (!spins) return fw_fail(S2B_ERR_INVALID, "spins is NULL");
+  if ((rc = check_ptrs({delta, g_f, g_flmn}))) return rc;
+  const FWSlices sl = spin_slices(nspins, spins);
+  const int E = batch * nspins;
+  if ((rc = check_slices((long)batch * nspins))) return rc;
+  const FWLayout lay = fw_layout(plan, E, 0, 0);
+  if ((rc = check_ws(lay, ws, ws_bytes))) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plan->fp64)
+    return inverse_adjoint_chain<double>(plan, E, sl, delta, g_f, g_flmn, 0, 1, (char*)ws, lay, st);
+  return inverse_adjoint_chain<float>(plan, E, sl, delta, g_f, g_flmn, 0, 1, (char*)ws, lay, st);
+}
+
+int s2b_fw_s2_to_subset_adjoint(s2b_fw_plan* plan, int batch, int nspins, const int* spins,
+                                const double* delta, const void* quads, const void* g_flmn,
+                                void* g_f, void* ws, size_t ws_bytes, void* stream) {
+  int rc;
+  if ((rc = check_plan(plan))) return rc;
+  if (batch < 1 || nspins < 1) return fw_fail(S2B_ERR_INVALID, "need batch >= 1 and nspins >= 1");
+  if (!spins) return fw_fail(S2B_ERR_INVALID, "spins is NULL");
+  if ((rc = check_ptrs({delta, quads, g_flmn, g_f}))) return rc;
+  const FWSlices sl = spin_slices(nspins, spins);
+  const int E = batch * nspins;
+  if ((rc = check_slices((long)batch * nspins))) return rc;
+  const FWLayout lay = fw_layout(plan, E, 0, 0);
+  if ((rc = check_ws(lay, ws, ws_bytes))) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plan->fp64)
+    return forward_adjoint_chain<double>(plan, E, sl, delta, quads, g_flmn, g_f, 0, 1,
+                                         (char*)ws, lay, st);
+  return forward_adjoint_chain<float>(plan, E, sl, delta, quads, g_flmn, g_f, 0, 1, (char*)ws,
+                                      lay, st);
+}
+
+int s2b_fw_so3_to_subset_adjoint(s2b_fw_plan* plan, int batch, int ngamma, int nspins,
+                                 const int* spins, const double* delta, const void* quads,
+                                 const void* g_flmn, void* g_f, void* ws, size_t ws_bytes,
+                                 void* stream) {
+  int rc;
+  if ((rc = check_plan(plan))) return rc;
+  if (batch < 1 || nspins < 1 || ngamma < 1)
+    return fw_fail(S2B_ERR_INVALID, "need batch, ngamma, nspins >= 1");
+  if (!spins) return fw_fail(S2B_ERR_INVALID, "spins is NULL");
+  if ((rc = check_ptrs({delta, quads, g_flmn, g_f}))) return rc;
+  const FWSlices sl = spin_slices(nspins, spins);
+  const int E = batch * nspins;
+  if ((rc = check_slices((long)batch * nspins))) return rc;
+  const FWLayout lay = fw_layout(plan, E, 0, E);
+  if ((rc = check_ws(lay, ws, ws_bytes))) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  char* w = (char*)ws;
+  void* C = w + lay.a + lay.b;
+  rc = plan->fp64 ? forward_adjoint_chain<double>(plan, E, sl, delta, quads, g_flmn, C, 0, 1, w,
+                                                  lay, st)
+                  : forward_adjoint_chain<float>(plan, E, sl, delta, quads, g_flmn, C, 0, 1, w,
+                                                 lay, st);
+  if (rc) return rc;
+  const long npix = (long)plan->ntheta * plan->nphi;
+  const long tot = (long)batch * npix;
+  const int blocks = (int)std::min<long>((tot + 255) / 256, 65535L);
+  if (plan->fp64)
+    fw_gamma_subset_adj_kernel<double><<<blocks, 256, 0, st>>>(C, g_f, batch, ngamma, nspins,
+                                                               npix, sl);
+  else
+    fw_gamma_subset_adj_kernel<float><<<blocks, 256, 0, st>>>(C, g_f, batch, ngamma, nspins,
+                                                              npix, sl);
+  FW_CK(cudaGetLastError());
+  return S2B_OK;
 }
 
 }  // extern "C"

@@ -8,7 +8,9 @@ Mirrors upstream (s2fft/precompute_transforms/custom_ops.py):
 Arrays carry upstream's layout ``[batch, n_s, ..., channels]``; ``DW`` is
 ``fourier_wigner.fourier_wigner_kernel(L)`` (or upstream's numpy pair). The work runs in
 the Fourier-Wigner kernels of ``libs2b.so`` with (batch x channels) maps per spin; the
-channel axis is moved next to the batch axis on the device around each call.
+channel axis is moved next to the batch axis on the device around each call. The ops are
+differentiable in their array input (adjoint entry points ``s2b_fw_*_adjoint``), as
+upstream's JAX versions are by autodiff.
 """
 
 from __future__ import annotations
@@ -40,6 +42,33 @@ def _channels_last(x):
     return x.permute(0, 2, 3, 4, 1).contiguous()
 
 
+class _OpFn(torch.autograd.Function):
+    """A linear op on channel-first device arrays: forward call(x, out), backward
+    adjoint(g, gx)."""
+
+    @staticmethod
+    def forward(ctx, xc, call, adjoint, out_shape):
+        ctx.adjoint, ctx.in_shape = adjoint, xc.shape
+        out = torch.empty(out_shape, dtype=xc.dtype, device=xc.device)
+        call(xc, out)
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        g = g.contiguous()
+        gx = torch.empty(ctx.in_shape, dtype=g.dtype, device=g.device)
+        ctx.adjoint(g, gx)
+        return gx, None, None, None
+
+
+def _apply(xc, call, adjoint, out_shape):
+    if xc.requires_grad and torch.is_grad_enabled():
+        return _OpFn.apply(xc, call, adjoint, out_shape)
+    out = torch.empty(out_shape, dtype=xc.dtype, device=xc.device)
+    call(xc, out)
+    return out
+
+
 def wigner_subset_to_s2(flmn, spins, DW, L: int, sampling: str = "mw",
                         precision: str = "f64"):
     """flmn [batch, n_s, L, 2L-1, ch] -> spin maps [batch, n_s, ntheta, nphi, ch]."""
@@ -58,13 +87,19 @@ def wigner_subset_to_s2(flmn, spins, DW, L: int, sampling: str = "mw",
     Bt, S, _, _, C = x.shape
     xc = _channels_first(x)
     nth, nph = _geometry(L, s)
-    out = torch.empty((Bt, C, S, nth, nph), dtype=cdt, device=x.device)
     plan = get_plan(x.device, L, s, precision)
-    ws = plan.workspace(OP_SUBSET_TO_S2, Bt * C, nspins=S)
-    _lib.check(_fwlib().s2b_fw_subset_to_s2(plan.ptr, Bt * C, S, spd.data_ptr(),
-                                            delta.data_ptr(), xc.data_ptr(), out.data_ptr(),
-                                            ws.data_ptr(), ws.numel(),
-                                            _lib.stream_handle(x.device)))
+
+    def run(name):
+        def call(a, b):
+            ws = plan.workspace(OP_SUBSET_TO_S2, Bt * C, nspins=S)
+            _lib.check(getattr(_fwlib(), name)(plan.ptr, Bt * C, S, spd.data_ptr(),
+                                               delta.data_ptr(), a.data_ptr(), b.data_ptr(),
+                                               ws.data_ptr(), ws.numel(),
+                                               _lib.stream_handle(a.device)))
+        return call
+
+    out = _apply(xc, run("s2b_fw_subset_to_s2"), run("s2b_fw_subset_to_s2_adjoint"),
+                 (Bt, C, S, nth, nph))
     return _ret(_channels_last(out), was_np, odev)
 
 
@@ -81,13 +116,19 @@ def s2_to_wigner_subset(fs, spins, DW, L: int, sampling: str = "mw", precision: 
     delta, quads = _precomps(DW, L, x.device)
     Bt, S, _, _, C = x.shape
     xc = _channels_first(x)
-    out = torch.empty((Bt, C, S, L, 2 * L - 1), dtype=cdt, device=x.device)
     plan = get_plan(x.device, L, s, precision)
-    ws = plan.workspace(OP_S2_TO_SUBSET, Bt * C, nspins=S)
-    _lib.check(_fwlib().s2b_fw_s2_to_subset(plan.ptr, Bt * C, S, spd.data_ptr(),
-                                            delta.data_ptr(), quads.data_ptr(), xc.data_ptr(),
-                                            out.data_ptr(), ws.data_ptr(), ws.numel(),
-                                            _lib.stream_handle(x.device)))
+
+    def run(name):
+        def call(a, b):
+            ws = plan.workspace(OP_S2_TO_SUBSET, Bt * C, nspins=S)
+            _lib.check(getattr(_fwlib(), name)(plan.ptr, Bt * C, S, spd.data_ptr(),
+                                               delta.data_ptr(), quads.data_ptr(), a.data_ptr(),
+                                               b.data_ptr(), ws.data_ptr(), ws.numel(),
+                                               _lib.stream_handle(a.device)))
+        return call
+
+    out = _apply(xc, run("s2b_fw_s2_to_subset"), run("s2b_fw_s2_to_subset_adjoint"),
+                 (Bt, C, S, L, 2 * L - 1))
     return _ret(_channels_last(out), was_np, odev)
 
 
@@ -107,11 +148,17 @@ def so3_to_wigner_subset(f, spins, DW, L: int, N: int, sampling: str = "mw",
     Bt, G, _, _, C = x.shape
     S = sp.shape[0]
     xc = _channels_first(x)
-    out = torch.empty((Bt, C, S, L, 2 * L - 1), dtype=cdt, device=x.device)
     plan = get_plan(x.device, L, s, precision)
-    ws = plan.workspace(OP_SO3_TO_SUBSET, Bt * C, nspins=S)
-    _lib.check(_fwlib().s2b_fw_so3_to_subset(plan.ptr, Bt * C, G, S, spd.data_ptr(),
-                                             delta.data_ptr(), quads.data_ptr(), xc.data_ptr(),
-                                             out.data_ptr(), ws.data_ptr(), ws.numel(),
-                                             _lib.stream_handle(x.device)))
+
+    def run(name):
+        def call(a, b):
+            ws = plan.workspace(OP_SO3_TO_SUBSET, Bt * C, nspins=S)
+            _lib.check(getattr(_fwlib(), name)(plan.ptr, Bt * C, G, S, spd.data_ptr(),
+                                               delta.data_ptr(), quads.data_ptr(), a.data_ptr(),
+                                               b.data_ptr(), ws.data_ptr(), ws.numel(),
+                                               _lib.stream_handle(a.device)))
+        return call
+
+    out = _apply(xc, run("s2b_fw_so3_to_subset"), run("s2b_fw_so3_to_subset_adjoint"),
+                 (Bt, C, S, L, 2 * L - 1))
     return _ret(_channels_last(out), was_np, odev)

@@ -48,6 +48,10 @@ def _fwlib():
                 "s2b_fw_subset_to_s2": [vp, ci, ci, vp, vp, vp, vp, vp, sz, vp],
                 "s2b_fw_s2_to_subset": [vp, ci, ci, vp, vp, vp, vp, vp, vp, sz, vp],
                 "s2b_fw_so3_to_subset": [vp, ci, ci, ci, vp, vp, vp, vp, vp, vp, sz, vp],
+                "s2b_fw_subset_to_s2_adjoint": [vp, ci, ci, vp, vp, vp, vp, vp, sz, vp],
+                "s2b_fw_s2_to_subset_adjoint": [vp, ci, ci, vp, vp, vp, vp, vp, vp, sz, vp],
+                "s2b_fw_so3_to_subset_adjoint": [vp, ci, ci, ci, vp, vp, vp, vp, vp, vp, sz,
+                                                 vp],
                 "s2b_fw_inverse_adjoint": [vp, ci, vp, vp, vp, vp, sz, vp],
                 "s2b_fw_forward_adjoint": [vp, ci, vp, vp, vp, vp, vp, sz, vp],
             }

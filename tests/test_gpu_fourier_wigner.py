@@ -268,3 +268,37 @@ def test_gradient_matches_recursion_wigner(s2b):
     loss2 = (s2b.wigner.inverse(x2, L, N, sampling="mw").real - g).pow(2).sum()
     (g2,) = torch.autograd.grad(loss2, x2)
     assert relerr(g1.cpu().numpy(), g2.cpu().numpy()) < 1e-9
+
+
+@pytest.mark.parametrize("sampling", ["mw", "mwss"])
+@pytest.mark.parametrize("precision,tol", [("f64", 1e-10), ("f32", 1e-5)])
+def test_subset_ops_adjoint_dot_products(s2b, sampling, precision, tol):
+    """Gradients of the three spin-subset ops (batch 2, 3 channels, spins {0, 3, -2}):
+    <A x, y> = <x, A^H y> through the s2b_fw_*_adjoint entry points."""
+    L, N = 10, 4
+    rng = np.random.default_rng(21)
+    ops = s2b.custom_ops
+    DW = s2b.fourier_wigner.fourier_wigner_kernel(L)
+    cdt = torch.complex128 if precision == "f64" else torch.complex64
+    nth, nph = (L + 1, 2 * L) if sampling == "mwss" else (L, 2 * L - 1)
+    sp = np.array([0, 3, -2])
+
+    def rnd(shape):
+        return torch.tensor(rng.normal(size=shape) + 1j * rng.normal(size=shape), dtype=cdt,
+                            device="cuda")
+
+    cases = [
+        (lambda x: ops.wigner_subset_to_s2(x, sp, DW, L, sampling, precision=precision),
+         (2, 3, L, 2 * L - 1, 3), (2, 3, nth, nph, 3)),
+        (lambda x: ops.s2_to_wigner_subset(x, sp, DW, L, sampling, precision=precision),
+         (2, 3, nth, nph, 3), (2, 3, L, 2 * L - 1, 3)),
+        (lambda x: ops.so3_to_wigner_subset(x, sp, DW, L, N, sampling, precision=precision),
+         (2, 2 * N - 1, nth, nph, 3), (2, 3, L, 2 * L - 1, 3)),
+    ]
+    for fn, ishape, oshape in cases:
+        x = rnd(ishape).requires_grad_(True)
+        y = rnd(oshape)
+        out = fn(x)
+        (gx,) = torch.autograd.grad(out, x, grad_outputs=y)
+        lhs, rhs = _vdot(out.detach(), y), _vdot(x.detach(), gx)
+        assert abs(lhs - rhs) <= tol * max(abs(lhs), 1e-30) * 10, (ishape, lhs, rhs)
