@@ -711,12 +711,12 @@ def main():
             "e2e": {"value": r["e2e"], "unit": UNIT, "h2d_bytes_per_step": r["h2d"],
                     "d2h_bytes_per_step": r["d2h"]},
             "gpu_launches": 8 * args.steps}
-    if not args.profile_case and not args.no_extra:
+    if not args.profile_case and not args.no_extra and world == 1:
         line["batched_precompute"] = run_batched_precompute(torch)
         line["healpix_iter3"] = run_healpix_iter(torch)
         line["batched_uneven"] = run_batched_uneven(torch)
         line["so3_fourier_wigner"] = run_so3(torch)
-    if not args.no_cpu_baseline and not args.profile_case:
+    if not args.no_cpu_baseline and not args.profile_case and world == 1:
         c = cpu_sample(args.L, args.cpu_budget)
         line["cpu_baseline"] = {"value": c["value"], "unit": UNIT, "cores": c["cores"],
                                 "kind": "port", "sample": c["sample"],
