@@ -459,8 +459,12 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) mw_cols_adj_ke
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
+// Threads of a transform CTA: two 8-element groups per thread in every fused pass (M / 16
+// threads) measured 3.7 % faster on the L=1024 step than one group per thread (M / 8)
+// and 7 % faster than four (M / 32): the second independent group hides shared-memory
+// latency and halves the warps that meet at each barrier.
 static int fft_threads(int M) {
-  int t = M / 8;
+  int t = M / 16;
   if (t > 512) t = 512;
   if (t < 32) t = 32;
   return t;
