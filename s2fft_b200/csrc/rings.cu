@@ -236,8 +236,11 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) mw_cols_kernel
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const FFTDesc d1 = *p.d1;
   const FFTDesc d2 = *p.d2;
+  // one DFT buffer for both transforms; the 2L-1 (2L) bins of the first that feed the
+  // second are kept, phase-multiplied, in tmp in between
   R2* s1 = reinterpret_cast<R2*>(smem_raw);
-  R2* s2 = s1 + padded_len(d1.M);
+  R2* s2 = s1;
+  R2* tmp = s1 + padded_len(d1.M > d2.M ? d1.M : d2.M);
   const int L = p.L;
   const int mlo = p.mw ? -(L - 1) : -L;
   const int ncm = L - mlo;
@@ -262,13 +265,16 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) mw_cols_kernel
   const int phi = L - 1;
   const int n2 = d2.n;  // 4L
   const R2* __restrict__ ph = reinterpret_cast<const R2*>(p.ph);
-  auto load2 = [&](int k) -> R2 {
-    // k = pp mod 4L for pp in [plo, phi]; ph is zero outside
-    const int pp = k <= phi ? k : k - n2;
-    if (pp < plo || pp > phi) return czero<R2>();
+  for (int pp = plo + (int)threadIdx.x; pp <= phi; pp += blockDim.x) {
     const int j = pmod(pp, n1);
     const R2 g = d1.bluestein ? s1[pidx(j)] : s1[pidx(bitrev(j, d1.logM))];
-    return cmul(g, ph[k]);
+    tmp[pp - plo] = cmul(g, ph[(pp + n2) % n2]);
+  }
+  __syncthreads();
+  auto load2 = [&](int k) -> R2 {
+    // k = pp mod 4L for pp in [plo, phi]; zero outside
+    const int pp = k <= phi ? k : k - n2;
+    return (pp < plo || pp > phi) ? czero<R2>() : tmp[pp - plo];
   };
   dft_run<Real>(s2, d2, p.tb, true, load2);
   const int nout = 2 * L + 1;
@@ -504,7 +510,8 @@ template <typename Real>
 cudaError_t launch_mw_cols(const ColsParams<Real>& p, int ncm, int batch, int M1, int M2,
                            cudaStream_t s) {
   using R2 = typename C2<Real>::t;
-  const size_t smem = (size_t)(padded_len(M1) + padded_len(M2)) * sizeof(R2);
+  // one DFT buffer plus the 2L bins carried between the two transforms
+  const size_t smem = (size_t)(padded_len(M1 > M2 ? M1 : M2) + 2 * p.L) * sizeof(R2);
   cudaError_t e = cudaFuncSetAttribute(mw_cols_kernel<Real>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
