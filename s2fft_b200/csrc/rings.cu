@@ -409,8 +409,11 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) mw_cols_adj_ke
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const FFTDesc d1 = *p.d1;
   const FFTDesc d2 = *p.d2;
+  // one DFT buffer for both transforms; the n1 inputs of the second, phase-multiplied,
+  // are kept in tmp in between
   R2* s1 = reinterpret_cast<R2*>(smem_raw);
-  R2* s2 = s1 + padded_len(d1.M);
+  R2* s2 = s1;
+  R2* tmp = s1 + padded_len(d1.M > d2.M ? d1.M : d2.M);
   const int L = p.L;
   const int mlo = p.mw ? -(L - 1) : -L;
   const int mi = blockIdx.x;
@@ -441,13 +444,13 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) mw_cols_adj_ke
   const int n1 = d1.n;
   const int n2 = d2.n;
   const R2* __restrict__ pha = reinterpret_cast<const R2*>(p.ph_adj);
-  auto load1 = [&](int j) -> R2 {
+  for (int j = threadIdx.x; j < n1; j += blockDim.x) {
     const int pp = j <= phi ? j : j - n1;  // the bin p in [plo, phi] with p = j (mod n1)
-    if (pp < plo) return czero<R2>();
     const int k = (pp + n2) % n2;
-    return cmul(dft_get<Real>(s2, d2, p.tb, false, k), pha[k]);
-  };
-  dft_run<Real>(s1, d1, p.tb, true, load1);  // unnormalised inverse DFT over n1
+    tmp[j] = pp < plo ? czero<R2>() : cmul(dft_get<Real>(s2, d2, p.tb, false, k), pha[k]);
+  }
+  __syncthreads();
+  dft_run<Real>(s1, d1, p.tb, true, [&](int j) { return tmp[j]; });  // unnormalised inverse DFT over n1
   const int par = ((m + p.spin) % 2 + 2) % 2;
   const Real sgn = par ? Real(-1) : Real(1);
   for (int t = threadIdx.x; t < p.nin; t += blockDim.x) {
@@ -526,7 +529,8 @@ template <typename Real>
 cudaError_t launch_mw_cols_adj(const ColsParams<Real>& p, int ncm, int batch, int M1, int M2,
                                int ncol_out, int mo_out, cudaStream_t s) {
   using R2 = typename C2<Real>::t;
-  const size_t smem = (size_t)(padded_len(M1) + padded_len(M2)) * sizeof(R2);
+  // one DFT buffer plus the n1 = 2L-1 or 2L inputs of the second transform
+  const size_t smem = (size_t)(padded_len(M1 > M2 ? M1 : M2) + 2 * p.L) * sizeof(R2);
   cudaError_t e = cudaFuncSetAttribute(mw_cols_adj_kernel<Real>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
