@@ -400,9 +400,10 @@ struct s2b_plan {
   size_t ws_w_fban = 0, ws_w_tmp = 0, ws_w_sub = 0;
   // Wigner: the spin transforms of different n run concurrently on internal streams, forked
   // from and joined back to the caller's stream with events; one workspace slice per stream
+  static constexpr int kMaxWStreams = 8;
   int nwstream = 0;
-  cudaStream_t wstream[4] = {};
-  cudaEvent_t wfork = nullptr, wjoin[4] = {};
+  cudaStream_t wstream[kMaxWStreams] = {};
+  cudaEvent_t wfork = nullptr, wjoin[kMaxWStreams] = {};
   // optional events recorded around the latitudinal launch ([0] inverse, [1] forward)
   int tile_fwd = 0, tile_inv = 0;  // latitudinal tile variants (s2b_plan_set_tuning)
   cudaEvent_t ev_begin[2] = {nullptr, nullptr};
@@ -1811,7 +1812,7 @@ static int build_wigner(s2b_plan* p) {
   const size_t c2 = 2 * p->rsz;
   p->ws_w_fban = (size_t)(2 * d.N - 1) * d.batch * p->npix * c2;
   p->ws_w_tmp = (size_t)d.batch * d.L * (2 * d.L - 1) * c2;
-  p->nwstream = std::min<int>(4, (int)p->subs.size());
+  p->nwstream = std::min<int>(s2b_plan::kMaxWStreams, (int)p->subs.size());
   if (p->nwstream > 1) {
     S2B_CK(cudaEventCreateWithFlags(&p->wfork, cudaEventDisableTiming));
     for (int k = 0; k < p->nwstream; ++k) {
@@ -1969,7 +1970,7 @@ int s2b_plan_destroy(s2b_plan* p) {
   if (!p) return S2B_OK;
   for (s2b_plan* sp : p->subs) s2b_plan_destroy(sp);
   for (void* a : p->allocs) cudaFree(a);
-  for (int k = 0; k < 4; ++k) {
+  for (int k = 0; k < s2b_plan::kMaxWStreams; ++k) {
     if (p->wstream[k]) cudaStreamDestroy(p->wstream[k]);
     if (p->wjoin[k]) cudaEventDestroy(p->wjoin[k]);
   }
