@@ -24,25 +24,27 @@ __device__ __forceinline__ double lnorm(int l) { return sqrt((2.0 * l + 1.0) / (
 
 // F [b][half][j][m + kPadLo][q] (Real2, or Real4 when dual) from flm [b][l][L-1+m];
 // the pad rows (m < 0, m = L) are written as zeros.
-template <typename Real>
+// Idx is the flat index type: 32-bit whenever the whole table fits, since 64-bit
+// division by a runtime divisor costs several times the 32-bit one and these
+// kernels are bound by their index arithmetic.
+template <typename Real, typename Idx>
 __global__ void prologue_kernel(StageParams p) {
   using R2 = R2_t<Real>;
   using R4 = R4_t<Real>;
   const int L = p.L, C = p.nclass, Q = p.Q, TR = p.TR;
-  const long per_b = (long)p.nhalf * C * TR * Q;
-  const long total = per_b * p.batch;
+  const Idx total = (Idx)p.nhalf * C * TR * Q * p.batch;
   const R2* flm = reinterpret_cast<const R2*>(p.flm);
-  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
-       idx += (long)gridDim.x * blockDim.x) {
-    long r = idx;
-    const int q = (int)(r % Q);
-    r /= Q;
-    const int m = (int)(r % TR) - kPadLo;
-    r /= TR;
-    const int j = (int)(r % C);
-    r /= C;
-    const int half = (int)(r % p.nhalf);
-    const int b = (int)(r / p.nhalf);
+  for (Idx idx = blockIdx.x * (Idx)blockDim.x + threadIdx.x; idx < total;
+       idx += (Idx)gridDim.x * blockDim.x) {
+    Idx r = idx;
+    const int q = (int)(r % (Idx)Q);
+    r /= (Idx)Q;
+    const int m = (int)(r % (Idx)TR) - kPadLo;
+    r /= (Idx)TR;
+    const int j = (int)(r % (Idx)C);
+    r /= (Idx)C;
+    const int half = (int)(r % (Idx)p.nhalf);
+    const int b = (int)(r / (Idx)p.nhalf);
     const int l = p.Lp > 0 ? j * Q + q : j + C * q;  // blocked: l = 32 block + column
     const int as = p.spin < 0 ? -p.spin : p.spin;
     const bool ok = m >= 0 && m < L && l < L && l >= m && l >= p.L0 && l >= as;
@@ -139,20 +141,22 @@ __device__ __forceinline__ R2_t<Real> spectrum_at(const StageParams& p, int b, i
 }
 
 // flm [b][l][L-1+m] from the projected sums acc [b][half][j][m][q].
-template <typename Real>
+template <typename Real, typename Idx>
 __global__ void epilogue_kernel(StageParams p) {
   using R2 = R2_t<Real>;
   const int L = p.L, C = p.nclass, Q = p.Q;
   const int W = 2 * L - 1;
-  const long total = (long)p.batch * L * W;
+  const Idx total = (Idx)p.batch * L * W;
   const int as = p.spin < 0 ? -p.spin : p.spin;
   const int lmin = as > p.L0 ? as : p.L0;
   const double sgn_s = (p.spin & 1) ? -1.0 : 1.0;
-  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
-       idx += (long)gridDim.x * blockDim.x) {
-    const int c = (int)(idx % W);
-    const int l = (int)((idx / W) % L);
-    const int b = (int)(idx / ((long)W * L));
+  for (Idx idx = blockIdx.x * (Idx)blockDim.x + threadIdx.x; idx < total;
+       idx += (Idx)gridDim.x * blockDim.x) {
+    const Idx lw = idx / (Idx)W;
+    const int c = (int)(idx - lw * (Idx)W);
+    const Idx bl = lw / (Idx)L;
+    const int l = (int)(lw - bl * (Idx)L);
+    const int b = (int)bl;
     const int m = c - (L - 1);
     const int am = m < 0 ? -m : m;
     double re = 0.0, im = 0.0;
@@ -248,12 +252,21 @@ static int grid_for(long n) {
   return (int)b;
 }
 
+// A flat index fits 32 bits when the last grid-stride step (index + grid size, at most
+// 65535 x 256 beyond the end) stays below 2^32.
+static bool fits32(long n) { return n + 65535L * 256 < (1L << 32); }
+
 cudaError_t launch_prologue(bool fp64, const StageParams& p, cudaStream_t s) {
   const long total = (long)p.batch * p.nhalf * p.nclass * p.TR * p.Q;
-  if (fp64)
-    prologue_kernel<double><<<grid_for(total), 256, 0, s>>>(p);
+  const bool i32 = fits32(total);
+  if (fp64 && i32)
+    prologue_kernel<double, uint32_t><<<grid_for(total), 256, 0, s>>>(p);
+  else if (fp64)
+    prologue_kernel<double, uint64_t><<<grid_for(total), 256, 0, s>>>(p);
+  else if (i32)
+    prologue_kernel<float, uint32_t><<<grid_for(total), 256, 0, s>>>(p);
   else
-    prologue_kernel<float><<<grid_for(total), 256, 0, s>>>(p);
+    prologue_kernel<float, uint64_t><<<grid_for(total), 256, 0, s>>>(p);
   return cudaGetLastError();
 }
 
@@ -268,10 +281,15 @@ cudaError_t launch_poles(bool fp64, const StageParams& p, cudaStream_t s) {
 
 cudaError_t launch_epilogue(bool fp64, const StageParams& p, cudaStream_t s) {
   const long total = (long)p.batch * p.L * (2 * p.L - 1);
-  if (fp64)
-    epilogue_kernel<double><<<grid_for(total), 256, 0, s>>>(p);
+  const bool i32 = fits32(total);
+  if (fp64 && i32)
+    epilogue_kernel<double, uint32_t><<<grid_for(total), 256, 0, s>>>(p);
+  else if (fp64)
+    epilogue_kernel<double, uint64_t><<<grid_for(total), 256, 0, s>>>(p);
+  else if (i32)
+    epilogue_kernel<float, uint32_t><<<grid_for(total), 256, 0, s>>>(p);
   else
-    epilogue_kernel<float><<<grid_for(total), 256, 0, s>>>(p);
+    epilogue_kernel<float, uint64_t><<<grid_for(total), 256, 0, s>>>(p);
   return cudaGetLastError();
 }
 
