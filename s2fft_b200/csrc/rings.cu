@@ -543,22 +543,26 @@ cudaError_t launch_mw_cols_adj(const ColsParams<Real>& p, int ncm, int batch, in
 }
 
 // ---------------------------------------------------------------------------
-// Ring-pair fold (equator-symmetric forward): one thread per (map, half, row, pair, component)
+// Ring-pair fold (equator-symmetric forward): one thread per (map, half, row, pair, component).
+// Idx is the flat index type (32-bit whenever the arrays fit: 64-bit division by a
+// runtime divisor would dominate these element-wise kernels).
 // ---------------------------------------------------------------------------
-template <typename Real>
+template <typename Real, typename Idx>
 __global__ void fold_pairs_kernel(FoldParams p) {
   using R2 = typename C2<Real>::t;
   const int per = p.dual ? 2 : 1;  // Real2 entries of one spectrum (dual: +m and -m)
   const int halves = p.dual ? 1 : p.nhalf;
-  const long total = (long)p.batch * halves * p.TR * p.Gs2 * per;
+  const Idx total = (Idx)p.batch * halves * p.TR * p.Gs2 * per;
   const R2* G = reinterpret_cast<const R2*>(p.G);
   R2* G2 = reinterpret_cast<R2*>(p.G2);
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
-       i += (long)gridDim.x * blockDim.x) {
-    const int c = (int)(i % per);
-    const int q = (int)((i / per) % p.Gs2);
-    const long row = i / ((long)per * p.Gs2);  // (b, half, m row)
-    const int mrow = (int)(row % p.TR);
+  for (Idx i = blockIdx.x * (Idx)blockDim.x + threadIdx.x; i < total;
+       i += (Idx)gridDim.x * blockDim.x) {
+    const int c = p.dual ? (int)(i & 1) : 0;
+    const Idx iq = p.dual ? i >> 1 : i;
+    const Idx rw = iq / (Idx)p.Gs2;
+    const int q = (int)(iq - rw * (Idx)p.Gs2);
+    const size_t row = rw;  // (b, half, m row)
+    const int mrow = (int)(rw % (Idx)p.TR);
     R2 e = czero<R2>(), o = czero<R2>();
     if (q < p.npair && mrow >= kPadLo && mrow < p.L + kPadLo) {
       const int qm = p.nrows - 1 - q;  // mirror ring
@@ -576,18 +580,20 @@ __global__ void fold_pairs_kernel(FoldParams p) {
 }
 
 // cross mode: one thread per (map, half, row, pair)
-template <typename Real>
+template <typename Real, typename Idx>
 __global__ void fold_cross_kernel(FoldParams p) {
   using R2 = typename C2<Real>::t;
-  const long total = (long)p.batch * 2 * p.TR * p.Gs2;
+  const Idx total = (Idx)p.batch * 2 * p.TR * p.Gs2;
   const R2* G = reinterpret_cast<const R2*>(p.G);
   R2* G2 = reinterpret_cast<R2*>(p.G2);
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
-       i += (long)gridDim.x * blockDim.x) {
-    const int q = (int)(i % p.Gs2);
-    const long row = i / p.Gs2;  // (b, half, m row)
-    const int mrow = (int)(row % p.TR);
-    const int half = (int)((row / p.TR) % 2);
+  for (Idx i = blockIdx.x * (Idx)blockDim.x + threadIdx.x; i < total;
+       i += (Idx)gridDim.x * blockDim.x) {
+    const Idx rw = i / (Idx)p.Gs2;
+    const int q = (int)(i - rw * (Idx)p.Gs2);
+    const long row = (long)rw;  // (b, half, m row)
+    const Idx bh = rw / (Idx)p.TR;
+    const int mrow = (int)(rw - bh * (Idx)p.TR);
+    const int half = (int)(bh & 1);
     const long orow = row + (half ? -1L : 1L) * p.TR;  // the other half, same map and m
     R2 a = czero<R2>(), z = czero<R2>();
     if (q < p.npair && mrow >= kPadLo && mrow < p.L + kPadLo) {
@@ -609,20 +615,30 @@ cudaError_t launch_fold_pairs(bool fp64, const FoldParams& p, cudaStream_t s) {
     long blocks = (total + 255) / 256;
     if (blocks > 65535L * 8) blocks = 65535L * 8;
     if (blocks < 1) blocks = 1;
-    if (fp64)
-      fold_cross_kernel<double><<<(unsigned)blocks, 256, 0, s>>>(p);
+    const bool i32 = total + 65535L * 8 * 256 < (1L << 32);
+    if (fp64 && i32)
+      fold_cross_kernel<double, uint32_t><<<(unsigned)blocks, 256, 0, s>>>(p);
+    else if (fp64)
+      fold_cross_kernel<double, uint64_t><<<(unsigned)blocks, 256, 0, s>>>(p);
+    else if (i32)
+      fold_cross_kernel<float, uint32_t><<<(unsigned)blocks, 256, 0, s>>>(p);
     else
-      fold_cross_kernel<float><<<(unsigned)blocks, 256, 0, s>>>(p);
+      fold_cross_kernel<float, uint64_t><<<(unsigned)blocks, 256, 0, s>>>(p);
     return cudaGetLastError();
   }
   const long total = (long)p.batch * (p.dual ? 1 : p.nhalf) * p.TR * p.Gs2 * (p.dual ? 2 : 1);
   long blocks = (total + 255) / 256;
   if (blocks > 65535L * 8) blocks = 65535L * 8;
   if (blocks < 1) blocks = 1;
-  if (fp64)
-    fold_pairs_kernel<double><<<(unsigned)blocks, 256, 0, s>>>(p);
+  const bool i32 = total + 65535L * 8 * 256 < (1L << 32);
+  if (fp64 && i32)
+    fold_pairs_kernel<double, uint32_t><<<(unsigned)blocks, 256, 0, s>>>(p);
+  else if (fp64)
+    fold_pairs_kernel<double, uint64_t><<<(unsigned)blocks, 256, 0, s>>>(p);
+  else if (i32)
+    fold_pairs_kernel<float, uint32_t><<<(unsigned)blocks, 256, 0, s>>>(p);
   else
-    fold_pairs_kernel<float><<<(unsigned)blocks, 256, 0, s>>>(p);
+    fold_pairs_kernel<float, uint64_t><<<(unsigned)blocks, 256, 0, s>>>(p);
   return cudaGetLastError();
 }
 
