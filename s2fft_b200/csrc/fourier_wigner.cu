@@ -789,7 +789,7 @@ __global__ void fw_gamma_subset_kernel(const void* fin, void* xout, int O, int G
       double re = 0.0, im = 0.0;
       for (int c = 0; c < G; ++c) {
         const R2 v = f[(o * G + c) * npix + px];
-        const long r = ((-(long)c * n) % G + G) % G;
+        const int r = ((-c * n) % G + G) % G;  // |c n| < G N, far below 2^31
         double sn, cs;
         sincospi(2.0 * (double)r / (double)G, &sn, &cs);
         re += (double)v.x * cs - (double)v.y * sn;
@@ -820,7 +820,7 @@ __global__ void fw_gamma_subset_adj_kernel(const void* xin, void* fout, int O, i
       for (int k = 0; k < S; ++k) {
         const int n = fw_n(sl, k);
         const R2 v = x[(o * S + k) * npix + px];
-        const long r = (((long)c * n) % G + G) % G;
+        const int r = ((c * n) % G + G) % G;
         double sn, cs;
         sincospi(2.0 * (double)r / (double)G, &sn, &cs);
         re += (double)v.x * cs - (double)v.y * sn;
