@@ -184,6 +184,24 @@ int s2b_plan_status(s2b_plan* plan, int* status);
  * front-end. No upstream counterpart. */
 int s2b_plan_set_tuning(s2b_plan* plan, int key, int value);
 
+/* The CUDA device ordinal a plan was created on (the device current at
+ * s2b_plan_create). Every execute call on a spin or Wigner plan returns
+ * S2B_ERR_INVALID, before launching anything, when the current device differs.
+ * No upstream counterpart (upstream's plan cache is per process,
+ * lib/include/plan_cache.h:15-44). */
+int s2b_plan_device(const s2b_plan* plan, int* device);
+
+/* Testing hook: overwrite the device ordinal recorded in the plan (and its
+ * Wigner sub-plans), so that the device check above can be exercised on a
+ * machine with one GPU. Never needed in normal use. No upstream counterpart. */
+int s2b_debug_set_plan_device(s2b_plan* plan, int device);
+
+/* Instrumentation: number of device allocations (cudaMalloc) the library has
+ * made since it was loaded: plan tables, and the temporary table of
+ * s2b_kernel_build with S2B_BF16X3. Execute calls add nothing to it. No
+ * upstream counterpart. */
+long long s2b_device_alloc_count(void);
+
 /* Instrumentation: record the caller's cudaEvent_t objects (passed as void*)
  * immediately before and after the latitudinal (recursion + projection) kernel
  * of every later inverse (forward = 0) or forward (forward = 1) call on this
@@ -204,9 +222,12 @@ int s2b_plan_set_events(s2b_plan* plan, int forward, void* ev_begin, void* ev_en
  *     S2B_NOALLOC_SCRATCH_BYTES are rejected with S2B_ERR_WORKSPACE. 32 MiB
  *     covers one mw-sampled map up to L ~ 1000 in float32 and L ~ 700 in
  *     float64; dh, with twice the rings, reaches about 5/6 of that.
- *   - The first call on a device (the current device, which must be the
- *     plan's) looks up the array's device address with cudaGetSymbolAddress;
- *     make that first call before any stream capture on that device.
+ *   - The current device must be the plan's (else S2B_ERR_INVALID). The
+ *     first call on a device looks up the array's device address with
+ *     cudaGetSymbolAddress and keeps it; make that first call before any
+ *     stream capture on that device. The kept address is not valid after a
+ *     cudaDeviceReset of that device: do not call this entry point on a
+ *     device after resetting it.
  *   - Every call on a device shares the one array: calls that can overlap on
  *     the GPU (different streams, threads or plans without ordering between
  *     them) race and corrupt each other's results. Order them on one stream.

@@ -66,6 +66,8 @@ _SIGS = {
                        + [ctypes.c_size_t, ctypes.c_void_p],
     "s2b_rotate_dls": [ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
                        ctypes.c_size_t, ctypes.c_void_p],
+    "s2b_plan_device": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)],
+    "s2b_debug_set_plan_device": [ctypes.c_void_p, ctypes.c_int],
 }
 
 
@@ -86,6 +88,8 @@ def lib():
             handle.s2b_last_error.restype = ctypes.c_char_p
             handle.s2b_rotate_workspace_size.argtypes = [ctypes.c_int]
             handle.s2b_rotate_workspace_size.restype = ctypes.c_size_t
+            handle.s2b_device_alloc_count.argtypes = []
+            handle.s2b_device_alloc_count.restype = ctypes.c_longlong
             _lib = handle
     return _lib
 

@@ -785,11 +785,11 @@ __global__ void fw_gamma_subset_kernel(const void* fin, void* xout, int O, int G
        i += (long)gridDim.x * blockDim.x) {
     const long o = i / npix, px = i % npix;
     for (int k = 0; k < S; ++k) {
-      const int n = fw_n(sl, k);
+      const int nm = ((fw_n(sl, k) % G) + G) % G;  // n mod G, so that c * nm < G^2 fits an int
       double re = 0.0, im = 0.0;
       for (int c = 0; c < G; ++c) {
         const R2 v = f[(o * G + c) * npix + px];
-        const int r = ((-c * n) % G + G) % G;  // |c n| < G N, far below 2^31
+        const int r = (G - (c * nm) % G) % G;  // (-c n) mod G
         double sn, cs;
         sincospi(2.0 * (double)r / (double)G, &sn, &cs);
         re += (double)v.x * cs - (double)v.y * sn;
@@ -818,9 +818,9 @@ __global__ void fw_gamma_subset_adj_kernel(const void* xin, void* fout, int O, i
     for (int c = 0; c < G; ++c) {
       double re = 0.0, im = 0.0;
       for (int k = 0; k < S; ++k) {
-        const int n = fw_n(sl, k);
+        const int nm = ((fw_n(sl, k) % G) + G) % G;  // n mod G: c * nm < G^2 fits an int
         const R2 v = x[(o * S + k) * npix + px];
-        const int r = ((c * n) % G + G) % G;
+        const int r = (c * nm) % G;
         double sn, cs;
         sincospi(2.0 * (double)r / (double)G, &sn, &cs);
         re += (double)v.x * cs - (double)v.y * sn;
@@ -1410,6 +1410,8 @@ int s2b_fw_so3_to_subset(s2b_fw_plan* plan, int batch, int ngamma, int nspins, c
   if ((rc = check_plan(plan))) return rc;
   if (batch < 1 || nspins < 1 || ngamma < 1)
     return fw_fail(S2B_ERR_INVALID, "need batch, ngamma, nspins >= 1");
+  if (ngamma > 46340)  // the gamma DFT's phase index c * n mod ngamma stays below 2^31
+    return fw_fail(S2B_ERR_INVALID, "ngamma must be <= 46340");
   if (!spins) return fw_fail(S2B_ERR_INVALID, "spins is NULL");
   if ((rc = check_ptrs({delta, quads, f, flmn}))) return rc;
   const FWSlices sl = spin_slices(nspins, spins);
@@ -1484,6 +1486,8 @@ int s2b_fw_so3_to_subset_adjoint(s2b_fw_plan* plan, int batch, int ngamma, int n
   if ((rc = check_plan(plan))) return rc;
   if (batch < 1 || nspins < 1 || ngamma < 1)
     return fw_fail(S2B_ERR_INVALID, "need batch, ngamma, nspins >= 1");
+  if (ngamma > 46340)  // the gamma DFT's phase index c * n mod ngamma stays below 2^31
+    return fw_fail(S2B_ERR_INVALID, "ngamma must be <= 46340");
   if (!spins) return fw_fail(S2B_ERR_INVALID, "spins is NULL");
   if ((rc = check_ptrs({delta, quads, g_flmn, g_f}))) return rc;
   const FWSlices sl = spin_slices(nspins, spins);

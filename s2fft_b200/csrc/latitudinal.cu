@@ -27,19 +27,6 @@ __global__ void lambda_kernel(int L, int spin, int nhalf, const RingInfo* __rest
   }
 }
 
-constexpr int kClassSlots = 64;
-
-int lat_nclass(bool fp64, int L) {
-  (void)fp64;
-  return (L + kClassSlots - 1) / kClassSlots;
-}
-
-int lat_qp(bool fp64, int L) {
-  (void)fp64;
-  (void)L;
-  return kClassSlots;
-}
-
 cudaError_t launch_lambda(bool fp64, int L, int spin, int nhalf, const RingInfo* rings, int nrings,
                           int Ls, void* lam, cudaStream_t s) {
   const long total = (long)nhalf * tab_rows(L) * Ls;

@@ -28,6 +28,9 @@ void* g_noalloc_addr[kMaxDevices] = {};
 
 // Device address of the scratch array on the current device, looked up on
 // the first call for that device (with it current) and cached afterwards.
+// The cache holds for the life of the device's primary context: after a
+// cudaDeviceReset the module is loaded again and the array may move, so a
+// program that resets a device must not call s2b_inverse_noalloc on it again.
 int scratch_address(void** out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
@@ -57,6 +60,8 @@ extern "C" int s2b_inverse_noalloc(s2b_plan* plan, const void* flm, void* f, voi
   size_t need = 0;
   int rc = s2b_workspace_size(plan, 0, &need);
   if (rc != S2B_OK) return rc;
+  // the scratch array used is the current device's, so that device must hold the plan
+  if ((rc = s2b::check_plan_device(plan)) != S2B_OK) return rc;
   if (need > S2B_NOALLOC_SCRATCH_BYTES) {
     char msg[256];
     std::snprintf(msg, sizeof msg,

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -43,6 +44,14 @@ static int fail(int code, const std::string& msg) {
 
 // Lets other translation units of the library report through s2b_last_error().
 int s2b::set_last_error(int code, const char* msg) { return fail(code, msg); }
+
+// Every device allocation of the library goes through here and is counted, so that a
+// caller (or a test) can check that a call allocated nothing.
+static std::atomic<long long> g_dev_allocs{0};
+cudaError_t s2b::dev_malloc_void(void** ptr, size_t bytes) {
+  g_dev_allocs.fetch_add(1, std::memory_order_relaxed);
+  return cudaMalloc(ptr, bytes);
+}
 
 #define S2B_CK(call)                                                                    \
   do {                                                                                  \
@@ -335,6 +344,7 @@ struct DevBuf {
 
 struct s2b_plan {
   s2b_desc d;
+  int device = -1;  // CUDA device the plan was created on (its tables live there)
   bool fp64;
   bool tc;      // S2B_BF16X3: tensor-core precompute contractions
   size_t rsz;   // sizeof(Real)
@@ -429,7 +439,7 @@ static int upload(s2b_plan* p, T** dst, const std::vector<T>& src) {
     return S2B_OK;
   }
   void* ptr = nullptr;
-  S2B_CK(cudaMalloc(&ptr, src.size() * sizeof(T)));
+  S2B_CK(dev_malloc(&ptr, src.size() * sizeof(T)));
   p->allocs.push_back(ptr);
   S2B_CK(cudaMemcpy(ptr, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
   *dst = reinterpret_cast<T*>(ptr);
@@ -478,8 +488,9 @@ static int build_plan(s2b_plan* p) {
   p->npix = d.sampling == S2B_HEALPIX ? 12L * d.nside * d.nside : (long)p->nth * p->nphi;
   p->dual = (d.spin == 0 && !d.reality) ? 1 : 0;
   p->nhalf = (d.spin == 0) ? 1 : 2;
-  p->nclass = lat_nclass(p->fp64, L);
-  p->Q = lat_qp(p->fp64, L);
+  // degree classes of the coefficient tables: l = j + nclass q with q < Q = 64 slots
+  p->Q = 64;
+  p->nclass = (L + p->Q - 1) / p->Q;
   p->TR = tab_rows(L);
 
   // ---- recursion tables: g[m][l], h[j][m][q], lbin[l]
@@ -658,16 +669,16 @@ static int build_plan(s2b_plan* p) {
     if ((rc = upload(p, &p->fwd_weights, w))) return rc;
   }
 
-  S2B_CK(cudaMalloc(&p->status, sizeof(int)));
+  S2B_CK(dev_malloc(&p->status, sizeof(int)));
   p->allocs.push_back(p->status);
   S2B_CK(cudaMemset(p->status, 0, sizeof(int)));
 
   // ---- forward start tables (device kernel, double arithmetic)
   if (p->fwd_nrings > 0) {
     const size_t nst = (size_t)p->nhalf * p->fwd_NB * p->fwd_nrings;
-    S2B_CK(cudaMalloc(&p->fwd_Mst, nst * sizeof(int)));
+    S2B_CK(dev_malloc(&p->fwd_Mst, nst * sizeof(int)));
     p->allocs.push_back(p->fwd_Mst);
-    S2B_CK(cudaMalloc(&p->fwd_Vst, fwd_start_bytes(p->fp64, L, p->nhalf, p->fwd_nrings)));
+    S2B_CK(dev_malloc(&p->fwd_Vst, fwd_start_bytes(p->fp64, L, p->nhalf, p->fwd_nrings)));
     p->allocs.push_back(p->fwd_Vst);
     FwdStartParams fp{};
     fp.L = L;
@@ -690,9 +701,9 @@ static int build_plan(s2b_plan* p) {
   if (p->fwd_sym) {
     const size_t nst = (size_t)p->nhalf * p->fwd_NB * p->sym_npair;
     const size_t vb = fwd_start_bytes(p->fp64, L, p->nhalf, p->sym_npair);
-    S2B_CK(cudaMalloc(&p->sym_Mst, kInvSegMax * nst * sizeof(int)));
+    S2B_CK(dev_malloc(&p->sym_Mst, kInvSegMax * nst * sizeof(int)));
     p->allocs.push_back(p->sym_Mst);
-    S2B_CK(cudaMalloc(&p->sym_Vst, kInvSegMax * vb));
+    S2B_CK(dev_malloc(&p->sym_Vst, kInvSegMax * vb));
     p->allocs.push_back(p->sym_Vst);
     p->sym_Mst1 = p->sym_Mst + nst;
     p->sym_Vst1 = static_cast<char*>(p->sym_Vst) + vb;
@@ -722,13 +733,13 @@ static int build_plan(s2b_plan* p) {
   // ---- start tables of the inverse rings (inverse kernel and adjoint of the inverse)
   if (p->inv_nrings > 0) {
     const size_t nst = (size_t)p->nhalf * p->fwd_NB * p->inv_nrings;
-    S2B_CK(cudaMalloc(&p->inv_Mst, nst * sizeof(int)));
+    S2B_CK(dev_malloc(&p->inv_Mst, nst * sizeof(int)));
     p->allocs.push_back(p->inv_Mst);
-    S2B_CK(cudaMalloc(&p->inv_Vst, fwd_start_bytes(p->fp64, L, p->nhalf, p->inv_nrings)));
+    S2B_CK(dev_malloc(&p->inv_Vst, fwd_start_bytes(p->fp64, L, p->nhalf, p->inv_nrings)));
     p->allocs.push_back(p->inv_Vst);
-    S2B_CK(cudaMalloc(&p->inv_Mst1, (kInvSegMax - 1) * nst * sizeof(int)));
+    S2B_CK(dev_malloc(&p->inv_Mst1, (kInvSegMax - 1) * nst * sizeof(int)));
     p->allocs.push_back(p->inv_Mst1);
-    S2B_CK(cudaMalloc(&p->inv_Vst1, (kInvSegMax - 1) *
+    S2B_CK(dev_malloc(&p->inv_Vst1, (kInvSegMax - 1) *
                                         fwd_start_bytes(p->fp64, L, p->nhalf, p->inv_nrings)));
     p->allocs.push_back(p->inv_Vst1);
     // launch shape of the inverse kernel, measured at L = 256 ... 2048 (MW, float and
@@ -764,9 +775,9 @@ static int build_plan(s2b_plan* p) {
     p->fwd_Ls = round4(p->fwd_nrings);
     const size_t bi = (size_t)p->nhalf * p->TR * p->inv_Ls * p->rsz;
     const size_t bf = (size_t)p->nhalf * p->TR * p->fwd_Ls * p->rsz;
-    S2B_CK(cudaMalloc(&p->inv_lam, bi));
+    S2B_CK(dev_malloc(&p->inv_lam, bi));
     p->allocs.push_back(p->inv_lam);
-    S2B_CK(cudaMalloc(&p->fwd_lam, bf));
+    S2B_CK(dev_malloc(&p->fwd_lam, bf));
     p->allocs.push_back(p->fwd_lam);
     if (p->inv_nrings > 0)
       S2B_CK(launch_lambda(p->fp64, L, d.spin, p->nhalf, p->inv_rings, p->inv_nrings, p->inv_Ls,
@@ -923,6 +934,21 @@ static FFTTables<Real> tables(const s2b_plan* p) {
   t.bfilt = reinterpret_cast<const typename FFTTables<Real>::R2*>(p->bf);
   return t;
 }
+
+// Execute calls launch on the current device; the plan's tables live on the device it was
+// created on, so the two must agree (a plan used from another device would hand one GPU's
+// pointers to another's kernels).
+static int check_device(const s2b_plan* p) {
+  int dev = -1;
+  S2B_CK(cudaGetDevice(&dev));
+  if (dev != p->device)
+    return fail(S2B_ERR_INVALID, "the current device (" + std::to_string(dev) +
+                                     ") is not the plan's device (" + std::to_string(p->device) +
+                                     "): make the plan's device current before the call");
+  return S2B_OK;
+}
+
+int s2b::check_plan_device(const s2b_plan* p) { return check_device(p); }
 
 static int check_ptr(const void* ptr, const char* what) {
   if (!ptr) return fail(S2B_ERR_ALIGN, std::string(what) + " is NULL");
@@ -1484,7 +1510,7 @@ static int build_kernel(s2b_plan* p, bool forward, void* K, cudaStream_t s) {
     // (rows l and k = theta for the forward, rows theta and k = l for the inverse)
     const size_t tb = (size_t)kp.nth * d.L * p->kM * sizeof(float) * (kp.complex_out ? 2 : 1);
     void* tmp = nullptr;
-    S2B_CK(cudaMalloc(&tmp, tb));
+    S2B_CK(dev_malloc(&tmp, tb));
     kp.out = tmp;
     cudaError_t e = launch_kernel_table(false, kp, s);
     if (e == cudaSuccess)
@@ -1842,29 +1868,35 @@ static int run_wigner(s2b_plan* p, bool forward, const void* in, void* out, char
     S2B_CK(cudaEventRecord(p->wfork, s));
     for (int k = 0; k < K; ++k) S2B_CK(cudaStreamWaitEvent(p->wstream[k], p->wfork, 0));
   }
-  for (int n = n0; n < d.N; ++n) {
+  rc = S2B_OK;
+  for (int n = n0; n < d.N && !rc; ++n) {
     const int k = (n - n0) % K;
     cudaStream_t sk = K > 1 ? p->wstream[k] : s;
     char* tmp = fban + align256(p->ws_w_fban) + (size_t)k * wigner_slot(p);
     char* subws = tmp + align256(p->ws_w_tmp);
     s2b_plan* sub = p->subs[n - n0];
     char* band = fban + (size_t)(d.N - 1 + n) * slice;
+    cudaError_t e = cudaSuccess;
     if (!forward) {
-      S2B_CK(launch_gather_n(p->fp64, in, tmp, d.batch, d.N, d.L, n, sk));
-      rc = exec_call(sub, 0, tmp, band, subws, sk);
-      if (rc) return rc;
+      e = launch_gather_n(p->fp64, in, tmp, d.batch, d.N, d.L, n, sk);
+      if (e == cudaSuccess) rc = exec_call(sub, 0, tmp, band, subws, sk);
     } else {
       rc = exec_call(sub, 1, band, tmp, subws, sk);
-      if (rc) return rc;
-      S2B_CK(launch_scatter_n(p->fp64, tmp, out, d.batch, d.N, d.L, n, d.L_lower, sk));
+      if (!rc) e = launch_scatter_n(p->fp64, tmp, out, d.batch, d.N, d.L, n, d.L_lower, sk);
     }
+    if (e != cudaSuccess) rc = fail(S2B_ERR_CUDA, std::string("Wigner gather/scatter: ") + cudaGetErrorString(e));
   }
   if (K > 1) {
+    // join every forked stream back to the caller's stream, after an error too, so that no
+    // work queued on them outlives the call (it uses the caller's workspace) and a stream
+    // capture of the caller's stream stays complete
     for (int k = 0; k < K; ++k) {
-      S2B_CK(cudaEventRecord(p->wjoin[k], p->wstream[k]));
-      S2B_CK(cudaStreamWaitEvent(s, p->wjoin[k], 0));
+      cudaError_t e = cudaEventRecord(p->wjoin[k], p->wstream[k]);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(s, p->wjoin[k], 0);
+      if (e != cudaSuccess && !rc) rc = fail(S2B_ERR_CUDA, std::string("Wigner join: ") + cudaGetErrorString(e));
     }
   }
+  if (rc) return rc;
   if (!forward) {
     S2B_CK(launch_gamma_inverse(p->fp64, fban, out, d.batch, d.N, p->npix, d.reality, s));
   } else if (d.reality) {
@@ -1880,7 +1912,7 @@ static int upload_to(std::vector<void*>* allocs, T** dst, const std::vector<T>& 
   *dst = nullptr;
   if (src.empty()) return S2B_OK;
   void* ptr = nullptr;
-  S2B_CK(cudaMalloc(&ptr, src.size() * sizeof(T)));
+  S2B_CK(dev_malloc(&ptr, src.size() * sizeof(T)));
   allocs->push_back(ptr);
   S2B_CK(cudaMemcpy(ptr, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
   *dst = reinterpret_cast<T*>(ptr);
@@ -1955,8 +1987,12 @@ int s2b_plan_create(const s2b_desc* desc, s2b_plan** out) {
   if (d.L > 8192) return fail(S2B_ERR_INVALID, "L > 8192 not supported");
   if (d.N < 0 || d.N > d.L) return fail(S2B_ERR_INVALID, "0 <= N <= L required");
   if (d.N > 0 && d.iter != 0) return fail(S2B_ERR_INVALID, "iter is not used by Wigner plans");
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fail(S2B_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
   s2b_plan* p = new s2b_plan();
   p->d = d;
+  p->device = dev;
   int rc = d.N > 0 ? build_wigner(p) : build_plan(p);
   if (rc) {
     s2b_plan_destroy(p);
@@ -1992,6 +2028,7 @@ int s2b_workspace_size(const s2b_plan* p, int forward, size_t* bytes) {
 int s2b_inverse(s2b_plan* p, const void* flm, void* f, void* ws, size_t ws_bytes, void* stream) {
   if (!p || p->d.N > 0) return fail(S2B_ERR_INVALID, "plan is NULL or a Wigner plan");
   int rc;
+  if ((rc = check_device(p))) return rc;
   if ((rc = check_ptr(flm, "flm")) || (rc = check_ptr(f, "f")) || (rc = check_ptr(ws, "workspace")))
     return rc;
   if (ws_bytes < ws_of(p, 0)) return fail(S2B_ERR_WORKSPACE, "workspace too small");
@@ -2001,6 +2038,7 @@ int s2b_inverse(s2b_plan* p, const void* flm, void* f, void* ws, size_t ws_bytes
 int s2b_forward(s2b_plan* p, const void* f, void* flm, void* ws, size_t ws_bytes, void* stream) {
   if (!p || p->d.N > 0) return fail(S2B_ERR_INVALID, "plan is NULL or a Wigner plan");
   int rc;
+  if ((rc = check_device(p))) return rc;
   if ((rc = check_ptr(flm, "flm")) || (rc = check_ptr(f, "f")) || (rc = check_ptr(ws, "workspace")))
     return rc;
   if (ws_bytes < ws_of(p, 1)) return fail(S2B_ERR_WORKSPACE, "workspace too small");
@@ -2012,6 +2050,7 @@ int s2b_inverse_adjoint(s2b_plan* p, const void* g_f, void* g_flm, void* ws, siz
   if (!p || p->d.N > 0) return fail(S2B_ERR_INVALID, "plan is NULL or a Wigner plan");
   if (p->d.reality) return fail(S2B_ERR_INVALID, "adjoints are defined for complex plans (reality = 0)");
   int rc;
+  if ((rc = check_device(p))) return rc;
   if ((rc = check_ptr(g_f, "g_f")) || (rc = check_ptr(g_flm, "g_flm")) ||
       (rc = check_ptr(ws, "workspace")))
     return rc;
@@ -2024,6 +2063,7 @@ int s2b_forward_adjoint(s2b_plan* p, const void* g_flm, void* g_f, void* ws, siz
   if (!p || p->d.N > 0) return fail(S2B_ERR_INVALID, "plan is NULL or a Wigner plan");
   if (p->d.reality) return fail(S2B_ERR_INVALID, "adjoints are defined for complex plans (reality = 0)");
   int rc;
+  if ((rc = check_device(p))) return rc;
   if ((rc = check_ptr(g_flm, "g_flm")) || (rc = check_ptr(g_f, "g_f")) ||
       (rc = check_ptr(ws, "workspace")))
     return rc;
@@ -2035,6 +2075,7 @@ int s2b_healpix_fft(s2b_plan* p, const void* f, void* ftm, void* stream) {
   if (!p || p->d.N > 0 || p->d.sampling != S2B_HEALPIX)
     return fail(S2B_ERR_INVALID, "plan must be a HEALPix spin plan");
   int rc;
+  if ((rc = check_device(p))) return rc;
   if ((rc = check_ptr(f, "f")) || (rc = check_ptr(ftm, "ftm"))) return rc;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   return p->fp64 ? run_healpix_fft<double>(p, f, ftm, s) : run_healpix_fft<float>(p, f, ftm, s);
@@ -2044,6 +2085,7 @@ int s2b_healpix_ifft(s2b_plan* p, const void* ftm, void* f, void* stream) {
   if (!p || p->d.N > 0 || p->d.sampling != S2B_HEALPIX)
     return fail(S2B_ERR_INVALID, "plan must be a HEALPix spin plan");
   int rc;
+  if ((rc = check_device(p))) return rc;
   if ((rc = check_ptr(f, "f")) || (rc = check_ptr(ftm, "ftm"))) return rc;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   return p->fp64 ? run_healpix_ifft<double>(p, ftm, f, s) : run_healpix_ifft<float>(p, ftm, f, s);
@@ -2058,6 +2100,7 @@ int s2b_kernel_size(const s2b_plan* p, int forward, size_t* bytes) {
 int s2b_kernel_build(s2b_plan* p, int forward, void* K, void* stream) {
   if (!p || p->d.N > 0) return fail(S2B_ERR_INVALID, "bad plan");
   int rc;
+  if ((rc = check_device(p))) return rc;
   if ((rc = check_ptr(K, "kernel"))) return rc;
   return build_kernel(p, forward != 0, K, reinterpret_cast<cudaStream_t>(stream));
 }
@@ -2066,6 +2109,7 @@ int s2b_precompute_inverse(s2b_plan* p, const void* K, const void* flm, void* f,
                            size_t ws_bytes, void* stream) {
   if (!p || p->d.N > 0) return fail(S2B_ERR_INVALID, "bad plan");
   int rc;
+  if ((rc = check_device(p))) return rc;
   if ((rc = check_ptr(K, "kernel")) || (rc = check_ptr(flm, "flm")) || (rc = check_ptr(f, "f")) ||
       (rc = check_ptr(ws, "workspace")))
     return rc;
@@ -2079,6 +2123,7 @@ int s2b_precompute_forward(s2b_plan* p, const void* K, const void* f, void* flm,
                            size_t ws_bytes, void* stream) {
   if (!p || p->d.N > 0) return fail(S2B_ERR_INVALID, "bad plan");
   int rc;
+  if ((rc = check_device(p))) return rc;
   if ((rc = check_ptr(K, "kernel")) || (rc = check_ptr(flm, "flm")) || (rc = check_ptr(f, "f")) ||
       (rc = check_ptr(ws, "workspace")))
     return rc;
@@ -2092,7 +2137,7 @@ static int check_pre_adjoint(const s2b_plan* p) {
   if (!p || p->d.N > 0) return fail(S2B_ERR_INVALID, "bad plan");
   if (p->d.reality) return fail(S2B_ERR_INVALID, "adjoints are defined for complex plans (reality = 0)");
   if (p->tc) return fail(S2B_ERR_INVALID, "adjoints need a float or double kernel table (not BF16x3)");
-  return S2B_OK;
+  return check_device(p);
 }
 
 int s2b_precompute_inverse_adjoint(s2b_plan* p, const void* K, const void* g_f, void* g_flm,
@@ -2125,6 +2170,7 @@ int s2b_wigner_inverse(s2b_plan* p, const void* flmn, void* f, void* ws, size_t 
                        void* stream) {
   if (!p || p->d.N < 1) return fail(S2B_ERR_INVALID, "plan is not a Wigner plan (desc.N > 0)");
   int rc;
+  if ((rc = check_device(p))) return rc;
   if ((rc = check_ptr(flmn, "flmn")) || (rc = check_ptr(f, "f")) || (rc = check_ptr(ws, "workspace")))
     return rc;
   if (ws_bytes < wigner_ws(p)) return fail(S2B_ERR_WORKSPACE, "workspace too small");
@@ -2135,6 +2181,7 @@ int s2b_wigner_forward(s2b_plan* p, const void* f, void* flmn, void* ws, size_t 
                        void* stream) {
   if (!p || p->d.N < 1) return fail(S2B_ERR_INVALID, "plan is not a Wigner plan (desc.N > 0)");
   int rc;
+  if ((rc = check_device(p))) return rc;
   if ((rc = check_ptr(flmn, "flmn")) || (rc = check_ptr(f, "f")) || (rc = check_ptr(ws, "workspace")))
     return rc;
   if (ws_bytes < wigner_ws(p)) return fail(S2B_ERR_WORKSPACE, "workspace too small");
@@ -2177,6 +2224,21 @@ int s2b_plan_set_tuning(s2b_plan* p, int key, int value) {
   else
     p->fwd_nseg = value;
   for (s2b_plan* sp : p->subs) s2b_plan_set_tuning(sp, key, value);
+  return S2B_OK;
+}
+
+long long s2b_device_alloc_count(void) { return g_dev_allocs.load(std::memory_order_relaxed); }
+
+int s2b_plan_device(const s2b_plan* p, int* device) {
+  if (!p || !device) return fail(S2B_ERR_INVALID, "plan and device must be non-NULL");
+  *device = p->device;
+  return S2B_OK;
+}
+
+int s2b_debug_set_plan_device(s2b_plan* p, int device) {
+  if (!p) return fail(S2B_ERR_INVALID, "plan must be non-NULL");
+  p->device = device;
+  for (s2b_plan* sp : p->subs) s2b_debug_set_plan_device(sp, device);
   return S2B_OK;
 }
 

@@ -9,6 +9,8 @@
 
 #include "s2b_fft.h"
 
+struct s2b_plan;
+
 namespace s2b {
 
 // Coefficient tables indexed by m are stored with kPadLo zero rows on both
@@ -26,10 +28,8 @@ struct RingInfo {
   double ls;   // log2 sin(theta/2)
 };
 
-int lat_nclass(bool fp64, int L);
 cudaError_t launch_lambda(bool fp64, int L, int spin, int nhalf, const RingInfo* rings, int nrings,
                           int Ls, void* lam, cudaStream_t s);
-int lat_qp(bool fp64, int L);
 
 // FFT descriptors (host copies, in the order of the requested lengths; their table
 // offsets index tw / chirp / bf) and the device tables they refer to.
@@ -46,5 +46,16 @@ int build_fft_set(const int* lengths, int count, bool fp64, std::vector<void*>* 
 
 // Records msg as the calling thread's s2b_last_error() text and returns code.
 int set_last_error(int code, const char* msg);
+
+// S2B_OK when the current device is the one the plan was created on, else an
+// S2B_ERR_INVALID status with the message set.
+int check_plan_device(const s2b_plan* p);
+
+// cudaMalloc through the library's allocation counter (s2b_device_alloc_count).
+cudaError_t dev_malloc_void(void** ptr, size_t bytes);
+template <typename T>
+cudaError_t dev_malloc(T** ptr, size_t bytes) {
+  return dev_malloc_void(reinterpret_cast<void**>(ptr), bytes);
+}
 
 }  // namespace s2b

@@ -14,6 +14,20 @@ from unittest import mock
 import numpy as np
 
 
+def upstream_root(argv) -> str:
+    """The upstream s2fft source tree: the first command-line argument, else the
+    ``S2FFT_UPSTREAM`` environment variable. There is no default location."""
+    import os
+
+    root = argv[1] if len(argv) > 1 else os.environ.get("S2FFT_UPSTREAM")
+    if not root:
+        raise SystemExit("give the upstream s2fft source tree as the first argument "
+                         "or in S2FFT_UPSTREAM")
+    if not os.path.isdir(os.path.join(root, "s2fft")):
+        raise SystemExit(f"{root} does not hold the upstream s2fft package")
+    return root
+
+
 def install(ref_root: str) -> None:
     if "s2fft" in sys.modules:
         return

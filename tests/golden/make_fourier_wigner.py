@@ -11,7 +11,7 @@ Imports upstream s2fft through ``_refstub`` (JAX is absent) and runs, unmodified
 
 Inputs come from upstream's own ``signal_generator.generate_flmn``. Writes
 ``fourier_wigner.npz`` and ``fourier_wigner.json``. Run from the repository root:
-``python tests/golden/make_fourier_wigner.py [upstream_root]``.
+``python tests/golden/make_fourier_wigner.py upstream_root``.
 """
 
 import json
@@ -90,4 +90,7 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    import _refstub
+
+    main(_refstub.upstream_root(sys.argv))

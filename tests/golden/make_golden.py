@@ -1,7 +1,7 @@
 """Generate golden input/output vectors from the upstream s2fft numpy code.
 
-Run in a container where the upstream source tree is mounted (default
-``/root/reference``); the fixtures it writes (``tests/golden/*.npz``) travel
+Run in a container where the upstream source tree is mounted (its path is the
+first argument, or ``S2FFT_UPSTREAM``); the fixtures it writes (``tests/golden/*.npz``) travel
 with the repository, the upstream tree does not. JAX is absent there, so the
 upstream package is imported through ``_refstub`` and only its numpy paths run:
 
@@ -14,7 +14,7 @@ upstream package is imported through ``_refstub`` and only its numpy paths run:
 * the signal generator itself (``generate_flm`` / ``generate_flmn``), so the
   seeded inputs are pinned too.
 
-Usage: ``python tests/golden/make_golden.py [upstream_root]``.
+Usage: ``python tests/golden/make_golden.py upstream_root``.
 """
 
 import json
@@ -132,4 +132,7 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    import _refstub
+
+    main(_refstub.upstream_root(sys.argv))

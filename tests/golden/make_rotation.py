@@ -5,7 +5,7 @@ here; its planes come from s2fft/recursions/risbo.py (numpy only), which this sc
 imports directly from the upstream tree and steps degree by degree exactly as
 rotate_flms does. The contraction is upstream's einsum written out in numpy.
 Writes ``rotation.npz``. Run from the repository root:
-``python tests/golden/make_rotation.py [upstream_root]``.
+``python tests/golden/make_rotation.py upstream_root``.
 """
 
 import importlib.util
@@ -51,4 +51,7 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    import _refstub
+
+    main(_refstub.upstream_root(sys.argv))

@@ -77,10 +77,12 @@ def test_noalloc_matches_workspace_inverse(cabi, rng, L, spin, sampling, precisi
 
     outs = [torch.full(shape, float("nan"), dtype=cdt, device="cuda") for _ in flms]
     allocated = torch.cuda.memory_allocated()
+    lib_allocs = lib.s2b_device_alloc_count()  # every cudaMalloc the library makes
     for x, out in zip(flms, outs):  # two calls in a row, sharing the scratch array
         _lib.check(lib.s2b_inverse_noalloc(plan.ptr, x.data_ptr(), out.data_ptr(), stream))
     torch.cuda.synchronize()
     assert torch.cuda.memory_allocated() == allocated
+    assert lib.s2b_device_alloc_count() == lib_allocs
     for out, ref in zip(outs, refs):
         err = relerr(out.cpu().numpy(), ref.cpu().numpy())
         assert err < TOL[precision], err
