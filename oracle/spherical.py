@@ -10,12 +10,21 @@ import numpy as np
 from . import healpix, quadrature, recursion, resampling, samples
 
 
+def _steps(backend):
+    """The latitudinal steps: the numpy restatement, or its C port (oracle/csrc/otf.c)."""
+    if backend == "c":
+        from . import cport
+
+        return cport
+    return recursion
+
+
 def _norm(L, L0):
     return np.sqrt((2 * np.arange(L0, L) + 1) / (4 * np.pi))
 
 
 def inverse(flm, L, spin=0, nside=None, sampling="mw", reality=False, precomps=None,
-            L_lower=0, max_steps=None):
+            L_lower=0, max_steps=None, backend="numpy"):
     """spherical.py:112-208."""
     sampling = sampling.lower()
     th = samples.thetas(L, sampling, nside)
@@ -23,7 +32,7 @@ def inverse(flm, L, spin=0, nside=None, sampling="mw", reality=False, precomps=N
     m0 = L - 1 if reality else 0
     flm = np.array(flm, dtype=np.complex128, copy=True)
     flm[L_lower:] *= _norm(L, L_lower)[:, None]
-    ftm = recursion.inverse_latitudinal_step(
+    ftm = _steps(backend).inverse_latitudinal_step(
         flm, th, L, spin, sampling, reality, precomps, L_lower, max_steps, nside)
     # pole rows carry only m = +-spin (176-184)
     if sampling in ("mw", "mwss"):
@@ -47,7 +56,7 @@ def inverse(flm, L, spin=0, nside=None, sampling="mw", reality=False, precomps=N
 
 
 def _forward_once(f, L, spin=0, nside=None, sampling="mw", reality=False, precomps=None,
-                  L_lower=0, max_steps=None):
+                  L_lower=0, max_steps=None, backend="numpy"):
     """spherical.py:467-588."""
     sampling = sampling.lower()
     if sampling == "mw":
@@ -75,13 +84,13 @@ def _forward_once(f, L, spin=0, nside=None, sampling="mw", reality=False, precom
     if sampling == "healpix":
         ftm[:, m0 + mo:] *= healpix.ring_phase_shifts_hp(L, nside, True, reality)
     if sampling == "mwss":
-        flm = recursion.forward_latitudinal_step(
+        flm = _steps(backend).forward_latitudinal_step(
             ftm[1:-1], th[1:-1], L, spin, sampling, reality, precomps, L_lower, max_steps)
         flm[L_lower:, L - 1 + spin] += (-1.0) ** np.abs(np.arange(L_lower, L) - spin) * \
             ftm[-1, L - 1 + spin + mo]
         flm[L_lower:, L - 1 - spin] += ftm[0, L - 1 - spin + mo]
     else:
-        flm = recursion.forward_latitudinal_step(
+        flm = _steps(backend).forward_latitudinal_step(
             ftm, th, L, spin, sampling, reality, precomps, L_lower, max_steps)
     flm[L_lower:] *= _norm(L, L_lower)[:, None]
     if reality:
@@ -92,14 +101,15 @@ def _forward_once(f, L, spin=0, nside=None, sampling="mw", reality=False, precom
 
 
 def forward(f, L, spin=0, nside=None, sampling="mw", reality=False, precomps=None,
-            L_lower=0, iter=0, max_steps=None):
+            L_lower=0, iter=0, max_steps=None, backend="numpy"):
     """forward + Jacobi refinement: flm = F(f); repeat: flm += F(f - I(flm)).
 
     spherical.py:425-464 and iterative_refinement.py:9-46.
     """
     kw = dict(L=L, spin=spin, nside=nside, sampling=sampling, reality=reality, L_lower=L_lower)
-    flm = _forward_once(f, precomps=precomps, max_steps=max_steps, **kw)
+    flm = _forward_once(f, precomps=precomps, max_steps=max_steps, backend=backend, **kw)
     for _ in range(iter or 0):
-        err = f - inverse(flm, max_steps=max_steps, **kw)
-        flm = flm + _forward_once(err, precomps=precomps, max_steps=max_steps, **kw)
+        err = f - inverse(flm, max_steps=max_steps, backend=backend, **kw)
+        flm = flm + _forward_once(err, precomps=precomps, max_steps=max_steps, backend=backend,
+                                  **kw)
     return flm
