@@ -399,6 +399,10 @@ struct s2b_plan {
   int* adj_col = nullptr;
   int adj_Gs = 4, adj_pole_s = -1, adj_pole_n = -1;
   void* col_ph_adj = nullptr;
+  // MW column chain: correction for the south-pole ring's odd (m + s) content (see
+  // mw_pole_correction); MWSS real maps: theta-Nyquist bin split between -L and +L
+  void* col_pole = nullptr;
+  int col_nyq_split = 0;
   size_t ws_adj_G = 0, ws_adj_y = 0;
   // precompute path: ring colatitudes of the kernel tables, table width
   double* kth_inv = nullptr;
@@ -475,6 +479,53 @@ static RingInfo ring_info(double th) {
   r.lc = std::log2(std::cos(th / 2.0));
   r.ls = std::log2(std::sin(th / 2.0));
   return r;
+}
+
+// Upstream resamples MW maps through MWSS at L (s2fft/utils/resampling.py:284-355) and
+// then rebuilds the full theta circle from those L+1 rings by the spin symmetry before the
+// x2 upsampling (resampling.py:64-160). For a band-limited map that detour is exact and the
+// device's direct chain (DFT over the 2L-1 extended samples, half-sample phase, zero-pad to
+// 4L, inverse DFT) gives the same values. The one difference is the MW ring at theta = pi:
+// it is its own mirror, so for phi-frequencies with odd m + s a map that is not band-limited
+// has a part there that the rebuilt circle turns into its antisymmetric image. That part is
+// one sample per column, so upstream's chain equals the direct chain plus x_pole * c, with
+// c = (upstream chain - direct chain)(unit impulse at the pole), here for k = 0..2L on the
+// MWSS(2L) rings, in the units of the device's inverse-DFT output (before the phi factor
+// and the weights). For real maps upstream takes the real part after the upsampling, which
+// turns c into Re(c) (the impulse is real and the direct chain's image of it is real).
+static std::vector<cd> mw_pole_correction(int L) {
+  const int n1 = 2 * L - 1, n2 = 2 * L, n4 = 4 * L;
+  std::vector<cd> w2(n2), w4(n4);  // roots of unity exp(2 pi i j / n)
+  for (int j = 0; j < n2; ++j) w2[j] = std::polar(1.0, 2.0 * kPi * j / n2);
+  for (int j = 0; j < n4; ++j) w4[j] = std::polar(1.0, 2.0 * kPi * j / n4);
+  auto r2 = [&](long e) { return w2[((e % n2) + n2) % n2]; };
+  auto r4 = [&](long e) { return w4[((e % n4) + n4) % n4]; };
+  // theta bins p = -(L-1)..L-1 of the impulse at t = L-1 after the half-sample phase:
+  // exp(-2 pi i p (L-1) / n1) exp(-i pi p / n1) / n1 = (-1)^p / n1
+  auto G = [&](int p) { return ((p & 1) ? -1.0 : 1.0) / (double)n1; };
+  // upstream: unnormalised inverse DFT over 2L (MWSS rings j = 0..L), the circle rebuilt
+  // with the odd-column sign -1, DFT over 2L divided by 2L, zero-pad (bin -L kept at -L),
+  // unnormalised inverse DFT over 4L
+  std::vector<cd> g(L + 1);
+  for (int j = 0; j <= L; ++j) {
+    cd v(0.0, 0.0);
+    for (int p = -(L - 1); p <= L - 1; ++p) v += G(p) * r2((long)p * j);
+    g[j] = v;
+  }
+  std::vector<cd> H(n2);  // bin q = -L..L-1 at index q + L
+  for (int q = -L; q < L; ++q) {
+    cd v(0.0, 0.0);
+    for (int j = 0; j < n2; ++j) v += (j <= L ? g[j] : -g[n2 - j]) * r2(-(long)q * j);
+    H[q + L] = v / (double)n2;
+  }
+  std::vector<cd> c(2 * L + 1);
+  for (int k = 0; k <= 2 * L; ++k) {
+    cd u(0.0, 0.0), direct(0.0, 0.0);
+    for (int q = -L; q < L; ++q) u += H[q + L] * r4((long)q * k);
+    for (int p = -(L - 1); p <= L - 1; ++p) direct += G(p) * r4((long)p * k);
+    c[k] = u - direct;
+  }
+  return c;
 }
 
 static int build_plan(s2b_plan* p) {
@@ -849,6 +900,13 @@ static int build_plan(s2b_plan* p) {
       pa[(pp + n2) % n2] = f;
     }
     if ((rc = upload_complex(p, &p->col_ph_adj, pa))) return rc;
+    if (p->fwd_mode == 1) {
+      std::vector<cd> c = mw_pole_correction(L);
+      if (d.reality)
+        for (cd& v : c) v = cd(v.real(), 0.0);
+      if ((rc = upload_complex(p, &p->col_pole, c))) return rc;
+    }
+    p->col_nyq_split = (p->fwd_mode == 2 && d.reality) ? 1 : 0;
   }
   const size_t maxsmem = (size_t)227 * 1024;
   auto padded = [](int M) { return (size_t)M + (size_t)(M >> 3); };  // ring FFT buffer layout
@@ -1288,6 +1346,7 @@ static int run_forward_adjoint(s2b_plan* p, const void* gflm, void* gf, char* ws
   cp.d2 = p->descs + p->col_d2;
   cp.weights = p->fwd_weights;
   cp.ph_adj = p->col_ph_adj;
+  cp.pole = p->col_pole;
   cp.tb = tables<Real>(p);
   cp.in = y;
   cp.out = ftm2;
@@ -1376,7 +1435,10 @@ static int run_forward_once(s2b_plan* p, const void* f, void* flm, char* ws, cud
     cp.scale = p->fwd_mode == 1 ? (2.0 * L) / (2.0 * L - 1.0) : 1.0;
     cp.d1 = p->descs + p->col_d1;
     cp.d2 = p->descs + p->col_d2;
+    cp.d2_pow2 = p->M2 == 4 * L;
     cp.ph = p->col_ph;
+    cp.pole = p->col_pole;
+    cp.nyq_split = p->col_nyq_split;
     cp.weights = p->fwd_weights;
     cp.tb = tables<Real>(p);
     cp.in = cols;
@@ -1634,7 +1696,10 @@ static int run_pre_forward(s2b_plan* p, const void* K, const void* f, void* flm,
     cp.scale = p->fwd_mode == 1 ? (2.0 * L) / (2.0 * L - 1.0) : 1.0;
     cp.d1 = p->descs + p->col_d1;
     cp.d2 = p->descs + p->col_d2;
+    cp.d2_pow2 = p->M2 == 4 * L;
     cp.ph = p->col_ph;
+    cp.pole = p->col_pole;
+    cp.nyq_split = p->col_nyq_split;
     cp.weights = p->fwd_weights;
     cp.tb = tables<Real>(p);
     cp.in = cols;
@@ -1771,6 +1836,7 @@ static int run_pre_forward_adjoint(s2b_plan* p, const void* K, const void* gflm,
     cc.d1 = p->descs + p->col_d1;
     cc.d2 = p->descs + p->col_d2;
     cc.ph_adj = p->col_ph_adj;
+    cc.pole = p->col_pole;
     cc.tb = tables<Real>(p);
     cc.in = raw;
     cc.out = cols;
@@ -1815,6 +1881,20 @@ static int exec_call(s2b_plan* p, int kind, const void* in, void* out, char* ws,
   }
 }
 
+// Column chain of a complex plan that transforms real maps (forward direction only):
+// Re(c) for the MW pole correction and the split theta-Nyquist bin for MWSS, as a reality
+// plan has them.
+static int use_real_map_chain(s2b_plan* p) {
+  if (p->fwd_mode == 1) {
+    std::vector<cd> c = mw_pole_correction(p->d.L);
+    for (cd& v : c) v = cd(v.real(), 0.0);
+    int rc;
+    if ((rc = upload_complex(p, &p->col_pole, c))) return rc;
+  }
+  p->col_nyq_split = p->fwd_mode == 2 ? 1 : 0;
+  return S2B_OK;
+}
+
 static int build_wigner(s2b_plan* p) {
   const s2b_desc& d = p->d;
   p->fp64 = d.precision == S2B_F64;
@@ -1830,9 +1910,12 @@ static int build_wigner(s2b_plan* p) {
     sd.N = 0;
     sd.iter = 0;
     s2b_plan* sub = nullptr;
-    const int rc = s2b_plan_create(&sd, &sub);
+    int rc = s2b_plan_create(&sd, &sub);
     if (rc) return rc;
     p->subs.push_back(sub);
+    // the slice n = 0 of a real signal is a real map: upstream transforms it as one
+    // (wigner.py:521-530), so its MW / MWSS column chain takes the real-map corrections
+    if (d.reality && n == 0 && (rc = use_real_map_chain(sub))) return rc;
     p->ws_w_sub = std::max(p->ws_w_sub, std::max(ws_of(sub, 0), ws_of(sub, 1)));
   }
   const size_t c2 = 2 * p->rsz;
@@ -1878,7 +1961,7 @@ static int run_wigner(s2b_plan* p, bool forward, const void* in, void* out, char
     char* band = fban + (size_t)(d.N - 1 + n) * slice;
     cudaError_t e = cudaSuccess;
     if (!forward) {
-      e = launch_gather_n(p->fp64, in, tmp, d.batch, d.N, d.L, n, sk);
+      e = launch_gather_n(p->fp64, in, tmp, d.batch, d.N, d.L, n, d.reality && n == 0, sk);
       if (e == cudaSuccess) rc = exec_call(sub, 0, tmp, band, subws, sk);
     } else {
       rc = exec_call(sub, 1, band, tmp, subws, sk);

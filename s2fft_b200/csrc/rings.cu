@@ -24,15 +24,75 @@
 #include "s2b_fft.h"
 #include "s2b_internal.h"
 #include "s2b_fft_dev.h"
+#include "s2b_fft_reg.h"
 
 namespace s2b {
+
+// Any-length DFT of one CTA on the register engine (M = 2^LOGM, blockDim.x = M / 16; d.M
+// must be M): inputs load(k), k < d.n; every output X_k (k < d.n, conjugated when inv,
+// times the Bluestein output chirp unless chirp_out is false) goes to emit(k, X_k) once,
+// from the thread that holds it (natural order k = j + T a for Bluestein lengths, the
+// bit-reversed positions of a power-of-two length). buf: RegFFT<LOGM, NBUF>::SMEM_ELEMS
+// elements. With sync_emit a barrier precedes the emits, so that emit may write buf.
+template <typename Real, int LOGM, int NBUF, typename Load, typename Emit>
+__device__ __forceinline__ void reg_dft(typename C2<Real>::t* buf, const FFTDesc& d,
+                                        const FFTTables<Real>& tb, bool inv, bool chirp_out,
+                                        bool sync_emit, Load load, Emit emit) {
+  using R2 = typename C2<Real>::t;
+  using RF = RegFFT<LOGM, NBUF>;
+  const int j = threadIdx.x;
+  const R2* tw = tb.tw + d.tw_off;
+  int ping = 0;
+  R2 x[16];
+  if (d.bluestein) {
+    const R2* __restrict__ ch = tb.chirp + d.chirp_off;
+    const R2* __restrict__ bf = tb.bfilt + d.bf_off;
+#pragma unroll
+    for (int a = 0; a < 16; ++a) {
+      const int k = j + RF::T * a;
+      R2 v = czero<R2>();
+      if (k < d.n) {
+        v = load(k);
+        if (inv) v = cconj(v);
+        v = cmul(v, ch[k]);
+      }
+      x[a] = v;
+    }
+    RF::dif(x, buf, tw, false, ping);
+#pragma unroll
+    for (int a = 0; a < 16; ++a) x[a] = cmul(x[a], bf[RF::point(j, a, 0)]);
+    RF::dit(x, buf, tw, true, ping);
+    if (sync_emit) __syncthreads();
+#pragma unroll
+    for (int a = 0; a < 16; ++a) {
+      const int k = j + RF::T * a;
+      if (k < d.n) {
+        R2 v = chirp_out ? cmul(x[a], ch[k]) : x[a];
+        emit(k, inv ? cconj(v) : v);
+      }
+    }
+  } else {
+#pragma unroll
+    for (int a = 0; a < 16; ++a) {
+      R2 v = load(j + RF::T * a);
+      x[a] = inv ? cconj(v) : v;
+    }
+    RF::dif(x, buf, tw, false, ping);
+    if (sync_emit) __syncthreads();
+#pragma unroll
+    for (int a = 0; a < 16; ++a) emit(bitrev(RF::point(j, a, 0), LOGM), inv ? cconj(x[a]) : x[a]);
+  }
+}
 
 // ---------------------------------------------------------------------------
 // Inverse rows: ftm [B][nrows][ncol] -> f (equiangular rows or HEALPix rings).
 // One CTA per (ring, map). Column c of ftm holds m = c - (L-1) - mo.
 // ---------------------------------------------------------------------------
-template <typename Real>
-__global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) inv_rows_kernel(RowsParams<Real> p) {
+// LOGM > 0: the register engine for uniform rings of one power-of-two working length 2^LOGM
+// (equiangular samplings; blockDim.x = 2^LOGM / 16); LOGM = 0: the shared-memory passes.
+template <typename Real, int LOGM, int NBUF>
+__global__ void __launch_bounds__(LOGM ? (1 << LOGM) / 16 : 512, (sizeof(Real) == 4 && LOGM < 13) ? 2 : 1)
+    inv_rows_kernel(RowsParams<Real> p) {
   using R2 = typename C2<Real>::t;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R2* s = reinterpret_cast<R2*>(smem_raw);
@@ -89,8 +149,31 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) inv_rows_kerne
     for (; m <= mhi; m += n) acc = cadd(acc, coef(m));
     return acc;
   };
-  dft_run<Real>(s, d, p.tb, true, load);
   const Real scale = (Real)(p.scale * (p.weights ? p.weights[t] : 1.0));
+  if constexpr (LOGM > 0) {
+    R2* outc = reinterpret_cast<R2*>(p.out) + (size_t)b * p.out_batch_stride + p.ring_off[t];
+    Real* outr = reinterpret_cast<Real*>(p.out) + (size_t)b * p.out_batch_stride + p.ring_off[t];
+    if (d.bluestein) {  // outputs in natural order: coalesced stores from the registers
+      reg_dft<Real, LOGM, NBUF>(s, d, p.tb, true, true, false, load, [&](int k, R2 v) {
+        if (p.real_out)
+          outr[k] = v.x * scale;
+        else
+          outc[k] = cscale(v, scale);
+      });
+    } else {  // bit-reversed positions: through shared memory to natural order
+      reg_dft<Real, LOGM, NBUF>(s, d, p.tb, true, true, true, load,
+                                [&](int k, R2 v) { s[ridx(k)] = v; });
+      __syncthreads();
+      for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        if (p.real_out)
+          outr[k] = s[ridx(k)].x * scale;
+        else
+          outc[k] = cscale(s[ridx(k)], scale);
+      }
+    }
+    return;
+  }
+  dft_run<Real>(s, d, p.tb, true, load);
   if (p.real_out) {
     Real* out = reinterpret_cast<Real*>(p.out) + (size_t)b * p.out_batch_stride + p.ring_off[t];
     for (int j = threadIdx.x; j < n; j += blockDim.x)
@@ -153,8 +236,9 @@ __device__ __forceinline__ void store_spectra(const RowsParams<Real>& p, int b, 
 // (dual: Real4 {+m, -m}; single: half 0 holds +m, half 1 holds -m), or, for
 // the MW/MWSS resampling chain, the transposed raw spectra Fc [B][ncolm][nrows].
 // ---------------------------------------------------------------------------
-template <typename Real>
-__global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) fwd_rows_kernel(RowsParams<Real> p) {
+template <typename Real, int LOGM, int NBUF>
+__global__ void __launch_bounds__(LOGM ? (1 << LOGM) / 16 : 512, (sizeof(Real) == 4 && LOGM < 13) ? 2 : 1)
+    fwd_rows_kernel(RowsParams<Real> p) {
   using R2 = typename C2<Real>::t;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R2* s = reinterpret_cast<R2*>(smem_raw);
@@ -174,14 +258,39 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) fwd_rows_kerne
     }
     return x;
   };
-  dft_run<Real>(s, d, p.tb, false, load);
+  if constexpr (LOGM > 0) {
+    if (p.mode == FWD_TO_COLS) {
+      // Fc[b][m + mshift][t] = scale * X_m for m in [mlo, L-1], straight from the registers
+      R2* out = reinterpret_cast<R2*>(p.out);
+      const int mlo = -(L - 1) - p.mo;
+      const int ncm = L - mlo;
+      reg_dft<Real, LOGM, NBUF>(s, d, p.tb, false, true, false, load, [&](int k, R2 v) {
+        const int m = k <= L - 1 ? k : k - n;
+        if (m >= mlo && m <= L - 1)
+          out[((size_t)b * ncm + (m - mlo)) * p.nrows + t] = cscale(v, (Real)p.scale);
+      });
+      return;
+    }
+    reg_dft<Real, LOGM, NBUF>(s, d, p.tb, false, true, true, load,
+                              [&](int k, R2 v) { s[ridx(k)] = v; });
+    __syncthreads();
+  } else {
+    dft_run<Real>(s, d, p.tb, false, load);
+  }
+  // X_k of this ring, k < n
+  auto get = [&](int k) -> R2 {
+    if constexpr (LOGM > 0)
+      return s[ridx(k)];
+    else
+      return dft_get<Real>(s, d, p.tb, false, k);
+  };
   const double w = p.weights ? p.weights[t] : 1.0;
   const double phi0 = p.phi0 ? p.phi0[t] : 0.0;
   if (p.mode == FWD_TO_RAW) {
     R2* out = reinterpret_cast<R2*>(p.out);
     for (int mi = threadIdx.x; mi < p.M; mi += blockDim.x) {
       const int m = p.m0 + mi;
-      R2 x = dft_get<Real>(s, d, p.tb, false, pmod(m, n));
+      R2 x = get(pmod(m, n));
       // real input on a ring of 2L pixels keeps m >= 0 only (the rfft half spectrum,
       // s2fft/utils/healpix_ffts.py:212-216)
       if (p.real_in && p.reality && n == 2 * L && m < 0) x = czero<R2>();
@@ -196,14 +305,14 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) fwd_rows_kerne
     const int ncm = L - mlo;
     for (int mi = threadIdx.x; mi < ncm; mi += blockDim.x) {
       const int m = mlo + mi;
-      R2 x = dft_get<Real>(s, d, p.tb, false, pmod(m, n));
+      R2 x = get(pmod(m, n));
       out[((size_t)b * ncm + mi) * p.nrows + t] = cscale(x, (Real)p.scale);
     }
     return;
   }
   // weighted, phase-shifted spectrum for m in [-(L-1), L-1] (periodic in n)
   auto val = [&](int m) -> R2 {
-    R2 x = dft_get<Real>(s, d, p.tb, false, pmod(m, n));
+    R2 x = get(pmod(m, n));
     double re = (double)x.x * w, im = (double)x.y * w;
     if (p.phi0) {
       double sn, cs;
@@ -230,8 +339,11 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) fwd_rows_kerne
 //   quadrature weights. The phi resampling 2L-1 -> 2L (resampling.py:248-281)
 //   reduces to the overall factor 2L/(2L-1) in the phi-Fourier domain.
 // ---------------------------------------------------------------------------
-template <typename Real>
-__global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) mw_cols_kernel(ColsParams<Real> p) {
+// LOGM > 0: both transforms on the register engine (d1.M = d2.M = 2^LOGM, the inverse DFT
+// of power-of-two length 4L; blockDim.x = 2^LOGM / 16); LOGM = 0: the shared-memory passes.
+template <typename Real, int LOGM, int NBUF>
+__global__ void __launch_bounds__(LOGM ? (1 << LOGM) / 16 : 512, (sizeof(Real) == 4 && LOGM < 13) ? 2 : 1)
+    mw_cols_kernel(ColsParams<Real> p) {
   using R2 = typename C2<Real>::t;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const FFTDesc d1 = *p.d1;
@@ -240,7 +352,8 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) mw_cols_kernel
   // second are kept, phase-multiplied, in tmp in between
   R2* s1 = reinterpret_cast<R2*>(smem_raw);
   R2* s2 = s1;
-  R2* tmp = s1 + padded_len(d1.M > d2.M ? d1.M : d2.M);
+  R2* tmp = s1 + (LOGM > 0 ? RegFFT<(LOGM > 0 ? LOGM : 8), NBUF>::SMEM_ELEMS
+                           : padded_len(d1.M > d2.M ? d1.M : d2.M));
   const int L = p.L;
   const int mlo = p.mw ? -(L - 1) : -L;
   const int ncm = L - mlo;
@@ -260,15 +373,23 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) mw_cols_kernel
     if (t <= L) return c[t];
     return cscale(c[2 * L - t], sgn);  // t = L+1+jj -> c[L-1-jj]
   };
-  dft_run<Real>(s1, d1, p.tb, false, load1);
   const int plo = p.mw ? -(L - 1) : -L;
   const int phi = L - 1;
   const int n2 = d2.n;  // 4L
   const R2* __restrict__ ph = reinterpret_cast<const R2*>(p.ph);
-  for (int pp = plo + (int)threadIdx.x; pp <= phi; pp += blockDim.x) {
-    const int j = pmod(pp, n1);
-    const R2 g = d1.bluestein ? s1[pidx(j)] : s1[pidx(bitrev(j, d1.logM))];
-    tmp[pp - plo] = cmul(g, ph[(pp + n2) % n2]);
+  if constexpr (LOGM > 0) {
+    // bin k of the theta DFT is p = k (k <= L-1) or k - n1; ph carries the Bluestein chirp
+    reg_dft<Real, LOGM, NBUF>(s1, d1, p.tb, false, false, false, load1, [&](int k, R2 v) {
+      const int pp = k <= phi ? k : k - n1;
+      if (pp >= plo) tmp[pp - plo] = cmul(v, ph[(pp + n2) % n2]);
+    });
+  } else {
+    dft_run<Real>(s1, d1, p.tb, false, load1);
+    for (int pp = plo + (int)threadIdx.x; pp <= phi; pp += blockDim.x) {
+      const int j = pmod(pp, n1);
+      const R2 g = d1.bluestein ? s1[pidx(j)] : s1[pidx(bitrev(j, d1.logM))];
+      tmp[pp - plo] = cmul(g, ph[(pp + n2) % n2]);
+    }
   }
   __syncthreads();
   auto load2 = [&](int k) -> R2 {
@@ -276,14 +397,41 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) mw_cols_kernel
     const int pp = k <= phi ? k : k - n2;
     return (pp < plo || pp > phi) ? czero<R2>() : tmp[pp - plo];
   };
-  dft_run<Real>(s2, d2, p.tb, true, load2);
+  // upstream's MWSS(L) detour (corrections described in ColsParams): the MW pole ring's odd
+  // (m + s) part, and for real MWSS maps the split theta-Nyquist bin (p = -L, tmp[0])
+  const R2* __restrict__ pole = (p.mw && par) ? reinterpret_cast<const R2*>(p.pole) : nullptr;
+  const R2 xpole = pole ? c[L - 1] : czero<R2>();
+  const R2 nyq = (!p.mw && p.nyq_split) ? tmp[0] : czero<R2>();
+  if constexpr (LOGM > 0) {
+    // the 4L outputs in natural order in shared memory (after a barrier: the transform's
+    // last exchange may still be read)
+    reg_dft<Real, LOGM, NBUF>(s2, d2, p.tb, true, true, true, load2,
+                              [&](int k, R2 v) { s2[ridx(k)] = v; });
+    __syncthreads();
+  } else {
+    dft_run<Real>(s2, d2, p.tb, true, load2);
+  }
   const int nout = 2 * L + 1;
   const int am = m < 0 ? -m : m;
   R2* out = reinterpret_cast<R2*>(p.out);
+  auto chain = [&](int t) -> R2 {
+    R2 u;
+    if constexpr (LOGM > 0)
+      u = s2[ridx(t)];
+    else
+      u = dft_get<Real>(s2, d2, p.tb, true, t);
+    if (pole) u = cadd(u, cmul(xpole, pole[t]));
+    if (t & 1) {  // i N sin(pi t / 2)
+      const Real sg = (t & 2) ? Real(-1) : Real(1);
+      u.x -= sg * nyq.y;
+      u.y += sg * nyq.x;
+    }
+    return u;
+  };
   if (p.raw) {
     if (m < p.m0) return;
     for (int t = threadIdx.x; t < nout; t += blockDim.x) {
-      R2 u = dft_get<Real>(s2, d2, p.tb, true, t);
+      R2 u = chain(t);
       u.x = (Real)((double)u.x * p.scale);
       u.y = (Real)((double)u.y * p.scale);
       out[((size_t)b * nout + t) * p.M + (m - p.m0)] = u;
@@ -291,7 +439,7 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) mw_cols_kernel
     return;
   }
   auto weighted = [&](int t) -> R2 {
-    R2 u = dft_get<Real>(s2, d2, p.tb, true, t);
+    R2 u = chain(t);
     const double f = p.scale * p.weights[t];
     u.x = (Real)((double)u.x * f);
     u.y = (Real)((double)u.y * f);
@@ -453,8 +601,24 @@ __global__ void __launch_bounds__(512, sizeof(Real) == 4 ? 2 : 1) mw_cols_adj_ke
   dft_run<Real>(s1, d1, p.tb, true, [&](int j) { return tmp[j]; });  // unnormalised inverse DFT over n1
   const int par = ((m + p.spin) % 2 + 2) % 2;
   const Real sgn = par ? Real(-1) : Real(1);
+  // transpose of the forward's pole correction: the pole ring gains sum_k conj(c_k) y_k
+  R2 gpole = czero<R2>();
+  if (p.mw && par && p.pole) {
+    const R2* __restrict__ pole = reinterpret_cast<const R2*>(p.pole);
+    R2 acc = czero<R2>();
+    for (int t = threadIdx.x; t < nout; t += blockDim.x) acc = cadd(acc, cmul(cconj(pole[t]), load2(t)));
+    for (int sh = 16; sh > 0; sh >>= 1) {
+      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, sh);
+      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, sh);
+    }
+    __shared__ R2 wsum[32];  // one partial sum per warp (blockDim.x <= 1024, a multiple of 32)
+    if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) gpole = cadd(gpole, wsum[w]);
+  }
   for (int t = threadIdx.x; t < p.nin; t += blockDim.x) {
     R2 x = dft_get<Real>(s1, d1, p.tb, true, t);
+    if (t == L - 1) x = cadd(x, gpole);
     if (p.mw) {
       if (t <= L - 2) x = cadd(x, cscale(dft_get<Real>(s1, d1, p.tb, true, 2 * L - 2 - t), sgn));
     } else {
@@ -479,50 +643,95 @@ static int fft_threads(int M) {
   return t;
 }
 
+// Register engine for one working length 2^LOGM: 10 <= LOGM <= 13 (1024 .. 8192 points; in
+// double up to 4096, where 16 points of a thread still fit the register file).
+static bool g_reg_engine = false;  // register engine on (pending validation)
+
+template <typename Real>
+static int reg_logm(int M) {
+  if (!g_reg_engine) return 0;
+  const int top = sizeof(Real) == 4 ? 13 : 12;
+  for (int lg = 10; lg <= top; ++lg)
+    if (M == (1 << lg)) return lg;
+  return 0;
+}
+static constexpr int kRegBufs = 1;  // exchange buffers of the register engine
+
+template <typename Real, typename Kernel, typename Params>
+static cudaError_t launch_fft_kernel(Kernel k, dim3 grid, int threads, size_t smem,
+                                     const Params& p, cudaStream_t s) {
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           cudaSharedmemCarveoutMaxShared);
+  if (e != cudaSuccess) return e;
+  k<<<grid, threads, smem, s>>>(p);
+  return cudaGetLastError();
+}
+
+template <typename Real, int LOGM>
+static size_t reg_smem(int extra) {
+  return ((size_t)RegFFT<LOGM, kRegBufs>::SMEM_ELEMS + extra) * sizeof(typename C2<Real>::t);
+}
+
+// the rows use the register engine when every ring has the same working length (no per-ring
+// descriptors: equiangular samplings) and no ring phase
+template <typename Real>
+static int rows_reg_logm(const RowsParams<Real>& p, int maxM) {
+  return (p.ring_desc == nullptr && p.phi0 == nullptr) ? reg_logm<Real>(maxM) : 0;
+}
+
 template <typename Real>
 cudaError_t launch_inv_rows(const RowsParams<Real>& p, int nrings, int batch, int maxM,
                             cudaStream_t s) {
   using R2 = typename C2<Real>::t;
+  const dim3 grid(nrings, batch);
+  switch (rows_reg_logm(p, maxM)) {
+    case 10: return launch_fft_kernel<Real>(inv_rows_kernel<Real, 10, kRegBufs>, grid, 64, reg_smem<Real, 10>(0), p, s);
+    case 11: return launch_fft_kernel<Real>(inv_rows_kernel<Real, 11, kRegBufs>, grid, 128, reg_smem<Real, 11>(0), p, s);
+    case 12: return launch_fft_kernel<Real>(inv_rows_kernel<Real, 12, kRegBufs>, grid, 256, reg_smem<Real, 12>(0), p, s);
+    case 13: return launch_fft_kernel<Real>(inv_rows_kernel<Real, 13, kRegBufs>, grid, 512, reg_smem<Real, 13>(0), p, s);
+    default: break;
+  }
   const size_t smem = (size_t)padded_len(maxM) * sizeof(R2);
-  cudaError_t e = cudaFuncSetAttribute(inv_rows_kernel<Real>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(inv_rows_kernel<Real>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                           cudaSharedmemCarveoutMaxShared);
-  if (e != cudaSuccess) return e;
-  inv_rows_kernel<Real><<<dim3(nrings, batch), fft_threads(maxM), smem, s>>>(p);
-  return cudaGetLastError();
+  return launch_fft_kernel<Real>(inv_rows_kernel<Real, 0, 1>, grid, fft_threads(maxM), smem, p, s);
 }
 
 template <typename Real>
 cudaError_t launch_fwd_rows(const RowsParams<Real>& p, int nrings, int batch, int maxM,
                             cudaStream_t s) {
   using R2 = typename C2<Real>::t;
+  const dim3 grid(nrings, batch);
+  switch (rows_reg_logm(p, maxM)) {
+    case 10: return launch_fft_kernel<Real>(fwd_rows_kernel<Real, 10, kRegBufs>, grid, 64, reg_smem<Real, 10>(0), p, s);
+    case 11: return launch_fft_kernel<Real>(fwd_rows_kernel<Real, 11, kRegBufs>, grid, 128, reg_smem<Real, 11>(0), p, s);
+    case 12: return launch_fft_kernel<Real>(fwd_rows_kernel<Real, 12, kRegBufs>, grid, 256, reg_smem<Real, 12>(0), p, s);
+    case 13: return launch_fft_kernel<Real>(fwd_rows_kernel<Real, 13, kRegBufs>, grid, 512, reg_smem<Real, 13>(0), p, s);
+    default: break;
+  }
   const size_t smem = (size_t)padded_len(maxM) * sizeof(R2);
-  cudaError_t e = cudaFuncSetAttribute(fwd_rows_kernel<Real>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(fwd_rows_kernel<Real>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                           cudaSharedmemCarveoutMaxShared);
-  if (e != cudaSuccess) return e;
-  fwd_rows_kernel<Real><<<dim3(nrings, batch), fft_threads(maxM), smem, s>>>(p);
-  return cudaGetLastError();
+  return launch_fft_kernel<Real>(fwd_rows_kernel<Real, 0, 1>, grid, fft_threads(maxM), smem, p, s);
 }
 
 template <typename Real>
 cudaError_t launch_mw_cols(const ColsParams<Real>& p, int ncm, int batch, int M1, int M2,
                            cudaStream_t s) {
   using R2 = typename C2<Real>::t;
+  const dim3 grid(ncm, batch);
+  // register engine: one working length for both transforms, the second a plain power of two
+  const int lg = (M1 == M2 && p.d2_pow2) ? reg_logm<Real>(M1) : 0;
+  const int extra = 2 * p.L;
+  switch (lg) {
+    case 10: return launch_fft_kernel<Real>(mw_cols_kernel<Real, 10, kRegBufs>, grid, 64, reg_smem<Real, 10>(extra), p, s);
+    case 11: return launch_fft_kernel<Real>(mw_cols_kernel<Real, 11, kRegBufs>, grid, 128, reg_smem<Real, 11>(extra), p, s);
+    case 12: return launch_fft_kernel<Real>(mw_cols_kernel<Real, 12, kRegBufs>, grid, 256, reg_smem<Real, 12>(extra), p, s);
+    case 13: return launch_fft_kernel<Real>(mw_cols_kernel<Real, 13, kRegBufs>, grid, 512, reg_smem<Real, 13>(extra), p, s);
+    default: break;
+  }
   // one DFT buffer plus the 2L bins carried between the two transforms
   const size_t smem = (size_t)(padded_len(M1 > M2 ? M1 : M2) + 2 * p.L) * sizeof(R2);
-  cudaError_t e = cudaFuncSetAttribute(mw_cols_kernel<Real>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(mw_cols_kernel<Real>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                           cudaSharedmemCarveoutMaxShared);
-  if (e != cudaSuccess) return e;
-  mw_cols_kernel<Real><<<dim3(ncm, batch), fft_threads(M1 > M2 ? M1 : M2), smem, s>>>(p);
-  return cudaGetLastError();
+  return launch_fft_kernel<Real>(mw_cols_kernel<Real, 0, 1>, grid, fft_threads(M1 > M2 ? M1 : M2),
+                                 smem, p, s);
 }
 
 template <typename Real>

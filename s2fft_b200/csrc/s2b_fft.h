@@ -68,9 +68,16 @@ struct ColsParams {
   double scale;         // overall factor of the chain
   const FFTDesc* d1;    // theta DFT over the periodic extension (2L-1 or 2L)
   const FFTDesc* d2;    // inverse DFT of length 4L
+  int d2_pow2;          // 4L is a power of two (d2 without Bluestein)
   const double* weights;// 2L+1 MWSS(2L) transform weights
   const void* ph;       // [4L] complex factor of theta-DFT bin p (at p mod 4L), 0 outside
   const void* ph_adj;   // [4L] adjoint chain: conj(half-sample phase) / n1 (at p mod 4L)
+  // MW: [2L+1] complex c_k, added as x_pole * c_k to the inverse-DFT output of columns with
+  // odd m + s (x_pole = the input column's value on the ring theta = pi); nullptr: none
+  const void* pole;
+  // MWSS real maps: the theta-Nyquist bin N (p = -L) counts half at -L and half at +L, i.e.
+  // i N sin(pi k / 2) is added to the output on ring k
+  int nyq_split;
   FFTTables<Real> tb;
   const void* in;       // Fc [B][ncm][nin]
   void* out;            // G  [B][half][m + kPadLo][Gs]; MWSS(2L) ring t -> row t-1,

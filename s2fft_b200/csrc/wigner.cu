@@ -23,8 +23,14 @@ static int wgrid(long n) {
 
 // tmp[b][l][c] = flmn[b][N-1+n][l][c] * (-1)^n sqrt((2l+1)/(16 pi^3)); the spin
 // transform that follows applies its own sqrt((2l+1)/4pi) on top, as upstream does.
+// real0 (real signals, slice n = 0): upstream runs that slice as a real spin-0 inverse,
+// which reads the orders m >= 0 only and takes the real part of their Hermitian extension
+// (wigner.py:176-187, spherical.py:176-208); the complex transform that follows does the
+// same when the orders are weighted by 0 (m < 0), 1 (m = 0) and 2 (m > 0) and the gamma DFT
+// keeps the real part of the slice.
 template <typename Real>
-__global__ void gather_n_kernel(const W2<Real>* flmn, W2<Real>* tmp, int B, int N, int L, int n) {
+__global__ void gather_n_kernel(const W2<Real>* flmn, W2<Real>* tmp, int B, int N, int L, int n,
+                                int real0) {
   const long per = (long)L * (2 * L - 1);
   const long total = per * B;
   const double pi = 3.141592653589793;
@@ -32,7 +38,9 @@ __global__ void gather_n_kernel(const W2<Real>* flmn, W2<Real>* tmp, int B, int 
        i += (long)gridDim.x * blockDim.x) {
     const long b = i / per, r = i % per;
     const int l = (int)(r / (2 * L - 1));
-    const double f = ((n & 1) ? -1.0 : 1.0) * sqrt((2.0 * l + 1.0) / (16.0 * pi * pi * pi));
+    const int m = (int)(r % (2 * L - 1)) - (L - 1);
+    double f = ((n & 1) ? -1.0 : 1.0) * sqrt((2.0 * l + 1.0) / (16.0 * pi * pi * pi));
+    if (real0) f *= m < 0 ? 0.0 : (m == 0 ? 1.0 : 2.0);
     W2<Real> v = flmn[(b * (2 * N - 1) + (N - 1 + n)) * per + r];
     v.x = (Real)(v.x * f);
     v.y = (Real)(v.y * f);
@@ -168,12 +176,14 @@ __global__ void gamma_forward_kernel(const void* f, W2<Real>* fban, int B, int N
 }
 
 cudaError_t launch_gather_n(bool fp64, const void* flmn, void* tmp, int B, int N, int L, int n,
-                            cudaStream_t s) {
+                            int real0, cudaStream_t s) {
   const long tot = (long)B * L * (2 * L - 1);
   if (fp64)
-    gather_n_kernel<double><<<wgrid(tot), 256, 0, s>>>((const double2*)flmn, (double2*)tmp, B, N, L, n);
+    gather_n_kernel<double><<<wgrid(tot), 256, 0, s>>>((const double2*)flmn, (double2*)tmp, B, N, L, n,
+                                                       real0);
   else
-    gather_n_kernel<float><<<wgrid(tot), 256, 0, s>>>((const float2*)flmn, (float2*)tmp, B, N, L, n);
+    gather_n_kernel<float><<<wgrid(tot), 256, 0, s>>>((const float2*)flmn, (float2*)tmp, B, N, L, n,
+                                                      real0);
   return cudaGetLastError();
 }
 

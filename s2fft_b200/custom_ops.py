@@ -21,7 +21,7 @@ import torch
 from . import _lib
 from .fourier_wigner import (OP_S2_TO_SUBSET, OP_SO3_TO_SUBSET, OP_SUBSET_TO_S2, _cdt,
                              _check_sampling, _fwlib, _geometry, _precomps, get_plan)
-from .spherical import _device, _ret, _to_device
+from .spherical import _device, _ret, _to_device, _dense, _aligned
 
 
 def _spins(spins, dev, L):
@@ -48,6 +48,7 @@ class _OpFn(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, xc, call, adjoint, out_shape):
+        xc = _aligned(_dense(xc))
         ctx.adjoint, ctx.in_shape = adjoint, xc.shape
         out = torch.empty(out_shape, dtype=xc.dtype, device=xc.device)
         call(xc, out)
@@ -55,7 +56,7 @@ class _OpFn(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, g):
-        g = g.contiguous()
+        g = _aligned(_dense(g))
         gx = torch.empty(ctx.in_shape, dtype=g.dtype, device=g.device)
         ctx.adjoint(g, gx)
         return gx, None, None, None

@@ -24,7 +24,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .spherical import _device, _ret, _to_device
+from .spherical import _device, _ret, _to_device, _dense, _aligned
 
 _SAMPLINGS = ("mw", "mwss")
 
@@ -177,6 +177,7 @@ class _FWInverseFn(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, x, plan, B, delta, out_shape, cdt):
+        x = _aligned(_dense(x))
         ctx.plan, ctx.B, ctx.delta, ctx.in_shape = plan, B, delta, x.shape
         out = torch.empty(out_shape, dtype=cdt, device=x.device)
         ws = plan.workspace(OP_INVERSE, B, False)
@@ -187,7 +188,7 @@ class _FWInverseFn(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, g):
-        g = g.contiguous()
+        g = _aligned(_dense(g))
         gx = torch.empty(ctx.in_shape, dtype=g.dtype, device=g.device)
         ws = ctx.plan.workspace(OP_INVERSE, ctx.B, False)
         _lib.check(_fwlib().s2b_fw_inverse_adjoint(ctx.plan.ptr, ctx.B, ctx.delta.data_ptr(),
@@ -201,6 +202,7 @@ class _FWForwardFn(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, x, plan, B, delta, quads, out_shape, cdt):
+        x = _aligned(_dense(x))
         ctx.plan, ctx.B, ctx.delta, ctx.quads, ctx.in_shape = plan, B, delta, quads, x.shape
         out = torch.empty(out_shape, dtype=cdt, device=x.device)
         ws = plan.workspace(OP_FORWARD, B, False)
@@ -211,7 +213,7 @@ class _FWForwardFn(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, g):
-        g = g.contiguous()
+        g = _aligned(_dense(g))
         gx = torch.empty(ctx.in_shape, dtype=g.dtype, device=g.device)
         ws = ctx.plan.workspace(OP_FORWARD, ctx.B, False)
         _lib.check(_fwlib().s2b_fw_forward_adjoint(

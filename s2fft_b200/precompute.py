@@ -19,7 +19,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .spherical import _check_method, _device, _dtypes, _ret, _to_device, f_shape
+from .spherical import _check_method, _device, _dtypes, _ret, _to_device, f_shape, _dense
 
 
 def _plan(dev, L, spin, nside, s, reality, precision, B):
@@ -101,13 +101,14 @@ class _PreInverseFn(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, x, plan, K, out_shape, cdt):
+        x = _aligned(_dense(x))
         ctx.plan, ctx.K, ctx.in_shape = plan, K, x.shape
         out = torch.empty(out_shape, dtype=cdt, device=x.device)
         return _pre_call("s2b_precompute_inverse", plan, K, x, out, False)
 
     @staticmethod
     def backward(ctx, g):
-        g = g.contiguous()
+        g = _aligned(_dense(g))
         gx = torch.empty(ctx.in_shape, dtype=g.dtype, device=g.device)
         _pre_call("s2b_precompute_inverse_adjoint", ctx.plan, ctx.K, g, gx, False)
         return gx, None, None, None, None
@@ -118,13 +119,14 @@ class _PreForwardFn(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, x, plan, K, out_shape, cdt):
+        x = _aligned(_dense(x))
         ctx.plan, ctx.K, ctx.in_shape = plan, K, x.shape
         out = torch.empty(out_shape, dtype=cdt, device=x.device)
         return _pre_call("s2b_precompute_forward", plan, K, x, out, True)
 
     @staticmethod
     def backward(ctx, g):
-        g = g.contiguous()
+        g = _aligned(_dense(g))
         gx = torch.empty(ctx.in_shape, dtype=g.dtype, device=g.device)
         _pre_call("s2b_precompute_forward_adjoint", ctx.plan, ctx.K, g, gx, True)
         return gx, None, None, None, None

@@ -18,10 +18,25 @@ Differentiation: when a torch input requires grad, the transforms run as
 ``torch.autograd.Function``s whose backward passes call the adjoint kernels
 (``s2b_inverse_adjoint`` / ``s2b_forward_adjoint``, recomputing the Wigner-d
 recursion instead of storing it); refinement iterations are composed from the
-single passes. Complex transforms only (``reality=False``).
+single passes. Real signals (``reality=True``) are differentiated through
+exact rewrites on the complex kernels: upstream's real inverse keeps the orders
+m >= 0 and reads the map off the Hermitian extension of the ring spectra, which
+is ``Re(inverse(D flm))`` with D = 1 at m = 0, 2 at m > 0 and 0 at m < 0; its
+real forward takes the real part of the (upsampled) map before the ring FFTs and
+mirrors the m < 0 half from m >= 0 (s2fft/transforms/spherical.py:176-208,
+526-588), which is the complex forward averaged with the conjugate of the
+complex forward of the phi-reflected map (MW / MWSS) and then mirrored. The same
+rewrites serve ``reality=True`` with spin != 0, which upstream's on-the-fly
+methods accept and treat the same way.
+
+``precomps`` and ``spmd`` are accepted for signature compatibility: the
+recursion tables are built on the device per plan, and one GPU runs each call,
+so a supplied value is ignored (with a ``UserWarning``).
 """
 
 from __future__ import annotations
+
+import warnings
 
 import numpy as np
 import torch
@@ -51,8 +66,6 @@ def _check_args(L, spin, nside, sampling, reality, L_lower):
         if nside is None:
             raise ValueError(f"Sampling scheme sampling={sampling} with nside={nside} not supported")
         assert L >= 2 * nside
-    if reality and spin != 0:
-        raise ValueError("reality=True requires spin 0")
     if not 0 <= L_lower < L:
         raise ValueError("L_lower must satisfy 0 <= L_lower < L")
     return s
@@ -77,6 +90,13 @@ def _device():
     return torch.device("cuda", torch.cuda.current_device())
 
 
+def _dense(t):
+    """A tensor whose memory holds its values: conjugate and negative views (lazy bits that
+    torch sets, e.g. on gradients flowing through torch.conj) are materialised, since the
+    C ABI reads raw memory."""
+    return t.resolve_conj().resolve_neg().contiguous()
+
+
 def _aligned(t):
     # the C ABI takes 16-byte aligned operands; a view into a larger tensor may not be
     return t if t.data_ptr() % 16 == 0 else t.clone()
@@ -86,13 +106,13 @@ def _to_device(x, dtype, device):
     """(contiguous, 16-byte aligned tensor on device, was_numpy, original device)."""
     if isinstance(x, np.ndarray):
         t = torch.from_numpy(np.ascontiguousarray(x))
-        return _aligned(t.to(device=device, dtype=dtype).contiguous()), True, None
+        return _aligned(_dense(t.to(device=device, dtype=dtype))), True, None
     if isinstance(x, torch.Tensor):
         dev = x.device
-        t = x.to(device=device if dev.type != "cuda" else dev, dtype=dtype).contiguous()
+        t = _dense(x.to(device=device if dev.type != "cuda" else dev, dtype=dtype))
         return _aligned(t), False, dev
     t = torch.as_tensor(np.asarray(x))
-    return _aligned(t.to(device=device, dtype=dtype).contiguous()), True, None
+    return _aligned(_dense(t.to(device=device, dtype=dtype))), True, None
 
 
 def _ret(t, was_numpy, dev):
@@ -115,6 +135,7 @@ class _InverseFn(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, flm, plan, f_shape_full, out_dtype):
+        flm = _aligned(_dense(flm))
         out = torch.empty(f_shape_full, dtype=out_dtype, device=flm.device)
         ws = plan.workspace(0)
         _lib.check(_lib.lib().s2b_inverse(plan.ptr, flm.data_ptr(), out.data_ptr(),
@@ -126,7 +147,7 @@ class _InverseFn(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, g):
-        g = g.contiguous()
+        g = _aligned(_dense(g))
         gflm = torch.empty(ctx.in_shape, dtype=g.dtype, device=g.device)
         ws = ctx.plan.workspace(2)
         _lib.check(_lib.lib().s2b_inverse_adjoint(ctx.plan.ptr, g.data_ptr(), gflm.data_ptr(),
@@ -140,6 +161,7 @@ class _ForwardFn(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, f, plan, flm_shape_full, out_dtype):
+        f = _aligned(_dense(f))
         out = torch.empty(flm_shape_full, dtype=out_dtype, device=f.device)
         ws = plan.workspace(1)
         _lib.check(_lib.lib().s2b_forward(plan.ptr, f.data_ptr(), out.data_ptr(),
@@ -151,7 +173,7 @@ class _ForwardFn(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, g):
-        g = g.contiguous()
+        g = _aligned(_dense(g))
         gf = torch.empty(ctx.in_shape, dtype=g.dtype, device=g.device)
         ws = ctx.plan.workspace(3)
         _lib.check(_lib.lib().s2b_forward_adjoint(ctx.plan.ptr, g.data_ptr(), gf.data_ptr(),
@@ -164,12 +186,39 @@ def _needs_grad(x):
     return isinstance(x, torch.Tensor) and x.requires_grad and torch.is_grad_enabled()
 
 
+def _warn_unused(precomps, spmd):
+    if precomps is not None:
+        warnings.warn("precomps is ignored: the recursion tables are built on the device "
+                      "per plan", UserWarning, stacklevel=3)
+    if spmd:
+        warnings.warn("spmd is ignored: each call runs on the current GPU", UserWarning,
+                      stacklevel=3)
+
+
+def _real_orders(L, device, dtype):
+    """D[L-1+m] = 1 at m = 0, 2 at m > 0, 0 at m < 0 (the Hermitian extension's weights)."""
+    d = torch.zeros(2 * L - 1, dtype=dtype, device=device)
+    d[L - 1] = 1
+    d[L:] = 2
+    return d
+
+
+def _mirror_real(y, L):
+    """Upstream's completion of a real signal's coefficients from the m >= 0 half:
+    flm[l, -m] = (-1)^m conj(flm[l, m]) (s2fft/transforms/spherical.py:577-582)."""
+    mc = torch.from_numpy((-1.0) ** (np.arange(1, L) % 2)).to(device=y.device,
+                                                              dtype=y.real.dtype)
+    neg = torch.flip(torch.conj(y[..., L:]) * mc, dims=[-1])
+    return torch.cat([neg, y[..., L - 1:]], dim=-1)
+
+
 def inverse(flm, L: int, spin: int = 0, nside: int = None, sampling: str = "mw",
             method: str = "cuda", reality: bool = False, precomps=None, spmd: bool = False,
             L_lower: int = 0, _ssht_backend: int = 1, precision: str = "f64"):
     """Inverse spin-SHT: flm [.., L, 2L-1] -> f on the sampling grid."""
     _check_method(method)
     s = _check_args(L, spin, nside, sampling, reality, L_lower)
+    _warn_unused(precomps, spmd)
     cdt, rdt = _dtypes(precision)
     dev = _device()
     x, was_np, odev = _to_device(flm, cdt, dev)
@@ -177,14 +226,18 @@ def inverse(flm, L: int, spin: int = 0, nside: int = None, sampling: str = "mw",
     if tuple(x.shape[-2:]) != (L, 2 * L - 1):
         raise ValueError(f"flm must have trailing shape {(L, 2 * L - 1)}, got {tuple(x.shape)}")
     B = int(np.prod(batch_shape)) if batch_shape else 1
-    plan = _lib.get_plan(x.device, L=L, spin=spin, nside=nside or 0, sampling=_lib.SAMPLING[s],
-                         reality=int(bool(reality)), L_lower=L_lower,
-                         precision=_lib.PRECISION[precision], batch=B, iter=0, N=0)
+    kw = dict(L=L, spin=spin, nside=nside or 0, sampling=_lib.SAMPLING[s], L_lower=L_lower,
+              precision=_lib.PRECISION[precision], batch=B, iter=0, N=0)
+    fs = batch_shape + f_shape(L, s, nside)
+    if reality and (spin != 0 or _needs_grad(x)):
+        # f = Re(I(D flm)) on the complex kernels: exactly upstream's real inverse (orders
+        # m >= 0 on the Hermitian extension), differentiable and valid for any spin
+        pc = _lib.get_plan(x.device, reality=0, **kw)
+        xd = x * _real_orders(L, x.device, rdt)
+        return _ret(_InverseFn.apply(xd, pc, fs, cdt).real.contiguous(), was_np, odev)
+    plan = _lib.get_plan(x.device, reality=int(bool(reality)), **kw)
     if _needs_grad(x):
-        if reality:
-            raise NotImplementedError("gradients are available for complex transforms (reality=False)")
-        return _ret(_InverseFn.apply(x, plan, batch_shape + f_shape(L, s, nside), cdt),
-                    was_np, odev)
+        return _ret(_InverseFn.apply(x, plan, fs, cdt), was_np, odev)
     out = torch.empty(batch_shape + f_shape(L, s, nside), dtype=rdt if reality else cdt,
                       device=x.device)
     ws = plan.workspace(False)
@@ -204,6 +257,7 @@ def forward(f, L: int, spin: int = 0, nside: int = None, sampling: str = "mw",
     """
     _check_method(method)
     s = _check_args(L, spin, nside, sampling, reality, L_lower)
+    _warn_unused(precomps, spmd)
     if iter is None:
         iter = 0
     cdt, rdt = _dtypes(precision)
@@ -220,18 +274,42 @@ def forward(f, L: int, spin: int = 0, nside: int = None, sampling: str = "mw",
         raise ValueError(f"f must have trailing shape {fs}, got {tuple(x.shape)}")
     batch_shape = tuple(x.shape[:-nd])
     B = int(np.prod(batch_shape)) if batch_shape else 1
-    if _needs_grad(x):
-        if reality:
-            raise NotImplementedError("gradients are available for complex transforms (reality=False)")
-        # refinement flm <- flm + F(f - I(flm)) composed from the differentiable single passes
+    if _needs_grad(x) or (reality and spin != 0):
+        # refinement flm <- flm + F(f - I(flm)) composed from the differentiable single
+        # passes on the complex kernels; real signals as upstream (module docstring)
         kw = dict(L=L, spin=spin, nside=nside or 0, sampling=_lib.SAMPLING[s], reality=0,
                   L_lower=L_lower, precision=_lib.PRECISION[precision], batch=B, N=0)
         p0 = _lib.get_plan(x.device, iter=0, **kw)
         flm_shape = batch_shape + (L, 2 * L - 1)
-        y = _ForwardFn.apply(x, p0, flm_shape, cdt)
+        if reality:
+            dord = _real_orders(L, x.device, rdt)
+            reflect = s in ("mw", "mwss")
+            if reflect:  # phi -> -phi on the ring grid
+                nph = fs[-1]
+                ridx = torch.from_numpy((-np.arange(nph)) % nph).to(x.device)
+
+            def fwd1(r):
+                y = _ForwardFn.apply(r.to(cdt), p0, flm_shape, cdt)
+                if reflect:
+                    # upstream takes the real part of the upsampled MW / MWSS map, which
+                    # averages each order m with the conjugate of the transform of the
+                    # phi-reflected map (s2fft/transforms/spherical.py:526-534)
+                    yr = _ForwardFn.apply(r.index_select(-1, ridx).to(cdt), p0, flm_shape,
+                                          cdt)
+                    y = 0.5 * (y + torch.conj(yr))
+                return _mirror_real(y, L)
+
+            def inv1(y):
+                return _InverseFn.apply(y * dord, p0, batch_shape + fs, cdt).real
+        else:
+            def fwd1(r):
+                return _ForwardFn.apply(r, p0, flm_shape, cdt)
+
+            def inv1(y):
+                return _InverseFn.apply(y, p0, batch_shape + fs, cdt)
+        y = fwd1(x)
         for _ in range(int(iter)):
-            r = x - _InverseFn.apply(y, p0, batch_shape + fs, cdt)
-            y = y + _ForwardFn.apply(r, p0, flm_shape, cdt)
+            y = y + fwd1(x - inv1(y))
         return _ret(y, was_np, odev)
     plan = _lib.get_plan(x.device, L=L, spin=spin, nside=nside or 0, sampling=_lib.SAMPLING[s],
                          reality=int(bool(reality)), L_lower=L_lower,

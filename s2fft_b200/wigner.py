@@ -7,7 +7,8 @@ transforms run by ``libs2b.so`` plus a DFT over gamma.
 
 When a torch input requires grad, the transform is composed from the
 differentiable spin transforms (whose backward passes run the adjoint kernels)
-and a gamma DFT written as a dense (2N-1) x (2N-1) product.
+and a gamma DFT written as a dense (2N-1) x (2N-1) product (complex signals) or
+torch's real DFT over gamma (real signals, slices n >= 0 as upstream).
 
 Difference from upstream: upstream's recursive methods raise ``Warning`` for
 N >= 8 (wigner.py:87-88); here N = 8 is accepted and ``Warning`` is raised from
@@ -77,36 +78,53 @@ def _lnorm(L, n, L_lower, device, dtype, inverse):
     return torch.from_numpy(v).to(device=device, dtype=dtype)[:, None]
 
 
-def _inverse_composed(x, L, N, nside, s, L_lower, precision):
+def _inverse_composed(x, L, N, nside, s, L_lower, precision, reality=False):
     """Differentiable inverse: 2N-1 spin(-n) inverses and the gamma inverse DFT
-    (s2fft/transforms/wigner.py:110-196)."""
+    (s2fft/transforms/wigner.py:110-196). Real signals as upstream: slices n >= 0 only
+    (n = 0 by the real spin-0 inverse) and an inverse real DFT over gamma."""
     rdt = x.real.dtype
-    fs = []
-    for j in range(2 * N - 1):
-        n = j - (N - 1)
-        t = x[..., j, :, :] * _lnorm(L, n, L_lower, x.device, rdt, True)
-        fs.append(_sph.inverse(t, L, -n, nside, s, L_lower=L_lower, precision=precision))
     gdim = len(f_shape(L, s, nside))
-    fban = torch.stack(fs, dim=-gdim - 1)  # [.., 2N-1 (n), grid]
+    cdt = x.dtype
+    fs = []
+    for n in range(0 if reality else -(N - 1), N):
+        j = N - 1 + n
+        t = x[..., j, :, :] * _lnorm(L, n, L_lower, x.device, rdt, True)
+        fs.append(_sph.inverse(t, L, -n, nside, s, L_lower=L_lower, precision=precision,
+                               reality=reality and n == 0).to(cdt))
+    fban = torch.stack(fs, dim=-gdim - 1)  # [.., n, grid]
+    if reality:
+        return torch.fft.irfft(fban, 2 * N - 1, dim=-gdim - 1, norm="forward")
     P = _gamma_phases(N, +1, x.device, x.dtype)
     return torch.movedim(torch.tensordot(fban, P, dims=([-gdim - 1], [1])), -1, -gdim - 1)
 
 
-def _forward_composed(x, L, N, nside, s, L_lower, precision):
+def _forward_composed(x, L, N, nside, s, L_lower, precision, reality=False):
     """Differentiable forward: gamma DFT times 2 pi/(2N-1), spin(-n) forwards
-    (s2fft/transforms/wigner.py:442-533)."""
+    (s2fft/transforms/wigner.py:442-533). Real signals as upstream: a real DFT over
+    gamma, slices n >= 0 (n = 0 by the real spin-0 forward), and the slices n < 0
+    mirrored, flmn[-n] = conj(flip(flmn[n] (-1)^|m| (-1)^n))."""
     rdt = x.real.dtype
     gdim = len(f_shape(L, s, nside))
-    P = _gamma_phases(N, -1, x.device, x.dtype) * (2 * np.pi / (2 * N - 1))
-    # fban[.., j, grid] = sum_k P[k, j] f[.., k, grid]
-    fban = torch.movedim(torch.tensordot(x, P, dims=([-gdim - 1], [0])), -1, -gdim - 1)
-    out = []
-    for j in range(2 * N - 1):
-        n = j - (N - 1)
-        fb = fban.select(-gdim - 1, j)
-        flm = _sph.forward(fb, L, -n, nside, s, L_lower=L_lower, precision=precision)
-        out.append(flm * _lnorm(L, n, L_lower, x.device, rdt, False))
-    return torch.stack(out, dim=-3)
+    if reality:
+        fban = torch.fft.rfft(x, dim=-gdim - 1, norm="backward") * (2 * np.pi / (2 * N - 1))
+    else:
+        P = _gamma_phases(N, -1, x.device, x.dtype) * (2 * np.pi / (2 * N - 1))
+        # fban[.., j, grid] = sum_k P[k, j] f[.., k, grid]
+        fban = torch.movedim(torch.tensordot(x, P, dims=([-gdim - 1], [0])), -1, -gdim - 1)
+    n0 = 0 if reality else -(N - 1)
+    out = {}
+    for n in range(n0, N):
+        fb = fban.select(-gdim - 1, n - n0)
+        if reality and n == 0:
+            fb = fb.real
+        flm = _sph.forward(fb, L, -n, nside, s, L_lower=L_lower, precision=precision,
+                           reality=reality and n == 0)
+        out[n] = flm * _lnorm(L, n, L_lower, x.device, rdt, False)
+    if reality:
+        sgn = torch.from_numpy((-1.0) ** np.abs(np.arange(-L + 1, L))).to(x.device, rdt)
+        for n in range(1, N):
+            out[-n] = torch.conj(torch.flip(out[n] * sgn * (-1) ** n, dims=[-1]))
+    return torch.stack([out[n] for n in range(-(N - 1), N)], dim=-3)
 
 
 def inverse(flmn, L: int, N: int, nside: int = None, sampling: str = "mw",
@@ -122,9 +140,8 @@ def inverse(flmn, L: int, N: int, nside: int = None, sampling: str = "mw",
     bs = tuple(x.shape[:-3])
     B = int(np.prod(bs)) if bs else 1
     if _needs_grad(x):
-        if reality:
-            raise NotImplementedError("gradients are available for complex transforms (reality=False)")
-        return _ret(_inverse_composed(x, L, N, nside, s, L_lower, precision), was_np, odev)
+        return _ret(_inverse_composed(x, L, N, nside, s, L_lower, precision, reality),
+                    was_np, odev)
     plan = _plan(x.device, L, N, nside, s, reality, L_lower, precision, B)
     out = torch.empty(bs + so3_f_shape(L, N, s, nside), dtype=rdt if reality else cdt,
                       device=x.device)
@@ -154,9 +171,8 @@ def forward(f, L: int, N: int, nside: int = None, sampling: str = "mw", method: 
     bs = tuple(x.shape[:-len(fs)])
     B = int(np.prod(bs)) if bs else 1
     if _needs_grad(x):
-        if reality:
-            raise NotImplementedError("gradients are available for complex transforms (reality=False)")
-        return _ret(_forward_composed(x, L, N, nside, s, L_lower, precision), was_np, odev)
+        return _ret(_forward_composed(x, L, N, nside, s, L_lower, precision, reality),
+                    was_np, odev)
     plan = _plan(x.device, L, N, nside, s, reality, L_lower, precision, B)
     out = torch.empty(bs + flmn_shape(L, N), dtype=cdt, device=x.device)
     ws = plan.workspace(True)
