@@ -29,6 +29,17 @@
 
 namespace s2b {
 
+// n consecutive values from 16-byte aligned shared memory by 16-byte loads
+template <typename V, int N>
+__device__ __forceinline__ void ld_vec16(V (&o)[N], const V* src) {
+  static_assert((N * sizeof(V)) % 16 == 0, "whole 16-byte vectors");
+  constexpr int NV = N * (int)sizeof(V) / 16;
+  uint4 t[NV];
+#pragma unroll
+  for (int i = 0; i < NV; ++i) t[i] = reinterpret_cast<const uint4*>(src)[i];
+  __builtin_memcpy(o, t, sizeof(t));
+}
+
 template <typename Real, bool DUAL, int T, int W, int R, bool VST, bool SYM>
 struct Inv2Layout {
   using Acc = std::conditional_t<DUAL, typename Vec<Real>::t4, typename Vec<Real>::t2>;
@@ -247,10 +258,13 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
     }                                                                                   \
     _Pragma("unroll") for (int x = 1; x >= 0; --x) {                                    \
       if (m <= Mb[x]) {                                                                 \
+        /* the warp's 8 h values of the row: 16-byte broadcast loads */                  \
+        Real hv[K / 2];                                                                 \
+        ld_vec16(hv, hS + (x * R + srow) * kFwdBlock);                                  \
         _Pragma("unroll") for (int kk = 0; kk < K / 2; ++kk) {                          \
           const int k = x * (K / 2) + kk;                                               \
           const int so = (x * R + srow) * kFwdBlock + kk;                               \
-          const Real h = hS[so];                                                        \
+          const Real h = hv[kk];                                                        \
           const Acc f = fS[so];                                                         \
           _Pragma("unroll") for (int i = 0; i < T; ++i) {                               \
             acc_fma(a[SYM ? (kk & 1) : x][i], CUR[k][i], f);                            \

@@ -271,11 +271,34 @@ static int ilog2(int x) {
   return r;
 }
 
+// Twiddle table of the register engine for M = 2^logM (the layout s2b_fft_reg.h reads):
+// the first DIF pass (NS0 stages, groups based at r < q0 = M / 2^NS0), rows k < NS0 of
+// tw[r 2^k]; then each radix-16 pass with smallest span q = 2^lq, lq = 4 (NMID - 1) down to 0,
+// rows k < 4 of tw[r 2^(logM - 4 - lq + k)] for r < q. tw[k] = exp(-2 pi i k / M).
+static std::vector<cd> reg_twiddles(int logM) {
+  const int M = 1 << logM;
+  const int ns0 = (logM & 3) ? (logM & 3) : 4;
+  const int nmid = (logM - ns0) / 4;
+  auto w = [&](long k) { return std::polar(1.0, -2.0 * kPi * (double)k / M); };
+  std::vector<cd> t;
+  const int q0 = M >> ns0;
+  for (int k = 0; k < ns0; ++k)
+    for (int r = 0; r < q0; ++r) t.push_back(w((long)r << k));
+  for (int p = 0; p < nmid; ++p) {
+    const int lq = 4 * (nmid - 1 - p);
+    const int sh = logM - 4 - lq;
+    for (int k = 0; k < 4; ++k)
+      for (int r = 0; r < (1 << lq); ++r) t.push_back(w(((long)r << sh) << k));
+  }
+  return t;
+}
+
 struct FFTBuild {
   std::vector<FFTDesc> descs;
-  std::vector<cd> tw, chirp, bf;
+  std::vector<cd> tw, chirp, bf, rtw, rbf;
   std::map<int, int> by_n;       // n -> desc index
   std::map<int, long> tw_by_M;   // M -> tw offset
+  std::map<int, long> rtw_by_M;  // M -> register-engine twiddle offset
   int maxM = 1;
 
   int add(int n) {
@@ -299,6 +322,20 @@ struct FFTBuild {
       d.tw_off = off;
     } else {
       d.tw_off = tt->second;
+    }
+    d.rtw_off = -1;
+    d.rbf_off = -1;
+    const bool reg = d.logM >= 10 && d.logM <= 13;
+    if (reg) {
+      auto rt = rtw_by_M.find(d.M);
+      if (rt == rtw_by_M.end()) {
+        d.rtw_off = (long)rtw.size();
+        const std::vector<cd> t = reg_twiddles(d.logM);
+        rtw.insert(rtw.end(), t.begin(), t.end());
+        rtw_by_M[d.M] = d.rtw_off;
+      } else {
+        d.rtw_off = rt->second;
+      }
     }
     if (d.bluestein) {
       d.chirp_off = (long)chirp.size();
@@ -325,6 +362,14 @@ struct FFTBuild {
         br[rv] = b[k] / (double)d.M;
       }
       bf.insert(bf.end(), br.begin(), br.end());
+      if (reg) {  // position 16 j + a at [a T + j]
+        const int T = d.M / 16;
+        d.rbf_off = (long)rbf.size();
+        std::vector<cd> rb(d.M);
+        for (int j = 0; j < T; ++j)
+          for (int a = 0; a < 16; ++a) rb[(size_t)a * T + j] = br[16 * j + a];
+        rbf.insert(rbf.end(), rb.begin(), rb.end());
+      }
     }
     maxM = std::max(maxM, d.M);
     const int idx = (int)descs.size();
@@ -385,6 +430,8 @@ struct s2b_plan {
   void* tw = nullptr;
   void* chirp = nullptr;
   void* bf = nullptr;
+  void* rtw = nullptr;  // register-engine twiddles and filters
+  void* rbf = nullptr;
   int row_desc = 0, col_d1 = 0, col_d2 = 0, maxM = 2, M1 = 2, M2 = 2;
   void* col_ph = nullptr;  // column chain: chirp * half-sample phase / n1 per 4L-bin
   // start tables of the inverse rings (inverse and its adjoint), ring -> column map of the
@@ -877,6 +924,8 @@ static int build_plan(s2b_plan* p) {
   if ((rc = upload_complex(p, &p->tw, fb.tw))) return rc;
   if ((rc = upload_complex(p, &p->chirp, fb.chirp))) return rc;
   if ((rc = upload_complex(p, &p->bf, fb.bf))) return rc;
+  if (!fb.rtw.empty() && (rc = upload_complex(p, &p->rtw, fb.rtw))) return rc;
+  if (!fb.rbf.empty() && (rc = upload_complex(p, &p->rbf, fb.rbf))) return rc;
   if (p->fwd_mode != 0) {
     // factor applied to theta-DFT bin pp (stored at k = pp mod 4L) before the
     // inverse 4L DFT: Bluestein output chirp, MW half-sample shift exp(-i pp pi/(2L-1)),
@@ -990,6 +1039,8 @@ static FFTTables<Real> tables(const s2b_plan* p) {
   t.tw = reinterpret_cast<const typename FFTTables<Real>::R2*>(p->tw);
   t.chirp = reinterpret_cast<const typename FFTTables<Real>::R2*>(p->chirp);
   t.bfilt = reinterpret_cast<const typename FFTTables<Real>::R2*>(p->bf);
+  t.rtw = reinterpret_cast<const typename FFTTables<Real>::R2*>(p->rtw);
+  t.rbf = reinterpret_cast<const typename FFTTables<Real>::R2*>(p->rbf);
   return t;
 }
 

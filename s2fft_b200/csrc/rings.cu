@@ -41,12 +41,12 @@ __device__ __forceinline__ void reg_dft(typename C2<Real>::t* buf, const FFTDesc
   using R2 = typename C2<Real>::t;
   using RF = RegFFT<LOGM, NBUF>;
   const int j = threadIdx.x;
-  const R2* tw = tb.tw + d.tw_off;
+  const R2* tw = tb.rtw + d.rtw_off;
   int ping = 0;
   R2 x[16];
   if (d.bluestein) {
     const R2* __restrict__ ch = tb.chirp + d.chirp_off;
-    const R2* __restrict__ bf = tb.bfilt + d.bf_off;
+    const R2* __restrict__ bf = tb.rbf + d.rbf_off;  // position 16 j + a at [a T + j]
 #pragma unroll
     for (int a = 0; a < 16; ++a) {
       const int k = j + RF::T * a;
@@ -60,7 +60,7 @@ __device__ __forceinline__ void reg_dft(typename C2<Real>::t* buf, const FFTDesc
     }
     RF::dif(x, buf, tw, false, ping);
 #pragma unroll
-    for (int a = 0; a < 16; ++a) x[a] = cmul(x[a], bf[RF::point(j, a, 0)]);
+    for (int a = 0; a < 16; ++a) x[a] = cmul(x[a], bf[a * RF::T + j]);
     RF::dit(x, buf, tw, true, ping);
     if (sync_emit) __syncthreads();
 #pragma unroll
@@ -645,25 +645,26 @@ static int fft_threads(int M) {
 
 // Register engine for one working length 2^LOGM: 10 <= LOGM <= 13 (1024 .. 8192 points; in
 // double up to 4096, where 16 points of a thread still fit the register file).
-static bool g_reg_engine = false;  // register engine on (pending validation)
-
 template <typename Real>
 static int reg_logm(int M) {
-  if (!g_reg_engine) return 0;
   const int top = sizeof(Real) == 4 ? 13 : 12;
   for (int lg = 10; lg <= top; ++lg)
     if (M == (1 << lg)) return lg;
   return 0;
 }
-static constexpr int kRegBufs = 1;  // exchange buffers of the register engine
+static constexpr int kRegBufs = 1;      // exchange buffers of the register engine
+static constexpr int kRegCarveout = 50;  // shared-memory share of L1 for it (percent)
 
+// carveout: the percentage of the unified L1 / shared memory given to shared memory. The
+// shared-memory passes want all of it (occupancy); the register engine is held to two or
+// three CTAs per SM by its registers and reads its twiddle, chirp and filter tables
+// through L1, so it keeps half for L1.
 template <typename Real, typename Kernel, typename Params>
 static cudaError_t launch_fft_kernel(Kernel k, dim3 grid, int threads, size_t smem,
-                                     const Params& p, cudaStream_t s) {
+                                     const Params& p, cudaStream_t s, int carveout = 100) {
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
-                           cudaSharedmemCarveoutMaxShared);
+  e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, carveout);
   if (e != cudaSuccess) return e;
   k<<<grid, threads, smem, s>>>(p);
   return cudaGetLastError();
@@ -687,10 +688,10 @@ cudaError_t launch_inv_rows(const RowsParams<Real>& p, int nrings, int batch, in
   using R2 = typename C2<Real>::t;
   const dim3 grid(nrings, batch);
   switch (rows_reg_logm(p, maxM)) {
-    case 10: return launch_fft_kernel<Real>(inv_rows_kernel<Real, 10, kRegBufs>, grid, 64, reg_smem<Real, 10>(0), p, s);
-    case 11: return launch_fft_kernel<Real>(inv_rows_kernel<Real, 11, kRegBufs>, grid, 128, reg_smem<Real, 11>(0), p, s);
-    case 12: return launch_fft_kernel<Real>(inv_rows_kernel<Real, 12, kRegBufs>, grid, 256, reg_smem<Real, 12>(0), p, s);
-    case 13: return launch_fft_kernel<Real>(inv_rows_kernel<Real, 13, kRegBufs>, grid, 512, reg_smem<Real, 13>(0), p, s);
+    case 10: return launch_fft_kernel<Real>(inv_rows_kernel<Real, 10, kRegBufs>, grid, 64, reg_smem<Real, 10>(0), p, s, kRegCarveout);
+    case 11: return launch_fft_kernel<Real>(inv_rows_kernel<Real, 11, kRegBufs>, grid, 128, reg_smem<Real, 11>(0), p, s, kRegCarveout);
+    case 12: return launch_fft_kernel<Real>(inv_rows_kernel<Real, 12, kRegBufs>, grid, 256, reg_smem<Real, 12>(0), p, s, kRegCarveout);
+    case 13: return launch_fft_kernel<Real>(inv_rows_kernel<Real, 13, kRegBufs>, grid, 512, reg_smem<Real, 13>(0), p, s, kRegCarveout);
     default: break;
   }
   const size_t smem = (size_t)padded_len(maxM) * sizeof(R2);
@@ -703,10 +704,10 @@ cudaError_t launch_fwd_rows(const RowsParams<Real>& p, int nrings, int batch, in
   using R2 = typename C2<Real>::t;
   const dim3 grid(nrings, batch);
   switch (rows_reg_logm(p, maxM)) {
-    case 10: return launch_fft_kernel<Real>(fwd_rows_kernel<Real, 10, kRegBufs>, grid, 64, reg_smem<Real, 10>(0), p, s);
-    case 11: return launch_fft_kernel<Real>(fwd_rows_kernel<Real, 11, kRegBufs>, grid, 128, reg_smem<Real, 11>(0), p, s);
-    case 12: return launch_fft_kernel<Real>(fwd_rows_kernel<Real, 12, kRegBufs>, grid, 256, reg_smem<Real, 12>(0), p, s);
-    case 13: return launch_fft_kernel<Real>(fwd_rows_kernel<Real, 13, kRegBufs>, grid, 512, reg_smem<Real, 13>(0), p, s);
+    case 10: return launch_fft_kernel<Real>(fwd_rows_kernel<Real, 10, kRegBufs>, grid, 64, reg_smem<Real, 10>(0), p, s, kRegCarveout);
+    case 11: return launch_fft_kernel<Real>(fwd_rows_kernel<Real, 11, kRegBufs>, grid, 128, reg_smem<Real, 11>(0), p, s, kRegCarveout);
+    case 12: return launch_fft_kernel<Real>(fwd_rows_kernel<Real, 12, kRegBufs>, grid, 256, reg_smem<Real, 12>(0), p, s, kRegCarveout);
+    case 13: return launch_fft_kernel<Real>(fwd_rows_kernel<Real, 13, kRegBufs>, grid, 512, reg_smem<Real, 13>(0), p, s, kRegCarveout);
     default: break;
   }
   const size_t smem = (size_t)padded_len(maxM) * sizeof(R2);
@@ -722,10 +723,10 @@ cudaError_t launch_mw_cols(const ColsParams<Real>& p, int ncm, int batch, int M1
   const int lg = (M1 == M2 && p.d2_pow2) ? reg_logm<Real>(M1) : 0;
   const int extra = 2 * p.L;
   switch (lg) {
-    case 10: return launch_fft_kernel<Real>(mw_cols_kernel<Real, 10, kRegBufs>, grid, 64, reg_smem<Real, 10>(extra), p, s);
-    case 11: return launch_fft_kernel<Real>(mw_cols_kernel<Real, 11, kRegBufs>, grid, 128, reg_smem<Real, 11>(extra), p, s);
-    case 12: return launch_fft_kernel<Real>(mw_cols_kernel<Real, 12, kRegBufs>, grid, 256, reg_smem<Real, 12>(extra), p, s);
-    case 13: return launch_fft_kernel<Real>(mw_cols_kernel<Real, 13, kRegBufs>, grid, 512, reg_smem<Real, 13>(extra), p, s);
+    case 10: return launch_fft_kernel<Real>(mw_cols_kernel<Real, 10, kRegBufs>, grid, 64, reg_smem<Real, 10>(extra), p, s, kRegCarveout);
+    case 11: return launch_fft_kernel<Real>(mw_cols_kernel<Real, 11, kRegBufs>, grid, 128, reg_smem<Real, 11>(extra), p, s, kRegCarveout);
+    case 12: return launch_fft_kernel<Real>(mw_cols_kernel<Real, 12, kRegBufs>, grid, 256, reg_smem<Real, 12>(extra), p, s, kRegCarveout);
+    case 13: return launch_fft_kernel<Real>(mw_cols_kernel<Real, 13, kRegBufs>, grid, 512, reg_smem<Real, 13>(extra), p, s, kRegCarveout);
     default: break;
   }
   // one DFT buffer plus the 2L bins carried between the two transforms

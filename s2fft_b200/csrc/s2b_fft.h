@@ -17,6 +17,11 @@ struct FFTDesc {
   long tw_off;    // offset of exp(-2 pi i k / M), k < M/2
   long chirp_off; // Bluestein: exp(-i pi k^2 / n), k < n
   long bf_off;    // Bluestein: FFT_M(conj chirp, wrapped) / M, bit-reversed order
+  // register engine (s2b_fft_reg.h; M = 2^10 .. 2^13, else -1): the twiddles of every pass in
+  // the order its threads read them, and the Bluestein filter at [a T + j] for the position
+  // 16 j + a that thread j holds in register a (T = M / 16)
+  long rtw_off;
+  long rbf_off;
 };
 
 template <typename Real>
@@ -25,6 +30,8 @@ struct FFTTables {
   const R2* tw;
   const R2* chirp;
   const R2* bfilt;
+  const R2* rtw = nullptr;   // register-engine twiddles (FFTDesc::rtw_off)
+  const R2* rbf = nullptr;   // register-engine Bluestein filters (FFTDesc::rbf_off)
 };
 
 enum RowsMode { FWD_TO_SPECTRA = 0, FWD_TO_COLS = 1, FWD_TO_RAW = 2 };

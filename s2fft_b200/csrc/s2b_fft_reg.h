@@ -87,19 +87,19 @@ __device__ __forceinline__ void reg_stage(R2* x, const R2 (&bp)[NS], bool inv) {
 }
 
 // NS fused radix-2 stages on the 2^NS points x[ST * a] (a < 2^NS) of one group whose base
-// point is r modulo its smallest span q; sh = log2(M / (2^NS q)). tw[k] = exp(-2 pi i k / M),
-// k < M/2 (conjugated when inv). DIF: spans decreasing; DIT: increasing. The stage of span
-// s q pairs points s apart and multiplies by b^(2^NS / (2 s)) exp(-i pi k / s), k the
-// position within the pair block, with b = tw[r 2^sh] (the same derivation as fft_pass).
+// point is r modulo its smallest span q. tws[k * stride] = b^(2^k), k < NS, with
+// b = exp(-2 pi i r 2^sh / M), sh = log2(M / (2^NS q)) (conjugated when inv): the twiddles
+// of the group, read from the register-engine table (FFTDesc::rtw_off), where consecutive
+// threads read consecutive entries. DIF: spans decreasing; DIT: increasing. The stage of
+// span s q pairs points s apart and multiplies by b^(2^NS / (2 s)) exp(-i pi k / s), k the
+// position within the pair block (the derivation of fft_pass in s2b_fft_dev.h).
 template <int NS, bool DIF, int ST, typename R2>
-__device__ __forceinline__ void reg_stages(R2* x, int r, int sh, const R2* __restrict__ tw,
+__device__ __forceinline__ void reg_stages(R2* x, const R2* __restrict__ tws, int stride,
                                            bool inv) {
-  // b^(2^k) = tw[r 2^(sh + k)]: every twiddle of the group is one of these times a
-  // constant root of unity of order <= 16
   R2 bp[NS];
 #pragma unroll
   for (int k = 0; k < NS; ++k) {
-    bp[k] = tw[(r << sh) << k];
+    bp[k] = tws[k * stride];
     if (inv) bp[k].y = -bp[k].y;
   }
   reg_stage<NS, DIF, ST, 0>(x, bp, inv);
@@ -144,26 +144,36 @@ struct RegFFT {
     ping ^= 1;
   }
 
-  template <typename R2>
-  __device__ __forceinline__ static void first_dif(R2 (&x)[16], const R2* tw, bool inv) {
-    constexpr int G = 1 << (4 - NS0);  // groups per thread, register stride G
-    const int j = threadIdx.x;
-#pragma unroll
-    for (int g = 0; g < G; ++g)
-      reg_stages<NS0, true, G>(x + g, j + T * g, 0, tw, inv);  // q = M / 2^NS0: sh = 0
+  // the twiddle table (FFTDesc::rtw_off): the first pass's rows (q0 entries each), then the
+  // radix-16 passes in DIF order (lq decreasing), 4 rows of 2^lq entries each
+  static constexpr int Q0 = M >> NS0;
+  __host__ __device__ static constexpr int mid_off(int lq) {
+    int off = NS0 * Q0;
+    for (int l = 4 * (NMID - 1); l > lq; l -= 4) off += 4 << l;
+    return off;
   }
+
+  // the first DIF / last DIT pass (spans M/2 .. M/2^NS0) on the points j + T a; groups
+  // based at r = j + T g, g < G (the register stride)
   template <typename R2>
-  __device__ __forceinline__ static void last_dit(R2 (&x)[16], const R2* tw, bool inv) {
+  __device__ __forceinline__ static void first_dif(R2 (&x)[16], const R2* rtw, bool inv) {
     constexpr int G = 1 << (4 - NS0);
     const int j = threadIdx.x;
 #pragma unroll
-    for (int g = 0; g < G; ++g) reg_stages<NS0, false, G>(x + g, j + T * g, 0, tw, inv);
+    for (int g = 0; g < G; ++g) reg_stages<NS0, true, G>(x + g, rtw + j + T * g, Q0, inv);
+  }
+  template <typename R2>
+  __device__ __forceinline__ static void last_dit(R2 (&x)[16], const R2* rtw, bool inv) {
+    constexpr int G = 1 << (4 - NS0);
+    const int j = threadIdx.x;
+#pragma unroll
+    for (int g = 0; g < G; ++g) reg_stages<NS0, false, G>(x + g, rtw + j + T * g, Q0, inv);
   }
   // a radix-16 pass with smallest span 2^lq
   template <bool DIF, typename R2>
-  __device__ __forceinline__ static void mid(R2 (&x)[16], int lq, const R2* tw, bool inv) {
+  __device__ __forceinline__ static void mid(R2 (&x)[16], int lq, const R2* rtw, bool inv) {
     const int r = threadIdx.x & ((1 << lq) - 1);
-    reg_stages<4, DIF, 1>(x, r, LOGM - 4 - lq, tw, inv);
+    reg_stages<4, DIF, 1>(x, rtw + mid_off(lq) + r, 1 << lq, inv);
   }
 
   // DIF: x holds points j + T a in natural order; on return x[a] holds the bit-reversed
