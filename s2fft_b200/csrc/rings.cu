@@ -151,17 +151,24 @@ __global__ void __launch_bounds__(LOGM ? (1 << LOGM) / 16 : 512, (sizeof(Real) =
   };
   const Real scale = (Real)(p.scale * (p.weights ? p.weights[t] : 1.0));
   if constexpr (LOGM > 0) {
+    // uniform rings without phases or aliasing (n >= ncol): X_k is the one C_m with
+    // m = k or k - n
+    auto load_eq = [&](int k) -> R2 {
+      const int m = k > mhi ? k - n : k;
+      if (m < mlo) return czero<R2>();
+      return (mirror && m < 0) ? cconj(row[L - 1 - m + p.mo]) : row[L - 1 + m + p.mo];
+    };
     R2* outc = reinterpret_cast<R2*>(p.out) + (size_t)b * p.out_batch_stride + p.ring_off[t];
     Real* outr = reinterpret_cast<Real*>(p.out) + (size_t)b * p.out_batch_stride + p.ring_off[t];
     if (d.bluestein) {  // outputs in natural order: coalesced stores from the registers
-      reg_dft<Real, LOGM, NBUF>(s, d, p.tb, true, true, false, load, [&](int k, R2 v) {
+      reg_dft<Real, LOGM, NBUF>(s, d, p.tb, true, true, false, load_eq, [&](int k, R2 v) {
         if (p.real_out)
           outr[k] = v.x * scale;
         else
           outc[k] = cscale(v, scale);
       });
     } else {  // bit-reversed positions: through shared memory to natural order
-      reg_dft<Real, LOGM, NBUF>(s, d, p.tb, true, true, true, load,
+      reg_dft<Real, LOGM, NBUF>(s, d, p.tb, true, true, true, load_eq,
                                 [&](int k, R2 v) { s[ridx(k)] = v; });
       __syncthreads();
       for (int k = threadIdx.x; k < n; k += blockDim.x) {
@@ -171,17 +178,17 @@ __global__ void __launch_bounds__(LOGM ? (1 << LOGM) / 16 : 512, (sizeof(Real) =
           outc[k] = cscale(s[ridx(k)], scale);
       }
     }
-    return;
-  }
-  dft_run<Real>(s, d, p.tb, true, load);
-  if (p.real_out) {
-    Real* out = reinterpret_cast<Real*>(p.out) + (size_t)b * p.out_batch_stride + p.ring_off[t];
-    for (int j = threadIdx.x; j < n; j += blockDim.x)
-      out[j] = dft_get<Real>(s, d, p.tb, true, j).x * scale;
   } else {
-    R2* out = reinterpret_cast<R2*>(p.out) + (size_t)b * p.out_batch_stride + p.ring_off[t];
-    for (int j = threadIdx.x; j < n; j += blockDim.x)
-      out[j] = cscale(dft_get<Real>(s, d, p.tb, true, j), scale);
+    dft_run<Real>(s, d, p.tb, true, load);
+    if (p.real_out) {
+      Real* out = reinterpret_cast<Real*>(p.out) + (size_t)b * p.out_batch_stride + p.ring_off[t];
+      for (int j = threadIdx.x; j < n; j += blockDim.x)
+        out[j] = dft_get<Real>(s, d, p.tb, true, j).x * scale;
+    } else {
+      R2* out = reinterpret_cast<R2*>(p.out) + (size_t)b * p.out_batch_stride + p.ring_off[t];
+      for (int j = threadIdx.x; j < n; j += blockDim.x)
+        out[j] = cscale(dft_get<Real>(s, d, p.tb, true, j), scale);
+    }
   }
 }
 

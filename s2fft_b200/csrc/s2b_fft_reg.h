@@ -93,15 +93,29 @@ __device__ __forceinline__ void reg_stage(R2* x, const R2 (&bp)[NS], bool inv) {
 // threads read consecutive entries. DIF: spans decreasing; DIT: increasing. The stage of
 // span s q pairs points s apart and multiplies by b^(2^NS / (2 s)) exp(-i pi k / s), k the
 // position within the pair block (the derivation of fft_pass in s2b_fft_dev.h).
-template <int NS, bool DIF, int ST, typename R2>
-__device__ __forceinline__ void reg_stages(R2* x, const R2* __restrict__ tws, int stride,
-                                           bool inv) {
-  R2 bp[NS];
+// the twiddles b^(2^k) = tws[k * stride], k < NS, of one group (conjugated when inv)
+template <int NS, typename R2>
+__device__ __forceinline__ void reg_twiddles(R2 (&bp)[NS], const R2* __restrict__ tws, int stride,
+                                             bool inv) {
 #pragma unroll
   for (int k = 0; k < NS; ++k) {
     bp[k] = tws[k * stride];
     if (inv) bp[k].y = -bp[k].y;
   }
+}
+
+// NS fused radix-2 stages on the 2^NS points x[ST * a] (a < 2^NS) of one group whose base
+// point is r modulo its smallest span q. tws[k * stride] = b^(2^k), k < NS, with
+// b = exp(-2 pi i r 2^sh / M), sh = log2(M / (2^NS q)) (conjugated when inv): the twiddles
+// of the group, read from the register-engine table (FFTDesc::rtw_off), where consecutive
+// threads read consecutive entries. DIF: spans decreasing; DIT: increasing. The stage of
+// span s q pairs points s apart and multiplies by b^(2^NS / (2 s)) exp(-i pi k / s), k the
+// position within the pair block (the derivation of fft_pass in s2b_fft_dev.h).
+template <int NS, bool DIF, int ST, typename R2>
+__device__ __forceinline__ void reg_stages(R2* x, const R2* __restrict__ tws, int stride,
+                                           bool inv) {
+  R2 bp[NS];
+  reg_twiddles(bp, tws, stride, inv);
   reg_stage<NS, DIF, ST, 0>(x, bp, inv);
 }
 
@@ -153,40 +167,42 @@ struct RegFFT {
     return off;
   }
 
-  // the first DIF / last DIT pass (spans M/2 .. M/2^NS0) on the points j + T a; groups
-  // based at r = j + T g, g < G (the register stride)
+  // twiddles of the first DIF / last DIT pass for this thread's G groups
   template <typename R2>
-  __device__ __forceinline__ static void first_dif(R2 (&x)[16], const R2* rtw, bool inv) {
+  __device__ __forceinline__ static void first_tw(R2 (&bp)[1 << (4 - NS0)][NS0], const R2* rtw,
+                                                  bool inv) {
     constexpr int G = 1 << (4 - NS0);
-    const int j = threadIdx.x;
 #pragma unroll
-    for (int g = 0; g < G; ++g) reg_stages<NS0, true, G>(x + g, rtw + j + T * g, Q0, inv);
+    for (int g = 0; g < G; ++g) reg_twiddles(bp[g], rtw + threadIdx.x + T * g, Q0, inv);
   }
+  // twiddles of the radix-16 pass with smallest span 2^lq
   template <typename R2>
-  __device__ __forceinline__ static void last_dit(R2 (&x)[16], const R2* rtw, bool inv) {
-    constexpr int G = 1 << (4 - NS0);
-    const int j = threadIdx.x;
-#pragma unroll
-    for (int g = 0; g < G; ++g) reg_stages<NS0, false, G>(x + g, rtw + j + T * g, Q0, inv);
-  }
-  // a radix-16 pass with smallest span 2^lq
-  template <bool DIF, typename R2>
-  __device__ __forceinline__ static void mid(R2 (&x)[16], int lq, const R2* rtw, bool inv) {
-    const int r = threadIdx.x & ((1 << lq) - 1);
-    reg_stages<4, DIF, 1>(x, rtw + mid_off(lq) + r, 1 << lq, inv);
+  __device__ __forceinline__ static void mid_tw(R2 (&bp)[4], int lq, const R2* rtw, bool inv) {
+    reg_twiddles(bp, rtw + mid_off(lq) + (threadIdx.x & ((1 << lq) - 1)), 1 << lq, inv);
   }
 
   // DIF: x holds points j + T a in natural order; on return x[a] holds the bit-reversed
-  // position point(j, a, 0) (the layout of the last pass, smallest span 1).
+  // position point(j, a, 0) (the layout of the last pass, smallest span 1). The radix-16
+  // passes share one loop body (a compact instruction footprint), and each pass's
+  // twiddles are loaded before the barrier that precedes it.
   template <typename R2>
   __device__ __forceinline__ static void dif(R2 (&x)[16], R2* buf, const R2* tw, bool inv,
                                              int& ping) {
-    first_dif(x, tw, inv);
+    constexpr int G = 1 << (4 - NS0);
+    R2 b0[G][NS0], bp[4];
+    first_tw(b0, tw, inv);
+    mid_tw(bp, 4 * (NMID - 1), tw, inv);
 #pragma unroll
+    for (int g = 0; g < G; ++g) reg_stage<NS0, true, G, 0>(x + g, b0[g], inv);
+#pragma unroll 1
     for (int p = 0; p < NMID; ++p) {
       const int lq = 4 * (NMID - 1 - p);
       exchange(x, buf, ping, p == 0 ? -1 : lq + 4, lq);
-      mid<true>(x, lq, tw, inv);
+      R2 cur[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) cur[k] = bp[k];
+      if (p + 1 < NMID) mid_tw(bp, lq - 4, tw, inv);
+      reg_stage<4, true, 1, 0>(x, cur, inv);
     }
   }
   // DIT: x holds bit-reversed positions in dif's output layout; on return, natural order
@@ -194,13 +210,23 @@ struct RegFFT {
   template <typename R2>
   __device__ __forceinline__ static void dit(R2 (&x)[16], R2* buf, const R2* tw, bool inv,
                                              int& ping) {
-#pragma unroll
+    constexpr int G = 1 << (4 - NS0);
+    R2 bp[4];
+    mid_tw(bp, 0, tw, inv);
+#pragma unroll 1
     for (int p = 0; p < NMID; ++p) {
       if (p > 0) exchange(x, buf, ping, 4 * (p - 1), 4 * p);
-      mid<false>(x, 4 * p, tw, inv);
+      R2 cur[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) cur[k] = bp[k];
+      if (p + 1 < NMID) mid_tw(bp, 4 * (p + 1), tw, inv);
+      reg_stage<4, false, 1, 0>(x, cur, inv);
     }
+    R2 b0[G][NS0];
+    first_tw(b0, tw, inv);
     exchange(x, buf, ping, 4 * (NMID - 1), -1);
-    last_dit(x, tw, inv);
+#pragma unroll
+    for (int g = 0; g < G; ++g) reg_stage<NS0, false, G, 0>(x + g, b0[g], inv);
   }
 };
 
