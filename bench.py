@@ -443,7 +443,9 @@ def run_batched_precompute(torch, L=512, B=64, steps=5, warmup=2):
 
 def run_batched_uneven(torch, nmaps=256, steps=3, warmup=1, seed=4242):
     """256 maps, L uniform in {64..1024}, spin 0..3, sampling in {mw, mwss, dh, gl}, float32:
-    inverse + forward of every map, grouped, autotuned and replayed as one CUDA graph,
+    inverse + forward of every map, grouped, autotuned and replayed as one CUDA graph: the
+    latitudinal kernels of all groups in persistent launches, or every group's own chain of
+    launches on concurrent streams (each timed; the headline is the autotuner's pick),
     against the same maps run one call at a time."""
     import s2fft_b200
     from s2fft_b200.batch import BatchedSHT
@@ -454,9 +456,18 @@ def run_batched_uneven(torch, nmaps=256, steps=3, warmup=1, seed=4242):
     specs = [(int(rng.choice(Ls)), int(rng.integers(0, 4)), str(rng.choice(smps)))
              for _ in range(nmaps)]
     flms = [seeded_flm(rng, L, sp) for L, sp, _ in specs]
-    b = BatchedSHT(specs, precision="f32")
-    b.load(flms)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    ms_sched = {}
+    for sched in (True, False):  # each schedule forced, tuned and timed as a graph
+        bs = BatchedSHT(specs, precision="f32", persistent=sched)
+        bs.load(flms)
+        ms_sched["persistent" if sched else "streams"] = _time(torch, bs.run, steps, warmup,
+                                                               flush)
+        if sched:
+            waves = bs.batch_schedule
+        del bs
+    b = BatchedSHT(specs, precision="f32")  # the autotuner's pick
+    b.load(flms)
     ms_graph = _time(torch, b.run, steps, warmup, flush)
     xs = [torch.as_tensor(x).to("cuda", torch.complex64) for x in flms]
 
@@ -480,11 +491,15 @@ def run_batched_uneven(torch, nmaps=256, steps=3, warmup=1, seed=4242):
                         "inverse + forward",
             "groups": len(b.groups),
             "graph_maps_per_s": nmaps / (ms_graph * 1e-3), "graph_ms": ms_graph,
+            "schedule": b.schedule,
+            "schedule_maps_per_s": {k: nmaps / (v * 1e-3) for k, v in ms_sched.items()},
+            "persistent_waves_ctas_per_sm": list(waves),
+            "autotuner_ms": b.timings,
             "sequential_maps_per_s": nmaps / (ms_seq * 1e-3), "sequential_ms": ms_seq,
             "max_rel_err_vs_unbatched": worst, "max_rel_roundtrip_err": rt,
-            "tiles": {"forward_half": sum(g.tiles[0] for g in b.groups),
-                      "inverse_one_ring": sum(g.tiles[1] & 1 for g in b.groups),
-                      "inverse_segments": {str(n): sum(g.tiles[2] == n for g in b.groups)
+            "tiles": {"forward_half": sum(g.tuning[0] for g in b.groups),
+                      "inverse_one_ring": sum(g.tuning[1] & 1 for g in b.groups),
+                      "inverse_segments": {str(n): sum(g.tuning[2] == n for g in b.groups)
                                            for n in (1, 2, 4)}}}
 
 

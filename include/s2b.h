@@ -238,6 +238,37 @@ int s2b_plan_set_events(s2b_plan* plan, int forward, void* ev_begin, void* ev_en
 #define S2B_NOALLOC_SCRATCH_BYTES ((size_t)32 << 20)
 int s2b_inverse_noalloc(s2b_plan* plan, const void* flm, void* f, void* stream);
 
+/* Uneven batches: the spin transforms of several plans (different L, spin,
+ * sampling, nside, batch; one device and one precision) in one call. Entry k
+ * transforms with plans[k] exactly as s2b_inverse / s2b_forward would (same
+ * layouts, results and refinement iterations), from in[k] to out[k] with the
+ * workspace ws[k] of ws_bytes[k] >= s2b_workspace_size(plans[k], 0 or 1)
+ * bytes. The stages around the latitudinal kernels run per plan on a few
+ * streams the batch owns (forked from and joined back to `stream`); the
+ * latitudinal kernels of all entries run as persistent launches, one per
+ * kernel variant (spin 0 or not, tile shape), whose CTAs pull (plan, tile)
+ * items from a device counter. Stream-ordered and capturable in a CUDA graph
+ * like the single-plan calls; the batch object may not be used by two calls
+ * at once. The plans must outlive the batch. s2b_batch_create allocates the
+ * counters and creates the streams and events.
+ * No upstream counterpart: upstream transforms one (L, spin, sampling) per
+ * call (s2fft/transforms/spherical.py:21-109, 352-464); these are those calls,
+ * fused across entries. */
+typedef struct s2b_batch s2b_batch;
+int s2b_batch_create(s2b_plan* const* plans, int nplans, s2b_batch** batch);
+int s2b_batch_destroy(s2b_batch* batch);
+int s2b_batch_inverse(s2b_batch* batch, const void* const* flm, void* const* f,
+                      void* const* workspace, const size_t* ws_bytes, void* stream);
+int s2b_batch_forward(s2b_batch* batch, const void* const* f, void* const* flm,
+                      void* const* workspace, const size_t* ws_bytes, void* stream);
+/* Schedule of a batch's calls. key 0: waves (1 to 4; default 1). The entries are
+ * dealt round-robin into waves; the per-plan stages of one wave (ring FFTs, which
+ * are memory-bound) run on the batch's streams while the persistent latitudinal
+ * launches of the next wave run on `stream`. key 1: CTAs per SM of the persistent
+ * launches (0, the default: as many as fit), which leaves room on each SM for the
+ * overlapping stages. Results do not depend on either. */
+int s2b_batch_set_option(s2b_batch* batch, int key, int value);
+
 /* Rotation of spherical-harmonic coefficients by the Euler angles (alpha, beta, gamma):
  *   flm'[l, m] = exp(-i m alpha) sum_n d^l_{m,n}(beta) exp(-i n gamma) flm[l, n],
  * replaces s2fft.utils.rotation.rotate_flms (s2fft/utils/rotation.py:9-64). flm and out

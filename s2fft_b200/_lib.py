@@ -68,6 +68,11 @@ _SIGS = {
                        ctypes.c_size_t, ctypes.c_void_p],
     "s2b_plan_device": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)],
     "s2b_debug_set_plan_device": [ctypes.c_void_p, ctypes.c_int],
+    "s2b_batch_create": [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)],
+    "s2b_batch_destroy": [ctypes.c_void_p],
+    "s2b_batch_inverse": [ctypes.c_void_p] * 5 + [ctypes.c_void_p],
+    "s2b_batch_forward": [ctypes.c_void_p] * 5 + [ctypes.c_void_p],
+    "s2b_batch_set_option": [ctypes.c_void_p, ctypes.c_int, ctypes.c_int],
 }
 
 
@@ -133,6 +138,48 @@ class Plan:
         try:
             if getattr(self, "ptr", None) and self.ptr.value:
                 lib().s2b_plan_destroy(self.ptr)
+        except Exception:
+            pass
+
+
+class Batch:
+    """An uneven batch of spin plans (s2b_batch_*): entry k transforms with plans[k]."""
+
+    def __init__(self, plans):
+        self.plans = list(plans)  # the plans must outlive the batch
+        arr = (ctypes.c_void_p * len(self.plans))(*[p.ptr.value for p in self.plans])
+        ptr = ctypes.c_void_p()
+        with torch.cuda.device(self.plans[0].device):
+            check(lib().s2b_batch_create(arr, len(self.plans), ctypes.byref(ptr)))
+        self.ptr = ptr
+
+    @staticmethod
+    def _ptrs(tensors):
+        return (ctypes.c_void_p * len(tensors))(*[t.data_ptr() for t in tensors])
+
+    def _call(self, fn, ins, outs, ws, stream):
+        n = len(self.plans)
+        if not (len(ins) == len(outs) == len(ws) == n):
+            raise ValueError(f"a batch of {n} entries needs {n} inputs, outputs and workspaces")
+        sizes = (ctypes.c_size_t * n)(*[w.numel() for w in ws])
+        check(fn(self.ptr, self._ptrs(ins), self._ptrs(outs), self._ptrs(ws), sizes,
+                 ctypes.c_void_p(stream.cuda_stream)))
+
+    def set_schedule(self, waves=1, ctas_per_sm=0):
+        """Waves of the staged execution and CTAs per SM of the persistent launches."""
+        check(lib().s2b_batch_set_option(self.ptr, 0, int(waves)))
+        check(lib().s2b_batch_set_option(self.ptr, 1, int(ctas_per_sm)))
+
+    def inverse(self, flms, fs, ws, stream):
+        self._call(lib().s2b_batch_inverse, flms, fs, ws, stream)
+
+    def forward(self, fs, flms, ws, stream):
+        self._call(lib().s2b_batch_forward, fs, flms, ws, stream)
+
+    def __del__(self):
+        try:
+            if getattr(self, "ptr", None) and self.ptr.value:
+                lib().s2b_batch_destroy(self.ptr)
         except Exception:
             pass
 

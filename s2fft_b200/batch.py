@@ -3,15 +3,33 @@
 A workload mixes band-limits, spins and samplings. Maps that share
 ``(L, spin, sampling, nside)`` form a group: one plan with ``batch`` equal to
 the group size, so each kernel of the chain processes the whole group in one
-launch. Groups run concurrently on several CUDA streams (largest first), the
-whole inverse + forward of all groups is captured once in a CUDA graph and
-replayed on every call, and an autotuner picks each group's latitudinal launch
-shapes (``s2b_plan_set_tuning``: tiles, inverse segments along m) by timing them
-on the group itself.
+launch. Two schedules:
 
-Only the host-side scheduling is new here; every transform runs the same
-kernels as :func:`s2fft_b200.inverse` / :func:`s2fft_b200.forward`, so each
-map's result equals the unbatched call on that map.
+* ``persistent=True``: all groups form one uneven batch
+  (``s2b_batch_inverse`` / ``s2b_batch_forward``). The ring FFTs and the other
+  per-group stages run on the batch's streams, and the latitudinal kernels of
+  all groups -- the O(L^3) part -- run as persistent launches, one per kernel
+  variant (spin 0 or not, tile shape), whose CTAs pull (group, tile) items
+  from a device work counter, so small groups fill the SMs that the large
+  ones leave idle in their tails. Waves (``s2b_batch_set_option``) let the
+  ring FFTs of one part of the batch overlap the persistent launches of the
+  next. The autotuner picks tile shapes and segment counts per class of
+  groups (spin 0, spin != 0) and the waves / CTAs per SM, by timing the whole
+  batch.
+* ``persistent=False``: every group runs its own chain of launches; groups run
+  concurrently on several CUDA streams (largest first), and the autotuner
+  picks each group's launch shapes (``s2b_plan_set_tuning``: tiles, inverse
+  segments along m) by timing them on the group itself.
+* ``persistent=None`` (default): the autotuner times both and keeps the
+  faster schedule (``self.schedule``, ``self.timings``).
+
+Either way the whole inverse + forward of all groups is captured once in a
+CUDA graph and replayed on every call.
+
+Only the scheduling is new here: every transform runs the same stages as
+:func:`s2fft_b200.inverse` / :func:`s2fft_b200.forward` (the persistent launches
+run the same per-tile code as the per-plan latitudinal kernels), so each map's
+result equals the unbatched call on that map.
 
 Example::
 
@@ -47,7 +65,10 @@ class _Group:
     flm_out: torch.Tensor = None
     ws_inv: torch.Tensor = None
     ws_fwd: torch.Tensor = None
-    tiles: tuple = (0, 0, 1)  # (forward tile, inverse tile, inverse segments along m)
+    # s2b_plan_set_tuning values (forward tile, inverse tile, inverse segments, forward
+    # segments) in force, and the tuned ones per schedule
+    tuning: tuple = None
+    tuned: dict = field(default_factory=dict)
 
     def work(self):
         nth = f_shape(self.L, self.sampling, self.nside)[0] if self.sampling != "healpix" \
@@ -58,7 +79,7 @@ class _Group:
 class BatchedSHT:
     """Inverse followed by forward spin transform of many maps of uneven size."""
 
-    def __init__(self, specs, precision="f32", streams=4, tune=True, graph=True):
+    def __init__(self, specs, precision="f32", streams=4, tune=True, graph=True, persistent=None):
         self.device = _device()
         self.precision = precision
         self.cdt, _ = _dtypes(precision)
@@ -91,6 +112,12 @@ class BatchedSHT:
             g.ws_inv = g.plan.workspace(0)
             g.ws_fwd = g.plan.workspace(1)
         self.streams = [torch.cuda.Stream(self.device) for _ in range(max(1, streams))]
+        # persistent: True / False force a schedule, None lets the autotuner pick one
+        self.requested = persistent
+        self.batch = _lib.Batch([g.plan for g in self.groups]) if persistent is not False else None
+        self.schedule = "persistent" if self.batch is not None else "streams"
+        self.batch_schedule = (1, 0)
+        self.timings = {}
         self.graph = None
         if tune:
             self.tune()
@@ -122,7 +149,17 @@ class BatchedSHT:
         _lib.check(lib.s2b_forward(g.plan.ptr, g.f.data_ptr(), g.flm_out.data_ptr(),
                                    g.ws_fwd.data_ptr(), g.ws_fwd.numel(), h))
 
-    def _run_all(self):
+    def _batch_inverse(self, stream):
+        gs = self.groups
+        self.batch.inverse([g.flm_in for g in gs], [g.f for g in gs], [g.ws_inv for g in gs],
+                           stream)
+
+    def _batch_forward(self, stream):
+        gs = self.groups
+        self.batch.forward([g.f for g in gs], [g.flm_out for g in gs], [g.ws_fwd for g in gs],
+                           stream)
+
+    def _run_streams(self):
         main = torch.cuda.current_stream(self.device)
         for s in self.streams:
             s.wait_stream(main)
@@ -130,6 +167,14 @@ class BatchedSHT:
             self._launch(g, self.streams[k % len(self.streams)])
         for s in self.streams:
             main.wait_stream(s)
+
+    def _run_all(self):
+        if self.schedule == "persistent":
+            main = torch.cuda.current_stream(self.device)
+            self._batch_inverse(main)
+            self._batch_forward(main)
+        else:
+            self._run_streams()
 
     def run(self):
         """Inverse then forward transform of every map (graph replay when captured)."""
@@ -140,6 +185,7 @@ class BatchedSHT:
 
     def capture(self):
         """Capture the launches of all groups in one CUDA graph (after one eager warm-up)."""
+        self.graph = None
         self._run_all()
         torch.cuda.synchronize(self.device)
         self.graph = torch.cuda.CUDAGraph()
@@ -148,25 +194,34 @@ class BatchedSHT:
         torch.cuda.synchronize(self.device)
 
     # -- autotuner --------------------------------------------------------------------
-    def tune(self, reps=3):
-        """Per group, time the launch shapes of the inverse and the forward latitudinal
-        kernels (tile x segments along m; forward segments apply to the equator-symmetric
-        forward) on the group itself and keep the fastest."""
-        lib = _lib.lib()
+    # s2b_plan_set_tuning keys: 0 forward tile, 1 inverse tile, 2 inverse segments along m,
+    # 3 forward segments along m (equator-symmetric forward)
+    _INV = [(t, n) for t in (2, 3) for n in (2, 4)]  # (inverse tile, segments)
+    _FWD = [(v, n) for v in (0, 1) for n in (2, 4)]  # (forward tile, segments)
+    _SCHED = [(1, 0), (2, 0), (2, 2), (3, 2)]  # (waves, CTAs per SM) of the persistent batch
+
+    def _timed(self, fn, reps):
         stream = torch.cuda.current_stream(self.device)
-        h = ctypes.c_void_p(stream.cuda_stream)
-
-        def timed(fn):
+        fn()
+        e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
+        e0.record(stream)
+        for _ in range(reps):
             fn()
-            e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
-            e0.record(stream)
-            for _ in range(reps):
-                fn()
-            e1.record(stream)
-            e1.synchronize()
-            return e0.elapsed_time(e1)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
 
-        inv = [(t, n) for t in (2, 3) for n in (2, 4)]  # (tile, segments along m)
+    @staticmethod
+    def _set(g, tuning):
+        lib = _lib.lib()
+        for key, v in enumerate(tuning):
+            _lib.check(lib.s2b_plan_set_tuning(g.plan.ptr, key, v))
+        g.tuning = tuple(tuning)
+
+    def _tune_streams(self, reps):
+        """Per group, the inverse and forward shapes timed on the group itself."""
+        lib = _lib.lib()
+        h = ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
         for g in self.groups:
             def call_inv():
                 _lib.check(lib.s2b_inverse(g.plan.ptr, g.flm_in.data_ptr(), g.f.data_ptr(),
@@ -176,27 +231,91 @@ class BatchedSHT:
                 _lib.check(lib.s2b_forward(g.plan.ptr, g.f.data_ptr(), g.flm_out.data_ptr(),
                                            g.ws_fwd.data_ptr(), g.ws_fwd.numel(), h))
 
+            cur = list(g.tuning)
             t = []
-            for tile, nseg in inv:
-                _lib.check(lib.s2b_plan_set_tuning(g.plan.ptr, 1, tile))
-                _lib.check(lib.s2b_plan_set_tuning(g.plan.ptr, 2, nseg))
-                t.append(timed(call_inv))
-            tile_inv, nseg = inv[int(np.argmin(t))]
-            _lib.check(lib.s2b_plan_set_tuning(g.plan.ptr, 1, tile_inv))
-            _lib.check(lib.s2b_plan_set_tuning(g.plan.ptr, 2, nseg))
+            for tile, nseg in self._INV:
+                cur[1], cur[2] = tile, nseg
+                self._set(g, cur)
+                t.append(self._timed(call_inv, reps))
+            cur[1], cur[2] = self._INV[int(np.argmin(t))]
             t = []
-            fwd = [(v, n) for v in (0, 1) for n in (2, 4)]  # (tile, segments along m)
-            for v, n in fwd:
-                _lib.check(lib.s2b_plan_set_tuning(g.plan.ptr, 0, v))
-                _lib.check(lib.s2b_plan_set_tuning(g.plan.ptr, 3, n))
-                t.append(timed(call_fwd))
-            tile_fwd, nseg_fwd = fwd[int(np.argmin(t))]
-            _lib.check(lib.s2b_plan_set_tuning(g.plan.ptr, 0, tile_fwd))
-            _lib.check(lib.s2b_plan_set_tuning(g.plan.ptr, 3, nseg_fwd))
-            g.tiles = (tile_fwd, tile_inv, nseg)
+            for v, n in self._FWD:
+                cur[0], cur[3] = v, n
+                self._set(g, cur)
+                t.append(self._timed(call_fwd, reps))
+            cur[0], cur[3] = self._FWD[int(np.argmin(t))]
+            self._set(g, cur)
+            g.tuned["streams"] = tuple(cur)
+
+    def _tune_persistent(self, reps):
+        """Shapes for the persistent schedule, then its waves and CTAs per SM, all timed on
+        the whole batch. Two candidates for the shapes: each group's own (from the
+        per-group tuner; a persistent launch then serves the groups that share a shape),
+        and shapes shared by each class of groups (spin 0, spin != 0), tuned on the batch."""
+        stream = torch.cuda.current_stream(self.device)
+
+        def run_both():
+            self._batch_inverse(stream)
+            self._batch_forward(stream)
+
+        self.batch.set_schedule(1, 0)
+        cands = []
+        if all("streams" in g.tuned for g in self.groups):
+            for g in self.groups:
+                self._set(g, g.tuned["streams"])
+            cands.append((self._timed(run_both, reps), [g.tuning for g in self.groups]))
+        for cls in (True, False):
+            members = [g for g in self.groups if (g.spin == 0) == cls]
+            if not members:
+                continue
+            for (kt, ks), opts, fn in (((1, 2), self._INV, lambda: self._batch_inverse(stream)),
+                                       ((0, 3), self._FWD, lambda: self._batch_forward(stream))):
+                def apply(c):
+                    for g in members:
+                        cur = list(g.tuning)
+                        cur[kt], cur[ks] = c
+                        self._set(g, cur)
+
+                t = []
+                for c in opts:
+                    apply(c)
+                    t.append(self._timed(fn, reps))
+                apply(opts[int(np.argmin(t))])
+        cands.append((self._timed(run_both, reps), [g.tuning for g in self.groups]))
+        best = min(cands, key=lambda c: c[0])[1]
+        for g, tu in zip(self.groups, best):
+            self._set(g, tu)
+        t = []
+        for waves, per_sm in self._SCHED:
+            self.batch.set_schedule(waves, per_sm)
+            t.append(self._timed(run_both, reps))
+        self.batch_schedule = self._SCHED[int(np.argmin(t))]
+        self.batch.set_schedule(*self.batch_schedule)
+        for g in self.groups:
+            g.tuned["persistent"] = g.tuning
+        return min(t)
+
+    def tune(self, reps=3):
+        """Pick launch shapes (and, with persistent=None, the schedule) by timing them."""
+        with torch.no_grad():
+            for g in self.groups:
+                self._set(g, (0, 3, 4, 4))
+            self._tune_streams(reps)  # per-group shapes: used by both schedules
+            t_str = None
+            if self.requested is not True:
+                t_str = self._timed(self._run_streams, reps)
+            t_pers = self._tune_persistent(reps) if self.batch is not None else None
+            if t_pers is not None and (t_str is None or t_pers <= t_str):
+                self.schedule = "persistent"
+            else:
+                self.schedule = "streams"
+                for g in self.groups:
+                    self._set(g, g.tuned["streams"])
+            self.timings = {"persistent_ms": t_pers, "streams_ms": t_str}
         torch.cuda.synchronize(self.device)
 
     def summary(self):
+        keys = ("forward_tile", "inverse_tile", "inverse_segments", "forward_segments")
         return [dict(L=g.L, spin=g.spin, sampling=g.sampling, maps=len(g.members),
-                     forward_tile=g.tiles[0], inverse_tile=g.tiles[1], inverse_segments=g.tiles[2])
+                     **dict(zip(keys, g.tuning or (None,) * 4)))
                 for g in self.groups]

@@ -254,8 +254,13 @@ __device__ __forceinline__ void fwd_pair_step(Real (&c0)[T], Real (&p0)[T], Real
 }
 
 // 3 CTAs per SM: the shared-memory footprint (two stages + partial sums) allows no more
+// One tile of the forward kernel: ring tile bx, block pair and segment by, (half, map) bz.
+// Returns false when a bounded wait ran out (the plan's status word is set). live: the
+// CTA's mbarriers were initialised by an earlier tile (persistent launches) and are
+// invalidated before they are set up again.
 template <typename Real, bool DUAL, int T, int W, int R, int SYM>
-__global__ void __launch_bounds__(W * 32, 3) lat_fwd2_kernel(const Fwd2Params p) {
+__device__ __forceinline__ bool lat_fwd2_tile(const Fwd2Params& p, int bx, int by, int bz,
+                                              unsigned char* smem_raw, bool& live) {
   using Lay = Fwd2Layout<Real, DUAL, T, W, R, SYM>;
   constexpr int GM = Lay::GM;
   using Acc = typename Lay::Acc;
@@ -264,7 +269,6 @@ __global__ void __launch_bounds__(W * 32, 3) lat_fwd2_kernel(const Fwd2Params p)
   constexpr int NT = Lay::NT;
   static_assert(R == 4 || R == 8, "the group body below is written for R = 4 or 8");
   constexpr int U = (2 * T + 31) / 32;  // act entries per lane: entry e = lane + 32 u -> (k, i) = (e / T, e % T)
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char* stage_base = smem_raw;
   Acc* buf = reinterpret_cast<Acc*>(smem_raw + 2 * Lay::stage_bytes);
   int* act = reinterpret_cast<int*>(smem_raw + 2 * Lay::stage_bytes + Lay::buf_bytes);
@@ -281,19 +285,19 @@ __global__ void __launch_bounds__(W * 32, 3) lat_fwd2_kernel(const Fwd2Params p)
   // ring tiles from the equator outwards: the largest tiles are scheduled first
   const int ntiles = (p.nrings + NRT - 1) / NRT;
   const int mid = ntiles >> 1;
-  const int t = (int)blockIdx.x;
+  const int t = bx;
   // (symmetric mode: the rings run from the pole to the equator, so the largest tiles last)
   const int tile = SYM ? ntiles - 1 - t : ((t & 1) ? mid - 1 - (t >> 1) : mid + (t >> 1));
   const int RS = p.tab_stride ? p.tab_stride : p.nrings;  // ring stride of the start tables
   const int r0 = tile * NRT;
-  // blockIdx.y = block pair + NB/2 * segment along m (boundaries of inv_mbound)
+  // by = block pair + NB/2 * segment along m (boundaries of inv_mbound)
   const int npair = NB / 2;
-  const int q = (int)blockIdx.y % npair, seg = (int)blockIdx.y / npair;
+  const int q = by % npair, seg = by / npair;
   const int kb0 = q, kb1 = NB - 1 - q;
   const int nseg = p.Mst1 ? p.nseg : 1;
   const int gstep = kInvSegMax / nseg, g0 = seg * gstep;
-  const int half = (int)(blockIdx.z % p.nhalf);
-  const int b = (int)(blockIdx.z / p.nhalf);
+  const int half = (int)(bz % p.nhalf);
+  const int b = (int)(bz / p.nhalf);
 
   const size_t nst = (size_t)p.nhalf * NB * RS;  // entries of one start table
   const int* __restrict__ Mtab = g0 ? p.Mst1 + (size_t)(g0 - 1) * nst : p.Mst;
@@ -327,15 +331,20 @@ __global__ void __launch_bounds__(W * 32, 3) lat_fwd2_kernel(const Fwd2Params p)
     atomicMax(&mk[1], mt1);
   }
   if (tid == 0) {
+    if (live) {
+      mbar_inval(&mbar[0]);
+      mbar_inval(&mbar[1]);
+    }
     mbar_init(&mbar[0], 1);
     mbar_init(&mbar[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
+  live = true;
   __syncthreads();
   const int mc0 = mk[0], mc1 = mk[1];
   const int mtop = mc0 > mc1 ? mc0 : mc1;
   const int mbot = inv_mbound(L, NB, q, g0 + gstep);  // lowest m of the segment
-  if (mtop < mbot) return;  // nothing significant in this tile and segment (uniform)
+  if (mtop < mbot) return true;  // nothing significant in this tile and segment (uniform)
   const int ngroups = (mtop + 1 - mbot) / R;  // mtop = -1 mod 8, mbot = 0 mod 8
 
   const Real* __restrict__ Hb = reinterpret_cast<const Real*>(p.Hb);
@@ -461,7 +470,7 @@ __global__ void __launch_bounds__(W * 32, 3) lat_fwd2_kernel(const Fwd2Params p)
         atomicExch(p.status, 1);
         mbar_wait(&mbar[(grp + 1) & 1], ((grp + 1) >> 1) & 1);
       }
-      return;
+      return false;
     }
     // warps' partial sums -> flm accumulator
     for (int it = tid; it < R * 2 * kFwdBlock; it += NT) {
@@ -491,6 +500,40 @@ __global__ void __launch_bounds__(W * 32, 3) lat_fwd2_kernel(const Fwd2Params p)
     }
     __syncthreads();
     if (tid == 0 && grp + 2 < ngroups) issue(grp + 2);
+  }
+  return true;
+}
+
+template <typename Real, bool DUAL, int T, int W, int R, int SYM>
+__global__ void __launch_bounds__(W * 32, 3) lat_fwd2_kernel(const Fwd2Params p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  bool live = false;
+  lat_fwd2_tile<Real, DUAL, T, W, R, SYM>(p, (int)blockIdx.x, (int)blockIdx.y,
+                                          (int)blockIdx.z, smem_raw, live);
+}
+
+// Persistent form over the plans of a batch (as lat_inv2_persistent).
+template <typename Real, bool DUAL, int T, int W, int R, int SYM>
+__global__ void __launch_bounds__(W * 32, 3) lat_fwd2_persistent(const Fwd2Batch w) {
+  using Lay = Fwd2Layout<Real, DUAL, T, W, R, SYM>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int item;
+  bool live = false;
+  for (;;) {
+    __syncthreads();  // the previous tile is done with shared memory and item
+    if (threadIdx.x == 0) item = atomicAdd(w.counter, 1);
+    __syncthreads();
+    const int it = item;
+    if (it >= w.start[w.nplans]) return;
+    int pl = 0;
+    while (w.start[pl + 1] <= it) ++pl;
+    const Fwd2Params& p = w.p[pl];
+    const int gx = (p.nrings + Lay::NRT - 1) / Lay::NRT;
+    const int gy = (p.NB / 2) * (p.Mst1 ? p.nseg : 1);
+    const int loc = it - w.start[pl];
+    if (!lat_fwd2_tile<Real, DUAL, T, W, R, SYM>(p, loc % gx, (loc / gx) % gy, loc / (gx * gy),
+                                                 smem_raw, live))
+      return;
   }
 }
 
@@ -532,6 +575,89 @@ static cudaError_t launch_fwd2_prec(bool fp64, bool dual, const Fwd2Params& p, c
                        : launch_fwd2_dual<float, 16, 8, SYM>(dual, p, s);
   return p.tile == 1 ? launch_fwd2_dual<double, 4, 4, SYM>(dual, p, s)
                      : launch_fwd2_dual<double, 8, 4, SYM>(dual, p, s);
+}
+
+template <typename Kernel>
+static cudaError_t persistent_grid(Kernel k, int threads, size_t smem, int items, int per_sm_cap,
+                                   int* grid) {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm_cap > 0 && per_sm > per_sm_cap) per_sm = per_sm_cap;
+  const long cap = (long)sms * (per_sm > 0 ? per_sm : 1);
+  *grid = (int)(items < cap ? items : cap);
+  return cudaSuccess;
+}
+
+template <typename Real, bool DUAL, int T, int R, int SYM>
+static cudaError_t launch_fwd2_batch_cfg(const Fwd2Params* ps, int n, int* counter, int per_sm,
+                                         cudaStream_t s) {
+  using Lay = Fwd2Layout<Real, DUAL, T, 4, R, SYM>;
+  auto kern = lat_fwd2_persistent<Real, DUAL, T, 4, R, SYM>;
+  cudaError_t err =
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::total);
+  if (err != cudaSuccess) return err;
+  Fwd2Batch w{};
+  w.nplans = n;
+  w.counter = counter;
+  w.start[0] = 0;
+  for (int i = 0; i < n; ++i) {
+    w.p[i] = ps[i];
+    const long gx = (ps[i].nrings + Lay::NRT - 1) / Lay::NRT;
+    const long gy = (long)(ps[i].NB / 2) * (ps[i].Mst1 ? ps[i].nseg : 1);
+    const long gz = (long)ps[i].nhalf * ps[i].batch;
+    const long tot = w.start[i] + (ps[i].nrings > 0 ? gx * gy * gz : 0);
+    if (tot > (1L << 30)) return cudaErrorInvalidValue;
+    w.start[i + 1] = (int)tot;
+  }
+  if (w.start[n] == 0) return cudaSuccess;
+  int grid = 0;
+  if ((err = persistent_grid(kern, Lay::NT, Lay::total, w.start[n], per_sm, &grid))) return err;
+  if ((err = cudaMemsetAsync(counter, 0, sizeof(int), s))) return err;
+  kern<<<grid, Lay::NT, Lay::total, s>>>(w);
+  return cudaGetLastError();
+}
+
+template <int SYM>
+static cudaError_t launch_fwd2_batch_prec(bool fp64, bool dual, const Fwd2Params* ps, int n,
+                                          int* counter, int per_sm, cudaStream_t s) {
+  const bool half = ps[0].tile == 1;
+  if constexpr (SYM == 2) {
+    if (dual) return cudaErrorInvalidValue;
+    if (!fp64)
+      return half ? launch_fwd2_batch_cfg<float, false, 8, 8, 2>(ps, n, counter, per_sm, s)
+                  : launch_fwd2_batch_cfg<float, false, 16, 8, 2>(ps, n, counter, per_sm, s);
+    return half ? launch_fwd2_batch_cfg<double, false, 4, 4, 2>(ps, n, counter, per_sm, s)
+                : launch_fwd2_batch_cfg<double, false, 8, 4, 2>(ps, n, counter, per_sm, s);
+  } else {
+#define S2B_FWD2B(REAL, TT, RR)                                                       \
+  return dual ? launch_fwd2_batch_cfg<REAL, true, TT, RR, SYM>(ps, n, counter, per_sm, s) \
+              : launch_fwd2_batch_cfg<REAL, false, TT, RR, SYM>(ps, n, counter, per_sm, s)
+    if (!fp64) {
+      if (half) S2B_FWD2B(float, 8, 8);
+      S2B_FWD2B(float, 16, 8);
+    }
+    if (half) S2B_FWD2B(double, 4, 4);
+    S2B_FWD2B(double, 8, 4);
+#undef S2B_FWD2B
+  }
+}
+
+cudaError_t launch_fwd2_batch(bool fp64, bool dual, const Fwd2Params* ps, int nplans,
+                              int* counter, int per_sm, cudaStream_t s) {
+  if (nplans <= 0) return cudaSuccess;
+  if (nplans > kBatchPlans) return cudaErrorInvalidValue;
+  for (int i = 0; i < nplans; ++i) {
+    if (ps[i].Mst1 && !(ps[i].nseg == 1 || ps[i].nseg == 2 || ps[i].nseg == 4))
+      return cudaErrorInvalidValue;
+    if (ps[i].sym != ps[0].sym || ps[i].cross != ps[0].cross || ps[i].tile != ps[0].tile)
+      return cudaErrorInvalidValue;
+  }
+  if (ps[0].sym && ps[0].cross) return launch_fwd2_batch_prec<2>(fp64, dual, ps, nplans, counter, per_sm, s);
+  return ps[0].sym ? launch_fwd2_batch_prec<1>(fp64, dual, ps, nplans, counter, per_sm, s)
+                   : launch_fwd2_batch_prec<0>(fp64, dual, ps, nplans, counter, per_sm, s);
 }
 
 cudaError_t launch_fwd2(bool fp64, bool dual, const Fwd2Params& p, cudaStream_t s) {

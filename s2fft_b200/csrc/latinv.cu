@@ -84,8 +84,13 @@ __device__ __forceinline__ void inv2_store(R2* ftm, const Acc& s, int L, int m, 
   }
 }
 
+// One tile of the inverse kernel: ring tile bx, block pair and segment by, (half, map) bz.
+// Returns false when a bounded wait ran out (the plan's status word is set). live: the
+// CTA's mbarriers were initialised by an earlier tile (persistent launches) and are
+// invalidated before they are set up again.
 template <typename Real, bool DUAL, int T, int W, int R, bool VST, bool SYM>
-__global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p) {
+__device__ __forceinline__ bool lat_inv2_tile(const Inv2Params& p, int bx, int by, int bz,
+                                              unsigned char* smem_raw, bool& live) {
   using Lay = Inv2Layout<Real, DUAL, T, W, R, VST, SYM>;
   constexpr int NE = Lay::NE;
   using Acc = typename Lay::Acc;
@@ -94,7 +99,6 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
   constexpr int NRT = Lay::NRT;
   constexpr int NT = Lay::NT;
   static_assert(R == 4 || R == 8, "the group body below is written for R = 4 or 8");
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char* stage_base = smem_raw;
   Acc* buf = reinterpret_cast<Acc*>(smem_raw + 2 * Lay::stage_bytes);
   const typename Vec<Real>::t2* vS = reinterpret_cast<const typename Vec<Real>::t2*>(
@@ -108,11 +112,11 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
   const int L = p.L;
   const int NB = p.NB;
   const int TR = tab_rows(L);
-  const int r0 = (int)blockIdx.x * NRT;
-  // blockIdx.y = block pair + NB/2 * segment; segment seg of nseg spans the boundaries
+  const int r0 = bx * NRT;
+  // by = block pair + NB/2 * segment; segment seg of nseg spans the boundaries
   // g = seg * kInvSegMax / nseg and g + kInvSegMax / nseg (inv_mbound)
   const int npair = NB / 2;
-  const int q = (int)blockIdx.y % npair, seg = (int)blockIdx.y / npair;
+  const int q = by % npair, seg = by / npair;
   const int kb0 = q, kb1 = NB - 1 - q;
   const int nseg = p.Mst1 ? p.nseg : 1;
   const int gstep = kInvSegMax / nseg, g0 = seg * gstep;
@@ -120,8 +124,8 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
   const size_t nst = (size_t)p.nhalf * NB * RS;
   const int* __restrict__ Mtab = g0 ? p.Mst1 + (size_t)(g0 - 1) * nst : p.Mst;
   const int mbot = inv_mbound(L, NB, q, g0 + gstep);  // lowest m of the segment
-  const int half = (int)(blockIdx.z % p.nhalf);
-  const int b = (int)(blockIdx.z / p.nhalf);
+  const int half = (int)(bz % p.nhalf);
+  const int b = (int)(bz / p.nhalf);
 
   // degrees of this warp: slot k < 8 -> l = 32 kb0 + 8 wp + k, slot k >= 8 -> 32 kb1 + 8 wp + k - 8,
   // so every warp works on both blocks of the CTA
@@ -142,7 +146,7 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
     Mb[x] = __reduce_max_sync(0xffffffffu, mx);
   }
   const int mtop = Mb[0] > Mb[1] ? Mb[0] : Mb[1];
-  if (mtop < mbot) return;  // nothing significant in this tile and segment (uniform)
+  if (mtop < mbot) return true;  // nothing significant in this tile and segment (uniform)
   const int ngroups = (mtop + 1 - mbot) / R;  // mtop = -1 mod 8, mbot = 0 mod 8
   const R2* __restrict__ Vst =
       g0 ? reinterpret_cast<const R2*>(p.Vst1) + (size_t)(g0 - 1) * nst * kFwdBlock
@@ -187,11 +191,17 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
     *reinterpret_cast<uint4*>(stage_base + x) = make_uint4(0, 0, 0, 0);
   __syncthreads();
   if (tid == 0) {
+    if (live) {
+      mbar_inval(&mbar[0]);
+      mbar_inval(&mbar[1]);
+      mbar_inval(&mbar[2]);
+    }
     mbar_init(&mbar[0], 1);
     mbar_init(&mbar[1], 1);
     mbar_init(&mbar[2], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
+  live = true;
   __syncthreads();
   if (tid == 0) {
     if constexpr (VST) {
@@ -303,7 +313,7 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
         atomicExch(p.status, 1);
         mbar_wait(&mbar[(grp + 1) & 1], ((grp + 1) >> 1) & 1);
       }
-      return;
+      return false;
     }
     // warps' partial sums -> ring spectra
     for (int it = tid; it < R * NRT; it += NT) {
@@ -336,6 +346,42 @@ __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p)
     }
     __syncthreads();
     if (tid == 0 && grp + 2 < ngroups) issue(grp + 2);
+  }
+  return true;
+}
+
+template <typename Real, bool DUAL, int T, int W, int R, bool VST, bool SYM>
+__global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  bool live = false;
+  lat_inv2_tile<Real, DUAL, T, W, R, VST, SYM>(p, (int)blockIdx.x, (int)blockIdx.y,
+                                               (int)blockIdx.z, smem_raw, live);
+}
+
+// Persistent form over the plans of a batch: every CTA takes (plan, tile) items from the
+// work counter until none are left; the items of the first plans (the batch orders its plans
+// by work, largest first) go first. Stops after a bounded wait ran out.
+template <typename Real, bool DUAL, int T, int W, int R, bool VST, bool SYM>
+__global__ void __launch_bounds__(W * 32, 3) lat_inv2_persistent(const Inv2Batch w) {
+  using Lay = Inv2Layout<Real, DUAL, T, W, R, VST, SYM>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int item;
+  bool live = false;
+  for (;;) {
+    __syncthreads();  // the previous tile is done with shared memory and item
+    if (threadIdx.x == 0) item = atomicAdd(w.counter, 1);
+    __syncthreads();
+    const int it = item;
+    if (it >= w.start[w.nplans]) return;
+    int pl = 0;
+    while (w.start[pl + 1] <= it) ++pl;
+    const Inv2Params& p = w.p[pl];
+    const int gx = (p.nrings + Lay::NRT - 1) / Lay::NRT;
+    const int gy = (p.NB / 2) * (p.Mst1 ? p.nseg : 1);
+    const int loc = it - w.start[pl];
+    if (!lat_inv2_tile<Real, DUAL, T, W, R, VST, SYM>(p, loc % gx, (loc / gx) % gy,
+                                                      loc / (gx * gy), smem_raw, live))
+      return;
   }
 }
 
@@ -373,6 +419,85 @@ static cudaError_t launch_inv2_prec(bool fp64, bool dual, const Inv2Params& p, c
   }
   return vst ? launch_inv2_dual<double, 1, true, SYM>(dual, p, s)
              : launch_inv2_dual<double, 1, false, SYM>(dual, p, s);
+}
+
+// CTAs of a persistent launch: what fits on the device at once, at most one per item
+template <typename Kernel>
+static cudaError_t persistent_grid(Kernel k, int threads, size_t smem, int items, int per_sm_cap,
+                                   int* grid) {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm_cap > 0 && per_sm > per_sm_cap) per_sm = per_sm_cap;
+  const long cap = (long)sms * (per_sm > 0 ? per_sm : 1);
+  *grid = (int)(items < cap ? items : cap);
+  return cudaSuccess;
+}
+
+template <typename Real, bool DUAL, int T, int R, bool VST, bool SYM>
+static cudaError_t launch_inv2_batch_cfg(const Inv2Params* ps, int n, int* counter, int per_sm,
+                                         cudaStream_t s) {
+  using Lay = Inv2Layout<Real, DUAL, T, 4, R, VST, SYM>;
+  auto kern = lat_inv2_persistent<Real, DUAL, T, 4, R, VST, SYM>;
+  cudaError_t err =
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::total);
+  if (err != cudaSuccess) return err;
+  Inv2Batch w{};
+  w.nplans = n;
+  w.counter = counter;
+  w.start[0] = 0;
+  for (int i = 0; i < n; ++i) {
+    w.p[i] = ps[i];
+    const long gx = (ps[i].nrings + Lay::NRT - 1) / Lay::NRT;
+    const long gy = (long)(ps[i].NB / 2) * (ps[i].Mst1 ? ps[i].nseg : 1);
+    const long gz = (long)ps[i].nhalf * ps[i].batch;
+    const long tot = w.start[i] + (ps[i].nrings > 0 ? gx * gy * gz : 0);
+    if (tot > (1L << 30)) return cudaErrorInvalidValue;
+    w.start[i + 1] = (int)tot;
+  }
+  if (w.start[n] == 0) return cudaSuccess;
+  int grid = 0;
+  if ((err = persistent_grid(kern, Lay::NT, Lay::total, w.start[n], per_sm, &grid))) return err;
+  if ((err = cudaMemsetAsync(counter, 0, sizeof(int), s))) return err;
+  kern<<<grid, Lay::NT, Lay::total, s>>>(w);
+  return cudaGetLastError();
+}
+
+template <bool SYM>
+static cudaError_t launch_inv2_batch_prec(bool fp64, bool dual, const Inv2Params* ps, int n,
+                                          int* counter, int per_sm, cudaStream_t s) {
+  // the launch shape of the first plan (the batch groups plans by it)
+  const bool vst = (ps[0].tile & 2) == 0;
+  const bool one = (ps[0].tile & 1) != 0;
+#define S2B_INV2B(REAL, TT, VV)                                                          \
+  return dual ? launch_inv2_batch_cfg<REAL, true, TT, 8, VV, SYM>(ps, n, counter, per_sm, s) \
+              : launch_inv2_batch_cfg<REAL, false, TT, 8, VV, SYM>(ps, n, counter, per_sm, s)
+  if (!fp64) {
+    if (one) {
+      if (vst) S2B_INV2B(float, 1, true);
+      S2B_INV2B(float, 1, false);
+    }
+    if (vst) S2B_INV2B(float, 2, true);
+    S2B_INV2B(float, 2, false);
+  }
+  if (vst) S2B_INV2B(double, 1, true);
+  S2B_INV2B(double, 1, false);
+#undef S2B_INV2B
+}
+
+cudaError_t launch_inv2_batch(bool fp64, bool dual, const Inv2Params* ps, int nplans,
+                              int* counter, int per_sm, cudaStream_t s) {
+  if (nplans <= 0) return cudaSuccess;
+  if (nplans > kBatchPlans) return cudaErrorInvalidValue;
+  for (int i = 0; i < nplans; ++i) {
+    if (ps[i].Mst1 && !(ps[i].nseg == 1 || ps[i].nseg == 2 || ps[i].nseg == 4))
+      return cudaErrorInvalidValue;
+    if (ps[i].sym != ps[0].sym || ps[i].tile != ps[0].tile) return cudaErrorInvalidValue;
+  }
+  return ps[0].sym ? launch_inv2_batch_prec<true>(fp64, dual, ps, nplans, counter, per_sm, s)
+                   : launch_inv2_batch_prec<false>(fp64, dual, ps, nplans, counter, per_sm, s);
 }
 
 cudaError_t launch_inv2(bool fp64, bool dual, const Inv2Params& p, cudaStream_t s) {

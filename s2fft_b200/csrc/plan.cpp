@@ -1114,9 +1114,13 @@ static int run_lowm_project(const s2b_plan* p, const Fwd2Params& lp, const RingI
   return S2B_OK;
 }
 
+// The inverse in three stages: before the latitudinal kernel (coefficient table, pole rows;
+// fills the kernel's parameters, nrings = 0 when there is nothing to recurse), the kernel,
+// and after it (low orders, ring FFTs). A batch runs each stage over all its plans, with
+// the kernels of all plans in persistent launches.
 template <typename Real>
-static int run_inverse(s2b_plan* p, const void* flm, void* f, char* ws, cudaStream_t s,
-                       const double* ring_w = nullptr) {
+static int inv_stage_pre(s2b_plan* p, const void* flm, char* ws, cudaStream_t s,
+                         Inv2Params* out) {
   const s2b_desc& d = p->d;
   const int L = d.L;
   void* F = ws;
@@ -1148,6 +1152,7 @@ static int run_inverse(s2b_plan* p, const void* flm, void* f, char* ws, cudaStre
   sp.Lp = p->fwd_NB * kFwdBlock;
   S2B_CK(launch_prologue(p->fp64, sp, s));
   S2B_CK(launch_poles(p->fp64, sp, s));
+  out->nrings = 0;
   if (p->inv_nrings > 0) {
     Inv2Params lp{};
     lp.L = L;
@@ -1177,11 +1182,19 @@ static int run_inverse(s2b_plan* p, const void* flm, void* f, char* ws, cudaStre
     lp.status = p->status;
     lp.tile = p->tile_inv;
     lp.mlo = lowm_orders(p);
-    if (p->ev_begin[0]) S2B_CK(cudaEventRecord(p->ev_begin[0], s));
-    S2B_CK(launch_inv2(p->fp64, p->dual, lp, s));
-    if (p->ev_end[0]) S2B_CK(cudaEventRecord(p->ev_end[0], s));
-    if (int rc_ = run_lowm_synth(p, lp, p->inv_rings, s)) return rc_;
+    *out = lp;
   }
+  return S2B_OK;
+}
+
+template <typename Real>
+static int inv_stage_post(s2b_plan* p, const Inv2Params& lp, void* f, char* ws, cudaStream_t s,
+                          const double* ring_w) {
+  const s2b_desc& d = p->d;
+  const int L = d.L;
+  void* ftm = ws + align256(p->ws_inv_F);
+  if (lp.nrings > 0)
+    if (int rc_ = run_lowm_synth(p, lp, p->inv_rings, s)) return rc_;
   RowsParams<Real> rp{};
   rp.L = L;
   rp.nrows = p->nth;
@@ -1202,6 +1215,20 @@ static int run_inverse(s2b_plan* p, const void* flm, void* f, char* ws, cudaStre
   rp.out = f;
   S2B_CK(launch_inv_rows<Real>(rp, p->nth, d.batch, p->maxM, s));
   return S2B_OK;
+}
+
+template <typename Real>
+static int run_inverse(s2b_plan* p, const void* flm, void* f, char* ws, cudaStream_t s,
+                       const double* ring_w = nullptr) {
+  Inv2Params lp{};
+  int rc;
+  if ((rc = inv_stage_pre<Real>(p, flm, ws, s, &lp))) return rc;
+  if (lp.nrings > 0) {
+    if (p->ev_begin[0]) S2B_CK(cudaEventRecord(p->ev_begin[0], s));
+    S2B_CK(launch_inv2(p->fp64, p->dual, lp, s));
+    if (p->ev_end[0]) S2B_CK(cudaEventRecord(p->ev_end[0], s));
+  }
+  return inv_stage_post<Real>(p, lp, f, ws, s, ring_w);
 }
 
 // HEALPix ring FFTs alone (s2fft/utils/healpix_ffts.py:187-423): per ring FFT, fftshift and
@@ -1419,8 +1446,12 @@ static int run_forward_adjoint(s2b_plan* p, const void* gflm, void* gf, char* ws
   return S2B_OK;
 }
 
+// The forward in the same three stages as the inverse: ring FFTs (and the column chain)
+// filling the latitudinal kernel's parameters (`lp`, and `lp_all` with every ring for the
+// low orders), the kernel, and the low orders with the epilogue.
 template <typename Real>
-static int run_forward_once(s2b_plan* p, const void* f, void* flm, char* ws, cudaStream_t s) {
+static int fwd_stage_pre(s2b_plan* p, const void* f, char* ws, cudaStream_t s, Fwd2Params* lp_out,
+                         Fwd2Params* lp_all_out) {
   const s2b_desc& d = p->d;
   const int L = d.L;
   char* cols = ws;
@@ -1531,7 +1562,7 @@ static int run_forward_once(s2b_plan* p, const void* f, void* flm, char* ws, cud
   lp.status = p->status;
   lp.tile = p->tile_fwd;
   lp.mlo = lowm_orders(p);
-  const Fwd2Params lp_all = lp;  // every ring and G: the low orders (lowm.cu) run on these
+  *lp_all_out = lp;  // every ring and G: the low orders (lowm.cu) run on these
   if (p->fwd_sym) {
     // ring pairs: the northern forward rings (and the equator) with their mirrors folded in
     lp.sym = 1;
@@ -1545,9 +1576,17 @@ static int run_forward_once(s2b_plan* p, const void* f, void* flm, char* ws, cud
     lp.G = G2;
     lp.Gs = p->Gs2;
   }
-  if (p->ev_begin[1]) S2B_CK(cudaEventRecord(p->ev_begin[1], s));
-  S2B_CK(launch_fwd2(p->fp64, p->dual, lp, s));
-  if (p->ev_end[1]) S2B_CK(cudaEventRecord(p->ev_end[1], s));
+  *lp_out = lp;
+  return S2B_OK;
+}
+
+template <typename Real>
+static int fwd_stage_post(s2b_plan* p, const Fwd2Params& lp_all, void* flm, char* ws,
+                          cudaStream_t s) {
+  const s2b_desc& d = p->d;
+  const int L = d.L;
+  char* G = ws + align256(p->ws_fwd_cols);
+  char* acc = G + align256(p->ws_fwd_G);
   if (int rc_ = run_lowm_project(p, lp_all, p->fwd_rings, s)) return rc_;
   StageParams sp{};
   sp.L = L;
@@ -1570,6 +1609,17 @@ static int run_forward_once(s2b_plan* p, const void* f, void* flm, char* ws, cud
   sp.flm_out = flm;
   S2B_CK(launch_epilogue(p->fp64, sp, s));
   return S2B_OK;
+}
+
+template <typename Real>
+static int run_forward_once(s2b_plan* p, const void* f, void* flm, char* ws, cudaStream_t s) {
+  Fwd2Params lp{}, lp_all{};
+  int rc;
+  if ((rc = fwd_stage_pre<Real>(p, f, ws, s, &lp, &lp_all))) return rc;
+  if (p->ev_begin[1]) S2B_CK(cudaEventRecord(p->ev_begin[1], s));
+  S2B_CK(launch_fwd2(p->fp64, p->dual, lp, s));
+  if (p->ev_end[1]) S2B_CK(cudaEventRecord(p->ev_end[1], s));
+  return fwd_stage_post<Real>(p, lp_all, flm, ws, s);
 }
 
 template <typename Real>
@@ -1932,6 +1982,203 @@ static int exec_call(s2b_plan* p, int kind, const void* in, void* out, char* ws,
   }
 }
 
+// ----------------------------------------------------------------------------
+// Batches of plans (an uneven batch: maps of different L, spin and sampling)
+// ----------------------------------------------------------------------------
+// Every stage before and after the latitudinal kernels runs per plan, spread over a few
+// streams; the latitudinal kernels of all plans run as persistent launches (latinv.cu,
+// latfwd.cu), one per kernel variant, whose CTAs pull (plan, tile) items from a device
+// counter until the batch's work is done.
+struct s2b_batch {
+  int device = -1;
+  bool fp64 = false;
+  std::vector<s2b_plan*> plans;
+  int* counters = nullptr;  // one work counter per launch slot (stream-ordered reuse)
+  int ncounters = 0;
+  static constexpr int kMaxStreams = 4;
+  static constexpr int kMaxWaves = 4;
+  int nstreams = 0;
+  cudaStream_t stream[kMaxStreams] = {};
+  cudaEvent_t fork = nullptr;
+  cudaEvent_t join[kMaxStreams] = {};
+  cudaEvent_t wave_done[kMaxWaves] = {};
+  int waves = 1;   // s2b_batch_set_option key 0
+  int per_sm = 0;  // key 1: CTAs per SM of the persistent launches (0: as many as fit)
+};
+
+// The lanes wait for everything issued so far on s (ev: an event of the batch).
+static int batch_fork(s2b_batch* b, cudaStream_t s, cudaEvent_t ev = nullptr) {
+  if (b->nstreams < 2) return S2B_OK;
+  if (!ev) {
+    ev = b->fork;
+    S2B_CK(cudaEventRecord(ev, s));
+  }
+  for (int k = 0; k < b->nstreams; ++k) S2B_CK(cudaStreamWaitEvent(b->stream[k], ev, 0));
+  return S2B_OK;
+}
+
+static int batch_join(s2b_batch* b, cudaStream_t s) {
+  if (b->nstreams < 2) return S2B_OK;
+  for (int k = 0; k < b->nstreams; ++k) {
+    S2B_CK(cudaEventRecord(b->join[k], b->stream[k]));
+    S2B_CK(cudaStreamWaitEvent(s, b->join[k], 0));
+  }
+  return S2B_OK;
+}
+
+static cudaStream_t batch_lane(const s2b_batch* b, int k, cudaStream_t s) {
+  return b->nstreams < 2 ? s : b->stream[k % b->nstreams];
+}
+
+// Entries of wave w when n entries are dealt round-robin into nw waves.
+static std::vector<int> wave_members(int n, int nw, int w) {
+  std::vector<int> m;
+  for (int k = w; k < n; k += nw) m.push_back(k);
+  return m;
+}
+
+// The latitudinal kernels of the entries `sel`: one persistent launch per kernel variant
+// (Key: the fields a launch must share) and per kBatchPlans entries.
+template <typename P, typename Key>
+static int batch_launch_lat(s2b_batch* b, const std::vector<int>& idx, const std::vector<P>& lp,
+                            const std::vector<int>& sel, Key key, int* slot, cudaStream_t s,
+                            cudaError_t (*launch)(bool, bool, const P*, int, int*, int,
+                                                  cudaStream_t)) {
+  std::vector<char> done(sel.size(), 0);
+  std::vector<P> grp;
+  for (size_t a = 0; a < sel.size(); ++a) {
+    const int k = sel[a];
+    if (done[a] || lp[k].nrings <= 0) continue;
+    const bool dual = b->plans[idx[k]]->dual;
+    grp.clear();
+    for (size_t c = a; c < sel.size() && (int)grp.size() < kBatchPlans; ++c) {
+      const int j = sel[c];
+      if (done[c] || lp[j].nrings <= 0 || b->plans[idx[j]]->dual != dual || !key(lp[j], lp[k]))
+        continue;
+      grp.push_back(lp[j]);
+      done[c] = 1;
+    }
+    S2B_CK(launch(b->fp64, dual, grp.data(), (int)grp.size(),
+                  b->counters + ((*slot)++ % b->ncounters), b->per_sm, s));
+  }
+  return S2B_OK;
+}
+
+// Stage-wise execution of entries idx[0..n): every entry's pre-stage on the lanes, the
+// latitudinal kernels of each wave as persistent launches on s, and each wave's post-stages
+// on the lanes once its launches are done. With several waves, the lanes' work of one wave
+// (the ring FFTs are memory-bound) can overlap the latitudinal launches (FP32-bound) of the
+// next. pre(k, lane, &lp[k]) and post(k, lane, lp[k]) run the stages of entry k.
+template <typename P, typename Pre, typename Key, typename Post>
+static int batch_staged(s2b_batch* b, const std::vector<int>& idx, cudaStream_t s, Pre pre,
+                        Key key, Post post,
+                        cudaError_t (*launch)(bool, bool, const P*, int, int*, int, cudaStream_t)) {
+  const int n = (int)idx.size();
+  const int nw = std::max(1, std::min(std::min(b->waves, n), (int)s2b_batch::kMaxWaves));
+  std::vector<P> lp(n);
+  int rc, slot = 0;
+  if ((rc = batch_fork(b, s))) return rc;
+  for (int w = 0; w < nw; ++w) {
+    const std::vector<int> mem = wave_members(n, nw, w);
+    for (int k : mem)
+      if ((rc = pre(k, batch_lane(b, k, s), &lp[k]))) return rc;
+    if ((rc = batch_join(b, s))) return rc;
+    if ((rc = batch_launch_lat<P>(b, idx, lp, mem, key, &slot, s, launch))) return rc;
+    if (nw > 1) S2B_CK(cudaEventRecord(b->wave_done[w], s));
+    if (w > 0) {  // the previous wave's post-stages, behind this wave's pre-stages
+      if ((rc = batch_fork(b, s, b->wave_done[w - 1]))) return rc;
+      for (int k : wave_members(n, nw, w - 1))
+        if ((rc = post(k, batch_lane(b, k, s), lp[k]))) return rc;
+    }
+  }
+  if ((rc = batch_fork(b, s, nw > 1 ? b->wave_done[nw - 1] : nullptr))) return rc;
+  for (int k : wave_members(n, nw, nw - 1))
+    if ((rc = post(k, batch_lane(b, k, s), lp[k]))) return rc;
+  return batch_join(b, s);
+}
+
+// The entries idx[0..n) of the batch: inputs in[k], outputs out[k], workspaces ws[k].
+template <typename Real>
+static int batch_run_inverse(s2b_batch* b, const std::vector<int>& idx, const void* const* in,
+                             void* const* out, char* const* ws, cudaStream_t s) {
+  return batch_staged<Inv2Params>(
+      b, idx, s,
+      [&](int k, cudaStream_t ls, Inv2Params* lp) {
+        return inv_stage_pre<Real>(b->plans[idx[k]], in[k], ws[k], ls, lp);
+      },
+      [](const Inv2Params& x, const Inv2Params& y) { return x.sym == y.sym && x.tile == y.tile; },
+      [&](int k, cudaStream_t ls, const Inv2Params& lp) {
+        return inv_stage_post<Real>(b->plans[idx[k]], lp, out[k], ws[k], ls, nullptr);
+      },
+      launch_inv2_batch);
+}
+
+template <typename Real>
+static int batch_run_forward_once(s2b_batch* b, const std::vector<int>& idx, const void* const* in,
+                                  void* const* out, char* const* ws, cudaStream_t s) {
+  std::vector<Fwd2Params> all(idx.size());
+  return batch_staged<Fwd2Params>(
+      b, idx, s,
+      [&](int k, cudaStream_t ls, Fwd2Params* lp) {
+        return fwd_stage_pre<Real>(b->plans[idx[k]], in[k], ws[k], ls, lp, &all[k]);
+      },
+      [](const Fwd2Params& x, const Fwd2Params& y) {
+        return x.sym == y.sym && x.cross == y.cross && x.tile == y.tile;
+      },
+      [&](int k, cudaStream_t ls, const Fwd2Params&) {
+        return fwd_stage_post<Real>(b->plans[idx[k]], all[k], out[k], ws[k], ls);
+      },
+      launch_fwd2_batch);
+}
+
+// Forward of every entry, with each plan's Jacobi refinement iterations run batch-wide
+// (the entries with iter > it take part in iteration it), as run_forward does per plan.
+template <typename Real>
+static int batch_run_forward(s2b_batch* b, const void* const* f, void* const* flm,
+                             char* const* ws, cudaStream_t s) {
+  const int n = (int)b->plans.size();
+  std::vector<int> idx(n);
+  int maxit = 0;
+  for (int k = 0; k < n; ++k) {
+    idx[k] = k;
+    maxit = std::max(maxit, b->plans[k]->d.iter);
+  }
+  int rc = batch_run_forward_once<Real>(b, idx, f, flm, ws, s);
+  for (int it = 0; !rc && it < maxit; ++it) {
+    std::vector<int> sub;
+    std::vector<const void*> in_f, in_flm;
+    std::vector<void*> fr, dflm, acc_flm;
+    std::vector<char*> wsub;
+    for (int k = 0; k < n; ++k) {
+      const s2b_plan* p = b->plans[k];
+      if (p->d.iter <= it) continue;
+      char* r = ws[k] + std::max(fwd_once_ws(p), inv_ws(p));
+      sub.push_back(k);
+      in_f.push_back(f[k]);
+      in_flm.push_back(flm[k]);
+      acc_flm.push_back(flm[k]);
+      fr.push_back(r);
+      dflm.push_back(r + align256(p->ws_iter_f));
+      wsub.push_back(ws[k]);
+    }
+    if ((rc = batch_run_inverse<Real>(b, sub, in_flm.data(), fr.data(), wsub.data(), s))) break;
+    for (size_t k = 0; k < sub.size(); ++k) {
+      const s2b_plan* p = b->plans[sub[k]];
+      const long nf = (long)p->d.batch * p->npix * (p->d.reality ? 1 : 2);
+      S2B_CK(launch_sub(p->fp64, nf, in_f[k], fr[k], fr[k], s));
+    }
+    std::vector<const void*> fr_in(fr.begin(), fr.end());
+    if ((rc = batch_run_forward_once<Real>(b, sub, fr_in.data(), dflm.data(), wsub.data(), s)))
+      break;
+    for (size_t k = 0; k < sub.size(); ++k) {
+      const s2b_plan* p = b->plans[sub[k]];
+      const long nflm = (long)p->d.batch * p->d.L * (2 * p->d.L - 1);
+      S2B_CK(launch_axpy(p->fp64, nflm, 1.0, dflm[k], acc_flm[k], s));
+    }
+  }
+  return rc;
+}
+
 // Column chain of a complex plan that transforms real maps (forward direction only):
 // Re(c) for the MW pole correction and the split theta-Nyquist bin for MWSS, as a reality
 // plan has them.
@@ -2203,6 +2450,109 @@ int s2b_forward_adjoint(s2b_plan* p, const void* g_flm, void* g_f, void* ws, siz
     return rc;
   if (ws_bytes < ws_of(p, 3)) return fail(S2B_ERR_WORKSPACE, "workspace too small");
   return exec_call(p, 3, g_flm, g_f, (char*)ws, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int s2b_batch_create(s2b_plan* const* plans, int nplans, s2b_batch** out) {
+  g_last_error.clear();
+  if (!plans || !out) return fail(S2B_ERR_INVALID, "plans and batch must be non-NULL");
+  if (nplans < 1) return fail(S2B_ERR_INVALID, "a batch needs at least one plan");
+  for (int k = 0; k < nplans; ++k) {
+    const s2b_plan* p = plans[k];
+    if (!p || p->d.N > 0) return fail(S2B_ERR_INVALID, "batch entries must be spin plans");
+    if (p->device != plans[0]->device)
+      return fail(S2B_ERR_INVALID, "the plans of a batch must share one device");
+    if (p->fp64 != plans[0]->fp64)
+      return fail(S2B_ERR_INVALID, "the plans of a batch must share one precision");
+  }
+  int rc;
+  if ((rc = check_device(plans[0]))) return rc;
+  s2b_batch* b = new s2b_batch();
+  b->device = plans[0]->device;
+  b->fp64 = plans[0]->fp64;
+  b->plans.assign(plans, plans + nplans);
+  b->ncounters = 8;
+  cudaError_t e = dev_malloc(&b->counters, sizeof(int) * b->ncounters);
+  b->nstreams = nplans > 1 ? std::min(nplans, s2b_batch::kMaxStreams) : 0;
+  for (int w = 0; e == cudaSuccess && w < s2b_batch::kMaxWaves; ++w)
+    e = cudaEventCreateWithFlags(&b->wave_done[w], cudaEventDisableTiming);
+  if (e == cudaSuccess && b->nstreams > 1) {
+    e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+    for (int k = 0; e == cudaSuccess && k < b->nstreams; ++k) {
+      e = cudaStreamCreateWithFlags(&b->stream[k], cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join[k], cudaEventDisableTiming);
+    }
+  }
+  if (e != cudaSuccess) {
+    s2b_batch_destroy(b);
+    return fail(S2B_ERR_CUDA, std::string("s2b_batch_create: ") + cudaGetErrorString(e));
+  }
+  *out = b;
+  return S2B_OK;
+}
+
+int s2b_batch_destroy(s2b_batch* b) {
+  if (!b) return S2B_OK;
+  if (b->counters) cudaFree(b->counters);
+  for (int k = 0; k < s2b_batch::kMaxStreams; ++k) {
+    if (b->stream[k]) cudaStreamDestroy(b->stream[k]);
+    if (b->join[k]) cudaEventDestroy(b->join[k]);
+  }
+  for (int w = 0; w < s2b_batch::kMaxWaves; ++w)
+    if (b->wave_done[w]) cudaEventDestroy(b->wave_done[w]);
+  if (b->fork) cudaEventDestroy(b->fork);
+  delete b;
+  return S2B_OK;
+}
+
+int s2b_batch_set_option(s2b_batch* b, int key, int value) {
+  if (!b) return fail(S2B_ERR_INVALID, "batch must be non-NULL");
+  if (key == 0 && value >= 1 && value <= s2b_batch::kMaxWaves)
+    b->waves = value;
+  else if (key == 1 && value >= 0 && value <= 32)
+    b->per_sm = value;
+  else
+    return fail(S2B_ERR_INVALID, "key 0 (waves) takes 1 to 4, key 1 (CTAs per SM of the "
+                                 "persistent launches, 0 = as many as fit) 0 to 32");
+  return S2B_OK;
+}
+
+static int batch_check(s2b_batch* b, int kind, const void* const* in, void* const* out,
+                       void* const* ws, const size_t* ws_bytes) {
+  if (!b) return fail(S2B_ERR_INVALID, "batch is NULL");
+  if (!in || !out || !ws || !ws_bytes)
+    return fail(S2B_ERR_INVALID, "pointer arrays must be non-NULL");
+  int rc;
+  if ((rc = check_device(b->plans[0]))) return rc;
+  for (size_t k = 0; k < b->plans.size(); ++k) {
+    if ((rc = check_ptr(in[k], kind ? "f" : "flm")) || (rc = check_ptr(out[k], kind ? "flm" : "f")) ||
+        (rc = check_ptr(ws[k], "workspace")))
+      return rc;
+    if (ws_bytes[k] < ws_of(b->plans[k], kind))
+      return fail(S2B_ERR_WORKSPACE, "workspace of entry " + std::to_string(k) + " too small");
+  }
+  return S2B_OK;
+}
+
+int s2b_batch_inverse(s2b_batch* b, const void* const* flm, void* const* f, void* const* ws,
+                      const size_t* ws_bytes, void* stream) {
+  int rc;
+  if ((rc = batch_check(b, 0, flm, f, ws, ws_bytes))) return rc;
+  std::vector<int> idx(b->plans.size());
+  for (size_t k = 0; k < idx.size(); ++k) idx[k] = (int)k;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  char* const* w = reinterpret_cast<char* const*>(ws);
+  return b->fp64 ? batch_run_inverse<double>(b, idx, flm, f, w, s)
+                 : batch_run_inverse<float>(b, idx, flm, f, w, s);
+}
+
+int s2b_batch_forward(s2b_batch* b, const void* const* f, void* const* flm, void* const* ws,
+                      const size_t* ws_bytes, void* stream) {
+  int rc;
+  if ((rc = batch_check(b, 1, f, flm, ws, ws_bytes))) return rc;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  char* const* w = reinterpret_cast<char* const*>(ws);
+  return b->fp64 ? batch_run_forward<double>(b, f, flm, w, s)
+                 : batch_run_forward<float>(b, f, flm, w, s);
 }
 
 int s2b_healpix_fft(s2b_plan* p, const void* f, void* ftm, void* stream) {

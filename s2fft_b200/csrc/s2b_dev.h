@@ -86,6 +86,11 @@ __device__ __forceinline__ void mbar_init(uint64_t* mb, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mb)), "r"(count)
                : "memory");
 }
+// Invalidates an initialised mbarrier (no pending arrivals or transactions), so that the
+// location can be initialised again (a persistent kernel reusing it for its next tile).
+__device__ __forceinline__ void mbar_inval(uint64_t* mb) {
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(mb)) : "memory");
+}
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* mb, unsigned bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mb)),
                "r"(bytes)

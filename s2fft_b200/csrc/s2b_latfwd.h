@@ -108,6 +108,33 @@ struct Inv2Params {
 };
 cudaError_t launch_inv2(bool fp64, bool dual, const Inv2Params& p, cudaStream_t s);
 
+// Persistent latitudinal launches over the plans of a batch (one kernel variant: the same
+// precision, layout and symmetry): the plans' parameter blocks travel in the kernel
+// arguments, and every CTA takes (plan, tile) items from a device counter until none are
+// left. start[i] = tiles of plans 0..i-1; counter is zeroed by the launcher (stream-ordered).
+constexpr int kBatchPlans = 48;
+struct Inv2Batch {
+  int nplans;
+  int start[kBatchPlans + 1];
+  int* counter;
+  Inv2Params p[kBatchPlans];
+};
+struct Fwd2Batch {
+  int nplans;
+  int start[kBatchPlans + 1];
+  int* counter;
+  Fwd2Params p[kBatchPlans];
+};
+// kernel parameters are limited to 32764 bytes
+static_assert(sizeof(Inv2Batch) <= 32000 && sizeof(Fwd2Batch) <= 32000, "batch parameters");
+
+// nplans <= kBatchPlans plans of one variant; counter: one device int; per_sm: CTAs per SM
+// of the launch (0: as many as fit)
+cudaError_t launch_inv2_batch(bool fp64, bool dual, const Inv2Params* ps, int nplans,
+                              int* counter, int per_sm, cudaStream_t s);
+cudaError_t launch_fwd2_batch(bool fp64, bool dual, const Fwd2Params* ps, int nplans,
+                              int* counter, int per_sm, cudaStream_t s);
+
 cudaError_t launch_fwd_start(bool fp64, const FwdStartParams& p, cudaStream_t s);
 cudaError_t launch_fwd2(bool fp64, bool dual, const Fwd2Params& p, cudaStream_t s);
 size_t fwd_start_bytes(bool fp64, int L, int nhalf, int nrings);
