@@ -158,7 +158,8 @@ def measured_peaks():
 
 
 def simt_peak_tflops(torch, fp64):
-    """FP32 / FP64 FMA rate measured with the library's FMA-chain probe."""
+    """FP32 / FP64 FMA rate measured with the library's FMA-chain probe (fp64 = 2: FP32 by
+    packed-pair FMAs, fma.rn.f32x2)."""
     from s2fft_b200 import _lib
 
     lib = _lib.lib()
@@ -167,7 +168,7 @@ def simt_peak_tflops(torch, fp64):
     lib.s2b_fma_probe.restype = ctypes.c_int
     sms = torch.cuda.get_device_properties(0).multi_processor_count
     blocks, iters = sms * 8, 4000 if not fp64 else 2000
-    out = torch.empty(blocks * 256, dtype=torch.float64 if fp64 else torch.float32,
+    out = torch.empty(blocks * 256, dtype=torch.float64 if fp64 == 1 else torch.float32,
                       device="cuda")
     st = _lib.stream_handle(out.device)
     best = 0.0
@@ -178,7 +179,7 @@ def simt_peak_tflops(torch, fp64):
         e1.record()
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
-        flops = blocks * 256.0 * iters * 16 * 8 * 2
+        flops = blocks * 256.0 * iters * 16 * 8 * 2 * (2 if fp64 == 2 else 1)
         if rep > 0:
             best = max(best, flops / (ms * 1e-3) / 1e12)
     return best

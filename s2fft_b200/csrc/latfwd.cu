@@ -186,10 +186,17 @@ struct Fwd2Layout {
   static constexpr size_t g_bytes = (size_t)R * NRT * GM * sizeof(Acc);
   static constexpr size_t l_bytes = (size_t)R * NRT * sizeof(Real);
   static constexpr size_t stage_bytes = h_bytes + g_bytes + l_bytes;
-  // partial sums [R][W][2][32]
-  static constexpr size_t buf_bytes = (size_t)R * W * 2 * kFwdBlock * sizeof(Acc);
+  // partial sums [R][W][2][32], twice: a group's reduction and the next group's steps use
+  // different halves, so one barrier per group separates them
+  // (once when two copies would leave room for fewer than 3 CTAs per SM: then a second
+  // barrier per group)
+  static constexpr int buf_elems = R * W * 2 * kFwdBlock;
   static constexpr size_t act_bytes = (size_t)W * 2 * T * sizeof(int);
-  static constexpr size_t total = 2 * stage_bytes + buf_bytes + act_bytes + 16 + 16;
+  static constexpr size_t fixed_bytes = 2 * stage_bytes + act_bytes + 16 + 16;
+  static constexpr int NBUF =
+      3 * (fixed_bytes + 2 * buf_elems * sizeof(Acc) + 1024) <= 228 * 1024 ? 2 : 1;
+  static constexpr size_t buf_bytes = (size_t)NBUF * buf_elems * sizeof(Acc);
+  static constexpr size_t total = fixed_bytes + buf_bytes;
   static_assert(stage_bytes % 16 == 0 && buf_bytes % 16 == 0 && act_bytes % 16 == 0, "align");
   static_assert((2 * T) % 32 == 0 || 2 * T < 32, "act entries are spread over the lanes");
 };
@@ -270,7 +277,7 @@ __device__ __forceinline__ bool lat_fwd2_tile(const Fwd2Params& p, int bx, int b
   static_assert(R == 4 || R == 8, "the group body below is written for R = 4 or 8");
   constexpr int U = (2 * T + 31) / 32;  // act entries per lane: entry e = lane + 32 u -> (k, i) = (e / T, e % T)
   unsigned char* stage_base = smem_raw;
-  Acc* buf = reinterpret_cast<Acc*>(smem_raw + 2 * Lay::stage_bytes);
+  Acc* const bufs = reinterpret_cast<Acc*>(smem_raw + 2 * Lay::stage_bytes);
   int* act = reinterpret_cast<int*>(smem_raw + 2 * Lay::stage_bytes + Lay::buf_bytes);
   int* mk = act + W * 2 * T;  // CTA-wide first m per slot (2 ints)
   uint64_t* mbar = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(mk) + 16);
@@ -420,7 +427,18 @@ __device__ __forceinline__ bool lat_fwd2_tile(const Fwd2Params& p, int bx, int b
         if (lane + 32 * u < 2 * T && a_m[u] < mgrp && a_m[u] > na) na = a_m[u];
       next_act = __reduce_max_sync(0xffffffffu, na);
     }
+    // the next group starts states: their start values into L1 while this group runs
+    if (next_act >= 0 && next_act == mgrp - R) {
+#pragma unroll
+      for (int k = 0; k < 2; ++k)
+#pragma unroll
+        for (int i = 0; i < T; ++i)
+          if (act[(wp * 2 + k) * T + i] == next_act)
+            prefetch_l1(&Vst[(((size_t)half * NB + kb[k]) * RS + r0 + wp * T + i) * kFwdBlock +
+                             lane]);
+    }
     const unsigned char* st = stage_base + (size_t)(grp & 1) * Lay::stage_bytes;
+    Acc* const buf = bufs + (Lay::NBUF == 2 ? (grp & 1) * Lay::buf_elems : 0);
     const Real* hS = reinterpret_cast<const Real*>(st);
     const Acc* gS = reinterpret_cast<const Acc*>(st + Lay::h_bytes) + wp * T * GM;
     const Real* lS = reinterpret_cast<const Real*>(st + Lay::h_bytes + Lay::g_bytes) + wp * T;
@@ -472,6 +490,8 @@ __device__ __forceinline__ bool lat_fwd2_tile(const Fwd2Params& p, int bx, int b
       }
       return false;
     }
+    // every warp is past this group's stage: refill it for group grp + 2
+    if (tid == 0 && grp + 2 < ngroups) issue(grp + 2);
     // warps' partial sums -> flm accumulator
     for (int it = tid; it < R * 2 * kFwdBlock; it += NT) {
       const int S = it / (2 * kFwdBlock);
@@ -498,8 +518,7 @@ __device__ __forceinline__ bool lat_fwd2_tile(const Fwd2Params& p, int bx, int b
         red_add(out + (size_t)m * Lp + l, s);
       }
     }
-    __syncthreads();
-    if (tid == 0 && grp + 2 < ngroups) issue(grp + 2);
+    if constexpr (Lay::NBUF == 1) __syncthreads();  // buf is rewritten by the next group
   }
   return true;
 }

@@ -52,12 +52,20 @@ struct Inv2Layout {
   static constexpr size_t l_bytes = (size_t)R * NRT * sizeof(Real);
   static constexpr size_t stage_bytes = h_bytes + f_bytes + l_bytes;
   static constexpr int NE = SYM ? 2 : 1;  // partial sums per lane slot: (E, O) of a ring pair
-  static constexpr size_t buf_bytes = (size_t)R * W * NRT * NE * sizeof(Acc);
+  // warps' partial sums of one group, twice: a group's reduction and the next group's steps
+  // use different halves, so one barrier per group separates them
+  // (once when two copies would leave room for fewer than 3 CTAs per SM: then a second
+  // barrier per group)
+  static constexpr int buf_elems = R * W * NRT * NE;
   // start values of the CTA's states: [2 blocks][NRT rings][32] (d~_M, d~_{M+1})
   // (VST: staged by bulk copy; otherwise each lane reads its own from global memory, which
   // leaves room for one more CTA per SM)
   static constexpr size_t v_bytes = VST ? (size_t)2 * NRT * kFwdBlock * 2 * sizeof(Real) : 0;
-  static constexpr size_t total = 2 * stage_bytes + buf_bytes + v_bytes + 32;
+  static constexpr size_t fixed_bytes = 2 * stage_bytes + v_bytes + 32;
+  static constexpr int NBUF =
+      3 * (fixed_bytes + 2 * buf_elems * sizeof(Acc) + 1024) <= 228 * 1024 ? 2 : 1;
+  static constexpr size_t buf_bytes = (size_t)NBUF * buf_elems * sizeof(Acc);
+  static constexpr size_t total = fixed_bytes + buf_bytes;
   static_assert(W == 4, "two warps per 32-degree block, two blocks per CTA");
   static_assert(stage_bytes % 16 == 0 && buf_bytes % 16 == 0, "align");
 };
@@ -100,7 +108,7 @@ __device__ __forceinline__ bool lat_inv2_tile(const Inv2Params& p, int bx, int b
   constexpr int NT = Lay::NT;
   static_assert(R == 4 || R == 8, "the group body below is written for R = 4 or 8");
   unsigned char* stage_base = smem_raw;
-  Acc* buf = reinterpret_cast<Acc*>(smem_raw + 2 * Lay::stage_bytes);
+  Acc* const bufs = reinterpret_cast<Acc*>(smem_raw + 2 * Lay::stage_bytes);
   const typename Vec<Real>::t2* vS = reinterpret_cast<const typename Vec<Real>::t2*>(
       smem_raw + 2 * Lay::stage_bytes + Lay::buf_bytes);
   uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_raw + 2 * Lay::stage_bytes + Lay::buf_bytes +
@@ -229,8 +237,42 @@ __device__ __forceinline__ bool lat_inv2_tile(const Inv2Params& p, int bx, int b
     lmax = kb1 * kFwdBlock + kFwdBlock - 1;
   if (lmax > L - 1) lmax = L - 1;
 
+  // the reduction gives every thread one ring of the tile (NT is a multiple of NRT): its
+  // ftm rows (and, symmetric, its mirror's), looked up once
+  static_assert(NT % NRT == 0, "one reduction ring per thread");
+  const int rr_red = tid % NRT;
+  const int r_red = r0 + rr_red;
+  const bool ring_live = r_red < p.nrings;
+  R2* ftm_r = nullptr;
+  R2* ftm_rm = nullptr;  // symmetric: the mirror ring (none for the equator)
+  if (ring_live) {
+    ftm_r = reinterpret_cast<R2*>(p.ftm) + ((size_t)b * p.nrows + p.ring_row[r_red]) * p.ncol;
+    if (SYM && RS - 1 - r_red != r_red)
+      ftm_rm = reinterpret_cast<R2*>(p.ftm) +
+               ((size_t)b * p.nrows + p.ring_row[RS - 1 - r_red]) * p.ncol;
+  }
+  // start values read from global memory: each lane's line is prefetched into L1 one group
+  // before the group that starts the state (a group is thousands of cycles of FMAs)
+  auto vst_line = [&](int x, int i) {
+    return Vst + (((size_t)half * NB + (x ? kb1 : kb0)) * RS + r0 + lane * T + i) * kFwdBlock +
+           col0;
+  };
+  if constexpr (!VST) {
+#pragma unroll
+    for (int x = 0; x < 2; ++x)
+#pragma unroll
+      for (int i = 0; i < T; ++i)
+        if (Ms[x][i] >= 0 && Ms[x][i] == mtop) prefetch_l1(vst_line(x, i));
+  }
   for (int grp = 0; grp < ngroups; ++grp) {
     const int mgrp = mtop - grp * R;
+    if constexpr (!VST) {
+#pragma unroll
+      for (int x = 0; x < 2; ++x)
+#pragma unroll
+        for (int i = 0; i < T; ++i)
+          if (Ms[x][i] >= 0 && Ms[x][i] == mgrp - R) prefetch_l1(vst_line(x, i));
+    }
     const bool ok = mbar_wait(&mbar[grp & 1], (grp >> 1) & 1);
     // start the (ring, block) states whose first group start is this group's
 #pragma unroll
@@ -238,10 +280,8 @@ __device__ __forceinline__ bool lat_inv2_tile(const Inv2Params& p, int bx, int b
 #pragma unroll
       for (int i = 0; i < T; ++i)
         if (Ms[x][i] == mgrp) {
-          const R2* src =
-              VST ? vS + ((size_t)x * NRT + lane * T + i) * kFwdBlock + col0
-                  : Vst + (((size_t)half * NB + (x ? kb1 : kb0)) * RS + r0 + lane * T + i) *
-                              kFwdBlock + col0;
+          const R2* src = VST ? vS + ((size_t)x * NRT + lane * T + i) * kFwdBlock + col0
+                              : vst_line(x, i);
 #pragma unroll
           for (int kk = 0; kk < K / 2; ++kk) {
             const R2 sv = src[kk];
@@ -250,6 +290,7 @@ __device__ __forceinline__ bool lat_inv2_tile(const Inv2Params& p, int bx, int b
           }
         }
     const unsigned char* st = stage_base + (size_t)(grp & 1) * Lay::stage_bytes;
+    Acc* const buf = bufs + (Lay::NBUF == 2 ? (grp & 1) * Lay::buf_elems : 0);
     const Real* hS = reinterpret_cast<const Real*>(st) + col0;
     const Acc* fS = reinterpret_cast<const Acc*>(st + Lay::h_bytes) + col0;
     const Real* lS = reinterpret_cast<const Real*>(st + Lay::h_bytes + Lay::f_bytes) + lane * T;
@@ -271,11 +312,13 @@ __device__ __forceinline__ bool lat_inv2_tile(const Inv2Params& p, int bx, int b
         /* the warp's 8 h values of the row: 16-byte broadcast loads */                  \
         Real hv[K / 2];                                                                 \
         ld_vec16(hv, hS + (x * R + srow) * kFwdBlock);                                  \
+        /* and its 8 coefficients: 16-byte loads (each a one-wavefront broadcast) */    \
+        Acc fv[K / 2];                                                                  \
+        ld_vec16(fv, fS + (x * R + srow) * kFwdBlock);                                  \
         _Pragma("unroll") for (int kk = 0; kk < K / 2; ++kk) {                          \
           const int k = x * (K / 2) + kk;                                               \
-          const int so = (x * R + srow) * kFwdBlock + kk;                               \
           const Real h = hv[kk];                                                        \
-          const Acc f = fS[so];                                                         \
+          const Acc f = fv[kk];                                                         \
           _Pragma("unroll") for (int i = 0; i < T; ++i) {                               \
             acc_fma(a[SYM ? (kk & 1) : x][i], CUR[k][i], f);                            \
             PRV[k][i] = fma(lam[i] * h, CUR[k][i], -PRV[k][i]);                         \
@@ -315,13 +358,14 @@ __device__ __forceinline__ bool lat_inv2_tile(const Inv2Params& p, int bx, int b
       }
       return false;
     }
-    // warps' partial sums -> ring spectra
+    // every warp is past this group's stage: refill it for group grp + 2
+    if (tid == 0 && grp + 2 < ngroups) issue(grp + 2);
+    // warps' partial sums -> ring spectra (NT is a multiple of NRT: one ring per thread)
     for (int it = tid; it < R * NRT; it += NT) {
       const int S = it / NRT;
-      const int rr = it % NRT;
       const int m = mgrp - S;
-      const int r = r0 + rr;
-      if (m < p.mlo || m > lmax || r >= p.nrings) continue;
+      if (m < p.mlo || m > lmax || !ring_live) continue;
+      const int rr = rr_red;
       Acc s = buf[((S * W + 0) * NRT + rr) * NE];
 #pragma unroll
       for (int x = 1; x < W; ++x) acc_add(s, buf[((S * W + x) * NRT + rr) * NE]);
@@ -330,22 +374,16 @@ __device__ __forceinline__ bool lat_inv2_tile(const Inv2Params& p, int bx, int b
         Acc o = buf[((S * W + 0) * NRT + rr) * NE + 1];
 #pragma unroll
         for (int x = 1; x < W; ++x) acc_add(o, buf[((S * W + x) * NRT + rr) * NE + 1]);
-        const int rm = RS - 1 - r;
-        if (rm != r) {
+        if (ftm_rm) {
           Acc d = s;
           acc_fma(d, Real(-1), o);
-          inv2_store<DUAL>(reinterpret_cast<R2*>(p.ftm) +
-                               ((size_t)b * p.nrows + p.ring_row[rm]) * p.ncol,
-                           d, L, m, p.mo, half);
+          inv2_store<DUAL>(ftm_rm, d, L, m, p.mo, half);
         }
         acc_add(s, o);
       }
-      inv2_store<DUAL>(
-          reinterpret_cast<R2*>(p.ftm) + ((size_t)b * p.nrows + p.ring_row[r]) * p.ncol, s, L,
-          m, p.mo, half);
+      inv2_store<DUAL>(ftm_r, s, L, m, p.mo, half);
     }
-    __syncthreads();
-    if (tid == 0 && grp + 2 < ngroups) issue(grp + 2);
+    if constexpr (Lay::NBUF == 1) __syncthreads();  // buf is rewritten by the next group
   }
   return true;
 }

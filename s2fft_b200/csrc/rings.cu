@@ -25,8 +25,20 @@
 #include "s2b_internal.h"
 #include "s2b_fft_dev.h"
 #include "s2b_fft_reg.h"
+#include "s2b_dev.h"
 
 namespace s2b {
+
+// CTAs per SM the register-engine kernels are compiled for (launch bounds): 32 warps per SM
+// in float (the points of a 2^LOGM transform take 2^(LOGM-4) threads; 64 registers, a few
+// bytes of spills at most), 16 in double (twice the registers per point); one CTA of 512
+// threads for 8192 points. The shared-memory passes (LOGM = 0): two in float, one in double.
+template <typename Real>
+__host__ __device__ constexpr int reg_min_blocks(int logm) {
+  return logm == 0    ? (sizeof(Real) == 4 ? 2 : 1)
+         : logm >= 13 ? 1
+                      : ((sizeof(Real) == 4 ? 1024 : 512) >> (logm - 4));
+}
 
 // Any-length DFT of one CTA on the register engine (M = 2^LOGM, blockDim.x = M / 16; d.M
 // must be M): inputs load(k), k < d.n; every output X_k (k < d.n, conjugated when inv,
@@ -47,6 +59,10 @@ __device__ __forceinline__ void reg_dft(typename C2<Real>::t* buf, const FFTDesc
   if (d.bluestein) {
     const R2* __restrict__ ch = tb.chirp + d.chirp_off;
     const R2* __restrict__ bf = tb.rbf + d.rbf_off;  // position 16 j + a at [a T + j]
+    // the filter is read after the forward passes: its lines into L1 now, so that those
+    // reads do not wait on L2
+#pragma unroll
+    for (int a = 0; a < 16; ++a) prefetch_l1(bf + a * RF::T + j);
 #pragma unroll
     for (int a = 0; a < 16; ++a) {
       const int k = j + RF::T * a;
@@ -91,7 +107,7 @@ __device__ __forceinline__ void reg_dft(typename C2<Real>::t* buf, const FFTDesc
 // LOGM > 0: the register engine for uniform rings of one power-of-two working length 2^LOGM
 // (equiangular samplings; blockDim.x = 2^LOGM / 16); LOGM = 0: the shared-memory passes.
 template <typename Real, int LOGM, int NBUF>
-__global__ void __launch_bounds__(LOGM ? (1 << LOGM) / 16 : 512, (sizeof(Real) == 4 && LOGM < 13) ? 2 : 1)
+__global__ void __launch_bounds__(LOGM ? (1 << LOGM) / 16 : 512, reg_min_blocks<Real>(LOGM))
     inv_rows_kernel(RowsParams<Real> p) {
   using R2 = typename C2<Real>::t;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -244,7 +260,7 @@ __device__ __forceinline__ void store_spectra(const RowsParams<Real>& p, int b, 
 // the MW/MWSS resampling chain, the transposed raw spectra Fc [B][ncolm][nrows].
 // ---------------------------------------------------------------------------
 template <typename Real, int LOGM, int NBUF>
-__global__ void __launch_bounds__(LOGM ? (1 << LOGM) / 16 : 512, (sizeof(Real) == 4 && LOGM < 13) ? 2 : 1)
+__global__ void __launch_bounds__(LOGM ? (1 << LOGM) / 16 : 512, reg_min_blocks<Real>(LOGM))
     fwd_rows_kernel(RowsParams<Real> p) {
   using R2 = typename C2<Real>::t;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -349,7 +365,7 @@ __global__ void __launch_bounds__(LOGM ? (1 << LOGM) / 16 : 512, (sizeof(Real) =
 // LOGM > 0: both transforms on the register engine (d1.M = d2.M = 2^LOGM, the inverse DFT
 // of power-of-two length 4L; blockDim.x = 2^LOGM / 16); LOGM = 0: the shared-memory passes.
 template <typename Real, int LOGM, int NBUF>
-__global__ void __launch_bounds__(LOGM ? (1 << LOGM) / 16 : 512, (sizeof(Real) == 4 && LOGM < 13) ? 2 : 1)
+__global__ void __launch_bounds__(LOGM ? (1 << LOGM) / 16 : 512, reg_min_blocks<Real>(LOGM))
     mw_cols_kernel(ColsParams<Real> p) {
   using R2 = typename C2<Real>::t;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -659,13 +675,11 @@ static int reg_logm(int M) {
     if (M == (1 << lg)) return lg;
   return 0;
 }
-static constexpr int kRegBufs = 1;      // exchange buffers of the register engine
-static constexpr int kRegCarveout = 50;  // shared-memory share of L1 for it (percent)
+static constexpr int kRegBufs = 1;  // exchange buffers of the register engine
 
 // carveout: the percentage of the unified L1 / shared memory given to shared memory. The
-// shared-memory passes want all of it (occupancy); the register engine is held to two or
-// three CTAs per SM by its registers and reads its twiddle, chirp and filter tables
-// through L1, so it keeps half for L1.
+// shared-memory passes want all of it (occupancy); the register engine takes what its
+// CTAs per SM need (reg_carveout) and leaves the rest to L1.
 template <typename Real, typename Kernel, typename Params>
 static cudaError_t launch_fft_kernel(Kernel k, dim3 grid, int threads, size_t smem,
                                      const Params& p, cudaStream_t s, int carveout = 100) {
@@ -682,6 +696,16 @@ static size_t reg_smem(int extra) {
   return ((size_t)RegFFT<LOGM, kRegBufs>::SMEM_ELEMS + extra) * sizeof(typename C2<Real>::t);
 }
 
+// shared-memory share of the unified L1 (percent) for the register engine: room for the
+// CTAs per SM of its launch bounds, the rest stays L1 for its twiddle, chirp and filter
+// tables
+template <typename Real, int LOGM>
+static int reg_carveout(int extra) {
+  const size_t need = (size_t)reg_min_blocks<Real>(LOGM) * (reg_smem<Real, LOGM>(extra) + 1024);
+  const int pct = (int)((100 * need + 228 * 1024 - 1) / (228 * 1024)) + 1;
+  return pct < 100 ? pct : 100;
+}
+
 // the rows use the register engine when every ring has the same working length (no per-ring
 // descriptors: equiangular samplings) and no ring phase
 template <typename Real>
@@ -695,10 +719,10 @@ cudaError_t launch_inv_rows(const RowsParams<Real>& p, int nrings, int batch, in
   using R2 = typename C2<Real>::t;
   const dim3 grid(nrings, batch);
   switch (rows_reg_logm(p, maxM)) {
-    case 10: return launch_fft_kernel<Real>(inv_rows_kernel<Real, 10, kRegBufs>, grid, 64, reg_smem<Real, 10>(0), p, s, kRegCarveout);
-    case 11: return launch_fft_kernel<Real>(inv_rows_kernel<Real, 11, kRegBufs>, grid, 128, reg_smem<Real, 11>(0), p, s, kRegCarveout);
-    case 12: return launch_fft_kernel<Real>(inv_rows_kernel<Real, 12, kRegBufs>, grid, 256, reg_smem<Real, 12>(0), p, s, kRegCarveout);
-    case 13: return launch_fft_kernel<Real>(inv_rows_kernel<Real, 13, kRegBufs>, grid, 512, reg_smem<Real, 13>(0), p, s, kRegCarveout);
+    case 10: return launch_fft_kernel<Real>(inv_rows_kernel<Real, 10, kRegBufs>, grid, 64, reg_smem<Real, 10>(0), p, s, reg_carveout<Real, 10>(0));
+    case 11: return launch_fft_kernel<Real>(inv_rows_kernel<Real, 11, kRegBufs>, grid, 128, reg_smem<Real, 11>(0), p, s, reg_carveout<Real, 11>(0));
+    case 12: return launch_fft_kernel<Real>(inv_rows_kernel<Real, 12, kRegBufs>, grid, 256, reg_smem<Real, 12>(0), p, s, reg_carveout<Real, 12>(0));
+    case 13: return launch_fft_kernel<Real>(inv_rows_kernel<Real, 13, kRegBufs>, grid, 512, reg_smem<Real, 13>(0), p, s, reg_carveout<Real, 13>(0));
     default: break;
   }
   const size_t smem = (size_t)padded_len(maxM) * sizeof(R2);
@@ -711,10 +735,10 @@ cudaError_t launch_fwd_rows(const RowsParams<Real>& p, int nrings, int batch, in
   using R2 = typename C2<Real>::t;
   const dim3 grid(nrings, batch);
   switch (rows_reg_logm(p, maxM)) {
-    case 10: return launch_fft_kernel<Real>(fwd_rows_kernel<Real, 10, kRegBufs>, grid, 64, reg_smem<Real, 10>(0), p, s, kRegCarveout);
-    case 11: return launch_fft_kernel<Real>(fwd_rows_kernel<Real, 11, kRegBufs>, grid, 128, reg_smem<Real, 11>(0), p, s, kRegCarveout);
-    case 12: return launch_fft_kernel<Real>(fwd_rows_kernel<Real, 12, kRegBufs>, grid, 256, reg_smem<Real, 12>(0), p, s, kRegCarveout);
-    case 13: return launch_fft_kernel<Real>(fwd_rows_kernel<Real, 13, kRegBufs>, grid, 512, reg_smem<Real, 13>(0), p, s, kRegCarveout);
+    case 10: return launch_fft_kernel<Real>(fwd_rows_kernel<Real, 10, kRegBufs>, grid, 64, reg_smem<Real, 10>(0), p, s, reg_carveout<Real, 10>(0));
+    case 11: return launch_fft_kernel<Real>(fwd_rows_kernel<Real, 11, kRegBufs>, grid, 128, reg_smem<Real, 11>(0), p, s, reg_carveout<Real, 11>(0));
+    case 12: return launch_fft_kernel<Real>(fwd_rows_kernel<Real, 12, kRegBufs>, grid, 256, reg_smem<Real, 12>(0), p, s, reg_carveout<Real, 12>(0));
+    case 13: return launch_fft_kernel<Real>(fwd_rows_kernel<Real, 13, kRegBufs>, grid, 512, reg_smem<Real, 13>(0), p, s, reg_carveout<Real, 13>(0));
     default: break;
   }
   const size_t smem = (size_t)padded_len(maxM) * sizeof(R2);
@@ -730,10 +754,10 @@ cudaError_t launch_mw_cols(const ColsParams<Real>& p, int ncm, int batch, int M1
   const int lg = (M1 == M2 && p.d2_pow2) ? reg_logm<Real>(M1) : 0;
   const int extra = 2 * p.L;
   switch (lg) {
-    case 10: return launch_fft_kernel<Real>(mw_cols_kernel<Real, 10, kRegBufs>, grid, 64, reg_smem<Real, 10>(extra), p, s, kRegCarveout);
-    case 11: return launch_fft_kernel<Real>(mw_cols_kernel<Real, 11, kRegBufs>, grid, 128, reg_smem<Real, 11>(extra), p, s, kRegCarveout);
-    case 12: return launch_fft_kernel<Real>(mw_cols_kernel<Real, 12, kRegBufs>, grid, 256, reg_smem<Real, 12>(extra), p, s, kRegCarveout);
-    case 13: return launch_fft_kernel<Real>(mw_cols_kernel<Real, 13, kRegBufs>, grid, 512, reg_smem<Real, 13>(extra), p, s, kRegCarveout);
+    case 10: return launch_fft_kernel<Real>(mw_cols_kernel<Real, 10, kRegBufs>, grid, 64, reg_smem<Real, 10>(extra), p, s, reg_carveout<Real, 10>(extra));
+    case 11: return launch_fft_kernel<Real>(mw_cols_kernel<Real, 11, kRegBufs>, grid, 128, reg_smem<Real, 11>(extra), p, s, reg_carveout<Real, 11>(extra));
+    case 12: return launch_fft_kernel<Real>(mw_cols_kernel<Real, 12, kRegBufs>, grid, 256, reg_smem<Real, 12>(extra), p, s, reg_carveout<Real, 12>(extra));
+    case 13: return launch_fft_kernel<Real>(mw_cols_kernel<Real, 13, kRegBufs>, grid, 512, reg_smem<Real, 13>(extra), p, s, reg_carveout<Real, 13>(extra));
     default: break;
   }
   // one DFT buffer plus the 2L bins carried between the two transforms

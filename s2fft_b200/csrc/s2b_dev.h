@@ -23,6 +23,11 @@ struct Vec<double> {
   using t4 = double4;
 };
 
+// hint: bring the 128-byte line holding p (global memory) into L1
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
 template <typename T2>
 __device__ __forceinline__ void red_add(T2* addr, T2 v);
 template <>
