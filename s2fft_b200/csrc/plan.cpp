@@ -449,6 +449,7 @@ struct s2b_plan {
   // MW column chain: correction for the south-pole ring's odd (m + s) content (see
   // mw_pole_correction); MWSS real maps: theta-Nyquist bin split between -L and +L
   void* col_pole = nullptr;
+  void* col_imp = nullptr;  // impulse responses of the chain (col_impulse)
   int col_nyq_split = 0;
   size_t ws_adj_G = 0, ws_adj_y = 0;
   // precompute path: ring colatitudes of the kernel tables, table width
@@ -573,6 +574,66 @@ static std::vector<cd> mw_pole_correction(int L) {
     c[k] = u - direct;
   }
   return c;
+}
+
+// Response of the forward column chain (to the MWSS(2L) rings t = 0..2L, in the units of
+// the device's inverse-DFT output, before the overall factor and the weights) to a unit
+// impulse on the samples that are their own mirror in the theta extension of a column with
+// odd m + s: MW the pole ring (the direct chain's image of it plus the pole correction
+// `pole`), MWSS the poles t = 0 and t = L ([2][2L+1], with the Nyquist split for real
+// maps). The paired-column kernel keeps these samples out of the transform it shares
+// between two columns and adds them through this table.
+static std::vector<cd> col_impulse(int L, bool mw, const std::vector<cd>& pole, bool nyq_split) {
+  const int n4 = 4 * L, nout = 2 * L + 1;
+  std::vector<cd> w4(n4);
+  for (int j = 0; j < n4; ++j) w4[j] = std::polar(1.0, 2.0 * kPi * j / n4);
+  auto r4 = [&](long e) { return w4[((e % n4) + n4) % n4]; };
+  if (mw) {
+    // bins after the half-sample phase and 1/n1: (-1)^p / n1 (see mw_pole_correction)
+    const double n1 = 2.0 * L - 1.0;
+    std::vector<cd> imp(nout);
+    for (int k = 0; k < nout; ++k) {
+      cd v(0.0, 0.0);
+      for (int p = -(L - 1); p <= L - 1; ++p) v += ((p & 1) ? -1.0 : 1.0) / n1 * r4((long)p * k);
+      imp[k] = v + pole[k];
+    }
+    return imp;
+  }
+  // MWSS: bins 1 / n1 (t = 0) and (-1)^p / n1 (t = L), p = -L..L-1
+  const double n1 = 2.0 * L;
+  std::vector<cd> imp(2 * nout);
+  for (int which = 0; which < 2; ++which) {
+    for (int k = 0; k < nout; ++k) {
+      cd v(0.0, 0.0);
+      for (int p = -L; p <= L - 1; ++p)
+        v += ((which && (p & 1)) ? -1.0 : 1.0) / n1 * r4((long)p * k);
+      if (nyq_split && (k & 1)) {  // i N sin(pi k / 2), N = bin -L
+        const double N = ((which && (L & 1)) ? -1.0 : 1.0) / n1;
+        v += cd(0.0, ((k & 2) ? -1.0 : 1.0) * N);
+      }
+      imp[which * nout + k] = v;
+    }
+  }
+  return imp;
+}
+
+// The column chain's correction tables (pole correction, impulse responses, Nyquist split)
+// for complex maps or, real_map, as upstream treats real maps.
+static int set_col_tables(s2b_plan* p, bool real_map) {
+  const int L = p->d.L;
+  int rc;
+  std::vector<cd> c;
+  if (p->fwd_mode == 1) {
+    c = mw_pole_correction(L);
+    if (real_map)
+      for (cd& v : c) v = cd(v.real(), 0.0);
+    if ((rc = upload_complex(p, &p->col_pole, c))) return rc;
+  }
+  p->col_nyq_split = (p->fwd_mode == 2 && real_map) ? 1 : 0;
+  if ((rc = upload_complex(p, &p->col_imp,
+                           col_impulse(L, p->fwd_mode == 1, c, p->col_nyq_split != 0))))
+    return rc;
+  return S2B_OK;
 }
 
 static int build_plan(s2b_plan* p) {
@@ -949,13 +1010,7 @@ static int build_plan(s2b_plan* p) {
       pa[(pp + n2) % n2] = f;
     }
     if ((rc = upload_complex(p, &p->col_ph_adj, pa))) return rc;
-    if (p->fwd_mode == 1) {
-      std::vector<cd> c = mw_pole_correction(L);
-      if (d.reality)
-        for (cd& v : c) v = cd(v.real(), 0.0);
-      if ((rc = upload_complex(p, &p->col_pole, c))) return rc;
-    }
-    p->col_nyq_split = (p->fwd_mode == 2 && d.reality) ? 1 : 0;
+    if ((rc = set_col_tables(p, d.reality != 0))) return rc;
   }
   const size_t maxsmem = (size_t)227 * 1024;
   auto padded = [](int M) { return (size_t)M + (size_t)(M >> 3); };  // ring FFT buffer layout
@@ -1520,6 +1575,7 @@ static int fwd_stage_pre(s2b_plan* p, const void* f, char* ws, cudaStream_t s, F
     cp.d2_pow2 = p->M2 == 4 * L;
     cp.ph = p->col_ph;
     cp.pole = p->col_pole;
+    cp.imp = p->col_imp;
     cp.nyq_split = p->col_nyq_split;
     cp.weights = p->fwd_weights;
     cp.tb = tables<Real>(p);
@@ -1800,6 +1856,7 @@ static int run_pre_forward(s2b_plan* p, const void* K, const void* f, void* flm,
     cp.d2_pow2 = p->M2 == 4 * L;
     cp.ph = p->col_ph;
     cp.pole = p->col_pole;
+    cp.imp = p->col_imp;
     cp.nyq_split = p->col_nyq_split;
     cp.weights = p->fwd_weights;
     cp.tb = tables<Real>(p);
@@ -2183,14 +2240,7 @@ static int batch_run_forward(s2b_batch* b, const void* const* f, void* const* fl
 // Re(c) for the MW pole correction and the split theta-Nyquist bin for MWSS, as a reality
 // plan has them.
 static int use_real_map_chain(s2b_plan* p) {
-  if (p->fwd_mode == 1) {
-    std::vector<cd> c = mw_pole_correction(p->d.L);
-    for (cd& v : c) v = cd(v.real(), 0.0);
-    int rc;
-    if ((rc = upload_complex(p, &p->col_pole, c))) return rc;
-  }
-  p->col_nyq_split = p->fwd_mode == 2 ? 1 : 0;
-  return S2B_OK;
+  return p->fwd_mode != 0 ? set_col_tables(p, true) : S2B_OK;
 }
 
 static int build_wigner(s2b_plan* p) {

@@ -362,95 +362,17 @@ __global__ void __launch_bounds__(LOGM ? (1 << LOGM) / 16 : 512, reg_min_blocks<
 //   quadrature weights. The phi resampling 2L-1 -> 2L (resampling.py:248-281)
 //   reduces to the overall factor 2L/(2L-1) in the phi-Fourier domain.
 // ---------------------------------------------------------------------------
-// LOGM > 0: both transforms on the register engine (d1.M = d2.M = 2^LOGM, the inverse DFT
-// of power-of-two length 4L; blockDim.x = 2^LOGM / 16); LOGM = 0: the shared-memory passes.
-template <typename Real, int LOGM, int NBUF>
-__global__ void __launch_bounds__(LOGM ? (1 << LOGM) / 16 : 512, reg_min_blocks<Real>(LOGM))
-    mw_cols_kernel(ColsParams<Real> p) {
+// The column chain's output for column m of map b: chain(t) = the inverse-DFT value on
+// MWSS(2L) ring t (t = 0..2L) with the pole and Nyquist corrections, before the overall
+// factor and the weights; writes it in the layout ColsParams describes (raw, ring pairs,
+// or rows), and the zero padding once per map (column m = 0).
+template <typename Real, typename Chain>
+__device__ __forceinline__ void cols_emit(const ColsParams<Real>& p, int b, int m, Chain chain) {
   using R2 = typename C2<Real>::t;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const FFTDesc d1 = *p.d1;
-  const FFTDesc d2 = *p.d2;
-  // one DFT buffer for both transforms; the 2L-1 (2L) bins of the first that feed the
-  // second are kept, phase-multiplied, in tmp in between
-  R2* s1 = reinterpret_cast<R2*>(smem_raw);
-  R2* s2 = s1;
-  R2* tmp = s1 + (LOGM > 0 ? RegFFT<(LOGM > 0 ? LOGM : 8), NBUF>::SMEM_ELEMS
-                           : padded_len(d1.M > d2.M ? d1.M : d2.M));
   const int L = p.L;
-  const int mlo = p.mw ? -(L - 1) : -L;
-  const int ncm = L - mlo;
-  const int mi = blockIdx.x;
-  const int b = blockIdx.y;
-  const int m = mlo + mi;
-  if (m < -(L - 1)) return;  // MWSS m = -L never reaches the recursion
-  const R2* c = reinterpret_cast<const R2*>(p.in) + ((size_t)b * ncm + mi) * p.nin;
-  const int par = ((m + p.spin) % 2 + 2) % 2;
-  const Real sgn = par ? Real(-1) : Real(1);
-  const int n1 = d1.n;
-  auto load1 = [&](int t) -> R2 {
-    if (p.mw) {
-      if (t < L) return c[t];
-      return cscale(c[2 * L - 2 - t], sgn);  // t = L + jj -> c[L-2-jj]
-    }
-    if (t <= L) return c[t];
-    return cscale(c[2 * L - t], sgn);  // t = L+1+jj -> c[L-1-jj]
-  };
-  const int plo = p.mw ? -(L - 1) : -L;
-  const int phi = L - 1;
-  const int n2 = d2.n;  // 4L
-  const R2* __restrict__ ph = reinterpret_cast<const R2*>(p.ph);
-  if constexpr (LOGM > 0) {
-    // bin k of the theta DFT is p = k (k <= L-1) or k - n1; ph carries the Bluestein chirp
-    reg_dft<Real, LOGM, NBUF>(s1, d1, p.tb, false, false, false, load1, [&](int k, R2 v) {
-      const int pp = k <= phi ? k : k - n1;
-      if (pp >= plo) tmp[pp - plo] = cmul(v, ph[(pp + n2) % n2]);
-    });
-  } else {
-    dft_run<Real>(s1, d1, p.tb, false, load1);
-    for (int pp = plo + (int)threadIdx.x; pp <= phi; pp += blockDim.x) {
-      const int j = pmod(pp, n1);
-      const R2 g = d1.bluestein ? s1[pidx(j)] : s1[pidx(bitrev(j, d1.logM))];
-      tmp[pp - plo] = cmul(g, ph[(pp + n2) % n2]);
-    }
-  }
-  __syncthreads();
-  auto load2 = [&](int k) -> R2 {
-    // k = pp mod 4L for pp in [plo, phi]; zero outside
-    const int pp = k <= phi ? k : k - n2;
-    return (pp < plo || pp > phi) ? czero<R2>() : tmp[pp - plo];
-  };
-  // upstream's MWSS(L) detour (corrections described in ColsParams): the MW pole ring's odd
-  // (m + s) part, and for real MWSS maps the split theta-Nyquist bin (p = -L, tmp[0])
-  const R2* __restrict__ pole = (p.mw && par) ? reinterpret_cast<const R2*>(p.pole) : nullptr;
-  const R2 xpole = pole ? c[L - 1] : czero<R2>();
-  const R2 nyq = (!p.mw && p.nyq_split) ? tmp[0] : czero<R2>();
-  if constexpr (LOGM > 0) {
-    // the 4L outputs in natural order in shared memory (after a barrier: the transform's
-    // last exchange may still be read)
-    reg_dft<Real, LOGM, NBUF>(s2, d2, p.tb, true, true, true, load2,
-                              [&](int k, R2 v) { s2[ridx(k)] = v; });
-    __syncthreads();
-  } else {
-    dft_run<Real>(s2, d2, p.tb, true, load2);
-  }
   const int nout = 2 * L + 1;
   const int am = m < 0 ? -m : m;
   R2* out = reinterpret_cast<R2*>(p.out);
-  auto chain = [&](int t) -> R2 {
-    R2 u;
-    if constexpr (LOGM > 0)
-      u = s2[ridx(t)];
-    else
-      u = dft_get<Real>(s2, d2, p.tb, true, t);
-    if (pole) u = cadd(u, cmul(xpole, pole[t]));
-    if (t & 1) {  // i N sin(pi t / 2)
-      const Real sg = (t & 2) ? Real(-1) : Real(1);
-      u.x -= sg * nyq.y;
-      u.y += sg * nyq.x;
-    }
-    return u;
-  };
   if (p.raw) {
     if (m < p.m0) return;
     for (int t = threadIdx.x; t < nout; t += blockDim.x) {
@@ -564,6 +486,215 @@ __global__ void __launch_bounds__(LOGM ? (1 << LOGM) / 16 : 512, reg_min_blocks<
         }
     }
   }
+}
+
+// LOGM > 0: both transforms on the register engine (d1.M = d2.M = 2^LOGM, the inverse DFT
+// of power-of-two length 4L; blockDim.x = 2^LOGM / 16); LOGM = 0: the shared-memory passes.
+template <typename Real, int LOGM, int NBUF>
+__global__ void __launch_bounds__(LOGM ? (1 << LOGM) / 16 : 512, reg_min_blocks<Real>(LOGM))
+    mw_cols_kernel(ColsParams<Real> p) {
+  using R2 = typename C2<Real>::t;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const FFTDesc d1 = *p.d1;
+  const FFTDesc d2 = *p.d2;
+  // one DFT buffer for both transforms; the 2L-1 (2L) bins of the first that feed the
+  // second are kept, phase-multiplied, in tmp in between
+  R2* s1 = reinterpret_cast<R2*>(smem_raw);
+  R2* s2 = s1;
+  R2* tmp = s1 + (LOGM > 0 ? RegFFT<(LOGM > 0 ? LOGM : 8), NBUF>::SMEM_ELEMS
+                           : padded_len(d1.M > d2.M ? d1.M : d2.M));
+  const int L = p.L;
+  const int mlo = p.mw ? -(L - 1) : -L;
+  const int ncm = L - mlo;
+  const int mi = blockIdx.x;
+  const int b = blockIdx.y;
+  const int m = mlo + mi;
+  if (m < -(L - 1)) return;  // MWSS m = -L never reaches the recursion
+  const R2* c = reinterpret_cast<const R2*>(p.in) + ((size_t)b * ncm + mi) * p.nin;
+  const int par = ((m + p.spin) % 2 + 2) % 2;
+  const Real sgn = par ? Real(-1) : Real(1);
+  const int n1 = d1.n;
+  auto load1 = [&](int t) -> R2 {
+    if (p.mw) {
+      if (t < L) return c[t];
+      return cscale(c[2 * L - 2 - t], sgn);  // t = L + jj -> c[L-2-jj]
+    }
+    if (t <= L) return c[t];
+    return cscale(c[2 * L - t], sgn);  // t = L+1+jj -> c[L-1-jj]
+  };
+  const int plo = p.mw ? -(L - 1) : -L;
+  const int phi = L - 1;
+  const int n2 = d2.n;  // 4L
+  const R2* __restrict__ ph = reinterpret_cast<const R2*>(p.ph);
+  if constexpr (LOGM > 0) {
+    // bin k of the theta DFT is p = k (k <= L-1) or k - n1; ph carries the Bluestein chirp
+    reg_dft<Real, LOGM, NBUF>(s1, d1, p.tb, false, false, false, load1, [&](int k, R2 v) {
+      const int pp = k <= phi ? k : k - n1;
+      if (pp >= plo) tmp[pp - plo] = cmul(v, ph[(pp + n2) % n2]);
+    });
+  } else {
+    dft_run<Real>(s1, d1, p.tb, false, load1);
+    for (int pp = plo + (int)threadIdx.x; pp <= phi; pp += blockDim.x) {
+      const int j = pmod(pp, n1);
+      const R2 g = d1.bluestein ? s1[pidx(j)] : s1[pidx(bitrev(j, d1.logM))];
+      tmp[pp - plo] = cmul(g, ph[(pp + n2) % n2]);
+    }
+  }
+  __syncthreads();
+  auto load2 = [&](int k) -> R2 {
+    // k = pp mod 4L for pp in [plo, phi]; zero outside
+    const int pp = k <= phi ? k : k - n2;
+    return (pp < plo || pp > phi) ? czero<R2>() : tmp[pp - plo];
+  };
+  // upstream's MWSS(L) detour (corrections described in ColsParams): the MW pole ring's odd
+  // (m + s) part, and for real MWSS maps the split theta-Nyquist bin (p = -L, tmp[0])
+  const R2* __restrict__ pole = (p.mw && par) ? reinterpret_cast<const R2*>(p.pole) : nullptr;
+  const R2 xpole = pole ? c[L - 1] : czero<R2>();
+  const R2 nyq = (!p.mw && p.nyq_split) ? tmp[0] : czero<R2>();
+  if constexpr (LOGM > 0) {
+    // the 4L outputs in natural order in shared memory (after a barrier: the transform's
+    // last exchange may still be read)
+    reg_dft<Real, LOGM, NBUF>(s2, d2, p.tb, true, true, true, load2,
+                              [&](int k, R2 v) { s2[ridx(k)] = v; });
+    __syncthreads();
+  } else {
+    dft_run<Real>(s2, d2, p.tb, true, load2);
+  }
+  auto chain = [&](int t) -> R2 {
+    R2 u;
+    if constexpr (LOGM > 0)
+      u = s2[ridx(t)];
+    else
+      u = dft_get<Real>(s2, d2, p.tb, true, t);
+    if (pole) u = cadd(u, cmul(xpole, pole[t]));
+    if (t & 1) {  // i N sin(pi t / 2)
+      const Real sg = (t & 2) ? Real(-1) : Real(1);
+      u.x -= sg * nyq.y;
+      u.y += sg * nyq.x;
+    }
+    return u;
+  };
+  cols_emit(p, b, m, chain);
+}
+
+// Two columns per CTA on the register engine: m and m + 1 have opposite parities
+// (-1)^(m+s), so their theta extensions x_A, x_B are mirror-symmetric with opposite signs
+// (MW: x[n1-1-t] = s x[t]; MWSS: x[n1-t] = s x[t]), and so are the inverse-DFT outputs
+// u_A, u_B on the 4L circle (u[-t] = s u[t]: the half-sample phase keeps the symmetry). The
+// chain is linear and the same for both columns, so it runs once on z = x_A + i x_B and
+// u_A = (z'_t + s_A z'_-t) / 2, u_B = (z'_t - s_A z'_-t) / 2i separate the outputs. Parts
+// that break the symmetry stay out of z and are added per column:
+//   * the samples that are their own mirror (MW: the pole t = L-1; MWSS: t = 0 and L) of
+//     the odd column, through the chain's response to a unit impulse there
+//     (ColsParams::imp, which includes the pole and Nyquist corrections);
+//   * MWSS: the theta-Nyquist bin p = -L, which only the even column has (u gets
+//     N (-i)^t, and the split correction for real maps).
+// The last column of the odd count 2L-1 runs alone (x_B = 0).
+template <typename Real, int LOGM, int NBUF>
+__global__ void __launch_bounds__((1 << LOGM) / 16, reg_min_blocks<Real>(LOGM))
+    mw_cols_pair_kernel(ColsParams<Real> p) {
+  using R2 = typename C2<Real>::t;
+  using RF = RegFFT<LOGM, NBUF>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const FFTDesc d1 = *p.d1;
+  const FFTDesc d2 = *p.d2;
+  R2* s = reinterpret_cast<R2*>(smem_raw);
+  R2* tmp = s + RF::SMEM_ELEMS;
+  const int L = p.L;
+  const int mlo = p.mw ? -(L - 1) : -L;
+  const int ncm = L - mlo;
+  const int b = blockIdx.y;
+  const int mA = -(L - 1) + 2 * (int)blockIdx.x;
+  const bool hasB = mA + 1 <= L - 1;
+  const R2* cA = reinterpret_cast<const R2*>(p.in) + ((size_t)b * ncm + (mA - mlo)) * p.nin;
+  const R2* cB = cA + p.nin;
+  const bool oddA = (((mA + p.spin) % 2) + 2) % 2 == 1;
+  const Real sA = oddA ? Real(-1) : Real(1);
+  // extended sequence of a column, its self-mirrored samples left out when it is odd
+  auto xcol = [&](const R2* c, bool odd, int t) -> R2 {
+    const Real sg = odd ? Real(-1) : Real(1);
+    if (p.mw) {
+      if (t < L) return (odd && t == L - 1) ? czero<R2>() : c[t];
+      return cscale(c[2 * L - 2 - t], sg);
+    }
+    if (t <= L) return (odd && (t == 0 || t == L)) ? czero<R2>() : c[t];
+    return cscale(c[2 * L - t], sg);
+  };
+  auto load1 = [&](int t) -> R2 {
+    R2 v = xcol(cA, oddA, t);
+    if (hasB) {
+      const R2 w = xcol(cB, !oddA, t);
+      v.x -= w.y;
+      v.y += w.x;
+    }
+    return v;
+  };
+  const int plo = p.mw ? -(L - 1) : -L;
+  const int phi = L - 1;
+  const int n1 = d1.n;
+  const int n2 = d2.n;  // 4L
+  const R2* __restrict__ ph = reinterpret_cast<const R2*>(p.ph);
+  reg_dft<Real, LOGM, NBUF>(s, d1, p.tb, false, false, false, load1, [&](int k, R2 v) {
+    const int pp = k <= phi ? k : k - n1;
+    if (pp >= plo) tmp[pp - plo] = cmul(v, ph[(pp + n2) % n2]);
+  });
+  __syncthreads();
+  // MWSS: the Nyquist bin (tmp[0]) belongs to the even column alone
+  const R2 nyqZ = p.mw ? czero<R2>() : tmp[0];
+  auto load2 = [&](int k) -> R2 {
+    const int pp = k <= phi ? k : k - n2;
+    return (pp < plo || pp > phi || (!p.mw && pp == -L)) ? czero<R2>() : tmp[pp - plo];
+  };
+  reg_dft<Real, LOGM, NBUF>(s, d2, p.tb, true, true, true, load2,
+                            [&](int k, R2 v) { s[ridx(k)] = v; });
+  __syncthreads();
+  const R2* __restrict__ imp = reinterpret_cast<const R2*>(p.imp);
+  const int nout = 2 * L + 1;
+  // column A (B): sym = +1 (-1) picks u_A (u_B) out of z'
+  auto chain = [&](bool colA, int t) -> R2 {
+    const R2 zp = s[ridx(t)], zm = s[ridx(t == 0 ? 0 : n2 - t)];
+    R2 d;
+    d.x = (Real)0.5 * (colA ? zp.x + sA * zm.x : zp.x - sA * zm.x);
+    d.y = (Real)0.5 * (colA ? zp.y + sA * zm.y : zp.y - sA * zm.y);
+    R2 u = d;
+    if (!colA) {  // divide by i
+      u.x = d.y;
+      u.y = -d.x;
+    }
+    const bool odd = colA == oddA;
+    const R2* c = colA ? cA : cB;
+    if (odd) {
+      if (p.mw) {
+        u = cadd(u, cmul(c[L - 1], imp[t]));
+      } else {
+        u = cadd(u, cmul(c[0], imp[t]));
+        u = cadd(u, cmul(c[L], imp[nout + t]));
+      }
+    } else if (!p.mw) {
+      // N (-i)^t from the Nyquist bin, N = the even column's bin -L
+      R2 N = nyqZ;
+      if (!colA) {  // nyqZ = i N_B
+        N.x = nyqZ.y;
+        N.y = -nyqZ.x;
+      }
+      R2 e = N;
+      switch (t & 3) {
+        case 1: e.x = N.y; e.y = -N.x; break;    // -i N
+        case 2: e.x = -N.x; e.y = -N.y; break;   // -N
+        case 3: e.x = -N.y; e.y = N.x; break;    // i N
+        default: break;
+      }
+      u = cadd(u, e);
+      if (p.nyq_split && (t & 1)) {  // i N sin(pi t / 2)
+        const Real sg = (t & 2) ? Real(-1) : Real(1);
+        u.x -= sg * N.y;
+        u.y += sg * N.x;
+      }
+    }
+    return u;
+  };
+  cols_emit(p, b, mA, [&](int t) { return chain(true, t); });
+  if (hasB) cols_emit(p, b, mA + 1, [&](int t) { return chain(false, t); });
 }
 
 // ---------------------------------------------------------------------------
@@ -753,6 +884,17 @@ cudaError_t launch_mw_cols(const ColsParams<Real>& p, int ncm, int batch, int M1
   // register engine: one working length for both transforms, the second a plain power of two
   const int lg = (M1 == M2 && p.d2_pow2) ? reg_logm<Real>(M1) : 0;
   const int extra = 2 * p.L;
+  if (p.imp) {
+    // columns m, m+1 per CTA: L CTAs per map cover m = -(L-1) .. L-1
+    const dim3 gp(p.L, batch);
+    switch (lg) {
+      case 10: return launch_fft_kernel<Real>(mw_cols_pair_kernel<Real, 10, kRegBufs>, gp, 64, reg_smem<Real, 10>(extra), p, s, reg_carveout<Real, 10>(extra));
+      case 11: return launch_fft_kernel<Real>(mw_cols_pair_kernel<Real, 11, kRegBufs>, gp, 128, reg_smem<Real, 11>(extra), p, s, reg_carveout<Real, 11>(extra));
+      case 12: return launch_fft_kernel<Real>(mw_cols_pair_kernel<Real, 12, kRegBufs>, gp, 256, reg_smem<Real, 12>(extra), p, s, reg_carveout<Real, 12>(extra));
+      case 13: return launch_fft_kernel<Real>(mw_cols_pair_kernel<Real, 13, kRegBufs>, gp, 512, reg_smem<Real, 13>(extra), p, s, reg_carveout<Real, 13>(extra));
+      default: break;
+    }
+  }
   switch (lg) {
     case 10: return launch_fft_kernel<Real>(mw_cols_kernel<Real, 10, kRegBufs>, grid, 64, reg_smem<Real, 10>(extra), p, s, reg_carveout<Real, 10>(extra));
     case 11: return launch_fft_kernel<Real>(mw_cols_kernel<Real, 11, kRegBufs>, grid, 128, reg_smem<Real, 11>(extra), p, s, reg_carveout<Real, 11>(extra));

@@ -82,6 +82,12 @@ struct ColsParams {
   // MW: [2L+1] complex c_k, added as x_pole * c_k to the inverse-DFT output of columns with
   // odd m + s (x_pole = the input column's value on the ring theta = pi); nullptr: none
   const void* pole;
+  // the chain's response (before scale and weights) to a unit impulse on the samples that are
+  // their own mirror in the theta extension, for columns with odd m + s: MW [2L+1] (the pole
+  // ring t = L-1, pole correction included), MWSS [2][2L+1] (t = 0, t = L; Nyquist split
+  // included). Set: the register engine transforms two columns per CTA
+  // (mw_cols_pair_kernel); nullptr: one column per CTA
+  const void* imp;
   // MWSS real maps: the theta-Nyquist bin N (p = -L) counts half at -L and half at +L, i.e.
   // i N sin(pi k / 2) is added to the output on ring k
   int nyq_split;
