@@ -50,6 +50,10 @@ def parse_args():
                     help="seconds of host work for the CPU baseline sample")
     ap.add_argument("--profile-case", action="store_true",
                     help="small case for ncu: 2 steps, no baseline, no clocks")
+    ap.add_argument("--batch-profile", choices=["persistent", "streams"], default=None,
+                    help="the 256-map uneven batch, one eager inverse + forward of the given "
+                         "schedule between cudaProfilerStart/Stop (ncu --profile-from-start "
+                         "off)")
     return ap.parse_args()
 
 
@@ -451,12 +455,9 @@ def run_batched_uneven(torch, nmaps=256, steps=3, warmup=1, seed=4242):
     import s2fft_b200
     from s2fft_b200.batch import BatchedSHT
 
-    rng = np.random.default_rng(seed)
     Ls = [64, 128, 256, 512, 1024]
     smps = ["mw", "mwss", "dh", "gl"]
-    specs = [(int(rng.choice(Ls)), int(rng.integers(0, 4)), str(rng.choice(smps)))
-             for _ in range(nmaps)]
-    flms = [seeded_flm(rng, L, sp) for L, sp, _ in specs]
+    specs, flms = uneven_specs(nmaps, seed)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
     ms_sched = {}
     for sched in (True, False):  # each schedule forced, tuned and timed as a graph
@@ -502,6 +503,36 @@ def run_batched_uneven(torch, nmaps=256, steps=3, warmup=1, seed=4242):
                       "inverse_one_ring": sum(g.tuning[1] & 1 for g in b.groups),
                       "inverse_segments": {str(n): sum(g.tuning[2] == n for g in b.groups)
                                            for n in (1, 2, 4)}}}
+
+
+def uneven_specs(nmaps=256, seed=4242):
+    """The uneven 256-map mix: L uniform in {64..1024}, spin 0..3, four samplings."""
+    rng = np.random.default_rng(seed)
+    Ls = [64, 128, 256, 512, 1024]
+    smps = ["mw", "mwss", "dh", "gl"]
+    specs = [(int(rng.choice(Ls)), int(rng.integers(0, 4)), str(rng.choice(smps)))
+             for _ in range(nmaps)]
+    return specs, [seeded_flm(rng, L, sp) for L, sp, _ in specs]
+
+
+def profile_batched_uneven(torch, schedule):
+    """One eager inverse + forward of the uneven mix under the given schedule (tuned),
+    bracketed by cudaProfilerStart/Stop for a launch list of that call alone."""
+    from s2fft_b200.batch import BatchedSHT
+
+    specs, flms = uneven_specs()
+    b = BatchedSHT(specs, precision="f32", persistent=schedule == "persistent", graph=False)
+    b.load(flms)
+    b.run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
+    torch.cuda.profiler.start()
+    e0.record()
+    b.run()
+    e1.record()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    return {"schedule": schedule, "eager_ms": e0.elapsed_time(e1), "groups": len(b.groups)}
 
 
 def run_healpix_iter(torch, nside=256, L=512, steps=5, warmup=2):
@@ -675,6 +706,9 @@ def main():
     if args.tc_profile:
         print(json.dumps(run_batched_precompute(torch, L=args.L if args.L != 1024 else 256, B=64,
                                                 steps=1, warmup=1)))
+        return
+    if args.batch_profile:
+        print(json.dumps(profile_batched_uneven(torch, args.batch_profile)))
         return
     if args.profile_case:
         args.steps, args.warmup = 2, 1
