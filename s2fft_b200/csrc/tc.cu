@@ -208,7 +208,7 @@ __global__ void __launch_bounds__(256) pack_kernel_b2(const float2* __restrict__
 }
 
 // ---------------------------------------------------------------------------
-// the MMA kernel: grid (ceil(M/4), nlt, nbg), 128 threads
+// the MMA kernel: grid (nlt, ceil(M/4), nbg), 128 threads
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(128, 1) tc_forward_kernel(TcParams p) {
   extern __shared__ __align__(1024) unsigned char smem[];
@@ -217,7 +217,9 @@ __global__ void __launch_bounds__(128, 1) tc_forward_kernel(TcParams p) {
   uint64_t* done = empty + kStages;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int mg = blockIdx.x, lt = blockIdx.y, bg = blockIdx.z;
+  // l tiles vary fastest: the CTAs of one m group run side by side and read the same
+  // data blocks (B), which L2 then serves to all but the first
+  const int lt = blockIdx.x, mg = blockIdx.y, bg = blockIdx.z;
   const int mi0 = mg * kMPerCta;
   const int nm = min(kMPerCta, p.M - mi0);
 
@@ -382,7 +384,8 @@ cudaError_t launch_tc_forward(TcParams p, cudaStream_t s) {
   cudaError_t e = cudaFuncSetAttribute(tc_forward_kernel,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  dim3 grid((p.M + kMPerCta - 1) / kMPerCta, p.nlt, p.nbg);
+  dim3 grid(p.nlt, (p.M + kMPerCta - 1) / kMPerCta, p.nbg);
+  if (grid.y > 65535 || grid.z > 65535) return cudaErrorInvalidConfiguration;
   tc_forward_kernel<<<grid, 128, smem, s>>>(p);
   return cudaGetLastError();
 }
