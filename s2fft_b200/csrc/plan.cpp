@@ -462,6 +462,10 @@ struct s2b_plan {
   size_t ws_w_fban = 0, ws_w_tmp = 0, ws_w_sub = 0;
   // Wigner: the spin transforms of different n run concurrently on internal streams, forked
   // from and joined back to the caller's stream with events; one workspace slice per stream
+  // spin != 0: a second stream on which the low orders (lowm.cu) run beside the latitudinal
+  // kernel of a single-plan call
+  cudaStream_t aux = nullptr;
+  cudaEvent_t aux_fork = nullptr, aux_join = nullptr;
   static constexpr int kMaxWStreams = 8;
   int nwstream = 0;
   cudaStream_t wstream[kMaxWStreams] = {};
@@ -1054,6 +1058,11 @@ static int build_plan(s2b_plan* p) {
   if (p->tc)
     p->ws_pre_fwd = align256(p->ws_pre_fwd) + tc_packed_b_bytes(p->knth_fwd, d.batch, p->kM, hpc);
   p->ws_pre_inv = p->tc ? tc_packed_b_bytes(L, d.batch, p->kM, hpc) : 0;
+  if (d.spin != 0) {  // orders m < |s| (lowm.cu) run beside the latitudinal kernels
+    S2B_CK(cudaStreamCreateWithFlags(&p->aux, cudaStreamNonBlocking));
+    S2B_CK(cudaEventCreateWithFlags(&p->aux_fork, cudaEventDisableTiming));
+    S2B_CK(cudaEventCreateWithFlags(&p->aux_join, cudaEventDisableTiming));
+  }
   S2B_CK(cudaDeviceSynchronize());
   return S2B_OK;
 }
@@ -1244,11 +1253,11 @@ static int inv_stage_pre(s2b_plan* p, const void* flm, char* ws, cudaStream_t s,
 
 template <typename Real>
 static int inv_stage_post(s2b_plan* p, const Inv2Params& lp, void* f, char* ws, cudaStream_t s,
-                          const double* ring_w) {
+                          const double* ring_w, bool lowm_done = false) {
   const s2b_desc& d = p->d;
   const int L = d.L;
   void* ftm = ws + align256(p->ws_inv_F);
-  if (lp.nrings > 0)
+  if (lp.nrings > 0 && !lowm_done)
     if (int rc_ = run_lowm_synth(p, lp, p->inv_rings, s)) return rc_;
   RowsParams<Real> rp{};
   rp.L = L;
@@ -1278,12 +1287,23 @@ static int run_inverse(s2b_plan* p, const void* flm, void* f, char* ws, cudaStre
   Inv2Params lp{};
   int rc;
   if ((rc = inv_stage_pre<Real>(p, flm, ws, s, &lp))) return rc;
+  bool lowm_done = false;
   if (lp.nrings > 0) {
+    // the low orders (columns m < |s|, disjoint from the kernel's) beside the kernel: a few
+    // CTAs of long sequential loops that would otherwise run alone after it
+    if (lp.mlo > 0 && p->aux) {
+      S2B_CK(cudaEventRecord(p->aux_fork, s));
+      S2B_CK(cudaStreamWaitEvent(p->aux, p->aux_fork, 0));
+      if ((rc = run_lowm_synth(p, lp, p->inv_rings, p->aux))) return rc;
+      S2B_CK(cudaEventRecord(p->aux_join, p->aux));
+      lowm_done = true;
+    }
     if (p->ev_begin[0]) S2B_CK(cudaEventRecord(p->ev_begin[0], s));
     S2B_CK(launch_inv2(p->fp64, p->dual, lp, s));
     if (p->ev_end[0]) S2B_CK(cudaEventRecord(p->ev_end[0], s));
+    if (lowm_done) S2B_CK(cudaStreamWaitEvent(s, p->aux_join, 0));
   }
-  return inv_stage_post<Real>(p, lp, f, ws, s, ring_w);
+  return inv_stage_post<Real>(p, lp, f, ws, s, ring_w, lowm_done);
 }
 
 // HEALPix ring FFTs alone (s2fft/utils/healpix_ffts.py:187-423): per ring FFT, fftshift and
@@ -1638,12 +1658,13 @@ static int fwd_stage_pre(s2b_plan* p, const void* f, char* ws, cudaStream_t s, F
 
 template <typename Real>
 static int fwd_stage_post(s2b_plan* p, const Fwd2Params& lp_all, void* flm, char* ws,
-                          cudaStream_t s) {
+                          cudaStream_t s, bool lowm_done = false) {
   const s2b_desc& d = p->d;
   const int L = d.L;
   char* G = ws + align256(p->ws_fwd_cols);
   char* acc = G + align256(p->ws_fwd_G);
-  if (int rc_ = run_lowm_project(p, lp_all, p->fwd_rings, s)) return rc_;
+  if (!lowm_done)
+    if (int rc_ = run_lowm_project(p, lp_all, p->fwd_rings, s)) return rc_;
   StageParams sp{};
   sp.L = L;
   sp.L0 = d.L_lower;
@@ -1672,10 +1693,19 @@ static int run_forward_once(s2b_plan* p, const void* f, void* flm, char* ws, cud
   Fwd2Params lp{}, lp_all{};
   int rc;
   if ((rc = fwd_stage_pre<Real>(p, f, ws, s, &lp, &lp_all))) return rc;
+  // the low orders (rows m < |s| of the accumulator, disjoint from the kernel's) beside it
+  const bool lowm_aux = lp_all.mlo > 0 && lp_all.nrings > 0 && p->aux;
+  if (lowm_aux) {
+    S2B_CK(cudaEventRecord(p->aux_fork, s));
+    S2B_CK(cudaStreamWaitEvent(p->aux, p->aux_fork, 0));
+    if ((rc = run_lowm_project(p, lp_all, p->fwd_rings, p->aux))) return rc;
+    S2B_CK(cudaEventRecord(p->aux_join, p->aux));
+  }
   if (p->ev_begin[1]) S2B_CK(cudaEventRecord(p->ev_begin[1], s));
   S2B_CK(launch_fwd2(p->fp64, p->dual, lp, s));
   if (p->ev_end[1]) S2B_CK(cudaEventRecord(p->ev_end[1], s));
-  return fwd_stage_post<Real>(p, lp_all, flm, ws, s);
+  if (lowm_aux) S2B_CK(cudaStreamWaitEvent(s, p->aux_join, 0));
+  return fwd_stage_post<Real>(p, lp_all, flm, ws, s, lowm_aux);
 }
 
 template <typename Real>
@@ -2437,6 +2467,9 @@ int s2b_plan_destroy(s2b_plan* p) {
   if (!p) return S2B_OK;
   for (s2b_plan* sp : p->subs) s2b_plan_destroy(sp);
   for (void* a : p->allocs) cudaFree(a);
+  if (p->aux) cudaStreamDestroy(p->aux);
+  if (p->aux_fork) cudaEventDestroy(p->aux_fork);
+  if (p->aux_join) cudaEventDestroy(p->aux_join);
   for (int k = 0; k < s2b_plan::kMaxWStreams; ++k) {
     if (p->wstream[k]) cudaStreamDestroy(p->wstream[k]);
     if (p->wjoin[k]) cudaEventDestroy(p->wjoin[k]);
