@@ -82,6 +82,62 @@ __global__ void prologue_kernel(StageParams p) {
   }
 }
 
+// Blocked layout (p.Lp > 0, Q = 32): the same table, a 32 (m) x 32 (l) tile per CTA through
+// shared memory, since flm is [l][m] and F is [m][l]: the coefficients are read with
+// consecutive threads on consecutive m, the table (and g) with consecutive threads on
+// consecutive l. grid (ceil(TR / 32), C, batch * nhalf), 32 x 8 threads.
+template <typename Real>
+__global__ void __launch_bounds__(256) prologue_tiled_kernel(StageParams p) {
+  using R2 = R2_t<Real>;
+  using R4 = R4_t<Real>;
+  __shared__ R2 ta[32][33], tc[32][33];  // [q][m]: flm at +m and at -m, padded
+  const int L = p.L, C = p.nclass, TR = p.TR;
+  const int m0 = (int)blockIdx.x * 32 - kPadLo, j = blockIdx.y;
+  const int half = (int)(blockIdx.z % p.nhalf), b = (int)(blockIdx.z / p.nhalf);
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const R2* flm = reinterpret_cast<const R2*>(p.flm) + (size_t)b * L * (2 * L - 1);
+  for (int qq = ty; qq < 32; qq += 8) {
+    const int l = 32 * j + qq, m = m0 + tx;
+    R2 a, c;
+    a.x = a.y = c.x = c.y = 0;
+    if (m >= 0 && m < L && l < L && l >= m) {
+      const R2* row = flm + (size_t)l * (2 * L - 1) + (L - 1);
+      if (p.dual || half == 0) a = row[m];
+      if (p.dual || half == 1) c = row[-m];
+    }
+    ta[qq][tx] = a;
+    tc[qq][tx] = c;
+  }
+  __syncthreads();
+  const int as = p.spin < 0 ? -p.spin : p.spin;
+  const double sgn_s = (p.spin & 1) ? -1.0 : 1.0;
+  for (int mm = ty; mm < 32; mm += 8) {
+    const int m = m0 + mm, mrow = m + kPadLo, l = 32 * j + tx;
+    if (mrow >= TR) continue;
+    const bool ok = m >= 0 && m < L && l < L && l >= m && l >= p.L0 && l >= as;
+    const double g = ok ? p.g[(size_t)m * L + l] * lnorm(l) : 0.0;
+    const double sgn_m = (m & 1) ? -1.0 : 1.0;
+    const size_t idx = ((((size_t)b * p.nhalf + half) * C + j) * TR + mrow) * 32 + tx;
+    if (p.dual) {
+      const R2 a = ta[tx][mm], c = tc[tx][mm];
+      const double gn = m > 0 ? g * sgn_m : 0.0;
+      R4 o;
+      o.x = (Real)(g * a.x);
+      o.y = (Real)(g * a.y);
+      o.z = (Real)(gn * c.x);
+      o.w = (Real)(gn * c.y);
+      reinterpret_cast<R4*>(p.F)[idx] = o;
+    } else {
+      const R2 a = half == 0 ? ta[tx][mm] : tc[tx][mm];
+      const double f = half == 0 ? g * sgn_s : (m > 0 ? g * sgn_m : 0.0);
+      R2 o;
+      o.x = (Real)(f * a.x);
+      o.y = (Real)(f * a.y);
+      reinterpret_cast<R2*>(p.F)[idx] = o;
+    }
+  }
+}
+
 // Pole rows of the inverse: ftm[pole][L-1+ms+mo] = (-1)^s sum_l sign_l N_l flm[l][L-1+ms],
 // south (theta = pi): ms = s, sign_l = (-1)^(l-s); north (theta = 0): ms = -s, sign 1.
 template <typename Real>
@@ -140,88 +196,120 @@ __device__ __forceinline__ R2_t<Real> spectrum_at(const StageParams& p, int b, i
   return z;
 }
 
-// flm [b][l][L-1+m] from the projected sums acc [b][half][j][m][q].
-template <typename Real, typename Idx>
-__global__ void epilogue_kernel(StageParams p) {
+// flm[b][l][L-1+m] from the projected sums acc [b][half][j][m][q] (one element).
+template <typename Real>
+__device__ __forceinline__ R2_t<Real> epi_value(const StageParams& p, int b, int l, int m) {
   using R2 = R2_t<Real>;
   const int L = p.L, C = p.nclass, Q = p.Q;
-  const int W = 2 * L - 1;
-  const Idx total = (Idx)p.batch * L * W;
   const int as = p.spin < 0 ? -p.spin : p.spin;
   const int lmin = as > p.L0 ? as : p.L0;
   const double sgn_s = (p.spin & 1) ? -1.0 : 1.0;
+  const int am = m < 0 ? -m : m;
+  double re = 0.0, im = 0.0;
+  if (l >= lmin && am <= l) {
+    const int j = l % C, q = l / C;
+    // offset of (m, l) in one [batch][half] slice of the forward sums, in R2/R4 units
+    const size_t cell = p.Lp > 0 ? (size_t)am * p.Lp + l : ((size_t)j * L + am) * Q + q;
+    const size_t slice = p.Lp > 0 ? (size_t)L * p.Lp : (size_t)C * L * Q;
+    const double g = p.g[(size_t)am * L + l];
+    double ar = 0.0, ai = 0.0;
+    bool conj_mirror = false;
+    if (p.dual) {
+      const R2* A = reinterpret_cast<const R2*>(p.acc);
+      const R2 a = A[((size_t)b * slice + cell) * 2 + (m < 0 ? 1 : 0)];
+      ar = a.x;
+      ai = a.y;
+    } else if (m >= 0 || p.nhalf > 1) {
+      const int half = m >= 0 ? 0 : 1;
+      const R2* A = reinterpret_cast<const R2*>(p.acc);
+      const R2 a = A[((size_t)b * p.nhalf + half) * slice + cell];
+      ar = a.x;
+      ai = a.y;
+    } else {
+      // reality: flm[l, -m] = (-1)^m conj(flm[l, m])
+      const R2* A = reinterpret_cast<const R2*>(p.acc);
+      const R2 a = A[(size_t)b * slice + cell];
+      ar = a.x;
+      ai = a.y;
+      conj_mirror = true;
+    }
+    // d-projection with the m < 0 symmetry sign (-1)^(m+s) (spin folded below)
+    double f = g;
+    if (m < 0 && !conj_mirror) f *= ((am + p.spin) % 2 + 2) % 2 ? -1.0 : 1.0;
+    re = f * ar;
+    im = f * ai;
+    // closed-form pole rings (each present pole: theta = pi contributes at m = s, theta = 0 at
+    // m = -s)
+    if (!conj_mirror) {
+      if (p.pole_south >= 0 && m == p.spin) {
+        const R2 s = spectrum_at<Real>(p, b, p.pole_south, m);
+        const double sg = ((l - p.spin) % 2 + 2) % 2 ? -1.0 : 1.0;
+        re += sg * s.x;
+        im += sg * s.y;
+      }
+      if (p.pole_north >= 0 && m == -p.spin) {
+        const R2 s = spectrum_at<Real>(p, b, p.pole_north, m);
+        re += s.x;
+        im += s.y;
+      }
+    }
+    const double nl = lnorm(l) * sgn_s;
+    re *= nl;
+    im *= nl;
+    if (conj_mirror) {
+      // value above is flm[l, |m|]; mirror (-1)^m conj(.)
+      const double sm = (am & 1) ? -1.0 : 1.0;
+      im = -im;
+      re *= sm;
+      im *= sm;
+    }
+  }
+  R2 o;
+  o.x = (Real)re;
+  o.y = (Real)im;
+  return o;
+}
+
+// flm [b][l][L-1+m] from the projected sums, one element per thread (any layout).
+template <typename Real, typename Idx>
+__global__ void epilogue_kernel(StageParams p) {
+  const int L = p.L;
+  const int W = 2 * L - 1;
+  const Idx total = (Idx)p.batch * L * W;
   for (Idx idx = blockIdx.x * (Idx)blockDim.x + threadIdx.x; idx < total;
        idx += (Idx)gridDim.x * blockDim.x) {
     const Idx lw = idx / (Idx)W;
     const int c = (int)(idx - lw * (Idx)W);
     const Idx bl = lw / (Idx)L;
     const int l = (int)(lw - bl * (Idx)L);
-    const int b = (int)bl;
-    const int m = c - (L - 1);
-    const int am = m < 0 ? -m : m;
-    double re = 0.0, im = 0.0;
-    if (l >= lmin && am <= l) {
-      const int j = l % C, q = l / C;
-      // offset of (m, l) in one [batch][half] slice of the forward sums, in R2/R4 units
-      const size_t cell = p.Lp > 0 ? (size_t)am * p.Lp + l : ((size_t)j * L + am) * Q + q;
-      const size_t slice = p.Lp > 0 ? (size_t)L * p.Lp : (size_t)C * L * Q;
-      const double g = p.g[(size_t)am * L + l];
-      double ar = 0.0, ai = 0.0;
-      bool conj_mirror = false;
-      if (p.dual) {
-        const R2* A = reinterpret_cast<const R2*>(p.acc);
-        const R2 a = A[((size_t)b * slice + cell) * 2 + (m < 0 ? 1 : 0)];
-        ar = a.x;
-        ai = a.y;
-      } else if (m >= 0 || p.nhalf > 1) {
-        const int half = m >= 0 ? 0 : 1;
-        const R2* A = reinterpret_cast<const R2*>(p.acc);
-        const R2 a = A[((size_t)b * p.nhalf + half) * slice + cell];
-        ar = a.x;
-        ai = a.y;
-      } else {
-        // reality: flm[l, -m] = (-1)^m conj(flm[l, m])
-        const R2* A = reinterpret_cast<const R2*>(p.acc);
-        const R2 a = A[(size_t)b * slice + cell];
-        ar = a.x;
-        ai = a.y;
-        conj_mirror = true;
-      }
-      // d-projection with the m < 0 symmetry sign (-1)^(m+s) (spin folded below)
-      double f = g;
-      if (m < 0 && !conj_mirror) f *= ((am + p.spin) % 2 + 2) % 2 ? -1.0 : 1.0;
-      re = f * ar;
-      im = f * ai;
-      // closed-form pole rings (each present pole: theta = pi contributes at m = s, theta = 0 at
-      // m = -s)
-      if (!conj_mirror) {
-        if (p.pole_south >= 0 && m == p.spin) {
-          const R2 s = spectrum_at<Real>(p, b, p.pole_south, m);
-          const double sg = ((l - p.spin) % 2 + 2) % 2 ? -1.0 : 1.0;
-          re += sg * s.x;
-          im += sg * s.y;
-        }
-        if (p.pole_north >= 0 && m == -p.spin) {
-          const R2 s = spectrum_at<Real>(p, b, p.pole_north, m);
-          re += s.x;
-          im += s.y;
-        }
-      }
-      const double nl = lnorm(l) * sgn_s;
-      re *= nl;
-      im *= nl;
-      if (conj_mirror) {
-        // value above is flm[l, |m|]; mirror (-1)^m conj(.)
-        const double sm = (am & 1) ? -1.0 : 1.0;
-        im = -im;
-        re *= sm;
-        im *= sm;
-      }
-    }
-    R2 o;
-    o.x = (Real)re;
-    o.y = (Real)im;
-    reinterpret_cast<R2*>(p.flm_out)[idx] = o;
+    reinterpret_cast<R2_t<Real>*>(p.flm_out)[idx] = epi_value<Real>(p, (int)bl, l, c - (L - 1));
+  }
+}
+
+// Blocked layouts: the sums are [m][l] and flm is [l][m], so a CTA transposes a 32 x 32
+// tile through shared memory: it computes the tile with consecutive threads on
+// consecutive l (coalesced reads of the sums and of g) and writes it with consecutive
+// threads on consecutive m. grid (ceil((2L-1)/32), ceil(L/32), batch), 32 x 8 threads.
+template <typename Real>
+__global__ void __launch_bounds__(256) epilogue_tiled_kernel(StageParams p) {
+  using R2 = R2_t<Real>;
+  __shared__ R2 tile[32][33];  // [c][l], padded
+  const int L = p.L, W = 2 * L - 1;
+  const int c0 = blockIdx.x * 32, l0 = blockIdx.y * 32, b = blockIdx.z;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  for (int cc = ty; cc < 32; cc += 8) {
+    const int c = c0 + cc, l = l0 + tx;
+    R2 v;
+    v.x = 0;
+    v.y = 0;
+    if (c < W && l < L) v = epi_value<Real>(p, b, l, c - (L - 1));
+    tile[cc][tx] = v;
+  }
+  __syncthreads();
+  R2* out = reinterpret_cast<R2*>(p.flm_out) + (size_t)b * L * W;
+  for (int ll = ty; ll < 32; ll += 8) {
+    const int l = l0 + ll, c = c0 + tx;
+    if (l < L && c < W) out[(size_t)l * W + c] = tile[tx][ll];
   }
 }
 
@@ -257,6 +345,14 @@ static int grid_for(long n) {
 static bool fits32(long n) { return n + 65535L * 256 < (1L << 32); }
 
 cudaError_t launch_prologue(bool fp64, const StageParams& p, cudaStream_t s) {
+  if (p.Lp > 0 && p.Q == 32 && (long)p.batch * p.nhalf <= 65535 && p.nclass <= 65535) {
+    const dim3 grid((p.TR + 31) / 32, p.nclass, p.batch * p.nhalf);
+    if (fp64)
+      prologue_tiled_kernel<double><<<grid, dim3(32, 8), 0, s>>>(p);
+    else
+      prologue_tiled_kernel<float><<<grid, dim3(32, 8), 0, s>>>(p);
+    return cudaGetLastError();
+  }
   const long total = (long)p.batch * p.nhalf * p.nclass * p.TR * p.Q;
   const bool i32 = fits32(total);
   if (fp64 && i32)
@@ -280,6 +376,14 @@ cudaError_t launch_poles(bool fp64, const StageParams& p, cudaStream_t s) {
 }
 
 cudaError_t launch_epilogue(bool fp64, const StageParams& p, cudaStream_t s) {
+  if (p.Lp > 0 && p.batch <= 65535) {
+    const dim3 grid((2 * p.L - 1 + 31) / 32, (p.L + 31) / 32, p.batch);
+    if (fp64)
+      epilogue_tiled_kernel<double><<<grid, dim3(32, 8), 0, s>>>(p);
+    else
+      epilogue_tiled_kernel<float><<<grid, dim3(32, 8), 0, s>>>(p);
+    return cudaGetLastError();
+  }
   const long total = (long)p.batch * p.L * (2 * p.L - 1);
   const bool i32 = fits32(total);
   if (fp64 && i32)
