@@ -9,7 +9,10 @@
  * calls (s2b_inverse, s2b_forward, s2b_wigner_*, s2b_precompute_*) are
  * stream-ordered on the given cudaStream_t (passed as void*) and perform no
  * device allocation and no host synchronisation, so they can be captured in a
- * CUDA graph once the plan exists. Plan creation allocates the plan's tables;
+ * CUDA graph once the plan exists. Several host threads may call one plan at
+ * once, each with its own workspace and stream (spin plans with spin != 0 and
+ * Wigner plans fork to streams the plan owns; the fork is made atomic per
+ * plan). Plan creation allocates the plan's tables;
  * s2b_kernel_build with S2B_BF16X3 allocates and frees a temporary table.
  *
  * Array layouts (row-major, innermost last), for B = desc.batch maps:

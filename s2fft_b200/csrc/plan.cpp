@@ -466,6 +466,9 @@ struct s2b_plan {
   // kernel of a single-plan call
   cudaStream_t aux = nullptr;
   cudaEvent_t aux_fork = nullptr, aux_join = nullptr;
+  // makes each event record + wait pair of a fork atomic, so that calls from several host
+  // threads on one plan do not fork from each other's streams
+  std::mutex fork_mu;
   static constexpr int kMaxWStreams = 8;
   int nwstream = 0;
   cudaStream_t wstream[kMaxWStreams] = {};
@@ -1292,8 +1295,11 @@ static int run_inverse(s2b_plan* p, const void* flm, void* f, char* ws, cudaStre
     // the low orders (columns m < |s|, disjoint from the kernel's) beside the kernel: a few
     // CTAs of long sequential loops that would otherwise run alone after it
     if (lp.mlo > 0 && p->aux) {
-      S2B_CK(cudaEventRecord(p->aux_fork, s));
-      S2B_CK(cudaStreamWaitEvent(p->aux, p->aux_fork, 0));
+      {
+        std::lock_guard<std::mutex> lk(p->fork_mu);
+        S2B_CK(cudaEventRecord(p->aux_fork, s));
+        S2B_CK(cudaStreamWaitEvent(p->aux, p->aux_fork, 0));
+      }
       if ((rc = run_lowm_synth(p, lp, p->inv_rings, p->aux))) return rc;
       S2B_CK(cudaEventRecord(p->aux_join, p->aux));
       lowm_done = true;
@@ -1696,8 +1702,11 @@ static int run_forward_once(s2b_plan* p, const void* f, void* flm, char* ws, cud
   // the low orders (rows m < |s| of the accumulator, disjoint from the kernel's) beside it
   const bool lowm_aux = lp_all.mlo > 0 && lp_all.nrings > 0 && p->aux;
   if (lowm_aux) {
-    S2B_CK(cudaEventRecord(p->aux_fork, s));
-    S2B_CK(cudaStreamWaitEvent(p->aux, p->aux_fork, 0));
+    {
+      std::lock_guard<std::mutex> lk(p->fork_mu);
+      S2B_CK(cudaEventRecord(p->aux_fork, s));
+      S2B_CK(cudaStreamWaitEvent(p->aux, p->aux_fork, 0));
+    }
     if ((rc = run_lowm_project(p, lp_all, p->fwd_rings, p->aux))) return rc;
     S2B_CK(cudaEventRecord(p->aux_join, p->aux));
   }
@@ -2326,6 +2335,7 @@ static int run_wigner(s2b_plan* p, bool forward, const void* in, void* out, char
   int rc;
   if (forward) S2B_CK(launch_gamma_forward(p->fp64, in, fban, d.batch, d.N, p->npix, d.reality, s));
   if (K > 1) {
+    std::lock_guard<std::mutex> lk(p->fork_mu);
     S2B_CK(cudaEventRecord(p->wfork, s));
     for (int k = 0; k < K; ++k) S2B_CK(cudaStreamWaitEvent(p->wstream[k], p->wfork, 0));
   }
