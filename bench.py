@@ -50,6 +50,9 @@ def parse_args():
                     help="seconds of host work for the CPU baseline sample")
     ap.add_argument("--profile-case", action="store_true",
                     help="small case for ncu: 2 steps, no baseline, no clocks")
+    ap.add_argument("--healpix-profile", action="store_true",
+                    help="HEALPix nside=256 L=512 real float32: one inverse and one forward "
+                         "with 3 iterations between cudaProfilerStart/Stop")
     ap.add_argument("--batch-profile", choices=["persistent", "streams"], default=None,
                     help="the 256-map uneven batch, one eager inverse + forward of the given "
                          "schedule between cudaProfilerStart/Stop (ncu --profile-from-start "
@@ -535,6 +538,34 @@ def profile_batched_uneven(torch, schedule):
     return {"schedule": schedule, "eager_ms": e0.elapsed_time(e1), "groups": len(b.groups)}
 
 
+def profile_healpix(torch, nside=256, L=512):
+    """One float32 HEALPix inverse and forward (3 iterations) after a warm-up call, between
+    cudaProfilerStart/Stop."""
+    import s2fft_b200
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    flm = torch.from_numpy(seeded_flm(np.random.default_rng(7), L, 0, True)).to(dev,
+                                                                                 torch.complex64)
+
+    def call():
+        f = s2fft_b200.inverse(flm, L, 0, nside, "healpix", reality=True, precision="f32")
+        return s2fft_b200.forward(f, L, 0, nside, "healpix", reality=True, iter=3,
+                                  precision="f32")
+
+    call()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
+    torch.cuda.profiler.start()
+    e0.record()
+    g = call()
+    e1.record()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    err = ((g - flm).abs().max() / flm.abs().max()).item()
+    return {"workload": f"healpix nside={nside} L={L} reality f32, inverse + forward iter=3",
+            "eager_ms": e0.elapsed_time(e1), "roundtrip_max_rel_err": err}
+
+
 def run_healpix_iter(torch, nside=256, L=512, steps=5, warmup=2):
     """HEALPix nside=256, L=512, real signal: inverse + forward with 3 refinement iterations."""
     import s2fft_b200
@@ -706,6 +737,9 @@ def main():
     if args.tc_profile:
         print(json.dumps(run_batched_precompute(torch, L=args.L if args.L != 1024 else 256, B=64,
                                                 steps=1, warmup=1)))
+        return
+    if args.healpix_profile:
+        print(json.dumps(profile_healpix(torch)))
         return
     if args.batch_profile:
         print(json.dumps(profile_batched_uneven(torch, args.batch_profile)))

@@ -195,7 +195,29 @@ __global__ void __launch_bounds__(LOGM ? (1 << LOGM) / 16 : 512, reg_min_blocks<
       }
     }
   } else {
-    dft_run<Real>(s, d, p.tb, true, load);
+    // rings with fewer pixels than columns (HEALPix polar rings): the aliased sums X_k are
+    // spread over the CTA (thread = bin k and chunk c of its aliases) and combined in a
+    // fixed order, instead of one thread per bin walking all ncol / n aliases
+    R2* xs = p.alias_off ? s + p.alias_off : nullptr;
+    const bool pre = xs != nullptr && n < p.ncol;
+    if (pre) {
+      const int nc = n < (int)blockDim.x ? (int)blockDim.x / n : 1;
+      for (int u = threadIdx.x; u < n * nc; u += blockDim.x) {
+        const int k = u % n, c = u / n;
+        const int mk = mlo + pmod(k - mlo, n);  // lowest m == k (mod n) in range
+        R2 acc = czero<R2>();
+        for (int m = mk + c * n; m <= mhi; m += n * nc) acc = cadd(acc, coef(m));
+        xs[u] = acc;
+      }
+      __syncthreads();
+      for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        R2 acc = xs[k];
+        for (int c = 1; c < nc; ++c) acc = cadd(acc, xs[c * n + k]);
+        xs[k] = acc;  // the chunks c >= 1 of bin k lie above n: no other bin reads slot k
+      }
+      __syncthreads();
+    }
+    dft_run<Real>(s, d, p.tb, true, [&](int k) -> R2 { return pre ? xs[k] : load(k); });
     if (p.real_out) {
       Real* out = reinterpret_cast<Real*>(p.out) + (size_t)b * p.out_batch_stride + p.ring_off[t];
       for (int j = threadIdx.x; j < n; j += blockDim.x)
@@ -856,8 +878,17 @@ cudaError_t launch_inv_rows(const RowsParams<Real>& p, int nrings, int batch, in
     case 13: return launch_fft_kernel<Real>(inv_rows_kernel<Real, 13, kRegBufs>, grid, 512, reg_smem<Real, 13>(0), p, s, reg_carveout<Real, 13>(0));
     default: break;
   }
-  const size_t smem = (size_t)padded_len(maxM) * sizeof(R2);
-  return launch_fft_kernel<Real>(inv_rows_kernel<Real, 0, 1>, grid, fft_threads(maxM), smem, p, s);
+  // shared-memory passes, plus (when it fits) the buffer of the aliased sums
+  RowsParams<Real> q = p;
+  const int nt = fft_threads(maxM);
+  size_t smem = (size_t)padded_len(maxM) * sizeof(R2);
+  const size_t extra = (size_t)(nt > maxM ? nt : maxM) * sizeof(R2);
+  q.alias_off = 0;
+  if (smem + extra <= (size_t)227 * 1024) {
+    q.alias_off = padded_len(maxM);
+    smem += extra;
+  }
+  return launch_fft_kernel<Real>(inv_rows_kernel<Real, 0, 1>, grid, nt, smem, q, s);
 }
 
 template <typename Real>

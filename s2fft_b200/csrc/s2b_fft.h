@@ -59,6 +59,8 @@ struct RowsParams {
                         // (nullptr: 1)
   const double* phi0;   // HEALPix ring phase (nullptr: none)
   const int* col_of_ring; // forward spectra: column of ring t (nullptr: t)
+  int alias_off;        // inverse, shared-memory passes: offset (complex elements) of the
+                        // aliased-sum buffer in shared memory (0: none; set by the launcher)
   FFTTables<Real> tb;
   const void* in;
   void* out;
