@@ -325,7 +325,7 @@ struct FFTBuild {
     }
     d.rtw_off = -1;
     d.rbf_off = -1;
-    const bool reg = d.logM >= 10 && d.logM <= 13;
+    const bool reg = d.logM >= 8 && d.logM <= 13;
     if (reg) {
       auto rt = rtw_by_M.find(d.M);
       if (rt == rtw_by_M.end()) {

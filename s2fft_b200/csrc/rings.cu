@@ -35,9 +35,12 @@ namespace s2b {
 // threads for 8192 points. The shared-memory passes (LOGM = 0): two in float, one in double.
 template <typename Real>
 __host__ __device__ constexpr int reg_min_blocks(int logm) {
+  // (registers are allocated per warp: a CTA of fewer than 32 threads counts as one warp;
+  // 256 points, whose 16 threads do the work of a warp, get half the warps per SM)
   return logm == 0    ? (sizeof(Real) == 4 ? 2 : 1)
          : logm >= 13 ? 1
-                      : ((sizeof(Real) == 4 ? 1024 : 512) >> (logm - 4));
+                      : (((sizeof(Real) == 4 ? 1024 : 512) >> (logm <= 8 ? 1 : 0)) >>
+                         (logm - 4 > 5 ? logm - 4 : 5));
 }
 
 // Any-length DFT of one CTA on the register engine (M = 2^LOGM, blockDim.x = M / 16; d.M
@@ -824,7 +827,7 @@ static int fft_threads(int M) {
 template <typename Real>
 static int reg_logm(int M) {
   const int top = sizeof(Real) == 4 ? 13 : 12;
-  for (int lg = 10; lg <= top; ++lg)
+  for (int lg = 8; lg <= top; ++lg)
     if (M == (1 << lg)) return lg;
   return 0;
 }
@@ -872,6 +875,8 @@ cudaError_t launch_inv_rows(const RowsParams<Real>& p, int nrings, int batch, in
   using R2 = typename C2<Real>::t;
   const dim3 grid(nrings, batch);
   switch (rows_reg_logm(p, maxM)) {
+    case 8: return launch_fft_kernel<Real>(inv_rows_kernel<Real, 8, kRegBufs>, grid, 16, reg_smem<Real, 8>(0), p, s, reg_carveout<Real, 8>(0));
+    case 9: return launch_fft_kernel<Real>(inv_rows_kernel<Real, 9, kRegBufs>, grid, 32, reg_smem<Real, 9>(0), p, s, reg_carveout<Real, 9>(0));
     case 10: return launch_fft_kernel<Real>(inv_rows_kernel<Real, 10, kRegBufs>, grid, 64, reg_smem<Real, 10>(0), p, s, reg_carveout<Real, 10>(0));
     case 11: return launch_fft_kernel<Real>(inv_rows_kernel<Real, 11, kRegBufs>, grid, 128, reg_smem<Real, 11>(0), p, s, reg_carveout<Real, 11>(0));
     case 12: return launch_fft_kernel<Real>(inv_rows_kernel<Real, 12, kRegBufs>, grid, 256, reg_smem<Real, 12>(0), p, s, reg_carveout<Real, 12>(0));
@@ -897,6 +902,8 @@ cudaError_t launch_fwd_rows(const RowsParams<Real>& p, int nrings, int batch, in
   using R2 = typename C2<Real>::t;
   const dim3 grid(nrings, batch);
   switch (rows_reg_logm(p, maxM)) {
+    case 8: return launch_fft_kernel<Real>(fwd_rows_kernel<Real, 8, kRegBufs>, grid, 16, reg_smem<Real, 8>(0), p, s, reg_carveout<Real, 8>(0));
+    case 9: return launch_fft_kernel<Real>(fwd_rows_kernel<Real, 9, kRegBufs>, grid, 32, reg_smem<Real, 9>(0), p, s, reg_carveout<Real, 9>(0));
     case 10: return launch_fft_kernel<Real>(fwd_rows_kernel<Real, 10, kRegBufs>, grid, 64, reg_smem<Real, 10>(0), p, s, reg_carveout<Real, 10>(0));
     case 11: return launch_fft_kernel<Real>(fwd_rows_kernel<Real, 11, kRegBufs>, grid, 128, reg_smem<Real, 11>(0), p, s, reg_carveout<Real, 11>(0));
     case 12: return launch_fft_kernel<Real>(fwd_rows_kernel<Real, 12, kRegBufs>, grid, 256, reg_smem<Real, 12>(0), p, s, reg_carveout<Real, 12>(0));
@@ -919,6 +926,8 @@ cudaError_t launch_mw_cols(const ColsParams<Real>& p, int ncm, int batch, int M1
     // columns m, m+1 per CTA: L CTAs per map cover m = -(L-1) .. L-1
     const dim3 gp(p.L, batch);
     switch (lg) {
+      case 8: return launch_fft_kernel<Real>(mw_cols_pair_kernel<Real, 8, kRegBufs>, gp, 16, reg_smem<Real, 8>(extra), p, s, reg_carveout<Real, 8>(extra));
+      case 9: return launch_fft_kernel<Real>(mw_cols_pair_kernel<Real, 9, kRegBufs>, gp, 32, reg_smem<Real, 9>(extra), p, s, reg_carveout<Real, 9>(extra));
       case 10: return launch_fft_kernel<Real>(mw_cols_pair_kernel<Real, 10, kRegBufs>, gp, 64, reg_smem<Real, 10>(extra), p, s, reg_carveout<Real, 10>(extra));
       case 11: return launch_fft_kernel<Real>(mw_cols_pair_kernel<Real, 11, kRegBufs>, gp, 128, reg_smem<Real, 11>(extra), p, s, reg_carveout<Real, 11>(extra));
       case 12: return launch_fft_kernel<Real>(mw_cols_pair_kernel<Real, 12, kRegBufs>, gp, 256, reg_smem<Real, 12>(extra), p, s, reg_carveout<Real, 12>(extra));
@@ -927,6 +936,8 @@ cudaError_t launch_mw_cols(const ColsParams<Real>& p, int ncm, int batch, int M1
     }
   }
   switch (lg) {
+    case 8: return launch_fft_kernel<Real>(mw_cols_kernel<Real, 8, kRegBufs>, grid, 16, reg_smem<Real, 8>(extra), p, s, reg_carveout<Real, 8>(extra));
+    case 9: return launch_fft_kernel<Real>(mw_cols_kernel<Real, 9, kRegBufs>, grid, 32, reg_smem<Real, 9>(extra), p, s, reg_carveout<Real, 9>(extra));
     case 10: return launch_fft_kernel<Real>(mw_cols_kernel<Real, 10, kRegBufs>, grid, 64, reg_smem<Real, 10>(extra), p, s, reg_carveout<Real, 10>(extra));
     case 11: return launch_fft_kernel<Real>(mw_cols_kernel<Real, 11, kRegBufs>, grid, 128, reg_smem<Real, 11>(extra), p, s, reg_carveout<Real, 11>(extra));
     case 12: return launch_fft_kernel<Real>(mw_cols_kernel<Real, 12, kRegBufs>, grid, 256, reg_smem<Real, 12>(extra), p, s, reg_carveout<Real, 12>(extra));
