@@ -142,13 +142,17 @@ __global__ void pack_kernel_a(const float* __restrict__ K, int nth, int L, int M
 
 
 // data (map b, summation index t, column mi; complex float) -> Bp[mi][bg][tc][hi/lo][block],
-// row n = 2 (b - 64 bg) + (0: real, 1: imaginary part), through shared memory: a CTA takes 8 columns mi, one t chunk (64) and 8
-// maps (16 rows n), reads the spectra with 64-byte coalesced segments (the 8 columns of a
-// (b, t) pair), and writes every (column, core row group) as 1 KB of contiguous 16-byte
-// stores (8 consecutive k of one row per store, hi and lo).
-constexpr int kPackMaps = 8;
-constexpr int kPackCols = 8;
+// row n = 2 (b - 64 bg) + (0: real, 1: imaginary part), through shared memory: a CTA takes
+// 16 columns mi, one t chunk (64) and 4 maps (8 rows n, one core row group), reads the
+// spectra in 128-byte segments (the 16 columns of a (b, t) pair), and writes every column
+// as 1 KB of contiguous 16-byte stores (8 consecutive k of one row per store, hi and lo).
+constexpr int kPackMaps = 4;
+constexpr int kPackCols = 16;
 constexpr int kPackTP = kTileK + 2;  // padded t row (float2)
+// float2 per column slice: padded so that 16 consecutive columns fall 2 float2 (4 banks)
+// apart modulo 16 (32 banks) while staying 16-byte aligned for the float4 reads
+constexpr int kPackSC = kPackMaps * kPackTP + 10;
+static_assert(kPackSC % 16 == 2, "column slices 4 banks apart");
 
 __global__ void __launch_bounds__(256) pack_kernel_b2(const float2* __restrict__ X, int B,
                                                       int kdim, int M, long in_map, int in_row,
@@ -156,7 +160,7 @@ __global__ void __launch_bounds__(256) pack_kernel_b2(const float2* __restrict__
                                                       __nv_bfloat16* __restrict__ out) {
   // cplx: chunks tc >= ntc / 2 repeat the summation indices of chunk tc - ntc / 2 with the
   // rows (re, im) replaced by (-im, re), so that [Re K | Im K] x this gives the complex product
-  __shared__ __align__(16) float2 S[kPackCols][kPackMaps][kPackTP];
+  __shared__ __align__(16) float2 S[kPackCols * kPackSC];
   const int tid = threadIdx.x;
   const int mi0 = blockIdx.x * kPackCols;
   const int tc = blockIdx.y;
@@ -166,21 +170,23 @@ __global__ void __launch_bounds__(256) pack_kernel_b2(const float2* __restrict__
   const int bg = blockIdx.z / (64 / kPackMaps), sub = blockIdx.z % (64 / kPackMaps);
   const int bl0 = bg * 64 + sub * kPackMaps;  // first map of the CTA
   for (int e = tid; e < kPackCols * kPackMaps * kTileK; e += 256) {
-    const int c = e & 7, tl = (e >> 3) % kTileK, bl = e / (8 * kTileK);
+    const int c = e % kPackCols, tl = (e / kPackCols) % kTileK, bl = e / (kPackCols * kTileK);
     const int b = bl0 + bl, t = tq * kTileK + tl, mi = mi0 + c;
     float2 v = make_float2(0.f, 0.f);
     if (b < B && t < kdim && mi < M) v = X[(size_t)b * in_map + (size_t)t * in_row + in_col0 + mi];
-    S[c][bl][tl] = v;
+    S[c * kPackSC + bl * kPackTP + tl] = v;
   }
   __syncthreads();
-  // unit = 8 consecutive k of one row n of one column: id -> (c, row group, u), u fastest
-  for (int id = tid; id < kPackCols * 2 * 64; id += 256) {
-    const int u = id & 63, rgp = (id >> 6) & 1, c = id >> 7;
+  // unit = 8 consecutive k of one row n of one column: id -> (c, u), u = 8 kg + row fastest
+  constexpr int kU = 8 * (kTileK / 8);
+  for (int id = tid; id < kPackCols * kU; id += 256) {
+    const int u = id % kU, c = id / kU;
     const int mi = mi0 + c;
     if (mi >= M) continue;
-    const int nl = rgp * 8 + (u & 7);  // row within the CTA's 16 rows
+    const int nl = u & 7;  // row within the CTA's 8 rows
     const int kg = u >> 3;
-    const float4* src = reinterpret_cast<const float4*>(&S[c][nl >> 1][kg * 8]);
+    const float4* src =
+        reinterpret_cast<const float4*>(&S[c * kPackSC + (nl >> 1) * kPackTP + kg * 8]);
     float x[8];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -199,7 +205,7 @@ __global__ void __launch_bounds__(256) pack_kernel_b2(const float2* __restrict__
       hi[j] = __float2bfloat16_rn(x[j]);
       lo[j] = __float2bfloat16_rn(x[j] - __bfloat162float(hi[j]));
     }
-    const int n = sub * 16 + nl;
+    const int n = sub * 8 + nl;
     __nv_bfloat16* blk = out + (((size_t)mi * nbg + bg) * ntc + tc) * 2 * kBlk;
     const int off = core_off(n, kg * 8) / 2;
     *reinterpret_cast<uint4*>(blk + off) = *reinterpret_cast<const uint4*>(hi);
