@@ -505,7 +505,7 @@ def run_batched_uneven(torch, nmaps=256, steps=3, warmup=1, seed=4242):
             "tiles": {"forward_half": sum(g.tuning[0] for g in b.groups),
                       "inverse_one_ring": sum(g.tuning[1] & 1 for g in b.groups),
                       "inverse_segments": {str(n): sum(g.tuning[2] == n for g in b.groups)
-                                           for n in (1, 2, 4)}}}
+                                           for n in (1, 2, 4, 8)}}}
 
 
 def uneven_specs(nmaps=256, seed=4242):

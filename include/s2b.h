@@ -179,8 +179,8 @@ int s2b_plan_status(s2b_plan* plan, int* status);
  * sub-plans): key 0 = forward tile (value 0: 16 rings per warp in float / 8 in double;
  * 1: half of that, twice the CTAs), key 1 = inverse tile (value bit 0: one ring per
  * lane instead of two in float; bit 1: start values read from global memory instead of
- * staged in shared memory), key 2 = inverse segments along m (value 1, 2 or 4: each
- * CTA's m-range split into that many independently restarted parts; default 4), key 3 =
+ * staged in shared memory), key 2 = inverse segments along m (value 1, 2, 4 or 8: each
+ * CTA's m-range split into that many independently restarted parts; default 8), key 3 =
  * forward segments along m (same values; used by the equator-symmetric spin-0 forward).
  * Results agree to rounding; only the speed differs, which
  * depends on band-limit, batch and sampling. Used by the autotuner of the batched

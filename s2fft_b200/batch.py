@@ -196,8 +196,8 @@ class BatchedSHT:
     # -- autotuner --------------------------------------------------------------------
     # s2b_plan_set_tuning keys: 0 forward tile, 1 inverse tile, 2 inverse segments along m,
     # 3 forward segments along m (equator-symmetric forward)
-    _INV = [(t, n) for t in (2, 3) for n in (2, 4)]  # (inverse tile, segments)
-    _FWD = [(v, n) for v in (0, 1) for n in (2, 4)]  # (forward tile, segments)
+    _INV = [(t, n) for t in (2, 3) for n in (4, 8)]  # (inverse tile, segments)
+    _FWD = [(v, n) for v in (0, 1) for n in (4, 8)]  # (forward tile, segments)
     _SCHED = [(1, 0), (2, 0), (2, 2), (3, 2)]  # (waves, CTAs per SM) of the persistent batch
 
     def _timed(self, fn, reps):
@@ -299,7 +299,7 @@ class BatchedSHT:
         """Pick launch shapes (and, with persistent=None, the schedule) by timing them."""
         with torch.no_grad():
             for g in self.groups:
-                self._set(g, (0, 3, 4, 4))
+                self._set(g, (0, 3, 8, 8))
             self._tune_streams(reps)  # per-group shapes: used by both schedules
             t_str = None
             if self.requested is not True:

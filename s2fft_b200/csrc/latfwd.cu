@@ -669,7 +669,7 @@ cudaError_t launch_fwd2_batch(bool fp64, bool dual, const Fwd2Params* ps, int np
   if (nplans <= 0) return cudaSuccess;
   if (nplans > kBatchPlans) return cudaErrorInvalidValue;
   for (int i = 0; i < nplans; ++i) {
-    if (ps[i].Mst1 && !(ps[i].nseg == 1 || ps[i].nseg == 2 || ps[i].nseg == 4))
+    if (ps[i].Mst1 && !(ps[i].nseg == 1 || ps[i].nseg == 2 || ps[i].nseg == 4 || ps[i].nseg == 8))
       return cudaErrorInvalidValue;
     if (ps[i].sym != ps[0].sym || ps[i].cross != ps[0].cross || ps[i].tile != ps[0].tile)
       return cudaErrorInvalidValue;
@@ -681,7 +681,7 @@ cudaError_t launch_fwd2_batch(bool fp64, bool dual, const Fwd2Params* ps, int np
 
 cudaError_t launch_fwd2(bool fp64, bool dual, const Fwd2Params& p, cudaStream_t s) {
   if (p.nrings <= 0) return cudaSuccess;
-  if (p.Mst1 && !(p.nseg == 1 || p.nseg == 2 || p.nseg == 4)) return cudaErrorInvalidValue;
+  if (p.Mst1 && !(p.nseg == 1 || p.nseg == 2 || p.nseg == 4 || p.nseg == 8)) return cudaErrorInvalidValue;
   if (p.sym && p.cross) return launch_fwd2_prec<2>(fp64, dual, p, s);
   return p.sym ? launch_fwd2_prec<1>(fp64, dual, p, s) : launch_fwd2_prec<0>(fp64, dual, p, s);
 }

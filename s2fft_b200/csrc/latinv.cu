@@ -530,7 +530,7 @@ cudaError_t launch_inv2_batch(bool fp64, bool dual, const Inv2Params* ps, int np
   if (nplans <= 0) return cudaSuccess;
   if (nplans > kBatchPlans) return cudaErrorInvalidValue;
   for (int i = 0; i < nplans; ++i) {
-    if (ps[i].Mst1 && !(ps[i].nseg == 1 || ps[i].nseg == 2 || ps[i].nseg == 4))
+    if (ps[i].Mst1 && !(ps[i].nseg == 1 || ps[i].nseg == 2 || ps[i].nseg == 4 || ps[i].nseg == 8))
       return cudaErrorInvalidValue;
     if (ps[i].sym != ps[0].sym || ps[i].tile != ps[0].tile) return cudaErrorInvalidValue;
   }
@@ -540,7 +540,7 @@ cudaError_t launch_inv2_batch(bool fp64, bool dual, const Inv2Params* ps, int np
 
 cudaError_t launch_inv2(bool fp64, bool dual, const Inv2Params& p, cudaStream_t s) {
   if (p.nrings <= 0) return cudaSuccess;
-  if (p.Mst1 && !(p.nseg == 1 || p.nseg == 2 || p.nseg == 4)) return cudaErrorInvalidValue;
+  if (p.Mst1 && !(p.nseg == 1 || p.nseg == 2 || p.nseg == 4 || p.nseg == 8)) return cudaErrorInvalidValue;
   return p.sym ? launch_inv2_prec<true>(fp64, dual, p, s)
                : launch_inv2_prec<false>(fp64, dual, p, s);
 }

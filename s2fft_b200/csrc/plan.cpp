@@ -440,7 +440,7 @@ struct s2b_plan {
   void* inv_Vst = nullptr;
   int* inv_Mst1 = nullptr;  // restart tables of the inverse kernel's m-split
   void* inv_Vst1 = nullptr;
-  int inv_nseg = 1;         // segments along m of the inverse kernel (1, 2, 4)
+  int inv_nseg = 1;         // segments along m of the inverse kernel (1, 2, 4, 8)
   // equator-symmetric inverse (spin 0, rings symmetric about the equator): ring pairs
   int inv_sym = 0, inv_npair = 0;
   int* adj_col = nullptr;
@@ -488,7 +488,7 @@ struct s2b_plan {
   void* sym_Vst = nullptr;
   int* sym_Mst1 = nullptr;
   void* sym_Vst1 = nullptr;
-  int fwd_nseg = 1;  // segments along m of the forward kernel (1, 2, 4)
+  int fwd_nseg = 1;  // segments along m of the forward kernel (1, 2, 4, 8)
 };
 
 template <typename T>
@@ -890,11 +890,11 @@ static int build_plan(s2b_plan* p) {
     fp.Mst1 = p->sym_Mst1;
     fp.Vst1 = p->sym_Vst1;
     S2B_CK(launch_fwd_start(p->fp64, fp, 0));
-    // launch shape measured at L = 256 ... 2048 (MW, MWSS, GL, DH, float and double): four
-    // segments along m; spin-0 float takes 8 ring pairs per warp up to L = 512, 16 above
-    // (spin != 0: 16 throughout)
+    // launch shape measured at L = 256 ... 1024 (MW, HEALPix; float): eight segments along
+    // m (against four: 8-12 % faster up to L = 512, 2 % at 1024); spin-0 float takes 8 ring
+    // pairs per warp up to L = 256, 16 above (spin != 0: 16 throughout)
     p->fwd_nseg = kInvSegMax;
-    p->tile_fwd = (!p->fp64 && L <= 512 && !p->fwd_cross) ? 1 : 0;
+    p->tile_fwd = (!p->fp64 && L <= 256 && !p->fwd_cross) ? 1 : 0;
   }
   // ---- start tables of the inverse rings (inverse kernel and adjoint of the inverse)
   if (p->inv_nrings > 0) {
@@ -908,11 +908,12 @@ static int build_plan(s2b_plan* p) {
     S2B_CK(dev_malloc(&p->inv_Vst1, (kInvSegMax - 1) *
                                         fwd_start_bytes(p->fp64, L, p->nhalf, p->inv_nrings)));
     p->allocs.push_back(p->inv_Vst1);
-    // launch shape of the inverse kernel, measured at L = 256 ... 2048 (MW, float and
-    // double): four segments along m, start values read from global memory (shared memory
-    // for 3 CTAs per SM), two rings per lane in float from L = 1024 and one below
+    // launch shape of the inverse kernel, measured at L = 256 ... 1024 (MW, HEALPix; float):
+    // eight segments along m (against four: 10-11 % faster at L = 256 and 512 with the
+    // tiles below, 1 % at 1024), start values read from global memory (shared memory for 3
+    // CTAs per SM), two rings per lane in float from L = 512 and one below
     p->inv_nseg = kInvSegMax;
-    p->tile_inv = (!p->fp64 && L >= 1024) ? 2 : 3;
+    p->tile_inv = (!p->fp64 && L >= 512) ? 2 : 3;
     // symmetric inverse: one ring pair per lane (two would double the partial sums in
     // shared memory and drop to 2 CTAs per SM; measured slower at L = 256 ... 2048)
     if (p->inv_sym) p->tile_inv = 3;
@@ -2787,11 +2788,11 @@ int s2b_plan_status(s2b_plan* p, int* status) {
 int s2b_plan_set_tuning(s2b_plan* p, int key, int value) {
   if (!p) return fail(S2B_ERR_INVALID, "plan must be non-NULL");
   const bool tile = (key == 0 && (value == 0 || value == 1)) || (key == 1 && value >= 0 && value <= 3);
-  const bool seg = (key == 2 || key == 3) && (value == 1 || value == 2 || value == 4);
+  const bool seg = (key == 2 || key == 3) && (value == 1 || value == 2 || value == 4 || value == 8);
   if (!tile && !seg)
     return fail(S2B_ERR_INVALID,
                 "key 0 (forward tile) takes 0 or 1, key 1 (inverse tile) 0 to 3, keys 2 and 3 "
-                "(inverse / forward segments along m) 1, 2 or 4");
+                "(inverse / forward segments along m) 1, 2, 4 or 8");
   if (key == 0)
     p->tile_fwd = value;
   else if (key == 1)

@@ -19,7 +19,7 @@ __host__ __device__ inline int fwd_nblocks(int L) { return 2 * ((L + 2 * kFwdBlo
 // of 8, so every segment starts on a group boundary; a run with S segments (S dividing
 // kInvSegMax) uses every (kInvSegMax / S)-th boundary. Segment k >= 1 restarts the states
 // begun above its top boundary b from exact values at m = b - 1.
-constexpr int kInvSegMax = 4;
+constexpr int kInvSegMax = 8;
 __host__ __device__ inline int inv_mbound(int L, int NB, int q, int k) {
   int top = (NB - 1 - q) * 32 + 31;
   if (top > L - 1) top = L - 1;
@@ -76,7 +76,7 @@ struct Fwd2Params {
   int cross;
   int tab_stride;           // ring stride of Mst / Vst (0: nrings)
   // split along m as in the inverse kernel (inv_mbound): restart tables
-  // [kInvSegMax - 1][table] (nullptr: one segment) and the number of segments (1, 2, 4)
+  // [kInvSegMax - 1][table] (nullptr: one segment) and the number of segments (1, 2, 4, 8)
   const int* Mst1;
   const void* Vst1;
   int nseg;
@@ -89,7 +89,7 @@ struct Inv2Params {
   const void* Vst;
   const int* Mst1;          // restart tables of the m-split (nullptr: one segment)
   const void* Vst1;
-  int nseg;                 // segments along m: 1, 2 or 4 (with Mst1)
+  int nseg;                 // segments along m: 1, 2, 4 or 8 (with Mst1)
   // equator-symmetric mode (spin 0): the nrings rings are the northern members of ring
   // pairs (ring q and tab_stride - 1 - q) plus the equator; a lane sums the degrees with
   // l + m even (E) and odd (O) apart and adds E + O to ring q and E - O to its mirror
