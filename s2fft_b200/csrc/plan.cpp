@@ -548,38 +548,38 @@ static RingInfo ring_info(double th) {
 // MWSS(2L) rings, in the units of the device's inverse-DFT output (before the phi factor
 // and the weights). For real maps upstream takes the real part after the upsampling, which
 // turns c into Re(c) (the impulse is real and the direct chain's image of it is real).
+// Unnormalised inverse DFT y_k = sum_j x_j exp(+2 pi i jk / n), any length, O(n log n).
+static std::vector<cd> idft_host(std::vector<cd> x) {
+  for (cd& v : x) v = std::conj(v);
+  x = dft_host(std::move(x));
+  for (cd& v : x) v = std::conj(v);
+  return x;
+}
+
+// The chain's sums over theta bins, each a DFT over bins p at index p mod n (O(L log L)).
 static std::vector<cd> mw_pole_correction(int L) {
   const int n1 = 2 * L - 1, n2 = 2 * L, n4 = 4 * L;
-  std::vector<cd> w2(n2), w4(n4);  // roots of unity exp(2 pi i j / n)
-  for (int j = 0; j < n2; ++j) w2[j] = std::polar(1.0, 2.0 * kPi * j / n2);
-  for (int j = 0; j < n4; ++j) w4[j] = std::polar(1.0, 2.0 * kPi * j / n4);
-  auto r2 = [&](long e) { return w2[((e % n2) + n2) % n2]; };
-  auto r4 = [&](long e) { return w4[((e % n4) + n4) % n4]; };
   // theta bins p = -(L-1)..L-1 of the impulse at t = L-1 after the half-sample phase:
   // exp(-2 pi i p (L-1) / n1) exp(-i pi p / n1) / n1 = (-1)^p / n1
   auto G = [&](int p) { return ((p & 1) ? -1.0 : 1.0) / (double)n1; };
+  auto bins = [&](int n) {
+    std::vector<cd> a(n, cd(0.0, 0.0));
+    for (int p = -(L - 1); p <= L - 1; ++p) a[((p % n) + n) % n] = G(p);
+    return a;
+  };
   // upstream: unnormalised inverse DFT over 2L (MWSS rings j = 0..L), the circle rebuilt
   // with the odd-column sign -1, DFT over 2L divided by 2L, zero-pad (bin -L kept at -L),
   // unnormalised inverse DFT over 4L
-  std::vector<cd> g(L + 1);
-  for (int j = 0; j <= L; ++j) {
-    cd v(0.0, 0.0);
-    for (int p = -(L - 1); p <= L - 1; ++p) v += G(p) * r2((long)p * j);
-    g[j] = v;
-  }
-  std::vector<cd> H(n2);  // bin q = -L..L-1 at index q + L
-  for (int q = -L; q < L; ++q) {
-    cd v(0.0, 0.0);
-    for (int j = 0; j < n2; ++j) v += (j <= L ? g[j] : -g[n2 - j]) * r2(-(long)q * j);
-    H[q + L] = v / (double)n2;
-  }
+  const std::vector<cd> g = idft_host(bins(n2));  // g[j], j = 0..L used
+  std::vector<cd> ext(n2);
+  for (int j = 0; j < n2; ++j) ext[j] = j <= L ? g[j] : -g[n2 - j];
+  const std::vector<cd> E = dft_host(ext);  // E[q mod n2] = 2L H[q]
+  std::vector<cd> B(n4, cd(0.0, 0.0));
+  for (int q = -L; q < L; ++q) B[((q % n4) + n4) % n4] = E[((q % n2) + n2) % n2] / (double)n2;
+  const std::vector<cd> u = idft_host(B);
+  const std::vector<cd> direct = idft_host(bins(n4));
   std::vector<cd> c(2 * L + 1);
-  for (int k = 0; k <= 2 * L; ++k) {
-    cd u(0.0, 0.0), direct(0.0, 0.0);
-    for (int q = -L; q < L; ++q) u += H[q + L] * r4((long)q * k);
-    for (int p = -(L - 1); p <= L - 1; ++p) direct += G(p) * r4((long)p * k);
-    c[k] = u - direct;
-  }
+  for (int k = 0; k <= 2 * L; ++k) c[k] = u[k] - direct[k];
   return c;
 }
 
@@ -592,28 +592,29 @@ static std::vector<cd> mw_pole_correction(int L) {
 // between two columns and adds them through this table.
 static std::vector<cd> col_impulse(int L, bool mw, const std::vector<cd>& pole, bool nyq_split) {
   const int n4 = 4 * L, nout = 2 * L + 1;
-  std::vector<cd> w4(n4);
-  for (int j = 0; j < n4; ++j) w4[j] = std::polar(1.0, 2.0 * kPi * j / n4);
-  auto r4 = [&](long e) { return w4[((e % n4) + n4) % n4]; };
+  // sum over theta bins p of b(p) exp(2 pi i p k / 4L), k = 0..2L: an inverse DFT over 4L
+  auto chain = [&](int plo, auto b) {
+    std::vector<cd> a(n4, cd(0.0, 0.0));
+    for (int p = plo; p <= L - 1; ++p) a[((p % n4) + n4) % n4] = b(p);
+    return idft_host(a);
+  };
   if (mw) {
     // bins after the half-sample phase and 1/n1: (-1)^p / n1 (see mw_pole_correction)
     const double n1 = 2.0 * L - 1.0;
+    const std::vector<cd> d = chain(-(L - 1), [&](int p) { return cd(((p & 1) ? -1.0 : 1.0) / n1, 0.0); });
     std::vector<cd> imp(nout);
-    for (int k = 0; k < nout; ++k) {
-      cd v(0.0, 0.0);
-      for (int p = -(L - 1); p <= L - 1; ++p) v += ((p & 1) ? -1.0 : 1.0) / n1 * r4((long)p * k);
-      imp[k] = v + pole[k];
-    }
+    for (int k = 0; k < nout; ++k) imp[k] = d[k] + pole[k];
     return imp;
   }
   // MWSS: bins 1 / n1 (t = 0) and (-1)^p / n1 (t = L), p = -L..L-1
   const double n1 = 2.0 * L;
   std::vector<cd> imp(2 * nout);
   for (int which = 0; which < 2; ++which) {
+    const std::vector<cd> d = chain(-L, [&](int p) {
+      return cd(((which && (p & 1)) ? -1.0 : 1.0) / n1, 0.0);
+    });
     for (int k = 0; k < nout; ++k) {
-      cd v(0.0, 0.0);
-      for (int p = -L; p <= L - 1; ++p)
-        v += ((which && (p & 1)) ? -1.0 : 1.0) / n1 * r4((long)p * k);
+      cd v = d[k];
       if (nyq_split && (k & 1)) {  // i N sin(pi k / 2), N = bin -L
         const double N = ((which && (L & 1)) ? -1.0 : 1.0) / n1;
         v += cd(0.0, ((k & 2) ? -1.0 : 1.0) * N);
@@ -1285,6 +1286,35 @@ static int inv_stage_post(s2b_plan* p, const Inv2Params& lp, void* f, char* ws, 
   return S2B_OK;
 }
 
+// Fork of the plan's auxiliary stream from s (atomic per plan) and its join back to s.
+static int aux_fork(s2b_plan* p, cudaStream_t s) {
+  std::lock_guard<std::mutex> lk(p->fork_mu);
+  S2B_CK(cudaEventRecord(p->aux_fork, s));
+  S2B_CK(cudaStreamWaitEvent(p->aux, p->aux_fork, 0));
+  return S2B_OK;
+}
+
+static int aux_join(s2b_plan* p, cudaStream_t s) {
+  S2B_CK(cudaEventRecord(p->aux_join, p->aux));
+  S2B_CK(cudaStreamWaitEvent(s, p->aux_join, 0));
+  return S2B_OK;
+}
+
+// The latitudinal kernel of a single-plan call, between the plan's timing events.
+static int launch_lat_inv(s2b_plan* p, const Inv2Params& lp, cudaStream_t s) {
+  if (p->ev_begin[0]) S2B_CK(cudaEventRecord(p->ev_begin[0], s));
+  S2B_CK(launch_inv2(p->fp64, p->dual, lp, s));
+  if (p->ev_end[0]) S2B_CK(cudaEventRecord(p->ev_end[0], s));
+  return S2B_OK;
+}
+
+static int launch_lat_fwd(s2b_plan* p, const Fwd2Params& lp, cudaStream_t s) {
+  if (p->ev_begin[1]) S2B_CK(cudaEventRecord(p->ev_begin[1], s));
+  S2B_CK(launch_fwd2(p->fp64, p->dual, lp, s));
+  if (p->ev_end[1]) S2B_CK(cudaEventRecord(p->ev_end[1], s));
+  return S2B_OK;
+}
+
 template <typename Real>
 static int run_inverse(s2b_plan* p, const void* flm, void* f, char* ws, cudaStream_t s,
                        const double* ring_w = nullptr) {
@@ -1296,19 +1326,19 @@ static int run_inverse(s2b_plan* p, const void* flm, void* f, char* ws, cudaStre
     // the low orders (columns m < |s|, disjoint from the kernel's) beside the kernel: a few
     // CTAs of long sequential loops that would otherwise run alone after it
     if (lp.mlo > 0 && p->aux) {
-      {
-        std::lock_guard<std::mutex> lk(p->fork_mu);
-        S2B_CK(cudaEventRecord(p->aux_fork, s));
-        S2B_CK(cudaStreamWaitEvent(p->aux, p->aux_fork, 0));
+      if ((rc = aux_fork(p, s))) return rc;
+      if ((rc = run_lowm_synth(p, lp, p->inv_rings, p->aux))) {
+        aux_join(p, s);
+        return rc;
       }
-      if ((rc = run_lowm_synth(p, lp, p->inv_rings, p->aux))) return rc;
-      S2B_CK(cudaEventRecord(p->aux_join, p->aux));
       lowm_done = true;
     }
-    if (p->ev_begin[0]) S2B_CK(cudaEventRecord(p->ev_begin[0], s));
-    S2B_CK(launch_inv2(p->fp64, p->dual, lp, s));
-    if (p->ev_end[0]) S2B_CK(cudaEventRecord(p->ev_end[0], s));
-    if (lowm_done) S2B_CK(cudaStreamWaitEvent(s, p->aux_join, 0));
+    rc = launch_lat_inv(p, lp, s);
+    if (lowm_done) {
+      const int jr = aux_join(p, s);  // after a failed launch too: nothing outlives the call
+      if (!rc) rc = jr;
+    }
+    if (rc) return rc;
   }
   return inv_stage_post<Real>(p, lp, f, ws, s, ring_w, lowm_done);
 }
@@ -1703,18 +1733,18 @@ static int run_forward_once(s2b_plan* p, const void* f, void* flm, char* ws, cud
   // the low orders (rows m < |s| of the accumulator, disjoint from the kernel's) beside it
   const bool lowm_aux = lp_all.mlo > 0 && lp_all.nrings > 0 && p->aux;
   if (lowm_aux) {
-    {
-      std::lock_guard<std::mutex> lk(p->fork_mu);
-      S2B_CK(cudaEventRecord(p->aux_fork, s));
-      S2B_CK(cudaStreamWaitEvent(p->aux, p->aux_fork, 0));
+    if ((rc = aux_fork(p, s))) return rc;
+    if ((rc = run_lowm_project(p, lp_all, p->fwd_rings, p->aux))) {
+      aux_join(p, s);
+      return rc;
     }
-    if ((rc = run_lowm_project(p, lp_all, p->fwd_rings, p->aux))) return rc;
-    S2B_CK(cudaEventRecord(p->aux_join, p->aux));
   }
-  if (p->ev_begin[1]) S2B_CK(cudaEventRecord(p->ev_begin[1], s));
-  S2B_CK(launch_fwd2(p->fp64, p->dual, lp, s));
-  if (p->ev_end[1]) S2B_CK(cudaEventRecord(p->ev_end[1], s));
-  if (lowm_aux) S2B_CK(cudaStreamWaitEvent(s, p->aux_join, 0));
+  rc = launch_lat_fwd(p, lp, s);
+  if (lowm_aux) {
+    const int jr = aux_join(p, s);  // after a failed launch too: nothing outlives the call
+    if (!rc) rc = jr;
+  }
+  if (rc) return rc;
   return fwd_stage_post<Real>(p, lp_all, flm, ws, s, lowm_aux);
 }
 
@@ -2167,9 +2197,10 @@ static int batch_launch_lat(s2b_batch* b, const std::vector<int>& idx, const std
 // (the ring FFTs are memory-bound) can overlap the latitudinal launches (FP32-bound) of the
 // next. pre(k, lane, &lp[k]) and post(k, lane, lp[k]) run the stages of entry k.
 template <typename P, typename Pre, typename Key, typename Post>
-static int batch_staged(s2b_batch* b, const std::vector<int>& idx, cudaStream_t s, Pre pre,
-                        Key key, Post post,
-                        cudaError_t (*launch)(bool, bool, const P*, int, int*, int, cudaStream_t)) {
+static int batch_staged_body(s2b_batch* b, const std::vector<int>& idx, cudaStream_t s, Pre pre,
+                             Key key, Post post,
+                             cudaError_t (*launch)(bool, bool, const P*, int, int*, int,
+                                                   cudaStream_t)) {
   const int n = (int)idx.size();
   const int nw = std::max(1, std::min(std::min(b->waves, n), (int)s2b_batch::kMaxWaves));
   std::vector<P> lp(n);
@@ -2192,6 +2223,21 @@ static int batch_staged(s2b_batch* b, const std::vector<int>& idx, cudaStream_t 
   for (int k : wave_members(n, nw, nw - 1))
     if ((rc = post(k, batch_lane(b, k, s), lp[k]))) return rc;
   return batch_join(b, s);
+}
+
+// The staged execution; after a failure the batch's streams are still joined back to s, so
+// that no work queued on them outlives the call and a capture of s stays complete.
+template <typename P, typename Pre, typename Key, typename Post>
+static int batch_staged(s2b_batch* b, const std::vector<int>& idx, cudaStream_t s, Pre pre,
+                        Key key, Post post,
+                        cudaError_t (*launch)(bool, bool, const P*, int, int*, int, cudaStream_t)) {
+  const int rc = batch_staged_body<P>(b, idx, s, pre, key, post, launch);
+  if (rc && b->nstreams > 1) {
+    const std::string msg = g_last_error;
+    batch_join(b, s);
+    g_last_error = msg;  // report the first failure
+  }
+  return rc;
 }
 
 // The entries idx[0..n) of the batch: inputs in[k], outputs out[k], workspaces ws[k].
