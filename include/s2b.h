@@ -276,12 +276,14 @@ int s2b_batch_set_option(s2b_batch* batch, int key, int value);
  *   flm'[l, m] = exp(-i m alpha) sum_n d^l_{m,n}(beta) exp(-i n gamma) flm[l, n],
  * replaces s2fft.utils.rotation.rotate_flms (s2fft/utils/rotation.py:9-64). flm and out
  * are [batch][L][2L-1] complex (double for precision S2B_F64, float for S2B_F32); the
- * arithmetic is double in both. dl == NULL: the Wigner-d planes at beta are generated
- * on the device by Risbo's recursion (upstream s2fft/recursions/risbo.py:4-120);
- * otherwise dl holds them in the layout of upstream's generate_rotate_dls,
- * [L][2L-1][2L-1] float64 with d^l_{m,n} at [l][L-1+m][L-1+n]. The workspace
- * (s2b_rotate_workspace_size(L) bytes, caller-owned) holds two planes and the phase
- * tables. Stream-ordered; no allocation. */
+ * arithmetic is double in both. dl == NULL: the Wigner-d values at beta are generated
+ * on the device by the three-term recurrence in the degree of every (m, n) (upstream
+ * builds the planes with Risbo's recursion, s2fft/recursions/risbo.py:4-120; the two
+ * agree to rounding), L <= 8192; otherwise dl holds them in the layout of upstream's
+ * generate_rotate_dls, [L][2L-1][2L-1] float64 with d^l_{m,n} at [l][L-1+m][L-1+n].
+ * The workspace (s2b_rotate_workspace_size(L) bytes, caller-owned) holds the
+ * recurrence coefficients, the start values and the phase tables. Results do not
+ * depend on the launch order (fixed-order sums). Stream-ordered; no allocation. */
 size_t s2b_rotate_workspace_size(int L);
 int s2b_rotate_flms(int L, int batch, int precision, double alpha, double beta, double gamma,
                     const void* flm, void* out, const double* dl, void* ws, size_t ws_bytes,
@@ -289,7 +291,7 @@ int s2b_rotate_flms(int L, int batch, int precision, double alpha, double beta, 
 
 /* The planes d^l_{m,n}(beta), 0 <= l < L, in the layout of upstream's
  * generate_rotate_dls (s2fft/utils/rotation.py:75-96): dl[l][L-1+m][L-1+n] float64,
- * zero where |m| > l or |n| > l (the call clears dl first). */
+ * zero where |m| > l or |n| > l; every entry is written. L <= 8192. */
 int s2b_rotate_dls(int L, double beta, double* dl, void* ws, size_t ws_bytes, void* stream);
 
 /* Fourier-Wigner transforms on SO(3) and the spin-subset lifting ops (mw / mwss only).

@@ -6,10 +6,11 @@
 
     flm'[l, m] = exp(-i m alpha) sum_n d^l_{m,n}(beta) exp(-i n gamma) flm[l, n].
 
-Without ``dl_array`` the Wigner-d planes at beta are generated on the device degree by
-degree by Risbo's recursion (upstream s2fft/recursions/risbo.py:4-120) inside one
-cooperative kernel; with it (the layout of ``generate_rotate_dls``, rotation.py:75-96)
-only the contraction runs. The arithmetic is double; complex64 inputs are returned as
+Without ``dl_array`` the Wigner-d values at beta are generated on the device by the
+three-term recurrence in the degree of every (m, n), fused with the contraction (upstream
+builds the planes with Risbo's recursion, s2fft/recursions/risbo.py:4-120; the two agree
+to rounding); with it (the layout of ``generate_rotate_dls``, rotation.py:75-96) only the
+contraction runs. The arithmetic is double; complex64 inputs are returned as
 complex64. A leading batch dimension is accepted (upstream takes one map).
 """
 

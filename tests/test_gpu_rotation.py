@@ -34,7 +34,7 @@ def test_rotation_golden(s2b, fixture, k):
     L = int(fixture[f"r{k}/L"])
     rot = tuple(fixture[f"r{k}/rotation"])
     flm, ref = fixture[f"r{k}/flm"], fixture[f"r{k}/rotated"]
-    # planes by Risbo's recursion on the device
+    # Wigner-d values by the degree recurrence on the device
     r = s2b.rotation.rotate_flms(flm, L, rot)
     assert relerr(r, ref) < 1e-12, relerr(r, ref)
     # float32 in and out (double arithmetic inside)
@@ -58,3 +58,29 @@ def test_rotation_inverse_and_batch(s2b, rng):
     assert relerr(back, flm) < 1e-10, relerr(back, flm)
     single = s2b.rotation.rotate_flms(flm[1], L, rot)
     assert relerr(single, r[1]) < 1e-13
+
+
+@pytest.mark.parametrize("L,beta", [(48, 0.05), (48, np.pi / 2), (37, 3.1), (20, 0.0)])
+def test_rotation_planes_against_risbo(s2b, L, beta):
+    """generate_rotate_dls against the oracle's Risbo planes, including betas whose start
+    values underflow (0.05, 3.1: the scaled path) and an odd band-limit."""
+    dl = s2b.rotation.generate_rotate_dls(L, beta).cpu().numpy()
+    ref = oracle.rotation.generate_rotate_dls(L, beta)
+    assert np.abs(dl - ref).max() < 1e-12, np.abs(dl - ref).max()
+
+
+@pytest.mark.parametrize("L,rot", [(1024, (0.3, 0.05, -1.2)), (600, (2.0, 3.05, 0.4)),
+                                   (2049, (0.5, 1.1, 2.5))])
+def test_rotation_unitary_large(s2b, rng, L, rot):
+    """Rotation keeps the power of every degree, sum_m |flm'[l, m]|^2 = sum_m |flm[l, m]|^2,
+    and rotating back restores flm: at L = 1024 and 600 with betas near 0 and pi (start
+    values below 2^-960, renormalised recurrences) and at L = 2049 (two n per lane)."""
+    import torch
+
+    flm = torch.from_numpy(oracle.signal.generate_flm(rng, L, 0, 0, False)).cuda()
+    r = s2b.rotation.rotate_flms(flm, L, rot)
+    p0 = (flm.abs() ** 2).sum(-1)
+    p1 = (r.abs() ** 2).sum(-1)
+    assert float(((p1 - p0).abs() / p0.clamp_min(1e-300)).max()) < 1e-11
+    back = s2b.rotation.rotate_flms(r, L, (-rot[2], -rot[1], -rot[0]))
+    assert float((back - flm).abs().max() / flm.abs().max()) < 1e-10
