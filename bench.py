@@ -53,6 +53,9 @@ def parse_args():
     ap.add_argument("--healpix-profile", action="store_true",
                     help="HEALPix nside=256 L=512 real float32: one inverse and one forward "
                          "with 3 iterations between cudaProfilerStart/Stop")
+    ap.add_argument("--rotate-profile", action="store_true",
+                    help="rotate_flms at --L (float64, one map): warm-up, five timed calls, "
+                         "then one call between cudaProfilerStart/Stop")
     ap.add_argument("--batch-profile", choices=["persistent", "streams"], default=None,
                     help="the 256-map uneven batch, one eager inverse + forward of the given "
                          "schedule between cudaProfilerStart/Stop (ncu --profile-from-start "
@@ -538,6 +541,36 @@ def profile_batched_uneven(torch, schedule):
     return {"schedule": schedule, "eager_ms": e0.elapsed_time(e1), "groups": len(b.groups)}
 
 
+def profile_rotation(torch, L=1024, rot=(0.7, 1.9, -2.4)):
+    """rotate_flms of one float64 map (Euler angles rot): CUDA-event times of five calls
+    after a warm-up, the largest change of a degree's power and the round-trip error, then
+    one call between cudaProfilerStart/Stop."""
+    from s2fft_b200 import rotation
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    flm = torch.from_numpy(seeded_flm(np.random.default_rng(11), L, 0, False)).to(dev)
+    r = rotation.rotate_flms(flm, L, rot)
+    back = rotation.rotate_flms(r, L, (-rot[2], -rot[1], -rot[0]))
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
+        e0.record()
+        rotation.rotate_flms(flm, L, rot)
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    torch.cuda.profiler.start()
+    rotation.rotate_flms(flm, L, rot)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    p0, p1 = (flm.abs() ** 2).sum(-1), (r.abs() ** 2).sum(-1)
+    return {"workload": f"rotate_flms L={L} f64, one map, rotation {rot}",
+            "ms_min": min(ts), "ms_median": float(np.median(ts)),
+            "power_max_rel_change": float(((p1 - p0).abs() / p0.clamp_min(1e-300)).max()),
+            "roundtrip_max_rel_err": float((back - flm).abs().max() / flm.abs().max())}
+
+
 def profile_healpix(torch, nside=256, L=512):
     """One float32 HEALPix inverse and forward (3 iterations) after a warm-up call, between
     cudaProfilerStart/Stop."""
@@ -743,6 +776,9 @@ def main():
         return
     if args.batch_profile:
         print(json.dumps(profile_batched_uneven(torch, args.batch_profile)))
+        return
+    if args.rotate_profile:
+        print(json.dumps(profile_rotation(torch, args.L)))
         return
     if args.profile_case:
         args.steps, args.warmup = 2, 1
