@@ -240,10 +240,10 @@ __device__ __forceinline__ double reduce_perm(double* x) {
   return r;
 }
 
-// asynchronous global -> shared copies of B bytes (zero-filled when !valid)
+// asynchronous global -> shared copies of B bytes (zero-filled when !valid); d is a
+// shared-space address
 template <int B>
-__device__ __forceinline__ void cp_async(void* dst, const void* src, bool valid) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+__device__ __forceinline__ void cp_async(unsigned d, const void* src, bool valid) {
   if constexpr (B == 16)
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src),
                  "r"(valid ? 16 : 0)
@@ -313,7 +313,7 @@ __device__ __forceinline__ void rotate_stage(const RotParams& p, double4* uvq, i
   for (int e = threadIdx.x; e < 2 * kRotChunk * MT; e += blockDim.x) {
     const int h = e & 1, lc = (e >> 1) / MT, i = (e >> 1) % MT, l = l0 + lc;
     const double4* src = p.UVQ + (size_t)min(l, p.L - 1) * p.L + min(m0 + i, p.L - 1);
-    cp_async<16>(reinterpret_cast<char*>(uvq + lc * MT + i) + 16 * h,
+    cp_async<16>((unsigned)__cvta_generic_to_shared(uvq + lc * MT + i) + 16 * h,
                  reinterpret_cast<const char*>(src) + 16 * h, l < p.L);
   }
 }
@@ -413,27 +413,39 @@ __global__ void __launch_bounds__(kRotThreads, 2) rotate_lrec_kernel(RotParams p
     }
     const R2* const fb =
         contract ? reinterpret_cast<const R2*>(p.flm) + (size_t)b * L * NN + L - 1 : nullptr;
-    // copies of degree ll into ring stage st (zero where nothing has started)
-    auto issue = [&](int ll, int st) {
+    // copies of consecutive degrees ll = m0, m0 + 1, ... into ring stage st (zero where
+    // nothing has started); with one n per lane the source pointers advance by one row
+    // per call, with more they are recomputed (fewer live registers)
+    const unsigned rbase = (unsigned)__cvta_generic_to_shared(ring + tid);
+    const double2* tq = p.T + (size_t)m0 * L + min(an[0], L - 1);
+    const R2* fq = contract ? fb + (size_t)m0 * NN + nv[0] : nullptr;
+    int ll = m0;
+    auto issue = [&](int st) {
 #pragma unroll
       for (int s = 0; s < S; ++s) {
         const bool vt = ll < L && ll >= wmin[s];
+        const unsigned r = rbase + (unsigned)(((st * S + s) * 3) * nt) * 16u;
         const int lt = min(ll, L - 1);
-        double2* r = ring + ((st * S + s) * 3) * nt + tid;
-        cp_async<16>(r, p.T + (size_t)lt * L + min(an[s], L - 1), vt);
+        const double2* ts = S == 1 ? tq : p.T + (size_t)lt * L + min(an[s], L - 1);
+        const R2* fs = S == 1 ? fq : fb + (size_t)lt * NN + nv[s];
+        cp_async<16>(r, ts, vt);
         if constexpr (contract) {
           const bool vf = vt && an[s] <= ll;
-          const R2* row = fb + (size_t)lt * NN;
-          cp_async<sizeof(R2)>(r + nt, row + nv[s], vf);
-          cp_async<sizeof(R2)>(r + 2 * nt, row - nv[s], vf);
+          cp_async<sizeof(R2)>(r + 16u * nt, fs, vf);
+          cp_async<sizeof(R2)>(r + 32u * nt, fs - 2 * nv[s], vf);
         }
       }
+      if (S == 1 && ll + 1 < L) {
+        tq += L;
+        if constexpr (contract) fq += NN;
+      }
+      ++ll;
     };
     rotate_stage<MT>(p, uvq, m0, m0);
     cp_async_commit();
 #pragma unroll
     for (int k = 0; k < D - 1; ++k) {
-      issue(m0 + k, k);
+      issue(k);
       cp_async_commit();
     }
     cp_async_wait<D - 1>();  // the coefficients of the first chunk
@@ -456,7 +468,7 @@ __global__ void __launch_bounds__(kRotThreads, 2) rotate_lrec_kernel(RotParams p
     for (int l = m0; l < L; ++l) {
       const bool step = l + 1 < L;
       // copies D - 1 degrees ahead, and the next chunk's coefficients at a chunk start
-      issue(l + D - 1, rs == 0 ? D - 1 : rs - 1);
+      issue(rs == 0 ? D - 1 : rs - 1);  // degree l + D - 1
       if (lc == 0 && l + kRotChunk < L)
         rotate_stage<MT>(p, uvq + (ub ^ 1) * kRotChunk * MT, l + kRotChunk, m0);
       cp_async_commit();
