@@ -541,10 +541,10 @@ def profile_batched_uneven(torch, schedule):
     return {"schedule": schedule, "eager_ms": e0.elapsed_time(e1), "groups": len(b.groups)}
 
 
-def profile_rotation(torch, L=1024, rot=(0.7, 1.9, -2.4)):
+def profile_rotation(torch, L=1024, rot=(0.7, 1.9, -2.4), profile=True):
     """rotate_flms of one float64 map (Euler angles rot): CUDA-event times of five calls
     after a warm-up, the largest change of a degree's power and the round-trip error, then
-    one call between cudaProfilerStart/Stop."""
+    (profile) one call between cudaProfilerStart/Stop."""
     from s2fft_b200 import rotation
 
     dev = torch.device("cuda", torch.cuda.current_device())
@@ -560,10 +560,11 @@ def profile_rotation(torch, L=1024, rot=(0.7, 1.9, -2.4)):
         e1.record()
         torch.cuda.synchronize()
         ts.append(e0.elapsed_time(e1))
-    torch.cuda.profiler.start()
-    rotation.rotate_flms(flm, L, rot)
-    torch.cuda.synchronize()
-    torch.cuda.profiler.stop()
+    if profile:
+        torch.cuda.profiler.start()
+        rotation.rotate_flms(flm, L, rot)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
     p0, p1 = (flm.abs() ** 2).sum(-1), (r.abs() ** 2).sum(-1)
     return {"workload": f"rotate_flms L={L} f64, one map, rotation {rot}",
             "ms_min": min(ts), "ms_median": float(np.median(ts)),
@@ -853,6 +854,7 @@ def main():
         line["healpix_iter3"] = run_healpix_iter(torch)
         line["batched_uneven"] = run_batched_uneven(torch)
         line["so3_fourier_wigner"] = run_so3(torch)
+        line["rotation"] = profile_rotation(torch, 1024, profile=False)
     if not args.no_cpu_baseline and not args.profile_case and world == 1:
         ref = CpuReference(args.L)
         ref.step()  # warm-up (thread pool, page faults)
