@@ -56,6 +56,9 @@ def parse_args():
     ap.add_argument("--rotate-profile", action="store_true",
                     help="rotate_flms at --L (float64, one map): warm-up, five timed calls, "
                          "then one call between cudaProfilerStart/Stop")
+    ap.add_argument("--planes-profile", action="store_true",
+                    help="generate_rotate_dls at --L and beta = pi/2: warm-up, three timed "
+                         "calls, then one call between cudaProfilerStart/Stop")
     ap.add_argument("--batch-profile", choices=["persistent", "streams"], default=None,
                     help="the 256-map uneven batch, one eager inverse + forward of the given "
                          "schedule between cudaProfilerStart/Stop (ncu --profile-from-start "
@@ -572,6 +575,31 @@ def profile_rotation(torch, L=1024, rot=(0.7, 1.9, -2.4), profile=True):
             "roundtrip_max_rel_err": float((back - flm).abs().max() / flm.abs().max())}
 
 
+def profile_planes(torch, L=256, beta=np.pi / 2):
+    """generate_rotate_dls(L, beta) (the Fourier-Wigner Delta planes at pi/2): CUDA-event
+    times of three calls after a warm-up, the write rate of the [L][2L-1][2L-1] float64
+    output, then one call between cudaProfilerStart/Stop."""
+    from s2fft_b200 import rotation
+
+    out = rotation.generate_rotate_dls(L, beta)
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
+        e0.record()
+        out = rotation.generate_rotate_dls(L, beta)
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    torch.cuda.profiler.start()
+    out = rotation.generate_rotate_dls(L, beta)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    nbytes = out.numel() * 8
+    return {"workload": f"generate_rotate_dls L={L} beta={beta:.6f}", "ms_min": min(ts),
+            "output_bytes": nbytes, "write_gbs": nbytes / (min(ts) * 1e6)}
+
+
 def profile_healpix(torch, nside=256, L=512):
     """One float32 HEALPix inverse and forward (3 iterations) after a warm-up call, between
     cudaProfilerStart/Stop."""
@@ -780,6 +808,9 @@ def main():
         return
     if args.rotate_profile:
         print(json.dumps(profile_rotation(torch, args.L)))
+        return
+    if args.planes_profile:
+        print(json.dumps(profile_planes(torch, args.L)))
         return
     if args.profile_case:
         args.steps, args.warmup = 2, 1
