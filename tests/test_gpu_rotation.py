@@ -84,3 +84,15 @@ def test_rotation_unitary_large(s2b, rng, L, rot):
     assert float(((p1 - p0).abs() / p0.clamp_min(1e-300)).max()) < 1e-11
     back = s2b.rotation.rotate_flms(r, L, (-rot[2], -rot[1], -rot[0]))
     assert float((back - flm).abs().max() / flm.abs().max()) < 1e-10
+
+
+@pytest.mark.parametrize("L", [1, 2, 3, 9])
+def test_rotation_small_band_limits(s2b, rng, L):
+    """The smallest band-limits (one warp, one CTA per cluster, partial order tiles)."""
+    rot = (0.4, 2.2, -0.9)
+    flm = oracle.signal.generate_flm(rng, L, 0, 0, False)
+    r = s2b.rotation.rotate_flms(flm, L, rot)
+    ref = oracle.rotation.rotate_flms(flm, L, rot)
+    assert relerr(r, ref) < 1e-13, relerr(r, ref)
+    dl = s2b.rotation.generate_rotate_dls(L, rot[1]).cpu().numpy()
+    assert np.abs(dl - oracle.rotation.generate_rotate_dls(L, rot[1])).max() < 1e-14
