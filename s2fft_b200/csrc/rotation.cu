@@ -27,13 +27,14 @@
 // Schedule: a cluster of CTAs owns MT orders m0..m0+MT-1 (with their negatives) and all
 // n; lanes run along n in zigzag order (0, -1, 1, -2, ...) dealt to the cluster's CTAs
 // and warps in turn, so short and long n are shared alike. Each lane carries MT x S
-// recurrences in registers and walks l from m0 to L-1. Per degree a warp reduces its
-// 4 MT sums (+-m, re / im) by halving shuffles into shared memory; every kRotChunk
-// degrees one cluster barrier, then each CTA sums its share of the outputs over the
-// cluster's warps through distributed shared memory in a fixed order (deterministic, no
-// atomics) and writes them with exp(-i m alpha). The planes path writes every entry of
-// [L][2L-1][2L-1] once, zeros included, and is bound by that write. All arithmetic is
-// double.
+// recurrences in registers and walks l from m0 to L-1; its operands (T[l][|n|],
+// flm[l][+-n]) arrive through a cp.async ring in shared memory a few degrees ahead. Per
+// degree a warp reduces its 4 MT sums (+-m, re / im) by halving shuffles into shared
+// memory. Every kRotChunk degrees a CTA sums its warps and publishes the result with a
+// cluster arrive; after the matching wait, at the end of the next chunk, each CTA sums its
+// share of the outputs over the cluster's CTAs through distributed shared memory in rank
+// order (deterministic, no atomics) and writes them with exp(-i m alpha). The planes path
+// writes every entry of [L][2L-1][2L-1] once, zeros included. All arithmetic is double.
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
