@@ -674,6 +674,264 @@ __global__ void __launch_bounds__(kRotThreads, 2) rotate_lrec_kernel(RotParams p
   }
 }
 
+// FP64 tensor-core step: D (8 x 8) += A (8 x 4) B (4 x 8), lane t holding A[t/4][t%4],
+// B[t%4][t/4] and D[t/4][2 (t%4) + {0, 1}] (mma.m8n8k4 .f64 fragments)
+__device__ __forceinline__ void dmma_884(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// The contraction on the FP64 tensor cores (one n per fetching lane, 8 orders per tile).
+// A warp owns a warp slot of 32 n (fetched as in rotate_lrec_kernel, one per lane) and the
+// tile's 8 orders; for the arithmetic lane t takes order m0 + t/4 and the 8 n of positions
+// 4j + t%4, j = 0..7, so its 8 recurrences are exactly its A fragments of 8 MMA steps. The
+// B fragments are the weights of those n: lane t supplies component t/4 (+m re, +m im,
+// -m re, -m im; zero for t/4 >= 4), read from a per-warp table that each lane fills for
+// its own n. D[order][component] is the warp's sum over its 32 n, so no shuffle reduction
+// runs; lanes with t%4 < 2 park their two components in the same per-warp slots as
+// rotate_lrec_kernel, and the cluster reduction is the same.
+// Dynamic shared memory: ring [D][3][nt] double2 | uvq [2][kRotChunk][8] double4 |
+// ybuf [nw][32][4] double | sbuf [kRotChunk][nw][32] | cpart [3][kRotChunk][32].
+template <typename R2>
+__global__ void __launch_bounds__(kRotThreads, 2) rotate_mma_kernel(RotParams p) {
+  extern __shared__ double4 smem4[];
+  constexpr int MT = 8, D = 4;
+  const int L = p.L, NN = 2 * L - 1;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nt = blockDim.x;
+  const int nw = p.nw, nr = p.nr, rank = blockIdx.x;
+  const int m0 = blockIdx.y * MT;
+  double2* const ring = reinterpret_cast<double2*>(smem4);
+  double4* const uvq = smem4 + (D * 3 * nt) / 2;
+  double* const ybuf = reinterpret_cast<double*>(uvq + 2 * kRotChunk * MT);
+  double* const sbuf = ybuf + nw * 32 * 4;
+  double* const cpart = sbuf + kRotChunk * nw * 4 * MT;
+  double* const yw = ybuf + warp * 32 * 4;
+
+  // the fetching lane's n (zigzag order, as rotate_lrec_kernel)
+  const int gw = warp * nr + rank;
+  const int wmin = 16 * gw;  // least |n| of the warp slot
+  const int jf = gw * 32 + lane;
+  const int nf = (jf & 1) ? -((jf + 1) >> 1) : (jf >> 1);
+  const bool okf = jf < NN;
+  const int nvf = okf ? nf : 0, anf = okf ? abs(nf) : L;
+  const double2 eph = okf ? p.eg[L - 1 + nf] : make_double2(0.0, 0.0);
+  // the arithmetic lane's order and n
+  const int row = lane >> 2, q = lane & 3;
+  const int m = m0 + row;
+  int nv[8], an[8];
+  double nd[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const int jj = gw * 32 + 4 * j + q;
+    const int n = (jj & 1) ? -((jj + 1) >> 1) : (jj >> 1);
+    const bool ok = jj < NN;
+    nv[j] = ok ? n : 0;
+    an[j] = ok ? abs(n) : L;
+    nd[j] = (double)nv[j];
+  }
+  const int wlo = max(m0, wmin), whi = min(L - 1, max(m0 + MT - 1, wmin + 16));
+
+  int ck = 0, pb = 0, plf = 0, plc = 0;
+#pragma unroll 1
+  for (int b = 0; b < p.batch; ++b) {
+    {  // degrees below m0: the tile's rows are zero there
+      const int tot = m0 * 2 * MT;
+#pragma unroll 1
+      for (int e = rank * nt + tid; e < tot; e += nr * nt) {
+        const int l = e / (2 * MT), ci = e % (2 * MT), mm = m0 + (ci >> 1);
+        if (mm >= L || (mm == 0 && (ci & 1))) continue;
+        RotIO<R2>::put(p.out, ((size_t)b * L + l) * NN + L - 1 + ((ci & 1) ? -mm : mm),
+                       make_double2(0.0, 0.0));
+      }
+    }
+    const R2* const fb = reinterpret_cast<const R2*>(p.flm) + (size_t)b * L * NN + L - 1;
+    const unsigned rbase = (unsigned)__cvta_generic_to_shared(ring + tid);
+    const double2* tq = p.T + (size_t)m0 * L + min(anf, L - 1);
+    const R2* fq = fb + (size_t)m0 * NN + nvf;
+    int ll = m0;
+    auto issue = [&](int st) {  // the fetching lane's operands of degree ll into stage st
+      const bool vt = ll < L && ll >= wmin;
+      const unsigned r = rbase + (unsigned)(st * 3 * nt) * 16u;
+      cp_async<16>(r, tq, vt);
+      const bool vf = vt && anf <= ll;
+      cp_async<sizeof(R2)>(r + 16u * nt, fq, vf);
+      cp_async<sizeof(R2)>(r + 32u * nt, fq - 2 * nvf, vf);
+      if (ll + 1 < L) {
+        tq += L;
+        fq += NN;
+      }
+      ++ll;
+    };
+    rotate_stage<MT>(p, uvq, m0, m0);
+    cp_async_commit();
+#pragma unroll
+    for (int k = 0; k < D - 1; ++k) {
+      issue(k);
+      cp_async_commit();
+    }
+    cp_async_wait<D - 1>();
+    __syncthreads();
+
+    double v[8], vp[8];
+    int kx[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      v[j] = 0.0;
+      vp[j] = 0.0;
+      kx[j] = 0;
+    }
+    bool scaled = false;  // some lane of the warp carries a start value below 2^-960
+    int lc = 0, ub = 0, rs = 0;
+#pragma unroll 1
+    for (int l = m0; l < L; ++l) {
+      const bool step = l + 1 < L;
+      __syncwarp();  // every lane is done with the stage the next copies overwrite
+      issue(rs == 0 ? D - 1 : rs - 1);  // degree l + D - 1
+      if (lc == 0 && l + kRotChunk < L)
+        rotate_stage<MT>(p, uvq + (ub ^ 1) * kRotChunk * MT, l + kRotChunk, m0);
+      cp_async_commit();
+      cp_async_wait<D - 1>();
+      __syncwarp();  // the warp's copies of this degree are visible to all its lanes
+      const double2* const rg = ring + rs * 3 * nt + warp * 32;  // T of the warp's n
+      const int rso = rs;
+      rs = rs == D - 1 ? 0 : rs + 1;
+      double* const slot = sbuf + (lc * nw + warp) * (4 * MT);
+      if (l >= wmin) {  // some entry of the warp has started (warp-uniform)
+        {  // the weights of the fetching lane's n: e^{-in gamma} flm[n], (-1)^n e^{in gamma} flm[-n]
+          double2 xa, xb;
+          const double2* r = ring + rso * 3 * nt + tid;
+          if constexpr (sizeof(R2) == 16) {
+            xa = r[nt];
+            xb = r[2 * nt];
+          } else {
+            const float2 fa = *reinterpret_cast<const float2*>(r + nt);
+            const float2 fc = *reinterpret_cast<const float2*>(r + 2 * nt);
+            xa = make_double2(fa.x, fa.y);
+            xb = make_double2(fc.x, fc.y);
+          }
+          const double sg = (nvf & 1) ? -1.0 : 1.0;
+          double4 y;
+          y.x = xa.x * eph.x - xa.y * eph.y;
+          y.y = xa.x * eph.y + xa.y * eph.x;
+          y.z = sg * (xb.x * eph.x + xb.y * eph.y);
+          y.w = sg * (xb.y * eph.x - xb.x * eph.y);
+          reinterpret_cast<double4*>(yw)[lane] = y;
+        }
+        // entries starting at this degree (only inside the warp slot's start window)
+        if (l >= wlo && l <= whi) {
+          bool neg = false;
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            if (l == max(m, an[j])) {  // E[l][col] (symmetries of d)
+              int col;
+              bool flip = false;
+              if (m >= an[j]) {
+                col = nv[j];
+              } else if (nv[j] > 0) {
+                col = m;
+                flip = ((m - nv[j]) & 1) != 0;
+              } else {
+                col = -m;
+              }
+              const RotXD e0 = p.start[(size_t)l * NN + L - 1 + col];
+              v[j] = flip ? -e0.m : e0.m;
+              kx[j] = e0.e;
+              vp[j] = 0.0;
+            }
+            neg |= kx[j] < 0;
+          }
+          scaled = __any_sync(0xffffffffu, neg) || scaled;
+        }
+        __syncwarp();  // the weight table is written
+        const double4 uv = uvq[(ub * kRotChunk + lc) * MT + row];
+        auto advance = [&](auto sc_tag) {
+          constexpr bool SC = decltype(sc_tag)::value;
+          double d0 = 0.0, d1 = 0.0, e0 = 0.0, e1 = 0.0;  // two accumulators: even, odd j
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const int k = 4 * j + q;
+            const double2 tk = rg[k];
+            const double y = row < 4 ? yw[k * 4 + row] : 0.0;
+            double dv = v[j];
+            if constexpr (SC) dv *= pow2k(kx[j]);
+            if (j & 1)
+              dmma_884(e0, e1, dv, y);
+            else
+              dmma_884(d0, d1, dv, y);
+            if (step) {
+              const double t = fma(uv.z, nd[j], p.cb);
+              double vn = (uv.x * tk.x) * fma(t, v[j], -(uv.y * tk.y) * vp[j]);
+              double vc = v[j];
+              if constexpr (SC) {  // renormalise by up to 2^64 once |vn| >= 2^65
+                const bool big =
+                    kx[j] < 0 && (__double2hiint(vn) & 0x7ff00000) > ((1023 + 64) << 20);
+                const int sh = big ? min(64, -kx[j]) : 0;
+                const double f = __hiloint2double((1023 - sh) << 20, 0);
+                vn *= f;
+                vc *= f;
+                kx[j] += sh;
+              }
+              vp[j] = vc;
+              v[j] = vn;
+            }
+          }
+          if (q < 2)
+            reinterpret_cast<double2*>(slot)[2 * row + q] = make_double2(d0 + e0, d1 + e1);
+          if constexpr (SC) {
+            bool neg = false;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) neg |= kx[j] < 0;
+            scaled = __any_sync(0xffffffffu, neg);
+          }
+        };
+        if (scaled)
+          advance(std::true_type{});
+        else
+          advance(std::false_type{});
+      } else if (q < 2) {
+        reinterpret_cast<double2*>(slot)[2 * row + q] = make_double2(0.0, 0.0);
+      }
+
+      if (lc == kRotChunk - 1 || l == L - 1) {
+        __syncthreads();  // sums of the chunk and the next chunk's coefficients in place
+        double* const cp = cpart + (ck % 3) * kRotChunk * 4 * MT;
+        const int nv4 = (lc + 1) * 4 * MT;
+        for (int e = tid; e < nv4; e += nt) {
+          const double* src = sbuf + (size_t)(e / (4 * MT)) * nw * 4 * MT + e % (4 * MT);
+          double t = 0.0;
+#pragma unroll
+          for (int w = 0; w < kRotThreads / 32; ++w)
+            if (w < nw) t += src[w * 4 * MT];
+          cp[e] = t;
+        }
+        __syncthreads();  // sbuf free for the next chunk
+        if (ck > 0) {     // the previous chunk: every CTA has published it
+          cluster_wait();
+          rotate_flush<R2, MT>(p, cpart + ((ck - 1) % 3) * kRotChunk * 4 * MT, pb, plf, plc, m0,
+                               rank);
+        }
+        cluster_arrive();
+        pb = b;
+        plf = l - lc;
+        plc = lc;
+        ++ck;
+        ub ^= 1;
+        lc = 0;
+      } else {
+        ++lc;
+      }
+    }
+    cp_async_wait<0>();
+  }
+  if (ck > 0) {
+    cluster_wait();
+    rotate_flush<R2, MT>(p, cpart + ((ck - 1) % 3) * kRotChunk * 4 * MT, pb, plf, plc, m0, rank);
+    cluster_arrive();  // no CTA leaves while others read its sums
+    cluster_wait();
+  }
+}
+
 // rotation with caller-supplied planes dl[l][L-1+m][L-1+n]: one warp per (map, l, m)
 template <typename R2>
 __global__ void rotate_planes_kernel(RotParams p) {
@@ -755,6 +1013,33 @@ cudaError_t launch_lrec(const RotParams& p, cudaStream_t s) {
   return cudaLaunchKernelEx(&cfg, kern, p);
 }
 
+template <typename R2>
+cudaError_t launch_mma(const RotParams& p, cudaStream_t s) {
+  constexpr int MT = 8;
+  // ring, uvq, ybuf, sbuf and cpart (rotate_mma_kernel)
+  const size_t nt = 32 * (size_t)p.nw;
+  const size_t smem = (size_t)4 * 3 * nt * 16 + 2 * kRotChunk * MT * 32 +
+                      ((size_t)p.nw * 32 * 4 + (size_t)kRotChunk * p.nw * 4 * MT +
+                       3 * kRotChunk * 4 * MT) * 8;
+  void (*kern)(RotParams) = rotate_mma_kernel<R2>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)p.nr, (unsigned)((p.L + MT - 1) / MT), 1);
+  cfg.blockDim = dim3((unsigned)(32 * p.nw), 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)p.nr;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, p);
+}
+
 template <typename R2, bool PL>
 cudaError_t launch_shape(const RotParams& p, const RotShape& sh, cudaStream_t s) {
   switch (sh.s * 16 + sh.mt) {
@@ -803,6 +1088,7 @@ cudaError_t rotate_launch(RotParams p, cudaStream_t s) {
   rotate_start_final_kernel<<<dim3(nb, L), 128, 0, s>>>(p);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
+  if (p.flm && sh.s == 1 && sh.mt == 8) return launch_mma<R2>(p, s);
   return p.flm ? launch_shape<R2, false>(p, sh, s) : launch_shape<double2, true>(p, sh, s);
 }
 
