@@ -33,8 +33,11 @@
 // memory. Every kRotChunk degrees a CTA sums its warps and publishes the result with a
 // cluster arrive; after the matching wait, at the end of the next chunk, each CTA sums its
 // share of the outputs over the cluster's CTAs through distributed shared memory in rank
-// order (deterministic, no atomics) and writes them with exp(-i m alpha). The planes path
-// writes every entry of [L][2L-1][2L-1] once, zeros included. All arithmetic is double.
+// order (deterministic, no atomics) and writes them with exp(-i m alpha). With 8 orders
+// per tile and one n per lane (rotate_mma_kernel; clusters of up to 16 CTAs up to
+// L = 2048) the sum over a warp's 32 n runs on the FP64 tensor cores instead of shuffles.
+// The planes path writes every entry of [L][2L-1][2L-1] once, zeros included. All
+// arithmetic is double.
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
@@ -1037,6 +1040,15 @@ cudaError_t launch_mma(const RotParams& p, cudaStream_t s) {
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
+  if (p.nr > kRotMaxCluster) {  // non-portable cluster size: launch only where one fits
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    int nclusters = 0;
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveClusters(&nclusters, kern, &cfg);
+    if (e != cudaSuccess || nclusters < 1) {
+      (void)cudaGetLastError();
+      return cudaErrorNotSupported;
+    }
+  }
   return cudaLaunchKernelEx(&cfg, kern, p);
 }
 
@@ -1088,7 +1100,19 @@ cudaError_t rotate_launch(RotParams p, cudaStream_t s) {
   rotate_start_final_kernel<<<dim3(nb, L), 128, 0, s>>>(p);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  if (p.flm && sh.s == 1 && sh.mt == 8) return launch_mma<R2>(p, s);
+  if (p.flm) {
+    const int slots = (NN + 31) / 32, wmax = kRotThreads / 32;
+    if (sh.s == 2 && slots <= 2 * kRotMaxCluster * wmax) {
+      // up to 4096 n (L <= 2048): the tensor-core kernel with one n per lane in clusters of
+      // up to 16 CTAs, where the device has them; else two n per lane below
+      RotParams q = p;
+      q.nw = wmax;
+      q.nr = (slots + wmax - 1) / wmax;
+      e = launch_mma<R2>(q, s);
+      if (e != cudaErrorNotSupported) return e;
+    }
+    if (sh.s == 1 && sh.mt == 8) return launch_mma<R2>(p, s);
+  }
   return p.flm ? launch_shape<R2, false>(p, sh, s) : launch_shape<double2, true>(p, sh, s);
 }
 

@@ -70,11 +70,12 @@ def test_rotation_planes_against_risbo(s2b, L, beta):
 
 
 @pytest.mark.parametrize("L,rot", [(1024, (0.3, 0.05, -1.2)), (600, (2.0, 3.05, 0.4)),
-                                   (2049, (0.5, 1.1, 2.5))])
+                                   (1500, (0.3, 2.9, 1.0)), (2049, (0.5, 1.1, 2.5))])
 def test_rotation_unitary_large(s2b, rng, L, rot):
     """Rotation keeps the power of every degree, sum_m |flm'[l, m]|^2 = sum_m |flm[l, m]|^2,
     and rotating back restores flm: at L = 1024 and 600 with betas near 0 and pi (start
-    values below 2^-960, renormalised recurrences) and at L = 2049 (two n per lane)."""
+    values below 2^-960, renormalised recurrences), at L = 1500 (clusters of 12 CTAs on
+    the tensor-core path) and at L = 2049 (four n per lane)."""
     import torch
 
     flm = torch.from_numpy(oracle.signal.generate_flm(rng, L, 0, 0, False)).cuda()
