@@ -37,6 +37,7 @@
 
 #include "s2b.h"
 #include "s2b_fft.h"
+#include "s2b_dev.h"
 #include "s2b_fft_dev.h"
 #include "s2b_internal.h"
 #include "s2b_wigner.h"  // launch_wigner_mirror
@@ -79,7 +80,8 @@ template <typename Real>
 struct FWTile {
   static constexpr int R = 4;
   static constexpr int E = 4;
-  static constexpr int QU = 2;  // summation indices per load batch
+  // summation indices a thread's copies run ahead (cp.async ring in shared memory)
+  static constexpr int D = sizeof(Real) == 4 ? 4 : 3;
 };
 
 template <typename Real>
@@ -105,12 +107,14 @@ struct FWContractParams {
 // FWD: out[e][l][m] = (2pi)^2 i^(m-n) sum_{0 <= b <= l} D[l][b][m] D[l][b][n] Gf[e][b][m],
 //      where Gf[b] = G[b] + (-1)^(m+n) G[-b] (b > 0), Gf[0] = G[0] (fw_cols_fwd_kernel).
 // Lanes run along m; each thread keeps R x E complex sums. The n-column weights of a chunk
-// of kFwQ summation indices are staged in shared memory and read as broadcasts. The slice
-// tiles run along blockIdx.x, so the CTAs that read the same planes run together.
+// of kFwQ summation indices are staged in shared memory and read as broadcasts; each
+// thread's own operands of an index (E coefficients, R plane values) arrive by cp.async a
+// few indices ahead. The slice tiles run along blockIdx.x, so the CTAs that read the same
+// planes run together.
 template <typename Real, bool FWD>
 __global__ void __launch_bounds__(kFwLanes) fw_contract_kernel(FWContractParams<Real> p) {
   using R2 = typename C2<Real>::t;
-  constexpr int R = FWTile<Real>::R, E = FWTile<Real>::E, QU = FWTile<Real>::QU;
+  constexpr int R = FWTile<Real>::R, E = FWTile<Real>::E, D = FWTile<Real>::D;
   const int L = p.L, W = 2 * L - 1;
   const int ci = blockIdx.y * kFwLanes + threadIdx.x;  // column index m + L - 1
   const bool live = ci < W;
@@ -160,6 +164,31 @@ __global__ void __launch_bounds__(kFwLanes) fw_contract_kernel(FWContractParams<
   }
 
   const double pi = 3.141592653589793;
+  // each thread's operands of summation index q (its coefficients of the E slices and its
+  // plane values of the R rows) reach shared memory by cp.async, D - 1 indices ahead of
+  // their arithmetic; only the thread itself reads its slots
+  __shared__ __align__(16) R2 xr[D][E][kFwLanes];
+  __shared__ __align__(16) double wr[D][R][kFwLanes];
+  auto issue = [&](int q, int st) {
+    if (!live || q > qhi) return;
+#pragma unroll
+    for (int s = 0; s < E; ++s)
+      cp_async<sizeof(R2)>(smem_u32(&xr[st][s][threadIdx.x]), X + xoff[s] + (long)q * W + ci,
+                           true);
+#pragma unroll
+    for (int j = 0; j < R; ++j) {  // rows past L-1 read row L-1 and get weight 0
+      const int r = min(r0 + j, L - 1);
+      const double* src = FWD ? p.delta + ((long)r * W + (q + L - 1)) * W + ci
+                              : p.delta + ((long)q * W + (r + L - 1)) * W + ci;
+      cp_async<8>(smem_u32(&wr[st][j][threadIdx.x]), src, true);
+    }
+  };
+#pragma unroll
+  for (int k = 0; k < D - 1; ++k) {
+    issue(qlo + k, k);
+    cp_async_commit();
+  }
+  int rs = 0;  // ring stage of the current index
   for (int q0 = qlo; q0 <= qhi; q0 += kFwQ) {
     // stage the n-column weights of this chunk
     for (int t = threadIdx.x; t < kFwQ * R * E; t += kFwLanes) {
@@ -177,41 +206,32 @@ __global__ void __launch_bounds__(kFwLanes) fw_contract_kernel(FWContractParams<
     }
     __syncthreads();
     const int qend = min(kFwQ, qhi - q0 + 1);
-    if (live) {
-      // QU summation indices per step, all their loads issued before the arithmetic
-      // (rows past L-1 and indices past qhi read row L-1 / index qhi and get weight 0)
-      for (int qq0 = 0; qq0 < qend; qq0 += QU) {
-        R2 x[QU][E];
-        Real w1[QU][R];
+    for (int qq = 0; qq < qend; ++qq) {
+      issue(q0 + qq + D - 1, rs == 0 ? D - 1 : rs - 1);
+      cp_async_commit();
+      cp_async_wait<D - 1>();  // this thread's copies of index q0 + qq
+      if (live) {
+        R2 x[E];
+        Real w1[R];
 #pragma unroll
-        for (int u = 0; u < QU; ++u) {
-          const int q = q0 + min(qq0 + u, qend - 1);
+        for (int s = 0; s < E; ++s) x[s] = xr[rs][s][threadIdx.x];
 #pragma unroll
-          for (int s = 0; s < E; ++s) x[u][s] = X[xoff[s] + (long)q * W + ci];
+        for (int j = 0; j < R; ++j) w1[j] = (Real)wr[rs][j][threadIdx.x];
 #pragma unroll
-          for (int j = 0; j < R; ++j) {
-            const int r = min(r0 + j, L - 1);
-            w1[u][j] = FWD ? (Real)__ldg(p.delta + ((long)r * W + (q + L - 1)) * W + ci)
-                           : (Real)__ldg(p.delta + ((long)q * W + (r + L - 1)) * W + ci);
-          }
-        }
+        for (int j = 0; j < R; ++j) {
 #pragma unroll
-        for (int u = 0; u < QU; ++u) {
-          if (qq0 + u >= qend) break;
-#pragma unroll
-          for (int j = 0; j < R; ++j) {
-#pragma unroll
-            for (int s = 0; s < E; ++s) {
-              const Real w = w1[u][j] * wn[qq0 + u][j][s];
-              acc[j][s].x = fma(w, x[u][s].x, acc[j][s].x);
-              acc[j][s].y = fma(w, x[u][s].y, acc[j][s].y);
-            }
+          for (int s = 0; s < E; ++s) {
+            const Real w = w1[j] * wn[qq][j][s];
+            acc[j][s].x = fma(w, x[s].x, acc[j][s].x);
+            acc[j][s].y = fma(w, x[s].y, acc[j][s].y);
           }
         }
       }
+      rs = rs == D - 1 ? 0 : rs + 1;
     }
     __syncthreads();
   }
+  cp_async_wait<0>();
   if (!live) return;
 
   R2* O = reinterpret_cast<R2*>(p.out);

@@ -46,6 +46,7 @@
 #include <type_traits>
 
 #include "s2b.h"
+#include "s2b_dev.h"
 #include "s2b_internal.h"
 #include "s2b_rotation.h"
 
@@ -242,25 +243,6 @@ __device__ __forceinline__ double reduce_perm(double* x) {
 #pragma unroll
   for (int o = 16 / V; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
   return r;
-}
-
-// asynchronous global -> shared copies of B bytes (zero-filled when !valid); d is a
-// shared-space address
-template <int B>
-__device__ __forceinline__ void cp_async(unsigned d, const void* src, bool valid) {
-  if constexpr (B == 16)
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src),
-                 "r"(valid ? 16 : 0)
-                 : "memory");
-  else
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src),
-                 "r"(valid ? 8 : 0)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
 // split cluster barrier: arrive publishes this thread's earlier shared-memory writes to

@@ -109,6 +109,28 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
       "l"(src), "r"(bytes), "r"(smem_u32(mb))
       : "memory");
 }
+// Per-thread asynchronous global -> shared copy of B (8 or 16) bytes to the shared-space
+// address d (zero-filled when !valid: the source is not read), and its group fences.
+template <int B>
+__device__ __forceinline__ void cp_async(unsigned d, const void* src, bool valid) {
+  static_assert(B == 8 || B == 16, "cp.async of 8 or 16 bytes");
+  if constexpr (B == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src),
+                 "r"(valid ? 16 : 0)
+                 : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src),
+                 "r"(valid ? 8 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // Bounded wait for the phase with the given parity; false when it ran out.
 __device__ __forceinline__ bool mbar_wait(uint64_t* mb, unsigned parity) {
   const uint32_t a = smem_u32(mb);
