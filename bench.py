@@ -59,6 +59,10 @@ def parse_args():
     ap.add_argument("--planes-profile", action="store_true",
                     help="generate_rotate_dls at --L and beta = pi/2: warm-up, three timed "
                          "calls, then one call between cudaProfilerStart/Stop")
+    ap.add_argument("--fw-profile", action="store_true",
+                    help="Fourier-Wigner SO(3) transforms at --L (N=8, MW, float32): warm-up, "
+                         "five timed inverse and forward calls, then one of each between "
+                         "cudaProfilerStart/Stop")
     ap.add_argument("--batch-profile", choices=["persistent", "streams"], default=None,
                     help="the 256-map uneven batch, one eager inverse + forward of the given "
                          "schedule between cudaProfilerStart/Stop (ncu --profile-from-start "
@@ -600,6 +604,42 @@ def profile_planes(torch, L=256, beta=np.pi / 2):
             "output_bytes": nbytes, "write_gbs": nbytes / (min(ts) * 1e6)}
 
 
+def profile_fourier_wigner(torch, L=256, N=8, prec="f32"):
+    """Fourier-Wigner inverse and forward of one seeded MW signal: CUDA-event minimum of five
+    calls each after a warm-up, the round-trip error, then one inverse and one forward
+    between cudaProfilerStart/Stop."""
+    from s2fft_b200 import fourier_wigner as fw
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    rng = np.random.default_rng(8)
+    flmn = np.stack([seeded_flm(rng, L, n) for n in range(-(N - 1), N)])
+    x = torch.from_numpy(flmn).to(dev).to(torch.complex64 if prec == "f32" else torch.complex128)
+    pre = fw.fourier_wigner_kernel(L)
+    f = fw.inverse_transform(x, L, N, pre, precision=prec)
+    g = fw.forward_transform(f, L, N, pre, precision=prec)
+    torch.cuda.synchronize()
+    out = {"workload": f"Fourier-Wigner mw L={L} N={N} {prec}, one signal"}
+    for name, fn in (("inverse", lambda: fw.inverse_transform(x, L, N, pre, precision=prec)),
+                     ("forward", lambda: fw.forward_transform(f, L, N, pre, precision=prec))):
+        ts = []
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        out[name + "_ms"] = min(ts)
+    torch.cuda.profiler.start()
+    f = fw.inverse_transform(x, L, N, pre, precision=prec)
+    fw.forward_transform(f, L, N, pre, precision=prec)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    out["roundtrip_max_rel_err"] = float((g.to(torch.complex128) - x.to(torch.complex128)).abs()
+                                         .max() / x.abs().max())
+    return out
+
+
 def profile_healpix(torch, nside=256, L=512):
     """One float32 HEALPix inverse and forward (3 iterations) after a warm-up call, between
     cudaProfilerStart/Stop."""
@@ -811,6 +851,9 @@ def main():
         return
     if args.planes_profile:
         print(json.dumps(profile_planes(torch, args.L)))
+        return
+    if args.fw_profile:
+        print(json.dumps(profile_fourier_wigner(torch, args.L)))
         return
     if args.profile_case:
         args.steps, args.warmup = 2, 1
