@@ -343,28 +343,38 @@ __global__ void __launch_bounds__(kRotThreads, 2) rotate_lrec_kernel(RotParams p
   const int mask = contract ? (lane >> (5 - LV)) & (V - 1) : 0;
   const int pm = mask >> 2, cm = mask & 3;
 
-  // this lane's n, one per S (zigzag order j -> 0, -1, 1, -2, 2, ...)
-  int nv[S], an[S], wmin[S];
+  // this lane's n, one per S: the contraction deals n in zigzag order (j -> 0, -1, 1, -2,
+  // 2, ...) so that every warp slot holds short and long n alike; the planes take n in
+  // natural order (j -> j - (L-1)), so that a warp's stores cover 32 consecutive columns
+  int nv[S], an[S], wmin[S], wmax[S];
   double nd[S];
   double2 eph[S];
 #pragma unroll
   for (int s = 0; s < S; ++s) {
     const int gw = (s * nw + warp) * nr + rank;  // warp slot in the cluster's n order
     const int j = gw * 32 + lane;
-    const int n = (j & 1) ? -((j + 1) >> 1) : (j >> 1);
+    const int n = PL ? j - (L - 1) : (j & 1) ? -((j + 1) >> 1) : (j >> 1);
     const bool ok = j < NN;
     nv[s] = ok ? n : 0;
     nd[s] = (double)nv[s];
     an[s] = ok ? abs(n) : L;  // L: never starts
-    wmin[s] = 16 * gw;        // least |n| of the warp slot
+    if constexpr (PL) {  // least and largest |n| of the warp slot's (valid) n
+      const int lo = gw * 32 - (L - 1), hi = min(lo + 31, L - 1);
+      wmin[s] = (lo <= 0 && hi >= 0) ? 0 : min(abs(lo), abs(hi));
+      wmax[s] = max(abs(lo), abs(hi));
+    } else {
+      wmin[s] = 16 * gw;
+      wmax[s] = 16 * gw + 16;
+    }
     eph[s] = ok && contract ? p.eg[L - 1 + n] : make_double2(0.0, 0.0);
   }
   // degrees at which some entry of the warp slot starts: max(m, |n|) over its orders and lanes
-  int wlo[S], whi[S];
+  int wlo[S], whi[S], wany = wmin[0];  // wany: least |n| of the warp
 #pragma unroll
   for (int s = 0; s < S; ++s) {
     wlo[s] = max(m0, wmin[s]);
-    whi[s] = min(L - 1, max(m0 + MT - 1, wmin[s] + 16));
+    whi[s] = min(L - 1, max(m0 + MT - 1, wmax[s]));
+    wany = min(wany, wmin[s]);
   }
 
   const int nmaps = contract ? p.batch : 1;
@@ -604,7 +614,7 @@ __global__ void __launch_bounds__(kRotThreads, 2) rotate_lrec_kernel(RotParams p
           scaled = __any_sync(0xffffffffu, neg);
         }
       };
-      if (l >= wmin[0]) {  // some entry of the warp has started (warp-uniform)
+      if (l >= wany) {  // some entry of the warp has started (warp-uniform)
         if (scaled)
           advance(std::true_type{});
         else

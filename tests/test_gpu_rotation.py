@@ -110,3 +110,19 @@ def test_rotation_f32_batch(s2b, rng):
     assert r32.dtype == np.complex64 and relerr(r32, r64) < 1e-6, relerr(r32, r64)
     one = s2b.rotation.rotate_flms(flm[2].astype(np.complex64), L, rot)
     assert np.array_equal(one, r32[2])
+
+
+def test_rotation_planes_two_n_per_lane(s2b, rng):
+    """Planes at L = 1040 (36 GB; two n per lane, natural n order) passed back as dl_array
+    give the rotation computed without them."""
+    import torch
+
+    L = 1040
+    rot = (0.9, 1.3, -0.6)
+    flm = torch.from_numpy(oracle.signal.generate_flm(rng, L, 0, 0, False)).cuda()
+    dl = s2b.rotation.generate_rotate_dls(L, rot[1])
+    r1 = s2b.rotation.rotate_flms(flm, L, rot, dl_array=dl)
+    del dl
+    torch.cuda.empty_cache()
+    r0 = s2b.rotation.rotate_flms(flm, L, rot)
+    assert float((r1 - r0).abs().max() / r0.abs().max()) < 1e-12
