@@ -101,3 +101,35 @@ def test_fourier_wigner_arguments_rejected_on_host(lib):
         assert lib.s2b_last_error()
     assert lib.s2b_fw_plan_create(8, 2, 0, 0, None) == 1
     assert lib.s2b_fw_workspace_size(None, 0, 1, 0, 1) == 0
+
+
+def test_rotation_arguments_rejected_on_host(lib):
+    """s2b_rotate_flms / s2b_rotate_dls check L, buffers, aliasing, precision and the
+    workspace size before any CUDA call; the workspace size grows with L."""
+    vp, sz = ctypes.c_void_p, ctypes.c_size_t
+    lib.s2b_rotate_workspace_size.restype = sz
+    lib.s2b_rotate_workspace_size.argtypes = [ctypes.c_int]
+    lib.s2b_rotate_flms.restype = ctypes.c_int
+    lib.s2b_rotate_flms.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int] + \
+        [ctypes.c_double] * 3 + [vp, vp, vp, vp, sz, vp]
+    lib.s2b_rotate_dls.restype = ctypes.c_int
+    lib.s2b_rotate_dls.argtypes = [ctypes.c_int, ctypes.c_double, vp, vp, sz, vp]
+    assert lib.s2b_rotate_workspace_size(0) == 0
+    w8, w64 = lib.s2b_rotate_workspace_size(8), lib.s2b_rotate_workspace_size(64)
+    assert 0 < w8 < w64
+    a, b, ws = vp(16), vp(4096), vp(1 << 20)  # never dereferenced: rejected first
+    cases = [
+        (0, 1, 0, a, b, None, ws, w8),         # L < 1
+        (8, 0, 0, a, b, None, ws, w8),         # batch < 1
+        (8, 1, 0, None, b, None, ws, w8),      # no input
+        (8, 1, 0, a, a, None, ws, w8),         # out aliases flm
+        (8, 1, 5, a, b, None, ws, w8),         # precision
+        (9000, 1, 0, a, b, None, ws, 1 << 62),  # L above the recurrence limit, no planes
+    ]
+    for L, B, prec, x, y, dl, w, wb in cases:
+        assert lib.s2b_rotate_flms(L, B, prec, 0.1, 0.2, 0.3, x, y, dl, w, wb, None) == 1
+        assert lib.s2b_last_error()
+    assert lib.s2b_rotate_flms(8, 1, 0, 0.1, 0.2, 0.3, a, b, None, ws, w8 - 1, None) == 3
+    assert lib.s2b_rotate_dls(9000, 0.2, b, ws, 1 << 62, None) == 1
+    assert lib.s2b_rotate_dls(8, 0.2, b, ws, w8 - 1, None) == 3
+    assert lib.s2b_rotate_dls(8, 0.2, None, ws, w8, None) == 1
