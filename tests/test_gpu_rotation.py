@@ -126,3 +126,18 @@ def test_rotation_planes_two_n_per_lane(s2b, rng):
     torch.cuda.empty_cache()
     r0 = s2b.rotation.rotate_flms(flm, L, rot)
     assert float((r1 - r0).abs().max() / r0.abs().max()) < 1e-12
+
+
+def test_rotation_batch_tensor_core_path(s2b, rng):
+    """A batch of two maps at L = 1024 (the tensor-core kernel walks the maps one after the
+    other, continuing its chunk sequence): each map equals its own call."""
+    import torch
+
+    L = 1024
+    rot = (2.1, 0.6, 1.4)
+    flm = torch.from_numpy(np.stack([oracle.signal.generate_flm(rng, L, 0, 0, False)
+                                     for _ in range(2)])).cuda()
+    r = s2b.rotation.rotate_flms(flm, L, rot)
+    for k in range(2):
+        one = s2b.rotation.rotate_flms(flm[k], L, rot)
+        assert torch.equal(one, r[k])
