@@ -977,6 +977,11 @@ RotShape rotate_shape(int L, int sms) {
   if (r.s == 1) {
     r.mt = 8;
     while (r.mt > 2 && (long)r.nr * ((L + r.mt - 1) / r.mt) < 2L * sms) r.mt >>= 1;
+    // four orders per tile: CTAs of 4 warps in twice the clusters (L = 512: 0.60 -> 0.55 ms)
+    if (r.mt == 4 && r.nw == wmax && 2 * r.nr <= kRotMaxCluster) {
+      r.nw /= 2;
+      r.nr *= 2;
+    }
   } else {
     r.mt = r.s == 2 ? 4 : 2;
   }
