@@ -708,15 +708,35 @@ __global__ void __launch_bounds__(512) fw_gamma_fft_kernel(const void* in, void*
 
 // quads[j] = sum_{|k| <= 2L-2} w(-k) e^{+2 pi i k j / (4L-3)}, w the MW weights
 // (w(+-1) = +-i pi/2, w(even k) = 2/(1-k^2), else 0); construct.py:629-634.
-__global__ void fw_quads_kernel(int L, double2* quads) {
-  // one warp per output j, the 4L-3 terms split over the lanes and summed by shuffles
+// roots[r] = e^{2 pi i r / n}, r in [0, n)
+__global__ void fw_roots_kernel(int n, double2* roots) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    double sn, cs;
+    sincospi(2.0 * (double)r / (double)n, &sn, &cs);
+    roots[r] = make_double2(cs, sn);
+  }
+}
+
+// exponent index (a b) mod n (n > 0), for any signs of a and b
+__device__ __forceinline__ int fw_mulmod(long a, long b, int n) {
+  return (int)(((a * b) % n + n) % n);
+}
+
+__global__ void fw_quads_kernel(int L, double2* quads, const double2* __restrict__ rootsP) {
+  // one warp per output j, the 4L-3 terms split over the lanes and summed by shuffles; the
+  // exponent index of term k = k0 + 32 t advances by 32 j (mod P)
   const int P = 4 * L - 3;
   const int j = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5);
   const int lane = threadIdx.x & 31;
   if (j >= P) return;  // whole warps leave together (blockDim is a multiple of 32)
   double re = 0.0, im = 0.0;
+  int r = fw_mulmod(-(2 * L - 2) + lane, j, P);
+  const int dr = fw_mulmod(32, j, P);
   for (int k = -(2 * L - 2) + lane; k <= 2 * L - 2; k += 32) {
     const int mk = -k;
+    const int rk = r;
+    r += dr;
+    if (r >= P) r -= P;
     double wr = 0.0, wi = 0.0;
     if (mk == 1)
       wi = 1.5707963267948966;
@@ -726,11 +746,9 @@ __global__ void fw_quads_kernel(int L, double2* quads) {
       wr = 2.0 / (1.0 - (double)mk * (double)mk);
     else
       continue;
-    const long r = (((long)k * j) % P + P) % P;
-    double sn, cs;
-    sincospi(2.0 * (double)r / (double)P, &sn, &cs);
-    re += wr * cs - wi * sn;
-    im += wr * sn + wi * cs;
+    const double2 e = rootsP[rk];
+    re += wr * e.x - wi * e.y;
+    im += wr * e.y + wi * e.x;
   }
   for (int o = 16; o > 0; o >>= 1) {
     re += __shfl_xor_sync(0xffffffffu, re, o);
@@ -747,20 +765,23 @@ __global__ void fw_quads_kernel(int L, double2* quads) {
 // wrapped terms off the 2L-1 kept outputs (the spectrum spans at most 2L values).
 // One warp per output; exponents reduced exactly.
 __global__ void fw_weights_from_quads_kernel(int L, const double2* __restrict__ quads,
-                                             double2* __restrict__ w) {
+                                             double2* __restrict__ w,
+                                             const double2* __restrict__ rootsP) {
   const int P = 4 * L - 3;
   const int o = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5);
   const int lane = threadIdx.x & 31;
   if (o >= P) return;
   const int k = o - (2 * L - 2);
   double re = 0.0, im = 0.0;
+  int r = fw_mulmod(-lane, k, P);  // (-j k) mod P, advancing by (-32 k) mod P
+  const int dr = fw_mulmod(-32, k, P);
   for (int j = lane; j < P; j += 32) {
-    const long r = ((-(long)j * k) % P + P) % P;
-    double sn, cs;
-    sincospi(2.0 * (double)r / (double)P, &sn, &cs);
+    const double2 e = rootsP[r];
     const double2 q = quads[j];
-    re += q.x * cs - q.y * sn;
-    im += q.x * sn + q.y * cs;
+    re += q.x * e.x - q.y * e.y;
+    im += q.x * e.y + q.y * e.x;
+    r += dr;
+    if (r >= P) r -= P;
   }
   for (int sh = 16; sh > 0; sh >>= 1) {
     re += __shfl_xor_sync(0xffffffffu, re, sh);
@@ -770,20 +791,21 @@ __global__ void fw_weights_from_quads_kernel(int L, const double2* __restrict__ 
 }
 
 __global__ void fw_quads_pow2_kernel(int L, int Q, const double2* __restrict__ w,
-                                     double2* __restrict__ quadsQ) {
+                                     double2* __restrict__ quadsQ,
+                                     const double2* __restrict__ rootsQ) {
   const int P = 4 * L - 3;
   const int j = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5);
   const int lane = threadIdx.x & 31;
   if (j >= Q) return;
   double re = 0.0, im = 0.0;
+  int r = fw_mulmod(lane - (2 * L - 2), j, Q);  // (k j) mod Q, advancing by 32 j (Q = 2^q)
+  const int dr = fw_mulmod(32, j, Q);
   for (int o = lane; o < P; o += 32) {
-    const int k = o - (2 * L - 2);
-    const long r = (((long)k * j) % Q + Q) % Q;
-    double sn, cs;
-    sincospi(2.0 * (double)r / (double)Q, &sn, &cs);
+    const double2 e = rootsQ[r];
     const double2 v = w[o];
-    re += v.x * cs - v.y * sn;
-    im += v.x * sn + v.y * cs;
+    re += v.x * e.x - v.y * e.y;
+    im += v.x * e.y + v.y * e.x;
+    r = (r + dr) & (Q - 1);
   }
   for (int sh = 16; sh > 0; sh >>= 1) {
     re += __shfl_xor_sync(0xffffffffu, re, sh);
@@ -865,6 +887,8 @@ struct s2b_fw_plan {
   int device;
   std::vector<void*> allocs;
   FFTSet fft;  // host[0]: length nphi, host[1]: length Q, host[2]: 2N-1 (gamma_fft)
+  double2* rootsP = nullptr;  // e^{2 pi i r / P}, r in [0, P)
+  double2* rootsQ = nullptr;  // e^{2 pi i r / Q}, r in [0, Q)
   ~s2b_fw_plan() {
     for (void* a : allocs) cudaFree(a);
   }
@@ -1007,9 +1031,9 @@ int forward_chain(const s2b_fw_plan* p, int E, const FWSlices& sl, const double*
   double2* wk = reinterpret_cast<double2*>(ws + lay.a + lay.b + lay.c);
   double2* qQ = wk + p->P;
   fw_weights_from_quads_kernel<<<(p->P + 3) / 4, 128, 0, st>>>(
-      p->L, reinterpret_cast<const double2*>(quads), wk);
+      p->L, reinterpret_cast<const double2*>(quads), wk, p->rootsP);
   FW_CK(cudaGetLastError());
-  fw_quads_pow2_kernel<<<(p->Q + 3) / 4, 128, 0, st>>>(p->L, p->Q, wk, qQ);
+  fw_quads_pow2_kernel<<<(p->Q + 3) / 4, 128, 0, st>>>(p->L, p->Q, wk, qQ, p->rootsQ);
   FW_CK(cudaGetLastError());
   FWFftParams<Real> f = fft_params<Real>(p, E, sl);
   f.quads = qQ;
@@ -1072,9 +1096,9 @@ int forward_adjoint_chain(const s2b_fw_plan* p, int E, const FWSlices& sl, const
   double2* wk = reinterpret_cast<double2*>(ws + lay.a + lay.b + lay.c);
   double2* qQ = wk + p->P;
   fw_weights_from_quads_kernel<<<(p->P + 3) / 4, 128, 0, st>>>(
-      p->L, reinterpret_cast<const double2*>(quads), wk);
+      p->L, reinterpret_cast<const double2*>(quads), wk, p->rootsP);
   FW_CK(cudaGetLastError());
-  fw_quads_pow2_kernel<<<(p->Q + 3) / 4, 128, 0, st>>>(p->L, p->Q, wk, qQ);
+  fw_quads_pow2_kernel<<<(p->Q + 3) / 4, 128, 0, st>>>(p->L, p->Q, wk, qQ, p->rootsQ);
   FW_CK(cudaGetLastError());
   int rc = contract<Real>(p, false, E, sl, delta, coef, A, st, 1);
   if (rc) return rc;
@@ -1230,6 +1254,24 @@ int s2b_fw_plan_create(int L, int N, int sampling, int precision, s2b_fw_plan** 
     delete p;
     return rc;
   }
+  // root tables of the quadrature weights (built once; the weights are recomputed from the
+  // caller's quads on every forward call)
+  for (int t = 0; t < 2; ++t) {
+    const int n = t == 0 ? p->P : p->Q;
+    void* d = nullptr;
+    e = cudaMalloc(&d, (size_t)n * sizeof(double2));
+    if (e == cudaSuccess) {
+      p->allocs.push_back(d);
+      fw_roots_kernel<<<(n + 255) / 256, 256>>>(n, reinterpret_cast<double2*>(d));
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+      delete p;
+      return fw_fail(S2B_ERR_CUDA, std::string("root tables: ") + cudaGetErrorString(e));
+    }
+    (t == 0 ? p->rootsP : p->rootsQ) = reinterpret_cast<double2*>(d);
+  }
   // the column chain keeps a DFT buffer and Q values in shared memory
   const size_t cs = p->fp64 ? 16 : 8;
   const int bufM = std::max(p->fft.host[0].M, p->fft.host[1].M);
@@ -1250,8 +1292,8 @@ int s2b_fw_quads(s2b_fw_plan* plan, void* quads, void* stream) {
   int rc;
   if ((rc = check_plan(plan))) return rc;
   if ((rc = check_ptrs({quads}))) return rc;
-  fw_quads_kernel<<<(plan->P + 3) / 4, 128, 0, (cudaStream_t)stream>>>(plan->L,
-                                                                       (double2*)quads);
+  fw_quads_kernel<<<(plan->P + 3) / 4, 128, 0, (cudaStream_t)stream>>>(
+      plan->L, (double2*)quads, plan->rootsP);
   FW_CK(cudaGetLastError());
   return S2B_OK;
 }
