@@ -547,19 +547,22 @@ __global__ void __launch_bounds__(512) fw_cols_fwd_adj_kernel(FWFftParams<Real> 
 //            reality: real output from n >= 0 (irfft: n = 0 real part, n > 0 doubled)
 //   forward: x[N-1+n][b][px] = sum_g f[b][g][px] e^{-2 pi i n g / G}, n in [n0, N-1]
 // (fourier_wigner.py:80-87 and 241-248). A table of the G roots e^{2 pi i j / G} sits in
-// shared memory; the exponent n g is reduced mod G exactly.
+// shared memory; the exponent n g is reduced mod G exactly. The sums run in the transform's
+// precision (at most 2N-1 < 24 terms).
 constexpr int kGamK = 8;
 
 template <typename Real, bool FWD>
 __global__ void fw_gamma_kernel(const void* in, void* out, int B, int N, long npix, int reality,
                                 double scale) {
   using R2 = typename C2<Real>::t;
-  extern __shared__ double2 roots[];
+  extern __shared__ __align__(16) unsigned char groots_raw[];
+  R2* const roots = reinterpret_cast<R2*>(groots_raw);
   const int G = 2 * N - 1;
   for (int j = threadIdx.x; j < G; j += blockDim.x) {
     double sn, cs;
     sincospi(2.0 * (double)j / (double)G, &sn, &cs);
-    roots[j] = make_double2(cs, sn);
+    roots[j].x = (Real)cs;
+    roots[j].y = (Real)sn;
   }
   __syncthreads();
   const long total = (long)B * npix;
@@ -571,21 +574,21 @@ __global__ void fw_gamma_kernel(const void* in, void* out, int B, int N, long np
       const R2* x = reinterpret_cast<const R2*>(in);
       {
         const int g0 = blockIdx.y * kGamK;
-        double re[kGamK], im[kGamK];
+        Real re[kGamK], im[kGamK];
 #pragma unroll
-        for (int u = 0; u < kGamK; ++u) re[u] = im[u] = 0.0;
+        for (int u = 0; u < kGamK; ++u) re[u] = im[u] = Real(0);
         for (int n = nlo; n < N; ++n) {
           const R2 v = x[((long)(N - 1 + n) * B + b) * npix + px];
-          double vr = v.x, vi = v.y;
+          Real vr = v.x, vi = v.y;
           if (reality) {
-            if (n == 0) vi = 0.0;
-            else { vr *= 2.0; vi *= 2.0; }
+            if (n == 0) vi = Real(0);
+            else { vr *= Real(2); vi *= Real(2); }
           }
           const int step = ((n % G) + G) % G;
           int r = (int)(((long)step * g0) % G);
 #pragma unroll
           for (int u = 0; u < kGamK; ++u) {
-            const double2 w = roots[r];
+            const R2 w = roots[r];
             re[u] += vr * w.x - vi * w.y;
             im[u] += vr * w.y + vi * w.x;
             r += step;
@@ -611,15 +614,15 @@ __global__ void fw_gamma_kernel(const void* in, void* out, int B, int N, long np
       R2* x = reinterpret_cast<R2*>(out);
       {
         const int n0 = nlo + (int)blockIdx.y * kGamK;
-        double re[kGamK], im[kGamK];
+        Real re[kGamK], im[kGamK];
 #pragma unroll
-        for (int u = 0; u < kGamK; ++u) re[u] = im[u] = 0.0;
+        for (int u = 0; u < kGamK; ++u) re[u] = im[u] = Real(0);
         for (int g = 0; g < G; ++g) {
-          double vr, vi;
+          Real vr, vi;
           const long o = (b * G + g) * npix + px;
           if (reality) {
             vr = reinterpret_cast<const Real*>(in)[o];
-            vi = 0.0;
+            vi = Real(0);
           } else {
             const R2 v = reinterpret_cast<const R2*>(in)[o];
             vr = v.x;
@@ -630,7 +633,7 @@ __global__ void fw_gamma_kernel(const void* in, void* out, int B, int N, long np
           int r = (int)(((long)step * (((n0 % G) + G) % G)) % G);
 #pragma unroll
           for (int u = 0; u < kGamK; ++u) {
-            const double2 w = roots[r];
+            const R2 w = roots[r];
             re[u] += vr * w.x - vi * w.y;
             im[u] += vr * w.y + vi * w.x;
             r += step;
