@@ -92,6 +92,7 @@ struct FWContractParams {
   const double* delta;  // [L][2L-1][2L-1]
   const void* in;       // INV: coefficients (slice layout fw_coef_slice); FWD: Gf [E][L][2L-1]
   void* out;            // INV: Y [E][2L-1][2L-1]; FWD: coefficients
+  const double2* thW;   // e^{i pi r / (2L-1)} at [r + L], |r| <= L (plan table)
   // adjoints: INV with adj writes the rows a >= 0 only, [E][L][2L-1], times (2pi)^2 and
   // i^(n-m) (the adjoint of the forward's last step); FWD with adj scales row l by c_l
   // without phase (the adjoint of the inverse's first step; the phases come from
@@ -264,9 +265,8 @@ __global__ void __launch_bounds__(kFwLanes) fw_contract_kernel(FWContractParams<
           Y[(long)(r + L - 1) * W + ci] = v;
           if (r > 0) Y[(long)(L - 1 - r) * W + ci] = (((m + n) & 1) ? cscale(v, Real(-1)) : v);
         } else {  // e^{+-i a pi / (2L-1)}
-          double sn, cs;
-          sincospi((double)r / (double)W, &sn, &cs);
-          const Real c = (Real)cs, sv = (Real)sn;
+          const double2 t = p.thW[r + L];
+          const Real c = (Real)t.x, sv = (Real)t.y;
           R2 u;
           u.x = v.x * c - v.y * sv;
           u.y = v.x * sv + v.y * c;
@@ -293,6 +293,7 @@ struct FWFftParams {
   FFTTables<Real> tb;
   const void* quads;  // complex128 [P]: the beta-convolution weights (quadsQ)
   const void* wconv;  // complex128 [4L-3]: w[k], k = -(2L-2) .. 2L-2
+  const double2* thW;  // e^{i pi r / (2L-1)} at [r + L], |r| <= L (plan table)
   const void* in;
   void* out;
 };
@@ -386,11 +387,10 @@ __global__ void __launch_bounds__(512) fw_cols_fwd_kernel(FWFftParams<Real> p, i
   for (int b = blo + (int)threadIdx.x; b <= L - 1; b += blockDim.x) {
     R2 v = cscale(dft_get<Real>(s, p.dphi, p.tb, false, pmod(b, nx)), inx);
     if (!p.mwss) {  // e^{-i b pi / (2L-1)}
-      double sn, cs;
-      sincospi(-(double)b / (double)W, &sn, &cs);
+      const double2 t = p.thW[L - b];  // e^{-i b pi / (2L-1)}
       const R2 u = v;
-      v.x = u.x * (Real)cs - u.y * (Real)sn;
-      v.y = u.x * (Real)sn + u.y * (Real)cs;
+      v.x = u.x * (Real)t.x - u.y * (Real)t.y;
+      v.y = u.x * (Real)t.y + u.y * (Real)t.x;
     }
     tmp[b - blo] = v;
   }
@@ -456,9 +456,8 @@ __global__ void __launch_bounds__(512) fw_cols_inv_adj_kernel(FWFftParams<Real> 
     R2 yp = dft_get<Real>(s, p.dphi, p.tb, false, a);
     R2 ym = a > 0 ? dft_get<Real>(s, p.dphi, p.tb, false, na - a) : czero<R2>();
     if (!p.mwss) {  // e^{-i a theta0} on Y[a], e^{+i a theta0} on Y[-a]
-      double sn, cs;
-      sincospi((double)a / (double)W, &sn, &cs);
-      const Real c = (Real)cs, sv = (Real)sn;
+      const double2 t = p.thW[a + L];
+      const Real c = (Real)t.x, sv = (Real)t.y;
       const R2 u = yp, v = ym;
       yp.x = u.x * c + u.y * sv;
       yp.y = u.y * c - u.x * sv;
@@ -516,11 +515,10 @@ __global__ void __launch_bounds__(512) fw_cols_fwd_adj_kernel(FWFftParams<Real> 
       x = cadd(x, cmul(Gf[(long)(L - 1) * W + col], cw));
     }
     if (!p.mwss) {  // conj(e^{-i v pi / (2L-1)})
-      double sn, cs;
-      sincospi((double)v / (double)W, &sn, &cs);
+      const double2 t = p.thW[v + L];
       const R2 u = x;
-      x.x = u.x * (Real)cs - u.y * (Real)sn;
-      x.y = u.x * (Real)sn + u.y * (Real)cs;
+      x.x = u.x * (Real)t.x - u.y * (Real)t.y;
+      x.y = u.x * (Real)t.y + u.y * (Real)t.x;
     }
     tmp[v - blo] = x;
   }
@@ -720,6 +718,16 @@ __global__ void fw_roots_kernel(int n, double2* roots) {
   }
 }
 
+// tab[i] = e^{i pi (i - L) / (2L-1)}, i in [0, 2L]: the MW theta0 phases of the column chains
+__global__ void fw_theta_phase_kernel(int L, double2* tab) {
+  const int W = 2 * L - 1;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= 2 * L; i += gridDim.x * blockDim.x) {
+    double sn, cs;
+    sincospi((double)(i - L) / (double)W, &sn, &cs);
+    tab[i] = make_double2(cs, sn);
+  }
+}
+
 // exponent index (a b) mod n (n > 0), for any signs of a and b
 __device__ __forceinline__ int fw_mulmod(long a, long b, int n) {
   return (int)(((a * b) % n + n) % n);
@@ -892,6 +900,7 @@ struct s2b_fw_plan {
   FFTSet fft;  // host[0]: length nphi, host[1]: length Q, host[2]: 2N-1 (gamma_fft)
   double2* rootsP = nullptr;  // e^{2 pi i r / P}, r in [0, P)
   double2* rootsQ = nullptr;  // e^{2 pi i r / Q}, r in [0, Q)
+  double2* thW = nullptr;     // e^{i pi r / (2L-1)} at [r + L], |r| <= L
   ~s2b_fw_plan() {
     for (void* a : allocs) cudaFree(a);
   }
@@ -963,6 +972,7 @@ FWFftParams<Real> fft_params(const s2b_fw_plan* p, int E, const FWSlices& sl) {
   f.dphi = p->fft.host[0];
   f.dP = p->fft.host[1];
   f.tb = tables<Real>(p);
+  f.thW = p->thW;
   return f;
 }
 
@@ -981,6 +991,7 @@ int contract(const s2b_fw_plan* p, bool fwd, int E, const FWSlices& sl, const do
              const void* in, void* out, cudaStream_t st, int adj = 0) {
   FWContractParams<Real> c{};
   c.adj = adj;
+  c.thW = p->thW;
   c.L = p->L;
   c.E = E;
   c.mwss = p->mwss;
@@ -1259,21 +1270,24 @@ int s2b_fw_plan_create(int L, int N, int sampling, int precision, s2b_fw_plan** 
   }
   // root tables of the quadrature weights (built once; the weights are recomputed from the
   // caller's quads on every forward call)
-  for (int t = 0; t < 2; ++t) {
-    const int n = t == 0 ? p->P : p->Q;
+  for (int t = 0; t < 3; ++t) {
+    const int n = t == 0 ? p->P : t == 1 ? p->Q : 2 * L + 1;
     void* d = nullptr;
     e = cudaMalloc(&d, (size_t)n * sizeof(double2));
     if (e == cudaSuccess) {
       p->allocs.push_back(d);
-      fw_roots_kernel<<<(n + 255) / 256, 256>>>(n, reinterpret_cast<double2*>(d));
+      if (t < 2)
+        fw_roots_kernel<<<(n + 255) / 256, 256>>>(n, reinterpret_cast<double2*>(d));
+      else
+        fw_theta_phase_kernel<<<(n + 255) / 256, 256>>>(L, reinterpret_cast<double2*>(d));
       e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
       delete p;
-      return fw_fail(S2B_ERR_CUDA, std::string("root tables: ") + cudaGetErrorString(e));
+      return fw_fail(S2B_ERR_CUDA, std::string("phase tables: ") + cudaGetErrorString(e));
     }
-    (t == 0 ? p->rootsP : p->rootsQ) = reinterpret_cast<double2*>(d);
+    (t == 0 ? p->rootsP : t == 1 ? p->rootsQ : p->thW) = reinterpret_cast<double2*>(d);
   }
   // the column chain keeps a DFT buffer and Q values in shared memory
   const size_t cs = p->fp64 ? 16 : 8;
