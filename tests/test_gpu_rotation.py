@@ -141,3 +141,17 @@ def test_rotation_batch_tensor_core_path(s2b, rng):
     for k in range(2):
         one = s2b.rotation.rotate_flms(flm[k], L, rot)
         assert torch.equal(one, r[k])
+
+
+def test_rotation_f32_tensor_core_path(s2b, rng):
+    """complex64 maps on the tensor-core kernel (L = 1024) against the float64 rotation."""
+    import torch
+
+    L = 1024
+    rot = (0.2, 2.4, -1.7)
+    flm = torch.from_numpy(oracle.signal.generate_flm(rng, L, 0, 0, False)).cuda()
+    r64 = s2b.rotation.rotate_flms(flm, L, rot)
+    r32 = s2b.rotation.rotate_flms(flm.to(torch.complex64), L, rot)
+    assert r32.dtype == torch.complex64
+    err = float((r32.to(torch.complex128) - r64).abs().max() / r64.abs().max())
+    assert err < 1e-6, err
