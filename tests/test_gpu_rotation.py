@@ -155,3 +155,14 @@ def test_rotation_f32_tensor_core_path(s2b, rng):
     assert r32.dtype == torch.complex64
     err = float((r32.to(torch.complex128) - r64).abs().max() / r64.abs().max())
     assert err < 1e-6, err
+
+
+def test_rotation_against_oracle_L256(s2b, rng):
+    """The device rotation at L = 256 (shuffle kernel, two orders per tile) against the
+    oracle's Risbo-based rotation of the same map."""
+    L = 256
+    rot = (1.1, 2.3, -0.4)
+    flm = oracle.signal.generate_flm(rng, L, 0, 0, False)
+    ref = oracle.rotation.rotate_flms(flm, L, rot)
+    r = s2b.rotation.rotate_flms(flm, L, rot)
+    assert relerr(r, ref) < 1e-12, relerr(r, ref)
