@@ -112,12 +112,12 @@ def test_rotation_f32_batch(s2b, rng):
     assert np.array_equal(one, r32[2])
 
 
-def test_rotation_planes_two_n_per_lane(s2b, rng):
-    """Planes at L = 1040 (36 GB; two n per lane, natural n order) passed back as dl_array
-    give the rotation computed without them."""
+@pytest.mark.parametrize("L", [512, 1040])
+def test_rotation_planes_passed_back(s2b, rng, L):
+    """Planes passed back as dl_array give the rotation computed without them: L = 512 (four
+    orders per tile in CTAs of four warps) and L = 1040 (36 GB; two n per lane)."""
     import torch
 
-    L = 1040
     rot = (0.9, 1.3, -0.6)
     flm = torch.from_numpy(oracle.signal.generate_flm(rng, L, 0, 0, False)).cuda()
     dl = s2b.rotation.generate_rotate_dls(L, rot[1])
