@@ -183,10 +183,17 @@ __global__ void rotate_start_carry_kernel(RotParams p) {
   if (ai >= NN) return;
   RotXD c = xd_make(1.0);
 #pragma unroll 1
-  for (int g = 0; g < G; ++g) {
-    const RotXD t = p.carry[(size_t)g * NN + ai];
-    p.carry[(size_t)g * NN + ai] = c;
-    c = xd_mul(c, t);
+  for (int g0 = 0; g0 < G; g0 += 8) {  // eight segment products in flight at a time
+    RotXD t[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (g0 + u < G) t[u] = p.carry[(size_t)(g0 + u) * NN + ai];
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (g0 + u < G) {
+        p.carry[(size_t)(g0 + u) * NN + ai] = c;
+        c = xd_mul(c, t[u]);
+      }
   }
 }
 
