@@ -96,6 +96,18 @@ __global__ void __launch_bounds__(256) prologue_tiled_kernel(StageParams p) {
   const int half = (int)(blockIdx.z % p.nhalf), b = (int)(blockIdx.z / p.nhalf);
   const int tx = threadIdx.x, ty = threadIdx.y;
   const R2* flm = reinterpret_cast<const R2*>(p.flm) + (size_t)b * L * (2 * L - 1);
+  // a thread keeps one l in the second pass: its four weights are loaded here, beside the
+  // coefficients, so that both wait on memory together
+  const int as = p.spin < 0 ? -p.spin : p.spin;
+  const int lt = 32 * j + tx;
+  double gk[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int m = m0 + ty + 8 * k;
+    const bool ok = m >= 0 && m < L && lt < L && lt >= m && lt >= p.L0 && lt >= as;
+    gk[k] = ok ? p.g[(size_t)m * L + lt] : 0.0;
+  }
+#pragma unroll
   for (int qq = ty; qq < 32; qq += 8) {
     const int l = 32 * j + qq, m = m0 + tx;
     R2 a, c;
@@ -109,13 +121,14 @@ __global__ void __launch_bounds__(256) prologue_tiled_kernel(StageParams p) {
     tc[qq][tx] = c;
   }
   __syncthreads();
-  const int as = p.spin < 0 ? -p.spin : p.spin;
   const double sgn_s = (p.spin & 1) ? -1.0 : 1.0;
-  for (int mm = ty; mm < 32; mm += 8) {
-    const int m = m0 + mm, mrow = m + kPadLo, l = 32 * j + tx;
+  const double nl = lnorm(lt);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int mm = ty + 8 * k;
+    const int m = m0 + mm, mrow = m + kPadLo;
     if (mrow >= TR) continue;
-    const bool ok = m >= 0 && m < L && l < L && l >= m && l >= p.L0 && l >= as;
-    const double g = ok ? p.g[(size_t)m * L + l] * lnorm(l) : 0.0;
+    const double g = gk[k] * nl;
     const double sgn_m = (m & 1) ? -1.0 : 1.0;
     const size_t idx = ((((size_t)b * p.nhalf + half) * C + j) * TR + mrow) * 32 + tx;
     if (p.dual) {
@@ -183,7 +196,6 @@ __global__ void poles_kernel(StageParams p) {
 template <typename Real>
 __device__ __forceinline__ R2_t<Real> spectrum_at(const StageParams& p, int b, int row, int m) {
   using R2 = R2_t<Real>;
-  const int L = p.L;
   const int am = m < 0 ? -m : m;
   const R2* G = reinterpret_cast<const R2*>(p.G);
   const size_t mr = (size_t)(am + kPadLo);
@@ -196,51 +208,62 @@ __device__ __forceinline__ R2_t<Real> spectrum_at(const StageParams& p, int b, i
   return z;
 }
 
-// flm[b][l][L-1+m] from the projected sums acc [b][half][j][m][q] (one element).
+// The loads behind one flm[b][l][L-1+m]: the projected sum at (|m|, l) of the half that
+// holds m, and the projection weight g[|m|][l]; ok is false outside l >= max(|s|, L0),
+// |m| <= l (the value is zero there), mirror marks a reality -m taken from +m.
+struct EpiCell {
+  double ar, ai, g;
+  bool ok, mirror;
+};
+
 template <typename Real>
-__device__ __forceinline__ R2_t<Real> epi_value(const StageParams& p, int b, int l, int m) {
+__device__ __forceinline__ EpiCell epi_fetch(const StageParams& p, int b, int l, int m) {
   using R2 = R2_t<Real>;
   const int L = p.L, C = p.nclass, Q = p.Q;
   const int as = p.spin < 0 ? -p.spin : p.spin;
   const int lmin = as > p.L0 ? as : p.L0;
-  const double sgn_s = (p.spin & 1) ? -1.0 : 1.0;
   const int am = m < 0 ? -m : m;
-  double re = 0.0, im = 0.0;
-  if (l >= lmin && am <= l) {
+  EpiCell e;
+  e.ar = e.ai = e.g = 0.0;
+  e.ok = l >= lmin && am <= l;
+  e.mirror = !p.dual && m < 0 && p.nhalf <= 1;
+  if (e.ok) {
     const int j = l % C, q = l / C;
     // offset of (m, l) in one [batch][half] slice of the forward sums, in R2/R4 units
     const size_t cell = p.Lp > 0 ? (size_t)am * p.Lp + l : ((size_t)j * L + am) * Q + q;
     const size_t slice = p.Lp > 0 ? (size_t)L * p.Lp : (size_t)C * L * Q;
-    const double g = p.g[(size_t)am * L + l];
-    double ar = 0.0, ai = 0.0;
-    bool conj_mirror = false;
-    if (p.dual) {
-      const R2* A = reinterpret_cast<const R2*>(p.acc);
-      const R2 a = A[((size_t)b * slice + cell) * 2 + (m < 0 ? 1 : 0)];
-      ar = a.x;
-      ai = a.y;
-    } else if (m >= 0 || p.nhalf > 1) {
-      const int half = m >= 0 ? 0 : 1;
-      const R2* A = reinterpret_cast<const R2*>(p.acc);
-      const R2 a = A[((size_t)b * p.nhalf + half) * slice + cell];
-      ar = a.x;
-      ai = a.y;
-    } else {
-      // reality: flm[l, -m] = (-1)^m conj(flm[l, m])
-      const R2* A = reinterpret_cast<const R2*>(p.acc);
-      const R2 a = A[(size_t)b * slice + cell];
-      ar = a.x;
-      ai = a.y;
-      conj_mirror = true;
-    }
+    const R2* A = reinterpret_cast<const R2*>(p.acc);
+    size_t at;
+    if (p.dual)
+      at = ((size_t)b * slice + cell) * 2 + (m < 0 ? 1 : 0);
+    else if (!e.mirror)
+      at = ((size_t)b * p.nhalf + (m >= 0 ? 0 : 1)) * slice + cell;
+    else  // reality: flm[l, -m] = (-1)^m conj(flm[l, m])
+      at = (size_t)b * slice + cell;
+    const R2 a = A[at];
+    e.ar = a.x;
+    e.ai = a.y;
+    e.g = p.g[(size_t)am * L + l];
+  }
+  return e;
+}
+
+// flm[b][l][L-1+m] from its fetched cell; nl = N_l (-1)^s, the degree's normalisation.
+template <typename Real>
+__device__ __forceinline__ R2_t<Real> epi_finish(const StageParams& p, int b, int l, int m,
+                                                 const EpiCell& e, double nl) {
+  using R2 = R2_t<Real>;
+  const int am = m < 0 ? -m : m;
+  double re = 0.0, im = 0.0;
+  if (e.ok) {
     // d-projection with the m < 0 symmetry sign (-1)^(m+s) (spin folded below)
-    double f = g;
-    if (m < 0 && !conj_mirror) f *= ((am + p.spin) % 2 + 2) % 2 ? -1.0 : 1.0;
-    re = f * ar;
-    im = f * ai;
+    double f = e.g;
+    if (m < 0 && !e.mirror) f *= ((am + p.spin) % 2 + 2) % 2 ? -1.0 : 1.0;
+    re = f * e.ar;
+    im = f * e.ai;
     // closed-form pole rings (each present pole: theta = pi contributes at m = s, theta = 0 at
     // m = -s)
-    if (!conj_mirror) {
+    if (!e.mirror) {
       if (p.pole_south >= 0 && m == p.spin) {
         const R2 s = spectrum_at<Real>(p, b, p.pole_south, m);
         const double sg = ((l - p.spin) % 2 + 2) % 2 ? -1.0 : 1.0;
@@ -253,10 +276,9 @@ __device__ __forceinline__ R2_t<Real> epi_value(const StageParams& p, int b, int
         im += s.y;
       }
     }
-    const double nl = lnorm(l) * sgn_s;
     re *= nl;
     im *= nl;
-    if (conj_mirror) {
+    if (e.mirror) {
       // value above is flm[l, |m|]; mirror (-1)^m conj(.)
       const double sm = (am & 1) ? -1.0 : 1.0;
       im = -im;
@@ -268,6 +290,16 @@ __device__ __forceinline__ R2_t<Real> epi_value(const StageParams& p, int b, int
   o.x = (Real)re;
   o.y = (Real)im;
   return o;
+}
+
+__device__ __forceinline__ double epi_norm(const StageParams& p, int l) {
+  return lnorm(l) * ((p.spin & 1) ? -1.0 : 1.0);
+}
+
+// flm[b][l][L-1+m] from the projected sums acc [b][half][j][m][q] (one element).
+template <typename Real>
+__device__ __forceinline__ R2_t<Real> epi_value(const StageParams& p, int b, int l, int m) {
+  return epi_finish<Real>(p, b, l, m, epi_fetch<Real>(p, b, l, m), epi_norm(p, l));
 }
 
 // flm [b][l][L-1+m] from the projected sums, one element per thread (any layout).
@@ -297,13 +329,22 @@ __global__ void __launch_bounds__(256) epilogue_tiled_kernel(StageParams p) {
   const int L = p.L, W = 2 * L - 1;
   const int c0 = blockIdx.x * 32, l0 = blockIdx.y * 32, b = blockIdx.z;
   const int tx = threadIdx.x, ty = threadIdx.y;
-  for (int cc = ty; cc < 32; cc += 8) {
-    const int c = c0 + cc, l = l0 + tx;
-    R2 v;
-    v.x = 0;
-    v.y = 0;
-    if (c < W && l < L) v = epi_value<Real>(p, b, l, c - (L - 1));
-    tile[cc][tx] = v;
+  // a thread keeps one l: all four cells' loads are issued before any is used, and the
+  // degree's normalisation is computed once
+  const int l = l0 + tx;
+  EpiCell e[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int c = c0 + ty + 8 * k;
+    e[k].ok = false;
+    e[k].mirror = false;
+    if (c < W && l < L) e[k] = epi_fetch<Real>(p, b, l, c - (L - 1));
+  }
+  const double nl = epi_norm(p, l);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int c = c0 + ty + 8 * k;
+    tile[ty + 8 * k][tx] = epi_finish<Real>(p, b, l, c - (L - 1), e[k], nl);
   }
   __syncthreads();
   R2* out = reinterpret_cast<R2*>(p.flm_out) + (size_t)b * L * W;
