@@ -1220,7 +1220,6 @@ static int inv_stage_pre(s2b_plan* p, const void* flm, char* ws, cudaStream_t s,
   sp.Q = kFwdBlock;
   sp.Lp = p->fwd_NB * kFwdBlock;
   S2B_CK(launch_prologue(p->fp64, sp, s));
-  S2B_CK(launch_poles(p->fp64, sp, s));
   out->nrings = 0;
   if (p->inv_nrings > 0) {
     Inv2Params lp{};
@@ -1501,7 +1500,6 @@ static int run_forward_adjoint(s2b_plan* p, const void* gflm, void* gf, char* ws
   sp.F = F;
   sp.ftm = y;
   S2B_CK(launch_prologue(p->fp64, sp, s));
-  S2B_CK(launch_poles(p->fp64, sp, s));
   Inv2Params lp{};
   lp.L = L;
   lp.nrings = p->fwd_nrings;

@@ -21,10 +21,11 @@ struct StageParams {
   const void* G;        // forward weighted spectra
   const void* acc;      // forward projected sums
   void* flm_out;        // forward output
+  int pole_blocks;      // set by launch_prologue: the pole rows ride on the prologue's grid
 };
 
+// the inverse coefficient table and the closed-form pole rows (pole_south / pole_north)
 cudaError_t launch_prologue(bool fp64, const StageParams& p, cudaStream_t s);
-cudaError_t launch_poles(bool fp64, const StageParams& p, cudaStream_t s);
 cudaError_t launch_epilogue(bool fp64, const StageParams& p, cudaStream_t s);
 cudaError_t launch_axpy(bool fp64, long n, double a, const void* x, void* y, cudaStream_t s);
 cudaError_t launch_sub(bool fp64, long n, const void* x, const void* y, void* z, cudaStream_t s);

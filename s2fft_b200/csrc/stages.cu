@@ -82,10 +82,59 @@ __global__ void prologue_kernel(StageParams p) {
   }
 }
 
+// Pole rows of the inverse: ftm[pole][L-1+ms+mo] = (-1)^s sum_l sign_l N_l flm[l][L-1+ms],
+// south (theta = pi): ms = s, sign_l = (-1)^(l-s); north (theta = 0): ms = -s, sign 1.
+// One CTA of 256 threads per (pole, map); red holds 2 x 256 doubles of shared memory.
+template <typename Real>
+__device__ __forceinline__ void poles_block(const StageParams& p, int which, int b, int tid,
+                                            double* red) {
+  using R2 = R2_t<Real>;
+  const int L = p.L;
+  const int row = which == 0 ? p.pole_south : p.pole_north;
+  if (row < 0) return;
+  const int ms = which == 0 ? p.spin : -p.spin;
+  const R2* flm = reinterpret_cast<const R2*>(p.flm) + (size_t)b * L * (2 * L - 1);
+  double sx = 0.0, sy = 0.0;
+#pragma unroll 1
+  for (int l = p.L0 + tid; l < L; l += 256) {
+    double f = lnorm(l);
+    if (which == 0 && (((l - p.spin) % 2 + 2) % 2)) f = -f;
+    const R2 a = flm[(size_t)l * (2 * L - 1) + L - 1 + ms];
+    sx += f * a.x;
+    sy += f * a.y;
+  }
+  red[tid] = sx;
+  red[256 + tid] = sy;
+  __syncthreads();
+  for (int st = 128; st > 0; st >>= 1) {
+    if (tid < st) {
+      red[tid] += red[tid + st];
+      red[256 + tid] += red[256 + tid + st];
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    const double sg = (p.spin & 1) ? -1.0 : 1.0;
+    R2 o;
+    o.x = (Real)(sg * red[0]);
+    o.y = (Real)(sg * red[256]);
+    R2* ftm = reinterpret_cast<R2*>(p.ftm) + ((size_t)b * p.nrows + row) * p.ncol;
+    ftm[L - 1 + ms + p.mo] = o;
+  }
+}
+
+// grid (2, batch), 256 threads
+template <typename Real>
+__global__ void __launch_bounds__(256) poles_kernel(StageParams p) {
+  __shared__ double red[2 * 256];
+  poles_block<Real>(p, blockIdx.x, blockIdx.y, threadIdx.x, red);
+}
+
 // Blocked layout (p.Lp > 0, Q = 32): the same table, a 32 (m) x 32 (l) tile per CTA through
 // shared memory, since flm is [l][m] and F is [m][l]: the coefficients are read with
 // consecutive threads on consecutive m, the table (and g) with consecutive threads on
-// consecutive l. grid (ceil(TR / 32), C, batch * nhalf), 32 x 8 threads.
+// consecutive l. grid (ceil(TR / 32) + pole_blocks, C, batch * nhalf), 32 x 8 threads; with
+// pole_blocks the last column of CTAs computes the pole rows instead (y = 0 south, 1 north).
 template <typename Real>
 __global__ void __launch_bounds__(256) prologue_tiled_kernel(StageParams p) {
   using R2 = R2_t<Real>;
@@ -95,6 +144,11 @@ __global__ void __launch_bounds__(256) prologue_tiled_kernel(StageParams p) {
   const int m0 = (int)blockIdx.x * 32 - kPadLo, j = blockIdx.y;
   const int half = (int)(blockIdx.z % p.nhalf), b = (int)(blockIdx.z / p.nhalf);
   const int tx = threadIdx.x, ty = threadIdx.y;
+  if (p.pole_blocks && blockIdx.x == gridDim.x - 1) {
+    static_assert(sizeof(ta) >= 2 * 256 * sizeof(double), "pole reduction fits the tile");
+    if (j < 2 && half == 0) poles_block<Real>(p, j, b, ty * 32 + tx, reinterpret_cast<double*>(&ta[0][0]));
+    return;
+  }
   const R2* flm = reinterpret_cast<const R2*>(p.flm) + (size_t)b * L * (2 * L - 1);
   // a thread keeps one l in the second pass: its four weights are loaded here, beside the
   // coefficients, so that both wait on memory together
@@ -148,47 +202,6 @@ __global__ void __launch_bounds__(256) prologue_tiled_kernel(StageParams p) {
       o.y = (Real)(f * a.y);
       reinterpret_cast<R2*>(p.F)[idx] = o;
     }
-  }
-}
-
-// Pole rows of the inverse: ftm[pole][L-1+ms+mo] = (-1)^s sum_l sign_l N_l flm[l][L-1+ms],
-// south (theta = pi): ms = s, sign_l = (-1)^(l-s); north (theta = 0): ms = -s, sign 1.
-template <typename Real>
-__global__ void poles_kernel(StageParams p) {
-  using R2 = R2_t<Real>;
-  const int L = p.L;
-  const int b = blockIdx.y;
-  const int which = blockIdx.x;  // 0 south, 1 north
-  const int row = which == 0 ? p.pole_south : p.pole_north;
-  if (row < 0) return;
-  const int ms = which == 0 ? p.spin : -p.spin;
-  const R2* flm = reinterpret_cast<const R2*>(p.flm) + (size_t)b * L * (2 * L - 1);
-  double sx = 0.0, sy = 0.0;
-  for (int l = p.L0 + threadIdx.x; l < L; l += blockDim.x) {
-    double f = lnorm(l);
-    if (which == 0 && (((l - p.spin) % 2 + 2) % 2)) f = -f;
-    const R2 a = flm[(size_t)l * (2 * L - 1) + L - 1 + ms];
-    sx += f * a.x;
-    sy += f * a.y;
-  }
-  __shared__ double red[2][256];
-  red[0][threadIdx.x] = sx;
-  red[1][threadIdx.x] = sy;
-  __syncthreads();
-  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
-    if (threadIdx.x < st) {
-      red[0][threadIdx.x] += red[0][threadIdx.x + st];
-      red[1][threadIdx.x] += red[1][threadIdx.x + st];
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    const double sg = (p.spin & 1) ? -1.0 : 1.0;
-    R2 o;
-    o.x = (Real)(sg * red[0][0]);
-    o.y = (Real)(sg * red[1][0]);
-    R2* ftm = reinterpret_cast<R2*>(p.ftm) + ((size_t)b * p.nrows + row) * p.ncol;
-    ftm[L - 1 + ms + p.mo] = o;
   }
 }
 
@@ -385,14 +398,29 @@ static int grid_for(long n) {
 // 65535 x 256 beyond the end) stays below 2^32.
 static bool fits32(long n) { return n + 65535L * 256 < (1L << 32); }
 
+static cudaError_t launch_poles(bool fp64, const StageParams& p, cudaStream_t s) {
+  if (p.pole_south < 0 && p.pole_north < 0) return cudaSuccess;
+  if (fp64)
+    poles_kernel<double><<<dim3(2, p.batch), 256, 0, s>>>(p);
+  else
+    poles_kernel<float><<<dim3(2, p.batch), 256, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_prologue(bool fp64, const StageParams& p, cudaStream_t s) {
   if (p.Lp > 0 && p.Q == 32 && (long)p.batch * p.nhalf <= 65535 && p.nclass <= 65535) {
-    const dim3 grid((p.TR + 31) / 32, p.nclass, p.batch * p.nhalf);
+    StageParams q = p;
+    const bool poles = p.pole_south >= 0 || p.pole_north >= 0;
+    // the pole rows ride on one extra column of CTAs when there are two classes for them
+    q.pole_blocks = poles && p.nclass >= 2 ? 1 : 0;
+    const dim3 grid((p.TR + 31) / 32 + q.pole_blocks, p.nclass, p.batch * p.nhalf);
     if (fp64)
-      prologue_tiled_kernel<double><<<grid, dim3(32, 8), 0, s>>>(p);
+      prologue_tiled_kernel<double><<<grid, dim3(32, 8), 0, s>>>(q);
     else
-      prologue_tiled_kernel<float><<<grid, dim3(32, 8), 0, s>>>(p);
-    return cudaGetLastError();
+      prologue_tiled_kernel<float><<<grid, dim3(32, 8), 0, s>>>(q);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && poles && !q.pole_blocks) e = launch_poles(fp64, p, s);
+    return e;
   }
   const long total = (long)p.batch * p.nhalf * p.nclass * p.TR * p.Q;
   const bool i32 = fits32(total);
@@ -404,16 +432,9 @@ cudaError_t launch_prologue(bool fp64, const StageParams& p, cudaStream_t s) {
     prologue_kernel<float, uint32_t><<<grid_for(total), 256, 0, s>>>(p);
   else
     prologue_kernel<float, uint64_t><<<grid_for(total), 256, 0, s>>>(p);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_poles(bool fp64, const StageParams& p, cudaStream_t s) {
-  if (p.pole_south < 0 && p.pole_north < 0) return cudaSuccess;
-  if (fp64)
-    poles_kernel<double><<<dim3(2, p.batch), 256, 0, s>>>(p);
-  else
-    poles_kernel<float><<<dim3(2, p.batch), 256, 0, s>>>(p);
-  return cudaGetLastError();
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = launch_poles(fp64, p, s);
+  return e;
 }
 
 cudaError_t launch_epilogue(bool fp64, const StageParams& p, cudaStream_t s) {
