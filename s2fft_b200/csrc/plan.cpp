@@ -1194,8 +1194,8 @@ static int inv_stage_pre(s2b_plan* p, const void* flm, char* ws, cudaStream_t s,
   const int L = d.L;
   void* F = ws;
   void* ftm = ws + align256(p->ws_inv_F);
-  S2B_CK(cudaMemsetAsync(ftm, 0, p->ws_inv_ftm, s));
   StageParams sp{};
+  sp.ftm_zero_bytes = p->ws_inv_ftm;
   sp.L = L;
   sp.L0 = d.L_lower;
   sp.spin = d.spin;
@@ -1478,8 +1478,8 @@ static int run_forward_adjoint(s2b_plan* p, const void* gflm, void* gf, char* ws
   char* F = ws;
   char* y = F + align256(p->ws_inv_F);
   char* ftm2 = y + align256(p->ws_adj_y);
-  S2B_CK(cudaMemsetAsync(y, 0, p->ws_adj_y, s));
   StageParams sp{};
+  sp.ftm_zero_bytes = p->ws_adj_y;
   sp.L = L;
   sp.L0 = d.L_lower;
   sp.spin = d.spin;
@@ -1568,8 +1568,14 @@ static int fwd_stage_pre(s2b_plan* p, const void* f, char* ws, cudaStream_t s, F
   char* G = cols + align256(p->ws_fwd_cols);
   char* acc = G + align256(p->ws_fwd_G);
   char* G2 = acc + align256(p->ws_fwd_acc);
-  S2B_CK(cudaMemsetAsync(acc, 0, p->ws_fwd_acc, s));
   RowsParams<Real> rp{};
+  // the ring transforms clear the accumulators (a whole number of 16-byte units)
+  if (p->ws_fwd_acc % 16 == 0) {
+    rp.zero = acc;
+    rp.zero16 = (long)(p->ws_fwd_acc / 16);
+  } else {
+    S2B_CK(cudaMemsetAsync(acc, 0, p->ws_fwd_acc, s));
+  }
   rp.L = L;
   rp.nrows = p->fwd_mode ? p->nth : p->fwd_nrows;
   rp.mo = p->fwd_mode == 2 ? 1 : 0;

@@ -292,6 +292,12 @@ __global__ void __launch_bounds__(LOGM ? (1 << LOGM) / 16 : 512, reg_min_blocks<
   R2* s = reinterpret_cast<R2*>(smem_raw);
   const int t = blockIdx.x;
   const int b = blockIdx.y;
+  if (p.zero) {
+    // the latitudinal kernel's accumulators, cleared here instead of by a memset of their own
+    const long nth = (long)gridDim.x * gridDim.y * blockDim.x;
+    for (long i = ((long)b * gridDim.x + t) * blockDim.x + threadIdx.x; i < p.zero16; i += nth)
+      reinterpret_cast<float4*>(p.zero)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
   const FFTDesc d = p.desc[p.ring_desc ? p.ring_desc[t] : 0];
   const int n = d.n;
   const int L = p.L;

@@ -64,6 +64,8 @@ struct RowsParams {
   FFTTables<Real> tb;
   const void* in;
   void* out;
+  void* zero;           // forward: a buffer the CTAs clear beside the transforms (nullptr: none)
+  long zero16;          // its size in 16-byte units
 };
 
 // MW / MWSS forward resampling chain, one CTA per (m column, map).

@@ -21,7 +21,9 @@ struct StageParams {
   const void* G;        // forward weighted spectra
   const void* acc;      // forward projected sums
   void* flm_out;        // forward output
+  size_t ftm_zero_bytes;  // > 0: launch_prologue zeroes that many bytes of ftm first
   int pole_blocks;      // set by launch_prologue: the pole rows ride on the prologue's grid
+  int zero_ftm;         // set by launch_prologue: the prologue's CTAs zero ftm themselves
 };
 
 // the inverse coefficient table and the closed-form pole rows (pole_south / pole_north)

@@ -94,6 +94,13 @@ __device__ __forceinline__ void poles_block(const StageParams& p, int which, int
   if (row < 0) return;
   const int ms = which == 0 ? p.spin : -p.spin;
   const R2* flm = reinterpret_cast<const R2*>(p.flm) + (size_t)b * L * (2 * L - 1);
+  R2* ftm = reinterpret_cast<R2*>(p.ftm) + ((size_t)b * p.nrows + row) * p.ncol;
+  if (p.zero_ftm) {
+    // the pole row is this CTA's to clear; the reduction's barriers order it before the store
+    R2 z;
+    z.x = z.y = 0;
+    for (int c = tid; c < p.ncol; c += 256) ftm[c] = z;
+  }
   double sx = 0.0, sy = 0.0;
 #pragma unroll 1
   for (int l = p.L0 + tid; l < L; l += 256) {
@@ -118,7 +125,6 @@ __device__ __forceinline__ void poles_block(const StageParams& p, int which, int
     R2 o;
     o.x = (Real)(sg * red[0]);
     o.y = (Real)(sg * red[256]);
-    R2* ftm = reinterpret_cast<R2*>(p.ftm) + ((size_t)b * p.nrows + row) * p.ncol;
     ftm[L - 1 + ms + p.mo] = o;
   }
 }
@@ -130,11 +136,30 @@ __global__ void __launch_bounds__(256) poles_kernel(StageParams p) {
   poles_block<Real>(p, blockIdx.x, blockIdx.y, threadIdx.x, red);
 }
 
+// Zeroes ftm [batch][nrows][ncol] before the latitudinal kernel accumulates into it, in units
+// of 256 entries of one row spread over the prologue's tile CTAs (cta of ncta); with
+// pole_blocks the pole rows are left to their pole CTAs.
+template <typename Real>
+__device__ __forceinline__ void zero_ftm_rows(const StageParams& p, int cta, int ncta, int tid) {
+  using R2 = R2_t<Real>;
+  const int nseg = (p.ncol + 255) / 256;
+  const int units = p.batch * p.nrows * nseg;  // below 2^31 (launch_prologue)
+  R2 z;
+  z.x = z.y = 0;
+  for (int u = cta; u < units; u += ncta) {
+    const int rg = u / nseg, c = (u - rg * nseg) * 256 + tid;
+    const int row = rg % p.nrows;
+    if (p.pole_blocks && (row == p.pole_south || row == p.pole_north)) continue;
+    if (c < p.ncol) reinterpret_cast<R2*>(p.ftm)[(size_t)rg * p.ncol + c] = z;
+  }
+}
+
 // Blocked layout (p.Lp > 0, Q = 32): the same table, a 32 (m) x 32 (l) tile per CTA through
 // shared memory, since flm is [l][m] and F is [m][l]: the coefficients are read with
 // consecutive threads on consecutive m, the table (and g) with consecutive threads on
 // consecutive l. grid (ceil(TR / 32) + pole_blocks, C, batch * nhalf), 32 x 8 threads; with
-// pole_blocks the last column of CTAs computes the pole rows instead (y = 0 south, 1 north).
+// pole_blocks the last column of CTAs computes the pole rows instead (y = 0 south, 1 north),
+// with zero_ftm the tile CTAs also clear ftm.
 template <typename Real>
 __global__ void __launch_bounds__(256) prologue_tiled_kernel(StageParams p) {
   using R2 = R2_t<Real>;
@@ -148,6 +173,11 @@ __global__ void __launch_bounds__(256) prologue_tiled_kernel(StageParams p) {
     static_assert(sizeof(ta) >= 2 * 256 * sizeof(double), "pole reduction fits the tile");
     if (j < 2 && half == 0) poles_block<Real>(p, j, b, ty * 32 + tx, reinterpret_cast<double*>(&ta[0][0]));
     return;
+  }
+  if (p.zero_ftm) {
+    const int gx = (int)gridDim.x - p.pole_blocks;
+    zero_ftm_rows<Real>(p, (int)blockIdx.x + gx * (j + (int)gridDim.y * (int)blockIdx.z),
+                        gx * (int)gridDim.y * (int)gridDim.z, ty * 32 + tx);
   }
   const R2* flm = reinterpret_cast<const R2*>(p.flm) + (size_t)b * L * (2 * L - 1);
   // a thread keeps one l in the second pass: its four weights are loaded here, beside the
@@ -413,6 +443,14 @@ cudaError_t launch_prologue(bool fp64, const StageParams& p, cudaStream_t s) {
     const bool poles = p.pole_south >= 0 || p.pole_north >= 0;
     // the pole rows ride on one extra column of CTAs when there are two classes for them
     q.pole_blocks = poles && p.nclass >= 2 ? 1 : 0;
+    // ftm is cleared by the same CTAs when it is exactly the [batch][nrows][ncol] table
+    const long units = (long)p.batch * p.nrows * ((p.ncol + 255) / 256);
+    q.zero_ftm = p.ftm_zero_bytes > 0 && units < (1L << 31) &&
+                 p.ftm_zero_bytes == (size_t)p.batch * p.nrows * p.ncol * (fp64 ? 16 : 8);
+    if (p.ftm_zero_bytes > 0 && !q.zero_ftm) {
+      const cudaError_t e = cudaMemsetAsync(p.ftm, 0, p.ftm_zero_bytes, s);
+      if (e != cudaSuccess) return e;
+    }
     const dim3 grid((p.TR + 31) / 32 + q.pole_blocks, p.nclass, p.batch * p.nhalf);
     if (fp64)
       prologue_tiled_kernel<double><<<grid, dim3(32, 8), 0, s>>>(q);
@@ -421,6 +459,10 @@ cudaError_t launch_prologue(bool fp64, const StageParams& p, cudaStream_t s) {
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess && poles && !q.pole_blocks) e = launch_poles(fp64, p, s);
     return e;
+  }
+  if (p.ftm_zero_bytes > 0) {
+    const cudaError_t e = cudaMemsetAsync(p.ftm, 0, p.ftm_zero_bytes, s);
+    if (e != cudaSuccess) return e;
   }
   const long total = (long)p.batch * p.nhalf * p.nclass * p.TR * p.Q;
   const bool i32 = fits32(total);
