@@ -525,6 +525,7 @@ __device__ __forceinline__ bool lat_fwd2_tile(const Fwd2Params& p, int bx, int b
 
 template <typename Real, bool DUAL, int T, int W, int R, int SYM>
 __global__ void __launch_bounds__(W * 32, 3) lat_fwd2_kernel(const Fwd2Params p) {
+  chain_enter();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   bool live = false;
   lat_fwd2_tile<Real, DUAL, T, W, R, SYM>(p, (int)blockIdx.x, (int)blockIdx.y,
@@ -565,8 +566,7 @@ static cudaError_t launch_fwd2_cfg(const Fwd2Params& p, cudaStream_t s) {
   if (err != cudaSuccess) return err;
   const int ntiles = (p.nrings + Lay::NRT - 1) / Lay::NRT;
   dim3 grid(ntiles, (p.NB / 2) * (p.Mst1 ? p.nseg : 1), p.nhalf * p.batch);
-  kern<<<grid, Lay::NT, Lay::total, s>>>(p);
-  return cudaGetLastError();
+  return launch_chained(kern, grid, dim3(Lay::NT), Lay::total, s, p);
 }
 
 template <typename Real, int T, int R, int SYM>

@@ -390,6 +390,7 @@ __device__ __forceinline__ bool lat_inv2_tile(const Inv2Params& p, int bx, int b
 
 template <typename Real, bool DUAL, int T, int W, int R, bool VST, bool SYM>
 __global__ void __launch_bounds__(W * 32, 3) lat_inv2_kernel(const Inv2Params p) {
+  chain_enter();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   bool live = false;
   lat_inv2_tile<Real, DUAL, T, W, R, VST, SYM>(p, (int)blockIdx.x, (int)blockIdx.y,
@@ -432,8 +433,7 @@ static cudaError_t launch_inv2_cfg(const Inv2Params& p, cudaStream_t s) {
   if (err != cudaSuccess) return err;
   dim3 grid((p.nrings + Lay::NRT - 1) / Lay::NRT, (p.NB / 2) * (p.Mst1 ? p.nseg : 1),
             p.nhalf * p.batch);
-  kern<<<grid, Lay::NT, Lay::total, s>>>(p);
-  return cudaGetLastError();
+  return launch_chained(kern, grid, dim3(Lay::NT), Lay::total, s, p);
 }
 
 template <typename Real, int T, bool VST, bool SYM>

@@ -112,6 +112,7 @@ __device__ __forceinline__ void reg_dft(typename C2<Real>::t* buf, const FFTDesc
 template <typename Real, int LOGM, int NBUF>
 __global__ void __launch_bounds__(LOGM ? (1 << LOGM) / 16 : 512, reg_min_blocks<Real>(LOGM))
     inv_rows_kernel(RowsParams<Real> p) {
+  chain_enter();
   using R2 = typename C2<Real>::t;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R2* s = reinterpret_cast<R2*>(smem_raw);
@@ -287,6 +288,7 @@ __device__ __forceinline__ void store_spectra(const RowsParams<Real>& p, int b, 
 template <typename Real, int LOGM, int NBUF>
 __global__ void __launch_bounds__(LOGM ? (1 << LOGM) / 16 : 512, reg_min_blocks<Real>(LOGM))
     fwd_rows_kernel(RowsParams<Real> p) {
+  chain_enter();
   using R2 = typename C2<Real>::t;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R2* s = reinterpret_cast<R2*>(smem_raw);
@@ -524,6 +526,7 @@ __device__ __forceinline__ void cols_emit(const ColsParams<Real>& p, int b, int 
 template <typename Real, int LOGM, int NBUF>
 __global__ void __launch_bounds__(LOGM ? (1 << LOGM) / 16 : 512, reg_min_blocks<Real>(LOGM))
     mw_cols_kernel(ColsParams<Real> p) {
+  chain_enter();
   using R2 = typename C2<Real>::t;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const FFTDesc d1 = *p.d1;
@@ -624,6 +627,7 @@ __global__ void __launch_bounds__(LOGM ? (1 << LOGM) / 16 : 512, reg_min_blocks<
 template <typename Real, int LOGM, int NBUF>
 __global__ void __launch_bounds__((1 << LOGM) / 16, reg_min_blocks<Real>(LOGM))
     mw_cols_pair_kernel(ColsParams<Real> p) {
+  chain_enter();
   using R2 = typename C2<Real>::t;
   using RF = RegFFT<LOGM, NBUF>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -849,8 +853,7 @@ static cudaError_t launch_fft_kernel(Kernel k, dim3 grid, int threads, size_t sm
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, carveout);
   if (e != cudaSuccess) return e;
-  k<<<grid, threads, smem, s>>>(p);
-  return cudaGetLastError();
+  return launch_chained(k, grid, dim3(threads), smem, s, p);
 }
 
 template <typename Real, int LOGM>

@@ -7,6 +7,7 @@
 
 #include <cstdint>
 #include <type_traits>
+#include <utility>
 
 namespace s2b {
 
@@ -129,6 +130,32 @@ __device__ __forceinline__ void cp_async_commit() {
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Programmatic dependent launch along a stream's chain of kernels: a kernel launched by
+// launch_chained may have its CTAs made resident while its predecessor's last CTAs still run.
+// Every such kernel calls chain_enter() before its first global-memory access: it lets the
+// next kernel of the chain launch and then waits until the predecessor has completed and its
+// writes are visible (without the launch attribute both are no-ops).
+__device__ __forceinline__ void chain_enter() {
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_chained(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                                  cudaStream_t s, Args&&... args) {
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
 // Bounded wait for the phase with the given parity; false when it ran out.

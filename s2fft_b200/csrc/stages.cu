@@ -10,6 +10,7 @@
 #include <cstdint>
 #include <type_traits>
 
+#include "s2b_dev.h"
 #include "s2b_internal.h"
 #include "s2b_stages.h"
 
@@ -162,6 +163,7 @@ __device__ __forceinline__ void zero_ftm_rows(const StageParams& p, int cta, int
 // with zero_ftm the tile CTAs also clear ftm.
 template <typename Real>
 __global__ void __launch_bounds__(256) prologue_tiled_kernel(StageParams p) {
+  chain_enter();
   using R2 = R2_t<Real>;
   using R4 = R4_t<Real>;
   __shared__ R2 ta[32][33], tc[32][33];  // [q][m]: flm at +m and at -m, padded
@@ -367,6 +369,7 @@ __global__ void epilogue_kernel(StageParams p) {
 // threads on consecutive m. grid (ceil((2L-1)/32), ceil(L/32), batch), 32 x 8 threads.
 template <typename Real>
 __global__ void __launch_bounds__(256) epilogue_tiled_kernel(StageParams p) {
+  chain_enter();
   using R2 = R2_t<Real>;
   __shared__ R2 tile[32][33];  // [c][l], padded
   const int L = p.L, W = 2 * L - 1;
@@ -452,11 +455,8 @@ cudaError_t launch_prologue(bool fp64, const StageParams& p, cudaStream_t s) {
       if (e != cudaSuccess) return e;
     }
     const dim3 grid((p.TR + 31) / 32 + q.pole_blocks, p.nclass, p.batch * p.nhalf);
-    if (fp64)
-      prologue_tiled_kernel<double><<<grid, dim3(32, 8), 0, s>>>(q);
-    else
-      prologue_tiled_kernel<float><<<grid, dim3(32, 8), 0, s>>>(q);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = fp64 ? launch_chained(prologue_tiled_kernel<double>, grid, dim3(32, 8), 0, s, q)
+                         : launch_chained(prologue_tiled_kernel<float>, grid, dim3(32, 8), 0, s, q);
     if (e == cudaSuccess && poles && !q.pole_blocks) e = launch_poles(fp64, p, s);
     return e;
   }
@@ -482,11 +482,8 @@ cudaError_t launch_prologue(bool fp64, const StageParams& p, cudaStream_t s) {
 cudaError_t launch_epilogue(bool fp64, const StageParams& p, cudaStream_t s) {
   if (p.Lp > 0 && p.batch <= 65535) {
     const dim3 grid((2 * p.L - 1 + 31) / 32, (p.L + 31) / 32, p.batch);
-    if (fp64)
-      epilogue_tiled_kernel<double><<<grid, dim3(32, 8), 0, s>>>(p);
-    else
-      epilogue_tiled_kernel<float><<<grid, dim3(32, 8), 0, s>>>(p);
-    return cudaGetLastError();
+    return fp64 ? launch_chained(epilogue_tiled_kernel<double>, grid, dim3(32, 8), 0, s, p)
+                : launch_chained(epilogue_tiled_kernel<float>, grid, dim3(32, 8), 0, s, p);
   }
   const long total = (long)p.batch * p.L * (2 * p.L - 1);
   const bool i32 = fits32(total);
