@@ -134,12 +134,13 @@ __device__ __forceinline__ void cp_async_wait() {
 
 // Programmatic dependent launch along a stream's chain of kernels: a kernel launched by
 // launch_chained may have its CTAs made resident while its predecessor's last CTAs still run.
-// Every such kernel calls chain_enter() before its first global-memory access: it lets the
-// next kernel of the chain launch and then waits until the predecessor has completed and its
-// writes are visible (without the launch attribute both are no-ops).
+// Every such kernel calls chain_enter() before its first global-memory access: it waits until
+// the predecessor has completed and its writes are visible, then lets the next kernel of the
+// chain launch, so that at most one grid waits ahead of the running one (without the launch
+// attribute both are no-ops).
 __device__ __forceinline__ void chain_enter() {
-  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
   asm volatile("griddepcontrol.wait;\n" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
 }
 
 template <typename... KArgs, typename... Args>
