@@ -922,7 +922,9 @@ def main():
             "clocks": r["clocks"],
             "e2e": {"value": r["e2e"], "unit": UNIT, "h2d_bytes_per_step": r["h2d"],
                     "d2h_bytes_per_step": r["d2h"]},
-            "gpu_launches": 8 * args.steps}
+            # per step: prologue (with the pole rows), inverse latitudinal, inverse ring FFTs,
+            # forward ring FFTs, column chain, forward latitudinal, epilogue
+            "gpu_launches": 7 * args.steps}
     if not args.profile_case and not args.no_extra and world == 1:
         line["batched_precompute"] = run_batched_precompute(torch)
         line["healpix_iter3"] = run_healpix_iter(torch)
