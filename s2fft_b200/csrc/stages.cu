@@ -173,7 +173,8 @@ __global__ void __launch_bounds__(256) prologue_tiled_kernel(StageParams p) {
   const int tx = threadIdx.x, ty = threadIdx.y;
   if (p.pole_blocks && blockIdx.x == gridDim.x - 1) {
     static_assert(sizeof(ta) >= 2 * 256 * sizeof(double), "pole reduction fits the tile");
-    if (j < 2 && half == 0) poles_block<Real>(p, j, b, ty * 32 + tx, reinterpret_cast<double*>(&ta[0][0]));
+    if (j < 2 && half == 0)
+      poles_block<Real>(p, j, b, ty * 32 + tx, reinterpret_cast<double*>(&ta[0][0]));
     return;
   }
   if (p.zero_ftm) {
